@@ -1,0 +1,207 @@
+"""ctypes mirror of include/avd.h.
+
+The structures here are byte-for-byte the C structs; `load()` binds every exported function with
+its prototype. Nothing here falls back to Python arithmetic: without the built library, `load()`
+raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libavd_b200.so"
+
+u32 = C.c_uint32
+u64 = C.c_uint64
+f32 = C.c_float
+
+
+class AvdSampleFormat(C.Structure):
+    _fields_ = [("kind", u32), ("depth", u32)]
+
+
+class AvdGeometry(C.Structure):
+    _fields_ = [
+        ("width", u32),
+        ("height", u32),
+        ("chroma", u32),
+        ("chroma_siting", u32),
+        ("input", AvdSampleFormat),
+        ("output", AvdSampleFormat),
+    ]
+
+
+class AvdPlane(C.Structure):
+    _fields_ = [("ptr", u64), ("bytes", u64), ("width", u32), ("height", u32)]
+
+
+class AvdPrefilter(C.Structure):
+    _fields_ = [("kind", u32), ("sigma_s", f32), ("sigma_r", f32), ("strength_scale", f32)]
+
+
+class AvdMotionSearch(C.Structure):
+    _fields_ = [
+        ("blksize", u32),
+        ("overlap", u32),
+        ("search_radius", u32),
+        ("max_search_escalation", u32),
+        ("pyramid_levels", u32),
+        ("estimation", u32),
+        ("refine_radius", u32),
+    ]
+
+
+class AvdMotionCompensation(C.Structure):
+    _fields_ = [("active", u32), ("search", AvdMotionSearch)]
+
+
+class AvdNlmTuning(C.Structure):
+    _fields_ = [
+        ("has_search_radius", u32),
+        ("search_radius", u32),
+        ("has_patch_radius", u32),
+        ("patch_radius", u32),
+        ("has_strength", u32),
+        ("strength", f32),
+        ("has_self_weight", u32),
+        ("self_weight", f32),
+    ]
+
+
+class AvdDenoisingMode(C.Structure):
+    _fields_ = [("temporal", u32), ("radius", u32)]
+
+
+class AvdHqParams(C.Structure):
+    _fields_ = [
+        ("auto_strength", u32),
+        ("noise_floor", u32),
+        ("has_sigma_override", u32),
+        ("sigma_override", f32),
+        ("temporal_confidence", u32),
+        ("thsad_scale", f32),
+        ("sigma_scale", f32),
+    ]
+
+
+class AvdNlmeansAlgorithm(C.Structure):
+    _fields_ = [
+        ("variant", u32),
+        ("prefilter", AvdPrefilter),
+        ("motion_compensation", AvdMotionCompensation),
+        ("tuning", AvdNlmTuning),
+        ("mode", AvdDenoisingMode),
+        ("hq", AvdHqParams),
+    ]
+
+
+class AvdNl4dOptions(C.Structure):
+    _fields_ = [
+        ("motion", AvdMotionSearch),
+        ("has_sigma", u32),
+        ("sigma", f32),
+        ("sigma_scale", f32),
+        ("thsad_scale", f32),
+        ("refine", u32),
+        ("spatial_radius", u32),
+        ("has_lambda_ht", u32),
+        ("lambda_ht", f32),
+        ("lambda_ht_scale", f32),
+        ("c_min", f32),
+        ("kaiser_beta", f32),
+        ("field_lambda", f32),
+        ("noise_map", u32),
+        ("pooled_threshold", u32),
+        ("grain_data", u32),
+        ("temporal_radius", u32),
+    ]
+
+
+class AvdEngineSpec(C.Structure):
+    _fields_ = [
+        ("kind", u32),
+        ("has_luma", u32),
+        ("has_chroma", u32),
+        ("nlm_luma", AvdNlmeansAlgorithm),
+        ("nlm_chroma", AvdNlmeansAlgorithm),
+        ("nl4d_luma", AvdNl4dOptions),
+        ("nl4d_chroma", AvdNl4dOptions),
+        ("geometry", AvdGeometry),
+    ]
+
+
+class AvdTuning(C.Structure):
+    _fields_ = [("deterministic", u32), ("reserved", u32)]
+
+
+class AvdWindowSpan(C.Structure):
+    _fields_ = [("behind", u64), ("ahead", u64), ("edges", u32), ("reserved", u32)]
+
+
+class AvdEngineTiming(C.Structure):
+    _fields_ = [("device_time", C.c_double), ("frames", u64)]
+
+
+class AvdPassTimings(C.Structure):
+    _fields_ = [("has_luma", u32), ("has_chroma", u32), ("luma", AvdEngineTiming), ("chroma", AvdEngineTiming)]
+
+
+_P = C.POINTER
+_E = C.c_void_p  # AvdEngine*
+
+# name -> (restype, argtypes); the exact set of entry points include/avd.h declares.
+PROTOTYPES: dict[str, tuple] = {
+    "avd_abi_version": (u32, []),
+    "avd_status_message": (C.c_char_p, [C.c_int]),
+    "avd_default_nlmeans": (None, [_P(AvdNlmeansAlgorithm)]),
+    "avd_default_nl4d": (None, [_P(AvdNl4dOptions)]),
+    "avd_default_motion_search": (None, [_P(AvdMotionSearch)]),
+    "avd_nlmeans_variant_for": (u32, [u32]),
+    "avd_nlmeans_temporal_radius_for": (u32, [u32]),
+    "avd_nlmeans_search_radius_for": (u32, [u32]),
+    "avd_search_escalation_for": (u32, [u32]),
+    "avd_hq_default_strength": (f32, [u32, u32]),
+    "avd_spec_validate": (C.c_int, [_P(AvdEngineSpec), C.c_char_p, C.c_size_t]),
+    "avd_spec_window_span": (C.c_int, [_P(AvdEngineSpec), _P(AvdWindowSpan)]),
+    "avd_engine_create": (C.c_int, [_P(AvdEngineSpec), _P(AvdTuning), _P(_E)]),
+    "avd_engine_destroy": (None, [_E]),
+    "avd_engine_set_stream": (C.c_int, [_E, C.c_void_p]),
+    "avd_engine_push": (C.c_int, [_E, _P(AvdPlane), C.c_size_t, _P(C.c_size_t)]),
+    "avd_engine_push_context": (C.c_int, [_E, _P(AvdPlane), C.c_size_t]),
+    "avd_engine_emit_into": (C.c_int, [_E, _P(AvdPlane), C.c_size_t]),
+    "avd_engine_finish": (C.c_int, [_E, _P(C.c_size_t)]),
+    "avd_engine_reset": (C.c_int, [_E]),
+    "avd_engine_window_span": (C.c_int, [_E, _P(AvdWindowSpan)]),
+    "avd_engine_max_held_frames": (C.c_int, [_E, _P(C.c_size_t)]),
+    "avd_engine_timing": (C.c_int, [_E, _P(AvdPassTimings)]),
+    "avd_engine_sample_device_time": (C.c_int, [_E, u32]),
+    "avd_engine_last_error": (C.c_char_p, [_E]),
+    "avd_engine_fail_for_test": (C.c_int, [_E]),
+    "avd_last_error": (C.c_char_p, []),
+}
+
+_lib: C.CDLL | None = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Loads libavd_b200.so and binds every prototype; raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"libavd_b200.so is not built ({p}); run `python av-denoise_b200/build.py` or "
+            "`__graft_entry__.build()` first. There is no CPU fallback."
+        )
+    lib = C.CDLL(str(p))
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib

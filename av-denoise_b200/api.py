@@ -1,0 +1,589 @@
+"""Python mirror of av-denoise-core's public engine API, over the C ABI of libavd_b200.
+
+Names, defaults and error behaviour follow the Rust crate (av-denoise-core/src/lib.rs:27-92):
+`EngineSpec`, `Geometry`, `SampleFormat`, `ChromaLayout`, `DevicePlane`, `NlmeansAlgorithm`,
+`NlmeansOptions`, `NlmeansHqOptions`, `HqParams`, `NlmTuning`, `DenoisingMode`, `Nl4dOptions`,
+`MotionSearch`, `MotionEstimation`, `MotionCompensationMode`, `PrefilterMode`, `Preset`,
+`build_engine`, and an `Engine` with push / push_context / emit_into / finish / reset.
+Errors are raised as the `Error` variants of av-denoise-core/src/error.rs:3-19.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+from . import _abi
+
+# ---- errors (av-denoise-core/src/error.rs:3-19) ------------------------------------------------
+
+
+class AvdError(Exception):
+    status = -1
+
+
+class InvalidOptions(AvdError):
+    status = 1
+
+
+class InvalidGeometry(AvdError):
+    status = 2
+
+
+class PlaneMismatch(AvdError):
+    status = 3
+
+
+class OutputsPending(AvdError):
+    status = 4
+
+
+class NothingToEmit(AvdError):
+    status = 5
+
+
+class ContextAfterPush(AvdError):
+    status = 6
+
+
+class NeedsReset(AvdError):
+    status = 7
+
+
+class GpuError(AvdError):
+    status = 8
+
+
+_ERRORS = {c.status: c for c in (InvalidOptions, InvalidGeometry, PlaneMismatch, OutputsPending, NothingToEmit,
+                                 ContextAfterPush, NeedsReset, GpuError)}
+
+
+def _raise(status: int, message: str) -> None:
+    if status == 0:
+        return
+    cls = _ERRORS.get(status, AvdError)
+    raise cls(message or _abi.load().avd_status_message(status).decode())
+
+
+# ---- geometry ----------------------------------------------------------------------------------
+
+
+class ChromaLayout(enum.IntEnum):
+    """engine/frame.rs:386-397."""
+
+    GRAY = 0
+    YUV420 = 1
+    YUV422 = 2
+    YUV444 = 3
+
+    def plane_count(self) -> int:
+        return 1 if self == ChromaLayout.GRAY else 3
+
+    def chroma_dims(self, width: int, height: int) -> Optional[tuple[int, int]]:
+        if self == ChromaLayout.GRAY:
+            return None
+        if self == ChromaLayout.YUV420:
+            return (width + 1) // 2, (height + 1) // 2
+        if self == ChromaLayout.YUV422:
+            return (width + 1) // 2, height
+        return width, height
+
+
+class ChromaSiting(enum.IntEnum):
+    LEFT = 0
+    CENTER = 1
+    TOP_LEFT = 2
+    UNKNOWN = 3
+
+
+@dataclass(frozen=True)
+class SampleFormat:
+    """engine/plane.rs:8-17: `U8`, `U16 { depth }` or `F32`."""
+
+    kind: int
+    depth: int = 0
+
+    @staticmethod
+    def u8() -> "SampleFormat":
+        return SampleFormat(0, 8)
+
+    @staticmethod
+    def u16(depth: int) -> "SampleFormat":
+        return SampleFormat(1, depth)
+
+    @staticmethod
+    def f32() -> "SampleFormat":
+        return SampleFormat(2, 0)
+
+    def max_value(self) -> float:
+        return {0: 255.0, 1: float((1 << self.depth) - 1), 2: 1.0}[self.kind]
+
+    def samples_per_word(self) -> int:
+        return {0: 4, 1: 2, 2: 1}[self.kind]
+
+    def plane_bytes(self, pixels: int) -> int:
+        spw = self.samples_per_word()
+        return (pixels + spw - 1) // spw * 4
+
+    def _c(self) -> _abi.AvdSampleFormat:
+        return _abi.AvdSampleFormat(self.kind, self.depth if self.kind == 1 else 0)
+
+
+@dataclass
+class Geometry:
+    """engine/frame.rs:446-459."""
+
+    width: int
+    height: int
+    chroma: ChromaLayout = ChromaLayout.YUV420
+    input: SampleFormat = field(default_factory=SampleFormat.u8)
+    output: SampleFormat = field(default_factory=SampleFormat.u8)
+    chroma_siting: ChromaSiting = ChromaSiting.UNKNOWN
+
+    def plane_dims(self, index: int) -> tuple[int, int]:
+        if index == 0:
+            return self.width, self.height
+        dims = ChromaLayout(self.chroma).chroma_dims(self.width, self.height)
+        return dims if dims else (self.width, self.height)
+
+    def plane_count(self) -> int:
+        return ChromaLayout(self.chroma).plane_count()
+
+    def _c(self) -> _abi.AvdGeometry:
+        return _abi.AvdGeometry(self.width, self.height, int(self.chroma), int(self.chroma_siting), self.input._c(),
+                                self.output._c())
+
+
+@dataclass
+class DevicePlane:
+    """engine/plane.rs:265-297: a borrowed, packed device plane (stride = width, whole words)."""
+
+    ptr: int
+    bytes: int
+    width: int
+    height: int
+
+    @staticmethod
+    def from_tensor(t, width: int, height: int) -> "DevicePlane":
+        """Borrows a contiguous CUDA torch tensor as a plane."""
+        if not t.is_cuda or not t.is_contiguous():
+            raise PlaneMismatch("a device plane must be a contiguous CUDA tensor")
+        return DevicePlane(t.data_ptr(), t.numel() * t.element_size(), width, height)
+
+    def _c(self) -> _abi.AvdPlane:
+        return _abi.AvdPlane(self.ptr, self.bytes, self.width, self.height)
+
+
+# ---- options ------------------------------------------------------------------------------------
+
+
+class Preset(enum.IntEnum):
+    """options.rs:151-165."""
+
+    VERYFAST = 0
+    FAST = 1
+    BASE = 2
+    SLOW = 3
+    VERYSLOW = 4
+
+
+class NlmeansVariant(enum.IntEnum):
+    FAST = 0
+    HQ = 1
+
+
+def nlmeans_variant_for(preset: Preset) -> NlmeansVariant:
+    return NlmeansVariant(_abi.load().avd_nlmeans_variant_for(int(preset)))
+
+
+def nlmeans_temporal_radius_for(preset: Preset) -> int:
+    return int(_abi.load().avd_nlmeans_temporal_radius_for(int(preset)))
+
+
+def nlmeans_search_radius_for(preset: Preset) -> int:
+    return int(_abi.load().avd_nlmeans_search_radius_for(int(preset)))
+
+
+def search_escalation_for(preset: Preset) -> Optional[int]:
+    v = int(_abi.load().avd_search_escalation_for(int(preset)))
+    return v or None
+
+
+def hq_default_strength(channels: int, temporal_radius: int) -> float:
+    """nlmeans/params.rs:27-33; channels 1 = luma, 2 = chroma."""
+    return float(_abi.load().avd_hq_default_strength(channels, temporal_radius))
+
+
+@dataclass
+class PrefilterMode:
+    """nlmeans/prefilter/mod.rs:15-26: kind 0 None, 1 Bilateral, 2 NlmSpatial."""
+
+    kind: int = 0
+    sigma_s: float = 0.0
+    sigma_r: float = 0.0
+    strength_scale: float = 0.0
+
+    @staticmethod
+    def none() -> "PrefilterMode":
+        return PrefilterMode()
+
+    @staticmethod
+    def bilateral(sigma_s: float, sigma_r: float) -> "PrefilterMode":
+        return PrefilterMode(1, sigma_s, sigma_r, 0.0)
+
+    @staticmethod
+    def nlm_spatial(strength_scale: float = 0.4) -> "PrefilterMode":
+        return PrefilterMode(2, 0.0, 0.0, strength_scale)
+
+    def _c(self) -> _abi.AvdPrefilter:
+        return _abi.AvdPrefilter(self.kind, self.sigma_s, self.sigma_r, self.strength_scale)
+
+
+class MotionEstimation(enum.IntEnum):
+    AUTO = 0
+    DIRECT = 1
+    CHAINED = 2
+
+
+@dataclass
+class MotionSearch:
+    """motion/search.rs:5-44."""
+
+    blksize: int = 16
+    overlap: int = 8
+    search_radius: int = 4
+    max_search_escalation: int = 4
+    pyramid_levels: int = 2
+    estimation: MotionEstimation = MotionEstimation.AUTO
+    refine_radius: int = 2
+
+    def _c(self) -> _abi.AvdMotionSearch:
+        return _abi.AvdMotionSearch(self.blksize, self.overlap, self.search_radius, self.max_search_escalation,
+                                    self.pyramid_levels, int(self.estimation), self.refine_radius)
+
+
+@dataclass
+class MotionCompensationMode:
+    """motion/search.rs:58-89: `None` (search is None) or `Mvtools { .. }`."""
+
+    search: Optional[MotionSearch] = None
+
+    def _c(self) -> _abi.AvdMotionCompensation:
+        s = self.search or MotionSearch()
+        return _abi.AvdMotionCompensation(1 if self.search else 0, s._c())
+
+
+@dataclass
+class NlmTuning:
+    """nlmeans/options.rs:94-101."""
+
+    search_radius: Optional[int] = None
+    patch_radius: Optional[int] = None
+    strength: Optional[float] = None
+    self_weight: Optional[float] = None
+
+    def _c(self) -> _abi.AvdNlmTuning:
+        def h(v):
+            return (0, 0) if v is None else (1, v)
+
+        sr, pr, st, sw = h(self.search_radius), h(self.patch_radius), h(self.strength), h(self.self_weight)
+        return _abi.AvdNlmTuning(sr[0], sr[1], pr[0], pr[1], st[0], float(st[1]), sw[0], float(sw[1]))
+
+
+@dataclass
+class DenoisingMode:
+    """nlmeans/options.rs:84-92: `Spacial` (radius None) or `Temporal { radius }`."""
+
+    radius: Optional[int] = None
+
+    @staticmethod
+    def spacial() -> "DenoisingMode":
+        return DenoisingMode(None)
+
+    @staticmethod
+    def temporal(radius: int) -> "DenoisingMode":
+        return DenoisingMode(radius)
+
+    def _c(self) -> _abi.AvdDenoisingMode:
+        return _abi.AvdDenoisingMode(0 if self.radius is None else 1, self.radius or 0)
+
+
+@dataclass
+class HqParams:
+    """nlmeans/params.rs:113-158."""
+
+    auto_strength: bool = True
+    noise_floor: bool = True
+    sigma_override: Optional[float] = None
+    temporal_confidence: bool = True
+    thsad_scale: float = 1.0
+    sigma_scale: float = 1.0
+
+    @staticmethod
+    def with_sigma(sigma: float) -> "HqParams":
+        return HqParams(sigma_override=sigma)
+
+    def _c(self) -> _abi.AvdHqParams:
+        return _abi.AvdHqParams(int(self.auto_strength), int(self.noise_floor), int(self.sigma_override is not None),
+                                float(self.sigma_override or 0.0), int(self.temporal_confidence), self.thsad_scale,
+                                self.sigma_scale)
+
+
+@dataclass
+class NlmeansOptions:
+    """nlmeans/options.rs:4-20."""
+
+    prefilter: PrefilterMode = field(default_factory=PrefilterMode)
+    motion_compensation: MotionCompensationMode = field(default_factory=MotionCompensationMode)
+    tuning: NlmTuning = field(default_factory=NlmTuning)
+    mode: DenoisingMode = field(default_factory=DenoisingMode)
+
+
+@dataclass
+class NlmeansHqOptions:
+    """nlmeans/options.rs:22-29."""
+
+    nlm: NlmeansOptions = field(default_factory=NlmeansOptions)
+    hq: HqParams = field(default_factory=HqParams)
+
+
+@dataclass
+class NlmeansAlgorithm:
+    """nlmeans/options.rs:41-46: `Fast(NlmeansOptions)` or `Hq(NlmeansHqOptions)`."""
+
+    variant: NlmeansVariant
+    options: NlmeansOptions
+    hq: HqParams = field(default_factory=HqParams)
+
+    @staticmethod
+    def fast(options: NlmeansOptions) -> "NlmeansAlgorithm":
+        return NlmeansAlgorithm(NlmeansVariant.FAST, options)
+
+    @staticmethod
+    def hq_(options: NlmeansHqOptions) -> "NlmeansAlgorithm":
+        return NlmeansAlgorithm(NlmeansVariant.HQ, options.nlm, options.hq)
+
+    def _c(self) -> _abi.AvdNlmeansAlgorithm:
+        o = self.options
+        return _abi.AvdNlmeansAlgorithm(int(self.variant), o.prefilter._c(), o.motion_compensation._c(),
+                                        o.tuning._c(), o.mode._c(), self.hq._c())
+
+
+@dataclass
+class Nl4dOptions:
+    """nl4d/options.rs:11-92."""
+
+    motion: MotionSearch = field(default_factory=MotionSearch)
+    sigma: Optional[float] = None
+    sigma_scale: float = 1.0
+    thsad_scale: float = 1.0
+    refine: int = 2
+    spatial_radius: int = 9
+    lambda_ht: Optional[float] = None
+    lambda_ht_scale: float = 1.0
+    c_min: float = 0.05
+    kaiser_beta: float = 2.0
+    field_lambda: float = 1.0
+    noise_map: bool = True
+    pooled_threshold: bool = True
+    grain_data: bool = False
+    temporal_radius: int = 2
+
+    def _c(self) -> _abi.AvdNl4dOptions:
+        return _abi.AvdNl4dOptions(self.motion._c(), int(self.sigma is not None), float(self.sigma or 0.0),
+                                   self.sigma_scale, self.thsad_scale, self.refine, self.spatial_radius,
+                                   int(self.lambda_ht is not None), float(self.lambda_ht or 0.0),
+                                   self.lambda_ht_scale, self.c_min, self.kaiser_beta, self.field_lambda,
+                                   int(self.noise_map), int(self.pooled_threshold), int(self.grain_data),
+                                   self.temporal_radius)
+
+
+@dataclass
+class EngineSpec:
+    """engine/spec.rs:146-157: `Nlmeans { luma, chroma, geometry }` or `Nl4d { .. }`."""
+
+    kind: int
+    geometry: Geometry
+    luma: object = None
+    chroma: object = None
+
+    @staticmethod
+    def nlmeans(luma: Optional[NlmeansAlgorithm], chroma: Optional[NlmeansAlgorithm],
+                geometry: Geometry) -> "EngineSpec":
+        return EngineSpec(0, geometry, luma, chroma)
+
+    @staticmethod
+    def nl4d(luma: Optional[Nl4dOptions], chroma: Optional[Nl4dOptions], geometry: Geometry) -> "EngineSpec":
+        return EngineSpec(1, geometry, luma, chroma)
+
+    def _c(self) -> _abi.AvdEngineSpec:
+        s = _abi.AvdEngineSpec()
+        s.kind = self.kind
+        s.has_luma = int(self.luma is not None)
+        s.has_chroma = int(self.chroma is not None)
+        lib = _abi.load()
+        lib.avd_default_nlmeans(C.byref(s.nlm_luma))
+        lib.avd_default_nlmeans(C.byref(s.nlm_chroma))
+        lib.avd_default_nl4d(C.byref(s.nl4d_luma))
+        lib.avd_default_nl4d(C.byref(s.nl4d_chroma))
+        if self.kind == 0:
+            if self.luma is not None:
+                s.nlm_luma = self.luma._c()
+            if self.chroma is not None:
+                s.nlm_chroma = self.chroma._c()
+        else:
+            if self.luma is not None:
+                s.nl4d_luma = self.luma._c()
+            if self.chroma is not None:
+                s.nl4d_chroma = self.chroma._c()
+        s.geometry = self.geometry._c()
+        return s
+
+    def validate(self) -> None:
+        """engine/spec.rs:291-345 plus the per-pass build checks; raises the matching error."""
+        lib = _abi.load()
+        buf = C.create_string_buffer(1024)
+        st = lib.avd_spec_validate(C.byref(self._c()), buf, 1024)
+        _raise(st, buf.value.decode())
+
+    def window_span(self) -> "WindowSpan":
+        out = _abi.AvdWindowSpan()
+        _raise(_abi.load().avd_spec_window_span(C.byref(self._c()), C.byref(out)), "")
+        return WindowSpan(out.behind, out.ahead, "shifted" if out.edges else "repeat")
+
+    def max_held_frames(self) -> int:
+        return self.window_span().behind
+
+
+@dataclass
+class WindowSpan:
+    """engine/mod.rs:40-62."""
+
+    behind: int
+    ahead: int
+    edges: str
+
+    def frame_count(self) -> int:
+        return self.behind + 1 + self.ahead
+
+
+@dataclass
+class EngineTiming:
+    device_time: float
+    frames: int
+
+
+@dataclass
+class PassTimings:
+    luma: Optional[EngineTiming]
+    chroma: Optional[EngineTiming]
+
+
+# ---- engine -------------------------------------------------------------------------------------
+
+
+def _planes(planes: Sequence[DevicePlane]):
+    arr = (_abi.AvdPlane * max(1, len(planes)))()
+    for i, p in enumerate(planes):
+        arr[i] = p._c()
+    return arr, len(planes)
+
+
+class Engine:
+    """engine/mod.rs:158-211 (`Engine`), through the C ABI."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        self._lib = _abi.load()
+
+    def _check(self, status: int) -> None:
+        if status:
+            msg = self._lib.avd_engine_last_error(self._h)
+            _raise(status, msg.decode() if msg else "")
+
+    def set_stream(self, stream: int) -> None:
+        """Queues every later call on CUDA stream `stream` (a `cudaStream_t` as an int)."""
+        self._check(self._lib.avd_engine_set_stream(self._h, C.c_void_p(stream)))
+
+    def push(self, planes: Sequence[DevicePlane]) -> int:
+        arr, n = _planes(planes)
+        ready = C.c_size_t(0)
+        self._check(self._lib.avd_engine_push(self._h, arr, n, C.byref(ready)))
+        return ready.value
+
+    def push_context(self, planes: Sequence[DevicePlane]) -> None:
+        arr, n = _planes(planes)
+        self._check(self._lib.avd_engine_push_context(self._h, arr, n))
+
+    def emit_into(self, planes: Sequence[DevicePlane]) -> None:
+        arr, n = _planes(planes)
+        self._check(self._lib.avd_engine_emit_into(self._h, arr, n))
+
+    def finish(self) -> int:
+        tail = C.c_size_t(0)
+        self._check(self._lib.avd_engine_finish(self._h, C.byref(tail)))
+        return tail.value
+
+    def reset(self) -> None:
+        self._check(self._lib.avd_engine_reset(self._h))
+
+    def window_span(self) -> WindowSpan:
+        out = _abi.AvdWindowSpan()
+        self._check(self._lib.avd_engine_window_span(self._h, C.byref(out)))
+        return WindowSpan(out.behind, out.ahead, "shifted" if out.edges else "repeat")
+
+    def max_held_frames(self) -> int:
+        out = C.c_size_t(0)
+        self._check(self._lib.avd_engine_max_held_frames(self._h, C.byref(out)))
+        return out.value
+
+    def timing(self) -> PassTimings:
+        out = _abi.AvdPassTimings()
+        self._check(self._lib.avd_engine_timing(self._h, C.byref(out)))
+        luma = EngineTiming(out.luma.device_time, out.luma.frames) if out.has_luma else None
+        chroma = EngineTiming(out.chroma.device_time, out.chroma.frames) if out.has_chroma else None
+        return PassTimings(luma, chroma)
+
+    def sample_device_time(self, every: int) -> None:
+        self._check(self._lib.avd_engine_sample_device_time(self._h, every))
+
+    def fail_for_test(self) -> None:
+        self._check(self._lib.avd_engine_fail_for_test(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.avd_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+@dataclass
+class TuningConfig:
+    """tune/setup.rs (`TuningConfig`): kept for API parity."""
+
+    deterministic: bool = True
+
+
+def build_engine(spec: EngineSpec, tuning: Optional[TuningConfig] = None) -> Engine:
+    """tune/setup.rs:79-91 (`build_engine`): validates, then builds on the current CUDA device."""
+    lib = _abi.load()
+    t = _abi.AvdTuning(int((tuning or TuningConfig()).deterministic), 0)
+    h = C.c_void_p()
+    st = lib.avd_engine_create(C.byref(spec._c()), C.byref(t), C.byref(h))
+    if st:
+        msg = lib.avd_last_error()
+        _raise(st, msg.decode() if msg else "")
+    return Engine(h)

@@ -1,0 +1,791 @@
+// The engine behind the C ABI: a planar engine (luma pass, chroma pass, passthrough ring) over
+// per-plane-group passes, mirroring av-denoise-core's engine layer:
+//   - PlanarEngine  <- engine/planar.rs:104-580
+//   - NlmPass       <- nlmeans/engine.rs:29-318 with the NlmDenoiser ring of
+//                      nlmeans/denoiser/{mod.rs,ring.rs,stages.rs}
+// Host state (ring head, loaded frames, ready slot, tail, poison flag) follows the reference
+// step for step; the GPU work is queued on the caller's stream with no host synchronisation on
+// the push / emit path.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <optional>
+#include <string>
+#include <vector>
+
+#include "avd_internal.h"
+#include "kernels.h"
+
+namespace avd {
+
+namespace {
+
+// Error carried out of a call: a status plus its message.
+struct Failure {
+    AvdStatus status;
+    std::string message;
+};
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() {
+        if (ptr) cudaFree(ptr);
+    }
+    cudaError_t alloc(size_t n) {
+        bytes = n;
+        return cudaMalloc(&ptr, n ? n : 4);
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(ptr);
+    }
+};
+
+std::string cuda_message(const char* what, cudaError_t e) {
+    return std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+}
+
+PlaneFormat plane_format(const AvdSampleFormat& f) {
+    PlaneFormat p;
+    p.kind = static_cast<int>(f.kind);
+    p.samples_per_word = static_cast<int>(samples_per_word(f));
+    p.max_value = sample_max_value(f);
+    return p;
+}
+
+// Timing of one pass: CUDA events around sampled frames (engine/timing.rs:22-70).
+struct DeviceTimer {
+    uint32_t every = 0;
+    uint64_t frame_counter = 0;
+    double total = 0.0;
+    uint64_t frames = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+
+    ~DeviceTimer() {
+        for (auto& p : pending) {
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+    }
+    bool begin(cudaStream_t s, cudaEvent_t* start) {
+        uint64_t n = frame_counter++;
+        if (every == 0 || n % every != 0) return false;
+        cudaEventCreate(start);
+        cudaEventRecord(*start, s);
+        return true;
+    }
+    void end(cudaStream_t s, cudaEvent_t start) {
+        cudaEvent_t stop;
+        cudaEventCreate(&stop);
+        cudaEventRecord(stop, s);
+        pending.emplace_back(start, stop);
+    }
+    AvdEngineTiming collect() {
+        for (auto& p : pending) {
+            float ms = 0.0f;
+            if (cudaEventSynchronize(p.second) == cudaSuccess && cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) {
+                total += ms * 1e-3;
+                frames += 1;
+            }
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+        pending.clear();
+        AvdEngineTiming t;
+        t.device_time = total;
+        t.frames = frames;
+        return t;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// A pass over one plane group.
+class Pass {
+   public:
+    virtual ~Pass() = default;
+    virtual std::optional<Failure> push(const AvdPlane* planes, size_t* ready) = 0;
+    virtual std::optional<Failure> push_context(const AvdPlane* planes) = 0;
+    virtual std::optional<Failure> emit_into(const AvdPlane* planes) = 0;
+    virtual std::optional<Failure> finish(size_t* tail) = 0;
+    virtual void reset() = 0;
+    virtual size_t max_held_frames() const = 0;
+    virtual AvdWindowSpan window_span() const = 0;
+    virtual uint32_t next_frame() const = 0;
+    virtual std::optional<uint32_t> emitted_frame() const = 0;
+    virtual AvdEngineTiming timing() = 0;
+    virtual void sample_device_time(uint32_t every) = 0;
+    virtual std::optional<Failure> fail_for_test() = 0;
+    cudaStream_t stream = nullptr;
+};
+
+// ---------------------------------------------------------------------------------------------
+// NLMeans pass: nlmeans/engine.rs:29-318 over the ring of nlmeans/denoiser/mod.rs:40-591.
+class NlmPass final : public Pass {
+   public:
+    static std::optional<Failure> create(const AvdNlmeansAlgorithm& alg, Channels channels, uint32_t width,
+                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
+                                         std::unique_ptr<Pass>* result) {
+        auto pass = std::unique_ptr<NlmPass>(new NlmPass());
+        pass->params_ = resolve_nlm_params(alg, channels);
+        pass->held_ = nlm_held_frames(alg, channels);
+        pass->width_ = width;
+        pass->height_ = height;
+        pass->in_ = in;
+        pass->out_ = out;
+        const NlmParams& p = pass->params_;
+        if (p.hq && !p.hq_params.has_sigma_override)
+            return Failure{AVD_ERR_INVALID_OPTIONS,
+                           "NLMeans-HQ with the automatic noise estimate is not available in this build yet; set "
+                           "hq.sigma_override"};
+        if (p.prefilter.kind != AVD_PREFILTER_NONE)
+            return Failure{AVD_ERR_INVALID_OPTIONS, "prefilters are not available in this build"};
+        if (p.motion.active && p.temporal_radius > 0)
+            return Failure{AVD_ERR_INVALID_OPTIONS, "NLMeans motion compensation is not available in this build"};
+        if (p.hq && p.hq_params.temporal_confidence && p.temporal_radius > 0)
+            return Failure{AVD_ERR_INVALID_OPTIONS,
+                           "NLMeans-HQ temporal confidence is not available in this build yet; set "
+                           "hq.temporal_confidence = false"};
+        if (auto f = pass->allocate()) return f;
+        *result = std::move(pass);
+        return std::nullopt;
+    }
+
+    std::optional<Failure> push(const AvdPlane* planes, size_t* ready) override {
+        if (poisoned_) return Failure{AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET)};
+        if (ready_slot_ >= 0 || tail_remaining_ > 0)
+            return Failure{AVD_ERR_OUTPUTS_PENDING, avd_status_message(AVD_ERR_OUTPUTS_PENDING)};
+        if (auto f = check_planes(planes, in_)) return f;
+        if (auto f = guard(push_planes(planes))) return f;
+        pushed_ = true;
+        int slot = -1;
+        if (auto f = guard(denoise_submit(&slot))) return f;
+        ready_slot_ = slot;
+        *ready = slot >= 0 ? 1 : 0;
+        return std::nullopt;
+    }
+
+    std::optional<Failure> push_context(const AvdPlane* planes) override {
+        if (poisoned_) return Failure{AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET)};
+        if (ready_slot_ >= 0 || tail_remaining_ > 0)
+            return Failure{AVD_ERR_OUTPUTS_PENDING, avd_status_message(AVD_ERR_OUTPUTS_PENDING)};
+        if (auto f = check_planes(planes, in_)) return f;
+        if (pushed_) return Failure{AVD_ERR_CONTEXT_AFTER_PUSH, avd_status_message(AVD_ERR_CONTEXT_AFTER_PUSH)};
+        return guard(push_planes(planes));
+    }
+
+    std::optional<Failure> emit_into(const AvdPlane* planes) override {
+        if (poisoned_) return Failure{AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET)};
+        if (auto f = check_planes(planes, out_)) return f;
+        if (ready_slot_ >= 0) {
+            int slot = ready_slot_;
+            ready_slot_ = -1;
+            emitted_ = centre_frame();
+            return guard(write_out(slot, planes));
+        }
+        if (tail_remaining_ == 0) return Failure{AVD_ERR_NOTHING_TO_EMIT, avd_status_message(AVD_ERR_NOTHING_TO_EMIT)};
+        int slot = -1;
+        if (auto f = guard(next_tail_frame(&slot))) return f;
+        emitted_ = centre_frame();
+        if (auto f = guard(write_out(slot, planes))) return f;
+        tail_remaining_ -= 1;
+        if (tail_remaining_ == 0) restart_stream();
+        return std::nullopt;
+    }
+
+    std::optional<Failure> finish(size_t* tail) override {
+        if (poisoned_) return Failure{AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET)};
+        if (ready_slot_ >= 0 || tail_remaining_ > 0)
+            return Failure{AVD_ERR_OUTPUTS_PENDING, avd_status_message(AVD_ERR_OUTPUTS_PENDING)};
+        // nlmeans/denoiser/mod.rs:538-545 (`flush_target`).
+        tail_remaining_ = std::min<size_t>(real_pushes_, params_.temporal_radius);
+        if (tail_remaining_ == 0) restart_stream();
+        *tail = tail_remaining_;
+        return std::nullopt;
+    }
+
+    void reset() override {
+        ready_slot_ = -1;
+        emitted_.reset();
+        tail_remaining_ = 0;
+        poisoned_ = false;
+        restart_stream();
+    }
+
+    size_t max_held_frames() const override { return held_; }
+
+    AvdWindowSpan window_span() const override {
+        AvdWindowSpan s{};
+        s.behind = held_;
+        s.ahead = held_;
+        s.edges = 0;
+        return s;
+    }
+
+    uint32_t next_frame() const override { return static_cast<uint32_t>(real_pushes_); }
+    std::optional<uint32_t> emitted_frame() const override { return emitted_; }
+    AvdEngineTiming timing() override { return timer_.collect(); }
+    void sample_device_time(uint32_t every) override { timer_.every = every; }
+    std::optional<Failure> fail_for_test() override {
+        poisoned_ = true;
+        return Failure{AVD_ERR_GPU, "forced failure"};
+    }
+
+   private:
+    NlmPass() = default;
+
+    size_t pixels() const { return static_cast<size_t>(width_) * height_; }
+    size_t frame_elems() const { return pixels() * params_.channel_count(); }
+    uint32_t total_frames() const { return params_.total_frames(); }
+
+    std::optional<Failure> allocate() {
+        const size_t fe = frame_elems();
+        cudaError_t e;
+        if ((e = ring_.alloc(fe * total_frames() * sizeof(float))) != cudaSuccess) return gpu_failure("ring", e);
+        for (auto& o : outputs_)
+            if ((e = o.alloc(fe * sizeof(float))) != cudaSuccess) return gpu_failure("output slot", e);
+        if ((e = derived_.alloc(16 * sizeof(float))) != cudaSuccess) return gpu_failure("derived words", e);
+        // Fixed derived words (nlmeans/denoiser/noise.rs `fixed_derived_values`): the strength and,
+        // with an HQ sigma override, the noise offset.
+        float words[16] = {0};
+        const bool has_sigma = params_.hq && params_.hq_params.has_sigma_override;
+        const float sigma = params_.hq_params.sigma_override;
+        words[0] = h2_inv_norm_with(params_, has_sigma, sigma);
+        float sig[2] = {sigma, sigma};
+        words[1] = has_sigma ? noise_offset_with(params_, sig, 2) : 0.0f;
+        if ((e = cudaMemcpy(derived_.ptr, words, sizeof(words), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return gpu_failure("derived upload", e);
+        slot_frames_.assign(total_frames(), 0u);
+        return std::nullopt;
+    }
+
+    static Failure gpu_failure(const char* what, cudaError_t e) { return Failure{AVD_ERR_GPU, cuda_message(what, e)}; }
+
+    std::optional<Failure> guard(std::optional<Failure> f) {
+        if (f && f->status == AVD_ERR_GPU) poisoned_ = true;
+        return f;
+    }
+
+    std::optional<Failure> check_planes(const AvdPlane* planes, const AvdSampleFormat& fmt) const {
+        // engine/plane.rs:348-377 (`check_planes`); the planar engine already checked the count.
+        const uint64_t need = plane_bytes(fmt, pixels());
+        for (uint32_t i = 0; i < params_.channel_count(); ++i) {
+            const AvdPlane& p = planes[i];
+            if (p.width != width_ || p.height != height_) {
+                char m[160];
+                std::snprintf(m, sizeof(m), "plane %u is %ux%u, expected %ux%u", i, p.width, p.height, width_, height_);
+                return Failure{AVD_ERR_PLANE_MISMATCH, m};
+            }
+            if (p.bytes < need) {
+                char m[160];
+                std::snprintf(m, sizeof(m), "plane %u handle holds %llu bytes, needs %llu", i,
+                              (unsigned long long)p.bytes, (unsigned long long)need);
+                return Failure{AVD_ERR_PLANE_MISMATCH, m};
+            }
+            if (p.ptr == 0) return Failure{AVD_ERR_PLANE_MISMATCH, "a plane has a null device pointer"};
+        }
+        return std::nullopt;
+    }
+
+    float bias() const { return params_.channels == Channels::Chroma ? 0.5f : 0.0f; }
+
+    float* slot_ptr(size_t slot) const { return ring_.as<float>() + slot * frame_elems(); }
+
+    // nlmeans/denoiser/mod.rs:484-512 (`push_planes`) without look-ahead, then stages.rs:15-26.
+    std::optional<Failure> push_planes(const AvdPlane* planes) {
+        const size_t slot = ring_head_ % total_frames();
+        const void* p0 = reinterpret_cast<const void*>(planes[0].ptr);
+        const void* p1 = params_.channel_count() > 1 ? reinterpret_cast<const void*>(planes[1].ptr) : nullptr;
+        cudaError_t e = launch_ingest(p0, p1, slot_ptr(slot), static_cast<int64_t>(pixels()),
+                                      static_cast<int>(params_.channel_count()), plane_format(in_), bias(), stream);
+        if (e != cudaSuccess) return gpu_failure("ingest launch", e);
+        slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
+        advance_ring();
+        return prime_leading_edge_if_first();
+    }
+
+    // ring.rs:12-20.
+    void advance_ring() {
+        ring_head_ += 1;
+        if (frames_loaded_ < total_frames()) frames_loaded_ += 1;
+        real_pushes_ += 1;
+    }
+
+    // ring.rs:106-123: Repeat edges copy the first frame into the d leading slots.
+    std::optional<Failure> prime_leading_edge_if_first() {
+        const uint32_t d = params_.temporal_radius;
+        if (d == 0 || frames_loaded_ != 1) return std::nullopt;
+        for (uint32_t i = 0; i < d; ++i) {
+            if (auto f = duplicate_last_frame()) return f;
+            frames_loaded_ += 1;
+        }
+        return std::nullopt;
+    }
+
+    // ring.rs:128-146.
+    std::optional<Failure> duplicate_last_frame() {
+        const size_t tf = total_frames();
+        const size_t last = (ring_head_ - 1) % tf;
+        const size_t next = ring_head_ % tf;
+        cudaError_t e = cudaMemcpyAsync(slot_ptr(next), slot_ptr(last), frame_elems() * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return gpu_failure("slot copy", e);
+        slot_frames_[next] = slot_frames_[last];
+        ring_head_ += 1;
+        return std::nullopt;
+    }
+
+    // ring.rs:182-194.
+    size_t ring_start() const { return ring_head_ % total_frames(); }
+    int phys_frame(int logical) const {
+        const int tf = static_cast<int>(total_frames());
+        int wrapped = ((logical % tf) + tf) % tf;
+        return (static_cast<int>(ring_start()) + wrapped) % tf;
+    }
+    uint32_t centre_frame() const { return slot_frames_[phys_frame(static_cast<int>(params_.temporal_radius))]; }
+
+    // nlmeans/denoiser/mod.rs:517-532 (`denoise_submit_gpu`).
+    std::optional<Failure> denoise_submit(int* out_slot) {
+        *out_slot = -1;
+        if (frames_loaded_ < total_frames()) return std::nullopt;
+        const int slot = next_output_slot_;
+        next_output_slot_ = (slot + 1) % 2;
+
+        cudaEvent_t start{};
+        bool timed = timer_.begin(stream, &start);
+        const int d = static_cast<int>(params_.temporal_radius);
+        NlmLaunch a{};
+        a.ring = ring_.as<float>();
+        a.width = static_cast<int>(width_);
+        a.height = static_cast<int>(height_);
+        a.channels = static_cast<int>(params_.channel_count());
+        a.frame_elems = static_cast<int64_t>(frame_elems());
+        a.slot_centre = phys_frame(d);
+        a.pairs = d;
+        for (int k = 0; k < d; ++k) {
+            const int q_k = -d + k;
+            a.slot_fwd[k] = phys_frame(d + q_k);
+            a.slot_bwd[k] = phys_frame(d - q_k);
+        }
+        a.patch_radius = static_cast<int>(params_.patch_radius);
+        a.search_radius = static_cast<int>(params_.search_radius);
+        a.derived = derived_.as<float>();
+        a.h2_word = 0;
+        a.offset_word = 1;
+        a.spatial_lut = nullptr;
+        a.conf = nullptr;
+        a.wref = params_.self_weight;
+        a.out = outputs_[slot].as<float>();
+        cudaError_t e = launch_nlm(a, stream);
+        if (e != cudaSuccess) return gpu_failure("nlm launch", e);
+        if (timed) timer_.end(stream, start);
+        *out_slot = slot;
+        return std::nullopt;
+    }
+
+    // nlmeans/denoiser/mod.rs:557-573 (`flush_step_gpu`) without look-ahead.
+    std::optional<Failure> next_tail_frame(int* slot) {
+        for (;;) {
+            if (auto f = duplicate_last_frame()) return f;
+            if (frames_loaded_ < total_frames()) frames_loaded_ += 1;
+            if (auto f = denoise_submit(slot)) return f;
+            if (*slot >= 0) return std::nullopt;
+        }
+    }
+
+    std::optional<Failure> write_out(int slot, const AvdPlane* planes) {
+        void* p0 = reinterpret_cast<void*>(planes[0].ptr);
+        void* p1 = params_.channel_count() > 1 ? reinterpret_cast<void*>(planes[1].ptr) : nullptr;
+        cudaError_t e = launch_egress(outputs_[slot].as<float>(), p0, p1, static_cast<int64_t>(pixels()),
+                                      static_cast<int>(params_.channel_count()), plane_format(out_), bias(), stream);
+        if (e != cudaSuccess) return gpu_failure("egress launch", e);
+        return std::nullopt;
+    }
+
+    // nlmeans/denoiser/mod.rs:580-590 (`reset_stream_state`) and engine.rs:138-141.
+    void restart_stream() {
+        ring_head_ = 0;
+        frames_loaded_ = 0;
+        next_output_slot_ = 0;
+        real_pushes_ = 0;
+        pushed_ = false;
+    }
+
+    NlmParams params_;
+    size_t held_ = 0;
+    uint32_t width_ = 0, height_ = 0;
+    AvdSampleFormat in_{}, out_{};
+    DeviceBuffer ring_;
+    DeviceBuffer outputs_[2];
+    DeviceBuffer derived_;
+    std::vector<uint32_t> slot_frames_;
+    size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;
+    int next_output_slot_ = 0;
+    int ready_slot_ = -1;
+    size_t tail_remaining_ = 0;
+    bool pushed_ = false;
+    bool poisoned_ = false;
+    std::optional<uint32_t> emitted_;
+    DeviceTimer timer_;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Passthrough ring (engine/passthrough.rs): the uncleaned plane group of recent frames.
+class PassthroughRing {
+   public:
+    std::optional<Failure> init(size_t slots, size_t planes, uint64_t bytes) {
+        slots_.resize(slots);
+        bytes_ = bytes;
+        for (auto& s : slots_) {
+            s.resize(planes);
+            for (auto& b : s) {
+                b = std::make_unique<DeviceBuffer>();
+                cudaError_t e = b->alloc(bytes);
+                if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("passthrough ring", e)};
+            }
+        }
+        return std::nullopt;
+    }
+    size_t slots() const { return slots_.size(); }
+    cudaError_t store(uint32_t frame, const AvdPlane* planes, size_t n, cudaStream_t s) {
+        auto& slot = slots_[frame % slots_.size()];
+        for (size_t i = 0; i < n; ++i) {
+            cudaError_t e = cudaMemcpyAsync(slot[i]->ptr, reinterpret_cast<const void*>(planes[i].ptr), bytes_,
+                                            cudaMemcpyDeviceToDevice, s);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    cudaError_t load(uint32_t frame, const AvdPlane* planes, size_t n, cudaStream_t s) {
+        auto& slot = slots_[frame % slots_.size()];
+        for (size_t i = 0; i < n; ++i) {
+            cudaError_t e = cudaMemcpyAsync(reinterpret_cast<void*>(planes[i].ptr), slot[i]->ptr, bytes_,
+                                            cudaMemcpyDeviceToDevice, s);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+
+   private:
+    std::vector<std::vector<std::unique_ptr<DeviceBuffer>>> slots_;
+    uint64_t bytes_ = 0;
+};
+
+}  // namespace
+
+}  // namespace avd
+
+// ---------------------------------------------------------------------------------------------
+// The planar engine: engine/planar.rs:104-580.
+struct AvdEngine {
+    AvdGeometry geometry{};
+    std::unique_ptr<avd::Pass> luma, chroma;
+    std::unique_ptr<avd::PassthroughRing> passthrough;
+    bool passthrough_luma = false;  // which group the ring holds
+    bool poisoned = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+
+    avd::Pass* lead() const { return luma ? luma.get() : chroma.get(); }
+};
+
+namespace {
+
+using avd::Failure;
+
+thread_local std::string g_last_error;
+
+AvdStatus fail_global(AvdStatus st, const std::string& message) {
+    g_last_error = message;
+    return st;
+}
+
+AvdStatus record(AvdEngine* e, AvdStatus st, const std::string& message) {
+    if (e) e->last_error = st == AVD_OK ? std::string() : message;
+    return st;
+}
+
+AvdStatus record(AvdEngine* e, const std::optional<Failure>& f) {
+    if (!f) return record(e, AVD_OK, "");
+    return record(e, f->status, f->message);
+}
+
+// engine/frame.rs + planar.rs `check_planes`: all planes of the frame, each at its own size.
+std::optional<Failure> check_frame_planes(const AvdGeometry& g, const AvdPlane* planes, size_t n,
+                                          const AvdSampleFormat& fmt) {
+    const size_t expected = avd::plane_count(g.chroma);
+    if (n != expected) {
+        return Failure{AVD_ERR_PLANE_MISMATCH,
+                       "expected " + std::to_string(expected) + " planes, got " + std::to_string(n)};
+    }
+    for (size_t i = 0; i < n; ++i) {
+        uint32_t w, h;
+        avd::plane_dims(g, i, &w, &h);
+        if (planes[i].width != w || planes[i].height != h) {
+            return Failure{AVD_ERR_PLANE_MISMATCH, "plane " + std::to_string(i) + " is " +
+                                                       std::to_string(planes[i].width) + "x" +
+                                                       std::to_string(planes[i].height) + ", expected " +
+                                                       std::to_string(w) + "x" + std::to_string(h)};
+        }
+        uint64_t need = avd::plane_bytes(fmt, static_cast<uint64_t>(w) * h);
+        if (planes[i].bytes < need) {
+            return Failure{AVD_ERR_PLANE_MISMATCH, "plane " + std::to_string(i) + " holds " +
+                                                       std::to_string(planes[i].bytes) + " bytes, needs " +
+                                                       std::to_string(need)};
+        }
+    }
+    return std::nullopt;
+}
+
+// planar.rs:375-407 (`forward`): each pass in luma, chroma order; they must agree; a failure
+// after one pass moved poisons the engine.
+template <typename F>
+std::optional<Failure> forward(AvdEngine* e, size_t* agreed_out, F&& call) {
+    std::optional<size_t> agreed;
+    std::optional<Failure> failure;
+    avd::Pass* passes[2] = {e->luma.get(), e->chroma.get()};
+    for (int i = 0; i < 2; ++i) {
+        avd::Pass* p = passes[i];
+        if (!p) continue;
+        size_t value = 0;
+        if (auto f = call(p, i == 0, &value)) {
+            failure = f;
+            break;
+        }
+        if (agreed && *agreed != value) {
+            failure = Failure{AVD_ERR_GPU, "the luma pass returned " + std::to_string(*agreed) +
+                                               " but the chroma pass " + std::to_string(value)};
+            break;
+        }
+        agreed = value;
+    }
+    if (failure) {
+        if (agreed) e->poisoned = true;
+        return failure;
+    }
+    if (agreed_out) *agreed_out = agreed.value_or(0);
+    return std::nullopt;
+}
+
+const AvdPlane* group_planes(const AvdPlane* planes, bool luma) { return luma ? planes : planes + 1; }
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != device) cudaSetDevice(device);
+        else prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, AvdEngine** out) {
+    (void)tuning;
+    if (!spec || !out) return AVD_ERR_NULL_ARG;
+    *out = nullptr;
+    g_last_error.clear();
+    std::string message;
+    AvdStatus st = avd::validate_spec(*spec, &message);
+    if (st != AVD_OK) return fail_global(st, message);
+    if (spec->kind == AVD_ENGINE_NL4D)
+        return fail_global(AVD_ERR_INVALID_OPTIONS, "the NL4D engine is not available in this build yet");
+
+    auto engine = std::make_unique<AvdEngine>();
+    engine->geometry = spec->geometry;
+    cudaError_t dev_err = cudaGetDevice(&engine->device);
+    if (dev_err != cudaSuccess) return fail_global(AVD_ERR_GPU, avd::cuda_message("cudaGetDevice", dev_err));
+    const AvdGeometry& g = spec->geometry;
+    if (spec->has_luma) {
+        if (auto f = avd::NlmPass::create(spec->nlm_luma, avd::Channels::Luma, g.width, g.height, g.input, g.output,
+                                          &engine->luma))
+            return fail_global(f->status, f->message);
+    }
+    if (spec->has_chroma) {
+        uint32_t cw, ch;
+        avd::plane_dims(g, 1, &cw, &ch);
+        if (auto f = avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
+                                          &engine->chroma))
+            return fail_global(f->status, f->message);
+    }
+    const bool gray = g.chroma == AVD_CHROMA_GRAY;
+    const bool cleans_luma = engine->luma != nullptr;
+    if (!gray && cleans_luma != (engine->chroma != nullptr)) {
+        // planar.rs:210-220: one slot more than the cleaned pass holds frames.
+        engine->passthrough = std::make_unique<avd::PassthroughRing>();
+        engine->passthrough_luma = !cleans_luma;
+        const size_t index = cleans_luma ? 1 : 0;
+        const size_t planes = cleans_luma ? 2 : 1;
+        uint32_t w, h;
+        avd::plane_dims(g, index, &w, &h);
+        uint64_t bytes = avd::plane_bytes(g.input, static_cast<uint64_t>(w) * h);
+        if (auto f = engine->passthrough->init(engine->lead()->max_held_frames() + 1, planes, bytes))
+            return fail_global(f->status, f->message);
+    }
+    *out = engine.release();
+    return AVD_OK;
+}
+
+void avd_engine_destroy(AvdEngine* engine) {
+    if (!engine) return;
+    DeviceGuard dg(engine->device);
+    if (engine->stream) cudaStreamSynchronize(engine->stream);
+    delete engine;
+}
+
+AvdStatus avd_engine_set_stream(AvdEngine* engine, void* stream) {
+    if (!engine) return AVD_ERR_NULL_ARG;
+    engine->stream = static_cast<cudaStream_t>(stream);
+    if (engine->luma) engine->luma->stream = engine->stream;
+    if (engine->chroma) engine->chroma->stream = engine->stream;
+    return AVD_OK;
+}
+
+AvdStatus avd_engine_push(AvdEngine* e, const AvdPlane* planes, size_t n, size_t* ready) {
+    if (!e || !planes || !ready) return AVD_ERR_NULL_ARG;
+    DeviceGuard dg(e->device);
+    if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
+    if (auto f = check_frame_planes(e->geometry, planes, n, e->geometry.input)) return record(e, f);
+    const uint32_t frame = e->lead()->next_frame();
+    size_t value = 0;
+    auto f = forward(e, &value, [&](avd::Pass* p, bool luma, size_t* v) {
+        return p->push(group_planes(planes, luma), v);
+    });
+    if (f) return record(e, f);
+    if (e->passthrough) {
+        const AvdPlane* src = e->passthrough_luma ? planes : planes + 1;
+        size_t np = e->passthrough_luma ? 1 : 2;
+        cudaError_t err = e->passthrough->store(frame, src, np, e->stream);
+        if (err != cudaSuccess) {
+            e->poisoned = true;
+            return record(e, AVD_ERR_GPU, avd::cuda_message("passthrough store", err));
+        }
+    }
+    *ready = value;
+    return record(e, AVD_OK, "");
+}
+
+AvdStatus avd_engine_push_context(AvdEngine* e, const AvdPlane* planes, size_t n) {
+    if (!e || !planes) return AVD_ERR_NULL_ARG;
+    DeviceGuard dg(e->device);
+    if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
+    if (auto f = check_frame_planes(e->geometry, planes, n, e->geometry.input)) return record(e, f);
+    const uint32_t frame = e->lead()->next_frame();
+    auto f = forward(e, nullptr, [&](avd::Pass* p, bool luma, size_t* v) {
+        *v = 0;
+        return p->push_context(group_planes(planes, luma));
+    });
+    if (f) return record(e, f);
+    if (e->passthrough) {
+        const AvdPlane* src = e->passthrough_luma ? planes : planes + 1;
+        size_t np = e->passthrough_luma ? 1 : 2;
+        cudaError_t err = e->passthrough->store(frame, src, np, e->stream);
+        if (err != cudaSuccess) {
+            e->poisoned = true;
+            return record(e, AVD_ERR_GPU, avd::cuda_message("passthrough store", err));
+        }
+    }
+    return record(e, AVD_OK, "");
+}
+
+AvdStatus avd_engine_emit_into(AvdEngine* e, const AvdPlane* planes, size_t n) {
+    if (!e || !planes) return AVD_ERR_NULL_ARG;
+    DeviceGuard dg(e->device);
+    if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
+    if (auto f = check_frame_planes(e->geometry, planes, n, e->geometry.output)) return record(e, f);
+    auto f = forward(e, nullptr, [&](avd::Pass* p, bool luma, size_t* v) {
+        *v = 0;
+        return p->emit_into(group_planes(planes, luma));
+    });
+    if (f) return record(e, f);
+    if (e->passthrough) {
+        auto frame = e->lead()->emitted_frame();
+        const AvdPlane* dst = e->passthrough_luma ? planes : planes + 1;
+        size_t np = e->passthrough_luma ? 1 : 2;
+        cudaError_t err = e->passthrough->load(frame.value_or(0), dst, np, e->stream);
+        if (err != cudaSuccess) {
+            e->poisoned = true;
+            return record(e, AVD_ERR_GPU, avd::cuda_message("passthrough load", err));
+        }
+    }
+    return record(e, AVD_OK, "");
+}
+
+AvdStatus avd_engine_finish(AvdEngine* e, size_t* tail) {
+    if (!e || !tail) return AVD_ERR_NULL_ARG;
+    DeviceGuard dg(e->device);
+    if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
+    size_t value = 0;
+    auto f = forward(e, &value, [&](avd::Pass* p, bool, size_t* v) { return p->finish(v); });
+    if (f) return record(e, f);
+    *tail = value;
+    return record(e, AVD_OK, "");
+}
+
+AvdStatus avd_engine_reset(AvdEngine* e) {
+    if (!e) return AVD_ERR_NULL_ARG;
+    if (e->luma) e->luma->reset();
+    if (e->chroma) e->chroma->reset();
+    e->poisoned = false;
+    return record(e, AVD_OK, "");
+}
+
+AvdStatus avd_engine_window_span(const AvdEngine* e, AvdWindowSpan* out) {
+    if (!e || !out) return AVD_ERR_NULL_ARG;
+    *out = e->lead()->window_span();
+    return AVD_OK;
+}
+
+AvdStatus avd_engine_max_held_frames(const AvdEngine* e, size_t* out) {
+    if (!e || !out) return AVD_ERR_NULL_ARG;
+    *out = e->lead()->max_held_frames();
+    return AVD_OK;
+}
+
+AvdStatus avd_engine_timing(AvdEngine* e, AvdPassTimings* out) {
+    if (!e || !out) return AVD_ERR_NULL_ARG;
+    DeviceGuard dg(e->device);
+    std::memset(out, 0, sizeof(*out));
+    if (e->luma) {
+        out->has_luma = 1;
+        out->luma = e->luma->timing();
+    }
+    if (e->chroma) {
+        out->has_chroma = 1;
+        out->chroma = e->chroma->timing();
+    }
+    return AVD_OK;
+}
+
+AvdStatus avd_engine_sample_device_time(AvdEngine* e, uint32_t every) {
+    if (!e) return AVD_ERR_NULL_ARG;
+    if (e->luma) e->luma->sample_device_time(every);
+    if (e->chroma) e->chroma->sample_device_time(every);
+    return AVD_OK;
+}
+
+const char* avd_engine_last_error(const AvdEngine* e) { return e ? e->last_error.c_str() : ""; }
+
+const char* avd_last_error(void) { return g_last_error.c_str(); }
+
+AvdStatus avd_engine_fail_for_test(AvdEngine* e) {
+    if (!e) return AVD_ERR_NULL_ARG;
+    auto f = e->lead()->fail_for_test();
+    return record(e, f);
+}
+
+}  // extern "C"
+
+void avd_set_last_error(const std::string& m) { g_last_error = m; }

@@ -1,0 +1,52 @@
+// Launch interfaces of the CUDA kernels (host-callable, no CUDA types beyond cudaStream_t).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace avd {
+
+constexpr int kMaxPairs = 8;
+
+// Sample layout of a caller plane: u8/u16 packed into 32-bit words, or f32.
+struct PlaneFormat {
+    int kind;  // AvdSampleKind
+    int samples_per_word;
+    float max_value;
+};
+
+// av-denoise-core/src/engine/kernels.rs:25-90 (`ingest_words`, `ingest_f32`): planes -> one
+// interleaved f32 ring slot.
+cudaError_t launch_ingest(const void* plane0, const void* plane1, float* slot, int64_t pixels, int channels,
+                          PlaneFormat fmt, float bias, cudaStream_t stream);
+
+// av-denoise-core/src/engine/kernels.rs:103-184 (`egress_words`, `egress_f32`): an interleaved f32
+// frame -> caller planes, zeroing the word padding.
+cudaError_t launch_egress(const float* frame, void* plane0, void* plane1, int64_t pixels, int channels,
+                          PlaneFormat fmt, float bias, cudaStream_t stream);
+
+// One NLM output frame: every temporal pair pass, the single-frame pass and the finish, in one
+// launch.
+struct NlmLaunch {
+    const float* ring;  // f32 ring, `slots` frames of width*height*channels
+    int width, height, channels;
+    int64_t frame_elems;  // width*height*channels
+    int slot_centre;
+    int pairs;  // temporal radius d
+    int slot_fwd[kMaxPairs];  // pair k (q_k = -d + k): frame centre + q_k
+    int slot_bwd[kMaxPairs];  // frame centre - q_k
+    int patch_radius, search_radius;
+    const float* derived;  // device words; h2 at `h2_word`, pair noise offset at `offset_word`
+    int h2_word, offset_word;
+    const float* spatial_lut;  // (2a+1)^2 single-pass offsets, or null for zeros
+    const float* conf;  // per-block confidence, or null
+    int64_t conf_fwd_off[kMaxPairs], conf_bwd_off[kMaxPairs];
+    int conf_step, blocks_x, blocks_y;
+    float wref;
+    float* out;  // width*height*channels
+};
+
+cudaError_t launch_nlm(const NlmLaunch& args, cudaStream_t stream);
+
+}  // namespace avd

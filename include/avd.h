@@ -1,0 +1,349 @@
+/*
+ * avd.h - C ABI of the B200 denoising engine (NLMeans, NLMeans-HQ, NL4D and the noise estimator).
+ *
+ * Every entry point mirrors one item of av-denoise-core's public Rust API. The citation beside each
+ * names the reference interface it replaces, by its path inside the av-denoise project.
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes and PODs. Device buffers are raw CUDA device addresses
+ *    (`uint64_t`), borrowed for the duration of one call, exactly like the reference's
+ *    `DevicePlane<'a>` (av-denoise-core/src/engine/plane.rs:54-86).
+ *  - `Option<T>` fields become a `has_x` flag plus the value.
+ *  - Every call returns an `AvdStatus`; statuses map 1:1 onto `Error`
+ *    (av-denoise-core/src/error.rs:3-19), plus `AVD_ERR_NULL_ARG` for a null pointer argument.
+ *  - A failed state-changing call poisons the engine until `avd_engine_reset`, exactly as the
+ *    reference engine does (av-denoise-core/src/engine/mod.rs:167).
+ *  - An engine is `Send` but not `Sync`: one thread at a time may call into one engine.
+ */
+#ifndef AVD_H
+#define AVD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AVD_ABI_VERSION 1u
+
+#if defined(__GNUC__)
+#define AVD_API __attribute__((visibility("default")))
+#else
+#define AVD_API
+#endif
+
+/* ---- status -------------------------------------------------------------------------------- */
+
+/* av-denoise-core/src/error.rs:3-19 (`Error` variants, same order). */
+typedef enum AvdStatus {
+    AVD_OK = 0,
+    AVD_ERR_INVALID_OPTIONS = 1,
+    AVD_ERR_INVALID_GEOMETRY = 2,
+    AVD_ERR_PLANE_MISMATCH = 3,
+    AVD_ERR_OUTPUTS_PENDING = 4,
+    AVD_ERR_NOTHING_TO_EMIT = 5,
+    AVD_ERR_CONTEXT_AFTER_PUSH = 6,
+    AVD_ERR_NEEDS_RESET = 7,
+    AVD_ERR_GPU = 8, /* Error::Gpu: any CUDA failure, which poisons the engine */
+    AVD_ERR_NULL_ARG = 9
+} AvdStatus;
+
+/* ---- geometry ------------------------------------------------------------------------------ */
+
+/* av-denoise-core/src/engine/plane.rs:8-17 (`SampleFormat`). */
+typedef enum AvdSampleKind { AVD_SAMPLE_U8 = 0, AVD_SAMPLE_U16 = 1, AVD_SAMPLE_F32 = 2 } AvdSampleKind;
+
+typedef struct AvdSampleFormat {
+    uint32_t kind;  /* AvdSampleKind */
+    uint32_t depth; /* significant bits for AVD_SAMPLE_U16, in 9..=16; ignored otherwise */
+} AvdSampleFormat;
+
+/* av-denoise-core/src/engine/frame.rs:10-20 (`ChromaLayout`). */
+typedef enum AvdChromaLayout {
+    AVD_CHROMA_GRAY = 0,
+    AVD_CHROMA_YUV420 = 1,
+    AVD_CHROMA_YUV422 = 2,
+    AVD_CHROMA_YUV444 = 3
+} AvdChromaLayout;
+
+/* av-denoise-core/src/engine/frame.rs:54-66 (`ChromaSiting`): carried, never changes output. */
+typedef enum AvdChromaSiting {
+    AVD_SITING_LEFT = 0,
+    AVD_SITING_CENTER = 1,
+    AVD_SITING_TOP_LEFT = 2,
+    AVD_SITING_UNKNOWN = 3
+} AvdChromaSiting;
+
+/* av-denoise-core/src/engine/frame.rs:73-81 (`Geometry`). */
+typedef struct AvdGeometry {
+    uint32_t width;
+    uint32_t height;
+    uint32_t chroma; /* AvdChromaLayout */
+    uint32_t chroma_siting; /* AvdChromaSiting */
+    AvdSampleFormat input;
+    AvdSampleFormat output;
+} AvdGeometry;
+
+/* av-denoise-core/src/engine/plane.rs:54-86 (`DevicePlane`): a packed plane, stride = width,
+ * `bytes` >= SampleFormat::plane_bytes(width * height) (whole 32-bit words). */
+typedef struct AvdPlane {
+    uint64_t ptr; /* CUDA device address */
+    uint64_t bytes;
+    uint32_t width;
+    uint32_t height;
+} AvdPlane;
+
+/* ---- NLMeans options ----------------------------------------------------------------------- */
+
+/* av-denoise-core/src/options.rs:151-165 (`Preset`). */
+typedef enum AvdPreset {
+    AVD_PRESET_VERYFAST = 0,
+    AVD_PRESET_FAST = 1,
+    AVD_PRESET_BASE = 2,
+    AVD_PRESET_SLOW = 3,
+    AVD_PRESET_VERYSLOW = 4
+} AvdPreset;
+
+/* av-denoise-core/src/nlmeans/prefilter/mod.rs:15-26 (`PrefilterMode`). */
+typedef enum AvdPrefilterKind {
+    AVD_PREFILTER_NONE = 0,
+    AVD_PREFILTER_BILATERAL = 1,
+    AVD_PREFILTER_NLM_SPATIAL = 2
+} AvdPrefilterKind;
+
+typedef struct AvdPrefilter {
+    uint32_t kind; /* AvdPrefilterKind */
+    float sigma_s; /* Bilateral */
+    float sigma_r; /* Bilateral */
+    float strength_scale; /* NlmSpatial */
+} AvdPrefilter;
+
+/* av-denoise-core/src/motion/search.rs:94-113 (`MotionEstimation`). */
+typedef enum AvdEstimationKind {
+    AVD_ESTIMATION_AUTO = 0,
+    AVD_ESTIMATION_DIRECT = 1,
+    AVD_ESTIMATION_CHAINED = 2
+} AvdEstimationKind;
+
+/* av-denoise-core/src/motion/search.rs:5-53 (`MotionSearch`), also the payload of
+ * `MotionCompensationMode::Mvtools` (search.rs:58-89). */
+typedef struct AvdMotionSearch {
+    uint32_t blksize;
+    uint32_t overlap;
+    uint32_t search_radius;
+    uint32_t max_search_escalation;
+    uint32_t pyramid_levels;
+    uint32_t estimation; /* AvdEstimationKind */
+    uint32_t refine_radius; /* Chained only */
+} AvdMotionSearch;
+
+/* av-denoise-core/src/motion/search.rs:58-89 (`MotionCompensationMode`). */
+typedef struct AvdMotionCompensation {
+    uint32_t active; /* 0 = None, 1 = Mvtools { search } */
+    AvdMotionSearch search;
+} AvdMotionCompensation;
+
+/* av-denoise-core/src/nlmeans/options.rs:94-101 (`NlmTuning`). */
+typedef struct AvdNlmTuning {
+    uint32_t has_search_radius;
+    uint32_t search_radius;
+    uint32_t has_patch_radius;
+    uint32_t patch_radius;
+    uint32_t has_strength;
+    float strength;
+    uint32_t has_self_weight;
+    float self_weight;
+} AvdNlmTuning;
+
+/* av-denoise-core/src/nlmeans/options.rs:84-92 (`DenoisingMode`). */
+typedef struct AvdDenoisingMode {
+    uint32_t temporal; /* 0 = Spacial, 1 = Temporal { radius } */
+    uint32_t radius;
+} AvdDenoisingMode;
+
+/* av-denoise-core/src/nlmeans/params.rs:113-158 (`HqParams`). */
+typedef struct AvdHqParams {
+    uint32_t auto_strength;
+    uint32_t noise_floor;
+    uint32_t has_sigma_override;
+    float sigma_override;
+    uint32_t temporal_confidence;
+    float thsad_scale;
+    float sigma_scale;
+} AvdHqParams;
+
+/* av-denoise-core/src/nlmeans/options.rs:4-46 (`NlmeansOptions`, `NlmeansHqOptions`,
+ * `NlmeansAlgorithm`). `variant` 0 = Fast(options), 1 = Hq(options + hq). */
+typedef struct AvdNlmeansAlgorithm {
+    uint32_t variant;
+    AvdPrefilter prefilter;
+    AvdMotionCompensation motion_compensation;
+    AvdNlmTuning tuning;
+    AvdDenoisingMode mode;
+    AvdHqParams hq;
+} AvdNlmeansAlgorithm;
+
+/* ---- NL4D options -------------------------------------------------------------------------- */
+
+/* av-denoise-core/src/nl4d/options.rs:11-92 (`Nl4dOptions`). */
+typedef struct AvdNl4dOptions {
+    AvdMotionSearch motion;
+    uint32_t has_sigma;
+    float sigma;
+    float sigma_scale;
+    float thsad_scale;
+    uint32_t refine;
+    uint32_t spatial_radius;
+    uint32_t has_lambda_ht;
+    float lambda_ht;
+    float lambda_ht_scale;
+    float c_min;
+    float kaiser_beta;
+    float field_lambda;
+    uint32_t noise_map;
+    uint32_t pooled_threshold;
+    uint32_t grain_data; /* accepted and validated; AV1 grain measurement is not built */
+    uint32_t temporal_radius;
+} AvdNl4dOptions;
+
+/* ---- engine spec --------------------------------------------------------------------------- */
+
+/* av-denoise-core/src/engine/spec.rs:146-157 (`EngineSpec`). */
+typedef enum AvdEngineKind { AVD_ENGINE_NLMEANS = 0, AVD_ENGINE_NL4D = 1 } AvdEngineKind;
+
+typedef struct AvdEngineSpec {
+    uint32_t kind; /* AvdEngineKind */
+    uint32_t has_luma;
+    uint32_t has_chroma;
+    AvdNlmeansAlgorithm nlm_luma; /* kind == NLMEANS */
+    AvdNlmeansAlgorithm nlm_chroma;
+    AvdNl4dOptions nl4d_luma; /* kind == NL4D */
+    AvdNl4dOptions nl4d_chroma;
+    AvdGeometry geometry;
+} AvdEngineSpec;
+
+/* av-denoise-core/src/tune/setup.rs:79-91 (`TuningConfig`): the reference picks tuned kernel
+ * candidates here. This build has one kernel per site plus a per-shape launch-shape cache. */
+typedef struct AvdTuning {
+    uint32_t deterministic; /* kept for API parity; every kernel here is deterministic */
+    uint32_t reserved;
+} AvdTuning;
+
+/* av-denoise-core/src/engine/mod.rs:40-62 (`WindowSpan`, `EdgePadding`). */
+typedef struct AvdWindowSpan {
+    uint64_t behind;
+    uint64_t ahead;
+    uint32_t edges; /* 0 = Repeat, 1 = Shifted */
+    uint32_t reserved;
+} AvdWindowSpan;
+
+/* av-denoise-core/src/engine/timing.rs (`EngineTiming`) and engine/mod.rs:113-120
+ * (`PassTimings`). Times in seconds of device time, gathered while sampling is on. */
+typedef struct AvdEngineTiming {
+    double device_time;
+    uint64_t frames;
+} AvdEngineTiming;
+
+typedef struct AvdPassTimings {
+    uint32_t has_luma;
+    uint32_t has_chroma;
+    AvdEngineTiming luma;
+    AvdEngineTiming chroma;
+} AvdPassTimings;
+
+typedef struct AvdEngine AvdEngine;
+
+/* ---- library-level helpers (host only, no GPU) ----------------------------------------------- */
+
+/* ABI version of the loaded library. */
+AVD_API uint32_t avd_abi_version(void);
+
+/* The message of the calling thread's last failed call that has no engine to keep it
+ * (`avd_engine_create`, `avd_spec_validate`); empty after a success. */
+AVD_API const char* avd_last_error(void);
+
+/* av-denoise-core/src/error.rs:3-19: the fixed text of a status. */
+AVD_API const char* avd_status_message(AvdStatus status);
+
+/* Default-filled option structs, matching the reference's `Default` impls:
+ * nlmeans/options.rs:5-29 + params.rs:147-158 (NLMeans), nl4d/options.rs:68-92 (NL4D),
+ * motion/search.rs:33-44 (MotionSearch), engine/frame.rs:73-81 (Geometry, caller sets sizes). */
+AVD_API void avd_default_nlmeans(AvdNlmeansAlgorithm* out);
+AVD_API void avd_default_nl4d(AvdNl4dOptions* out);
+AVD_API void avd_default_motion_search(AvdMotionSearch* out);
+
+/* Presets: av-denoise-core/src/nlmeans/options.rs:58-82 and options.rs:170-175.
+ * `avd_nlmeans_variant_for` returns 0 = Fast, 1 = Hq. `avd_search_escalation_for` returns 0 for
+ * `None`. */
+AVD_API uint32_t avd_nlmeans_variant_for(uint32_t preset);
+AVD_API uint32_t avd_nlmeans_temporal_radius_for(uint32_t preset);
+AVD_API uint32_t avd_nlmeans_search_radius_for(uint32_t preset);
+AVD_API uint32_t avd_search_escalation_for(uint32_t preset);
+
+/* av-denoise-core/src/nlmeans/params.rs:27-33 (`hq_default_strength`); channels 1 = luma,
+ * 2 = chroma. */
+AVD_API float avd_hq_default_strength(uint32_t channels, uint32_t temporal_radius);
+
+/* av-denoise-core/src/engine/spec.rs:291-345 (`EngineSpec::validate`) plus the per-pass
+ * parameter checks the reference runs at build time (nlmeans/params.rs:276-428,
+ * nl4d/params.rs:119-197, nl4d/options.rs:127-185). Writes the message of a failure into `msg`
+ * (may be NULL). Runs on the host only. */
+AVD_API AvdStatus avd_spec_validate(const AvdEngineSpec* spec, char* msg, size_t msg_len);
+
+/* av-denoise-core/src/engine/spec.rs:260-281 (`EngineSpec::max_held_frames`,
+ * `EngineSpec::window_span`) for a spec, without building an engine. */
+AVD_API AvdStatus avd_spec_window_span(const AvdEngineSpec* spec, AvdWindowSpan* out);
+
+/* ---- engine -------------------------------------------------------------------------------- */
+
+/* av-denoise-core/src/tune/setup.rs:79-91 (`build_engine`). Validates first, touching no GPU
+ * state on failure. `tuning` may be NULL. The engine runs on the current CUDA device. */
+AVD_API AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, AvdEngine** out);
+
+AVD_API void avd_engine_destroy(AvdEngine* engine);
+
+/* Sets the CUDA stream (`cudaStream_t`) every later call queues its work on; 0 = legacy default.
+ * The reference's equivalent is the CubeCL client's queue. */
+AVD_API AvdStatus avd_engine_set_stream(AvdEngine* engine, void* stream);
+
+/* av-denoise-core/src/engine/mod.rs:170 (`Engine::push`). `planes` holds every plane of the
+ * frame, luma first; `*ready` receives how many frames are ready to emit (0 or 1). */
+AVD_API AvdStatus avd_engine_push(AvdEngine* engine, const AvdPlane* planes, size_t n_planes, size_t* ready);
+
+/* av-denoise-core/src/engine/mod.rs:185 (`Engine::push_context`). */
+AVD_API AvdStatus avd_engine_push_context(AvdEngine* engine, const AvdPlane* planes, size_t n_planes);
+
+/* av-denoise-core/src/engine/mod.rs:188 (`Engine::emit_into`). */
+AVD_API AvdStatus avd_engine_emit_into(AvdEngine* engine, const AvdPlane* planes, size_t n_planes);
+
+/* av-denoise-core/src/engine/mod.rs:191 (`Engine::finish`). */
+AVD_API AvdStatus avd_engine_finish(AvdEngine* engine, size_t* tail);
+
+/* av-denoise-core/src/engine/mod.rs:194 (`Engine::reset`). */
+AVD_API AvdStatus avd_engine_reset(AvdEngine* engine);
+
+/* av-denoise-core/src/engine/mod.rs:196 (`Engine::window_span`). */
+AVD_API AvdStatus avd_engine_window_span(const AvdEngine* engine, AvdWindowSpan* out);
+
+/* av-denoise-core/src/engine/mod.rs:199 (`Engine::max_held_frames`). */
+AVD_API AvdStatus avd_engine_max_held_frames(const AvdEngine* engine, size_t* out);
+
+/* av-denoise-core/src/engine/mod.rs:207 (`Engine::timing`). */
+AVD_API AvdStatus avd_engine_timing(AvdEngine* engine, AvdPassTimings* out);
+
+/* av-denoise-core/src/engine/mod.rs:210 (`Engine::sample_device_time`). */
+AVD_API AvdStatus avd_engine_sample_device_time(AvdEngine* engine, uint32_t every);
+
+/* The message of the engine's last failed call (empty when none). */
+AVD_API const char* avd_engine_last_error(const AvdEngine* engine);
+
+/* Test hook mirroring `fail_through_guard_for_test` (av-denoise-core/src/nlmeans/engine.rs:194-199):
+ * forces a GPU-class failure through the poison guard, with no GPU work. */
+AVD_API AvdStatus avd_engine_fail_for_test(AvdEngine* engine);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AVD_H */

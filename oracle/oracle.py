@@ -1,0 +1,153 @@
+"""CPU ORACLE - test infrastructure only (see nlm_oracle.cpp). Loaded by tests/, by
+`__graft_entry__.smoke()` and by the CPU-baseline leg of bench.py, as the checker; the product
+never imports it.
+
+ctypes bindings to liboracle.so plus the stream-level restatement of the NLMeans engine with
+repeat edges (av-denoise-core/src/nlmeans/denoiser/ring.rs:103-146): output frame n is the
+windowed NLM of frames clamp(n + k, 0, N - 1), k in -d..=d.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+_lib = None
+_fp = C.POINTER(C.c_float)
+_dp = C.POINTER(C.c_double)
+_fpp = C.POINTER(_fp)
+_u32p = C.POINTER(C.c_uint32)
+
+
+def build() -> Path:
+    """Builds liboracle.so with its Makefile (gcc, -ffp-contract=off)."""
+    res = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{res.stdout}\n{res.stderr}")
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        l = C.CDLL(str(LIB))
+        l.orc_ingest_words.argtypes = [_u32p, _u32p, _fp, C.c_int64, C.c_int, C.c_int, C.c_float]
+        l.orc_ingest_f32.argtypes = [_fp, _fp, _fp, C.c_int64, C.c_int, C.c_float]
+        l.orc_egress_words.argtypes = [_fp, _u32p, _u32p, C.c_int64, C.c_int, C.c_int, C.c_float]
+        l.orc_egress_f32.argtypes = [_fp, _fp, _fp, C.c_int64, C.c_int, C.c_float]
+        l.orc_h2_inv_norm.argtypes = [C.c_float, C.c_int]
+        l.orc_h2_inv_norm.restype = C.c_float
+        l.orc_welsch_weight.argtypes = [C.c_float, C.c_float, C.c_float]
+        l.orc_welsch_weight.restype = C.c_float
+        l.orc_nlm_frame_f32.argtypes = [_fpp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                        C.c_float, _fp, _fpp, _fpp, C.c_int, C.c_int, C.c_int, C.c_float, _fp]
+        l.orc_nlm_frame_f64.argtypes = [_fpp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                        C.c_double, _fp, _fpp, _fpp, C.c_int, C.c_int, C.c_int, C.c_double, _dp]
+        _lib = l
+    return _lib
+
+
+def _f(a: np.ndarray):
+    return a.ctypes.data_as(_fp)
+
+
+def h2_inv_norm(strength: float, patch_radius: int) -> float:
+    return float(lib().orc_h2_inv_norm(strength, patch_radius))
+
+
+def welsch_weight(total: float, h2: float, offset: float) -> float:
+    return float(lib().orc_welsch_weight(total, h2, offset))
+
+
+def words_from_codes(codes: np.ndarray, fmt_kind: int) -> np.ndarray:
+    """Packs a plane of integer codes into little-endian 32-bit words (u8: 4 per word, u16: 2)."""
+    flat = codes.reshape(-1)
+    if fmt_kind == 0:
+        pad = (-flat.size) % 4
+        b = np.concatenate([flat.astype(np.uint8), np.zeros(pad, np.uint8)])
+    else:
+        pad = (-flat.size) % 2
+        b = np.concatenate([flat.astype(np.uint16), np.zeros(pad, np.uint16)])
+    return np.ascontiguousarray(b).view(np.uint32)
+
+
+def ingest(planes: list[np.ndarray], fmt_kind: int, max_value: float, bias: float = 0.0) -> np.ndarray:
+    """Planes (codes, or f32 for kind 2) -> one interleaved normalised f32 frame (H, W, C)."""
+    h, w = planes[0].shape
+    c = len(planes)
+    out = np.empty((h, w, c), np.float32)
+    if fmt_kind == 2:
+        p0 = np.ascontiguousarray(planes[0], np.float32)
+        p1 = np.ascontiguousarray(planes[-1], np.float32)
+        lib().orc_ingest_f32(_f(p0), _f(p1), _f(out), h * w, c, bias)
+        return out
+    w0 = words_from_codes(planes[0], fmt_kind)
+    w1 = words_from_codes(planes[-1], fmt_kind)
+    spw = 4 if fmt_kind == 0 else 2
+    lib().orc_ingest_words(w0.ctypes.data_as(_u32p), w1.ctypes.data_as(_u32p), _f(out), h * w, c, spw, max_value)
+    return out
+
+
+def egress(frame: np.ndarray, fmt_kind: int, max_value: float, bias: float = 0.0) -> list[np.ndarray]:
+    """Interleaved f32 frame (H, W, C) -> planes of codes (or f32 for kind 2)."""
+    h, w, c = frame.shape
+    fr = np.ascontiguousarray(frame, np.float32)
+    if fmt_kind == 2:
+        p = [np.empty((h, w), np.float32) for _ in range(2)]
+        lib().orc_egress_f32(_f(fr), _f(p[0]), _f(p[1]), h * w, c, bias)
+        return p[:c]
+    spw = 4 if fmt_kind == 0 else 2
+    words = (h * w + spw - 1) // spw
+    p = [np.zeros(words, np.uint32) for _ in range(2)]
+    lib().orc_egress_words(_f(fr), p[0].ctypes.data_as(_u32p), p[1].ctypes.data_as(_u32p), h * w, c, spw, max_value)
+    dt = np.uint8 if fmt_kind == 0 else np.uint16
+    return [q.view(dt)[: h * w].reshape(h, w).copy() for q in p[:c]]
+
+
+def nlm_frame(window: list[np.ndarray], d: int, a: int, s: int, h2: float, noise_offset: float = 0.0,
+              lut: np.ndarray | None = None, conf: list[tuple[np.ndarray, np.ndarray]] | None = None,
+              conf_step: int = 8, blocks: tuple[int, int] = (1, 1), wref: float = 1.0,
+              fp64: bool = False) -> np.ndarray:
+    """One windowed NLM output frame (FP32 mirror, or FP64). `window` holds 2d+1 (H, W, C) f32
+    frames, the centre at index d."""
+    assert len(window) == 2 * d + 1
+    h, w, c = window[0].shape
+    frames = [np.ascontiguousarray(f, np.float32) for f in window]
+    arr = (_fp * len(frames))(*[_f(f) for f in frames])
+    lut_p = _f(np.ascontiguousarray(lut, np.float32)) if lut is not None else None
+    cf = cb = None
+    keep = []
+    if conf:
+        fw = [np.ascontiguousarray(x[0], np.float32) for x in conf]
+        bw = [np.ascontiguousarray(x[1], np.float32) for x in conf]
+        keep += fw + bw
+        cf = (_fp * d)(*[_f(x) for x in fw])
+        cb = (_fp * d)(*[_f(x) for x in bw])
+    if fp64:
+        out = np.empty((h, w, c), np.float64)
+        lib().orc_nlm_frame_f64(arr, w, h, c, d, a, s, h2, noise_offset, lut_p, cf, cb, conf_step, blocks[0],
+                                blocks[1], wref, out.ctypes.data_as(_dp))
+    else:
+        out = np.empty((h, w, c), np.float32)
+        lib().orc_nlm_frame_f32(arr, w, h, c, d, a, s, h2, noise_offset, lut_p, cf, cb, conf_step, blocks[0],
+                                blocks[1], wref, _f(out))
+    return out
+
+
+def nlm_stream_repeat(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, wref: float = 1.0,
+                      noise_offset: float = 0.0) -> list[np.ndarray]:
+    """The fast NLMeans engine over a whole stream with repeat edges: one output per input."""
+    n = len(frames)
+    outs = []
+    for i in range(n):
+        window = [frames[min(max(i + k, 0), n - 1)] for k in range(-d, d + 1)]
+        outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, wref=wref))
+    return outs

@@ -1,0 +1,227 @@
+"""NLMeans through the C ABI on the GPU, against the CPU oracle on the same seeded frames.
+
+Bar: at the source bit depth >= 99.9% of samples identical and none more
+than 1 LSB apart; float outputs within 2e-5 absolute. Passthrough planes are bit exact."""
+
+import numpy as np
+import pytest
+
+from conftest import avd
+from gpu_util import Runner, assert_parity, oracle_pass
+
+pytestmark = pytest.mark.gpu
+
+
+def nlm(d=0, a=2, s=2, strength=1.2, wref=None):
+    mode = avd.DenoisingMode.temporal(d) if d else avd.DenoisingMode.spacial()
+    tuning = avd.NlmTuning(search_radius=a, patch_radius=s, strength=strength, self_weight=wref)
+    return avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(tuning=tuning, mode=mode))
+
+
+def clip(w, h, n, depth=8, chroma="gray", seed=0, sigma=10.0):
+    from av_denoise_b200 import synth
+
+    return synth.make_clip(w, h, n, depth=depth, chroma=chroma, sigma_luma=sigma, sigma_chroma=sigma * 0.6,
+                           global_motion=2, sprites=1, sprite_size=24, seed=seed)
+
+
+def fmt_for(depth):
+    return avd.SampleFormat.u8() if depth == 8 else avd.SampleFormat.u16(depth)
+
+
+@pytest.mark.parametrize(
+    "w,h,depth,d,a,s,strength",
+    [
+        (96, 64, 8, 0, 7, 3, 12.0),  # the 640x360 spatial workload's parameters
+        (70, 45, 8, 2, 5, 2, 8.0),  # the 1080p temporal luma parameters, odd sizes
+        (64, 40, 10, 1, 4, 2, 30.0),
+        (50, 37, 12, 0, 3, 1, 120.0),
+        (33, 17, 8, 1, 2, 0, 20.0),  # patch radius 0
+        (40, 24, 8, 1, 0, 2, 15.0),  # search radius 0: pairs only at q = 0
+        (48, 40, 8, 0, 4, 9, 40.0),  # patch radius above the separable threshold
+        (3, 3, 8, 1, 2, 1, 10.0),  # minimum frame
+    ],
+)
+def test_luma_parity(oracle, w, h, depth, d, a, s, strength):
+    fmt = fmt_for(depth)
+    frames = clip(w, h, 5, depth=depth, seed=w * h + d)
+    spec = avd.EngineSpec.nlmeans(nlm(d, a, s, strength), None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    want = oracle_pass(oracle, [[f[0]] for f in frames], fmt, d, a, s, strength)
+    assert len(got) == len(frames)
+    for g, wnt in zip(got, want):
+        assert_parity(g[0], wnt[0])
+
+
+def test_chroma_only_with_luma_passthrough(oracle):
+    w, h = 72, 50
+    frames = clip(w, h, 4, chroma="420", seed=3)
+    fmt = avd.SampleFormat.u8()
+    spec = avd.EngineSpec.nlmeans(None, nlm(0, 5, 2, 5.0), avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    want = oracle_pass(oracle, [[f[1], f[2]] for f in frames], fmt, 0, 5, 2, 5.0, chroma=True)
+    for i, (g, wnt) in enumerate(zip(got, want)):
+        assert np.array_equal(g[0], frames[i][0])  # luma passes through word for word
+        assert_parity(g[1], wnt[0])
+        assert_parity(g[2], wnt[1])
+
+
+def test_luma_temporal_with_chroma_passthrough(oracle):
+    w, h = 66, 38
+    frames = clip(w, h, 6, chroma="420", seed=4)
+    fmt = avd.SampleFormat.u8()
+    spec = avd.EngineSpec.nlmeans(nlm(2, 5, 2, 8.0), None, avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    want = oracle_pass(oracle, [[f[0]] for f in frames], fmt, 2, 5, 2, 8.0)
+    assert len(got) == 6
+    for i, (g, wnt) in enumerate(zip(got, want)):
+        assert_parity(g[0], wnt[0])
+        assert np.array_equal(g[1], frames[i][1]) and np.array_equal(g[2], frames[i][2])
+
+
+@pytest.mark.parametrize("layout", [avd.ChromaLayout.YUV444, avd.ChromaLayout.YUV422])
+def test_luma_and_chroma_10bit(oracle, layout):
+    w, h = 48, 36
+    name = {avd.ChromaLayout.YUV444: "444", avd.ChromaLayout.YUV422: "422"}[layout]
+    frames = clip(w, h, 4, depth=10, chroma=name, seed=9)
+    fmt = avd.SampleFormat.u16(10)
+    spec = avd.EngineSpec.nlmeans(nlm(1, 3, 2, 20.0), nlm(1, 3, 1, 12.0), avd.Geometry(w, h, layout, fmt, fmt))
+    got = Runner(spec).run(frames)
+    want_y = oracle_pass(oracle, [[f[0]] for f in frames], fmt, 1, 3, 2, 20.0)
+    want_c = oracle_pass(oracle, [[f[1], f[2]] for f in frames], fmt, 1, 3, 1, 12.0, chroma=True)
+    for g, wy, wc in zip(got, want_y, want_c):
+        assert_parity(g[0], wy[0])
+        assert_parity(g[1], wc[0])
+        assert_parity(g[2], wc[1])
+
+
+def test_float_planes(oracle):
+    w, h = 40, 30
+    rng = np.random.default_rng(1)
+    frames = [[rng.random((h, w), dtype=np.float32), (rng.random((h // 2, w // 2), dtype=np.float32) - 0.5),
+               (rng.random((h // 2, w // 2), dtype=np.float32) - 0.5)] for _ in range(3)]
+    fmt = avd.SampleFormat.f32()
+    spec = avd.EngineSpec.nlmeans(nlm(1, 2, 1, 60.0), nlm(1, 2, 1, 60.0),
+                                  avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    want_y = oracle_pass(oracle, [[f[0]] for f in frames], fmt, 1, 2, 1, 60.0)
+    want_c = oracle_pass(oracle, [[f[1], f[2]] for f in frames], fmt, 1, 2, 1, 60.0, chroma=True)
+    for g, wy, wc in zip(got, want_y, want_c):
+        np.testing.assert_allclose(g[0], wy[0], atol=2e-5, rtol=0)
+        np.testing.assert_allclose(g[1], wc[0], atol=2e-5, rtol=0)
+        np.testing.assert_allclose(g[2], wc[1], atol=2e-5, rtol=0)
+
+
+def test_self_weight_zero_and_uniform_frame(oracle):
+    w, h = 20, 20
+    fmt = avd.SampleFormat.u8()
+    frames = [[np.full((h, w), 77, np.uint8)] for _ in range(2)]
+    spec = avd.EngineSpec.nlmeans(nlm(0, 3, 2, 1.2, wref=0.0), None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    for g in got:
+        assert (g[0] == 77).all()
+
+
+def test_stream_shorter_than_window(oracle):
+    # d = 8 with two frames: both repeat edges fill the window (ring.rs:106-146).
+    w, h = 24, 20
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 2, seed=21)
+    spec = avd.EngineSpec.nlmeans(nlm(8, 2, 1, 10.0), None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    want = oracle_pass(oracle, [[f[0]] for f in frames], fmt, 8, 2, 1, 10.0)
+    assert len(got) == 2
+    for g, wnt in zip(got, want):
+        assert_parity(g[0], wnt[0])
+
+
+def test_engine_errors_and_poison():
+    import torch
+
+    w, h = 16, 16
+    fmt = avd.SampleFormat.u8()
+    spec = avd.EngineSpec.nlmeans(nlm(1, 2, 1, 10.0), None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    r = Runner(spec)
+    e = r.engine
+    frames = clip(w, h, 4, seed=5)
+    _, p0 = r.planes_for(frames[0], fmt)
+    _, p1 = r.planes_for(frames[1], fmt)
+    with pytest.raises(avd.NothingToEmit):
+        e.emit_into(r.out_planes())
+    assert e.push(p0) == 0
+    assert e.push(p1) == 1
+    with pytest.raises(avd.OutputsPending):
+        e.push(p1)
+    with pytest.raises(avd.ContextAfterPush):
+        e.emit_into(r.out_planes())
+        e.push_context(p0)
+    with pytest.raises(avd.PlaneMismatch):
+        e.push([avd.DevicePlane(p0[0].ptr, p0[0].bytes, w + 1, h)])
+    with pytest.raises(avd.PlaneMismatch):
+        e.push([avd.DevicePlane(p0[0].ptr, 8, w, h)])
+    with pytest.raises(avd.GpuError):
+        e.fail_for_test()
+    with pytest.raises(avd.NeedsReset):
+        e.push(p0)
+    e.reset()
+    assert e.push(p0) == 0
+    assert e.finish() == 1
+    r.emit()
+    with pytest.raises(avd.NothingToEmit):
+        e.emit_into(r.out_planes())
+    assert e.max_held_frames() == 1
+    span = e.window_span()
+    assert (span.behind, span.ahead, span.edges) == (1, 1, "repeat")
+    torch.cuda.synchronize()
+
+
+def test_push_context_reseeds_mid_clip(oracle):
+    # engine/mod.rs:74-81: context frames fill the window so a stream can start mid-clip. A
+    # stream that starts at frame 3 with frames 1..2 as context reproduces the full stream's
+    # output for frames >= 3 (up to the window reaching back to frame 1).
+    w, h = 30, 22
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 8, seed=8)
+    spec = avd.EngineSpec.nlmeans(nlm(1, 2, 1, 10.0), None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    full = Runner(spec).run(frames)
+    part = Runner(spec).run(frames[1:], context=1)
+    # Outputs of the reseeded stream are frames 1.. (frame 1 is the context frame itself).
+    for i in range(2, 7):
+        assert np.array_equal(part[i - 1][0], full[i][0])
+
+
+def test_device_timing():
+    w, h = 64, 48
+    fmt = avd.SampleFormat.u8()
+    spec = avd.EngineSpec.nlmeans(nlm(1, 3, 2, 10.0), None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    r = Runner(spec)
+    r.engine.sample_device_time(1)
+    r.run(clip(w, h, 4, seed=2))
+    t = r.engine.timing()
+    assert t.luma is not None and t.luma.frames == 4 and t.luma.device_time > 0
+    assert t.chroma is None
+
+
+def test_full_1080p_crops_match_oracle(oracle):
+    """Full-size frames (1920x1080, d=2, a=5, s=2): the oracle on interior crops with a margin of
+    a+s reproduces the GPU output inside the crop."""
+    from av_denoise_b200 import synth
+
+    frames = synth.temporal_1080p_clip(frames=5)
+    fmt = avd.SampleFormat.u8()
+    spec = avd.EngineSpec.nlmeans(nlm(2, 5, 2, 8.0), None, avd.Geometry(1920, 1080, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    m = 7
+    for (cx, cy) in [(0, 0), (900, 500), (1920 - 64, 1080 - 64)]:
+        x0, y0 = max(cx - m, 0), max(cy - m, 0)
+        x1, y1 = min(cx + 64 + m, 1920), min(cy + 64 + m, 1080)
+        crop = [[f[0][y0:y1, x0:x1]] for f in frames]
+        want = oracle_pass(oracle, crop, fmt, 2, 5, 2, 8.0)
+        for i in range(5):
+            g = got[i][0][y0:y1, x0:x1]
+            # Only pixels whose window stays inside the crop (or at true image edges) compare.
+            ix0 = 0 if x0 == 0 else m
+            iy0 = 0 if y0 == 0 else m
+            ix1 = (x1 - x0) if x1 == 1920 else (x1 - x0 - m)
+            iy1 = (y1 - y0) if y1 == 1080 else (y1 - y0 - m)
+            assert_parity(g[iy0:iy1, ix0:ix1], want[i][0][iy0:iy1, ix0:ix1])
