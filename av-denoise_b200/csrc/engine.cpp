@@ -382,6 +382,7 @@ class NlmPass final : public Pass {
         a.spatial_lut = nullptr;
         a.conf = nullptr;
         a.wref = params_.self_weight;
+        a.fast = params_.hq ? 0 : 1;
         a.out = outputs_[slot].as<float>();
         cudaError_t e = launch_nlm(a, stream);
         if (e != cudaSuccess) return gpu_failure("nlm launch", e);

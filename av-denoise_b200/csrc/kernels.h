@@ -44,6 +44,7 @@ struct NlmLaunch {
     int64_t conf_fwd_off[kMaxPairs], conf_bwd_off[kMaxPairs];
     int conf_step, blocks_x, blocks_y;
     float wref;
+    int fast;  // 1: no noise offsets and no confidence, so one strength weighs every lane
     float* out;  // width*height*channels
 };
 

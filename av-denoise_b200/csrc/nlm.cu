@@ -6,24 +6,28 @@
 // (2a+1)^2 window), then the single-frame pass (all q != 0), the patch distance
 //   D(p, q) = scale * sum over the (2s+1)^2 patch of sum_c (centre - neighbour)^2
 // gives the Welsch weight w = exp(-max(D - offset, 0) * h2), optionally times a per-block
-// confidence; the pass accumulates sum w*I(neighbour), sum w and max w, and the finish is
+// confidence; the passes accumulate sum w*I(neighbour), sum w and max w, and the finish is
 //   out = (I * wref * max_w + sum wI) / (wref * max_w + sum w)   (I if the denominator <= 1e-30).
 //
-// How (B200 layout): a CTA owns a 32 x TY output tile and walks every pass and offset with the
-// running sums in registers, so the accumulators never leave the SM. Per offset:
-//   phase 1 - row runs: each task owns 8 consecutive pixels of one tile row (plus the 2s halo),
-//             computes the squared differences against the neighbour frame staged in shared
-//             memory, and forms the 8 horizontal box sums with a running sum; one 16-byte store
-//             pair writes them to a double-buffered row-sum tile;
+// How (B200 layout). A CTA owns a 32 x TY output tile and keeps every running sum in registers,
+// so accumulators never leave the SM; each frame tile is read from HBM once per pass. The work
+// is walked in two-lane steps: lane 0 and lane 1 are two (neighbour tile, offset) pairs that run
+// side by side in packed f32x2 arithmetic (Blackwell's FADD2/FMUL2/FFMA2 issue two fp32 ops per
+// slot). A temporal pass pairs the forward frame at +q with the backward frame at -q; the
+// single-frame pass pairs two consecutive offsets. Per step:
+//   phase 1 - row runs: each thread owns 8 consecutive pixels of one tile row plus the 2s halo
+//             (its centre values stay in registers for the whole kernel), forms the squared
+//             differences of both lanes and their 8 horizontal box sums with running sums, and
+//             stores the lane pairs to a double-buffered row-sum tile;
 //   phase 2 - column strips: each thread owns V pixels of one column, forms the vertical box
-//             sums with a running sum, then the weight (one MUFU ex2) and the accumulation.
-// One barrier per offset (the row-sum tile is double buffered). The per-offset cost is ~15
-// issue slots per output pixel against one MUFU op, which is why the kernel is bound by issue
-// and the SFU, not by HBM: every frame tile is read from HBM once per pass.
+//             sums of both lanes, two MUFU ex2 give the weights, one FFMA2 accumulates w*I and
+//             one FADD2 the weight sums.
+// One barrier per step. The max weight is tracked as the minimum distance (exp is monotonic, so
+// this is exact) when every lane shares one strength and no offset or confidence applies.
 //
-// The box sums run in a different order from the reference's direct row-major patch sum, so
-// D can differ in the last bits; the weights feed a normalised average, and the parity tests
-// bound the effect on the quantised output.
+// The box sums run in a different order from the reference's direct row-major patch sum and
+// the two lanes are summed at the end, so results can differ from the reference in the last
+// bits; the parity tests bound the effect on the quantised output.
 
 #include <cuda_runtime.h>
 
@@ -36,25 +40,37 @@ namespace avd {
 
 namespace {
 
-constexpr int kTX = 32;       // tile columns
+constexpr int kTX = 32;        // tile columns
 constexpr int kThreads = 128;  // 4 warps: 32 columns x 4 strips
 constexpr int kRun = 8;        // phase-1 run length
-constexpr int kRuns = kTX / kRun;
 constexpr float kLog2e = 1.4426950408889634f;
 
+// Shared-memory strides are chosen so no phase reads or writes conflict in the banks:
+//  - phase 1 gives lane l the row (l & 7) and the run (l >> 3) of its warp's 8-row group, so a
+//    scalar (or float2, for two channels) read of a neighbour tile hits 32 distinct banks when
+//    the neighbour row stride, in pixels, is odd;
+//  - the row-sum tile is written as float4 by 8 rows at a time and read as float2 along a row,
+//    which is conflict free when its row stride is 4 x an odd number of floats.
 __host__ __device__ constexpr int round_up4(int v) { return (v + 3) & ~3; }
+__host__ __device__ constexpr int stride_4odd(int v) {
+    return (round_up4(v) / 4) % 2 ? round_up4(v) : round_up4(v) + 4;
+}
+__host__ __device__ constexpr int nbr_stride(int cols, int c) { return c * (cols | 1); }
+
+constexpr int kHsStride = stride_4odd(2 * kTX);  // 68 floats: 32 lane pairs per row-sum row
 
 template <int C, int S>
 struct Cfg {
     static constexpr int V = (32 - 2 * S) / 4 >= 1 ? (32 - 2 * S) / 4 : 1;  // outputs per column strip
     static constexpr int TY = 4 * V;                                       // tile rows
     static constexpr int HR = TY + 2 * S;                                  // row-sum rows
-    static constexpr int TASKS = HR * kRuns;                               // phase-1 tasks
+    static constexpr int TASK_SLOTS = (HR + 7) / 8 * 32;                   // phase-1 tasks (8-row groups)
+    static constexpr bool CTR_REG = C == 1 && TASK_SLOTS <= kThreads;      // centre run kept in registers
     static constexpr int CW = kTX + 2 * S;                                 // centre tile columns
-    static constexpr int CSTRIDE = round_up4(CW * C);                      // floats per centre row
+    static constexpr int CSTRIDE = nbr_stride(CW, C);                      // floats per centre row
     static constexpr int CROWS = TY + 2 * S;
     static constexpr int RUNW = kRun + 2 * S;  // pixels one run reads
-    static constexpr int RUNF4 = (RUNW * C + 3) / 4;
+    static constexpr int HS_BUF = HR * kHsStride;
 };
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -65,19 +81,27 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
-// The Welsch weight from an unscaled box sum `d` (sum of squared differences):
-// w = exp(-max(d * scale - off, 0) * h2) = 2^(max(...) * (-h2 * log2 e)).
-__device__ __forceinline__ float welsch(float d, float scale, float off, float neg_h2_log2e) {
-    float excess = fmaxf(fmaf(d, scale, -off), 0.0f);
-#ifdef AVD_NLM_ACCURATE_EXP
-    return expf(excess * (neg_h2_log2e / kLog2e));
-#else
-    return ex2_approx(excess * neg_h2_log2e);
-#endif
+__device__ __forceinline__ float min3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
 }
 
-// Stages frame `slot` over the tile's window into shared memory, coordinates clamped to the image
-// as the reference's `read_clamped_line` does (helpers.rs:20-32).
+__device__ __forceinline__ float max3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b as one FFMA2: b * (-1) + a.
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f, -1.0f), a); }
+
+// Stages a frame over the tile's window into shared memory, coordinates clamped to the image as
+// the reference's `read_clamped_line` does (helpers.rs:20-32).
 template <int C>
 __device__ void load_tile(float* tile, int stride, int rows, int cols, const float* __restrict__ frame, int x0, int y0,
                           int W, int H) {
@@ -98,160 +122,153 @@ __device__ void load_tile(float* tile, int stride, int rows, int cols, const flo
     }
 }
 
-// Phase 1 of one offset for one direction: 8 horizontal box sums of one tile row.
+// The centre values of one phase-1 run, each duplicated into both lanes of a pair: u (and v).
 template <int C, int S>
-__device__ __forceinline__ void row_run(const float* __restrict__ ctr_row, const float* __restrict__ nbr_row,
-                                        float* __restrict__ hs_out) {
-    using K = Cfg<C, S>;
-    float cv[K::RUNF4 * 4];
+struct CentreRun {
+    float2 u[Cfg<C, S>::RUNW];
+    float2 v[C == 2 ? Cfg<C, S>::RUNW : 1];
+
+    __device__ __forceinline__ void load(const float* ctr_row) {
 #pragma unroll
-    for (int i = 0; i < K::RUNF4; ++i) {
-        float4 v = *reinterpret_cast<const float4*>(ctr_row + 4 * i);
-        cv[4 * i] = v.x;
-        cv[4 * i + 1] = v.y;
-        cv[4 * i + 2] = v.z;
-        cv[4 * i + 3] = v.w;
-    }
-    float d[K::RUNW];
-#pragma unroll
-    for (int i = 0; i < K::RUNW; ++i) {
-        if (C == 1) {
-            float diff = cv[i] - nbr_row[i];
-            d[i] = diff * diff;
-        } else {
-            float2 n = *reinterpret_cast<const float2*>(nbr_row + 2 * i);
-            float du = cv[2 * i] - n.x;
-            float dv = cv[2 * i + 1] - n.y;
-            d[i] = fmaf(dv, dv, du * du);
+        for (int i = 0; i < Cfg<C, S>::RUNW; ++i) {
+            if (C == 1) {
+                u[i] = f2(ctr_row[i], ctr_row[i]);
+            } else {
+                float2 c = *reinterpret_cast<const float2*>(ctr_row + 2 * i);
+                u[i] = f2(c.x, c.x);
+                v[i] = f2(c.y, c.y);
+            }
         }
     }
-    float h[kRun];
-    float run = d[0];
+};
+
+// Phase 1 of one step: the 8 horizontal box sums of one tile row for both lanes, stored as lane
+// pairs. `n0` and `n1` point at the run's first halo pixel in each lane's neighbour tile.
+template <int C, int S>
+__device__ __forceinline__ void row_run(const CentreRun<C, S>& c, const float* __restrict__ n0,
+                                        const float* __restrict__ n1, float* __restrict__ hs_out) {
+    constexpr int RUNW = Cfg<C, S>::RUNW;
+    float2 d[RUNW];
 #pragma unroll
-    for (int i = 1; i <= 2 * S; ++i) run += d[i];
+    for (int i = 0; i < RUNW; ++i) {
+        if (C == 1) {
+            float2 diff = sub2(c.u[i], f2(n0[i], n1[i]));
+            d[i] = mul2(diff, diff);
+        } else {
+            float2 a = *reinterpret_cast<const float2*>(n0 + 2 * i);
+            float2 b = *reinterpret_cast<const float2*>(n1 + 2 * i);
+            float2 du = sub2(c.u[i], f2(a.x, b.x));
+            float2 dv = sub2(c.v[i], f2(a.y, b.y));
+            d[i] = fma2(dv, dv, mul2(du, du));
+        }
+    }
+    float2 h[kRun];
+    float2 run = d[0];
+#pragma unroll
+    for (int i = 1; i <= 2 * S; ++i) run = add2(run, d[i]);
     h[0] = run;
 #pragma unroll
     for (int j = 1; j < kRun; ++j) {
-        run = run + d[j + 2 * S] - d[j - 1];
+        run = sub2(add2(run, d[j + 2 * S]), d[j - 1]);
         h[j] = run;
     }
-    *reinterpret_cast<float4*>(hs_out) = make_float4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<float4*>(hs_out + 4) = make_float4(h[4], h[5], h[6], h[7]);
+#pragma unroll
+    for (int m = 0; m < kRun / 2; ++m)
+        *reinterpret_cast<float4*>(hs_out + 4 * m) = make_float4(h[2 * m].x, h[2 * m].y, h[2 * m + 1].x, h[2 * m + 1].y);
 }
 
-template <int C, int S>
+// Shared-memory layout of one CTA.
 struct Smem {
-    float* ctr;
-    float* nbr[2];
-    float* hs;  // [2 buffers][2 directions][HR][kTX]
-    int nstride;
-    int nrows, ncols;
+    float* ctr;     // centre frame, s halo, rows of CSTRIDE floats
+    float* nbr[2];  // neighbour tiles, s + a halo, rows of `nstride` floats
+    float* hs;      // [2 buffers][HR][kTX lane pairs], rows of kHsStride floats
+    int nstride, nrows, ncols;
 };
 
-// One pass (a temporal pair when PAIR, else the single-frame pass) over the whole window.
-template <int C, int S, bool PAIR, bool CONF>
-__device__ __forceinline__ void run_pass(const Smem<C, S>& sm, int A, float scale, float off_pair,
-                                         const float* __restrict__ lut, float neg_h2_log2e, const float* cf,
-                                         const float* cb, int& buf, float (&acc_tot)[Cfg<C, S>::V][C],
-                                         float (&ws_tot)[Cfg<C, S>::V], float (&wm)[Cfg<C, S>::V]) {
+// Per-thread accumulators: lane pairs, summed at the finish.
+template <int C, int V>
+struct Acc {
+    float2 a[C][V];  // sum w * I per channel
+    float2 ws[V];    // sum w
+    float m[V];      // min distance (FAST) or max weight (HQ)
+};
+
+// The lanes of one step: neighbour tiles and offsets (the neighbour of pixel p is p + (dx, dy)).
+struct Lanes {
+    const float* t0;
+    const float* t1;
+    int dx0, dy0, dx1, dy1;
+};
+
+// One two-lane step: phase 1, barrier, phase 2. FAST: one strength, no offsets, no confidence.
+template <int C, int S, bool FAST, bool CONF>
+__device__ __forceinline__ void step(const Smem& sm, int A, const Lanes& ln, int& buf, const CentreRun<C, S>& crun,
+                                     float2 kk, float2 scale2, float2 negoff, const float2* conf,
+                                     Acc<C, Cfg<C, S>::V>& acc) {
     using K = Cfg<C, S>;
     constexpr int V = K::V;
     const int tid = threadIdx.x;
-    const int col = tid & 31;
-    const int y0 = (tid >> 5) * V;
-    const int side = 2 * A + 1;
-    const int hs_plane = K::HR * kTX;
+    float* hs = sm.hs + buf * K::HS_BUF;
 
-    float acc[V][C];
-    float ws[V];
-#pragma unroll
-    for (int k = 0; k < V; ++k) {
-        ws[k] = 0.0f;
-#pragma unroll
-        for (int c = 0; c < C; ++c) acc[k][c] = 0.0f;
-    }
-
-    for (int qyi = 0; qyi < side; ++qyi) {
-        const int qy = qyi - A;
-        for (int qxi = 0; qxi < side; ++qxi) {
-            const int qx = qxi - A;
-            if (!PAIR && qx == 0 && qy == 0) continue;
-            float* hs = sm.hs + buf * 2 * hs_plane;
-
-            // Phase 1: row runs.
-            for (int task = tid; task < K::TASKS; task += kThreads) {
-                const int r = task / kRuns;
-                const int x0 = (task - r * kRuns) * kRun;
-                const float* crow = sm.ctr + r * K::CSTRIDE + x0 * C;
-                const float* nrow = sm.nbr[0] + (r + qy + A) * sm.nstride + (x0 + qx + A) * C;
-                row_run<C, S>(crow, nrow, hs + r * kTX + x0);
-                if (PAIR) {
-                    const float* brow = sm.nbr[1] + (r - qy + A) * sm.nstride + (x0 - qx + A) * C;
-                    row_run<C, S>(crow, brow, hs + hs_plane + r * kTX + x0);
-                }
-            }
-            __syncthreads();
-
-            // Phase 2: column strips.
-            const float off = PAIR ? off_pair : (lut ? __ldg(lut + qyi * side + qxi) : 0.0f);
-            float hv[V + 2 * S];
-#pragma unroll
-            for (int i = 0; i < V + 2 * S; ++i) hv[i] = hs[(y0 + i) * kTX + col];
-            float hb[PAIR ? V + 2 * S : 1];
-            if (PAIR) {
-#pragma unroll
-                for (int i = 0; i < V + 2 * S; ++i) hb[i] = hs[hs_plane + (y0 + i) * kTX + col];
-            }
-            float run = hv[0];
-#pragma unroll
-            for (int i = 1; i <= 2 * S; ++i) run += hv[i];
-            float runb = 0.0f;
-            if (PAIR) {
-                runb = hb[0];
-#pragma unroll
-                for (int i = 1; i <= 2 * S; ++i) runb += hb[i];
-            }
-            const float* nf = sm.nbr[0] + (y0 + S + qy + A) * sm.nstride + (col + S + qx + A) * C;
-            const float* nb = PAIR ? sm.nbr[1] + (y0 + S - qy + A) * sm.nstride + (col + S - qx + A) * C : nullptr;
-#pragma unroll
-            for (int k = 0; k < V; ++k) {
-                if (k > 0) {
-                    run = run + hv[k + 2 * S] - hv[k - 1];
-                    if (PAIR) runb = runb + hb[k + 2 * S] - hb[k - 1];
-                }
-                float w = welsch(run, scale, off, neg_h2_log2e);
-                if (CONF) w *= cf[k];
-                const float* pf = nf + k * sm.nstride;
-                if (!PAIR) {
-#pragma unroll
-                    for (int c = 0; c < C; ++c) acc[k][c] = fmaf(pf[c], w, acc[k][c]);
-                    ws[k] += w;
-                    wm[k] = fmaxf(wm[k], w);
-                } else {
-                    float wb = welsch(runb, scale, off, neg_h2_log2e);
-                    if (CONF) wb *= cb[k];
-                    const float* pb = nb + k * sm.nstride;
-#pragma unroll
-                    for (int c = 0; c < C; ++c) acc[k][c] = fmaf(pb[c], wb, fmaf(pf[c], w, acc[k][c]));
-                    ws[k] += w + wb;
-                    wm[k] = fmaxf(wm[k], fmaxf(w, wb));
-                }
-            }
-            buf ^= 1;
+    for (int slot = tid; slot < K::TASK_SLOTS; slot += kThreads) {
+        const int r = ((slot >> 5) << 3) + (slot & 7);
+        if (r >= K::HR) continue;
+        const int x0 = ((slot >> 3) & 3) * kRun;
+        const float* n0 = ln.t0 + (r + ln.dy0 + A) * sm.nstride + (x0 + ln.dx0 + A) * C;
+        const float* n1 = ln.t1 + (r + ln.dy1 + A) * sm.nstride + (x0 + ln.dx1 + A) * C;
+        if (K::CTR_REG) {
+            row_run<C, S>(crun, n0, n1, hs + r * kHsStride + 2 * x0);
+        } else {
+            CentreRun<C, S> c;
+            c.load(sm.ctr + r * K::CSTRIDE + x0 * C);
+            row_run<C, S>(c, n0, n1, hs + r * kHsStride + 2 * x0);
         }
     }
+    __syncthreads();
 
-    // The pass adds its register sums to the frame sums once, as each reference launch does.
+    const int col = tid & 31;
+    const int y0 = (tid >> 5) * V;
+    float2 hv[V + 2 * S];
+#pragma unroll
+    for (int i = 0; i < V + 2 * S; ++i) hv[i] = *reinterpret_cast<const float2*>(hs + (y0 + i) * kHsStride + 2 * col);
+    float2 dist = hv[0];
+#pragma unroll
+    for (int i = 1; i <= 2 * S; ++i) dist = add2(dist, hv[i]);
+    const float* p0 = ln.t0 + (y0 + S + ln.dy0 + A) * sm.nstride + (col + S + ln.dx0 + A) * C;
+    const float* p1 = ln.t1 + (y0 + S + ln.dy1 + A) * sm.nstride + (col + S + ln.dx1 + A) * C;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
-        ws_tot[k] += ws[k];
-#pragma unroll
-        for (int c = 0; c < C; ++c) acc_tot[k][c] += acc[k][c];
+        if (k > 0) dist = sub2(add2(dist, hv[k + 2 * S]), hv[k - 1]);
+        float2 w;
+        if (FAST) {
+            float2 e = mul2(dist, kk);
+            w = f2(ex2_approx(e.x), ex2_approx(e.y));
+            acc.m[k] = min3(acc.m[k], dist.x, dist.y);
+        } else {
+            float2 x = fma2(dist, scale2, negoff);
+            x = f2(fmaxf(x.x, 0.0f), fmaxf(x.y, 0.0f));
+            float2 e = mul2(x, kk);
+            w = f2(ex2_approx(e.x), ex2_approx(e.y));
+            if (CONF) w = mul2(w, conf[k]);
+            acc.m[k] = max3(acc.m[k], w.x, w.y);
+        }
+        const float* q0 = p0 + k * sm.nstride;
+        const float* q1 = p1 + k * sm.nstride;
+        if (C == 1) {
+            acc.a[0][k] = fma2(f2(q0[0], q1[0]), w, acc.a[0][k]);
+        } else {
+            float2 a = *reinterpret_cast<const float2*>(q0);
+            float2 b = *reinterpret_cast<const float2*>(q1);
+            acc.a[0][k] = fma2(f2(a.x, b.x), w, acc.a[0][k]);
+            acc.a[C - 1][k] = fma2(f2(a.y, b.y), w, acc.a[C - 1][k]);
+        }
+        acc.ws[k] = add2(acc.ws[k], w);
     }
+    buf ^= 1;
 }
 
-template <int C, int S>
-__global__ void __launch_bounds__(kThreads) nlm_window_kernel(NlmLaunch a) {
+template <int C, int S, bool FAST>
+__global__ void __launch_bounds__(kThreads, C == 1 && FAST ? 5 : 4) nlm_window_kernel(NlmLaunch a) {
     using K = Cfg<C, S>;
     constexpr int V = K::V;
     extern __shared__ __align__(16) float smem_raw[];
@@ -263,63 +280,101 @@ __global__ void __launch_bounds__(kThreads) nlm_window_kernel(NlmLaunch a) {
     const int tid = threadIdx.x;
     const int col = tid & 31;
     const int y0 = (tid >> 5) * V;
+    const int side = 2 * A + 1;
 
-    Smem<C, S> sm;
+    Smem sm;
     sm.nrows = K::TY + 2 * S + 2 * A;
     sm.ncols = kTX + 2 * S + 2 * A;
-    sm.nstride = round_up4(sm.ncols * C);
+    sm.nstride = nbr_stride(sm.ncols, C);
     sm.ctr = smem_raw;
-    sm.nbr[0] = sm.ctr + K::CROWS * K::CSTRIDE;
+    sm.nbr[0] = sm.ctr + round_up4(K::CROWS * K::CSTRIDE);
     sm.nbr[1] = sm.nbr[0] + sm.nrows * sm.nstride;
-    sm.hs = sm.nbr[1] + (a.pairs > 0 ? sm.nrows * sm.nstride : 0);
+    sm.hs = sm.nbr[0] + round_up4((a.pairs > 0 ? 2 : 1) * sm.nrows * sm.nstride);
 
     const float h2 = __ldg(a.derived + a.h2_word);
     const float off_pair = __ldg(a.derived + a.offset_word);
-    const float neg_h2_log2e = -h2 * kLog2e;
     const float scale = C == 1 ? 3.0f : 1.5f;
+    const float neg_h2_log2e = -h2 * kLog2e;
+    const float2 kk = FAST ? f2(scale * neg_h2_log2e, scale * neg_h2_log2e) : f2(neg_h2_log2e, neg_h2_log2e);
+    const float2 scale2 = f2(scale, scale);
 
     const float* centre = a.ring + a.slot_centre * a.frame_elems;
     load_tile<C>(sm.ctr, K::CSTRIDE, K::CROWS, K::CW, centre, X0 - S, Y0 - S, W, H);
+    __syncthreads();
 
-    float acc[V][C];
-    float ws[V];
-    float wm[V];
+    CentreRun<C, S> crun;
+    if (K::CTR_REG) {
+        const int r = ((tid >> 5) << 3) + (tid & 7);
+        const int x0 = ((tid >> 3) & 3) * kRun;
+        crun.load(sm.ctr + min(r, K::CROWS - 1) * K::CSTRIDE + x0 * C);
+    }
+
+    Acc<C, V> acc;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
-        ws[k] = 0.0f;
-        wm[k] = 0.0f;
+        acc.ws[k] = f2(0.0f, 0.0f);
+        acc.m[k] = FAST ? __int_as_float(0x7f800000) : 0.0f;  // +inf min distance / 0 max weight
 #pragma unroll
-        for (int c = 0; c < C; ++c) acc[k][c] = 0.0f;
+        for (int c = 0; c < C; ++c) acc.a[c][k] = f2(0.0f, 0.0f);
     }
 
     int buf = 0;
-    float cf[V], cb[V];
+    float2 conf[V];
     for (int p = 0; p < a.pairs; ++p) {
         __syncthreads();  // every thread is done with the previous pass's tiles
         load_tile<C>(sm.nbr[0], sm.nstride, sm.nrows, sm.ncols, a.ring + a.slot_fwd[p] * a.frame_elems, X0 - S - A,
                      Y0 - S - A, W, H);
         load_tile<C>(sm.nbr[1], sm.nstride, sm.nrows, sm.ncols, a.ring + a.slot_bwd[p] * a.frame_elems, X0 - S - A,
                      Y0 - S - A, W, H);
-        __syncthreads();
-        if (a.conf) {
+        const bool use_conf = !FAST && a.conf != nullptr;
 #pragma unroll
-            for (int k = 0; k < V; ++k) {
+        for (int k = 0; k < V; ++k) {
+            conf[k] = f2(1.0f, 1.0f);
+            if (use_conf) {
                 int gx = min(X0 + col, W - 1), gy = min(Y0 + y0 + k, H - 1);
                 int bc = min(gx / a.conf_step, a.blocks_x - 1);
                 int br = min(gy / a.conf_step, a.blocks_y - 1);
-                cf[k] = __ldg(a.conf + a.conf_fwd_off[p] + br * a.blocks_x + bc);
-                cb[k] = __ldg(a.conf + a.conf_bwd_off[p] + br * a.blocks_x + bc);
+                conf[k] = f2(__ldg(a.conf + a.conf_fwd_off[p] + br * a.blocks_x + bc),
+                             __ldg(a.conf + a.conf_bwd_off[p] + br * a.blocks_x + bc));
             }
-            run_pass<C, S, true, true>(sm, A, scale, off_pair, nullptr, neg_h2_log2e, cf, cb, buf, acc, ws, wm);
-        } else {
-            run_pass<C, S, true, false>(sm, A, scale, off_pair, nullptr, neg_h2_log2e, cf, cb, buf, acc, ws, wm);
+        }
+        __syncthreads();
+        Lanes ln{sm.nbr[0], sm.nbr[1], 0, 0, 0, 0};
+        const float2 negoff = f2(-off_pair, -off_pair);
+        for (int qy = -A; qy <= A; ++qy) {
+            for (int qx = -A; qx <= A; ++qx) {
+                ln.dx0 = qx;
+                ln.dy0 = qy;
+                ln.dx1 = -qx;
+                ln.dy1 = -qy;
+                if (use_conf)
+                    step<C, S, FAST, true>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
+                else
+                    step<C, S, FAST, false>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
+            }
         }
     }
 
+    // The single-frame pass: the window without its centre, two consecutive offsets per step.
     __syncthreads();
     load_tile<C>(sm.nbr[0], sm.nstride, sm.nrows, sm.ncols, centre, X0 - S - A, Y0 - S - A, W, H);
     __syncthreads();
-    run_pass<C, S, false, false>(sm, A, scale, 0.0f, a.spatial_lut, neg_h2_log2e, cf, cb, buf, acc, ws, wm);
+    {
+        Lanes ln{sm.nbr[0], sm.nbr[0], 0, 0, 0, 0};
+        const int n = side * side - 1;
+        const int mid = A * side + A;
+        for (int i = 0; i < n; i += 2) {
+            const int l0 = i < mid ? i : i + 1;
+            const int l1 = i + 1 < mid ? i + 1 : i + 2;
+            ln.dx0 = l0 % side - A;
+            ln.dy0 = l0 / side - A;
+            ln.dx1 = l1 % side - A;
+            ln.dy1 = l1 / side - A;
+            float2 negoff = f2(0.0f, 0.0f);
+            if (!FAST && a.spatial_lut) negoff = f2(-__ldg(a.spatial_lut + l0), -__ldg(a.spatial_lut + l1));
+            step<C, S, FAST, false>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
+        }
+    }
 
     // Finish (accumulate.rs:175-201), written straight to the output frame.
     const int gx = X0 + col;
@@ -327,14 +382,19 @@ __global__ void __launch_bounds__(kThreads) nlm_window_kernel(NlmLaunch a) {
     for (int k = 0; k < V; ++k) {
         const int gy = Y0 + y0 + k;
         if (gx >= W || gy >= H) continue;
+        const float max_w = FAST ? ex2_approx(acc.m[k] * kk.x) : acc.m[k];
+        const float wsum = acc.ws[k].x + acc.ws[k].y;
         const float* orig = sm.ctr + (y0 + k + S) * K::CSTRIDE + (col + S) * C;
-        const float self_weight = __fmul_rn(a.wref, wm[k]);
-        const float denom = __fadd_rn(self_weight, ws[k]);
+        const float self_weight = __fmul_rn(a.wref, max_w);
+        const float denom = __fadd_rn(self_weight, wsum);
         float* dst = a.out + ((int64_t)gy * W + gx) * C;
         if (denom > 1e-30f) {
             const float inv = __frcp_rn(denom);
 #pragma unroll
-            for (int c = 0; c < C; ++c) dst[c] = __fmul_rn(__fadd_rn(__fmul_rn(orig[c], self_weight), acc[k][c]), inv);
+            for (int c = 0; c < C; ++c) {
+                const float sum_wi = acc.a[c][k].x + acc.a[c][k].y;
+                dst[c] = __fmul_rn(__fadd_rn(__fmul_rn(orig[c], self_weight), sum_wi), inv);
+            }
         } else {
 #pragma unroll
             for (int c = 0; c < C; ++c) dst[c] = orig[c];
@@ -347,31 +407,31 @@ size_t smem_bytes(int A, int pairs) {
     using K = Cfg<C, S>;
     int nrows = K::TY + 2 * S + 2 * A;
     int ncols = kTX + 2 * S + 2 * A;
-    int nstride = round_up4(ncols * C);
-    size_t floats = (size_t)K::CROWS * K::CSTRIDE + (size_t)(pairs > 0 ? 2 : 1) * nrows * nstride +
-                    (size_t)2 * 2 * K::HR * kTX;
+    int nstride = nbr_stride(ncols, C);
+    size_t floats = (size_t)round_up4(K::CROWS * K::CSTRIDE) + (size_t)round_up4((pairs > 0 ? 2 : 1) * nrows * nstride) +
+                    (size_t)2 * K::HS_BUF;
     return floats * sizeof(float);
 }
 
-template <int C, int S>
-cudaError_t launch_cs(const NlmLaunch& a, cudaStream_t stream) {
+template <int C, int S, bool FAST>
+cudaError_t launch_csf(const NlmLaunch& a, cudaStream_t stream) {
     using K = Cfg<C, S>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(nlm_window_kernel<C, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        attr_err = cudaFuncSetAttribute(nlm_window_kernel<C, S, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         200 * 1024);
     });
     if (attr_err != cudaSuccess) return attr_err;
     dim3 grid((a.width + kTX - 1) / kTX, (a.height + K::TY - 1) / K::TY);
     size_t smem = smem_bytes<C, S>(a.search_radius, a.pairs);
-    nlm_window_kernel<C, S><<<grid, kThreads, smem, stream>>>(a);
+    nlm_window_kernel<C, S, FAST><<<grid, kThreads, smem, stream>>>(a);
     return cudaGetLastError();
 }
 
 template <int C, int S>
 cudaError_t dispatch_s(const NlmLaunch& a, cudaStream_t stream) {
-    if (a.patch_radius == S) return launch_cs<C, S>(a, stream);
+    if (a.patch_radius == S) return a.fast ? launch_csf<C, S, true>(a, stream) : launch_csf<C, S, false>(a, stream);
     if constexpr (S < 16) {
         return dispatch_s<C, S + 1>(a, stream);
     } else {
