@@ -181,6 +181,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_engine_last_error": (C.c_char_p, [_E]),
     "avd_engine_fail_for_test": (C.c_int, [_E]),
     "avd_last_error": (C.c_char_p, []),
+    "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,
+                                       _P(AvdPlane), C.c_size_t, _P(AvdPlane), C.c_size_t, C.c_void_p]),
 }
 
 _lib: C.CDLL | None = None

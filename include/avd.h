@@ -342,6 +342,28 @@ AVD_API const char* avd_engine_last_error(const AvdEngine* engine);
  * forces a GPU-class failure through the poison guard, with no GPU work. */
 AVD_API AvdStatus avd_engine_fail_for_test(AvdEngine* engine);
 
+/* ---- allocation-free entry point ----------------------------------------------------------- */
+
+/* No counterpart in the reference. One fast-variant NLMeans output frame for callers that cannot
+ * allocate device memory (a plugin inside another application's CUDA context, a real-time path
+ * that must not enter the allocator mid-stream, a sandbox without the allocation calls). It makes
+ * no cudaMalloc or cudaFree and calls no allocating library routine: its scratch lives in one
+ * file-scope device array of 32 MiB that every GPU loading this library holds until exit, and
+ * sizes that need more than that fail with AVD_ERR_INVALID_GEOMETRY (message in avd_last_error).
+ *
+ * `window` holds the (2 * temporal_radius + 1) input frames, oldest first, each as `channels`
+ * planes (1 = luma, 2 = the U and V planes); the centre frame is the one denoised, exactly as the
+ * engine denoises it with that window. `out` receives `channels` planes. Work is queued on
+ * `stream` (a cudaStream_t; NULL = legacy default) with no host synchronisation.
+ *
+ * The first call on a device looks up the array's device address with that device current, so
+ * make it before any stream capture. Every call shares the array and leaves its contents behind;
+ * each call writes every scratch word it reads, but calls whose GPU work overlaps race. */
+AVD_API AvdStatus avd_nlm_frame_static(const AvdNlmeansAlgorithm* algorithm, uint32_t channels, uint32_t width,
+                                       uint32_t height, AvdSampleFormat input, AvdSampleFormat output,
+                                       const AvdPlane* window, size_t n_window, const AvdPlane* out, size_t n_out,
+                                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif
