@@ -262,6 +262,17 @@ class NlmPass final : public Pass {
         words[1] = has_sigma ? noise_offset_with(params_, sig, 2) : 0.0f;
         if ((e = cudaMemcpy(derived_.ptr, words, sizeof(words), cudaMemcpyHostToDevice)) != cudaSuccess)
             return gpu_failure("derived upload", e);
+        if (params_.hq) {
+            // noise/correlation.rs:71-88 (`build_spatial_offset_lut`): with no measured grain
+            // correlation (rho = 0) every candidate but the centre takes the flat noise offset.
+            const uint32_t side = 2 * params_.search_radius + 1;
+            std::vector<float> lut(side * side, words[1]);
+            lut[params_.search_radius * side + params_.search_radius] = 0.0f;
+            if ((e = lut_.alloc(lut.size() * sizeof(float))) != cudaSuccess) return gpu_failure("offset table", e);
+            if ((e = cudaMemcpy(lut_.ptr, lut.data(), lut.size() * sizeof(float), cudaMemcpyHostToDevice)) !=
+                cudaSuccess)
+                return gpu_failure("offset table upload", e);
+        }
         slot_frames_.assign(total_frames(), 0u);
         return std::nullopt;
     }
@@ -379,7 +390,7 @@ class NlmPass final : public Pass {
         a.derived = derived_.as<float>();
         a.h2_word = 0;
         a.offset_word = 1;
-        a.spatial_lut = nullptr;
+        a.spatial_lut = params_.hq ? lut_.as<float>() : nullptr;
         a.conf = nullptr;
         a.wref = params_.self_weight;
         a.fast = params_.hq ? 0 : 1;
@@ -426,6 +437,7 @@ class NlmPass final : public Pass {
     DeviceBuffer ring_;
     DeviceBuffer outputs_[2];
     DeviceBuffer derived_;
+    DeviceBuffer lut_;
     std::vector<uint32_t> slot_frames_;
     size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;
     int next_output_slot_ = 0;

@@ -321,7 +321,10 @@ def run_gpu(args) -> None:
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "sfu", "kernel": "nlm_window_kernel<1,2> (luma, 604 offsets/pixel)",
                      "achieved": round(achieved, 2), "peak": round(mufu_peak, 2), "unit": "Gex2/s",
-                     "frac": round(achieved / mufu_peak, 4), "traffic": None,
+                     "frac": round(achieved / mufu_peak, 4),
+                     # dram__bytes_read.sum + dram__bytes_write.sum of this launch in one ncu
+                     # capture (profiles/nlm_window_kernel_luma_1080p_d2a5s2.md).
+                     "traffic": 41.52e6 + 0.151e6,
                      "peak_note": f"MUFU ex2: {sms} SMs x 16/clk x sm_max_mhz {peaks['sm_max_mhz']} "
                                   f"({peaks['source']})",
                      "launch_ms": round(t_launch * 1e3, 4)},
@@ -421,8 +424,38 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def run_once() -> None:
+    """One luma NLM launch of the workload (1920x1080, d=2, a=5, s=2): the small case the kernel
+    profiles are captured on (three pushes fill the window once; ~60 MB on the device)."""
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import synth
+
+    clip = synth.make_clip(W, H, 3, depth=8, chroma="gray", sigma_luma=8.0, global_motion=4, sprites=3, seed=7)
+    fmt = avd.SampleFormat.u8()
+    t = avd.NlmTuning(search_radius=LUMA["a"], patch_radius=LUMA["s"], strength=LUMA["strength"])
+    alg = avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(tuning=t, mode=avd.DenoisingMode.temporal(LUMA["d"])))
+    eng = avd.build_engine(avd.EngineSpec.nlmeans(alg, None, avd.Geometry(W, H, avd.ChromaLayout.GRAY, fmt, fmt)))
+    out = torch.zeros(plane_words(fmt, W, H), dtype=torch.int32, device="cuda")
+    bufs = []
+    for f in clip:
+        flat = f[0].reshape(-1)
+        b = torch.from_numpy(np.concatenate([flat, np.zeros((-flat.size) % 4, np.uint8)]).view(np.int32)).cuda()
+        bufs.append(b)
+        if eng.push([avd.DevicePlane.from_tensor(b, W, H)]):
+            eng.emit_into([avd.DevicePlane.from_tensor(out, W, H)])
+    torch.cuda.synchronize()
+    eng.close()
+    print("one luma NLM launch done")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
+    ap.add_argument("--once", action="store_true", help="run one luma NLM launch (profiling case) and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -430,7 +463,9 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.once:
+        run_once()
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -143,11 +143,11 @@ def nlm_frame(window: list[np.ndarray], d: int, a: int, s: int, h2: float, noise
 
 
 def nlm_stream_repeat(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, wref: float = 1.0,
-                      noise_offset: float = 0.0, fp64: bool = False) -> list[np.ndarray]:
+                      noise_offset: float = 0.0, fp64: bool = False, lut: np.ndarray | None = None) -> list[np.ndarray]:
     """The fast NLMeans engine over a whole stream with repeat edges: one output per input."""
     n = len(frames)
     outs = []
     for i in range(n):
         window = [frames[min(max(i + k, 0), n - 1)] for k in range(-d, d + 1)]
-        outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, wref=wref, fp64=fp64))
+        outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, lut=lut, wref=wref, fp64=fp64))
     return outs

@@ -97,8 +97,26 @@ class Runner:
         return outs
 
 
+def hq_fixed_words(strength: float, sigma: float, s: int, channels: int, a: int):
+    """h2, the noise offset and the spatial offset table of NLMeans-HQ with a pinned sigma, in the
+    reference's f32 arithmetic (nlmeans/params.rs:221-268, noise/correlation.rs:43-88 at rho 0)."""
+    f = np.float32
+    area = f((2 * s + 1) ** 2)
+    eff = f(strength) * f(sigma) * f(255.0)
+    h2 = f(65025.0) / (((f(3.0) * eff) * eff) * area)
+    scale = f(3.0) if channels == 1 else f(1.5)
+    sum_sq = f(0.0)
+    for _ in range(channels):
+        sum_sq = f(sum_sq + f(sigma) * f(sigma))
+    offset = ((f(2.0) * scale) * sum_sq) * area
+    side = 2 * a + 1
+    lut = np.full(side * side, offset, np.float32)
+    lut[a * side + a] = 0.0
+    return float(h2), float(offset), lut
+
+
 def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, wref=1.0, chroma=False,
-                out_fmt=None, exact=False):
+                out_fmt=None, exact=False, hq_sigma=None):
     """The oracle's output planes for one plane group over a stream (repeat edges).
 
     Returns the FP32-mirror output planes; with `exact`, also the FP64 outputs as (H, W, C)
@@ -106,13 +124,15 @@ def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, 
     out_fmt = out_fmt or fmt
     bias = 0.5 if (chroma and fmt.kind == 2) else 0.0
     f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), bias) for p in frames]
-    h2 = oracle.h2_inv_norm(strength, s)
-    outs = oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref)
+    h2, off, lut = oracle.h2_inv_norm(strength, s), 0.0, None
+    if hq_sigma is not None:
+        h2, off, lut = hq_fixed_words(strength, hq_sigma, s, 2 if chroma else 1, a)
+    outs = oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut)
     obias = 0.5 if (chroma and out_fmt.kind == 2) else 0.0
     planes = [oracle.egress(o, out_fmt.kind, out_fmt.max_value(), obias) for o in outs]
     if not exact:
         return planes
-    return planes, oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, fp64=True)
+    return planes, oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, fp64=True)
 
 
 # A sample whose exact (FP64) value lies within this distance, in normalised units, of a rounding

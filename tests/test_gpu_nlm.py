@@ -30,9 +30,11 @@ def fmt_for(depth):
     return avd.SampleFormat.u8() if depth == 8 else avd.SampleFormat.u16(depth)
 
 
-def check_group(oracle, got_planes, frames, fmt, d, a, s, strength, chroma=False, min_raw=0.99, wref=1.0):
+def check_group(oracle, got_planes, frames, fmt, d, a, s, strength, chroma=False, min_raw=0.99, wref=1.0,
+                hq_sigma=None):
     """Compares one plane group of every emitted frame with the oracle; returns the stats."""
-    want, exact = oracle_pass(oracle, frames, fmt, d, a, s, strength, wref=wref, chroma=chroma, exact=True)
+    want, exact = oracle_pass(oracle, frames, fmt, d, a, s, strength, wref=wref, chroma=chroma, exact=True,
+                              hq_sigma=hq_sigma)
     par = Parity()
     for g, wn, ex in zip(got_planes, want, exact):
         for c in range(len(wn)):
@@ -252,3 +254,38 @@ def test_full_1080p_crops_match_oracle(oracle):
             g = got[i][0][y0:y1, x0:x1]
             par.add(g[iy0:iy1, ix0:ix1], want[i][0][iy0:iy1, ix0:ix1], exact[i][iy0:iy1, ix0:ix1, 0], 255.0)
     print(par.check())
+
+
+def hq(d, a, s, sigma, strength=None, confidence=False):
+    mode = avd.DenoisingMode.temporal(d) if d else avd.DenoisingMode.spacial()
+    tuning = avd.NlmTuning(search_radius=a, patch_radius=s, strength=strength)
+    params = avd.HqParams(sigma_override=sigma, temporal_confidence=confidence)
+    return avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(nlm=avd.NlmeansOptions(tuning=tuning, mode=mode), hq=params))
+
+
+@pytest.mark.parametrize("d,a,s,sigma", [(1, 4, 2, 10.0 / 255), (0, 5, 3, 6.0 / 255), (2, 3, 1, 14.0 / 255)])
+def test_hq_pinned_sigma_luma(oracle, d, a, s, sigma):
+    """NLMeans-HQ with sigma_override: strength = hq_default_strength * sigma * 255 and the noise
+    floor subtracted from every distance (flat spatial table at rho = 0)."""
+    w, h = 120, 72
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 4, seed=40 + d)
+    spec = avd.EngineSpec.nlmeans(hq(d, a, s, sigma), None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    strength = avd.hq_default_strength(1, d)
+    # The noise floor clamps many distances to 0, so many weights are exactly 1 and many outputs
+    # exact means of integer codes: ~10% of samples are half-code ties here.
+    check_group(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, a, s, strength, hq_sigma=sigma,
+                min_raw=0.95)
+
+
+def test_hq_pinned_sigma_chroma_10bit(oracle):
+    w, h = 96, 64
+    fmt = avd.SampleFormat.u16(10)
+    frames = clip(w, h, 3, depth=10, chroma="420", seed=44)
+    sigma = 5.0 / 255
+    spec = avd.EngineSpec.nlmeans(None, hq(0, 4, 2, sigma, strength=0.9),
+                                  avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    check_group(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, 0, 4, 2, 0.9, chroma=True,
+                hq_sigma=sigma, min_raw=0.95)
