@@ -151,3 +151,103 @@ def nlm_stream_repeat(frames: list[np.ndarray], d: int, a: int, s: int, h2: floa
         window = [frames[min(max(i + k, 0), n - 1)] for k in range(-d, d + 1)]
         outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, lut=lut, wref=wref, fp64=fp64))
     return outs
+
+
+# ---- NL4D collaborative filter (collab_oracle.cpp) ------------------------------------------------
+
+class CollabArgs(C.Structure):
+    _fields_ = [
+        ("ring", _fp), ("mv_field", C.POINTER(C.c_int32)), ("confidence", _fp),
+        ("neighbour_slots", C.POINTER(C.c_uint32)), ("sigma", _fp), ("noise_curve", _fp),
+        ("dct_profile", _fp), ("kaiser", _fp), ("accum", C.POINTER(C.c_int32)),
+        ("wsum", C.POINTER(C.c_int32)), ("group_weight", _fp),
+        ("width", C.c_int), ("height", C.c_int), ("channels", C.c_int), ("centre_slot", C.c_int),
+        ("radius", C.c_int), ("grid_frames", C.c_int), ("refine", C.c_int), ("spatial_radius", C.c_int),
+        ("k_max", C.c_int), ("mv_stride", C.c_int), ("conf_stride", C.c_int), ("blk_step", C.c_int),
+        ("blksize", C.c_int), ("blocks_x", C.c_int), ("blocks_y", C.c_int),
+        ("c_min", C.c_float), ("lambda_ht", C.c_float), ("accum_scale", C.c_float), ("pool_ratio", C.c_float),
+        ("weight_scale", C.c_float), ("pooled", C.c_int), ("curve_valid", C.c_int),
+    ]
+
+
+def dct_noise_profile(rho: float) -> np.ndarray:
+    out = np.empty(8, np.float32)
+    l = lib()
+    l.orc_dct_noise_profile.argtypes = [C.c_float, _fp]
+    l.orc_dct_noise_profile(rho, _f(out))
+    return out
+
+
+def kaiser_window(beta: float) -> np.ndarray:
+    out = np.empty(8, np.float32)
+    l = lib()
+    l.orc_kaiser_window.argtypes = [C.c_float, _fp]
+    l.orc_kaiser_window(beta, _f(out))
+    return out
+
+
+def cross_frame_accum_scale(spatial_radius: int, temporal_radius: int) -> float:
+    l = lib()
+    l.orc_cross_frame_accum_scale.argtypes = [C.c_uint32, C.c_uint32]
+    l.orc_cross_frame_accum_scale.restype = C.c_float
+    return float(l.orc_cross_frame_accum_scale(spatial_radius, temporal_radius))
+
+
+def weight_scale(sigma: float, profile: np.ndarray) -> float:
+    """aggregate.rs:79-99: sigma^2 * g_max^2 in f32, floored at 1e-12."""
+    f = np.float32
+    g = f(np.max(profile))
+    norm = ((f(sigma) * f(sigma)) * g) * g
+    return float(norm) if np.isfinite(norm) and norm > f(1e-12) else 1e-12
+
+
+def grid_frames(radius: int) -> int:
+    """collab/mod.rs:48-54."""
+    return 1 if radius == 0 else (2 if radius == 1 else 4)
+
+
+def refs_along(dim: int) -> int:
+    return (dim - 8 + 3) // 4 + 1
+
+
+def collab_fused(ring: np.ndarray, width: int, height: int, channels: int, *, centre_slot=0, radius=0,
+                 mv_field=None, confidence=None, neighbour_slots=None, c_min=0.0, refine=0, spatial_radius=4,
+                 k_max=8, sigma=(0.02,), lambda_ht=5.3, rho=0.0, profile=None, kaiser_beta=0.0,
+                 noise_curve=None, pooled=None, blksize=16, blk_step=8, blocks_x=1, blocks_y=1,
+                 mv_stride=2, conf_stride=1, weight_scale_override=None):
+    """One `collab_fused` launch on the CPU. Returns (accum, wsum, group_weight)."""
+    ring = np.ascontiguousarray(ring, np.float32)
+    frames = ring.size // (width * height * channels)
+    profile = dct_noise_profile(rho) if profile is None else np.asarray(profile, np.float32)
+    kaiser = kaiser_window(kaiser_beta)
+    sig = np.asarray(sigma, np.float32)
+    if sig.size < channels:
+        sig = np.full(channels, sig[0], np.float32)
+    ws = weight_scale(float(sig[0]), profile) if weight_scale_override is None else weight_scale_override
+    mv = np.ascontiguousarray(mv_field if mv_field is not None else np.zeros(2, np.int32), np.int32)
+    conf = np.ascontiguousarray(confidence if confidence is not None else np.ones(1, np.float32), np.float32)
+    slots = np.ascontiguousarray(neighbour_slots if neighbour_slots is not None else np.zeros(1, np.uint32),
+                                 np.uint32)
+    curve = np.ascontiguousarray(noise_curve if noise_curve is not None else np.zeros(16, np.float32), np.float32)
+    accum = np.zeros(width * height * channels * frames, np.int32)
+    wsum = np.zeros(width * height * frames, np.int32)
+    gw = np.zeros(refs_along(width) * refs_along(height), np.float32)
+    a = CollabArgs()
+    a.ring, a.mv_field, a.confidence = _f(ring), mv.ctypes.data_as(C.POINTER(C.c_int32)), _f(conf)
+    a.neighbour_slots = slots.ctypes.data_as(C.POINTER(C.c_uint32))
+    a.sigma, a.noise_curve, a.dct_profile, a.kaiser = _f(sig), _f(curve), _f(profile), _f(kaiser)
+    a.accum, a.wsum = accum.ctypes.data_as(C.POINTER(C.c_int32)), wsum.ctypes.data_as(C.POINTER(C.c_int32))
+    a.group_weight = _f(gw)
+    a.width, a.height, a.channels, a.centre_slot = width, height, channels, centre_slot
+    a.radius, a.grid_frames, a.refine, a.spatial_radius, a.k_max = radius, grid_frames(radius), refine, \
+        spatial_radius, k_max
+    a.mv_stride, a.conf_stride, a.blk_step, a.blksize = mv_stride, conf_stride, blk_step, blksize
+    a.blocks_x, a.blocks_y = blocks_x, blocks_y
+    a.c_min, a.lambda_ht = c_min, lambda_ht
+    a.accum_scale = cross_frame_accum_scale(spatial_radius, radius)
+    a.pool_ratio, a.pooled = (pooled or 0.0), int(pooled is not None)
+    a.weight_scale, a.curve_valid = ws, int(noise_curve is not None)
+    l = lib()
+    l.orc_collab_fused.argtypes = [C.POINTER(CollabArgs)]
+    l.orc_collab_fused(C.byref(a))
+    return accum, wsum, gw
