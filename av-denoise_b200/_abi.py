@@ -149,6 +149,15 @@ class AvdPassTimings(C.Structure):
     _fields_ = [("has_luma", u32), ("has_chroma", u32), ("luma", AvdEngineTiming), ("chroma", AvdEngineTiming)]
 
 
+class AvdCollabPass(C.Structure):
+    _fields_ = [(n, u64) for n in ("ring", "mv_field", "confidence", "neighbour_slots", "noise", "noise_curve",
+                                   "dct_profile", "kaiser", "accum", "wsum", "group_weight")] + \
+               [(n, u32) for n in ("width", "height", "channels", "centre_slot", "sigma_word", "weight_scale_word",
+                                   "curve_valid_word", "radius", "refine", "spatial_radius", "k_max", "mv_stride",
+                                   "conf_stride", "blk_step", "blksize", "blocks_x", "blocks_y", "pooled")] + \
+               [(n, f32) for n in ("c_min", "lambda_ht", "accum_scale", "pool_ratio")]
+
+
 _P = C.POINTER
 _E = C.c_void_p  # AvdEngine*
 
@@ -181,6 +190,10 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_engine_last_error": (C.c_char_p, [_E]),
     "avd_engine_fail_for_test": (C.c_int, [_E]),
     "avd_last_error": (C.c_char_p, []),
+    "avd_collab_pass": (C.c_int, [_P(AvdCollabPass), C.c_void_p]),
+    "avd_dct_noise_profile": (None, [f32, _P(f32)]),
+    "avd_kaiser_window": (None, [f32, _P(f32)]),
+    "avd_cross_frame_accum_scale": (f32, [u32, u32]),
     "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,
                                        _P(AvdPlane), C.c_size_t, _P(AvdPlane), C.c_size_t, C.c_void_p]),
 }

@@ -1,0 +1,699 @@
+// NL4D collaborative filter for sm_100a: group search, 2D DCT + Haar hard/pooled threshold,
+// inverse transforms and fixed-point aggregation, one launch per pass.
+//
+// What it computes (av-denoise-core/src/collab/kernels/fused/mod.rs:170-891): for every reference
+// patch (8x8 on a step-4 grid of the centre frame) the best 8 positions of the centre frame's
+// spatial window (self match pinned first, ties keep the earlier position), optionally grown into
+// volumes along the neighbour frames' motion (fused/trajectory.rs), a 2D DCT per member, a Haar
+// along the stack (or time and volumes), a hard or pooled threshold against lambda x the
+// propagated noise, the inverse transforms, and a Kaiser-tapered fixed-point scatter of every
+// member into its own frame's accumulator region, weighted by 1 / (retained variance).
+//
+// How (B200): one 8-lane group per reference patch, lane `sub` owning column `sub` of every patch
+// the group touches, so every candidate read and every scatter is an 8-wide coalesced access.
+// Cross-lane sums use the xor-1/2/4 shuffle butterfly and the 8x8 transposes a per-group shared
+// region, both scoped to the group's own 8 lanes (`__shfl_*_sync` with the group's mask and
+// `__syncwarp(mask)`), so groups of one warp may take different trip counts through their
+// clipped windows: no block barrier is ever needed. The group's 8 members x 8 values stay in
+// registers through the transforms. Accumulation is integer atomics, so the output does not
+// depend on scheduling.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.h"
+
+namespace avd {
+
+namespace {
+
+constexpr int P = 8;
+constexpr int STEP = 4;
+constexpr int MAX_K = 8;
+constexpr int kGroups = 16;  // reference patches per CTA
+constexpr int kThreads = kGroups * 8;
+constexpr float kUnfilled = 3.0e38f;
+constexpr float kSelfPin = -1.0e38f;
+constexpr float kReciprocalFloor = 1e-12f;
+constexpr float kAccumClamp = 5.0f;
+constexpr float kWeightGain = 5.0f;
+constexpr float kVarianceFloor = 1.0e-20f;
+constexpr float kFrac1Sqrt2 = 0.70710678118654752440f;
+constexpr int kCurveBins = 16;
+
+// The orthonormal 8-point DCT-II taps, c_row * cos(pi * (2 col + 1) row / 16), in f32.
+__constant__ float c_dct[8][8];
+
+struct GroupCtx {
+    unsigned mask;  // this group's 8 lanes of the warp
+    int sub;        // lane within the group
+};
+
+__device__ __forceinline__ float reduce8(const GroupCtx& g, float v) {
+    v += __shfl_xor_sync(g.mask, v, 1);
+    v += __shfl_xor_sync(g.mask, v, 2);
+    v += __shfl_xor_sync(g.mask, v, 4);
+    return v;
+}
+
+__device__ __forceinline__ uint32_t pack_pos_t(uint32_t x, uint32_t y, uint32_t t) {
+    return (t << 26) | (y << 13) | x;
+}
+
+__device__ __forceinline__ uint32_t clamp_top_left(int v, uint32_t max_pos) {
+    return v < 0 ? 0u : (v > static_cast<int>(max_pos) ? max_pos : static_cast<uint32_t>(v));
+}
+
+// fused/plane_ops.rs:38-53: insert into the group's sorted top-8 (one slot per lane); a tie never
+// displaces an incumbent.
+__device__ __forceinline__ void shift_insert8(const GroupCtx& g, float& best_d, uint32_t& best_pos, float d,
+                                              uint32_t packed) {
+    float prev_d = __shfl_up_sync(g.mask, best_d, 1, 8);
+    uint32_t prev_pos = __shfl_up_sync(g.mask, best_pos, 1, 8);
+    if (d < best_d) {
+        if (g.sub == 0 || d >= prev_d) {
+            best_d = d;
+            best_pos = packed;
+        } else {
+            best_d = prev_d;
+            best_pos = prev_pos;
+        }
+    }
+}
+
+// The lane's share of the distance from `ref` (its 8 x C column) to the candidate at (x, y).
+template <int C>
+__device__ __forceinline__ float column_ssd(const float (&ref)[P * C], const float* __restrict__ frame, int width,
+                                            uint32_t x, uint32_t y, int sub) {
+    float s = 0.0f;
+    const float* p = frame + (static_cast<size_t>(y) * width + x + sub) * C;
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            float d = ref[r * C + c] - __ldg(p + static_cast<size_t>(r) * width * C + c);
+            s = fmaf(d, d, s);
+        }
+    }
+    return s;
+}
+
+__device__ __forceinline__ void dct8_fwd(float (&line)[P]) {
+    float s[4], d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        s[k] = line[k] + line[7 - k];
+        d[k] = line[k] - line[7 - k];
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        float even = 0.0f, odd = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            even = fmaf(s[k], c_dct[2 * m][k], even);
+            odd = fmaf(d[k], c_dct[2 * m + 1][k], odd);
+        }
+        line[2 * m] = even;
+        line[2 * m + 1] = odd;
+    }
+}
+
+__device__ __forceinline__ void dct8_inv(float (&line)[P]) {
+    float snap[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) snap[j] = line[j];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float even = 0.0f, odd = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            even = fmaf(snap[2 * m], c_dct[2 * m][k], even);
+            odd = fmaf(snap[2 * m + 1], c_dct[2 * m + 1][k], odd);
+        }
+        line[k] = even + odd;
+        line[7 - k] = even - odd;
+    }
+}
+
+// An 8x8 transpose across the group's lanes through its own shared region of kRegion floats; the
+// index skew of one float every 32 keeps the column reads off a shared bank.
+constexpr int kRegion = 72;
+__device__ __forceinline__ void transpose8(const GroupCtx& g, float* region, float (&v)[P]) {
+#pragma unroll
+    for (int i = 0; i < P; ++i) region[i * 8 + g.sub + (i * 8 + g.sub) / 32] = v[i];
+    __syncwarp(g.mask);
+#pragma unroll
+    for (int i = 0; i < P; ++i) v[i] = region[g.sub * 8 + i + (g.sub * 8 + i) / 32];
+    __syncwarp(g.mask);
+}
+
+
+// fused/pooled.rs: keep a coefficient on the mean energy of itself and its four frequency
+// neighbours; lane `sub` holds vertical frequency `sub`, slot i horizontal frequency i. Returns
+// the lane's retained variance.
+__device__ __forceinline__ float pooled_threshold(const GroupCtx& g, float (&s)[MAX_K][P], const float (&v)[MAX_K],
+                                                  const float (&prof)[P], int k_use, float threshold,
+                                                  float dc_lambda) {
+    const int sub = g.sub;
+    const bool dc_lane = sub == 0, has_up = sub > 0, has_down = sub < 7;
+    const float vertical = 1.0f + (has_up ? 1.0f : 0.0f) + (has_down ? 1.0f : 0.0f);
+    const float bar = threshold * threshold;
+    const float first_col = bar * (vertical + (sub == 1 ? 0.0f : 1.0f));
+    const float second_col = bar * (vertical + (dc_lane ? 1.0f : 2.0f));
+    const float middle_col = bar * (vertical + 2.0f);
+    const float last_col = bar * (vertical + 1.0f);
+    const float prof_sub = prof[sub];
+    float retained = 0.0f;
+#pragma unroll
+    for (int j = 0; j < MAX_K; ++j) {
+        const float lane_var = v[j] * prof_sub;
+        const float lane_inv = 1.0f / fmaxf(lane_var, kVarianceFloor);
+        float e0 = s[j][0] * s[j][0] * lane_inv * (1.0f / fmaxf(prof[0], kVarianceFloor));
+        float current = dc_lane ? 0.0f : e0;
+        float previous = 0.0f;
+        float kept_profile = 0.0f;
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            const float coeff = s[j][i];
+            float next = 0.0f;
+            if (i < 7) next = s[j][i + 1] * s[j][i + 1] * lane_inv * (1.0f / fmaxf(prof[i + 1], kVarianceFloor));
+            const float shuffled_up = __shfl_up_sync(g.mask, current, 1, 8);
+            const float shuffled_down = __shfl_down_sync(g.mask, current, 1, 8);
+            float sum = current + (has_down ? shuffled_down : 0.0f) + (has_up ? shuffled_up : 0.0f);
+            if (i > 0) sum += previous;
+            if (i < 7) sum += next;
+            const float col_bar = i == 0 ? first_col : (i == 1 ? second_col : (i == 7 ? last_col : middle_col));
+            bool keep = sum >= col_bar;
+            if (i == 0) {
+                const bool own = fabsf(coeff) >= dc_lambda * sqrtf(lane_var * prof[0]);
+                keep = dc_lane ? own : keep;
+                if (j == 0) keep = keep || dc_lane;
+            }
+            kept_profile += keep ? prof[i] : 0.0f;
+            if (j < k_use && !keep) s[j][i] = 0.0f;
+            previous = current;
+            current = next;
+        }
+        if (j < k_use) retained += kept_profile * lane_var;
+    }
+    return retained;
+}
+
+// The Haar ladder over the stack of k_use members (transforms.rs:124-191) and its variance shadow.
+__device__ __forceinline__ void haar_level(float (&s)[MAX_K][P], int len, bool inverse) {
+    const int half = len / 2;
+#pragma unroll
+    for (int pos = 0; pos < P; ++pos) {
+        float snap[MAX_K];
+#pragma unroll
+        for (int k = 0; k < MAX_K; ++k) snap[k] = s[k][pos];
+#pragma unroll
+        for (int p = 0; p < MAX_K / 2; ++p) {
+            if (p >= half) break;
+            if (!inverse) {
+                s[p][pos] = (snap[2 * p] + snap[2 * p + 1]) * kFrac1Sqrt2;
+                s[half + p][pos] = (snap[2 * p] - snap[2 * p + 1]) * kFrac1Sqrt2;
+            } else {
+                s[2 * p][pos] = (snap[p] + snap[half + p]) * kFrac1Sqrt2;
+                s[2 * p + 1][pos] = (snap[p] - snap[half + p]) * kFrac1Sqrt2;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void variance_level(float (&v)[MAX_K], int len) {
+    const int half = len / 2;
+    float snap[MAX_K];
+#pragma unroll
+    for (int k = 0; k < MAX_K; ++k) snap[k] = v[k];
+#pragma unroll
+    for (int p = 0; p < MAX_K / 2; ++p) {
+        if (p >= half) break;
+        const float mean = (snap[2 * p] + snap[2 * p + 1]) * 0.5f;
+        v[p] = mean;
+        v[half + p] = mean;
+    }
+}
+
+// fused/grid.rs: strided Haar levels (time inside a volume, then across volumes).
+template <int START, int STRIDE, int LEN>
+__device__ __forceinline__ void strided_level(float (&vals)[MAX_K], bool inverse, bool variance) {
+    constexpr int half = LEN / 2;
+    float snap[LEN];
+#pragma unroll
+    for (int k = 0; k < LEN; ++k) snap[k] = vals[START + k * STRIDE];
+#pragma unroll
+    for (int p = 0; p < half; ++p) {
+        if (variance) {
+            const float mean = (snap[2 * p] + snap[2 * p + 1]) * 0.5f;
+            vals[START + p * STRIDE] = mean;
+            vals[START + (half + p) * STRIDE] = mean;
+        } else if (!inverse) {
+            vals[START + p * STRIDE] = (snap[2 * p] + snap[2 * p + 1]) * kFrac1Sqrt2;
+            vals[START + (half + p) * STRIDE] = (snap[2 * p] - snap[2 * p + 1]) * kFrac1Sqrt2;
+        } else {
+            vals[START + 2 * p * STRIDE] = (snap[p] + snap[half + p]) * kFrac1Sqrt2;
+            vals[START + (2 * p + 1) * STRIDE] = (snap[p] - snap[half + p]) * kFrac1Sqrt2;
+        }
+    }
+}
+
+template <int START, int STRIDE, int LEN>
+__device__ __forceinline__ void strided_fwd(float (&vals)[MAX_K], bool variance) {
+    if constexpr (LEN >= 4) strided_level<START, STRIDE, 4>(vals, false, variance);
+    if constexpr (LEN >= 2) strided_level<START, STRIDE, 2>(vals, false, variance);
+}
+
+template <int START, int STRIDE, int LEN>
+__device__ __forceinline__ void strided_inv(float (&vals)[MAX_K]) {
+    if constexpr (LEN >= 2) strided_level<START, STRIDE, 2>(vals, true, false);
+    if constexpr (LEN >= 4) strided_level<START, STRIDE, 4>(vals, true, false);
+}
+
+template <int GF, int V = 0>
+__device__ __forceinline__ void volumes_fwd(float (&vals)[MAX_K], bool variance) {
+    if constexpr (V < MAX_K / GF) {
+        strided_fwd<V * GF, 1, GF>(vals, variance);
+        volumes_fwd<GF, V + 1>(vals, variance);
+    }
+}
+
+template <int GF, int F = 0>
+__device__ __forceinline__ void frames_fwd(float (&vals)[MAX_K], bool variance) {
+    if constexpr (F < GF) {
+        strided_fwd<F, GF, MAX_K / GF>(vals, variance);
+        frames_fwd<GF, F + 1>(vals, variance);
+    }
+}
+
+template <int GF, int V = 0>
+__device__ __forceinline__ void volumes_inv(float (&vals)[MAX_K]) {
+    if constexpr (V < MAX_K / GF) {
+        strided_inv<V * GF, 1, GF>(vals);
+        volumes_inv<GF, V + 1>(vals);
+    }
+}
+
+template <int GF, int F = 0>
+__device__ __forceinline__ void frames_inv(float (&vals)[MAX_K]) {
+    if constexpr (F < GF) {
+        strided_inv<F, GF, MAX_K / GF>(vals);
+        frames_inv<GF, F + 1>(vals);
+    }
+}
+
+template <int GF>
+__device__ __forceinline__ void grid_fwd(float (&s)[MAX_K][P]) {
+#pragma unroll
+    for (int pos = 0; pos < P; ++pos) {
+        float vals[MAX_K];
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) vals[m] = s[m][pos];
+        volumes_fwd<GF>(vals, false);
+        frames_fwd<GF>(vals, false);
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) s[m][pos] = vals[m];
+    }
+}
+
+template <int GF>
+__device__ __forceinline__ void grid_inv(float (&s)[MAX_K][P]) {
+#pragma unroll
+    for (int pos = 0; pos < P; ++pos) {
+        float vals[MAX_K];
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) vals[m] = s[m][pos];
+        frames_inv<GF>(vals);
+        volumes_inv<GF>(vals);
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) s[m][pos] = vals[m];
+    }
+}
+
+template <int GF>
+__device__ __forceinline__ void grid_variance(float (&v)[MAX_K]) {
+    volumes_fwd<GF>(v, true);
+    frames_fwd<GF>(v, true);
+}
+
+// aggregate.rs:147-160.
+__device__ __forceinline__ int32_t to_fixed(float value, float scale) {
+    return static_cast<int32_t>(roundf(fminf(fmaxf(value, -kAccumClamp), kAccumClamp) * scale));
+}
+
+__device__ __forceinline__ int32_t to_fixed_weight(float weight, float scale) {
+    return static_cast<int32_t>(roundf(fminf(fmaxf(weight, 0.0f), 1.0f) * scale * kWeightGain));
+}
+
+__device__ __forceinline__ uint32_t covering_lo(uint32_t patch_start, uint32_t blksize, uint32_t step) {
+    const uint32_t overhang = max(patch_start + P, blksize) - blksize;
+    return (overhang + step - 1) / step;
+}
+
+constexpr int kMaxRects = 16;  // MAX_COVERING_BLOCKS^2
+
+// fused/trajectory.rs (clipped walk): for each neighbour frame the best candidate over one refine
+// rectangle per covering motion block (blocks under c_min skipped, rectangles already searched and
+// positions the group holds skipped), inserted into the volume's sorted tail.
+template <int C, int GF, int FIRST>
+__device__ __forceinline__ void trajectory_search(const GroupCtx& g, const CollabLaunch& a, const float (&anchor)[P * C],
+                                                  uint32_t ax, uint32_t ay, float scale, float (&grid_d)[MAX_K],
+                                                  uint32_t (&grid_pos)[MAX_K]) {
+    constexpr int TAIL = GF - 1;
+    const uint32_t max_x = a.width - P, max_y = a.height - P;
+    const uint32_t covers = (a.blksize + a.blk_step - 1) / a.blk_step;
+    const uint32_t bx_hi = min(ax / a.blk_step, static_cast<uint32_t>(a.blocks_x - 1));
+    const uint32_t by_hi = min(ay / a.blk_step, static_cast<uint32_t>(a.blocks_y - 1));
+    const uint32_t bx_lo = min(covering_lo(ax, a.blksize, a.blk_step), bx_hi);
+    const uint32_t by_lo = min(covering_lo(ay, a.blksize, a.blk_step), by_hi);
+    for (int t = 0; t < 2 * a.radius; ++t) {
+        const int slot = static_cast<int>(a.neighbour_slots[t]);
+        const float* frame = a.ring + static_cast<size_t>(slot) * a.frame_elems;
+        const uint32_t packed_t = t + 1;
+        float frame_d = kUnfilled;
+        uint32_t frame_pos = 0;
+        uint32_t sl[kMaxRects], sr[kMaxRects], st[kMaxRects], sb[kMaxRects];
+        for (uint32_t i = 0; i < covers * covers; ++i) {
+            sl[i] = 1;
+            sr[i] = 0;
+            st[i] = 1;
+            sb[i] = 0;
+        }
+        for (uint32_t iy = 0; iy < covers; ++iy)
+            for (uint32_t ix = 0; ix < covers; ++ix) {
+                const uint32_t bx = bx_lo + ix, by = by_lo + iy;
+                if (bx > bx_hi || by > by_hi) continue;
+                const uint32_t block = by * a.blocks_x + bx;
+                if (!(__ldg(a.confidence + t * a.conf_stride + block) >= a.c_min)) continue;
+                const int mvx = __ldg(a.mv_field + t * a.mv_stride + block * 2);
+                const int mvy = __ldg(a.mv_field + t * a.mv_stride + block * 2 + 1);
+                const uint32_t left = clamp_top_left(static_cast<int>(ax) + mvx - a.refine, max_x);
+                const uint32_t right = clamp_top_left(static_cast<int>(ax) + mvx + a.refine, max_x);
+                const uint32_t top = clamp_top_left(static_cast<int>(ay) + mvy - a.refine, max_y);
+                const uint32_t bottom = clamp_top_left(static_cast<int>(ay) + mvy + a.refine, max_y);
+                bool contained = false;
+                for (uint32_t i = 0; i < covers * covers; ++i)
+                    contained |= left >= sl[i] && right <= sr[i] && top >= st[i] && bottom <= sb[i];
+                if (!contained) {
+                    for (uint32_t cy = top; cy <= bottom; ++cy)
+                        for (uint32_t cx = left; cx <= right; ++cx) {
+                            bool skip = false;
+                            for (uint32_t i = 0; i < covers * covers; ++i)
+                                skip |= cy >= st[i] && cy <= sb[i] && cx >= sl[i] && cx <= sr[i];
+                            const uint32_t packed = pack_pos_t(cx, cy, packed_t);
+#pragma unroll
+                            for (int k = 0; k < FIRST; ++k) skip |= grid_pos[k] == packed;
+                            if (skip) continue;
+                            const float d = reduce8(g, column_ssd<C>(anchor, frame, a.width, cx, cy, g.sub)) * scale;
+                            if (d < frame_d) {
+                                frame_d = d;
+                                frame_pos = packed;
+                            }
+                        }
+                }
+                sl[iy * covers + ix] = left;
+                sr[iy * covers + ix] = right;
+                st[iy * covers + ix] = top;
+                sb[iy * covers + ix] = bottom;
+            }
+        float carry_d = frame_d;
+        uint32_t carry_pos = frame_pos;
+#pragma unroll
+        for (int j = 0; j < TAIL; ++j) {
+            const float held_d = grid_d[FIRST + j];
+            const uint32_t held_pos = grid_pos[FIRST + j];
+            if (carry_d < held_d) {
+                grid_d[FIRST + j] = carry_d;
+                grid_pos[FIRST + j] = carry_pos;
+                carry_d = held_d;
+                carry_pos = held_pos;
+            }
+        }
+    }
+}
+
+template <int C, int GF, int VOL = 0>
+__device__ __forceinline__ void search_volumes(const GroupCtx& g, const CollabLaunch& a, const uint32_t (&member_pos)[MAX_K],
+                                               float scale, float (&grid_d)[MAX_K], uint32_t (&grid_pos)[MAX_K]) {
+    if constexpr (VOL < MAX_K / GF) {
+        constexpr int FIRST = VOL * GF;
+        const uint32_t anchor_packed = member_pos[VOL];
+        const uint32_t ax = anchor_packed & 0x1FFFu, ay = (anchor_packed >> 13) & 0x1FFFu;
+        grid_pos[FIRST] = anchor_packed;
+        grid_d[FIRST] = 0.0f;
+#pragma unroll
+        for (int j = 1; j < GF; ++j) {
+            grid_pos[FIRST + j] = 0;
+            grid_d[FIRST + j] = kUnfilled;
+        }
+        float anchor[P * C];
+        const float* centre = a.ring + static_cast<size_t>(a.centre_slot) * a.frame_elems;
+#pragma unroll
+        for (int r = 0; r < P; ++r)
+#pragma unroll
+            for (int c = 0; c < C; ++c)
+                anchor[r * C + c] = __ldg(centre + ((static_cast<size_t>(ay) + r) * a.width + ax + g.sub) * C + c);
+        trajectory_search<C, GF, FIRST + 1>(g, a, anchor, ax, ay, scale, grid_d, grid_pos);
+        search_volumes<C, GF, VOL + 1>(g, a, member_pos, scale, grid_d, grid_pos);
+    }
+}
+
+template <int C, int GF>
+__global__ void __launch_bounds__(kThreads) collab_kernel(CollabLaunch a) {
+    __shared__ float transpose_buf[kGroups * kRegion];
+    const int lane = threadIdx.x & 31;
+    const int group = threadIdx.x >> 3;
+    GroupCtx g;
+    g.sub = threadIdx.x & 7;
+    g.mask = 0xFFu << (lane & ~7);
+    float* region = transpose_buf + group * kRegion;
+
+    const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
+    const uint32_t ix = blockIdx.x * kGroups + group;
+    if (ix >= refs_x) return;  // the group's 8 lanes leave together; no barrier spans groups
+    const uint32_t iy = blockIdx.y;
+    const uint32_t max_x = a.width - P, max_y = a.height - P;
+    const uint32_t rx = min(ix * STEP, max_x), ry = min(iy * STEP, max_y);
+    const float scale = C == 1 ? 3.0f : 1.5f;
+    const float* centre = a.ring + static_cast<size_t>(a.centre_slot) * a.frame_elems;
+
+    float cur[P * C];
+#pragma unroll
+    for (int r = 0; r < P; ++r)
+#pragma unroll
+        for (int c = 0; c < C; ++c) cur[r * C + c] = __ldg(centre + ((static_cast<size_t>(ry) + r) * a.width + rx + g.sub) * C + c);
+
+    // Centre search (fused/centre.rs:213-258), row by row over the clipped window.
+    float best_d = kUnfilled;
+    uint32_t best_pos = 0;
+    float worst = kUnfilled;
+    const uint32_t left = clamp_top_left(static_cast<int>(rx) - a.spatial_radius, max_x);
+    const uint32_t right = clamp_top_left(static_cast<int>(rx) + a.spatial_radius, max_x);
+    const uint32_t top = clamp_top_left(static_cast<int>(ry) - a.spatial_radius, max_y);
+    const uint32_t bottom = clamp_top_left(static_cast<int>(ry) + a.spatial_radius, max_y);
+    for (uint32_t cy = top; cy <= bottom; ++cy)
+        for (uint32_t cx = left; cx <= right; ++cx) {
+            float d = reduce8(g, column_ssd<C>(cur, centre, a.width, cx, cy, g.sub)) * scale;
+            if (cx == rx && cy == ry) d = kSelfPin;
+            if (d < worst) {
+                shift_insert8(g, best_d, best_pos, d, pack_pos_t(cx, cy, 0));
+                worst = __shfl_sync(g.mask, best_d, 7, 8);
+            }
+        }
+    const uint32_t n_live = (right - left + 1) * (bottom - top + 1);
+    int k_use = 1;
+    while (static_cast<uint32_t>(k_use * 2) <= n_live && k_use * 2 <= a.k_max) k_use *= 2;
+    uint32_t member_pos[MAX_K];
+#pragma unroll
+    for (int m = 0; m < MAX_K; ++m) member_pos[m] = __shfl_sync(g.mask, best_pos, m, 8);
+
+    bool use_grid = false;
+    if constexpr (GF > 1) {
+        if (a.k_max == MAX_K) {
+            float grid_d[MAX_K];
+            uint32_t grid_pos[MAX_K];
+            search_volumes<C, GF>(g, a, member_pos, scale, grid_d, grid_pos);
+            use_grid = k_use == MAX_K;
+#pragma unroll
+            for (int v = 0; v < MAX_K / GF; ++v) use_grid = use_grid && grid_d[v * GF + GF - 1] < kUnfilled;
+            if (use_grid) {
+#pragma unroll
+                for (int m = 0; m < MAX_K; ++m) member_pos[m] = grid_pos[m];
+                k_use = MAX_K;
+            }
+        }
+    }
+
+    // filter_group (fused/mod.rs:559-850).
+    int member_slot[MAX_K];
+#pragma unroll
+    for (int m = 0; m < MAX_K; ++m) {
+        const uint32_t t = member_pos[m] >> 26;
+        member_slot[m] = t > 0 ? static_cast<int>(__ldg(a.neighbour_slots + t - 1)) : a.centre_slot;
+    }
+    float prof[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) prof[i] = __ldg(a.dct_profile + i);
+    float col_first = 0.0f;
+#pragma unroll
+    for (int r = 0; r < P; ++r) col_first += cur[r * C];
+    const float patch_luma = reduce8(g, col_first) / 64.0f;
+    const float bins = static_cast<float>(kCurveBins);
+    const float curve_pos = fminf(fmaxf(patch_luma * bins - 0.5f, 0.0f), bins - 1.0f);
+    const uint32_t lower = min(static_cast<uint32_t>(curve_pos), static_cast<uint32_t>(kCurveBins - 2));
+    const float fraction = curve_pos - static_cast<float>(lower);
+    const bool curve_valid = __ldg(a.noise + a.curve_valid_word) != 0.0f;
+    float ratio = 0.0f;
+    if (curve_valid) {
+        const float lo = __ldg(a.noise_curve + lower), hi = __ldg(a.noise_curve + lower + 1);
+        ratio = lo + (hi - lo) * fraction;
+    }
+    const float luma_scale = curve_valid ? fminf(fmaxf(ratio, 0.33f), 3.0f) : 1.0f;
+    const float first_lambda = a.lambda_ht * luma_scale;
+    const float second_lambda = a.lambda_ht;
+    const float weight_scale = __ldg(a.noise + a.weight_scale_word);
+    const uint32_t ref_idx = iy * refs_x + ix;
+    const int64_t plane = static_cast<int64_t>(a.width) * a.height;
+    float scaled_weight = 0.0f;
+    float kaiser_r[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) kaiser_r[r] = __ldg(a.kaiser + r);
+    const float kaiser_sub = __ldg(a.kaiser + g.sub);
+
+#pragma unroll 1
+    for (int c = 0; c < C; ++c) {
+        const float sig = __ldg(a.noise + a.sigma_word + c);
+        const float base_sig2 = sig * sig;
+        float s[MAX_K][P];
+        float mv[MAX_K];
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) {
+            const uint32_t mx = member_pos[m] & 0x1FFFu, my = (member_pos[m] >> 13) & 0x1FFFu;
+            const float* src = a.ring + static_cast<size_t>(member_slot[m]) * a.frame_elems;
+            mv[m] = base_sig2;
+#pragma unroll
+            for (int r = 0; r < P; ++r) s[m][r] = __ldg(src + ((static_cast<size_t>(my) + r) * a.width + mx + g.sub) * C + c);
+        }
+        if (GF > 1 && use_grid) {
+            grid_variance<(GF > 1 ? GF : 2)>(mv);
+        } else {
+            if (k_use >= 8) variance_level(mv, 8);
+            if (k_use >= 4) variance_level(mv, 4);
+            if (k_use >= 2) variance_level(mv, 2);
+        }
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) {
+            dct8_fwd(s[m]);
+            transpose8(g, region, s[m]);
+            dct8_fwd(s[m]);
+        }
+        if (GF > 1 && use_grid) {
+            grid_fwd<(GF > 1 ? GF : 2)>(s);
+        } else {
+            if (k_use >= 8) haar_level(s, 8, false);
+            if (k_use >= 4) haar_level(s, 4, false);
+            if (k_use >= 2) haar_level(s, 2, false);
+        }
+        const float channel_lambda = c == 0 ? first_lambda : second_lambda;
+        float retained = 0.0f;
+        if (a.pooled) {
+            retained = pooled_threshold(g, s, mv, prof, k_use, channel_lambda * a.pool_ratio, channel_lambda);
+        } else {
+            const float prof_sub = __ldg(a.dct_profile + g.sub);
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                const float factor = prof[i] * prof_sub;
+#pragma unroll
+                for (int j = 0; j < MAX_K; ++j) {
+                    if (j < k_use) {
+                        const float cv = mv[j] * factor;
+                        bool keep = fabsf(s[j][i]) >= channel_lambda * sqrtf(cv);
+                        if (j == 0 && i == 0 && g.sub == 0) keep = true;
+                        if (keep) retained += cv;
+                        else s[j][i] = 0.0f;
+                    }
+                }
+            }
+        }
+        const float sum = reduce8(g, retained);
+        const float weight = (isnan(sum) || isinf(sum)) ? 0.0f : 1.0f / fmaxf(sum, kReciprocalFloor);
+        if (c == 0) {
+            if (g.sub == 0) a.group_weight[ref_idx] = weight;
+            scaled_weight = weight * weight_scale;
+        }
+        if (GF > 1 && use_grid) {
+            grid_inv<(GF > 1 ? GF : 2)>(s);
+        } else {
+            if (k_use >= 2) haar_level(s, 2, true);
+            if (k_use >= 4) haar_level(s, 4, true);
+            if (k_use >= 8) haar_level(s, 8, true);
+        }
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) {
+            dct8_inv(s[m]);
+            transpose8(g, region, s[m]);
+            dct8_inv(s[m]);
+        }
+        // aggregate.rs:176-211 (`scatter_patch`).
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) {
+            if (m >= k_use) break;
+            const uint32_t mx = member_pos[m] & 0x1FFFu, my = (member_pos[m] >> 13) & 0x1FFFu;
+#pragma unroll
+            for (int r = 0; r < P; ++r) {
+                const float w = scaled_weight * (kaiser_r[r] * kaiser_sub);
+                const int64_t pixel = member_slot[m] * plane + (static_cast<int64_t>(my) + r) * a.width + mx + g.sub;
+                atomicAdd(a.accum + pixel * C + c, to_fixed(s[m][r] * w, a.accum_scale));
+                if (c == 0) atomicAdd(a.wsum + pixel, to_fixed_weight(w, a.accum_scale));
+            }
+        }
+    }
+}
+
+template <int C, int GF>
+cudaError_t launch_cg(const CollabLaunch& a, cudaStream_t stream) {
+    const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
+    const uint32_t refs_y = (a.height - P + STEP - 1) / STEP + 1;
+    dim3 grid((refs_x + kGroups - 1) / kGroups, refs_y);
+    collab_kernel<C, GF><<<grid, kThreads, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t upload_taps() {
+    static bool done = false;
+    if (done) return cudaSuccess;
+    float taps[8][8];
+    for (int row = 0; row < 8; ++row)
+        for (int col = 0; col < 8; ++col) {
+            const double scale = row == 0 ? 1.0 / 2.8284271247461903 : 0.5;
+            taps[row][col] = static_cast<float>(scale * cos(3.14159265358979323846 * (2.0 * col + 1.0) * row / 16.0));
+        }
+    cudaError_t e = cudaMemcpyToSymbol(c_dct, taps, sizeof(taps));
+    if (e == cudaSuccess) done = true;
+    return e;
+}
+
+}  // namespace
+
+cudaError_t launch_collab(const CollabLaunch& a, cudaStream_t stream) {
+    if (a.width < P || a.height < P || a.k_max < 1 || a.k_max > MAX_K || a.radius < 0 || a.radius > 8)
+        return cudaErrorInvalidValue;
+    if ((a.blksize + a.blk_step - 1) / max(a.blk_step, 1) > 4 || a.blk_step < 1) return cudaErrorInvalidValue;
+    cudaError_t e = upload_taps();
+    if (e != cudaSuccess) return e;
+    const int gf = a.radius == 0 ? 1 : (a.radius == 1 ? 2 : 4);
+    if (a.channels == 1) {
+        if (gf == 1) return launch_cg<1, 1>(a, stream);
+        if (gf == 2) return launch_cg<1, 2>(a, stream);
+        return launch_cg<1, 4>(a, stream);
+    }
+    if (a.channels == 2) {
+        if (gf == 1) return launch_cg<2, 1>(a, stream);
+        if (gf == 2) return launch_cg<2, 2>(a, stream);
+        return launch_cg<2, 4>(a, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace avd

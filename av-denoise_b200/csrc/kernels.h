@@ -50,4 +50,29 @@ struct NlmLaunch {
 
 cudaError_t launch_nlm(const NlmLaunch& args, cudaStream_t stream);
 
+// One NL4D collaborative-filter pass (collab/kernels/fused/mod.rs:170): every reference patch of
+// the centre slot, scattered into the per-slot fixed-point accumulators.
+struct CollabLaunch {
+    const float* ring;  // slots of width*height*channels f32
+    int width, height, channels, centre_slot;
+    int64_t frame_elems;
+    const int32_t* mv_field;        // per neighbour: blocks x (dx, dy)
+    const float* confidence;        // per neighbour: blocks
+    const uint32_t* neighbour_slots;  // ring slot of each neighbour index
+    const float* noise;             // derived words
+    int sigma_word, weight_scale_word, curve_valid_word;
+    const float* noise_curve;       // 16 ratios
+    const float* dct_profile;       // 8
+    const float* kaiser;            // 8
+    int32_t* accum;                 // slots x pixels x channels
+    int32_t* wsum;                  // slots x pixels
+    float* group_weight;            // refs
+    float c_min, lambda_ht, accum_scale, pool_ratio;
+    int pooled;
+    int radius, refine, spatial_radius, k_max;
+    int mv_stride, conf_stride, blk_step, blksize, blocks_x, blocks_y;
+};
+
+cudaError_t launch_collab(const CollabLaunch& args, cudaStream_t stream);
+
 }  // namespace avd

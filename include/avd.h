@@ -342,6 +342,43 @@ AVD_API const char* avd_engine_last_error(const AvdEngine* engine);
  * forces a GPU-class failure through the poison guard, with no GPU work. */
 AVD_API AvdStatus avd_engine_fail_for_test(AvdEngine* engine);
 
+/* ---- NL4D kernel-level entry points ------------------------------------------------------- */
+
+/* The arguments of one NL4D collaborative-filter pass over device buffers, as the reference's
+ * `collab_fused` launch takes them (av-denoise-core/src/collab/kernels/fused/mod.rs:170-234). */
+typedef struct AvdCollabPass {
+    uint64_t ring;            /* f32 frames, `slots` x height x width x channels, interleaved */
+    uint64_t mv_field;        /* i32 (dx, dy) per motion block per neighbour, `mv_stride` apart */
+    uint64_t confidence;      /* f32 per motion block per neighbour, `conf_stride` apart */
+    uint64_t neighbour_slots; /* u32 ring slot of each neighbour index */
+    uint64_t noise;           /* f32 derived words */
+    uint64_t noise_curve;     /* 16 f32 luma curve ratios */
+    uint64_t dct_profile;     /* 8 f32 per-frequency variance multipliers */
+    uint64_t kaiser;          /* 8 f32 aggregation taps */
+    uint64_t accum;           /* i32, slots x height x width x channels, accumulated into */
+    uint64_t wsum;            /* i32, slots x height x width, accumulated into */
+    uint64_t group_weight;    /* f32 per reference patch, written */
+    uint32_t width, height, channels, centre_slot;
+    uint32_t sigma_word, weight_scale_word, curve_valid_word; /* indices into `noise` */
+    uint32_t radius, refine, spatial_radius, k_max;
+    uint32_t mv_stride, conf_stride, blk_step, blksize, blocks_x, blocks_y;
+    uint32_t pooled;
+    float c_min, lambda_ht, accum_scale, pool_ratio;
+} AvdCollabPass;
+
+/* av-denoise-core/src/collab/kernels/fused/mod.rs:170 (`collab_fused`): one pass, queued on
+ * `stream`. Adds into `accum`/`wsum` (integer adds: the result does not depend on scheduling). */
+AVD_API AvdStatus avd_collab_pass(const AvdCollabPass* pass, void* stream);
+
+/* av-denoise-core/src/collab/kernels/transforms.rs:196-221 (`dct_noise_profile`). */
+AVD_API void avd_dct_noise_profile(float rho, float* out8);
+
+/* av-denoise-core/src/collab/kernels/aggregate.rs:114-132 (`kaiser_window`). */
+AVD_API void avd_kaiser_window(float beta, float* out8);
+
+/* av-denoise-core/src/collab/kernels/aggregate.rs:33-54 (`cross_frame_accum_scale`). */
+AVD_API float avd_cross_frame_accum_scale(uint32_t spatial_radius, uint32_t temporal_radius);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 
 /* No counterpart in the reference. One fast-variant NLMeans output frame for callers that cannot
