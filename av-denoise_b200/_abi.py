@@ -158,6 +158,13 @@ class AvdCollabPass(C.Structure):
                [(n, f32) for n in ("c_min", "lambda_ht", "accum_scale", "pool_ratio")]
 
 
+class AvdMotionPass(C.Structure):
+    _fields_ = [(n, u64) for n in ("pyramid", "neighbour_slots", "mv_field", "confidence", "noise")] + \
+               [(n, u32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize", "overlap",
+                                   "search_radius", "levels", "mv_stride", "conf_stride", "sad_floor_word")] + \
+               [("thsad", f32)]
+
+
 _P = C.POINTER
 _E = C.c_void_p  # AvdEngine*
 
@@ -194,6 +201,11 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_dct_noise_profile": (None, [f32, _P(f32)]),
     "avd_kaiser_window": (None, [f32, _P(f32)]),
     "avd_cross_frame_accum_scale": (f32, [u32, u32]),
+    "avd_motion_pyramid_floats": (u64, [u32, u32, u32, u32]),
+    "avd_motion_pyramid_build": (C.c_int, [u64, u32, u32, u32, u32, u32, u32, u64, u32, C.c_void_p]),
+    "avd_motion_search": (C.c_int, [_P(AvdMotionPass), C.c_void_p]),
+    "avd_sad_noise_floor": (f32, [u32, f32]),
+    "avd_thsad": (f32, [u32, f32]),
     "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,
                                        _P(AvdPlane), C.c_size_t, _P(AvdPlane), C.c_size_t, C.c_void_p]),
 }

@@ -75,4 +75,25 @@ struct CollabLaunch {
 
 cudaError_t launch_collab(const CollabLaunch& args, cudaStream_t stream);
 
+// Block-matching motion search (motion.cu). The pyramid must already hold every slot it reads.
+struct MotionLaunch {
+    const float* pyramid;
+    const uint32_t* neighbour_slots;
+    int32_t* mv_field;
+    float* confidence;  // may be null: no confidence is written
+    const float* noise;
+    int width, height, frame_count, centre_slot, neighbours;
+    int blksize, overlap, search_radius, coarse_radius, coarse_block_factor, levels;
+    int mv_stride, conf_stride, sad_floor_word;
+    float thsad;
+};
+
+int64_t pyramid_slot_pixels(int width, int height, int level);
+void pyramid_level_dims(int width, int height, int level, int* w, int* h);
+int64_t pyramid_level_base(int width, int height, int frame_count, int level);
+int64_t pyramid_floats(int width, int height, int frame_count, int levels);
+cudaError_t launch_pyramid_build(const float* ring, int channels, int width, int height, int frame_count,
+                                 int ring_slot, int levels, float* pyramid, int pyramid_slot, cudaStream_t stream);
+cudaError_t launch_motion_search(const MotionLaunch& args, cudaStream_t stream);
+
 }  // namespace avd

@@ -1,0 +1,360 @@
+// Block-matching motion search on sm_100a: the luma pyramid, the coarse pass on its smallest level
+// and the seeded fine pass at full resolution that writes each block's vector and confidence.
+//
+// Reference behaviour (av-denoise-core/src/motion):
+//   kernels/pyramid.rs:10-61     level 0 is lane 0 of a ring slot; each further level averages 2x2
+//                                pixels, the odd last row/column repeating its edge pixel.
+//   kernels/block_match.rs:117-215, 274-351, 656-760, 787-849
+//                                one search per (block, neighbour): the block's pixels and the
+//                                window the search reaches are staged clamped to the frame; every
+//                                candidate's SAD sums |centre - neighbour| row by row, left to
+//                                right; the lowest SAD wins with the first in row-major order on a
+//                                tie, and the window's centre wins a tie with that pick.
+//   kernels/block_match.rs:505-521  confidence = max(0, (T^2 - e^2) / (T^2 + e^2)),
+//                                e = max(SAD - floor, 0).
+//   analyse.rs:100-150           the coarse level: blksize max(b / 2^l, 2), step max(s / 2^l, 1),
+//                                its winner scaled by 2^l seeds every fine block it covers.
+//
+// Layout in HBM: the pyramid holds, level after level, `frame_count` slots of that level's
+// pixels, each slot padded to a multiple of 8 floats (32 bytes). Vectors are (dx, dy) i32 pairs per
+// block, `mv_stride` values per neighbour; confidence one f32 per block, `conf_stride` per
+// neighbour.
+//
+// Design: one CTA per (block, neighbour); every thread owns one candidate offset and sums its SAD
+// sequentially in the order above (the sum is bit-identical to the reference's for any grouping of
+// candidates, because each SAD is a sequential f32 sum in a fixed order). The argmin packs
+// (SAD bits, candidate index) into one 64-bit key: non-negative floats order like their bit
+// patterns, so the minimum key is the lowest SAD with the lowest index, found with warp shuffles.
+
+#include <cstdint>
+
+#include "kernels.h"
+
+namespace avd {
+namespace {
+
+constexpr int kMaxBlk = 32;
+constexpr int kMaxRadius = 8;
+constexpr float kNoSad = 1.0e30f;
+
+__device__ __forceinline__ int clamp_to(int v, int limit) { return v < 0 ? 0 : (v >= limit ? limit - 1 : v); }
+
+__global__ void pyramid_level0_kernel(const float* __restrict__ ring, float* __restrict__ dst, int64_t pixels,
+                                      int channels, int64_t src_slot_elems) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    dst[p] = ring[src_slot_elems + p * channels];
+}
+
+__global__ void pyramid_down_kernel(const float* __restrict__ src, float* __restrict__ dst, int src_w, int src_h,
+                                    int dst_w, int dst_h) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= dst_w || y >= dst_h) return;
+    const int sx = 2 * x, sy = 2 * y;
+    const int sx1 = sx + 1 < src_w ? sx + 1 : sx;
+    const int sy1 = sy + 1 < src_h ? sy + 1 : sy;
+    const float tl = src[sy * src_w + sx], tr = src[sy * src_w + sx1];
+    const float bl = src[sy1 * src_w + sx], br = src[sy1 * src_w + sx1];
+    dst[y * dst_w + x] = __fmul_rn(__fadd_rn(__fadd_rn(__fadd_rn(tl, tr), bl), br), 0.25f);
+}
+
+struct SearchLevel {
+    const float* pyramid;
+    int width, height;
+    int64_t level_base;  // first value of this level
+    int64_t slot_pixels;
+    int blksize, step, blocks_x, blocks_y;
+};
+
+// The best offset of one window, at thread 0. `sads` holds every candidate's SAD.
+template <int R>
+__device__ __forceinline__ void window_argmin(const float* sads, unsigned long long* warp_keys, int* best_index) {
+    constexpr int kSide = 2 * R + 1;
+    constexpr int kCand = kSide * kSide;
+    const int t = threadIdx.x;
+    unsigned long long key = ~0ull;
+    if (t < kCand) {
+        const float s = sads[t];
+        // Only SADs below the 1e30 start count, and NaN never compares below it.
+        if (s < kNoSad) key = (static_cast<unsigned long long>(__float_as_uint(s)) << 32) | static_cast<unsigned>(t);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other < key ? other : key;
+    }
+    if ((t & 31) == 0) warp_keys[t >> 5] = key;
+    __syncthreads();
+    if (t == 0) {
+        unsigned long long best = warp_keys[0];
+        for (int w = 1; w < static_cast<int>(blockDim.x >> 5); ++w) best = warp_keys[w] < best ? warp_keys[w] : best;
+        *best_index = best == ~0ull ? -1 : static_cast<int>(best & 0xffffffffu);
+    }
+}
+
+// Stages the block (clamped) and the window around `centre` (clamped) and scores every candidate.
+template <int R>
+__device__ __forceinline__ void score_window(const SearchLevel& L, int64_t centre_base, int64_t nbr_base, int ox,
+                                             int oy, int cdx, int cdy, float* centre_tile, float* window,
+                                             float* sads) {
+    constexpr int kSide = 2 * R + 1;
+    const int b = L.blksize;
+    const int wside = b + 2 * R;
+    const int t = threadIdx.x;
+    for (int i = t; i < b * b; i += blockDim.x) {
+        const int py = i / b, px = i - py * b;
+        const int sx = clamp_to(ox + px, L.width), sy = clamp_to(oy + py, L.height);
+        centre_tile[i] = L.pyramid[centre_base + static_cast<int64_t>(sy) * L.width + sx];
+    }
+    const int wx0 = ox + cdx - R, wy0 = oy + cdy - R;
+    for (int i = t; i < wside * wside; i += blockDim.x) {
+        const int wy = i / wside, wx = i - wy * wside;
+        const int sx = clamp_to(wx0 + wx, L.width), sy = clamp_to(wy0 + wy, L.height);
+        window[i] = L.pyramid[nbr_base + static_cast<int64_t>(sy) * L.width + sx];
+    }
+    __syncthreads();
+    if (t < kSide * kSide) {
+        const int dy = t / kSide, dx = t - dy * kSide;
+        float sad = 0.0f;
+        for (int iy = 0; iy < b; ++iy) {
+            const float* wrow = window + (iy + dy) * wside + dx;
+            const float* crow = centre_tile + iy * b;
+            for (int ix = 0; ix < b; ++ix) sad = __fadd_rn(sad, fabsf(__fsub_rn(crow[ix], wrow[ix])));
+        }
+        sads[t] = sad;
+    }
+    __syncthreads();
+}
+
+struct SearchArgs {
+    SearchLevel L;
+    const uint32_t* neighbour_slots;
+    int centre_slot;
+    int32_t* mv_field;
+    int mv_stride;
+    // Coarse only: how coarse blocks map onto the fine grid.
+    int level_scale, fine_blocks_x, fine_blocks_y, fine_step;
+    // Fine only.
+    int use_seed;
+    float* confidence;
+    int conf_stride;
+    const float* noise;
+    int sad_floor_word;
+    float thsad;
+};
+
+// Winner of one window around (cdx, cdy): the reference's `search_window` for a single centre.
+template <int R>
+__device__ __forceinline__ void search_one(const SearchArgs& a, int bx, int by, int n, int cdx, int cdy, int* out_dx,
+                                           int* out_dy, float* out_sad) {
+    constexpr int kSide = 2 * R + 1;
+    __shared__ float centre_tile[kMaxBlk * kMaxBlk];
+    __shared__ float window[(kMaxBlk + 2 * kMaxRadius) * (kMaxBlk + 2 * kMaxRadius)];
+    __shared__ float sads[kSide * kSide];
+    __shared__ unsigned long long warp_keys[(kSide * kSide + 31) / 32];
+    __shared__ int best_index;
+    const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
+    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(a.neighbour_slots[n]) * a.L.slot_pixels;
+    const int ox = bx * a.L.step, oy = by * a.L.step;
+    score_window<R>(a.L, centre_base, nbr_base, ox, oy, cdx, cdy, centre_tile, window, sads);
+    window_argmin<R>(sads, warp_keys, &best_index);
+    if (threadIdx.x == 0) {
+        float best_sad = kNoSad;
+        int bdx = cdx, bdy = cdy;
+        if (best_index >= 0) {
+            best_sad = sads[best_index];
+            bdx = cdx + (best_index % kSide) - R;
+            bdy = cdy + (best_index / kSide) - R;
+        }
+        // A tie resolves to the window's centre (block_match.rs:735-742).
+        const float centre_sad = sads[R * kSide + R];
+        if (centre_sad <= best_sad) {
+            best_sad = centre_sad;
+            bdx = cdx;
+            bdy = cdy;
+        }
+        *out_dx = bdx;
+        *out_dy = bdy;
+        *out_sad = best_sad;
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(320) coarse_kernel(SearchArgs a) {
+    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
+    int dx = 0, dy = 0;
+    float sad = 0.0f;
+    search_one<R>(a, bx, by, n, 0, 0, &dx, &dy, &sad);
+    if (threadIdx.x != 0) return;
+    // block_match.rs:190-214: every fine block inside this coarse block's region takes the scaled
+    // winner; the last coarse block on each axis reaches the fine grid's edge.
+    const int s = a.L.step * a.level_scale;
+    const int c0 = min(bx * s / a.fine_step, a.fine_blocks_x);
+    const int c1 = bx == static_cast<int>(gridDim.x) - 1 ? a.fine_blocks_x : min((bx + 1) * s / a.fine_step, a.fine_blocks_x);
+    const int r0 = min(by * s / a.fine_step, a.fine_blocks_y);
+    const int r1 = by == static_cast<int>(gridDim.y) - 1 ? a.fine_blocks_y : min((by + 1) * s / a.fine_step, a.fine_blocks_y);
+    int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride;
+    for (int r = r0; r < r1; ++r)
+        for (int c = c0; c < c1; ++c) {
+            mv[(r * a.fine_blocks_x + c) * 2] = dx * a.level_scale;
+            mv[(r * a.fine_blocks_x + c) * 2 + 1] = dy * a.level_scale;
+        }
+}
+
+template <int R>
+__global__ void __launch_bounds__(320) fine_kernel(SearchArgs a) {
+    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
+    int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
+    const int sdx = a.use_seed ? mv[0] : 0;
+    const int sdy = a.use_seed ? mv[1] : 0;
+    int dx = 0, dy = 0;
+    float sad = 0.0f;
+    search_one<R>(a, bx, by, n, sdx, sdy, &dx, &dy, &sad);
+    if (threadIdx.x != 0) return;
+    mv[0] = dx;
+    mv[1] = dy;
+    if (a.confidence) {
+        const float floor = a.noise[a.sad_floor_word];
+        float excess = __fsub_rn(sad, floor);
+        if (excess < 0.0f) excess = 0.0f;
+        const float t2 = __fmul_rn(a.thsad, a.thsad);
+        const float e2 = __fmul_rn(excess, excess);
+        float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
+        if (c < 0.0f) c = 0.0f;
+        a.confidence[static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx] = c;
+    }
+}
+
+template <int R>
+cudaError_t launch_search(bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
+    constexpr int kCand = (2 * R + 1) * (2 * R + 1);
+    const int threads = ((kCand + 31) / 32) * 32;
+    if (coarse)
+        coarse_kernel<R><<<grid, threads, 0, s>>>(a);
+    else
+        fine_kernel<R><<<grid, threads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t dispatch_search(int radius, bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
+    switch (radius) {
+        case 0: return launch_search<0>(coarse, a, grid, s);
+        case 1: return launch_search<1>(coarse, a, grid, s);
+        case 2: return launch_search<2>(coarse, a, grid, s);
+        case 3: return launch_search<3>(coarse, a, grid, s);
+        case 4: return launch_search<4>(coarse, a, grid, s);
+        case 5: return launch_search<5>(coarse, a, grid, s);
+        case 6: return launch_search<6>(coarse, a, grid, s);
+        case 7: return launch_search<7>(coarse, a, grid, s);
+        case 8: return launch_search<8>(coarse, a, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+int64_t pyramid_slot_pixels(int width, int height, int level) {
+    int w = width, h = height;
+    for (int l = 0; l < level; ++l) {
+        w = w / 2 > 1 ? w / 2 : 1;
+        h = h / 2 > 1 ? h / 2 : 1;
+    }
+    return (static_cast<int64_t>(w) * h + 7) / 8 * 8;
+}
+
+void pyramid_level_dims(int width, int height, int level, int* w, int* h) {
+    *w = width;
+    *h = height;
+    for (int l = 0; l < level; ++l) {
+        *w = *w / 2 > 1 ? *w / 2 : 1;
+        *h = *h / 2 > 1 ? *h / 2 : 1;
+    }
+}
+
+int64_t pyramid_level_base(int width, int height, int frame_count, int level) {
+    int64_t base = 0;
+    for (int l = 0; l < level; ++l) base += static_cast<int64_t>(frame_count) * pyramid_slot_pixels(width, height, l);
+    return base;
+}
+
+int64_t pyramid_floats(int width, int height, int frame_count, int levels) {
+    return pyramid_level_base(width, height, frame_count, levels);
+}
+
+cudaError_t launch_pyramid_build(const float* ring, int channels, int width, int height, int frame_count,
+                                 int ring_slot, int levels, float* pyramid, int pyramid_slot, cudaStream_t s) {
+    const int64_t pixels = static_cast<int64_t>(width) * height;
+    float* dst0 = pyramid + static_cast<int64_t>(pyramid_slot) * pyramid_slot_pixels(width, height, 0);
+    const int64_t src_elems = static_cast<int64_t>(ring_slot) * pixels * channels;
+    pyramid_level0_kernel<<<static_cast<unsigned>((pixels + 255) / 256), 256, 0, s>>>(ring, dst0, pixels, channels,
+                                                                                      src_elems);
+    for (int l = 1; l < levels; ++l) {
+        int sw, sh, dw, dh;
+        pyramid_level_dims(width, height, l - 1, &sw, &sh);
+        pyramid_level_dims(width, height, l, &dw, &dh);
+        const float* src = pyramid + pyramid_level_base(width, height, frame_count, l - 1) +
+                           static_cast<int64_t>(pyramid_slot) * pyramid_slot_pixels(width, height, l - 1);
+        float* dst = pyramid + pyramid_level_base(width, height, frame_count, l) +
+                     static_cast<int64_t>(pyramid_slot) * pyramid_slot_pixels(width, height, l);
+        dim3 block(16, 16), grid((dw + 15) / 16, (dh + 15) / 16);
+        pyramid_down_kernel<<<grid, block, 0, s>>>(src, dst, sw, sh, dw, dh);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
+    const int step = m.blksize - m.overlap;
+    const int blocks_x = (m.width + step - 1) / step > 1 ? (m.width + step - 1) / step : 1;
+    const int blocks_y = (m.height + step - 1) / step > 1 ? (m.height + step - 1) / step : 1;
+    const bool seeded = m.levels > 1;
+    if (seeded) {
+        const int level = m.levels - 1;
+        const int scale = 1 << level;
+        SearchArgs a{};
+        pyramid_level_dims(m.width, m.height, level, &a.L.width, &a.L.height);
+        a.L.pyramid = m.pyramid;
+        a.L.level_base = pyramid_level_base(m.width, m.height, m.frame_count, level);
+        a.L.slot_pixels = pyramid_slot_pixels(m.width, m.height, level);
+        a.L.blksize = (m.blksize / scale > 2 ? m.blksize / scale : 2) * m.coarse_block_factor;
+        a.L.step = step / scale > 1 ? step / scale : 1;
+        a.L.blocks_x = (a.L.width + a.L.step - 1) / a.L.step > 1 ? (a.L.width + a.L.step - 1) / a.L.step : 1;
+        a.L.blocks_y = (a.L.height + a.L.step - 1) / a.L.step > 1 ? (a.L.height + a.L.step - 1) / a.L.step : 1;
+        a.neighbour_slots = m.neighbour_slots;
+        a.centre_slot = m.centre_slot;
+        a.mv_field = m.mv_field;
+        a.mv_stride = m.mv_stride;
+        a.level_scale = scale;
+        a.fine_blocks_x = blocks_x;
+        a.fine_blocks_y = blocks_y;
+        a.fine_step = step;
+        if (a.L.blksize > kMaxBlk) return cudaErrorInvalidValue;
+        dim3 grid(a.L.blocks_x, a.L.blocks_y, m.neighbours);
+        if (cudaError_t e = dispatch_search(m.coarse_radius, true, a, grid, s)) return e;
+    }
+    SearchArgs a{};
+    a.L.pyramid = m.pyramid;
+    a.L.width = m.width;
+    a.L.height = m.height;
+    a.L.level_base = 0;
+    a.L.slot_pixels = pyramid_slot_pixels(m.width, m.height, 0);
+    a.L.blksize = m.blksize;
+    a.L.step = step;
+    a.L.blocks_x = blocks_x;
+    a.L.blocks_y = blocks_y;
+    a.neighbour_slots = m.neighbour_slots;
+    a.centre_slot = m.centre_slot;
+    a.mv_field = m.mv_field;
+    a.mv_stride = m.mv_stride;
+    a.use_seed = seeded ? 1 : 0;
+    a.confidence = m.confidence;
+    a.conf_stride = m.conf_stride;
+    a.noise = m.noise;
+    a.sad_floor_word = m.sad_floor_word;
+    a.thsad = m.thsad;
+    if (a.L.blksize > kMaxBlk) return cudaErrorInvalidValue;
+    dim3 grid(blocks_x, blocks_y, m.neighbours);
+    return dispatch_search(m.search_radius, false, a, grid, s);
+}
+
+}  // namespace avd

@@ -1,0 +1,100 @@
+// Host side of the motion search entry points: argument checks, then the pyramid and block-match
+// launches of motion.cu.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+
+#include "avd_internal.h"
+#include "kernels.h"
+
+void avd_set_last_error(const std::string& m);
+
+namespace {
+AvdStatus fail(AvdStatus s, const std::string& m) {
+    avd_set_last_error(m);
+    return s;
+}
+}  // namespace
+
+extern "C" {
+
+uint64_t avd_motion_pyramid_floats(uint32_t width, uint32_t height, uint32_t frame_count, uint32_t levels) {
+    return static_cast<uint64_t>(avd::pyramid_floats(static_cast<int>(width), static_cast<int>(height),
+                                                     static_cast<int>(frame_count), static_cast<int>(levels)));
+}
+
+AvdStatus avd_motion_pyramid_build(uint64_t ring, uint32_t channels, uint32_t width, uint32_t height,
+                                   uint32_t frame_count, uint32_t ring_slot, uint32_t levels, uint64_t pyramid,
+                                   uint32_t pyramid_slot, void* stream) {
+    if (!ring || !pyramid) return fail(AVD_ERR_NULL_ARG, "motion pyramid: null buffer");
+    if (channels < 1 || channels > 2 || width == 0 || height == 0)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "motion pyramid: bad geometry");
+    if (levels < 1 || levels > 3) return fail(AVD_ERR_INVALID_OPTIONS, "motion pyramid: levels must be in 1..=3");
+    if (pyramid_slot >= frame_count) return fail(AVD_ERR_INVALID_OPTIONS, "motion pyramid: slot past frame_count");
+    cudaError_t e = avd::launch_pyramid_build(reinterpret_cast<const float*>(ring), static_cast<int>(channels),
+                                              static_cast<int>(width), static_cast<int>(height),
+                                              static_cast<int>(frame_count), static_cast<int>(ring_slot),
+                                              static_cast<int>(levels), reinterpret_cast<float*>(pyramid),
+                                              static_cast<int>(pyramid_slot), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("motion pyramid launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+AvdStatus avd_motion_search(const AvdMotionPass* p, void* stream) {
+    if (!p || !p->pyramid || !p->neighbour_slots || !p->mv_field)
+        return fail(AVD_ERR_NULL_ARG, "motion search: null buffer");
+    if (p->width == 0 || p->height == 0 || p->neighbours == 0 || p->centre_slot >= p->frame_count)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "motion search: bad geometry");
+    if (p->blksize < 2 || p->blksize > 32 || p->overlap >= p->blksize)
+        return fail(AVD_ERR_INVALID_OPTIONS, "motion search: blksize must be in 2..=32 and overlap below it");
+    if (p->search_radius > 8) return fail(AVD_ERR_INVALID_OPTIONS, "motion search: search_radius must be at most 8");
+    if (p->levels < 1 || p->levels > 3) return fail(AVD_ERR_INVALID_OPTIONS, "motion search: levels must be in 1..=3");
+    if (p->confidence && (!p->noise || !(p->thsad > 0.0f)))
+        return fail(AVD_ERR_INVALID_OPTIONS, "motion search: confidence needs the noise words and a positive thsad");
+    const uint32_t step = p->blksize - p->overlap;
+    const uint32_t bx = (p->width + step - 1) / step, by = (p->height + step - 1) / step;
+    if (p->mv_stride < 2 * bx * by || (p->confidence && p->conf_stride < bx * by))
+        return fail(AVD_ERR_INVALID_OPTIONS, "motion search: field strides below the block count");
+    avd::MotionLaunch m{};
+    m.pyramid = reinterpret_cast<const float*>(p->pyramid);
+    m.neighbour_slots = reinterpret_cast<const uint32_t*>(p->neighbour_slots);
+    m.mv_field = reinterpret_cast<int32_t*>(p->mv_field);
+    m.confidence = reinterpret_cast<float*>(p->confidence);
+    m.noise = reinterpret_cast<const float*>(p->noise);
+    m.width = static_cast<int>(p->width);
+    m.height = static_cast<int>(p->height);
+    m.frame_count = static_cast<int>(p->frame_count);
+    m.centre_slot = static_cast<int>(p->centre_slot);
+    m.neighbours = static_cast<int>(p->neighbours);
+    m.blksize = static_cast<int>(p->blksize);
+    m.overlap = static_cast<int>(p->overlap);
+    m.search_radius = static_cast<int>(p->search_radius);
+    m.coarse_radius = static_cast<int>(p->search_radius);
+    m.coarse_block_factor = 1;
+    m.levels = static_cast<int>(p->levels);
+    m.mv_stride = static_cast<int>(p->mv_stride);
+    m.conf_stride = static_cast<int>(p->conf_stride);
+    m.sad_floor_word = static_cast<int>(p->sad_floor_word);
+    m.thsad = p->thsad;
+    cudaError_t e = avd::launch_motion_search(m, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("motion search launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+// confidence.rs:17-21: area * 2 * sigma / sqrt(pi), evaluated left to right in f32, with sqrt(pi)
+// the f32 square root of the f32 pi.
+float avd_sad_noise_floor(uint32_t blksize, float sigma) {
+    const float area = static_cast<float>(blksize * blksize);
+    const volatile float pi = 3.14159265358979323846f;
+    return area * 2.0f * sigma / std::sqrt(static_cast<float>(pi));
+}
+
+// confidence.rs:27-30.
+float avd_thsad(uint32_t blksize, float thsad_scale) {
+    const float area = static_cast<float>(blksize * blksize);
+    return thsad_scale * area * 0.02f;
+}
+
+}  // extern "C"

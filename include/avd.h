@@ -379,6 +379,42 @@ AVD_API void avd_kaiser_window(float beta, float* out8);
 /* av-denoise-core/src/collab/kernels/aggregate.rs:33-54 (`cross_frame_accum_scale`). */
 AVD_API float avd_cross_frame_accum_scale(uint32_t spatial_radius, uint32_t temporal_radius);
 
+/* ---- motion search kernel-level entry points ---------------------------------------------- */
+
+/* The floats a luma pyramid of `levels` levels over `frame_count` slots holds
+ * (av-denoise-core/src/motion/pyramid.rs:16-20, `pyramid_pixels_per_frame` x frames). */
+AVD_API uint64_t avd_motion_pyramid_floats(uint32_t width, uint32_t height, uint32_t frame_count, uint32_t levels);
+
+/* av-denoise-core/src/motion/pyramid.rs:82-107 (`run_pyramid_build`): lane 0 of ring slot
+ * `ring_slot` (f32, `channels` interleaved) becomes level 0 of pyramid slot `pyramid_slot`, and each
+ * further level averages 2x2 pixels of the one below. Queued on `stream`. */
+AVD_API AvdStatus avd_motion_pyramid_build(uint64_t ring, uint32_t channels, uint32_t width, uint32_t height,
+                                           uint32_t frame_count, uint32_t ring_slot, uint32_t levels,
+                                           uint64_t pyramid, uint32_t pyramid_slot, void* stream);
+
+/* One block-matching motion search over a built pyramid, as `run_analyse` runs it without the
+ * camera-model candidate and the truemotion stage (av-denoise-core/src/motion/analyse.rs:170-258),
+ * and as `run_confidence` runs it with `search_radius` 0 and one level (motion/confidence.rs:39-66). */
+typedef struct AvdMotionPass {
+    uint64_t pyramid;         /* f32, avd_motion_pyramid_floats(width, height, frame_count, levels) */
+    uint64_t neighbour_slots; /* u32 pyramid slot of each neighbour */
+    uint64_t mv_field;        /* i32 (dx, dy) per block per neighbour, `mv_stride` apart; written */
+    uint64_t confidence;      /* f32 per block per neighbour, `conf_stride` apart; 0 = not written */
+    uint64_t noise;           /* f32 words; the SAD floor is word `sad_floor_word` */
+    uint32_t width, height, frame_count, centre_slot, neighbours;
+    uint32_t blksize, overlap, search_radius, levels;
+    uint32_t mv_stride, conf_stride, sad_floor_word;
+    float thsad; /* av-denoise-core/src/motion/confidence.rs:27-30; must be > 0 with confidence */
+} AvdMotionPass;
+
+AVD_API AvdStatus avd_motion_search(const AvdMotionPass* pass, void* stream);
+
+/* av-denoise-core/src/motion/confidence.rs:17-21 (`sad_noise_floor`). */
+AVD_API float avd_sad_noise_floor(uint32_t blksize, float sigma);
+
+/* av-denoise-core/src/motion/confidence.rs:27-30 (`thsad`). */
+AVD_API float avd_thsad(uint32_t blksize, float thsad_scale);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 
 /* No counterpart in the reference. One fast-variant NLMeans output frame for callers that cannot

@@ -1,0 +1,196 @@
+// CPU ORACLE - test infrastructure only (see nlm_oracle.cpp for the rules it follows).
+//
+// A C++17 restatement of av-denoise's block-matching motion search without the camera-model
+// candidate and the truemotion stage:
+//   pyramid: av-denoise-core/src/motion/kernels/pyramid.rs:10-61 (lane-0 extract, 2x2 average,
+//            odd edge repeated) and motion/pyramid.rs:82-107 (levels built one after another);
+//   coarse:  motion/kernels/block_match.rs:117-215 and motion/analyse.rs:100-150 (the smallest
+//            level, blksize max(b/2^l, 2), step max(s/2^l, 1), winner x 2^l seeds the fine blocks
+//            of its region, the last coarse block reaching the fine grid's edge);
+//   fine:    block_match.rs:274-351 and 490-521 (seeded window, confidence);
+//   window:  block_match.rs:656-849 (clamped staging, SAD summed row by row left to right, lowest
+//            SAD with the first row-major index, the window's centre winning a tie, SADs at or
+//            above 1e30 never chosen).
+// Every f32 operation is one rounded operation in the reference's order (the build turns off
+// contraction), so the vectors and confidences are expected to match the CUDA path bit for bit.
+//
+// The pyramid layout is the CUDA path's (level after level, `frame_count` slots per level, each
+// slot padded to a multiple of 8 floats), so one buffer describes both.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+namespace {
+
+int64_t slot_pixels(int w, int h, int level) {
+    for (int l = 0; l < level; ++l) {
+        w = w / 2 > 1 ? w / 2 : 1;
+        h = h / 2 > 1 ? h / 2 : 1;
+    }
+    return (static_cast<int64_t>(w) * h + 7) / 8 * 8;
+}
+
+void level_dims(int w, int h, int level, int* lw, int* lh) {
+    for (int l = 0; l < level; ++l) {
+        w = w / 2 > 1 ? w / 2 : 1;
+        h = h / 2 > 1 ? h / 2 : 1;
+    }
+    *lw = w;
+    *lh = h;
+}
+
+int64_t level_base(int w, int h, int frames, int level) {
+    int64_t b = 0;
+    for (int l = 0; l < level; ++l) b += static_cast<int64_t>(frames) * slot_pixels(w, h, l);
+    return b;
+}
+
+int clamp_to(int v, int limit) { return v < 0 ? 0 : (v >= limit ? limit - 1 : v); }
+
+struct Level {
+    const float* base;  // first value of the level
+    int64_t slot;
+    int width, height, blksize, step, blocks_x, blocks_y;
+};
+
+struct Best {
+    int dx, dy;
+    float sad;
+};
+
+// block_match.rs:674-760 for one centre.
+Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy, int cdx, int cdy, int R) {
+    const int b = L.blksize, side = 2 * R + 1;
+    const float* cf = L.base + centre_slot * L.slot;
+    const float* nf = L.base + nbr_slot * L.slot;
+    std::vector<float> centre(b * b), sads(side * side);
+    for (int py = 0; py < b; ++py)
+        for (int px = 0; px < b; ++px)
+            centre[py * b + px] =
+                cf[static_cast<int64_t>(clamp_to(oy + py, L.height)) * L.width + clamp_to(ox + px, L.width)];
+    for (int dy = 0; dy < side; ++dy)
+        for (int dx = 0; dx < side; ++dx) {
+            float sad = 0.0f;
+            for (int iy = 0; iy < b; ++iy)
+                for (int ix = 0; ix < b; ++ix) {
+                    const int sx = clamp_to(ox + cdx - R + dx + ix, L.width);
+                    const int sy = clamp_to(oy + cdy - R + dy + iy, L.height);
+                    const float diff = centre[iy * b + ix] - nf[static_cast<int64_t>(sy) * L.width + sx];
+                    sad += std::fabs(diff);
+                }
+            sads[dy * side + dx] = sad;
+        }
+    Best best{cdx, cdy, 1.0e30f};
+    for (int i = 0; i < side * side; ++i)
+        if (sads[i] < best.sad) {
+            best.sad = sads[i];
+            best.dx = cdx + i % side - R;
+            best.dy = cdy + i / side - R;
+        }
+    const float centre_sad = sads[R * side + R];
+    if (centre_sad <= best.sad) best = Best{cdx, cdy, centre_sad};
+    return best;
+}
+
+}  // namespace
+
+extern "C" {
+
+struct OrcMotionArgs {
+    const float* pyramid;
+    const uint32_t* neighbour_slots;
+    int32_t* mv_field;
+    float* confidence;  // null: not written
+    const float* noise;
+    uint32_t width, height, frame_count, centre_slot, neighbours;
+    uint32_t blksize, overlap, search_radius, levels;
+    uint32_t mv_stride, conf_stride, sad_floor_word;
+    float thsad;
+};
+
+int64_t orc_motion_pyramid_floats(int w, int h, int frames, int levels) { return level_base(w, h, frames, levels); }
+
+void orc_motion_pyramid_build(const float* ring, int channels, int w, int h, int frames, int ring_slot, int levels,
+                              float* pyramid, int pyramid_slot) {
+    const int64_t pixels = static_cast<int64_t>(w) * h;
+    float* l0 = pyramid + pyramid_slot * slot_pixels(w, h, 0);
+    for (int64_t p = 0; p < pixels; ++p) l0[p] = ring[(ring_slot * pixels + p) * channels];
+    for (int l = 1; l < levels; ++l) {
+        int sw, sh, dw, dh;
+        level_dims(w, h, l - 1, &sw, &sh);
+        level_dims(w, h, l, &dw, &dh);
+        const float* src = pyramid + level_base(w, h, frames, l - 1) + pyramid_slot * slot_pixels(w, h, l - 1);
+        float* dst = pyramid + level_base(w, h, frames, l) + pyramid_slot * slot_pixels(w, h, l);
+        for (int y = 0; y < dh; ++y)
+            for (int x = 0; x < dw; ++x) {
+                const int sx = 2 * x, sy = 2 * y;
+                const int sx1 = sx + 1 < sw ? sx + 1 : sx, sy1 = sy + 1 < sh ? sy + 1 : sy;
+                const float sum = src[sy * sw + sx] + src[sy * sw + sx1] + src[sy1 * sw + sx] + src[sy1 * sw + sx1];
+                dst[y * dw + x] = sum * 0.25f;
+            }
+    }
+}
+
+void orc_motion_search(const OrcMotionArgs* a) {
+    const int w = static_cast<int>(a->width), h = static_cast<int>(a->height), frames = static_cast<int>(a->frame_count);
+    const int step = static_cast<int>(a->blksize - a->overlap);
+    const int bx_n = (w + step - 1) / step > 1 ? (w + step - 1) / step : 1;
+    const int by_n = (h + step - 1) / step > 1 ? (h + step - 1) / step : 1;
+    const int R = static_cast<int>(a->search_radius);
+    const bool seeded = a->levels > 1;
+    if (seeded) {
+        const int level = static_cast<int>(a->levels) - 1, scale = 1 << level;
+        Level L{};
+        level_dims(w, h, level, &L.width, &L.height);
+        L.base = a->pyramid + level_base(w, h, frames, level);
+        L.slot = slot_pixels(w, h, level);
+        L.blksize = static_cast<int>(a->blksize) / scale > 2 ? static_cast<int>(a->blksize) / scale : 2;
+        L.step = step / scale > 1 ? step / scale : 1;
+        L.blocks_x = (L.width + L.step - 1) / L.step > 1 ? (L.width + L.step - 1) / L.step : 1;
+        L.blocks_y = (L.height + L.step - 1) / L.step > 1 ? (L.height + L.step - 1) / L.step : 1;
+        const int s = L.step * scale;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+        for (int n = 0; n < static_cast<int>(a->neighbours); ++n)
+            for (int by = 0; by < L.blocks_y; ++by)
+                for (int bx = 0; bx < L.blocks_x; ++bx) {
+                    const Best b = search_window(L, static_cast<int>(a->centre_slot),
+                                                 static_cast<int>(a->neighbour_slots[n]), bx * L.step, by * L.step, 0,
+                                                 0, R);
+                    const int c0 = std::min(bx * s / step, bx_n);
+                    const int c1 = bx == L.blocks_x - 1 ? bx_n : std::min((bx + 1) * s / step, bx_n);
+                    const int r0 = std::min(by * s / step, by_n);
+                    const int r1 = by == L.blocks_y - 1 ? by_n : std::min((by + 1) * s / step, by_n);
+                    int32_t* mv = a->mv_field + static_cast<int64_t>(n) * a->mv_stride;
+                    for (int r = r0; r < r1; ++r)
+                        for (int c = c0; c < c1; ++c) {
+                            mv[(r * bx_n + c) * 2] = b.dx * scale;
+                            mv[(r * bx_n + c) * 2 + 1] = b.dy * scale;
+                        }
+                }
+    }
+    Level L{a->pyramid, slot_pixels(w, h, 0), w, h, static_cast<int>(a->blksize), step, bx_n, by_n};
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int n = 0; n < static_cast<int>(a->neighbours); ++n)
+        for (int by = 0; by < by_n; ++by)
+            for (int bx = 0; bx < bx_n; ++bx) {
+                int32_t* mv = a->mv_field + static_cast<int64_t>(n) * a->mv_stride + (by * bx_n + bx) * 2;
+                const int sdx = seeded ? mv[0] : 0, sdy = seeded ? mv[1] : 0;
+                const Best b = search_window(L, static_cast<int>(a->centre_slot), static_cast<int>(a->neighbour_slots[n]),
+                                             bx * step, by * step, sdx, sdy, R);
+                mv[0] = b.dx;
+                mv[1] = b.dy;
+                if (a->confidence) {
+                    const float floor = a->noise[a->sad_floor_word];
+                    float excess = b.sad - floor;
+                    if (excess < 0.0f) excess = 0.0f;
+                    const float t2 = a->thsad * a->thsad, e2 = excess * excess;
+                    float c = (t2 - e2) / (t2 + e2);
+                    if (c < 0.0f) c = 0.0f;
+                    a->confidence[static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx] = c;
+                }
+            }
+}
+
+}  // extern "C"

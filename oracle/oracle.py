@@ -251,3 +251,65 @@ def collab_fused(ring: np.ndarray, width: int, height: int, channels: int, *, ce
     l.orc_collab_fused.argtypes = [C.POINTER(CollabArgs)]
     l.orc_collab_fused(C.byref(a))
     return accum, wsum, gw
+
+
+# ---- block-matching motion search (motion_oracle.cpp) -------------------------------------------
+
+class MotionArgs(C.Structure):
+    _fields_ = [
+        ("pyramid", _fp), ("neighbour_slots", C.POINTER(C.c_uint32)), ("mv_field", C.POINTER(C.c_int32)),
+        ("confidence", _fp), ("noise", _fp),
+    ] + [(n, C.c_uint32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize",
+                                   "overlap", "search_radius", "levels", "mv_stride", "conf_stride",
+                                   "sad_floor_word")] + [("thsad", C.c_float)]
+
+
+def motion_pyramid(ring: np.ndarray, channels: int, width: int, height: int, levels: int) -> np.ndarray:
+    """Every ring slot's luma pyramid, in the CUDA path's layout."""
+    ring = np.ascontiguousarray(ring, np.float32)
+    frames = ring.size // (width * height * channels)
+    l = lib()
+    l.orc_motion_pyramid_floats.argtypes = [C.c_int] * 4
+    l.orc_motion_pyramid_floats.restype = C.c_int64
+    pyr = np.zeros(l.orc_motion_pyramid_floats(width, height, frames, levels), np.float32)
+    l.orc_motion_pyramid_build.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _fp, C.c_int]
+    for slot in range(frames):
+        l.orc_motion_pyramid_build(_f(ring), channels, width, height, frames, slot, levels, _f(pyr), slot)
+    return pyr
+
+
+def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
+                  *, blksize=16, overlap=8, search_radius=4, levels=2, confidence=False, sad_floor=0.0,
+                  thsad=0.0):
+    """One block-matching search (no camera model, no truemotion). Returns (mv (n, blocks, 2), conf)."""
+    step = blksize - overlap
+    bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
+    slots = np.ascontiguousarray(neighbour_slots, np.uint32)
+    n = slots.size
+    mv = np.zeros(n * bx * by * 2, np.int32)
+    conf = np.zeros(n * bx * by, np.float32)
+    noise = np.array([sad_floor], np.float32)
+    a = MotionArgs()
+    a.pyramid, a.neighbour_slots = _f(pyramid), slots.ctypes.data_as(C.POINTER(C.c_uint32))
+    a.mv_field = mv.ctypes.data_as(C.POINTER(C.c_int32))
+    a.confidence = _f(conf) if confidence else None
+    a.noise = _f(noise)
+    a.width, a.height, a.frame_count, a.centre_slot, a.neighbours = width, height, frames, centre_slot, n
+    a.blksize, a.overlap, a.search_radius, a.levels = blksize, overlap, search_radius, levels
+    a.mv_stride, a.conf_stride, a.sad_floor_word, a.thsad = bx * by * 2, bx * by, 0, thsad
+    l = lib()
+    l.orc_motion_search.argtypes = [C.POINTER(MotionArgs)]
+    l.orc_motion_search(C.byref(a))
+    return mv.reshape(n, bx * by, 2), conf.reshape(n, bx * by)
+
+
+def sad_noise_floor(blksize: int, sigma: float) -> float:
+    """motion/confidence.rs:17-21 in f32, left to right."""
+    f = np.float32
+    return float(f(f(f(blksize * blksize) * f(2.0)) * f(sigma)) / np.sqrt(f(np.pi)))
+
+
+def thsad(blksize: int, thsad_scale: float) -> float:
+    """motion/confidence.rs:27-30 in f32."""
+    f = np.float32
+    return float(f(f(thsad_scale) * f(blksize * blksize)) * f(0.02))

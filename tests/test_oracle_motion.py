@@ -1,0 +1,82 @@
+"""The CPU oracle's block-matching motion search on the reference's own block-match cases
+(av-denoise-core/src/motion/tests/block_match.rs:97-330) and the confidence formulas
+(motion/confidence.rs:75-100); the ABI's host formulas agree with the oracle's."""
+
+import numpy as np
+import pytest
+
+from motion_cases import shifted, textured
+
+
+def pair_ring(centre: np.ndarray, neighbour: np.ndarray) -> np.ndarray:
+    return np.stack([centre, neighbour]).astype(np.float32).reshape(-1)
+
+
+def test_clean_shift_is_found_exactly(oracle):
+    # block_match.rs:123-211: a (+2, +1) shift of rich content, 64x64, blksize 16 at step 16,
+    # radius 4, one level: the middle block's vector is exactly (2, 1).
+    c = textured(64, 64, 123)
+    n = shifted(c, 2, 1)
+    pyr = oracle.motion_pyramid(pair_ring(c, n), 1, 64, 64, 1)
+    mv, _ = oracle.motion_search(pyr, 64, 64, 2, 0, [1], blksize=16, overlap=0, search_radius=4, levels=1)
+    assert tuple(mv[0, 1 * 4 + 1]) == (2, 1)
+
+
+def test_uniform_mismatch_sad_from_confidence(oracle):
+    # block_match.rs:96-120: |delta| = 0.1 over a 16x16 block gives a SAD of 25.6, recovered from
+    # the confidence within 1%.
+    c = np.full((16, 16), 0.25, np.float32)
+    n = np.full((16, 16), 0.35, np.float32)
+    pyr = oracle.motion_pyramid(pair_ring(c, n), 1, 16, 16, 1)
+    expected = 256 * 0.1
+    th = 3.0 * expected
+    _, conf = oracle.motion_search(pyr, 16, 16, 2, 0, [1], blksize=16, overlap=0, search_radius=0, levels=1,
+                                   confidence=True, sad_floor=0.0, thsad=th)
+    c0 = float(conf[0, 0])
+    sad = th * np.sqrt((1.0 - c0) / (1.0 + c0))
+    assert abs(sad - expected) < expected * 0.01
+
+
+@pytest.mark.parametrize("levels", [1, 2])
+def test_flat_region_tie_resolves_to_zero_motion(oracle, levels):
+    # block_match.rs:275-330: every candidate ties on a flat block; the window's centre wins.
+    flat = np.full((32, 32), 0.5, np.float32)
+    pyr = oracle.motion_pyramid(pair_ring(flat, flat), 1, 32, 32, levels)
+    mv, conf = oracle.motion_search(pyr, 32, 32, 2, 0, [1], levels=levels, confidence=True, thsad=5.12)
+    assert not mv.any()
+    assert np.all(conf == 1.0)
+
+
+def test_global_shift_recovered_through_the_coarse_level(oracle):
+    # A shift beyond the fine radius (6 > 4) is reached through the coarse seed (x2 at level 1).
+    c = textured(96, 80, 7)
+    n = shifted(c, 6, -5)
+    pyr = oracle.motion_pyramid(pair_ring(c, n), 1, 96, 80, 2)
+    mv, _ = oracle.motion_search(pyr, 96, 80, 2, 0, [1], levels=2)
+    inner = mv[0].reshape(10, 12, 2)[2:-2, 2:-2]
+    assert np.mean(np.all(inner == (6, -5), axis=-1)) > 0.9
+
+
+def test_confidence_formulas_match_the_reference_tests(oracle, lib):
+    # confidence.rs:75-100.
+    sigma = 4.0 / 255.0
+    want = 256 * 2.0 * sigma / np.sqrt(np.pi)
+    assert abs(oracle.sad_noise_floor(16, sigma) - want) < 1e-6
+    assert oracle.sad_noise_floor(16, 0.0) == 0.0
+    assert abs(oracle.thsad(16, 2.0) - 2.0 * 256 * 0.02) < 1e-6
+    assert oracle.thsad(16, 1.0) > 0.0
+    for b, s in [(16, sigma), (8, 0.02), (32, 0.1), (16, 0.0)]:
+        assert np.float32(lib.avd_sad_noise_floor(b, s)) == np.float32(oracle.sad_noise_floor(b, s))
+    for b, t in [(16, 1.0), (8, 0.5), (32, 2.0)]:
+        assert np.float32(lib.avd_thsad(b, t)) == np.float32(oracle.thsad(b, t))
+
+
+def test_pyramid_layout_and_downscale(oracle, lib):
+    # pyramid.rs:10-37: odd sizes repeat the edge; slots are padded to 8 floats.
+    w, h = 13, 7
+    frame = np.arange(w * h, dtype=np.float32).reshape(h, w) / 100.0
+    pyr = oracle.motion_pyramid(frame.reshape(-1), 1, w, h, 2)
+    assert pyr.size == lib.avd_motion_pyramid_floats(w, h, 1, 2) == 96 + 24
+    l1 = pyr[96:96 + 18].reshape(3, 6)
+    f = frame
+    assert l1[0, 0] == np.float32((((f[0, 0] + f[0, 1]) + f[1, 0]) + f[1, 1]) * np.float32(0.25))
