@@ -149,10 +149,9 @@ class NlmPass final : public Pass {
             return Failure{AVD_ERR_INVALID_OPTIONS, "prefilters are not available in this build"};
         if (p.motion.active && p.temporal_radius > 0)
             return Failure{AVD_ERR_INVALID_OPTIONS, "NLMeans motion compensation is not available in this build"};
-        if (p.hq && p.hq_params.temporal_confidence && p.temporal_radius > 0)
-            return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "NLMeans-HQ temporal confidence is not available in this build yet; set "
-                           "hq.temporal_confidence = false"};
+        // nlmeans/denoiser/mod.rs:340-370: confidence without motion compensation scores every
+        // neighbour block where it stands (blksize 16, step 8, radius 0, one level).
+        pass->conf_pass_ = p.hq && p.hq_params.temporal_confidence && p.temporal_radius > 0;
         if (auto f = pass->allocate()) return f;
         *result = std::move(pass);
         return std::nullopt;
@@ -241,6 +240,13 @@ class NlmPass final : public Pass {
    private:
     NlmPass() = default;
 
+    static constexpr int kConfBlk = 16;
+    static constexpr int kConfStep = 8;
+    bool conf_pass_ = false;
+    uint32_t conf_bx_ = 0, conf_by_ = 0;
+    float thsad_ = 0.0f;
+    DeviceBuffer pyramid_, mv_scratch_, conf_;
+
     size_t pixels() const { return static_cast<size_t>(width_) * height_; }
     size_t frame_elems() const { return pixels() * params_.channel_count(); }
     uint32_t total_frames() const { return params_.total_frames(); }
@@ -260,6 +266,22 @@ class NlmPass final : public Pass {
         words[0] = h2_inv_norm_with(params_, has_sigma, sigma);
         float sig[2] = {sigma, sigma};
         words[1] = has_sigma ? noise_offset_with(params_, sig, 2) : 0.0f;
+        if (conf_pass_) {
+            // motion/confidence.rs:17-30; nlmeans/denoiser/noise.rs:365-368: the confidence floor
+            // uses the pinned sigma unscaled by any prefilter.
+            conf_bx_ = std::max<uint32_t>((width_ + kConfStep - 1) / kConfStep, 1);
+            conf_by_ = std::max<uint32_t>((height_ + kConfStep - 1) / kConfStep, 1);
+            const size_t blocks = static_cast<size_t>(conf_bx_) * conf_by_;
+            const size_t nbrs = 2 * params_.temporal_radius;
+            const size_t pyr = static_cast<size_t>(pyramid_floats(static_cast<int>(width_), static_cast<int>(height_),
+                                                                  static_cast<int>(total_frames()), 1));
+            if ((e = pyramid_.alloc(pyr * sizeof(float))) != cudaSuccess) return gpu_failure("confidence pyramid", e);
+            if ((e = mv_scratch_.alloc(nbrs * blocks * 2 * sizeof(int32_t))) != cudaSuccess)
+                return gpu_failure("confidence vectors", e);
+            if ((e = conf_.alloc(nbrs * blocks * sizeof(float))) != cudaSuccess) return gpu_failure("confidence", e);
+            words[2] = avd_sad_noise_floor(kConfBlk, has_sigma ? sigma : 0.0f);
+            thsad_ = avd_thsad(kConfBlk, params_.hq_params.thsad_scale);
+        }
         if ((e = cudaMemcpy(derived_.ptr, words, sizeof(words), cudaMemcpyHostToDevice)) != cudaSuccess)
             return gpu_failure("derived upload", e);
         if (params_.hq) {
@@ -317,6 +339,7 @@ class NlmPass final : public Pass {
         cudaError_t e = launch_ingest(p0, p1, slot_ptr(slot), static_cast<int64_t>(pixels()),
                                       static_cast<int>(params_.channel_count()), plane_format(in_), bias(), stream);
         if (e != cudaSuccess) return gpu_failure("ingest launch", e);
+        if (auto f = slot_written(slot)) return f;
         slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
         advance_ring();
         return prime_leading_edge_if_first();
@@ -348,8 +371,53 @@ class NlmPass final : public Pass {
         cudaError_t e = cudaMemcpyAsync(slot_ptr(next), slot_ptr(last), frame_elems() * sizeof(float),
                                         cudaMemcpyDeviceToDevice, stream);
         if (e != cudaSuccess) return gpu_failure("slot copy", e);
+        if (auto f = slot_written(next)) return f;
         slot_frames_[next] = slot_frames_[last];
         ring_head_ += 1;
+        return std::nullopt;
+    }
+
+    // nlmeans/denoiser/stages.rs:110-130: the confidence pyramid follows every ring slot write.
+    std::optional<Failure> slot_written(size_t slot) {
+        if (!conf_pass_) return std::nullopt;
+        cudaError_t e = launch_pyramid_build(ring_.as<float>(), static_cast<int>(params_.channel_count()),
+                                             static_cast<int>(width_), static_cast<int>(height_),
+                                             static_cast<int>(total_frames()), static_cast<int>(slot), 1,
+                                             pyramid_.as<float>(), static_cast<int>(slot), stream);
+        if (e != cudaSuccess) return gpu_failure("confidence pyramid launch", e);
+        return std::nullopt;
+    }
+
+    // nlmeans/dispatch/motion.rs:554-613 (`run_confidence_pass`): every neighbour in logical order,
+    // the centre skipped, scored where each block stands.
+    std::optional<Failure> run_confidence_pass() {
+        const int d = static_cast<int>(params_.temporal_radius);
+        MotionLaunch m{};
+        m.pyramid = pyramid_.as<float>();
+        m.neighbour_slots = nullptr;
+        int n = 0;
+        for (int l = 0; l <= 2 * d; ++l)
+            if (l != d) m.inline_slots[n++] = static_cast<uint32_t>(phys_frame(l));
+        m.mv_field = mv_scratch_.as<int32_t>();
+        m.confidence = conf_.as<float>();
+        m.noise = derived_.as<float>();
+        m.width = static_cast<int>(width_);
+        m.height = static_cast<int>(height_);
+        m.frame_count = static_cast<int>(total_frames());
+        m.centre_slot = phys_frame(d);
+        m.neighbours = n;
+        m.blksize = kConfBlk;
+        m.overlap = kConfBlk - kConfStep;
+        m.search_radius = 0;
+        m.coarse_radius = 0;
+        m.coarse_block_factor = 1;
+        m.levels = 1;
+        m.mv_stride = static_cast<int>(conf_bx_ * conf_by_ * 2);
+        m.conf_stride = static_cast<int>(conf_bx_ * conf_by_);
+        m.sad_floor_word = 2;
+        m.thsad = thsad_;
+        cudaError_t e = launch_motion_search(m, stream);
+        if (e != cudaSuccess) return gpu_failure("confidence launch", e);
         return std::nullopt;
     }
 
@@ -392,6 +460,20 @@ class NlmPass final : public Pass {
         a.offset_word = 1;
         a.spatial_lut = params_.hq ? lut_.as<float>() : nullptr;
         a.conf = nullptr;
+        if (conf_pass_) {
+            if (auto f = run_confidence_pass()) return f;
+            // dispatch/mod.rs:175-200: pair k (q_k = -d + k) weighs its forward frame by neighbour
+            // q_k + d and its backward frame by neighbour d - 1 - q_k.
+            const int stride = static_cast<int>(conf_bx_ * conf_by_);
+            a.conf = conf_.as<float>();
+            for (int k = 0; k < d; ++k) {
+                a.conf_fwd_off[k] = k * stride;
+                a.conf_bwd_off[k] = (2 * d - 1 - k) * stride;
+            }
+            a.conf_step = kConfStep;
+            a.blocks_x = static_cast<int>(conf_bx_);
+            a.blocks_y = static_cast<int>(conf_by_);
+        }
         a.wref = params_.self_weight;
         a.fast = params_.hq ? 0 : 1;
         a.out = outputs_[slot].as<float>();

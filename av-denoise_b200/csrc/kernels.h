@@ -77,8 +77,10 @@ cudaError_t launch_collab(const CollabLaunch& args, cudaStream_t stream);
 
 // Block-matching motion search (motion.cu). The pyramid must already hold every slot it reads.
 struct MotionLaunch {
+    static constexpr int kMaxInlineSlots = 16;
     const float* pyramid;
-    const uint32_t* neighbour_slots;
+    const uint32_t* neighbour_slots;  // device table, or null to read `inline_slots`
+    uint32_t inline_slots[kMaxInlineSlots];
     int32_t* mv_field;
     float* confidence;  // may be null: no confidence is written
     const float* noise;

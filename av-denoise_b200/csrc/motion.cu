@@ -36,6 +36,7 @@ namespace {
 constexpr int kMaxBlk = 32;
 constexpr int kMaxRadius = 8;
 constexpr float kNoSad = 1.0e30f;
+constexpr int kMaxNeighbours = MotionLaunch::kMaxInlineSlots;
 
 __device__ __forceinline__ int clamp_to(int v, int limit) { return v < 0 ? 0 : (v >= limit ? limit - 1 : v); }
 
@@ -129,7 +130,8 @@ __device__ __forceinline__ void score_window(const SearchLevel& L, int64_t centr
 
 struct SearchArgs {
     SearchLevel L;
-    const uint32_t* neighbour_slots;
+    const uint32_t* neighbour_slots;  // null: the slots are `slots`
+    uint32_t slots[kMaxNeighbours];
     int centre_slot;
     int32_t* mv_field;
     int mv_stride;
@@ -155,7 +157,8 @@ __device__ __forceinline__ void search_one(const SearchArgs& a, int bx, int by, 
     __shared__ unsigned long long warp_keys[(kSide * kSide + 31) / 32];
     __shared__ int best_index;
     const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
-    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(a.neighbour_slots[n]) * a.L.slot_pixels;
+    const uint32_t nbr_slot = a.neighbour_slots ? a.neighbour_slots[n] : a.slots[n];
+    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(nbr_slot) * a.L.slot_pixels;
     const int ox = bx * a.L.step, oy = by * a.L.step;
     score_window<R>(a.L, centre_base, nbr_base, ox, oy, cdx, cdy, centre_tile, window, sads);
     window_argmin<R>(sads, warp_keys, &best_index);
@@ -304,6 +307,7 @@ cudaError_t launch_pyramid_build(const float* ring, int channels, int width, int
 }
 
 cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
+    if (!m.neighbour_slots && m.neighbours > kMaxNeighbours) return cudaErrorInvalidValue;
     const int step = m.blksize - m.overlap;
     const int blocks_x = (m.width + step - 1) / step > 1 ? (m.width + step - 1) / step : 1;
     const int blocks_y = (m.height + step - 1) / step > 1 ? (m.height + step - 1) / step : 1;
@@ -321,6 +325,7 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
         a.L.blocks_x = (a.L.width + a.L.step - 1) / a.L.step > 1 ? (a.L.width + a.L.step - 1) / a.L.step : 1;
         a.L.blocks_y = (a.L.height + a.L.step - 1) / a.L.step > 1 ? (a.L.height + a.L.step - 1) / a.L.step : 1;
         a.neighbour_slots = m.neighbour_slots;
+        for (int i = 0; i < kMaxNeighbours; ++i) a.slots[i] = m.inline_slots[i];
         a.centre_slot = m.centre_slot;
         a.mv_field = m.mv_field;
         a.mv_stride = m.mv_stride;
@@ -343,6 +348,7 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     a.L.blocks_x = blocks_x;
     a.L.blocks_y = blocks_y;
     a.neighbour_slots = m.neighbour_slots;
+    for (int i = 0; i < kMaxNeighbours; ++i) a.slots[i] = m.inline_slots[i];
     a.centre_slot = m.centre_slot;
     a.mv_field = m.mv_field;
     a.mv_stride = m.mv_stride;

@@ -143,14 +143,35 @@ def nlm_frame(window: list[np.ndarray], d: int, a: int, s: int, h2: float, noise
 
 
 def nlm_stream_repeat(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, wref: float = 1.0,
-                      noise_offset: float = 0.0, fp64: bool = False, lut: np.ndarray | None = None) -> list[np.ndarray]:
-    """The fast NLMeans engine over a whole stream with repeat edges: one output per input."""
+                      noise_offset: float = 0.0, fp64: bool = False, lut: np.ndarray | None = None,
+                      conf_sigma: float | None = None, thsad_scale: float = 1.0) -> list[np.ndarray]:
+    """The NLMeans engine over a whole stream with repeat edges: one output per input. With
+    `conf_sigma`, every temporal weight is scaled by the HQ confidence pass at that pinned sigma."""
     n = len(frames)
     outs = []
     for i in range(n):
         window = [frames[min(max(i + k, 0), n - 1)] for k in range(-d, d + 1)]
-        outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, lut=lut, wref=wref, fp64=fp64))
+        conf, blocks = None, (1, 1)
+        if conf_sigma is not None and d > 0:
+            conf, blocks = hq_confidence(window, d, conf_sigma, thsad_scale)
+        outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, lut=lut, conf=conf, conf_step=8,
+                              blocks=blocks, wref=wref, fp64=fp64))
     return outs
+
+
+def hq_confidence(window: list[np.ndarray], d: int, sigma: float, thsad_scale: float = 1.0):
+    """The HQ confidence pass over one window (nlmeans/dispatch/motion.rs:554-613): lane 0 of every
+    frame, 16x16 blocks at step 8 scored where they stand against the centre, floor
+    sad_noise_floor(16, sigma), thsad(16, thsad_scale). Returns the (forward, backward) block
+    confidences of each pair k (q_k = -d + k) and the block grid."""
+    h, w, c = window[0].shape
+    ring = np.stack([np.ascontiguousarray(f, np.float32) for f in window]).reshape(-1)
+    pyr = motion_pyramid(ring, c, w, h, 1)
+    slots = [l for l in range(2 * d + 1) if l != d]
+    _, conf = motion_search(pyr, w, h, 2 * d + 1, d, slots, blksize=16, overlap=8, search_radius=0, levels=1,
+                            confidence=True, sad_floor=sad_noise_floor(16, sigma), thsad=thsad(16, thsad_scale))
+    blocks = (max(-(-w // 8), 1), max(-(-h // 8), 1))
+    return [(conf[k], conf[2 * d - 1 - k]) for k in range(d)], blocks
 
 
 # ---- NL4D collaborative filter (collab_oracle.cpp) ------------------------------------------------

@@ -31,10 +31,10 @@ def fmt_for(depth):
 
 
 def check_group(oracle, got_planes, frames, fmt, d, a, s, strength, chroma=False, min_raw=0.99, wref=1.0,
-                hq_sigma=None):
+                hq_sigma=None, hq_confidence=False, thsad_scale=1.0):
     """Compares one plane group of every emitted frame with the oracle; returns the stats."""
     want, exact = oracle_pass(oracle, frames, fmt, d, a, s, strength, wref=wref, chroma=chroma, exact=True,
-                              hq_sigma=hq_sigma)
+                              hq_sigma=hq_sigma, hq_confidence=hq_confidence, thsad_scale=thsad_scale)
     par = Parity()
     for g, wn, ex in zip(got_planes, want, exact):
         for c in range(len(wn)):
@@ -256,10 +256,10 @@ def test_full_1080p_crops_match_oracle(oracle):
     print(par.check())
 
 
-def hq(d, a, s, sigma, strength=None, confidence=False):
+def hq(d, a, s, sigma, strength=None, confidence=False, thsad_scale=1.0):
     mode = avd.DenoisingMode.temporal(d) if d else avd.DenoisingMode.spacial()
     tuning = avd.NlmTuning(search_radius=a, patch_radius=s, strength=strength)
-    params = avd.HqParams(sigma_override=sigma, temporal_confidence=confidence)
+    params = avd.HqParams(sigma_override=sigma, temporal_confidence=confidence, thsad_scale=thsad_scale)
     return avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(nlm=avd.NlmeansOptions(tuning=tuning, mode=mode), hq=params))
 
 
@@ -289,3 +289,33 @@ def test_hq_pinned_sigma_chroma_10bit(oracle):
     got = Runner(spec).run(frames)
     check_group(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, 0, 4, 2, 0.9, chroma=True,
                 hq_sigma=sigma, min_raw=0.95)
+
+
+@pytest.mark.parametrize("d,a,s,sigma,thsad_scale", [(1, 4, 2, 10.0 / 255, 1.0), (2, 3, 2, 6.0 / 255, 0.5),
+                                                     (3, 2, 1, 14.0 / 255, 2.0)])
+def test_hq_temporal_confidence_luma(oracle, d, a, s, sigma, thsad_scale):
+    """NLMeans-HQ with temporal confidence: each neighbour's 16x16 blocks (step 8) are scored where
+    they stand and every temporal weight is scaled by its block's confidence
+    (nlmeans/dispatch/motion.rs:554-613, kernels/fused.rs:317-324)."""
+    w, h = 136, 80
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 5, seed=60 + d)
+    spec = avd.EngineSpec.nlmeans(hq(d, a, s, sigma, confidence=True, thsad_scale=thsad_scale), None,
+                                  avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    strength = avd.hq_default_strength(1, d)
+    check_group(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, a, s, strength, hq_sigma=sigma,
+                hq_confidence=True, thsad_scale=thsad_scale, min_raw=0.95)
+
+
+def test_hq_temporal_confidence_chroma(oracle):
+    """Chroma scores lane 0 (U) of the interleaved ring (stages.rs:110-130)."""
+    w, h = 112, 64
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 4, chroma="420", seed=71)
+    sigma = 8.0 / 255
+    spec = avd.EngineSpec.nlmeans(None, hq(1, 3, 2, sigma, strength=0.8, confidence=True),
+                                  avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    check_group(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, 1, 3, 2, 0.8, chroma=True,
+                hq_sigma=sigma, hq_confidence=True, min_raw=0.95)
