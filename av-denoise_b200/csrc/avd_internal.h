@@ -75,6 +75,10 @@ float noise_offset_with(const NlmParams& p, const float* sigmas, int n);
 size_t nlm_held_frames(const AvdNlmeansAlgorithm& algorithm, Channels channels);
 size_t nl4d_held_frames(const AvdNl4dOptions& options, Channels channels);
 
+// nl4d/options.rs:101-132: the plane's resolved hard-threshold multiplier and pooled ratio.
+float nl4d_lambda_ht(const AvdNl4dOptions& options, Channels channels);
+float nl4d_pool_ratio(Channels channels);
+
 // Sample-format helpers (engine/plane.rs:229-263).
 float sample_max_value(const AvdSampleFormat& f);
 uint32_t samples_per_word(const AvdSampleFormat& f);

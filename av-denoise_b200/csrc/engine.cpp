@@ -18,113 +18,12 @@
 #include <vector>
 
 #include "avd_internal.h"
+#include "engine_parts.h"
 #include "kernels.h"
 
 namespace avd {
 
 namespace {
-
-// Error carried out of a call: a status plus its message.
-struct Failure {
-    AvdStatus status;
-    std::string message;
-};
-
-struct DeviceBuffer {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    DeviceBuffer() = default;
-    DeviceBuffer(const DeviceBuffer&) = delete;
-    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    ~DeviceBuffer() {
-        if (ptr) cudaFree(ptr);
-    }
-    cudaError_t alloc(size_t n) {
-        bytes = n;
-        return cudaMalloc(&ptr, n ? n : 4);
-    }
-    template <typename T>
-    T* as() const {
-        return static_cast<T*>(ptr);
-    }
-};
-
-std::string cuda_message(const char* what, cudaError_t e) {
-    return std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
-}
-
-PlaneFormat plane_format(const AvdSampleFormat& f) {
-    PlaneFormat p;
-    p.kind = static_cast<int>(f.kind);
-    p.samples_per_word = static_cast<int>(samples_per_word(f));
-    p.max_value = sample_max_value(f);
-    return p;
-}
-
-// Timing of one pass: CUDA events around sampled frames (engine/timing.rs:22-70).
-struct DeviceTimer {
-    uint32_t every = 0;
-    uint64_t frame_counter = 0;
-    double total = 0.0;
-    uint64_t frames = 0;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
-
-    ~DeviceTimer() {
-        for (auto& p : pending) {
-            cudaEventDestroy(p.first);
-            cudaEventDestroy(p.second);
-        }
-    }
-    bool begin(cudaStream_t s, cudaEvent_t* start) {
-        uint64_t n = frame_counter++;
-        if (every == 0 || n % every != 0) return false;
-        cudaEventCreate(start);
-        cudaEventRecord(*start, s);
-        return true;
-    }
-    void end(cudaStream_t s, cudaEvent_t start) {
-        cudaEvent_t stop;
-        cudaEventCreate(&stop);
-        cudaEventRecord(stop, s);
-        pending.emplace_back(start, stop);
-    }
-    AvdEngineTiming collect() {
-        for (auto& p : pending) {
-            float ms = 0.0f;
-            if (cudaEventSynchronize(p.second) == cudaSuccess && cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) {
-                total += ms * 1e-3;
-                frames += 1;
-            }
-            cudaEventDestroy(p.first);
-            cudaEventDestroy(p.second);
-        }
-        pending.clear();
-        AvdEngineTiming t;
-        t.device_time = total;
-        t.frames = frames;
-        return t;
-    }
-};
-
-// ---------------------------------------------------------------------------------------------
-// A pass over one plane group.
-class Pass {
-   public:
-    virtual ~Pass() = default;
-    virtual std::optional<Failure> push(const AvdPlane* planes, size_t* ready) = 0;
-    virtual std::optional<Failure> push_context(const AvdPlane* planes) = 0;
-    virtual std::optional<Failure> emit_into(const AvdPlane* planes) = 0;
-    virtual std::optional<Failure> finish(size_t* tail) = 0;
-    virtual void reset() = 0;
-    virtual size_t max_held_frames() const = 0;
-    virtual AvdWindowSpan window_span() const = 0;
-    virtual uint32_t next_frame() const = 0;
-    virtual std::optional<uint32_t> emitted_frame() const = 0;
-    virtual AvdEngineTiming timing() = 0;
-    virtual void sample_device_time(uint32_t every) = 0;
-    virtual std::optional<Failure> fail_for_test() = 0;
-    cudaStream_t stream = nullptr;
-};
 
 // ---------------------------------------------------------------------------------------------
 // NLMeans pass: nlmeans/engine.rs:29-318 over the ring of nlmeans/denoiser/mod.rs:40-591.
@@ -695,25 +594,28 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
     std::string message;
     AvdStatus st = avd::validate_spec(*spec, &message);
     if (st != AVD_OK) return fail_global(st, message);
-    if (spec->kind == AVD_ENGINE_NL4D)
-        return fail_global(AVD_ERR_INVALID_OPTIONS, "the NL4D engine is not available in this build yet");
 
     auto engine = std::make_unique<AvdEngine>();
     engine->geometry = spec->geometry;
     cudaError_t dev_err = cudaGetDevice(&engine->device);
     if (dev_err != cudaSuccess) return fail_global(AVD_ERR_GPU, avd::cuda_message("cudaGetDevice", dev_err));
     const AvdGeometry& g = spec->geometry;
+    const bool nl4d = spec->kind == AVD_ENGINE_NL4D;
     if (spec->has_luma) {
-        if (auto f = avd::NlmPass::create(spec->nlm_luma, avd::Channels::Luma, g.width, g.height, g.input, g.output,
-                                          &engine->luma))
-            return fail_global(f->status, f->message);
+        auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_luma, avd::Channels::Luma, g.width, g.height, g.input,
+                                              g.output, &engine->luma)
+                      : avd::NlmPass::create(spec->nlm_luma, avd::Channels::Luma, g.width, g.height, g.input,
+                                             g.output, &engine->luma);
+        if (f) return fail_global(f->status, f->message);
     }
     if (spec->has_chroma) {
         uint32_t cw, ch;
         avd::plane_dims(g, 1, &cw, &ch);
-        if (auto f = avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
-                                          &engine->chroma))
-            return fail_global(f->status, f->message);
+        auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
+                                              &engine->chroma)
+                      : avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
+                                             &engine->chroma);
+        if (f) return fail_global(f->status, f->message);
     }
     const bool gray = g.chroma == AVD_CHROMA_GRAY;
     const bool cleans_luma = engine->luma != nullptr;

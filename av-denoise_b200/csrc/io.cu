@@ -142,4 +142,31 @@ cudaError_t launch_egress(const float* frame, void* plane0, void* plane1, int64_
     return cudaGetLastError();
 }
 
+namespace {
+template <int C>
+__global__ void collab_normalise_kernel(int32_t* __restrict__ accum, int32_t* __restrict__ wsum,
+                                        float* __restrict__ out, int64_t pixels) {
+    const int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    const int32_t w = wsum[p];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const float acc = __int2float_rn(accum[p * C + c]);
+        out[p * C + c] = w != 0 ? __fdiv_rn(__fmul_rn(acc, 5.0f), __int2float_rn(w)) : acc;
+        accum[p * C + c] = 0;
+    }
+    wsum[p] = 0;
+}
+}  // namespace
+
+cudaError_t launch_collab_normalise(int32_t* accum, int32_t* wsum, float* out, int64_t pixels, int channels,
+                                    cudaStream_t stream) {
+    const unsigned blocks = static_cast<unsigned>((pixels + 255) / 256);
+    if (channels == 1)
+        collab_normalise_kernel<1><<<blocks, 256, 0, stream>>>(accum, wsum, out, pixels);
+    else
+        collab_normalise_kernel<2><<<blocks, 256, 0, stream>>>(accum, wsum, out, pixels);
+    return cudaGetLastError();
+}
+
 }  // namespace avd

@@ -75,6 +75,11 @@ struct CollabLaunch {
 
 cudaError_t launch_collab(const CollabLaunch& args, cudaStream_t stream);
 
+// collab/kernels/aggregate.rs:240-290 (`collab_normalise`): one region's accum * 5 / wsum (accum
+// itself where wsum is 0) into `out`, then the region zeroed.
+cudaError_t launch_collab_normalise(int32_t* accum, int32_t* wsum, float* out, int64_t pixels, int channels,
+                                    cudaStream_t stream);
+
 // Block-matching motion search (motion.cu). The pyramid must already hold every slot it reads.
 struct MotionLaunch {
     static constexpr int kMaxInlineSlots = 16;

@@ -1,0 +1,541 @@
+// NL4D pass over one plane group: the collaborative denoiser of av-denoise-core/src/nl4d with its
+// NLMeans-HQ front end, for a pinned sigma.
+//
+//   engine       <- nl4d/engine.rs:208-410 (push, push_context, emit_into, finish, reset, pending
+//                   regions, the lazily queued tail)
+//   denoiser     <- nl4d/denoiser.rs:363-600, 772-816 (head passes at a scene start, one middle pass
+//                   per push, tail passes at the end, accumulator regions cleared and normalised)
+//   pass         <- nl4d/collab_pass.rs:45-250 (regions zeroed, then one `collab_fused` launch)
+//   front ring   <- nlmeans/denoiser/ring.rs with shifted edges (nlmeans/edges.rs: no leading copies,
+//                   a short stream padded with its last frame at flush)
+//   motion       <- nlmeans/dispatch/motion.rs:173-229 (`match_neighbours`): every neighbour in
+//                   logical order against the pass's centre, confidence against the SAD floor
+//   derived      <- nlmeans/denoiser/noise.rs:343-382 (`fixed_derived_values`) for the pinned sigma:
+//                   sigma per channel, weight scale sigma^2 * g_max^2 (floored), no noise curve, the
+//                   motion SAD floor sad_noise_floor(blksize, sigma)
+//
+// Device layout: the f32 frame ring (slots x pixels x channels, interleaved), its luma pyramid,
+// the i32 accumulator ring (slots x pixels x channels) and weight ring (slots x pixels), two f32
+// output frames, and one table of neighbour slots for every (ring start, centre) pair so no pass
+// uploads anything. Every launch is queued on the caller's stream; nothing synchronises the host.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <deque>
+#include <vector>
+
+#include "avd_internal.h"
+#include "engine_parts.h"
+#include "kernels.h"
+
+namespace avd {
+namespace {
+
+constexpr int kPatch = 8;
+constexpr int kMaxK = 8;
+// Derived words of this pass: sigma per channel, then the weight scale, the curve flag and the
+// motion search's SAD floor.
+constexpr int kSigmaWord = 0, kWeightScaleWord = 2, kCurveValidWord = 3, kSadFloorWord = 4;
+
+int64_t pad8(int64_t n) { return (n + 7) / 8 * 8; }
+
+class Nl4dPass final : public Pass {
+   public:
+    static std::optional<Failure> create(const AvdNl4dOptions& o, Channels channels, uint32_t width,
+                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
+                                         std::unique_ptr<Pass>* result) {
+        if (!o.has_sigma)
+            return Failure{AVD_ERR_INVALID_OPTIONS,
+                           "NL4D with the automatic noise estimate is not available in this build yet; set sigma"};
+        const AvdMotionSearch& m = o.motion;
+        if (m.max_search_escalation > m.search_radius)
+            return Failure{AVD_ERR_INVALID_OPTIONS,
+                           "motion search escalation is not available in this build; set max_search_escalation "
+                           "to search_radius"};
+        const bool chained = m.estimation == AVD_ESTIMATION_CHAINED ||
+                             (m.estimation == AVD_ESTIMATION_AUTO && o.temporal_radius >= kChainedRadiusThreshold);
+        if (chained)
+            return Failure{AVD_ERR_INVALID_OPTIONS,
+                           "chained motion estimation is not available in this build; use estimation Direct"};
+        if (width < kPatch || height < kPatch) {
+            char msg[200];
+            std::snprintf(msg, sizeof(msg),
+                          "frame dimensions %ux%u must be at least %dx%d for the collaborative filter's patch grid",
+                          width, height, kPatch, kPatch);
+            return Failure{AVD_ERR_INVALID_GEOMETRY, msg};
+        }
+        auto p = std::unique_ptr<Nl4dPass>(new Nl4dPass());
+        p->opts_ = o;
+        p->channels_ = channels;
+        p->width_ = width;
+        p->height_ = height;
+        p->in_ = in;
+        p->out_ = out;
+        p->d_ = o.temporal_radius;
+        p->held_ = nl4d_held_frames(o, channels);
+        p->lambda_ = nl4d_lambda_ht(o, channels);
+        p->pool_ratio_ = nl4d_pool_ratio(channels);
+        p->accum_scale_ = avd_cross_frame_accum_scale(o.spatial_radius, o.temporal_radius);
+        p->step_ = static_cast<int>(m.blksize - m.overlap);
+        p->blocks_x_ = std::max<int>((static_cast<int>(width) + p->step_ - 1) / p->step_, 1);
+        p->blocks_y_ = std::max<int>((static_cast<int>(height) + p->step_ - 1) / p->step_, 1);
+        p->mv_stride_ = static_cast<int>(pad8(2LL * p->blocks_x_ * p->blocks_y_));
+        p->conf_stride_ = static_cast<int>(pad8(static_cast<int64_t>(p->blocks_x_) * p->blocks_y_));
+        p->thsad_ = avd_thsad(m.blksize, o.thsad_scale);
+        if (auto f = p->allocate()) return f;
+        *result = std::move(p);
+        return std::nullopt;
+    }
+
+    // nl4d/engine.rs:287-308.
+    std::optional<Failure> push(const AvdPlane* planes, size_t* ready) override {
+        if (poisoned_) return status(AVD_ERR_NEEDS_RESET);
+        if (!pending_.empty() || tail_remaining_ > 0) return status(AVD_ERR_OUTPUTS_PENDING);
+        if (auto f = check_planes(planes, in_)) return f;
+        cudaEvent_t start{};
+        const bool timed = timer_.begin(stream, &start);
+        if (auto f = guard(push_planes(planes))) return f;
+        pushed_ = true;
+        std::optional<uint32_t> region;
+        if (auto f = guard(submit_passes(&region))) return f;
+        if (timed) timer_.end(stream, start);
+        if (region) pending_.push_back(*region);
+        pushes_ += 1;
+        *ready = pending_.size();
+        return std::nullopt;
+    }
+
+    // nl4d/engine.rs:310-327.
+    std::optional<Failure> push_context(const AvdPlane* planes) override {
+        if (poisoned_) return status(AVD_ERR_NEEDS_RESET);
+        if (!pending_.empty() || tail_remaining_ > 0) return status(AVD_ERR_OUTPUTS_PENDING);
+        if (auto f = check_planes(planes, in_)) return f;
+        if (pushed_) return status(AVD_ERR_CONTEXT_AFTER_PUSH);
+        if (pushes_ == 0) continuation_ = true;
+        if (auto f = guard(push_planes(planes))) return f;
+        pushes_ += 1;
+        return std::nullopt;
+    }
+
+    // nl4d/engine.rs:329-366.
+    std::optional<Failure> emit_into(const AvdPlane* planes) override {
+        if (poisoned_) return status(AVD_ERR_NEEDS_RESET);
+        if (auto f = check_planes(planes, out_)) return f;
+        if (pending_.empty() && tail_remaining_ > 0) {
+            if (auto f = guard(queue_tail_regions())) return f;
+        }
+        if (pending_.empty()) return status(AVD_ERR_NOTHING_TO_EMIT);
+        const uint32_t slot = pending_.front();
+        pending_.pop_front();
+        emitted_ = slot_frames_[slot];
+        int out_slot = 0;
+        if (auto f = guard(normalise_region(slot, &out_slot))) return f;
+        if (auto f = guard(write_out(out_slot, planes))) return f;
+        if (tail_remaining_ > 0) {
+            tail_remaining_ -= 1;
+            if (tail_remaining_ == 0) restart_stream();
+        }
+        return std::nullopt;
+    }
+
+    // nl4d/engine.rs:368-381 with nl4d/denoiser.rs:496-505 (no look-ahead with a pinned sigma).
+    std::optional<Failure> finish(size_t* tail) override {
+        if (poisoned_) return status(AVD_ERR_NEEDS_RESET);
+        if (!pending_.empty() || tail_remaining_ > 0) return status(AVD_ERR_OUTPUTS_PENDING);
+        const size_t count = std::min<size_t>(real_pushes_, 2 * d_);
+        if (count == 0)
+            restart_stream();
+        else
+            tail_remaining_ = count;
+        *tail = count;
+        return std::nullopt;
+    }
+
+    void reset() override {
+        pending_.clear();
+        emitted_.reset();
+        poisoned_ = false;
+        restart_stream();
+    }
+
+    size_t max_held_frames() const override { return held_; }
+    AvdWindowSpan window_span() const override {
+        AvdWindowSpan s{};
+        s.behind = held_;
+        s.ahead = held_;
+        s.edges = 1;  // EdgePadding::Shifted
+        return s;
+    }
+    uint32_t next_frame() const override { return static_cast<uint32_t>(real_pushes_); }
+    std::optional<uint32_t> emitted_frame() const override { return emitted_; }
+    AvdEngineTiming timing() override { return timer_.collect(); }
+    void sample_device_time(uint32_t every) override { timer_.every = every; }
+    std::optional<Failure> fail_for_test() override {
+        poisoned_ = true;
+        return Failure{AVD_ERR_GPU, "forced failure"};
+    }
+
+   private:
+    Nl4dPass() = default;
+
+    static Failure status(AvdStatus s) { return Failure{s, avd_status_message(s)}; }
+    static Failure gpu_failure(const char* what, cudaError_t e) { return Failure{AVD_ERR_GPU, cuda_message(what, e)}; }
+    std::optional<Failure> guard(std::optional<Failure> f) {
+        if (f && f->status == AVD_ERR_GPU) poisoned_ = true;
+        return f;
+    }
+
+    uint32_t C() const { return static_cast<uint32_t>(channels_); }
+    uint32_t tf() const { return 2 * d_ + 1; }
+    size_t pixels() const { return static_cast<size_t>(width_) * height_; }
+    size_t frame_elems() const { return pixels() * C(); }
+    float bias() const { return channels_ == Channels::Chroma ? 0.5f : 0.0f; }
+    float* slot_ptr(size_t slot) const { return ring_.as<float>() + slot * frame_elems(); }
+
+    std::optional<Failure> allocate() {
+        cudaError_t e;
+        const size_t fe = frame_elems(), t = tf();
+        const int levels = static_cast<int>(opts_.motion.pyramid_levels);
+        if ((e = ring_.alloc(fe * t * sizeof(float))) != cudaSuccess) return gpu_failure("frame ring", e);
+        const int64_t pyr = pyramid_floats(static_cast<int>(width_), static_cast<int>(height_), static_cast<int>(t),
+                                           levels);
+        if ((e = pyramid_.alloc(static_cast<size_t>(pyr) * sizeof(float))) != cudaSuccess)
+            return gpu_failure("motion pyramid", e);
+        const size_t nbrs = 2 * d_;
+        if ((e = mv_.alloc(nbrs * mv_stride_ * sizeof(int32_t))) != cudaSuccess) return gpu_failure("motion field", e);
+        if ((e = conf_.alloc(nbrs * conf_stride_ * sizeof(float))) != cudaSuccess) return gpu_failure("confidence", e);
+        if ((e = accum_.alloc(fe * t * sizeof(int32_t))) != cudaSuccess) return gpu_failure("accumulator ring", e);
+        if ((e = wsum_.alloc(pixels() * t * sizeof(int32_t))) != cudaSuccess) return gpu_failure("weight ring", e);
+        const size_t refs = static_cast<size_t>((width_ - kPatch + 3) / 4 + 1) * ((height_ - kPatch + 3) / 4 + 1);
+        if ((e = group_weight_.alloc(refs * sizeof(float))) != cudaSuccess) return gpu_failure("group weights", e);
+        for (auto& o : outputs_)
+            if ((e = o.alloc(fe * sizeof(float))) != cudaSuccess) return gpu_failure("output slot", e);
+
+        // Fixed tables: derived words, the (unused) noise curve, the white-noise DCT profile
+        // (nl4d/denoiser.rs:273-277) and the Kaiser taps.
+        float words[8] = {0};
+        const float sigma = opts_.sigma;
+        words[kSigmaWord] = sigma;
+        words[kSigmaWord + 1] = sigma;
+        float profile[8], kaiser[8];
+        avd_dct_noise_profile(0.0f, profile);
+        avd_kaiser_window(opts_.kaiser_beta, kaiser);
+        float g_max = 0.0f;
+        for (float g : profile) g_max = std::max(g_max, g);
+        const float norm = sigma * sigma * g_max * g_max;
+        words[kWeightScaleWord] = (std::isfinite(norm) && norm > 1e-12f) ? norm : 1e-12f;
+        words[kCurveValidWord] = 0.0f;
+        words[kSadFloorWord] = avd_sad_noise_floor(opts_.motion.blksize, sigma);
+        std::vector<float> tables(8 + 16 + 8 + 8, 0.0f);
+        std::copy(words, words + 8, tables.begin());
+        std::copy(profile, profile + 8, tables.begin() + 24);
+        std::copy(kaiser, kaiser + 8, tables.begin() + 32);
+        if ((e = tables_.alloc(tables.size() * sizeof(float))) != cudaSuccess) return gpu_failure("tables", e);
+        if ((e = cudaMemcpy(tables_.ptr, tables.data(), tables.size() * sizeof(float), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return gpu_failure("tables upload", e);
+
+        // Neighbour slots of every (ring start, centre): logical order with the centre skipped.
+        std::vector<uint32_t> slot_tables(static_cast<size_t>(t) * t * nbrs);
+        for (uint32_t start = 0; start < t; ++start)
+            for (uint32_t centre = 0; centre < t; ++centre) {
+                uint32_t* row = slot_tables.data() + (static_cast<size_t>(start) * t + centre) * nbrs;
+                uint32_t n = 0;
+                for (uint32_t l = 0; l < t; ++l)
+                    if (l != centre) row[n++] = (start + l) % t;
+            }
+        if ((e = slot_tables_.alloc(slot_tables.size() * sizeof(uint32_t))) != cudaSuccess)
+            return gpu_failure("slot tables", e);
+        if ((e = cudaMemcpy(slot_tables_.ptr, slot_tables.data(), slot_tables.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return gpu_failure("slot tables upload", e);
+        slot_frames_.assign(t, 0u);
+        zeroed_.assign(t, false);
+        return std::nullopt;
+    }
+
+    const float* noise_words() const { return tables_.as<float>(); }
+    const float* noise_curve() const { return tables_.as<float>() + 8; }
+    const float* dct_profile() const { return tables_.as<float>() + 24; }
+    const float* kaiser_taps() const { return tables_.as<float>() + 32; }
+
+    std::optional<Failure> check_planes(const AvdPlane* planes, const AvdSampleFormat& fmt) const {
+        const uint64_t need = plane_bytes(fmt, pixels());
+        for (uint32_t i = 0; i < C(); ++i) {
+            const AvdPlane& p = planes[i];
+            if (p.width != width_ || p.height != height_) {
+                char m[160];
+                std::snprintf(m, sizeof(m), "plane %u is %ux%u, expected %ux%u", i, p.width, p.height, width_, height_);
+                return Failure{AVD_ERR_PLANE_MISMATCH, m};
+            }
+            if (p.bytes < need) {
+                char m[160];
+                std::snprintf(m, sizeof(m), "plane %u handle holds %llu bytes, needs %llu", i,
+                              (unsigned long long)p.bytes, (unsigned long long)need);
+                return Failure{AVD_ERR_PLANE_MISMATCH, m};
+            }
+            if (p.ptr == 0) return Failure{AVD_ERR_PLANE_MISMATCH, "a plane has a null device pointer"};
+        }
+        return std::nullopt;
+    }
+
+    // ---- front ring (shifted edges) ----------------------------------------------------------
+
+    size_t ring_start() const { return ring_head_ % tf(); }
+    uint32_t phys(uint32_t logical) const { return static_cast<uint32_t>((ring_start() + logical) % tf()); }
+    bool window_ready() const { return frames_loaded_ >= tf(); }
+
+    std::optional<Failure> build_pyramid(size_t slot) {
+        cudaError_t e = launch_pyramid_build(ring_.as<float>(), static_cast<int>(C()), static_cast<int>(width_),
+                                             static_cast<int>(height_), static_cast<int>(tf()),
+                                             static_cast<int>(slot), static_cast<int>(opts_.motion.pyramid_levels),
+                                             pyramid_.as<float>(), static_cast<int>(slot), stream);
+        if (e != cudaSuccess) return gpu_failure("pyramid launch", e);
+        return std::nullopt;
+    }
+
+    std::optional<Failure> push_planes(const AvdPlane* planes) {
+        const size_t slot = ring_head_ % tf();
+        const void* p0 = reinterpret_cast<const void*>(planes[0].ptr);
+        const void* p1 = C() > 1 ? reinterpret_cast<const void*>(planes[1].ptr) : nullptr;
+        cudaError_t e = launch_ingest(p0, p1, slot_ptr(slot), static_cast<int64_t>(pixels()), static_cast<int>(C()),
+                                      plane_format(in_), bias(), stream);
+        if (e != cudaSuccess) return gpu_failure("ingest launch", e);
+        if (auto f = build_pyramid(slot)) return f;
+        slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
+        ring_head_ += 1;
+        if (frames_loaded_ < tf()) frames_loaded_ += 1;
+        real_pushes_ += 1;
+        return std::nullopt;
+    }
+
+    // nlmeans/denoiser/ring.rs:128-146 and nlmeans/edges.rs:41-48.
+    std::optional<Failure> fill_ring_with_last_frame() {
+        while (!window_ready()) {
+            const size_t last = (ring_head_ - 1) % tf(), next = ring_head_ % tf();
+            cudaError_t e = cudaMemcpyAsync(slot_ptr(next), slot_ptr(last), frame_elems() * sizeof(float),
+                                            cudaMemcpyDeviceToDevice, stream);
+            if (e != cudaSuccess) return gpu_failure("slot copy", e);
+            if (auto f = build_pyramid(next)) return f;
+            slot_frames_[next] = slot_frames_[last];
+            ring_head_ += 1;
+            frames_loaded_ += 1;
+        }
+        return std::nullopt;
+    }
+
+    // ---- passes ----------------------------------------------------------------------------
+
+    const uint32_t* slot_table(uint32_t centre) const {
+        return slot_tables_.as<uint32_t>() + (ring_start() * tf() + centre) * (2 * d_);
+    }
+
+    // nlmeans/denoiser/machinery.rs:45-102 then dispatch/motion.rs:173-229.
+    std::optional<Failure> machinery_at(uint32_t centre) {
+        MotionLaunch m{};
+        m.pyramid = pyramid_.as<float>();
+        m.neighbour_slots = slot_table(centre);
+        m.mv_field = mv_.as<int32_t>();
+        m.confidence = conf_.as<float>();
+        m.noise = noise_words();
+        m.width = static_cast<int>(width_);
+        m.height = static_cast<int>(height_);
+        m.frame_count = static_cast<int>(tf());
+        m.centre_slot = static_cast<int>(phys(centre));
+        m.neighbours = static_cast<int>(2 * d_);
+        m.blksize = static_cast<int>(opts_.motion.blksize);
+        m.overlap = static_cast<int>(opts_.motion.overlap);
+        m.search_radius = static_cast<int>(opts_.motion.search_radius);
+        m.coarse_radius = m.search_radius;
+        m.coarse_block_factor = 1;
+        m.levels = static_cast<int>(opts_.motion.pyramid_levels);
+        m.mv_stride = mv_stride_;
+        m.conf_stride = conf_stride_;
+        m.sad_floor_word = kSadFloorWord;
+        m.thsad = thsad_;
+        cudaError_t e = launch_motion_search(m, stream);
+        if (e != cudaSuccess) return gpu_failure("motion search launch", e);
+        return std::nullopt;
+    }
+
+    enum class Clear { WholeRing, NewestRegion, Nothing };
+
+    // nl4d/collab_pass.rs:45-130 and 131-190.
+    std::optional<Failure> run_pass(uint32_t centre, Clear clear) {
+        const uint32_t centre_slot = phys(centre);
+        uint32_t c0 = 0, c1 = 0;
+        if (clear == Clear::WholeRing) {
+            c1 = tf();
+        } else if (clear == Clear::NewestRegion) {
+            const uint32_t newest = (centre_slot + d_) % tf();
+            c0 = newest;
+            c1 = zeroed_[newest] ? newest : newest + 1;
+        }
+        std::fill(zeroed_.begin(), zeroed_.end(), false);
+        passes_run_ += 1;
+        for (uint32_t s = c0; s < c1; ++s) {
+            cudaError_t e = cudaMemsetAsync(accum_.as<int32_t>() + s * frame_elems(), 0, frame_elems() * sizeof(int32_t),
+                                            stream);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(wsum_.as<int32_t>() + s * pixels(), 0, pixels() * sizeof(int32_t), stream);
+            if (e != cudaSuccess) return gpu_failure("accumulator clear", e);
+        }
+        CollabLaunch a{};
+        a.ring = ring_.as<float>();
+        a.width = static_cast<int>(width_);
+        a.height = static_cast<int>(height_);
+        a.channels = static_cast<int>(C());
+        a.centre_slot = static_cast<int>(centre_slot);
+        a.frame_elems = static_cast<int64_t>(frame_elems());
+        a.mv_field = mv_.as<int32_t>();
+        a.confidence = conf_.as<float>();
+        a.neighbour_slots = slot_table(centre);
+        a.noise = noise_words();
+        a.sigma_word = kSigmaWord;
+        a.weight_scale_word = kWeightScaleWord;
+        a.curve_valid_word = kCurveValidWord;
+        a.noise_curve = noise_curve();
+        a.dct_profile = dct_profile();
+        a.kaiser = kaiser_taps();
+        a.accum = accum_.as<int32_t>();
+        a.wsum = wsum_.as<int32_t>();
+        a.group_weight = group_weight_.as<float>();
+        a.c_min = opts_.c_min;
+        a.lambda_ht = lambda_;
+        a.accum_scale = accum_scale_;
+        a.pool_ratio = pool_ratio_;
+        a.pooled = opts_.pooled_threshold ? 1 : 0;
+        a.radius = static_cast<int>(d_);
+        a.refine = static_cast<int>(opts_.refine);
+        a.spatial_radius = static_cast<int>(opts_.spatial_radius);
+        a.k_max = kMaxK;
+        a.mv_stride = mv_stride_;
+        a.conf_stride = conf_stride_;
+        a.blk_step = step_;
+        a.blksize = static_cast<int>(opts_.motion.blksize);
+        a.blocks_x = blocks_x_;
+        a.blocks_y = blocks_y_;
+        cudaError_t e = launch_collab(a, stream);
+        if (e != cudaSuccess) return gpu_failure("collab launch", e);
+        return std::nullopt;
+    }
+
+    // nl4d/denoiser.rs:370-406 (`submit_passes`).
+    std::optional<Failure> submit_passes(std::optional<uint32_t>* region) {
+        region->reset();
+        if (!window_ready()) return std::nullopt;
+        const bool opens_scene = passes_run_ == 0 && !continuation_;
+        Clear clear = passes_run_ == 0 ? Clear::WholeRing : Clear::NewestRegion;
+        if (opens_scene) {
+            for (uint32_t centre = 0; centre < d_; ++centre) {
+                if (auto f = machinery_at(centre)) return f;
+                if (auto f = run_pass(centre, clear)) return f;
+                clear = Clear::Nothing;
+            }
+        }
+        if (auto f = machinery_at(d_)) return f;
+        if (auto f = run_pass(d_, clear)) return f;
+        if (passes_run_ <= d_) return std::nullopt;
+        *region = (phys(d_) + tf() - d_) % tf();
+        return std::nullopt;
+    }
+
+    // nl4d/denoiser.rs:544-596 (`finish_passes`).
+    std::optional<Failure> queue_tail_regions() {
+        const uint32_t emit = static_cast<uint32_t>(std::min<size_t>(real_pushes_, 2 * d_));
+        if (emit == 0) return std::nullopt;
+        const bool short_stream = real_pushes_ < tf();
+        if (short_stream) {
+            if (auto f = fill_ring_with_last_frame()) return f;
+        }
+        const uint32_t first = short_stream ? 0 : d_ + 1;
+        const uint32_t end = short_stream ? emit : 2 * d_ + 1;
+        const uint32_t last_real = short_stream ? emit - 1 : 2 * d_;
+        Clear clear = (short_stream || passes_run_ == 0) ? Clear::WholeRing : Clear::Nothing;
+        for (uint32_t centre = first; centre < end; ++centre) {
+            if (auto f = machinery_at(centre)) return f;
+            if (auto f = run_pass(centre, clear)) return f;
+            clear = Clear::Nothing;
+        }
+        const size_t owed = tail_remaining_;
+        if (emit != owed) {
+            char m[120];
+            std::snprintf(m, sizeof(m), "the tail completed %u of %zu owed regions", emit, owed);
+            return Failure{AVD_ERR_GPU, m};
+        }
+        for (uint32_t logical = last_real + 1 - emit; logical <= last_real; ++logical) pending_.push_back(phys(logical));
+        return std::nullopt;
+    }
+
+    // nl4d/denoiser.rs:772-816 and collab/kernels/aggregate.rs:240-290.
+    std::optional<Failure> normalise_region(uint32_t slot, int* out_slot) {
+        *out_slot = next_output_slot_;
+        next_output_slot_ = (next_output_slot_ + 1) % 2;
+        cudaError_t e = launch_collab_normalise(accum_.as<int32_t>() + slot * frame_elems(),
+                                                wsum_.as<int32_t>() + slot * pixels(), outputs_[*out_slot].as<float>(),
+                                                static_cast<int64_t>(pixels()), static_cast<int>(C()), stream);
+        if (e != cudaSuccess) return gpu_failure("normalise launch", e);
+        zeroed_[slot] = true;
+        return std::nullopt;
+    }
+
+    std::optional<Failure> write_out(int slot, const AvdPlane* planes) {
+        void* p0 = reinterpret_cast<void*>(planes[0].ptr);
+        void* p1 = C() > 1 ? reinterpret_cast<void*>(planes[1].ptr) : nullptr;
+        cudaError_t e = launch_egress(outputs_[slot].as<float>(), p0, p1, static_cast<int64_t>(pixels()),
+                                      static_cast<int>(C()), plane_format(out_), bias(), stream);
+        if (e != cudaSuccess) return gpu_failure("egress launch", e);
+        return std::nullopt;
+    }
+
+    // nl4d/engine.rs:166-171 with nl4d/denoiser.rs:598-610.
+    void restart_stream() {
+        ring_head_ = 0;
+        frames_loaded_ = 0;
+        real_pushes_ = 0;
+        passes_run_ = 0;
+        next_output_slot_ = 0;
+        continuation_ = false;
+        std::fill(zeroed_.begin(), zeroed_.end(), false);
+        tail_remaining_ = 0;
+        pushes_ = 0;
+        pushed_ = false;
+    }
+
+    AvdNl4dOptions opts_{};
+    Channels channels_ = Channels::Luma;
+    uint32_t width_ = 0, height_ = 0, d_ = 1;
+    AvdSampleFormat in_{}, out_{};
+    size_t held_ = 0;
+    float lambda_ = 0.0f, pool_ratio_ = 0.0f, accum_scale_ = 0.0f, thsad_ = 0.0f;
+    int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2, conf_stride_ = 1;
+
+    DeviceBuffer ring_, pyramid_, mv_, conf_, accum_, wsum_, group_weight_, tables_, slot_tables_;
+    DeviceBuffer outputs_[2];
+
+    size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;
+    std::vector<uint32_t> slot_frames_;
+    uint64_t passes_run_ = 0;
+    bool continuation_ = false;
+    std::vector<bool> zeroed_;
+    int next_output_slot_ = 0;
+
+    std::deque<uint32_t> pending_;
+    size_t tail_remaining_ = 0, pushes_ = 0;
+    bool pushed_ = false, poisoned_ = false;
+    std::optional<uint32_t> emitted_;
+    DeviceTimer timer_;
+};
+
+}  // namespace
+
+std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels channels, uint32_t width,
+                                        uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
+                                        std::unique_ptr<Pass>* result) {
+    return Nl4dPass::create(options, channels, width, height, in, out, result);
+}
+
+}  // namespace avd

@@ -294,10 +294,18 @@ size_t nlm_held_frames(const AvdNlmeansAlgorithm& alg, Channels channels) {
     return p.temporal_radius + (measures ? kLookaheadFrames : 0u);
 }
 
+// nl4d/engine.rs:33-35: the whole window either side, plus the noise look-ahead when measured.
 size_t nl4d_held_frames(const AvdNl4dOptions& o, Channels) {
     bool measures = o.has_sigma == 0;
-    return o.temporal_radius + (measures ? kLookaheadFrames : 0u);
+    return 2 * o.temporal_radius + (measures ? kLookaheadFrames : 0u);
 }
+
+float nl4d_lambda_ht(const AvdNl4dOptions& o, Channels c) {
+    return (o.has_lambda_ht ? o.lambda_ht : nl4d_default_lambda_ht(c)) * o.lambda_ht_scale;
+}
+
+// nl4d/options.rs:108-117: the calibrated pooled threshold 2.42 over the plane's default lambda.
+float nl4d_pool_ratio(Channels c) { return 2.42f / nl4d_default_lambda_ht(c); }
 
 AvdStatus validate_spec(const AvdEngineSpec& spec, std::string* message) {
     auto fail = [&](AvdStatus st, std::string m) {

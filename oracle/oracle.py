@@ -334,3 +334,121 @@ def thsad(blksize: int, thsad_scale: float) -> float:
     """motion/confidence.rs:27-30 in f32."""
     f = np.float32
     return float(f(f(thsad_scale) * f(blksize * blksize)) * f(0.02))
+
+
+# ---- NL4D engine over a stream (nl4d/engine.rs, nl4d/denoiser.rs) --------------------------------
+
+def collab_normalise(accum: np.ndarray, wsum: np.ndarray, channels: int) -> np.ndarray:
+    """collab/kernels/aggregate.rs:251-290: accum * 5 / wsum in f32, accum itself where wsum is 0."""
+    f = np.float32
+    acc = accum.reshape(-1, channels).astype(np.float32)
+    w = wsum.astype(np.float32)[:, None]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        v = (acc * f(5.0)).astype(np.float32) / np.where(w != 0, w, f(1.0))
+    return np.where(w != 0, v, acc).astype(np.float32)
+
+
+def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, overlap=8, search_radius=4,
+                levels=2, refine=2, spatial_radius=9, lambda_ht=4.158, c_min=0.05, kaiser_beta=2.0,
+                pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0) -> list[np.ndarray]:
+    """The NL4D engine with a pinned sigma and Direct motion (no camera model, no truemotion) over a
+    stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order.
+
+    It follows nl4d/engine.rs:287-381 and nl4d/denoiser.rs:370-596: a shifted-edge ring of 2d+1
+    slots; when the ring first fills at a scene start, head passes centred on logical 0..d-1, then
+    one pass centred on the middle slot per push; after more than d passes each middle pass
+    completes the region d slots behind it; at the end, tail passes centred on d+1..2d (or, for a
+    stream shorter than the ring, on every real frame after padding with the last frame). The
+    first `context` frames are priming pushes (no head passes)."""
+    h, w, c = frames[0].shape
+    tf = 2 * d + 1
+    step = blksize - overlap
+    bx, by = max(-(-w // step), 1), max(-(-h // step), 1)
+    ring = np.zeros((tf, h, w, c), np.float32)
+    accum = np.zeros((tf, h * w * c), np.int64)
+    wsum = np.zeros((tf, h * w), np.int64)
+    st = dict(head=0, loaded=0, real=0, passes=0, cont=context > 0)
+    slot_frames = [0] * tf
+    zeroed = [False] * tf
+    sad_floor = sad_noise_floor(blksize, sigma)
+    th = thsad(blksize, thsad_scale)
+
+    def phys(logical):
+        return (st["head"] % tf + logical) % tf
+
+    def run_pass(centre, clear):
+        cs = phys(centre)
+        if clear == "whole":
+            for s in range(tf):
+                accum[s] = 0
+                wsum[s] = 0
+        elif clear == "newest":
+            newest = (cs + d) % tf
+            if not zeroed[newest]:
+                accum[newest] = 0
+                wsum[newest] = 0
+        for i in range(tf):
+            zeroed[i] = False
+        st["passes"] += 1
+        slots = [phys(l) for l in range(tf) if l != centre]
+        pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
+        mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
+                                 search_radius=search_radius, levels=levels, confidence=True,
+                                 sad_floor=sad_floor, thsad=th)
+        acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
+                                  confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
+                                  c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
+                                  sigma=(sigma,) * c, lambda_ht=lambda_ht, kaiser_beta=kaiser_beta,
+                                  pooled=pool_ratio, blksize=blksize, blk_step=step, blocks_x=bx, blocks_y=by,
+                                  mv_stride=bx * by * 2, conf_stride=bx * by)
+        accum[:] += acc.reshape(tf, -1)
+        wsum[:] += ws.reshape(tf, -1)
+
+    def read_region(slot):
+        out = collab_normalise(accum[slot].astype(np.int32), wsum[slot].astype(np.int32), c).reshape(h, w, c)
+        accum[slot] = 0
+        wsum[slot] = 0
+        zeroed[slot] = True
+        return out
+
+    def push(frame):
+        s = st["head"] % tf
+        ring[s] = frame
+        slot_frames[s] = st["real"]
+        st["head"] += 1
+        st["loaded"] = min(st["loaded"] + 1, tf)
+        st["real"] += 1
+
+    outs = []
+    for i, frame in enumerate(frames):
+        push(frame)
+        if i < context or st["loaded"] < tf:
+            continue
+        clear = "whole" if st["passes"] == 0 else "newest"
+        if st["passes"] == 0 and not st["cont"]:
+            for centre in range(d):
+                run_pass(centre, clear)
+                clear = "none"
+        run_pass(d, clear)
+        if st["passes"] > d:
+            outs.append(read_region((phys(d) + tf - d) % tf))
+    emit = min(st["real"], 2 * d)
+    if emit == 0:
+        return outs
+    short = st["real"] < tf
+    if short:
+        while st["loaded"] < tf:
+            last, nxt = (st["head"] - 1) % tf, st["head"] % tf
+            ring[nxt] = ring[last]
+            slot_frames[nxt] = slot_frames[last]
+            st["head"] += 1
+            st["loaded"] += 1
+    centres = range(emit) if short else range(d + 1, 2 * d + 1)
+    last_real = emit - 1 if short else 2 * d
+    clear = "whole" if (short or st["passes"] == 0) else "none"
+    for centre in centres:
+        run_pass(centre, clear)
+        clear = "none"
+    for logical in range(last_real + 1 - emit, last_real + 1):
+        outs.append(read_region(phys(logical)))
+    return outs

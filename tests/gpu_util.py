@@ -157,7 +157,8 @@ class Parity:
         self.total = self.same = self.ties = self.same_nontie = self.nontie = 0
         self.max_lsb = 0
 
-    def add(self, got: np.ndarray, want: np.ndarray, exact: np.ndarray | None, max_value: float):
+    def add(self, got: np.ndarray, want: np.ndarray, exact: np.ndarray | None, max_value: float,
+            tie_band: float = TIE_BAND):
         diff = np.abs(got.astype(np.int64) - want.astype(np.int64))
         self.max_lsb = max(self.max_lsb, int(diff.max()) if diff.size else 0)
         self.total += diff.size
@@ -166,7 +167,7 @@ class Parity:
             tie = np.zeros(diff.shape, bool)
         else:
             t = np.clip(exact, 0.0, 1.0) * max_value + 0.5
-            tie = np.abs(t - np.rint(t)) < TIE_BAND * max_value
+            tie = np.abs(t - np.rint(t)) < tie_band * max_value
         self.ties += int(tie.sum())
         self.nontie += int((~tie).sum())
         self.same_nontie += int(((diff == 0) & ~tie).sum())

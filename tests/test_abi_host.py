@@ -141,16 +141,19 @@ def test_hq_sigma_scale_and_override_ranges():
 
 def test_window_spans():
     # engine/spec.rs:260-281: NLM holds d frames (plus the 8-frame look-ahead when HQ measures
-    # noise); NL4D holds d + 8 with shifted edges.
+    # noise); NL4D holds 2d (+ 8 when it measures noise) with shifted edges
+    # (nl4d/tests/engine.rs:739-773).
     s = avd.EngineSpec.nlmeans(nlm(2), None, geo()).window_span()
     assert (s.behind, s.ahead, s.edges) == (2, 2, "repeat")
     hq = avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(nlm=avd.NlmeansOptions(mode=avd.DenoisingMode.temporal(1))))
     s = avd.EngineSpec.nlmeans(hq, None, geo()).window_span()
     assert (s.behind, s.edges) == (9, "repeat")
     s = avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=3), None, geo()).window_span()
-    assert (s.behind, s.edges) == (11, "shifted")
-    s = avd.EngineSpec.nl4d(avd.Nl4dOptions(sigma=0.05), None, geo()).window_span()
-    assert s.behind == 2
+    assert (s.behind, s.edges) == (14, "shifted")
+    s = avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=2), None, geo()).window_span()
+    assert (s.behind, s.ahead) == (12, 12)
+    s = avd.EngineSpec.nl4d(avd.Nl4dOptions(sigma=0.03), None, geo()).window_span()
+    assert (s.behind, s.ahead) == (4, 4)
 
 
 def test_create_validates_before_touching_the_gpu():

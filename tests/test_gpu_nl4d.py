@@ -1,0 +1,121 @@
+"""The NL4D engine (pinned sigma, Direct motion) on the GPU through the C ABI against the oracle's
+stream restatement: the same ring, pass schedule, motion search, group filter and normalise.
+
+Motion vectors and confidences are bit-exact between the two; the group filter's f32 transforms
+differ in the last bits, which the fixed-point accumulators carry into outputs within about 3e-5
+(normalised) of each other. So a sample whose oracle value sits within 1e-4 of a rounding boundary
+is a tie, and the bar is the engine's: no sample more than 1 LSB apart, 99.9% of the rest identical."""
+
+import numpy as np
+import pytest
+
+from conftest import avd
+from gpu_util import Parity, Runner
+
+pytestmark = pytest.mark.gpu
+
+NL4D_TIE_BAND = 1e-4
+
+
+def clip(w, h, n, depth=8, chroma="gray", seed=0, sigma=10.0):
+    from av_denoise_b200 import synth
+
+    return synth.make_clip(w, h, n, depth=depth, chroma=chroma, sigma_luma=sigma, sigma_chroma=sigma * 0.6,
+                           global_motion=2, sprites=1, sprite_size=24, seed=seed)
+
+
+def opts(d, sigma, **kw):
+    return avd.Nl4dOptions(sigma=sigma, temporal_radius=d,
+                           motion=avd.MotionSearch(estimation=avd.MotionEstimation.DIRECT), **kw)
+
+
+def oracle_nl4d(oracle, frames, fmt, d, sigma, chroma=False, context=0, **kw):
+    f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), 0.0) for p in frames]
+    default_lambda = 3.234 if chroma else 4.158
+    lam = kw.pop("lambda_ht", None) or default_lambda
+    pooled = kw.pop("pooled_threshold", True)
+    outs = oracle.nl4d_stream(f32, d, sigma, lambda_ht=lam, pool_ratio=(2.42 / default_lambda) if pooled else None,
+                              context=context, **kw)
+    return [oracle.egress(o, fmt.kind, fmt.max_value(), 0.0) for o in outs], outs
+
+
+def check(oracle, got_planes, frames, fmt, d, sigma, chroma=False, context=0, **kw):
+    want, exact = oracle_nl4d(oracle, frames, fmt, d, sigma, chroma=chroma, context=context, **kw)
+    assert len(got_planes) == len(want)
+    par = Parity()
+    for g, wn, ex in zip(got_planes, want, exact):
+        for c in range(len(wn)):
+            par.add(g[c], wn[c], ex[..., c], fmt.max_value(), tie_band=NL4D_TIE_BAND)
+    st = par.check(min_raw=0.995)
+    print(st)
+    return st
+
+
+@pytest.mark.parametrize("w,h,n,d,sigma,sr", [(96, 64, 7, 1, 10.0 / 255, 4), (80, 56, 6, 2, 14.0 / 255, 9),
+                                              (72, 40, 9, 2, 6.0 / 255, 6)])
+def test_nl4d_luma_matches_oracle(oracle, w, h, n, d, sigma, sr):
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, n, seed=w + d)
+    spec = avd.EngineSpec.nl4d(opts(d, sigma, spatial_radius=sr), None,
+                               avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, spatial_radius=sr)
+
+
+def test_nl4d_plain_threshold_10bit(oracle):
+    w, h, d, sigma = 64, 48, 1, 8.0 / 255
+    fmt = avd.SampleFormat.u16(10)
+    frames = clip(w, h, 5, depth=10, seed=5)
+    o = opts(d, sigma, spatial_radius=5, pooled_threshold=False, lambda_ht=2.7, kaiser_beta=0.0, c_min=0.2)
+    spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, spatial_radius=5,
+          pooled_threshold=False, lambda_ht=2.7, kaiser_beta=0.0, c_min=0.2)
+
+
+def test_nl4d_chroma_with_luma_passthrough(oracle):
+    w, h, d, sigma = 96, 64, 1, 8.0 / 255
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 5, chroma="420", seed=9)
+    spec = avd.EngineSpec.nl4d(None, opts(d, sigma, spatial_radius=4),
+                               avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    for g, f in zip(got, frames):
+        assert np.array_equal(g[0], f[0])
+    check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, sigma, chroma=True,
+          spatial_radius=4)
+
+
+@pytest.mark.parametrize("n", [1, 2, 4])
+def test_nl4d_short_stream(oracle, n):
+    """A stream shorter than the ring is padded with its last frame at flush and every real frame
+    is a pass centre (nl4d/denoiser.rs:544-596)."""
+    w, h, d, sigma = 64, 40, 2, 10.0 / 255
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, n, seed=20 + n)
+    spec = avd.EngineSpec.nl4d(opts(d, sigma, spatial_radius=3), None,
+                               avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    assert len(got) == n
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, spatial_radius=3)
+
+
+def test_nl4d_continuation_skips_head_passes(oracle):
+    """Priming pushes mark a continuation: no head passes (nl4d/engine.rs:310-327)."""
+    w, h, d, sigma = 64, 48, 1, 10.0 / 255
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 7, seed=31)
+    spec = avd.EngineSpec.nl4d(opts(d, sigma, spatial_radius=3), None,
+                               avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames, context=2)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, context=2, spatial_radius=3)
+
+
+def test_nl4d_options_this_build_rejects():
+    fmt = avd.SampleFormat.u8()
+    g = avd.Geometry(64, 48, avd.ChromaLayout.GRAY, fmt, fmt)
+    with pytest.raises(avd.InvalidOptions, match="automatic noise estimate"):
+        avd.build_engine(avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=1), None, g))
+    chained = avd.Nl4dOptions(sigma=0.03, temporal_radius=3)
+    with pytest.raises(avd.InvalidOptions, match="chained"):
+        avd.build_engine(avd.EngineSpec.nl4d(chained, None, g))
