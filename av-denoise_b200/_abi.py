@@ -151,7 +151,7 @@ class AvdPassTimings(C.Structure):
 
 class AvdCollabPass(C.Structure):
     _fields_ = [(n, u64) for n in ("ring", "mv_field", "confidence", "neighbour_slots", "noise", "noise_curve",
-                                   "dct_profile", "kaiser", "accum", "wsum", "group_weight")] + \
+                                   "dct_profile", "kaiser", "accum", "wsum", "group_weight", "members")] + \
                [(n, u32) for n in ("width", "height", "channels", "centre_slot", "sigma_word", "weight_scale_word",
                                    "curve_valid_word", "radius", "refine", "spatial_radius", "k_max", "mv_stride",
                                    "conf_stride", "blk_step", "blksize", "blocks_x", "blocks_y", "pooled")] + \
@@ -198,6 +198,7 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_engine_fail_for_test": (C.c_int, [_E]),
     "avd_last_error": (C.c_char_p, []),
     "avd_collab_pass": (C.c_int, [_P(AvdCollabPass), C.c_void_p]),
+    "avd_collab_member_bytes": (u64, [u32, u32]),
     "avd_dct_noise_profile": (None, [f32, _P(f32)]),
     "avd_kaiser_window": (None, [f32, _P(f32)]),
     "avd_cross_frame_accum_scale": (f32, [u32, u32]),

@@ -351,18 +351,19 @@ __device__ __forceinline__ uint32_t covering_lo(uint32_t patch_start, uint32_t b
     return (overhang + step - 1) / step;
 }
 
-constexpr int kMaxRects = 16;  // MAX_COVERING_BLOCKS^2
-
 // fused/trajectory.rs (clipped walk): for each neighbour frame the best candidate over one refine
 // rectangle per covering motion block (blocks under c_min skipped, rectangles already searched and
-// positions the group holds skipped), inserted into the volume's sorted tail.
-template <int C, int GF, int FIRST>
+// positions the group holds skipped), inserted into the volume's sorted tail. COVERS (the covering
+// blocks per axis, ceil(blksize / step)) is a template argument so the rectangles searched so far
+// stay in registers. A skipped candidate can only matter if it would beat the frame's best so far,
+// so the skip test runs for those alone; the winner is the same.
+template <int C, int GF, int FIRST, int COVERS>
 __device__ __forceinline__ void trajectory_search(const GroupCtx& g, const CollabLaunch& a, const float (&anchor)[P * C],
                                                   uint32_t ax, uint32_t ay, float scale, float (&grid_d)[MAX_K],
                                                   uint32_t (&grid_pos)[MAX_K]) {
     constexpr int TAIL = GF - 1;
+    constexpr int RECTS = COVERS * COVERS;
     const uint32_t max_x = a.width - P, max_y = a.height - P;
-    const uint32_t covers = (a.blksize + a.blk_step - 1) / a.blk_step;
     const uint32_t bx_hi = min(ax / a.blk_step, static_cast<uint32_t>(a.blocks_x - 1));
     const uint32_t by_hi = min(ay / a.blk_step, static_cast<uint32_t>(a.blocks_y - 1));
     const uint32_t bx_lo = min(covering_lo(ax, a.blksize, a.blk_step), bx_hi);
@@ -373,15 +374,18 @@ __device__ __forceinline__ void trajectory_search(const GroupCtx& g, const Colla
         const uint32_t packed_t = t + 1;
         float frame_d = kUnfilled;
         uint32_t frame_pos = 0;
-        uint32_t sl[kMaxRects], sr[kMaxRects], st[kMaxRects], sb[kMaxRects];
-        for (uint32_t i = 0; i < covers * covers; ++i) {
+        uint32_t sl[RECTS], sr[RECTS], st[RECTS], sb[RECTS];
+#pragma unroll
+        for (int i = 0; i < RECTS; ++i) {
             sl[i] = 1;
             sr[i] = 0;
             st[i] = 1;
             sb[i] = 0;
         }
-        for (uint32_t iy = 0; iy < covers; ++iy)
-            for (uint32_t ix = 0; ix < covers; ++ix) {
+#pragma unroll
+        for (int iy = 0; iy < COVERS; ++iy)
+#pragma unroll
+            for (int ix = 0; ix < COVERS; ++ix) {
                 const uint32_t bx = bx_lo + ix, by = by_lo + iy;
                 if (bx > bx_hi || by > by_hi) continue;
                 const uint32_t block = by * a.blocks_x + bx;
@@ -393,29 +397,30 @@ __device__ __forceinline__ void trajectory_search(const GroupCtx& g, const Colla
                 const uint32_t top = clamp_top_left(static_cast<int>(ay) + mvy - a.refine, max_y);
                 const uint32_t bottom = clamp_top_left(static_cast<int>(ay) + mvy + a.refine, max_y);
                 bool contained = false;
-                for (uint32_t i = 0; i < covers * covers; ++i)
+#pragma unroll
+                for (int i = 0; i < RECTS; ++i)
                     contained |= left >= sl[i] && right <= sr[i] && top >= st[i] && bottom <= sb[i];
                 if (!contained) {
                     for (uint32_t cy = top; cy <= bottom; ++cy)
                         for (uint32_t cx = left; cx <= right; ++cx) {
+                            const float d = reduce8(g, column_ssd<C>(anchor, frame, a.width, cx, cy, g.sub)) * scale;
+                            if (!(d < frame_d)) continue;
                             bool skip = false;
-                            for (uint32_t i = 0; i < covers * covers; ++i)
+#pragma unroll
+                            for (int i = 0; i < RECTS; ++i)
                                 skip |= cy >= st[i] && cy <= sb[i] && cx >= sl[i] && cx <= sr[i];
                             const uint32_t packed = pack_pos_t(cx, cy, packed_t);
 #pragma unroll
                             for (int k = 0; k < FIRST; ++k) skip |= grid_pos[k] == packed;
                             if (skip) continue;
-                            const float d = reduce8(g, column_ssd<C>(anchor, frame, a.width, cx, cy, g.sub)) * scale;
-                            if (d < frame_d) {
-                                frame_d = d;
-                                frame_pos = packed;
-                            }
+                            frame_d = d;
+                            frame_pos = packed;
                         }
                 }
-                sl[iy * covers + ix] = left;
-                sr[iy * covers + ix] = right;
-                st[iy * covers + ix] = top;
-                sb[iy * covers + ix] = bottom;
+                sl[iy * COVERS + ix] = left;
+                sr[iy * COVERS + ix] = right;
+                st[iy * COVERS + ix] = top;
+                sb[iy * COVERS + ix] = bottom;
             }
         float carry_d = frame_d;
         uint32_t carry_pos = frame_pos;
@@ -433,7 +438,7 @@ __device__ __forceinline__ void trajectory_search(const GroupCtx& g, const Colla
     }
 }
 
-template <int C, int GF, int VOL = 0>
+template <int C, int GF, int COVERS, int VOL = 0>
 __device__ __forceinline__ void search_volumes(const GroupCtx& g, const CollabLaunch& a, const uint32_t (&member_pos)[MAX_K],
                                                float scale, float (&grid_d)[MAX_K], uint32_t (&grid_pos)[MAX_K]) {
     if constexpr (VOL < MAX_K / GF) {
@@ -454,20 +459,80 @@ __device__ __forceinline__ void search_volumes(const GroupCtx& g, const CollabLa
 #pragma unroll
             for (int c = 0; c < C; ++c)
                 anchor[r * C + c] = __ldg(centre + ((static_cast<size_t>(ay) + r) * a.width + ax + g.sub) * C + c);
-        trajectory_search<C, GF, FIRST + 1>(g, a, anchor, ax, ay, scale, grid_d, grid_pos);
-        search_volumes<C, GF, VOL + 1>(g, a, member_pos, scale, grid_d, grid_pos);
+        trajectory_search<C, GF, FIRST + 1, COVERS>(g, a, anchor, ax, ay, scale, grid_d, grid_pos);
+        search_volumes<C, GF, COVERS, VOL + 1>(g, a, member_pos, scale, grid_d, grid_pos);
     }
 }
 
-template <int C, int GF>
-__global__ void __launch_bounds__(kThreads) collab_kernel(CollabLaunch a) {
-    __shared__ float transpose_buf[kGroups * kRegion];
+// Keyed top-8 insert: the reference visits the window row by row and keeps ties in visiting order
+// (fused/plane_ops.rs:38-53), so its list is the 8 smallest (distance, visiting index) pairs. The
+// search here visits columns, comparing the pair, which keeps exactly the same list.
+__device__ __forceinline__ bool key_less(float d, uint32_t i, float bd, uint32_t bi) {
+    return d < bd || (d == bd && i < bi);
+}
+
+__device__ __forceinline__ void shift_insert8_key(const GroupCtx& g, float& best_d, uint32_t& best_i, float d,
+                                                  uint32_t i) {
+    const float prev_d = __shfl_up_sync(g.mask, best_d, 1, 8);
+    const uint32_t prev_i = __shfl_up_sync(g.mask, best_i, 1, 8);
+    if (key_less(d, i, best_d, best_i)) {
+        if (g.sub == 0 || !key_less(d, i, prev_d, prev_i)) {
+            best_d = d;
+            best_i = i;
+        } else {
+            best_d = prev_d;
+            best_i = prev_i;
+        }
+    }
+}
+
+template <int C>
+__device__ __forceinline__ void load_row(float (&dst)[C], const float* __restrict__ colp, uint32_t row, int width) {
+#pragma unroll
+    for (int c = 0; c < C; ++c) dst[c] = __ldg(colp + static_cast<size_t>(row) * width * C + c);
+}
+
+// The lane's column distance with the window rows held in a ring of 8 registers; PH is the ring
+// phase, so every index is a compile-time constant. Same operation order as column_ssd.
+template <int C, int PH>
+__device__ __forceinline__ float ring_ssd(const float (&ref)[P * C], const float (&ring)[P][C]) {
+    float s = 0.0f;
+#pragma unroll
+    for (int r = 0; r < P; ++r)
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const float d = ref[r * C + c] - ring[(PH + r) & 7][c];
+            s = fmaf(d, d, s);
+        }
+    return s;
+}
+
+template <int C, int PH>
+__device__ __forceinline__ void centre_step(const GroupCtx& g, const float (&cur)[P * C], float (&ring)[P][C],
+                                            const float* __restrict__ colp, int width, uint32_t top, uint32_t j,
+                                            uint32_t col, uint32_t ww, bool self_col, uint32_t self_row, float scale,
+                                            float& best_d, uint32_t& best_i, float& worst_d, uint32_t& worst_i) {
+    load_row<C>(ring[(PH + 7) & 7], colp, top + j + 7, width);
+    float d = reduce8(g, ring_ssd<C, PH>(cur, ring)) * scale;
+    if (self_col && j == self_row) d = kSelfPin;
+    const uint32_t i = j * ww + col;
+    if (d < kUnfilled && key_less(d, i, worst_d, worst_i)) {
+        shift_insert8_key(g, best_d, best_i, d, i);
+        worst_d = __shfl_sync(g.mask, best_d, 7, 8);
+        worst_i = __shfl_sync(g.mask, best_i, 7, 8);
+    }
+}
+
+// Member words per reference patch: 8 packed positions, then k_use | use_grid << 8.
+constexpr int kMemberWords = 9;
+
+template <int C, int GF, int COVERS>
+__global__ void __launch_bounds__(kThreads, 5) collab_search_kernel(CollabLaunch a) {
     const int lane = threadIdx.x & 31;
     const int group = threadIdx.x >> 3;
     GroupCtx g;
     g.sub = threadIdx.x & 7;
     g.mask = 0xFFu << (lane & ~7);
-    float* region = transpose_buf + group * kRegion;
 
     const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
     const uint32_t ix = blockIdx.x * kGroups + group;
@@ -484,36 +549,54 @@ __global__ void __launch_bounds__(kThreads) collab_kernel(CollabLaunch a) {
 #pragma unroll
         for (int c = 0; c < C; ++c) cur[r * C + c] = __ldg(centre + ((static_cast<size_t>(ry) + r) * a.width + rx + g.sub) * C + c);
 
-    // Centre search (fused/centre.rs:213-258), row by row over the clipped window.
-    float best_d = kUnfilled;
-    uint32_t best_pos = 0;
-    float worst = kUnfilled;
+    // Centre search (fused/centre.rs:213-258) over the clipped window, column by column with the
+    // column's rows sliding through registers: one load per candidate and lane.
     const uint32_t left = clamp_top_left(static_cast<int>(rx) - a.spatial_radius, max_x);
     const uint32_t right = clamp_top_left(static_cast<int>(rx) + a.spatial_radius, max_x);
     const uint32_t top = clamp_top_left(static_cast<int>(ry) - a.spatial_radius, max_y);
     const uint32_t bottom = clamp_top_left(static_cast<int>(ry) + a.spatial_radius, max_y);
-    for (uint32_t cy = top; cy <= bottom; ++cy)
-        for (uint32_t cx = left; cx <= right; ++cx) {
-            float d = reduce8(g, column_ssd<C>(cur, centre, a.width, cx, cy, g.sub)) * scale;
-            if (cx == rx && cy == ry) d = kSelfPin;
-            if (d < worst) {
-                shift_insert8(g, best_d, best_pos, d, pack_pos_t(cx, cy, 0));
-                worst = __shfl_sync(g.mask, best_d, 7, 8);
-            }
+    const uint32_t ww = right - left + 1, hh = bottom - top + 1;
+    float best_d = kUnfilled, worst_d = kUnfilled;
+    uint32_t best_i = 0xFFFFFFFFu, worst_i = 0xFFFFFFFFu;
+    for (uint32_t cx = left; cx <= right; ++cx) {
+        const float* colp = centre + static_cast<size_t>(cx + g.sub) * C;
+        const bool self_col = cx == rx;
+        const uint32_t col = cx - left, self_row = ry - top;
+        float ring[P][C];
+#pragma unroll
+        for (int r = 0; r < P - 1; ++r) load_row<C>(ring[r], colp, top + r, a.width);
+        for (uint32_t jb = 0; jb < hh; jb += 8) {
+#define AVD_CENTRE_STEP(PH)                                                                                      \
+    if (jb + PH < hh)                                                                                            \
+        centre_step<C, PH>(g, cur, ring, colp, a.width, top, jb + PH, col, ww, self_col, self_row, scale, best_d, \
+                           best_i, worst_d, worst_i);
+            AVD_CENTRE_STEP(0)
+            AVD_CENTRE_STEP(1)
+            AVD_CENTRE_STEP(2)
+            AVD_CENTRE_STEP(3)
+            AVD_CENTRE_STEP(4)
+            AVD_CENTRE_STEP(5)
+            AVD_CENTRE_STEP(6)
+            AVD_CENTRE_STEP(7)
+#undef AVD_CENTRE_STEP
         }
-    const uint32_t n_live = (right - left + 1) * (bottom - top + 1);
+    }
+    const uint32_t n_live = ww * hh;
     int k_use = 1;
     while (static_cast<uint32_t>(k_use * 2) <= n_live && k_use * 2 <= a.k_max) k_use *= 2;
     uint32_t member_pos[MAX_K];
 #pragma unroll
-    for (int m = 0; m < MAX_K; ++m) member_pos[m] = __shfl_sync(g.mask, best_pos, m, 8);
+    for (int m = 0; m < MAX_K; ++m) {
+        const uint32_t i = __shfl_sync(g.mask, best_i, m, 8);
+        member_pos[m] = i == 0xFFFFFFFFu ? 0u : pack_pos_t(left + i % ww, top + i / ww, 0);
+    }
 
     bool use_grid = false;
     if constexpr (GF > 1) {
         if (a.k_max == MAX_K) {
             float grid_d[MAX_K];
             uint32_t grid_pos[MAX_K];
-            search_volumes<C, GF>(g, a, member_pos, scale, grid_d, grid_pos);
+            search_volumes<C, GF, COVERS>(g, a, member_pos, scale, grid_d, grid_pos);
             use_grid = k_use == MAX_K;
 #pragma unroll
             for (int v = 0; v < MAX_K / GF; ++v) use_grid = use_grid && grid_d[v * GF + GF - 1] < kUnfilled;
@@ -524,6 +607,43 @@ __global__ void __launch_bounds__(kThreads) collab_kernel(CollabLaunch a) {
             }
         }
     }
+    uint32_t* words = a.members + static_cast<size_t>(iy * refs_x + ix) * kMemberWords;
+    uint32_t mine = member_pos[0];
+#pragma unroll
+    for (int m = 1; m < MAX_K; ++m) mine = g.sub == m ? member_pos[m] : mine;
+    words[g.sub] = mine;
+    if (g.sub == 0) words[MAX_K] = static_cast<uint32_t>(k_use) | (use_grid ? 0x100u : 0u);
+}
+
+template <int C, int GF>
+__global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch a) {
+    __shared__ float transpose_buf[kGroups * kRegion];
+    const int lane = threadIdx.x & 31;
+    const int group = threadIdx.x >> 3;
+    GroupCtx g;
+    g.sub = threadIdx.x & 7;
+    g.mask = 0xFFu << (lane & ~7);
+    float* region = transpose_buf + group * kRegion;
+
+    const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
+    const uint32_t ix = blockIdx.x * kGroups + group;
+    if (ix >= refs_x) return;
+    const uint32_t iy = blockIdx.y;
+    const uint32_t max_x = a.width - P, max_y = a.height - P;
+    const uint32_t rx = min(ix * STEP, max_x), ry = min(iy * STEP, max_y);
+    const float* centre = a.ring + static_cast<size_t>(a.centre_slot) * a.frame_elems;
+    float cur[P * C];
+#pragma unroll
+    for (int r = 0; r < P; ++r)
+#pragma unroll
+        for (int c = 0; c < C; ++c) cur[r * C + c] = __ldg(centre + ((static_cast<size_t>(ry) + r) * a.width + rx + g.sub) * C + c);
+    const uint32_t* words = a.members + static_cast<size_t>(iy * refs_x + ix) * kMemberWords;
+    uint32_t member_pos[MAX_K];
+#pragma unroll
+    for (int m = 0; m < MAX_K; ++m) member_pos[m] = __ldg(words + m);
+    const uint32_t meta = __ldg(words + MAX_K);
+    int k_use = static_cast<int>(meta & 0xFFu);
+    const bool use_grid = (meta & 0x100u) != 0;
 
     // filter_group (fused/mod.rs:559-850).
     int member_slot[MAX_K];
@@ -651,13 +771,25 @@ __global__ void __launch_bounds__(kThreads) collab_kernel(CollabLaunch a) {
     }
 }
 
-template <int C, int GF>
-cudaError_t launch_cg(const CollabLaunch& a, cudaStream_t stream) {
+template <int C, int GF, int COVERS>
+cudaError_t launch_cgc(const CollabLaunch& a, cudaStream_t stream) {
     const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
     const uint32_t refs_y = (a.height - P + STEP - 1) / STEP + 1;
     dim3 grid((refs_x + kGroups - 1) / kGroups, refs_y);
-    collab_kernel<C, GF><<<grid, kThreads, 0, stream>>>(a);
+    collab_search_kernel<C, GF, COVERS><<<grid, kThreads, 0, stream>>>(a);
+    collab_filter_kernel<C, GF><<<grid, kThreads, 0, stream>>>(a);
     return cudaGetLastError();
+}
+
+template <int C, int GF>
+cudaError_t launch_cg(const CollabLaunch& a, cudaStream_t stream) {
+    if (GF == 1) return launch_cgc<C, GF, 1>(a, stream);  // no volumes: the walk never runs
+    switch ((a.blksize + a.blk_step - 1) / a.blk_step) {
+        case 1: return launch_cgc<C, GF, 1>(a, stream);
+        case 2: return launch_cgc<C, GF, 2>(a, stream);
+        case 3: return launch_cgc<C, GF, 3>(a, stream);
+        default: return launch_cgc<C, GF, 4>(a, stream);
+    }
 }
 
 cudaError_t upload_taps() {
@@ -676,7 +808,14 @@ cudaError_t upload_taps() {
 
 }  // namespace
 
+size_t collab_member_words(int width, int height) {
+    if (width < P || height < P) return 0;
+    const size_t rx = (width - P + STEP - 1) / STEP + 1, ry = (height - P + STEP - 1) / STEP + 1;
+    return rx * ry * kMemberWords;
+}
+
 cudaError_t launch_collab(const CollabLaunch& a, cudaStream_t stream) {
+    if (!a.members) return cudaErrorInvalidValue;
     if (a.width < P || a.height < P || a.k_max < 1 || a.k_max > MAX_K || a.radius < 0 || a.radius > 8)
         return cudaErrorInvalidValue;
     if ((a.blksize + a.blk_step - 1) / max(a.blk_step, 1) > 4 || a.blk_step < 1) return cudaErrorInvalidValue;

@@ -54,6 +54,10 @@ void avd_kaiser_window(float beta, float* out8) {
     }
 }
 
+uint64_t avd_collab_member_bytes(uint32_t width, uint32_t height) {
+    return avd::collab_member_words(static_cast<int>(width), static_cast<int>(height)) * sizeof(uint32_t);
+}
+
 float avd_cross_frame_accum_scale(uint32_t spatial_radius, uint32_t temporal_radius) {
     const uint32_t refs_per_axis = (7 + 2 * spatial_radius) / 4 + 1;
     const double contribs = static_cast<double>(refs_per_axis) * refs_per_axis * 8.0;
@@ -63,7 +67,8 @@ float avd_cross_frame_accum_scale(uint32_t spatial_radius, uint32_t temporal_rad
 }
 
 AvdStatus avd_collab_pass(const AvdCollabPass* p, void* stream) {
-    if (!p || !p->ring || !p->accum || !p->wsum || !p->group_weight || !p->noise || !p->dct_profile || !p->kaiser)
+    if (!p || !p->ring || !p->accum || !p->wsum || !p->group_weight || !p->noise || !p->dct_profile || !p->kaiser ||
+        !p->members)
         return AVD_ERR_NULL_ARG;
     if (p->width < 8 || p->height < 8 || (p->channels != 1 && p->channels != 2) || p->k_max < 1 || p->k_max > 8 ||
         p->radius > 8 || p->spatial_radius > 16 || p->refine > 4 || p->blk_step == 0 ||
@@ -92,6 +97,7 @@ AvdStatus avd_collab_pass(const AvdCollabPass* p, void* stream) {
     a.accum = reinterpret_cast<int32_t*>(p->accum);
     a.wsum = reinterpret_cast<int32_t*>(p->wsum);
     a.group_weight = reinterpret_cast<float*>(p->group_weight);
+    a.members = reinterpret_cast<uint32_t*>(p->members);
     a.c_min = p->c_min;
     a.lambda_ht = p->lambda_ht;
     a.accum_scale = p->accum_scale;

@@ -67,6 +67,7 @@ struct CollabLaunch {
     int32_t* accum;                 // slots x pixels x channels
     int32_t* wsum;                  // slots x pixels
     float* group_weight;            // refs
+    uint32_t* members;              // scratch: collab_member_words(width, height) words
     float c_min, lambda_ht, accum_scale, pool_ratio;
     int pooled;
     int radius, refine, spatial_radius, k_max;
@@ -74,6 +75,8 @@ struct CollabLaunch {
 };
 
 cudaError_t launch_collab(const CollabLaunch& args, cudaStream_t stream);
+// The scratch words between the search and filter launches: 9 per reference patch.
+size_t collab_member_words(int width, int height);
 
 // collab/kernels/aggregate.rs:240-290 (`collab_normalise`): one region's accum * 5 / wsum (accum
 // itself where wsum is 0) into `out`, then the region zeroed.

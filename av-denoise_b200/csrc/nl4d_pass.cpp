@@ -211,6 +211,8 @@ class Nl4dPass final : public Pass {
         if ((e = wsum_.alloc(pixels() * t * sizeof(int32_t))) != cudaSuccess) return gpu_failure("weight ring", e);
         const size_t refs = static_cast<size_t>((width_ - kPatch + 3) / 4 + 1) * ((height_ - kPatch + 3) / 4 + 1);
         if ((e = group_weight_.alloc(refs * sizeof(float))) != cudaSuccess) return gpu_failure("group weights", e);
+        const size_t member_words = collab_member_words(static_cast<int>(width_), static_cast<int>(height_));
+        if ((e = members_.alloc(member_words * sizeof(uint32_t))) != cudaSuccess) return gpu_failure("group members", e);
         for (auto& o : outputs_)
             if ((e = o.alloc(fe * sizeof(float))) != cudaSuccess) return gpu_failure("output slot", e);
 
@@ -403,6 +405,7 @@ class Nl4dPass final : public Pass {
         a.accum = accum_.as<int32_t>();
         a.wsum = wsum_.as<int32_t>();
         a.group_weight = group_weight_.as<float>();
+        a.members = members_.as<uint32_t>();
         a.c_min = opts_.c_min;
         a.lambda_ht = lambda_;
         a.accum_scale = accum_scale_;
@@ -513,7 +516,7 @@ class Nl4dPass final : public Pass {
     float lambda_ = 0.0f, pool_ratio_ = 0.0f, accum_scale_ = 0.0f, thsad_ = 0.0f;
     int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2, conf_stride_ = 1;
 
-    DeviceBuffer ring_, pyramid_, mv_, conf_, accum_, wsum_, group_weight_, tables_, slot_tables_;
+    DeviceBuffer ring_, pyramid_, mv_, conf_, accum_, wsum_, group_weight_, members_, tables_, slot_tables_;
     DeviceBuffer outputs_[2];
 
     size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;

@@ -453,9 +453,60 @@ def run_once() -> None:
     print("one luma NLM launch done")
 
 
+def run_nl4d(pushes: int, size: str) -> None:
+    """The NL4D engine on one plane of synthetic content with a pinned sigma and Direct motion:
+    1920x1080 u8 or 3840x2160 10-bit luma, d=2, spatial radius 9, defaults otherwise. Prints the
+    device time of every push (CUDA events on the engine's stream) and the steady-state median as
+    one JSON line. The first 2d+1 pushes fill the ring (the last of them runs d+1 passes)."""
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import synth
+
+    w, h, depth = (1920, 1080, 8) if size == "1080" else (3840, 2160, 10)
+    d = 2
+    fmt = avd.SampleFormat.u8() if depth == 8 else avd.SampleFormat.u16(depth)
+    o = avd.Nl4dOptions(sigma=10.0 / 255, temporal_radius=d, spatial_radius=9,
+                        motion=avd.MotionSearch(estimation=avd.MotionEstimation.DIRECT))
+    eng = avd.build_engine(avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt)))
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    clip = synth.make_clip(w, h, 4, depth=depth, chroma="gray", sigma_luma=10.0, global_motion=2, sprites=3,
+                           sprite_size=200, seed=1)
+    dt = np.uint8 if depth == 8 else np.uint16
+    bufs = []
+    for f in clip:
+        flat = f[0].reshape(-1).astype(dt)
+        spw = 4 if depth == 8 else 2
+        bufs.append(torch.from_numpy(np.concatenate([flat, np.zeros((-flat.size) % spw, dt)]).view(np.int32)).cuda())
+    out = torch.zeros_like(bufs[0])
+    times = []
+    for i in range(pushes):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ready = eng.push([avd.DevicePlane.from_tensor(bufs[i % 4], w, h)])
+        for _ in range(ready):
+            eng.emit_into([avd.DevicePlane.from_tensor(out, w, h)])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    eng.close()
+    steady = times[2 * d + 1:]
+    ms = float(np.median(steady)) if steady else float("nan")
+    print(json.dumps({"workload": f"NL4D {w}x{h} luma u{depth} d=2 spatial_radius 9 pinned sigma, Direct motion",
+                      "ms_per_frame": round(ms, 4), "frames_per_s": round(1000.0 / ms, 2) if steady else None,
+                      "push_ms": [round(t, 3) for t in times]}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--once", action="store_true", help="run one luma NLM launch (profiling case) and exit")
+    ap.add_argument("--nl4d", type=int, default=0, metavar="PUSHES",
+                    help="time PUSHES pushes of the NL4D engine (secondary workload) and exit")
+    ap.add_argument("--nl4d-size", default="1080", choices=["1080", "2160"])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -465,6 +516,8 @@ def main() -> None:
     args = ap.parse_args()
     if args.once:
         run_once()
+    elif args.nl4d:
+        run_nl4d(args.nl4d, args.nl4d_size)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -358,6 +358,7 @@ typedef struct AvdCollabPass {
     uint64_t accum;           /* i32, slots x height x width x channels, accumulated into */
     uint64_t wsum;            /* i32, slots x height x width, accumulated into */
     uint64_t group_weight;    /* f32 per reference patch, written */
+    uint64_t members;         /* scratch of avd_collab_member_bytes(width, height) bytes */
     uint32_t width, height, channels, centre_slot;
     uint32_t sigma_word, weight_scale_word, curve_valid_word; /* indices into `noise` */
     uint32_t radius, refine, spatial_radius, k_max;
@@ -369,6 +370,11 @@ typedef struct AvdCollabPass {
 /* av-denoise-core/src/collab/kernels/fused/mod.rs:170 (`collab_fused`): one pass, queued on
  * `stream`. Adds into `accum`/`wsum` (integer adds: the result does not depend on scheduling). */
 AVD_API AvdStatus avd_collab_pass(const AvdCollabPass* pass, void* stream);
+
+/* The scratch bytes one collab pass over a width x height plane needs between its group search
+ * and its filter (the reference's split search profile hands the same member words over,
+ * av-denoise-core/src/collab/kernels/fused/split.rs). */
+AVD_API uint64_t avd_collab_member_bytes(uint32_t width, uint32_t height);
 
 /* av-denoise-core/src/collab/kernels/transforms.rs:196-221 (`dct_noise_profile`). */
 AVD_API void avd_dct_noise_profile(float rho, float* out8);

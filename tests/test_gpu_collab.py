@@ -50,6 +50,7 @@ def run_gpu(case: dict):
         "kaiser": t(kaiser, np.float32),
         "accum": torch.zeros(w * h * ch * frames, dtype=torch.int32, device="cuda"),
         "wsum": torch.zeros(w * h * frames, dtype=torch.int32, device="cuda"),
+        "members": torch.zeros(lib.avd_collab_member_bytes(w, h) // 4, dtype=torch.int32, device="cuda"),
         "gw": torch.zeros(((w - 8 + 3) // 4 + 1) * ((h - 8 + 3) // 4 + 1), dtype=torch.float32, device="cuda"),
     }
     p = _abi.AvdCollabPass()
@@ -57,6 +58,7 @@ def run_gpu(case: dict):
     p.neighbour_slots, p.noise, p.noise_curve = dev["slots"].data_ptr(), dev["noise"].data_ptr(), dev["curve"].data_ptr()
     p.dct_profile, p.kaiser = dev["prof"].data_ptr(), dev["kaiser"].data_ptr()
     p.accum, p.wsum, p.group_weight = dev["accum"].data_ptr(), dev["wsum"].data_ptr(), dev["gw"].data_ptr()
+    p.members = dev["members"].data_ptr()
     p.width, p.height, p.channels, p.centre_slot = w, h, ch, case.get("centre_slot", 0)
     p.sigma_word, p.weight_scale_word, p.curve_valid_word = 0, 2, 3
     p.radius, p.refine, p.spatial_radius, p.k_max = radius, case.get("refine", 0), sr, case.get("k_max", 8)
