@@ -229,8 +229,180 @@ __global__ void __launch_bounds__(320) fine_kernel(SearchArgs a) {
     }
 }
 
+// Register-blocked search for the common block sizes: one warp per (block, neighbour), several
+// blocks per CTA. Each work item is one candidate row and three adjacent offsets along it; per
+// block row it holds BLK + 2 window values in registers and scores the three offsets from them,
+// so a SAD term costs about two thirds of a shared load instead of two. Every SAD is still the
+// sequential row-major sum, so the vectors are the generic kernels' bit for bit.
+template <int BLK, int R>
+struct Blocked {
+    static constexpr int kSide = 2 * R + 1;
+    static constexpr int kGroups = (kSide + 2) / 3;
+    static constexpr int kItems = kSide * kGroups;
+    static constexpr int kRows = BLK + 2 * R;
+    static constexpr int kReach = kGroups * 3 + BLK - 1;                 // columns the last group reads
+    static constexpr int kStride = (kReach > kRows ? kReach : kRows) | 1;  // odd: spreads the banks
+    static constexpr int kWarps = BLK >= 32 ? 2 : 4;
+    static constexpr int kWindow = kStride * kRows;
+};
+
+template <int BLK, int R>
+__device__ __forceinline__ void blocked_window(const SearchLevel& L, int64_t centre_base, int64_t nbr_base, int ox,
+                                               int oy, int cdx, int cdy, float* centre_tile, float* window,
+                                               float* sads, int lane, unsigned long long* best_key) {
+    using B = Blocked<BLK, R>;
+    for (int i = lane; i < BLK * BLK; i += 32) {
+        const int py = i / BLK, px = i % BLK;
+        centre_tile[i] = L.pyramid[centre_base + static_cast<int64_t>(clamp_to(oy + py, L.height)) * L.width +
+                                   clamp_to(ox + px, L.width)];
+    }
+    const int wx0 = ox + cdx - R, wy0 = oy + cdy - R;
+    for (int i = lane; i < B::kWindow; i += 32) {
+        const int wy = i / B::kStride, wx = i % B::kStride;
+        window[i] = L.pyramid[nbr_base + static_cast<int64_t>(clamp_to(wy0 + wy, L.height)) * L.width +
+                              clamp_to(wx0 + wx, L.width)];
+    }
+    __syncwarp();
+    for (int item = lane; item < B::kItems; item += 32) {
+        const int dy = item / B::kGroups, dx0 = (item % B::kGroups) * 3;
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+        for (int iy = 0; iy < BLK; ++iy) {
+            const float* wrow = window + (iy + dy) * B::kStride + dx0;
+            const float* crow = centre_tile + iy * BLK;
+            float w[BLK + 2];
+#pragma unroll
+            for (int k = 0; k < BLK + 2; ++k) w[k] = wrow[k];
+#pragma unroll
+            for (int ix = 0; ix < BLK; ++ix) {
+                const float c = crow[ix];
+                s0 = __fadd_rn(s0, fabsf(__fsub_rn(c, w[ix])));
+                s1 = __fadd_rn(s1, fabsf(__fsub_rn(c, w[ix + 1])));
+                s2 = __fadd_rn(s2, fabsf(__fsub_rn(c, w[ix + 2])));
+            }
+        }
+        const float part[3] = {s0, s1, s2};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (dx0 + k < B::kSide) sads[dy * B::kSide + dx0 + k] = part[k];
+    }
+    __syncwarp();
+    unsigned long long key = ~0ull;
+    for (int i = lane; i < B::kSide * B::kSide; i += 32) {
+        const float v = sads[i];
+        if (v < kNoSad) {
+            const unsigned long long k = (static_cast<unsigned long long>(__float_as_uint(v)) << 32) | static_cast<unsigned>(i);
+            key = k < key ? k : key;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other < key ? other : key;
+    }
+    *best_key = key;
+}
+
+template <int BLK, int R>
+__device__ __forceinline__ void blocked_pick(const float* sads, unsigned long long key, int cdx, int cdy, int* out_dx,
+                                             int* out_dy, float* out_sad) {
+    using B = Blocked<BLK, R>;
+    float best_sad = kNoSad;
+    int bdx = cdx, bdy = cdy;
+    if (key != ~0ull) {
+        const int idx = static_cast<int>(key & 0xffffffffu);
+        best_sad = sads[idx];
+        bdx = cdx + idx % B::kSide - R;
+        bdy = cdy + idx / B::kSide - R;
+    }
+    const float centre_sad = sads[R * B::kSide + R];
+    if (centre_sad <= best_sad) {
+        best_sad = centre_sad;
+        bdx = cdx;
+        bdy = cdy;
+    }
+    *out_dx = bdx;
+    *out_dy = bdy;
+    *out_sad = best_sad;
+}
+
+template <int BLK, int R, bool COARSE>
+__global__ void __launch_bounds__(Blocked<BLK, R>::kWarps * 32) blocked_kernel(SearchArgs a) {
+    using B = Blocked<BLK, R>;
+    __shared__ float centre_tiles[B::kWarps][BLK * BLK];
+    __shared__ float windows[B::kWarps][B::kWindow];
+    __shared__ float sad_buf[B::kWarps][B::kSide * B::kSide];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bx = blockIdx.x * B::kWarps + warp, by = blockIdx.y, n = blockIdx.z;
+    if (bx >= a.L.blocks_x) return;  // the whole warp leaves; only warp-scoped syncs follow
+    const uint32_t nbr_slot = a.neighbour_slots ? a.neighbour_slots[n] : a.slots[n];
+    const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
+    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(nbr_slot) * a.L.slot_pixels;
+    const int ox = bx * a.L.step, oy = by * a.L.step;
+    int cdx = 0, cdy = 0;
+    int32_t* mv_fine = nullptr;
+    if (!COARSE) {
+        mv_fine = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
+        if (a.use_seed) {
+            cdx = mv_fine[0];
+            cdy = mv_fine[1];
+        }
+    }
+    unsigned long long key;
+    blocked_window<BLK, R>(a.L, centre_base, nbr_base, ox, oy, cdx, cdy, centre_tiles[warp], windows[warp],
+                           sad_buf[warp], lane, &key);
+    if (lane != 0) return;
+    int dx, dy;
+    float sad;
+    blocked_pick<BLK, R>(sad_buf[warp], key, cdx, cdy, &dx, &dy, &sad);
+    if (COARSE) {
+        const int s = a.L.step * a.level_scale;
+        const int c0 = min(bx * s / a.fine_step, a.fine_blocks_x);
+        const int c1 = bx == a.L.blocks_x - 1 ? a.fine_blocks_x : min((bx + 1) * s / a.fine_step, a.fine_blocks_x);
+        const int r0 = min(by * s / a.fine_step, a.fine_blocks_y);
+        const int r1 = by == a.L.blocks_y - 1 ? a.fine_blocks_y : min((by + 1) * s / a.fine_step, a.fine_blocks_y);
+        int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride;
+        for (int r = r0; r < r1; ++r)
+            for (int c = c0; c < c1; ++c) {
+                mv[(r * a.fine_blocks_x + c) * 2] = dx * a.level_scale;
+                mv[(r * a.fine_blocks_x + c) * 2 + 1] = dy * a.level_scale;
+            }
+        return;
+    }
+    mv_fine[0] = dx;
+    mv_fine[1] = dy;
+    if (a.confidence) {
+        const float floor = a.noise[a.sad_floor_word];
+        float excess = __fsub_rn(sad, floor);
+        if (excess < 0.0f) excess = 0.0f;
+        const float t2 = __fmul_rn(a.thsad, a.thsad);
+        const float e2 = __fmul_rn(excess, excess);
+        float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
+        if (c < 0.0f) c = 0.0f;
+        a.confidence[static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx] = c;
+    }
+}
+
+template <int BLK, int R>
+cudaError_t launch_blocked(bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
+    using B = Blocked<BLK, R>;
+    dim3 g((grid.x + B::kWarps - 1) / B::kWarps, grid.y, grid.z);
+    if (coarse)
+        blocked_kernel<BLK, R, true><<<g, B::kWarps * 32, 0, s>>>(a);
+    else
+        blocked_kernel<BLK, R, false><<<g, B::kWarps * 32, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <int R>
 cudaError_t launch_search(bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
+    if (R >= 1) {
+        switch (a.L.blksize) {
+            case 8: return launch_blocked<8, R>(coarse, a, grid, s);
+            case 16: return launch_blocked<16, R>(coarse, a, grid, s);
+            case 32: return launch_blocked<32, R>(coarse, a, grid, s);
+            default: break;
+        }
+    }
     constexpr int kCand = (2 * R + 1) * (2 * R + 1);
     const int threads = ((kCand + 31) / 32) * 32;
     if (coarse)
