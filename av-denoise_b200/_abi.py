@@ -207,6 +207,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_motion_search": (C.c_int, [_P(AvdMotionPass), C.c_void_p]),
     "avd_sad_noise_floor": (f32, [u32, f32]),
     "avd_thsad": (f32, [u32, f32]),
+    "avd_immerkaer_partials_len": (u64, [u32, u32]),
+    "avd_immerkaer": (C.c_int, [u64, u32, u32, u32, u64, u64, u64, C.c_void_p]),
     "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,
                                        _P(AvdPlane), C.c_size_t, _P(AvdPlane), C.c_size_t, C.c_void_p]),
 }

@@ -106,4 +106,11 @@ cudaError_t launch_pyramid_build(const float* ring, int channels, int width, int
                                  int ring_slot, int levels, float* pyramid, int pyramid_slot, cudaStream_t stream);
 cudaError_t launch_motion_search(const MotionLaunch& args, cudaStream_t stream);
 
+// Immerkær spatial noise estimate (immerkaer.cu) of one f32 frame (`channels` interleaved):
+// per 32x8 block partials (2 lanes each), optional frame totals (2 floats) and optional per-channel
+// lower quartile of the block sigmas (2 floats; unused channels 0). `scale` is sqrt(pi / 2) in f32.
+size_t immerkaer_partials_len(int width, int height);
+cudaError_t launch_immerkaer(const float* frame, int channels, int width, int height, float scale, float* partials,
+                             float* results, float* sigma_low, cudaStream_t stream);
+
 }  // namespace avd

@@ -1,5 +1,5 @@
-// Host side of the motion search entry points: argument checks, then the pyramid and block-match
-// launches of motion.cu.
+// Host side of the motion search and noise estimator entry points: argument checks, then the
+// launches of motion.cu and immerkaer.cu.
 
 #include <cuda_runtime.h>
 
@@ -95,6 +95,26 @@ float avd_sad_noise_floor(uint32_t blksize, float sigma) {
 float avd_thsad(uint32_t blksize, float thsad_scale) {
     const float area = static_cast<float>(blksize * blksize);
     return thsad_scale * area * 0.02f;
+}
+
+uint64_t avd_immerkaer_partials_len(uint32_t width, uint32_t height) {
+    return avd::immerkaer_partials_len(static_cast<int>(width), static_cast<int>(height));
+}
+
+// noise/spatial.rs:142-144: the scale is the f32 square root of the f32 pi / 2.
+AvdStatus avd_immerkaer(uint64_t frame, uint32_t channels, uint32_t width, uint32_t height, uint64_t partials,
+                        uint64_t results, uint64_t sigma_low, void* stream) {
+    if (!frame || !partials) return fail(AVD_ERR_NULL_ARG, "immerkaer: null buffer");
+    if (channels < 1 || channels > 2 || width == 0 || height == 0)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "immerkaer: bad geometry");
+    const volatile float half_pi = 1.57079632679489661923f;
+    const float scale = std::sqrt(static_cast<float>(half_pi));
+    cudaError_t e = avd::launch_immerkaer(reinterpret_cast<const float*>(frame), static_cast<int>(channels),
+                                          static_cast<int>(width), static_cast<int>(height), scale,
+                                          reinterpret_cast<float*>(partials), reinterpret_cast<float*>(results),
+                                          reinterpret_cast<float*>(sigma_low), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("immerkaer launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
 }
 
 }  // extern "C"

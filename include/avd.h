@@ -421,6 +421,21 @@ AVD_API float avd_sad_noise_floor(uint32_t blksize, float sigma);
 /* av-denoise-core/src/motion/confidence.rs:27-30 (`thsad`). */
 AVD_API float avd_thsad(uint32_t blksize, float thsad_scale);
 
+/* ---- noise estimator kernel-level entry points --------------------------------------------- */
+
+/* The floats of one frame's Immerkær partials: 2 lanes per 32x8 block
+ * (av-denoise-core/src/noise/spatial.rs:44-47, `partials_len`). */
+AVD_API uint64_t avd_immerkaer_partials_len(uint32_t width, uint32_t height);
+
+/* The Immerkær spatial estimate of one f32 frame (`channels` 1 or 2 interleaved, as a ring slot holds
+ * it): av-denoise-core/src/noise/spatial.rs:98-138 (`run_noise_estimate`: `nlm_noise_partial` into
+ * `partials`, `nlm_noise_reduce` into `results`, 2 floats) and the reading's per-channel lower
+ * quartile of the block sigmas (noise/kernels/sample.rs:181-203, 660-682) into `sigma_low`
+ * (2 floats, 0 for an unused channel). `results` and `sigma_low` may be 0 to skip them. Queued on
+ * `stream`. */
+AVD_API AvdStatus avd_immerkaer(uint64_t frame, uint32_t channels, uint32_t width, uint32_t height, uint64_t partials,
+                                uint64_t results, uint64_t sigma_low, void* stream);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 
 /* No counterpart in the reference. One fast-variant NLMeans output frame for callers that cannot

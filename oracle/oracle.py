@@ -452,3 +452,37 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     for logical in range(last_real + 1 - emit, last_real + 1):
         outs.append(read_region(phys(logical)))
     return outs
+
+
+# ---- Immerkær spatial noise estimate (noise_oracle.cpp) ------------------------------------------
+
+def immerkaer_scale() -> float:
+    """noise/spatial.rs:142-144: sqrt(pi / 2) in f32."""
+    return float(np.sqrt(np.float32(np.pi / 2)))
+
+
+def immerkaer(frame: np.ndarray, channels: int, width: int, height: int):
+    """Returns (partials, totals[2], sigma_low[2]) of one (H, W, C) f32 frame."""
+    l = lib()
+    l.orc_immerkaer_partials_len.argtypes = [C.c_int, C.c_int]
+    l.orc_immerkaer_partials_len.restype = C.c_int64
+    l.orc_immerkaer_partials.argtypes = [_fp, C.c_int, C.c_int, C.c_int, _fp]
+    l.orc_immerkaer_totals.argtypes = [_fp, C.c_int, _fp]
+    l.orc_immerkaer_sigma_low.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_float, _fp]
+    fr = np.ascontiguousarray(frame, np.float32)
+    partials = np.zeros(l.orc_immerkaer_partials_len(width, height), np.float32)
+    l.orc_immerkaer_partials(_f(fr), channels, width, height, _f(partials))
+    totals = np.zeros(2, np.float32)
+    l.orc_immerkaer_totals(_f(partials), partials.size // 2, _f(totals))
+    low = np.zeros(2, np.float32)
+    l.orc_immerkaer_sigma_low(_f(partials), channels, width, height, immerkaer_scale(), _f(low))
+    return partials, totals, low
+
+
+def immerkaer_sigma_low_from_partials(partials: np.ndarray, channels: int, width: int, height: int) -> np.ndarray:
+    l = lib()
+    l.orc_immerkaer_sigma_low.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_float, _fp]
+    low = np.zeros(2, np.float32)
+    l.orc_immerkaer_sigma_low(_f(np.ascontiguousarray(partials, np.float32)), channels, width, height,
+                              immerkaer_scale(), _f(low))
+    return low
