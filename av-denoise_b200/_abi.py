@@ -165,6 +165,13 @@ class AvdMotionPass(C.Structure):
                [("thsad", f32)]
 
 
+class AvdNlmBackward(C.Structure):
+    _fields_ = [(n, u64) for n in ("window", "grad_out", "grad_window", "grad_strength", "scratch")] + \
+               [(n, u32) for n in ("width", "height", "channels", "temporal_radius", "search_radius",
+                                   "patch_radius")] + \
+               [(n, f32) for n in ("strength", "self_weight", "pair_offset", "spatial_offset")]
+
+
 _P = C.POINTER
 _E = C.c_void_p  # AvdEngine*
 
@@ -209,6 +216,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_thsad": (f32, [u32, f32]),
     "avd_immerkaer_partials_len": (u64, [u32, u32]),
     "avd_immerkaer": (C.c_int, [u64, u32, u32, u32, u64, u64, u64, C.c_void_p]),
+    "avd_nlm_backward_scratch_bytes": (u64, [u32, u32]),
+    "avd_nlm_backward": (C.c_int, [_P(AvdNlmBackward), C.c_void_p]),
     "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,
                                        _P(AvdPlane), C.c_size_t, _P(AvdPlane), C.c_size_t, C.c_void_p]),
 }

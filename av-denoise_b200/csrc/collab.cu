@@ -65,23 +65,6 @@ __device__ __forceinline__ uint32_t clamp_top_left(int v, uint32_t max_pos) {
     return v < 0 ? 0u : (v > static_cast<int>(max_pos) ? max_pos : static_cast<uint32_t>(v));
 }
 
-// fused/plane_ops.rs:38-53: insert into the group's sorted top-8 (one slot per lane); a tie never
-// displaces an incumbent.
-__device__ __forceinline__ void shift_insert8(const GroupCtx& g, float& best_d, uint32_t& best_pos, float d,
-                                              uint32_t packed) {
-    float prev_d = __shfl_up_sync(g.mask, best_d, 1, 8);
-    uint32_t prev_pos = __shfl_up_sync(g.mask, best_pos, 1, 8);
-    if (d < best_d) {
-        if (g.sub == 0 || d >= prev_d) {
-            best_d = d;
-            best_pos = packed;
-        } else {
-            best_d = prev_d;
-            best_pos = prev_pos;
-        }
-    }
-}
-
 // The lane's share of the distance from `ref` (its 8 x C column) to the candidate at (x, y).
 template <int C>
 __device__ __forceinline__ float column_ssd(const float (&ref)[P * C], const float* __restrict__ frame, int width,

@@ -113,4 +113,18 @@ size_t immerkaer_partials_len(int width, int height);
 cudaError_t launch_immerkaer(const float* frame, int channels, int width, int height, float scale, float* partials,
                              float* results, float* sigma_low, cudaStream_t stream);
 
+// Adjoint of one windowed NLMeans frame (nlm_backward.cu).
+struct NlmBackwardLaunch {
+    const float* window;    // (2d+1) frames of width*height*channels f32, oldest first
+    const float* grad_out;  // width*height*channels
+    float* grad_window;     // like window; overwritten
+    float* grad_strength;   // 1 float; overwritten
+    float* scratch;         // nlm_backward_scratch_floats(width, height)
+    int width, height, channels, temporal_radius, search_radius, patch_radius;
+    float strength, h2, wref, pair_offset, spatial_offset;
+};
+size_t nlm_backward_scratch_floats(int width, int height);
+size_t nlm_backward_smem_bytes(int channels, int temporal_radius, int search_radius, int patch_radius);
+cudaError_t launch_nlm_backward(const NlmBackwardLaunch& args, cudaStream_t stream);
+
 }  // namespace avd

@@ -117,4 +117,46 @@ AvdStatus avd_immerkaer(uint64_t frame, uint32_t channels, uint32_t width, uint3
     return AVD_OK;
 }
 
+uint64_t avd_nlm_backward_scratch_bytes(uint32_t width, uint32_t height) {
+    return avd::nlm_backward_scratch_floats(static_cast<int>(width), static_cast<int>(height)) * sizeof(float);
+}
+
+AvdStatus avd_nlm_backward(const AvdNlmBackward* p, void* stream) {
+    if (!p || !p->window || !p->grad_out || !p->grad_window || !p->grad_strength || !p->scratch)
+        return fail(AVD_ERR_NULL_ARG, "nlm backward: null buffer");
+    if (p->channels < 1 || p->channels > 2 || p->width < 1 || p->height < 1)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "nlm backward: bad geometry");
+    if (p->temporal_radius > avd::kMaxTemporalRadius || p->search_radius > avd::kMaxSearchRadius ||
+        p->patch_radius > avd::kMaxPatchRadius)
+        return fail(AVD_ERR_INVALID_OPTIONS, "nlm backward: radius past the NLMeans limits");
+    if (avd::nlm_backward_smem_bytes(static_cast<int>(p->channels), static_cast<int>(p->temporal_radius),
+                                     static_cast<int>(p->search_radius), static_cast<int>(p->patch_radius)) >
+        200u * 1024u)
+        return fail(AVD_ERR_INVALID_OPTIONS,
+                    "nlm backward: (2d+1)(16+2(a+s))^2 x channels floats of gradient tiles exceed 200 KiB");
+    if (!(p->strength > 0.0f)) return fail(AVD_ERR_INVALID_OPTIONS, "nlm backward: strength must be positive");
+    avd::NlmBackwardLaunch l{};
+    l.window = reinterpret_cast<const float*>(p->window);
+    l.grad_out = reinterpret_cast<const float*>(p->grad_out);
+    l.grad_window = reinterpret_cast<float*>(p->grad_window);
+    l.grad_strength = reinterpret_cast<float*>(p->grad_strength);
+    l.scratch = reinterpret_cast<float*>(p->scratch);
+    l.width = static_cast<int>(p->width);
+    l.height = static_cast<int>(p->height);
+    l.channels = static_cast<int>(p->channels);
+    l.temporal_radius = static_cast<int>(p->temporal_radius);
+    l.search_radius = static_cast<int>(p->search_radius);
+    l.patch_radius = static_cast<int>(p->patch_radius);
+    l.strength = p->strength;
+    // nlmeans/params.rs:229-233, in the same f32 order as the forward's strength word.
+    const float area = static_cast<float>((2 * p->patch_radius + 1) * (2 * p->patch_radius + 1));
+    l.h2 = (255.0f * 255.0f) / ((3.0f * p->strength * p->strength) * area);
+    l.wref = p->self_weight;
+    l.pair_offset = p->pair_offset;
+    l.spatial_offset = p->spatial_offset;
+    cudaError_t e = avd::launch_nlm_backward(l, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("nlm backward launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
 }  // extern "C"

@@ -436,6 +436,32 @@ AVD_API uint64_t avd_immerkaer_partials_len(uint32_t width, uint32_t height);
 AVD_API AvdStatus avd_immerkaer(uint64_t frame, uint32_t channels, uint32_t width, uint32_t height, uint64_t partials,
                                 uint64_t results, uint64_t sigma_low, void* stream);
 
+/* ---- adjoint -------------------------------------------------------------------------------- */
+
+/* No Rust item in the reference: the adjoint the hot-path contract adds to the boundary
+ * (`avd_nlm_backward`, dL/d(frames) and dL/d(h)). It differentiates one output frame of the windowed
+ * NLMeans path (av-denoise-core/src/nlmeans/kernels/fused.rs:138-530, accumulate.rs:152-202): the
+ * window of 2d+1 normalised f32 frames (oldest first, `channels` interleaved, contiguous), the
+ * search radius a, the patch radius s, the strength (h2 = 255^2 / (3 strength^2 (2s+1)^2), as
+ * nlmeans/params.rs:229-233), the self weight, and the noise offsets of the pair and spatial
+ * offsets (both 0 for the fast variant; NLMeans-HQ with a pinned sigma passes its noise offset in
+ * both). Weights are recomputed, never stored; the max weight passes its gradient to the first offset
+ * that reaches it. Scratch: avd_nlm_backward_scratch_bytes(width, height) bytes. Shared memory bounds
+ * the window: (2d+1) (16 + 2 (a + s))^2 channels floats must stay within 200 KiB, else
+ * AVD_ERR_INVALID_OPTIONS. `grad_window` and `grad_strength` are overwritten; queued on `stream`. */
+typedef struct AvdNlmBackward {
+    uint64_t window;        /* f32, (2d+1) x height x width x channels */
+    uint64_t grad_out;      /* f32, height x width x channels: dL/d(output) */
+    uint64_t grad_window;   /* f32 like `window`: dL/d(frames), written */
+    uint64_t grad_strength; /* f32[1]: dL/d(strength), written */
+    uint64_t scratch;
+    uint32_t width, height, channels, temporal_radius, search_radius, patch_radius;
+    float strength, self_weight, pair_offset, spatial_offset;
+} AvdNlmBackward;
+
+AVD_API uint64_t avd_nlm_backward_scratch_bytes(uint32_t width, uint32_t height);
+AVD_API AvdStatus avd_nlm_backward(const AvdNlmBackward* args, void* stream);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 
 /* No counterpart in the reference. One fast-variant NLMeans output frame for callers that cannot

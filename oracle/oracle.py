@@ -486,3 +486,33 @@ def immerkaer_sigma_low_from_partials(partials: np.ndarray, channels: int, width
     l.orc_immerkaer_sigma_low(_f(np.ascontiguousarray(partials, np.float32)), channels, width, height,
                               immerkaer_scale(), _f(low))
     return low
+
+
+# ---- NLMeans adjoint (nlm_backward_oracle.cpp) -----------------------------------------------------
+
+def nlm_backward(window: list[np.ndarray], d: int, a: int, s: int, strength: float, grad_out: np.ndarray,
+                 wref: float = 1.0, pair_offset: float = 0.0, spatial_offset: float = 0.0):
+    """FP64 dL/d(window frames) (2d+1, H, W, C) and dL/d(strength) for dL/d(out) = grad_out."""
+    h, w, c = window[0].shape
+    frames = [np.ascontiguousarray(f, np.float32) for f in window]
+    arr = (_fp * len(frames))(*[_f(f) for f in frames])
+    g = np.ascontiguousarray(grad_out, np.float64)
+    gf = np.zeros((2 * d + 1, h, w, c), np.float64)
+    gs = C.c_double(0.0)
+    l = lib()
+    l.orc_nlm_backward_f64.argtypes = [_fpp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, _dp, _dp, C.POINTER(C.c_double)]
+    l.orc_nlm_backward_f64(arr, w, h, c, d, a, s, strength, wref, pair_offset, spatial_offset,
+                           g.ctypes.data_as(_dp), gf.ctypes.data_as(_dp), C.byref(gs))
+    return gf, gs.value
+
+
+def nlm_forward_f64(window: list[np.ndarray], d: int, a: int, s: int, strength: float, wref: float = 1.0,
+                    pair_offset: float = 0.0, spatial_offset: float = 0.0) -> np.ndarray:
+    """The FP64 forward with h2 taken in FP64 from `strength` (for finite differences)."""
+    h2 = 65025.0 / (3.0 * strength * strength * (2 * s + 1) ** 2)
+    side = 2 * a + 1
+    lut = np.full(side * side, spatial_offset, np.float32)
+    lut[a * side + a] = 0.0
+    return nlm_frame(window, d, a, s, h2, noise_offset=pair_offset, lut=lut if spatial_offset else None, wref=wref,
+                     fp64=True)
