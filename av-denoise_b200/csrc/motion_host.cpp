@@ -133,7 +133,8 @@ AvdStatus avd_nlm_backward(const AvdNlmBackward* p, void* stream) {
                                      static_cast<int>(p->search_radius), static_cast<int>(p->patch_radius)) >
         200u * 1024u)
         return fail(AVD_ERR_INVALID_OPTIONS,
-                    "nlm backward: (2d+1)(16+2(a+s))^2 x channels floats of gradient tiles exceed 200 KiB");
+                    "nlm backward: the staged frames and gradient tiles, 2 (2d+1)(32+2(a+s))(8+2(a+s)) x channels "
+                    "floats, exceed 200 KiB of shared memory");
     if (!(p->strength > 0.0f)) return fail(AVD_ERR_INVALID_OPTIONS, "nlm backward: strength must be positive");
     avd::NlmBackwardLaunch l{};
     l.window = reinterpret_cast<const float*>(p->window);

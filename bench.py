@@ -501,12 +501,85 @@ def run_nl4d(pushes: int, size: str) -> None:
                       "push_ms": [round(t, 3) for t in times]}))
 
 
+def run_adjoint(reps: int) -> None:
+    """The NLMeans adjoint (`avd_nlm_backward`) against its forward on the same window: 1920x1080
+    luma, d=2, a=5, s=2, strength 8, fast variant. The forward is the engine's push (ingest + the
+    windowed NLM launch) in steady state; both are timed with CUDA events on one stream. Prints one
+    JSON line with both times and their ratio."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import _abi, synth
+
+    lib = _abi.load()
+    w, h, d, a, s, strength = W, H, 2, 5, 2, 8.0
+    fmt = avd.SampleFormat.u8()
+    clip = synth.make_clip(w, h, 2 * d + 1, depth=8, chroma="gray", sigma_luma=8.0, global_motion=4, sprites=3,
+                           seed=7)
+    t = avd.NlmTuning(search_radius=a, patch_radius=s, strength=strength)
+    alg = avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(tuning=t, mode=avd.DenoisingMode.temporal(d)))
+    eng = avd.build_engine(avd.EngineSpec.nlmeans(alg, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt)))
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    bufs = []
+    for f in clip:
+        flat = f[0].reshape(-1)
+        bufs.append(torch.from_numpy(np.concatenate([flat, np.zeros((-flat.size) % 4, np.uint8)]).view(np.int32)).cuda())
+    out = torch.zeros_like(bufs[0])
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def push(i):
+        if eng.push([avd.DevicePlane.from_tensor(bufs[i % len(bufs)], w, h)]):
+            eng.emit_into([avd.DevicePlane.from_tensor(out, w, h)])
+
+    for i in range(3):
+        push(i)
+    fwd = [timed(lambda i=i: push(i)) for i in range(3, 3 + reps)]
+    eng.close()
+    window = torch.from_numpy(np.stack([f[0].astype(np.float32) / 255.0 for f in clip]).reshape(-1)).cuda()
+    g = torch.randn(w * h, device="cuda")
+    gw = torch.empty_like(window)
+    gs = torch.zeros(1, device="cuda")
+    scratch = torch.empty(lib.avd_nlm_backward_scratch_bytes(w, h) // 4, device="cuda")
+    p = _abi.AvdNlmBackward()
+    p.window, p.grad_out, p.grad_window, p.grad_strength = window.data_ptr(), g.data_ptr(), gw.data_ptr(), gs.data_ptr()
+    p.scratch = scratch.data_ptr()
+    p.width, p.height, p.channels, p.temporal_radius, p.search_radius, p.patch_radius = w, h, 1, d, a, s
+    p.strength, p.self_weight, p.pair_offset, p.spatial_offset = strength, 1.0, 0.0, 0.0
+
+    def backward():
+        st = lib.avd_nlm_backward(C.byref(p), C.c_void_p(stream.cuda_stream))
+        if st != 0:
+            raise RuntimeError(lib.avd_last_error().decode())
+
+    backward()
+    bwd = [timed(backward) for _ in range(reps)]
+    f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
+    print(json.dumps({"workload": "NLMeans adjoint, 1920x1080 luma f32 window, d=2 a=5 s=2 strength 8",
+                      "forward_ms": round(f_ms, 4), "backward_ms": round(b_ms, 4),
+                      "backward_over_forward": round(b_ms / f_ms, 3)}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--once", action="store_true", help="run one luma NLM launch (profiling case) and exit")
     ap.add_argument("--nl4d", type=int, default=0, metavar="PUSHES",
                     help="time PUSHES pushes of the NL4D engine (secondary workload) and exit")
     ap.add_argument("--nl4d-size", default="1080", choices=["1080", "2160"])
+    ap.add_argument("--adjoint", type=int, default=0, metavar="REPS",
+                    help="time the NLMeans adjoint against its forward REPS times and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -518,6 +591,8 @@ def main() -> None:
         run_once()
     elif args.nl4d:
         run_nl4d(args.nl4d, args.nl4d_size)
+    elif args.adjoint:
+        run_adjoint(args.adjoint)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -447,8 +447,8 @@ AVD_API AvdStatus avd_immerkaer(uint64_t frame, uint32_t channels, uint32_t widt
  * offsets (both 0 for the fast variant; NLMeans-HQ with a pinned sigma passes its noise offset in
  * both). Weights are recomputed, never stored; the max weight passes its gradient to the first offset
  * that reaches it. Scratch: avd_nlm_backward_scratch_bytes(width, height) bytes. Shared memory bounds
- * the window: (2d+1) (16 + 2 (a + s))^2 channels floats must stay within 200 KiB, else
- * AVD_ERR_INVALID_OPTIONS. `grad_window` and `grad_strength` are overwritten; queued on `stream`. */
+ * the window: the staged frames and gradient tiles, 2 (2d+1) (32 + 2(a+s)) (8 + 2(a+s)) channels
+ * floats, must stay within 200 KiB, else AVD_ERR_INVALID_OPTIONS. `grad_window` and `grad_strength` are overwritten; queued on `stream`. */
 typedef struct AvdNlmBackward {
     uint64_t window;        /* f32, (2d+1) x height x width x channels */
     uint64_t grad_out;      /* f32, height x width x channels: dL/d(output) */
