@@ -218,6 +218,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_immerkaer": (C.c_int, [u64, u32, u32, u32, u64, u64, u64, C.c_void_p]),
     "avd_nlm_backward_scratch_bytes": (u64, [u32, u32]),
     "avd_nlm_backward": (C.c_int, [_P(AvdNlmBackward), C.c_void_p]),
+    "avd_nlm_window_scratch_bytes": (u64, [u32]),
+    "avd_nlm_window": (C.c_int, [_P(AvdNlmBackward), C.c_void_p]),
     "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,
                                        _P(AvdPlane), C.c_size_t, _P(AvdPlane), C.c_size_t, C.c_void_p]),
 }

@@ -126,5 +126,9 @@ struct NlmBackwardLaunch {
 size_t nlm_backward_scratch_floats(int width, int height);
 size_t nlm_backward_smem_bytes(int channels, int temporal_radius, int search_radius, int patch_radius);
 cudaError_t launch_nlm_backward(const NlmBackwardLaunch& args, cudaStream_t stream);
+// Words for a kernel-level NLM launch: h2 at 0, the pair offset at 1, the (2a+1)^2 spatial offset
+// table (flat, 0 at the centre) from word 8.
+cudaError_t launch_window_words(float* words, float h2, float pair_offset, float spatial_offset, int a,
+                                cudaStream_t stream);
 
 }  // namespace avd

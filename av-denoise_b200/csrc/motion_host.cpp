@@ -160,4 +160,52 @@ AvdStatus avd_nlm_backward(const AvdNlmBackward* p, void* stream) {
     return AVD_OK;
 }
 
+uint64_t avd_nlm_window_scratch_bytes(uint32_t search_radius) {
+    return (8 + static_cast<uint64_t>(2 * search_radius + 1) * (2 * search_radius + 1)) * sizeof(float);
+}
+
+AvdStatus avd_nlm_window(const AvdNlmBackward* p, void* stream) {
+    if (!p || !p->window || !p->grad_out || !p->scratch) return fail(AVD_ERR_NULL_ARG, "nlm window: null buffer");
+    if (p->channels < 1 || p->channels > 2 || p->width < avd::kMinFrameDim || p->height < avd::kMinFrameDim)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "nlm window: bad geometry");
+    if (p->temporal_radius > avd::kMaxTemporalRadius || p->search_radius > avd::kMaxSearchRadius ||
+        p->patch_radius > avd::kMaxPatchRadius)
+        return fail(AVD_ERR_INVALID_OPTIONS, "nlm window: radius past the NLMeans limits");
+    if (!(p->strength > 0.0f)) return fail(AVD_ERR_INVALID_OPTIONS, "nlm window: strength must be positive");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const float area = static_cast<float>((2 * p->patch_radius + 1) * (2 * p->patch_radius + 1));
+    const float h2 = (255.0f * 255.0f) / ((3.0f * p->strength * p->strength) * area);
+    float* words = reinterpret_cast<float*>(p->scratch);
+    cudaError_t e = avd::launch_window_words(words, h2, p->pair_offset, p->spatial_offset,
+                                             static_cast<int>(p->search_radius), s);
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, cudaGetErrorString(e));
+    const int d = static_cast<int>(p->temporal_radius);
+    avd::NlmLaunch a{};
+    a.ring = reinterpret_cast<const float*>(p->window);
+    a.width = static_cast<int>(p->width);
+    a.height = static_cast<int>(p->height);
+    a.channels = static_cast<int>(p->channels);
+    a.frame_elems = static_cast<int64_t>(p->width) * p->height * p->channels;
+    a.slot_centre = d;
+    a.pairs = d;
+    for (int k = 0; k < d; ++k) {
+        a.slot_fwd[k] = k;
+        a.slot_bwd[k] = 2 * d - k;
+    }
+    a.patch_radius = static_cast<int>(p->patch_radius);
+    a.search_radius = static_cast<int>(p->search_radius);
+    a.derived = words;
+    a.h2_word = 0;
+    a.offset_word = 1;
+    const bool plain = p->pair_offset == 0.0f && p->spatial_offset == 0.0f;
+    a.spatial_lut = plain ? nullptr : words + 8;
+    a.conf = nullptr;
+    a.wref = p->self_weight;
+    a.fast = plain ? 1 : 0;
+    a.out = reinterpret_cast<float*>(p->grad_out);
+    e = avd::launch_nlm(a, s);
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("nlm window launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
 }  // extern "C"

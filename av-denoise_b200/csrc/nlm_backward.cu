@@ -398,4 +398,22 @@ cudaError_t launch_nlm_backward(const NlmBackwardLaunch& l, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void window_words_kernel(float* words, float h2, float pair_offset, float spatial_offset, int a) {
+    const int side = 2 * a + 1;
+    for (int i = threadIdx.x; i < side * side; i += blockDim.x)
+        words[8 + i] = i == a * side + a ? 0.0f : spatial_offset;
+    if (threadIdx.x == 0) {
+        words[0] = h2;
+        words[1] = pair_offset;
+    }
+}
+}  // namespace
+
+cudaError_t launch_window_words(float* words, float h2, float pair_offset, float spatial_offset, int a,
+                                cudaStream_t s) {
+    window_words_kernel<<<1, 128, 0, s>>>(words, h2, pair_offset, spatial_offset, a);
+    return cudaGetLastError();
+}
+
 }  // namespace avd

@@ -460,6 +460,14 @@ typedef struct AvdNlmBackward {
 } AvdNlmBackward;
 
 AVD_API uint64_t avd_nlm_backward_scratch_bytes(uint32_t width, uint32_t height);
+
+/* The forward the adjoint differentiates, at kernel level: one output frame of the windowed NLMeans
+ * path (the engine's launch, nlmeans/dispatch/mod.rs:627-679) from the same `AvdNlmBackward` fields
+ * (`window`, the radii, strength, self weight and offsets) into `grad_out`, which here receives the
+ * f32 output frame; `grad_window` and `grad_strength` are unused. `scratch` needs
+ * avd_nlm_window_scratch_bytes(search_radius) bytes. Queued on `stream`; allocates nothing. */
+AVD_API uint64_t avd_nlm_window_scratch_bytes(uint32_t search_radius);
+AVD_API AvdStatus avd_nlm_window(const AvdNlmBackward* args, void* stream);
 AVD_API AvdStatus avd_nlm_backward(const AvdNlmBackward* args, void* stream);
 
 /* ---- allocation-free entry point ----------------------------------------------------------- */
