@@ -172,6 +172,12 @@ class AvdNlmBackward(C.Structure):
                [(n, f32) for n in ("strength", "self_weight", "pair_offset", "spatial_offset")]
 
 
+class AvdBatchJob(C.Structure):
+    _fields_ = [("frames", u64), ("out", u64)] + \
+               [(n, u32) for n in ("n_frames", "centre", "temporal_radius", "width", "height")] + \
+               [(n, f32) for n in ("strength", "pair_offset", "spatial_offset")]
+
+
 _P = C.POINTER
 _E = C.c_void_p  # AvdEngine*
 
@@ -220,6 +226,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_nlm_backward": (C.c_int, [_P(AvdNlmBackward), C.c_void_p]),
     "avd_nlm_window_scratch_bytes": (u64, [u32]),
     "avd_nlm_window": (C.c_int, [_P(AvdNlmBackward), C.c_void_p]),
+    "avd_batch_scratch_bytes": (u64, [C.c_size_t, u32]),
+    "avd_batch_submit": (C.c_int, [_P(AvdBatchJob), C.c_size_t, u32, u32, u32, f32, u64, C.c_void_p]),
     "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,
                                        _P(AvdPlane), C.c_size_t, _P(AvdPlane), C.c_size_t, C.c_void_p]),
 }

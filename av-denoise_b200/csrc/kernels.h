@@ -50,6 +50,13 @@ struct NlmLaunch {
 
 cudaError_t launch_nlm(const NlmLaunch& args, cudaStream_t stream);
 
+// A batch of NLM launches (device array `jobs`, all with `channels`, `patch_radius` and `fast`) as one
+// persistent launch: `prefix` holds njobs + 1 running tile counts, `counter` one zeroed int.
+int nlm_tile_rows(int channels, int patch_radius);
+int nlm_tile_cols();
+cudaError_t launch_nlm_batch(const NlmLaunch* jobs, const int* prefix, int njobs, int* counter, int channels,
+                             int patch_radius, bool fast, int max_search_radius, int max_pairs, cudaStream_t stream);
+
 // One NL4D collaborative-filter pass (collab/kernels/fused/mod.rs:170): every reference patch of
 // the centre slot, scattered into the per-slot fixed-point accumulators.
 struct CollabLaunch {

@@ -267,16 +267,18 @@ __device__ __forceinline__ void step(const Smem& sm, int A, const Lanes& ln, int
     buf ^= 1;
 }
 
+extern __shared__ __align__(16) float smem_raw[];
+
+// One output tile (tile_x, tile_y) of the launch `a`; the whole CTA calls it.
 template <int C, int S, bool FAST>
-__global__ void __launch_bounds__(kThreads, C == 1 && FAST ? 5 : 4) nlm_window_kernel(NlmLaunch a) {
+__device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int tile_y) {
     using K = Cfg<C, S>;
     constexpr int V = K::V;
-    extern __shared__ __align__(16) float smem_raw[];
 
     const int A = a.search_radius;
     const int W = a.width, H = a.height;
-    const int X0 = blockIdx.x * kTX;
-    const int Y0 = blockIdx.y * K::TY;
+    const int X0 = tile_x * kTX;
+    const int Y0 = tile_y * K::TY;
     const int tid = threadIdx.x;
     const int col = tid & 31;
     const int y0 = (tid >> 5) * V;
@@ -402,6 +404,38 @@ __global__ void __launch_bounds__(kThreads, C == 1 && FAST ? 5 : 4) nlm_window_k
     }
 }
 
+template <int C, int S, bool FAST>
+__global__ void __launch_bounds__(kThreads, C == 1 && FAST ? 5 : 4) nlm_window_kernel(NlmLaunch a) {
+    nlm_tile<C, S, FAST>(a, blockIdx.x, blockIdx.y);
+}
+
+// Persistent batch: every CTA takes tiles from one counter until the batch's tiles run out. Tile t
+// belongs to the job j with prefix[j] <= t < prefix[j + 1]; jobs are whole launch descriptions.
+template <int C, int S, bool FAST>
+__global__ void __launch_bounds__(kThreads, C == 1 && FAST ? 5 : 4)
+    nlm_batch_kernel(const NlmLaunch* __restrict__ jobs, const int* __restrict__ prefix, int njobs, int* counter) {
+    using K = Cfg<C, S>;
+    __shared__ int tile_s;
+    const int total = prefix[njobs];
+    for (;;) {
+        __syncthreads();  // the previous tile is done with shared memory and `tile_s`
+        if (threadIdx.x == 0) tile_s = atomicAdd(counter, 1);
+        __syncthreads();
+        const int t = tile_s;
+        if (t >= total) return;
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const NlmLaunch& a = jobs[lo];
+        const int local = t - prefix[lo];
+        const int tiles_x = (a.width + kTX - 1) / kTX;
+        nlm_tile<C, S, FAST>(a, local % tiles_x, local / tiles_x);
+    }
+}
+
 template <int C, int S>
 size_t smem_bytes(int A, int pairs) {
     using K = Cfg<C, S>;
@@ -439,7 +473,59 @@ cudaError_t dispatch_s(const NlmLaunch& a, cudaStream_t stream) {
     }
 }
 
+template <int C, int S, bool FAST>
+cudaError_t batch_csf(const NlmLaunch* jobs, const int* prefix, int njobs, int* counter, int max_a, int max_pairs,
+                      cudaStream_t stream) {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(nlm_batch_kernel<C, S, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024);
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    const size_t smem = smem_bytes<C, S>(max_a, max_pairs);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nlm_batch_kernel<C, S, FAST>, kThreads, smem);
+    if (e != cudaSuccess) return e;
+    nlm_batch_kernel<C, S, FAST><<<sms * (per_sm > 0 ? per_sm : 1), kThreads, smem, stream>>>(jobs, prefix, njobs,
+                                                                                              counter);
+    return cudaGetLastError();
+}
+
+template <int C, int S>
+cudaError_t batch_s(int s, bool fast, const NlmLaunch* jobs, const int* prefix, int njobs, int* counter, int max_a,
+                    int max_pairs, cudaStream_t stream) {
+    if (s == S)
+        return fast ? batch_csf<C, S, true>(jobs, prefix, njobs, counter, max_a, max_pairs, stream)
+                    : batch_csf<C, S, false>(jobs, prefix, njobs, counter, max_a, max_pairs, stream);
+    if constexpr (S < 16) {
+        return batch_s<C, S + 1>(s, fast, jobs, prefix, njobs, counter, max_a, max_pairs, stream);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+}
+
 }  // namespace
+
+// Cfg<C, S>::TY: the tile height depends on the patch radius alone.
+int nlm_tile_rows(int /*channels*/, int patch_radius) {
+    const int v = (32 - 2 * patch_radius) / 4;
+    return 4 * (v >= 1 ? v : 1);
+}
+
+int nlm_tile_cols() { return kTX; }
+
+cudaError_t launch_nlm_batch(const NlmLaunch* jobs, const int* prefix, int njobs, int* counter, int channels,
+                             int patch_radius, bool fast, int max_search_radius, int max_pairs, cudaStream_t stream) {
+    if (channels == 1)
+        return batch_s<1, 0>(patch_radius, fast, jobs, prefix, njobs, counter, max_search_radius, max_pairs, stream);
+    if (channels == 2)
+        return batch_s<2, 0>(patch_radius, fast, jobs, prefix, njobs, counter, max_search_radius, max_pairs, stream);
+    return cudaErrorInvalidValue;
+}
 
 cudaError_t launch_nlm(const NlmLaunch& a, cudaStream_t stream) {
     if (a.pairs < 0 || a.pairs > kMaxPairs || a.search_radius < 0 || a.search_radius > 8 || a.patch_radius < 0 ||

@@ -572,6 +572,103 @@ def run_adjoint(reps: int) -> None:
                       "backward_over_forward": round(b_ms / f_ms, 3)}))
 
 
+def run_batch(reps: int) -> None:
+    """The batched NLMeans launch against the plain per-frame loop on a mix of 24 clips: resolution
+    from {640x360, 1280x720, 1920x1080, 2560x1440, 3840x2160}, depth from {8, 10, 12}, 4-17 frames,
+    temporal radius 1-8, a=4, s=2, NLMeans-HQ with each clip's sigma pinned (U(4, 24) in 8-bit
+    units: strength = hq_default_strength(luma, d) * sigma and the flat noise offset). Frames are
+    synthetic (six gratings, a pan, Gaussian noise, quantised to the clip's depth) generated on the
+    device; every frame of every clip is one job. Both arms are timed with CUDA events."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import _abi
+
+    lib = _abi.load()
+    rng = np.random.default_rng(3000)
+    a, s = 4, 2
+    sizes = [(640, 360), (1280, 720), (1920, 1080), (2560, 1440), (3840, 2160)]
+    jobs, keep, singles, pixels = [], [], [], 0
+    for i in range(24):
+        w, h = sizes[int(rng.integers(0, 5))]
+        depth = int(rng.choice([8, 10, 12]))
+        n = int(rng.integers(4, 18))
+        d = int(rng.integers(1, 9))
+        sigma = float(rng.uniform(4.0, 24.0)) / 255.0
+        y, x = torch.meshgrid(torch.arange(h, device="cuda", dtype=torch.float32),
+                              torch.arange(w, device="cuda", dtype=torch.float32), indexing="ij")
+        base = torch.zeros(h, w, device="cuda")
+        for _ in range(6):
+            f, th = float(rng.uniform(0.01, 0.3)), float(rng.uniform(0, np.pi))
+            base += float(rng.uniform(5, 30)) / 255.0 * torch.sin(2 * np.pi * f * (x * np.cos(th) + y * np.sin(th)))
+        base = (base + 0.5).clamp(16 / 255, 235 / 255)
+        levels = float(2 ** depth - 1)
+        gen = torch.Generator(device="cuda").manual_seed(1000 * 3 + i)
+        frames = torch.stack([torch.roll(base, shifts=(int(rng.integers(-4, 5)) * t,), dims=(1,)) +
+                              sigma * torch.randn(h, w, generator=gen, device="cuda") for t in range(n)])
+        frames = (frames.clamp(0, 1) * levels).round() / levels
+        keep.append(frames)
+        strength = float(avd.hq_default_strength(1, d)) * sigma * 255.0
+        offset = float(np.float32(2.0 * 3.0) * np.float32(sigma) ** 2 * np.float32((2 * s + 1) ** 2))
+        for c in range(n):
+            out = torch.empty(h * w, device="cuda")
+            keep.append(out)
+            jobs.append(_abi.AvdBatchJob(frames.data_ptr(), out.data_ptr(), n, c, d, w, h, strength, offset, offset))
+            singles.append((frames, c, d, strength, offset, out, w, h))
+            pixels += w * h
+    arr = (_abi.AvdBatchJob * len(jobs))(*jobs)
+    scratch = torch.empty(lib.avd_batch_scratch_bytes(len(jobs), a) // 4, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    win_scratch = torch.empty(lib.avd_nlm_window_scratch_bytes(a) // 4 + 1, device="cuda")
+    max_window = max(fr.shape[1] * fr.shape[2] * (2 * d + 1) for fr, _, d, *_ in singles)
+    win_buf = torch.empty(max_window, device="cuda")
+
+    def batched():
+        if lib.avd_batch_submit(arr, len(jobs), 1, a, s, 1.0, scratch.data_ptr(), C.c_void_p(stream.cuda_stream)):
+            raise RuntimeError(lib.avd_last_error().decode())
+
+    params = []
+    for frames, c, d, strength, offset, out, w, h in singles:
+        n = frames.shape[0]
+        idx = torch.tensor([min(max(c - d + k, 0), n - 1) for k in range(2 * d + 1)], device="cuda")
+        p = _abi.AvdNlmBackward()
+        p.window, p.grad_out, p.scratch = win_buf.data_ptr(), out.data_ptr(), win_scratch.data_ptr()
+        p.width, p.height, p.channels, p.temporal_radius, p.search_radius, p.patch_radius = w, h, 1, d, a, s
+        p.strength, p.self_weight, p.pair_offset, p.spatial_offset = strength, 1.0, offset, offset
+        params.append((frames, idx, p, (2 * d + 1) * w * h))
+
+    def per_frame():
+        # The plain loop: one windowed launch per frame (the window gathered into one buffer, as a
+        # per-clip ring holds it).
+        for frames, idx, p, count in params:
+            torch.index_select(frames, 0, idx, out=win_buf[:count].view(idx.numel(), *frames.shape[1:]))
+            if lib.avd_nlm_window(C.byref(p), C.c_void_p(stream.cuda_stream)):
+                raise RuntimeError(lib.avd_last_error().decode())
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    batched()
+    per_frame()
+    b_ms = float(np.median([timed(batched) for _ in range(reps)]))
+    l_ms = float(np.median([timed(per_frame) for _ in range(reps)]))
+    print(json.dumps({"workload": f"NLMeans-HQ pinned sigma, 24 mixed clips, {len(jobs)} frames, "
+                                  f"{pixels / 1e6:.1f} Mpixel, a=4 s=2, d 1-8",
+                      "batched_ms": round(b_ms, 3), "per_frame_loop_ms": round(l_ms, 3),
+                      "speedup": round(l_ms / b_ms, 3),
+                      "batched_frames_per_s": round(len(jobs) / b_ms * 1000.0, 2)}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--once", action="store_true", help="run one luma NLM launch (profiling case) and exit")
@@ -580,6 +677,8 @@ def main() -> None:
     ap.add_argument("--nl4d-size", default="1080", choices=["1080", "2160"])
     ap.add_argument("--adjoint", type=int, default=0, metavar="REPS",
                     help="time the NLMeans adjoint against its forward REPS times and exit")
+    ap.add_argument("--batch", type=int, default=0, metavar="REPS",
+                    help="time the batched launch against the per-frame loop REPS times and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -593,6 +692,8 @@ def main() -> None:
         run_nl4d(args.nl4d, args.nl4d_size)
     elif args.adjoint:
         run_adjoint(args.adjoint)
+    elif args.batch:
+        run_batch(args.batch)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -470,6 +470,30 @@ AVD_API uint64_t avd_nlm_window_scratch_bytes(uint32_t search_radius);
 AVD_API AvdStatus avd_nlm_window(const AvdNlmBackward* args, void* stream);
 AVD_API AvdStatus avd_nlm_backward(const AvdNlmBackward* args, void* stream);
 
+/* ---- batched launch ------------------------------------------------------------------------- */
+
+/* No Rust item in the reference: the batched launch the hot-path contract adds to the boundary
+ * (`avd_batch_submit`). Many clips of uneven resolution, window and strength, one denoised frame
+ * per job, in one persistent launch over a tile work queue. A job is one output frame: `frames`
+ * holds the clip's `n_frames` normalised f32 frames (height x width x channels each, contiguous),
+ * the window is frames clamp(centre - d + k), k in 0..=2d (the engine's repeat edges), and the
+ * result goes to `out`. Each job carries its own strength (h2 = 255^2 / (3 strength^2 (2s+1)^2)) and
+ * noise offsets (0 and 0 for the fast variant; NLMeans-HQ with a pinned sigma passes its offset in
+ * both). The batch shares channels, search radius, patch radius and self weight. */
+typedef struct AvdBatchJob {
+    uint64_t frames;
+    uint64_t out;
+    uint32_t n_frames, centre, temporal_radius, width, height;
+    float strength, pair_offset, spatial_offset;
+} AvdBatchJob;
+
+/* The scratch one batch of `n_jobs` jobs needs (job table, tile prefix, strength words). */
+AVD_API uint64_t avd_batch_scratch_bytes(size_t n_jobs, uint32_t search_radius);
+
+/* Queues the batch on `stream`: one copy of its table into `scratch`, then one launch. */
+AVD_API AvdStatus avd_batch_submit(const AvdBatchJob* jobs, size_t n_jobs, uint32_t channels, uint32_t search_radius,
+                                   uint32_t patch_radius, float self_weight, uint64_t scratch, void* stream);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 
 /* No counterpart in the reference. One fast-variant NLMeans output frame for callers that cannot
