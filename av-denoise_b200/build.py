@@ -35,6 +35,12 @@ COMMON = [
 ]
 
 
+# Per-file flags. The NL4D collaborative filter rounds every multiply and add on its own, as its CPU
+# restatement does (built with -ffp-contract=off), so its member choices and threshold decisions
+# agree bit for bit; -fmad=false keeps nvcc from fusing any of them.
+PER_FILE = {"collab.cu": ["-fmad=false"]}
+
+
 def _sources() -> list[Path]:
     return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
 
@@ -52,7 +58,7 @@ def _needs(obj: Path, src: Path, headers: list[Path]) -> bool:
 
 def _compile(src: Path, extra: list[str]) -> Path:
     obj = BUILD / (src.name + ".o")
-    cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
+    cmd = [NVCC, *ARCH, *COMMON, *PER_FILE.get(src.name, []), *extra, "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cpp":
         cmd = [HOST_CXX, "-std=c++17", "-O3", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wextra",
                f"-I{ROOT / 'include'}", f"-I{CSRC}", f"-I{CUDA_HOME / 'include'}", "-c", str(src), "-o", str(obj)]

@@ -16,7 +16,9 @@
 // `__syncwarp(mask)`), so groups of one warp may take different trip counts through their
 // clipped windows: no block barrier is ever needed. The group's 8 members x 8 values stay in
 // registers through the transforms. Accumulation is integer atomics, so the output does not
-// depend on scheduling.
+// depend on scheduling. Every multiply and add is rounded on its own (no fused multiply-add),
+// in the restatement's order, so the floats, and with them every threshold decision and member
+// choice, agree bit for bit with the CPU oracle.
 
 #include <cuda_runtime.h>
 
@@ -76,7 +78,7 @@ __device__ __forceinline__ float column_ssd(const float (&ref)[P * C], const flo
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             float d = ref[r * C + c] - __ldg(p + static_cast<size_t>(r) * width * C + c);
-            s = fmaf(d, d, s);
+            s = __fadd_rn(s, __fmul_rn(d, d));
         }
     }
     return s;
@@ -94,8 +96,8 @@ __device__ __forceinline__ void dct8_fwd(float (&line)[P]) {
         float even = 0.0f, odd = 0.0f;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            even = fmaf(s[k], c_dct[2 * m][k], even);
-            odd = fmaf(d[k], c_dct[2 * m + 1][k], odd);
+            even = __fadd_rn(even, __fmul_rn(s[k], c_dct[2 * m][k]));
+            odd = __fadd_rn(odd, __fmul_rn(d[k], c_dct[2 * m + 1][k]));
         }
         line[2 * m] = even;
         line[2 * m + 1] = odd;
@@ -111,8 +113,8 @@ __device__ __forceinline__ void dct8_inv(float (&line)[P]) {
         float even = 0.0f, odd = 0.0f;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
-            even = fmaf(snap[2 * m], c_dct[2 * m][k], even);
-            odd = fmaf(snap[2 * m + 1], c_dct[2 * m + 1][k], odd);
+            even = __fadd_rn(even, __fmul_rn(snap[2 * m], c_dct[2 * m][k]));
+            odd = __fadd_rn(odd, __fmul_rn(snap[2 * m + 1], c_dct[2 * m + 1][k]));
         }
         line[k] = even + odd;
         line[7 - k] = even - odd;
@@ -178,7 +180,7 @@ __device__ __forceinline__ float pooled_threshold(const GroupCtx& g, float (&s)[
             previous = current;
             current = next;
         }
-        if (j < k_use) retained += kept_profile * lane_var;
+        if (j < k_use) retained = __fadd_rn(retained, __fmul_rn(kept_profile, lane_var));
     }
     return retained;
 }
@@ -485,7 +487,7 @@ __device__ __forceinline__ float ring_ssd(const float (&ref)[P * C], const float
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const float d = ref[r * C + c] - ring[(PH + r) & 7][c];
-            s = fmaf(d, d, s);
+            s = __fadd_rn(s, __fmul_rn(d, d));
         }
     return s;
 }
@@ -643,14 +645,14 @@ __global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch
     for (int r = 0; r < P; ++r) col_first += cur[r * C];
     const float patch_luma = reduce8(g, col_first) / 64.0f;
     const float bins = static_cast<float>(kCurveBins);
-    const float curve_pos = fminf(fmaxf(patch_luma * bins - 0.5f, 0.0f), bins - 1.0f);
+    const float curve_pos = fminf(fmaxf(__fsub_rn(__fmul_rn(patch_luma, bins), 0.5f), 0.0f), bins - 1.0f);
     const uint32_t lower = min(static_cast<uint32_t>(curve_pos), static_cast<uint32_t>(kCurveBins - 2));
     const float fraction = curve_pos - static_cast<float>(lower);
     const bool curve_valid = __ldg(a.noise + a.curve_valid_word) != 0.0f;
     float ratio = 0.0f;
     if (curve_valid) {
         const float lo = __ldg(a.noise_curve + lower), hi = __ldg(a.noise_curve + lower + 1);
-        ratio = lo + (hi - lo) * fraction;
+        ratio = __fadd_rn(lo, __fmul_rn(__fsub_rn(hi, lo), fraction));
     }
     const float luma_scale = curve_valid ? fminf(fmaxf(ratio, 0.33f), 3.0f) : 1.0f;
     const float first_lambda = a.lambda_ht * luma_scale;

@@ -103,6 +103,7 @@ struct MotionLaunch {
     int blksize, overlap, search_radius, coarse_radius, coarse_block_factor, levels;
     int mv_stride, conf_stride, sad_floor_word;
     float thsad;
+    int seeded;  // 1: the field already holds every block's seed; no coarse pass
 };
 
 int64_t pyramid_slot_pixels(int width, int height, int level);
@@ -112,6 +113,14 @@ int64_t pyramid_floats(int width, int height, int frame_count, int levels);
 cudaError_t launch_pyramid_build(const float* ring, int channels, int width, int height, int frame_count,
                                  int ring_slot, int levels, float* pyramid, int pyramid_slot, cudaStream_t stream);
 cudaError_t launch_motion_search(const MotionLaunch& args, cudaStream_t stream);
+
+// motion/kernels/chain.rs (`mc_chain_compose`): every neighbour's seed as the walk of pair vectors
+// from the centre. Neighbour n is logical position n (n < centre) or n + 1 of a 2d+1 window; the pair
+// between logical g and g+1 sits in pair slot (head_mod + g) mod 2d, direction 0 older-to-newer and
+// 1 newer-to-older, `dir_stride` values apart, `slot_stride` per slot.
+cudaError_t launch_chain_compose(const int32_t* pair_ring, int32_t* mv_field, int mv_stride, int centre, int d,
+                                 int head_mod, int dir_stride, int slot_stride, int step, int width, int height,
+                                 int blocks_x, int blocks_y, cudaStream_t stream);
 
 // Immerkær spatial noise estimate (immerkaer.cu) of one f32 frame (`channels` interleaved):
 // per 32x8 block partials (2 lanes each), optional frame totals (2 floats) and optional per-channel

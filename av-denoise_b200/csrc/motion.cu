@@ -483,8 +483,9 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     const int step = m.blksize - m.overlap;
     const int blocks_x = (m.width + step - 1) / step > 1 ? (m.width + step - 1) / step : 1;
     const int blocks_y = (m.height + step - 1) / step > 1 ? (m.height + step - 1) / step : 1;
-    const bool seeded = m.levels > 1;
-    if (seeded) {
+    const bool coarse = m.levels > 1 && !m.seeded;
+    const bool seeded = coarse || m.seeded;
+    if (coarse) {
         const int level = m.levels - 1;
         const int scale = 1 << level;
         SearchArgs a{};
@@ -533,6 +534,48 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     if (a.L.blksize > kMaxBlk) return cudaErrorInvalidValue;
     dim3 grid(blocks_x, blocks_y, m.neighbours);
     return dispatch_search(m.search_radius, false, a, grid, s);
+}
+
+namespace {
+__global__ void chain_compose_kernel(const int32_t* __restrict__ pair_ring, int32_t* __restrict__ mv_field,
+                                     int mv_stride, int centre, int d, int head_mod, int dir_stride,
+                                     int slot_stride, int step, int width, int height, int blocks_x, int blocks_y) {
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y, n = blockIdx.z;
+    if (bx >= blocks_x || by >= blocks_y) return;
+    const int logical = n < centre ? n : n + 1;
+    const int k = logical - centre;
+    const bool forward = k > 0;
+    const int steps = forward ? k : -k;
+    const int slots = 2 * d;
+    const int start_gap = forward ? centre : centre - 1;
+    const int start = ((head_mod + start_gap) % slots + slots) % slots;
+    int pos_x = bx * step + step / 2, pos_y = by * step + step / 2;
+    int acc_x = 0, acc_y = 0;
+    for (int i = 0; i < steps; ++i) {
+        const int slot = forward ? (start + i) % slots : (start + slots - i) % slots;
+        const int cx = clamp_to(pos_x, width), cy = clamp_to(pos_y, height);
+        const int hc = min(cx / step, blocks_x - 1), hr = min(cy / step, blocks_y - 1);
+        const int base = slot * slot_stride + (forward ? 0 : dir_stride) + (hr * blocks_x + hc) * 2;
+        const int hop_x = pair_ring[base], hop_y = pair_ring[base + 1];
+        acc_x += hop_x;
+        acc_y += hop_y;
+        pos_x += hop_x;
+        pos_y += hop_y;
+    }
+    int32_t* out = mv_field + static_cast<int64_t>(n) * mv_stride + (by * blocks_x + bx) * 2;
+    out[0] = acc_x;
+    out[1] = acc_y;
+}
+}  // namespace
+
+cudaError_t launch_chain_compose(const int32_t* pair_ring, int32_t* mv_field, int mv_stride, int centre, int d,
+                                 int head_mod, int dir_stride, int slot_stride, int step, int width, int height,
+                                 int blocks_x, int blocks_y, cudaStream_t s) {
+    if (d < 1) return cudaErrorInvalidValue;
+    dim3 grid((blocks_x + 63) / 64, blocks_y, 2 * d);
+    chain_compose_kernel<<<grid, 64, 0, s>>>(pair_ring, mv_field, mv_stride, centre, d, head_mod, dir_stride,
+                                             slot_stride, step, width, height, blocks_x, blocks_y);
+    return cudaGetLastError();
 }
 
 }  // namespace avd

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 
@@ -78,8 +79,28 @@ AvdStatus avd_motion_search(const AvdMotionPass* p, void* stream) {
     m.conf_stride = static_cast<int>(p->conf_stride);
     m.sad_floor_word = static_cast<int>(p->sad_floor_word);
     m.thsad = p->thsad;
+    m.seeded = p->seeded ? 1 : 0;
     cudaError_t e = avd::launch_motion_search(m, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("motion search launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+AvdStatus avd_chain_compose(uint64_t pair_ring, uint64_t mv_field, uint32_t mv_stride, uint32_t centre,
+                            uint32_t temporal_radius, uint32_t head_mod, uint32_t dir_stride, uint32_t width,
+                            uint32_t height, uint32_t blksize, uint32_t overlap, void* stream) {
+    if (!pair_ring || !mv_field) return fail(AVD_ERR_NULL_ARG, "chain compose: null buffer");
+    if (temporal_radius < 1 || temporal_radius > avd::kMaxTemporalRadius || centre > 2 * temporal_radius ||
+        overlap >= blksize || width == 0 || height == 0)
+        return fail(AVD_ERR_INVALID_OPTIONS, "chain compose: bad window or geometry");
+    const int step = static_cast<int>(blksize - overlap);
+    const int bx = std::max<int>((static_cast<int>(width) + step - 1) / step, 1);
+    const int by = std::max<int>((static_cast<int>(height) + step - 1) / step, 1);
+    cudaError_t e = avd::launch_chain_compose(
+        reinterpret_cast<const int32_t*>(pair_ring), reinterpret_cast<int32_t*>(mv_field), static_cast<int>(mv_stride),
+        static_cast<int>(centre), static_cast<int>(temporal_radius), static_cast<int>(head_mod),
+        static_cast<int>(dir_stride), 2 * static_cast<int>(dir_stride), step, static_cast<int>(width),
+        static_cast<int>(height), bx, by, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("chain compose launch: ") + cudaGetErrorString(e));
     return AVD_OK;
 }
 

@@ -55,11 +55,10 @@ class Nl4dPass final : public Pass {
             return Failure{AVD_ERR_INVALID_OPTIONS,
                            "motion search escalation is not available in this build; set max_search_escalation "
                            "to search_radius"};
+        // motion/search.rs:133-139: Auto resolves to Chained { refine_radius: 2 } at d >= 3.
         const bool chained = m.estimation == AVD_ESTIMATION_CHAINED ||
                              (m.estimation == AVD_ESTIMATION_AUTO && o.temporal_radius >= kChainedRadiusThreshold);
-        if (chained)
-            return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "chained motion estimation is not available in this build; use estimation Direct"};
+        const uint32_t refine_radius = m.estimation == AVD_ESTIMATION_CHAINED ? m.refine_radius : kDefaultRefineRadius;
         if (width < kPatch || height < kPatch) {
             char msg[200];
             std::snprintf(msg, sizeof(msg),
@@ -85,6 +84,8 @@ class Nl4dPass final : public Pass {
         p->mv_stride_ = static_cast<int>(pad8(2LL * p->blocks_x_ * p->blocks_y_));
         p->conf_stride_ = static_cast<int>(pad8(static_cast<int64_t>(p->blocks_x_) * p->blocks_y_));
         p->thsad_ = avd_thsad(m.blksize, o.thsad_scale);
+        p->chained_ = chained;
+        p->refine_radius_ = static_cast<int>(refine_radius);
         if (auto f = p->allocate()) return f;
         *result = std::move(p);
         return std::nullopt;
@@ -207,6 +208,12 @@ class Nl4dPass final : public Pass {
         const size_t nbrs = 2 * d_;
         if ((e = mv_.alloc(nbrs * mv_stride_ * sizeof(int32_t))) != cudaSuccess) return gpu_failure("motion field", e);
         if ((e = conf_.alloc(nbrs * conf_stride_ * sizeof(float))) != cudaSuccess) return gpu_failure("confidence", e);
+        if (chained_) {
+            // motion/context.rs:110-140: 2d pair slots of two directions, each a padded field.
+            if ((e = pair_ring_.alloc(nbrs * 2 * mv_stride_ * sizeof(int32_t))) != cudaSuccess)
+                return gpu_failure("pair ring", e);
+            if ((e = cudaMemset(pair_ring_.ptr, 0, pair_ring_.bytes)) != cudaSuccess) return gpu_failure("pair ring", e);
+        }
         if ((e = accum_.alloc(fe * t * sizeof(int32_t))) != cudaSuccess) return gpu_failure("accumulator ring", e);
         if ((e = wsum_.alloc(pixels() * t * sizeof(int32_t))) != cudaSuccess) return gpu_failure("weight ring", e);
         const size_t refs = static_cast<size_t>((width_ - kPatch + 3) / 4 + 1) * ((height_ - kPatch + 3) / 4 + 1);
@@ -307,6 +314,7 @@ class Nl4dPass final : public Pass {
                                       plane_format(in_), bias(), stream);
         if (e != cudaSuccess) return gpu_failure("ingest launch", e);
         if (auto f = build_pyramid(slot)) return f;
+        if (auto f = pair_analyse(slot)) return f;
         slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
         ring_head_ += 1;
         if (frames_loaded_ < tf()) frames_loaded_ += 1;
@@ -322,11 +330,58 @@ class Nl4dPass final : public Pass {
                                             cudaMemcpyDeviceToDevice, stream);
             if (e != cudaSuccess) return gpu_failure("slot copy", e);
             if (auto f = build_pyramid(next)) return f;
+            if (chained_) {
+                // nlmeans/denoiser/stages.rs:201-209: a duplicated frame's pair is zero motion.
+                int32_t* pair = pair_ring_.as<int32_t>() + (ring_head_ % (2 * d_)) * 2 * mv_stride_;
+                if ((e = cudaMemsetAsync(pair, 0, 2 * mv_stride_ * sizeof(int32_t), stream)) != cudaSuccess)
+                    return gpu_failure("pair clear", e);
+            }
             slot_frames_[next] = slot_frames_[last];
             ring_head_ += 1;
             frames_loaded_ += 1;
         }
         return std::nullopt;
+    }
+
+    // nlmeans/denoiser/stages.rs:146-197 with motion/chain.rs:18-96: both directions between the
+    // frame just written and the one before it, into pair slot ring_head mod 2d (before the head
+    // advances). A stream's first frame has no older partner.
+    std::optional<Failure> pair_analyse(size_t newer) {
+        if (!chained_ || ring_head_ == 0) return std::nullopt;
+        const size_t older = (newer + tf() - 1) % tf();
+        int32_t* pair = pair_ring_.as<int32_t>() + (ring_head_ % (2 * d_)) * 2 * mv_stride_;
+        for (int dir = 0; dir < 2; ++dir) {
+            MotionLaunch m = search_launch();
+            m.neighbour_slots = nullptr;
+            m.inline_slots[0] = static_cast<uint32_t>(dir == 0 ? newer : older);
+            m.centre_slot = static_cast<int>(dir == 0 ? older : newer);
+            m.neighbours = 1;
+            m.mv_field = pair + dir * mv_stride_;
+            m.confidence = nullptr;
+            cudaError_t e = launch_motion_search(m, stream);
+            if (e != cudaSuccess) return gpu_failure("pair analyse launch", e);
+        }
+        return std::nullopt;
+    }
+
+    MotionLaunch search_launch() const {
+        MotionLaunch m{};
+        m.pyramid = pyramid_.as<float>();
+        m.noise = noise_words();
+        m.width = static_cast<int>(width_);
+        m.height = static_cast<int>(height_);
+        m.frame_count = static_cast<int>(tf());
+        m.blksize = static_cast<int>(opts_.motion.blksize);
+        m.overlap = static_cast<int>(opts_.motion.overlap);
+        m.search_radius = static_cast<int>(opts_.motion.search_radius);
+        m.coarse_radius = m.search_radius;
+        m.coarse_block_factor = 1;
+        m.levels = static_cast<int>(opts_.motion.pyramid_levels);
+        m.mv_stride = mv_stride_;
+        m.conf_stride = conf_stride_;
+        m.sad_floor_word = kSadFloorWord;
+        m.thsad = thsad_;
+        return m;
     }
 
     // ---- passes ----------------------------------------------------------------------------
@@ -337,6 +392,28 @@ class Nl4dPass final : public Pass {
 
     // nlmeans/denoiser/machinery.rs:45-102 then dispatch/motion.rs:173-229.
     std::optional<Failure> machinery_at(uint32_t centre) {
+        if (chained_) {
+            // nlmeans/dispatch/motion.rs:138-171 then analyse.rs:273-316: every neighbour's seed
+            // chained from the pair ring, then refined `refine_radius` around it with confidence.
+            cudaError_t e = launch_chain_compose(pair_ring_.as<int32_t>(), mv_.as<int32_t>(), mv_stride_,
+                                                 static_cast<int>(centre), static_cast<int>(d_),
+                                                 static_cast<int>(ring_head_ % (2 * d_)), mv_stride_, 2 * mv_stride_,
+                                                 step_, static_cast<int>(width_), static_cast<int>(height_), blocks_x_,
+                                                 blocks_y_, stream);
+            if (e != cudaSuccess) return gpu_failure("chain compose launch", e);
+            MotionLaunch m = search_launch();
+            m.neighbour_slots = slot_table(centre);
+            m.mv_field = mv_.as<int32_t>();
+            m.confidence = conf_.as<float>();
+            m.centre_slot = static_cast<int>(phys(centre));
+            m.neighbours = static_cast<int>(2 * d_);
+            m.search_radius = refine_radius_;
+            m.coarse_radius = refine_radius_;
+            m.seeded = 1;
+            e = launch_motion_search(m, stream);
+            if (e != cudaSuccess) return gpu_failure("seeded refine launch", e);
+            return std::nullopt;
+        }
         MotionLaunch m{};
         m.pyramid = pyramid_.as<float>();
         m.neighbour_slots = slot_table(centre);
@@ -517,6 +594,9 @@ class Nl4dPass final : public Pass {
     int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2, conf_stride_ = 1;
 
     DeviceBuffer ring_, pyramid_, mv_, conf_, accum_, wsum_, group_weight_, members_, tables_, slot_tables_;
+    DeviceBuffer pair_ring_;
+    bool chained_ = false;
+    int refine_radius_ = 2;
     DeviceBuffer outputs_[2];
 
     size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;

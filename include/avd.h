@@ -411,9 +411,21 @@ typedef struct AvdMotionPass {
     uint32_t blksize, overlap, search_radius, levels;
     uint32_t mv_stride, conf_stride, sad_floor_word;
     float thsad; /* av-denoise-core/src/motion/confidence.rs:27-30; must be > 0 with confidence */
+    uint32_t seeded; /* 1: `mv_field` already holds each block's seed and the search skips the coarse
+                      * pass, as `run_seeded_refine` does (motion/analyse.rs:273-316) */
 } AvdMotionPass;
 
 AVD_API AvdStatus avd_motion_search(const AvdMotionPass* pass, void* stream);
+
+/* av-denoise-core/src/nlmeans/dispatch/motion.rs:619-690 (`run_chain_compose`) with
+ * motion/kernels/chain.rs:20-72: every neighbour's seed of a pass centred on logical `centre` of a
+ * 2d+1 window, walked through the pair ring from the centre (neighbour n is logical n, or n + 1 past
+ * the centre). The pair between logical g and g+1 is in slot (head_mod + g) mod 2d; each slot holds
+ * the older-to-newer field, then the newer-to-older field, `dir_stride` i32 apart. Writes
+ * `mv_field` (2d neighbours, `mv_stride` apart). Queued on `stream`. */
+AVD_API AvdStatus avd_chain_compose(uint64_t pair_ring, uint64_t mv_field, uint32_t mv_stride, uint32_t centre,
+                                    uint32_t temporal_radius, uint32_t head_mod, uint32_t dir_stride, uint32_t width,
+                                    uint32_t height, uint32_t blksize, uint32_t overlap, void* stream);
 
 /* av-denoise-core/src/motion/confidence.rs:17-21 (`sad_noise_floor`). */
 AVD_API float avd_sad_noise_floor(uint32_t blksize, float sigma);

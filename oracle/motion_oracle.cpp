@@ -7,7 +7,9 @@
 //   coarse:  motion/kernels/block_match.rs:117-215 and motion/analyse.rs:100-150 (the smallest
 //            level, blksize max(b/2^l, 2), step max(s/2^l, 1), winner x 2^l seeds the fine blocks
 //            of its region, the last coarse block reaching the fine grid's edge);
-//   fine:    block_match.rs:274-351 and 490-521 (seeded window, confidence);
+//   fine:    block_match.rs:274-351 and 490-521 (seeded window, confidence); with `seeded` the field
+//            already holds the seeds and the coarse pass is skipped (analyse.rs:273-316, the
+//            refine of chained seeds);
 //   window:  block_match.rs:656-849 (clamped staging, SAD summed row by row left to right, lowest
 //            SAD with the first row-major index, the window's centre winning a tie, SADs at or
 //            above 1e30 never chosen).
@@ -108,6 +110,7 @@ struct OrcMotionArgs {
     uint32_t blksize, overlap, search_radius, levels;
     uint32_t mv_stride, conf_stride, sad_floor_word;
     float thsad;
+    uint32_t seeded;  // 1: mv_field holds the seeds; no coarse pass (motion/analyse.rs:273-316)
 };
 
 int64_t orc_motion_pyramid_floats(int w, int h, int frames, int levels) { return level_base(w, h, frames, levels); }
@@ -139,8 +142,9 @@ void orc_motion_search(const OrcMotionArgs* a) {
     const int bx_n = (w + step - 1) / step > 1 ? (w + step - 1) / step : 1;
     const int by_n = (h + step - 1) / step > 1 ? (h + step - 1) / step : 1;
     const int R = static_cast<int>(a->search_radius);
-    const bool seeded = a->levels > 1;
-    if (seeded) {
+    const bool coarse = a->levels > 1 && !a->seeded;
+    const bool seeded = coarse || a->seeded;
+    if (coarse) {
         const int level = static_cast<int>(a->levels) - 1, scale = 1 << level;
         Level L{};
         level_dims(w, h, level, &L.width, &L.height);

@@ -282,7 +282,7 @@ class MotionArgs(C.Structure):
         ("confidence", _fp), ("noise", _fp),
     ] + [(n, C.c_uint32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize",
                                    "overlap", "search_radius", "levels", "mv_stride", "conf_stride",
-                                   "sad_floor_word")] + [("thsad", C.c_float)]
+                                   "sad_floor_word")] + [("thsad", C.c_float), ("seeded", C.c_uint32)]
 
 
 def motion_pyramid(ring: np.ndarray, channels: int, width: int, height: int, levels: int) -> np.ndarray:
@@ -301,13 +301,14 @@ def motion_pyramid(ring: np.ndarray, channels: int, width: int, height: int, lev
 
 def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
                   *, blksize=16, overlap=8, search_radius=4, levels=2, confidence=False, sad_floor=0.0,
-                  thsad=0.0):
-    """One block-matching search (no camera model, no truemotion). Returns (mv (n, blocks, 2), conf)."""
+                  thsad=0.0, seeds: np.ndarray | None = None):
+    """One block-matching search (no camera model, no truemotion). Returns (mv (n, blocks, 2), conf).
+    With `seeds` (n, blocks, 2) the search refines around them and skips the coarse pass."""
     step = blksize - overlap
     bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
     slots = np.ascontiguousarray(neighbour_slots, np.uint32)
     n = slots.size
-    mv = np.zeros(n * bx * by * 2, np.int32)
+    mv = np.zeros(n * bx * by * 2, np.int32) if seeds is None else np.ascontiguousarray(seeds, np.int32).reshape(-1).copy()
     conf = np.zeros(n * bx * by, np.float32)
     noise = np.array([sad_floor], np.float32)
     a = MotionArgs()
@@ -318,6 +319,7 @@ def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, cen
     a.width, a.height, a.frame_count, a.centre_slot, a.neighbours = width, height, frames, centre_slot, n
     a.blksize, a.overlap, a.search_radius, a.levels = blksize, overlap, search_radius, levels
     a.mv_stride, a.conf_stride, a.sad_floor_word, a.thsad = bx * by * 2, bx * by, 0, thsad
+    a.seeded = int(seeds is not None)
     l = lib()
     l.orc_motion_search.argtypes = [C.POINTER(MotionArgs)]
     l.orc_motion_search(C.byref(a))
@@ -348,9 +350,34 @@ def collab_normalise(accum: np.ndarray, wsum: np.ndarray, channels: int) -> np.n
     return np.where(w != 0, v, acc).astype(np.float32)
 
 
+def chain_compose(pairs: dict, centre: int, d: int, head_mod: int, step: int, width: int, height: int, bx: int,
+                  by: int) -> np.ndarray:
+    """motion/kernels/chain.rs: every neighbour's seed walked through the pair ring from the centre;
+    `pairs[slot]` holds (older-to-newer, newer-to-older) fields of (blocks, 2)."""
+    slots = 2 * d
+    seeds = np.zeros((2 * d, bx * by, 2), np.int32)
+    for n in range(2 * d):
+        logical = n if n < centre else n + 1
+        k = logical - centre
+        forward = k > 0
+        start = (head_mod + (centre if forward else centre - 1)) % slots
+        for b in range(bx * by):
+            px, py = (b % bx) * step + step // 2, (b // bx) * step + step // 2
+            ax = ay = 0
+            for i in range(abs(k)):
+                slot = (start + i) % slots if forward else (start + slots - i) % slots
+                cx, cy = min(max(px, 0), width - 1), min(max(py, 0), height - 1)
+                hb = min(cy // step, by - 1) * bx + min(cx // step, bx - 1)
+                hop = pairs[slot][0 if forward else 1][hb]
+                ax, ay, px, py = ax + int(hop[0]), ay + int(hop[1]), px + int(hop[0]), py + int(hop[1])
+            seeds[n, b] = (ax, ay)
+    return seeds
+
+
 def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, overlap=8, search_radius=4,
                 levels=2, refine=2, spatial_radius=9, lambda_ht=4.158, c_min=0.05, kaiser_beta=2.0,
-                pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0) -> list[np.ndarray]:
+                pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0, chained: bool = False,
+                refine_radius: int = 2) -> list[np.ndarray]:
     """The NL4D engine with a pinned sigma and Direct motion (no camera model, no truemotion) over a
     stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order.
 
@@ -392,9 +419,15 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         st["passes"] += 1
         slots = [phys(l) for l in range(tf) if l != centre]
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
-        mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
-                                 search_radius=search_radius, levels=levels, confidence=True,
-                                 sad_floor=sad_floor, thsad=th)
+        if chained:
+            seeds = chain_compose(pairs, centre, d, st["head"] % (2 * d), step, w, h, bx, by)
+            mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
+                                     search_radius=refine_radius, levels=levels, confidence=True,
+                                     sad_floor=sad_floor, thsad=th, seeds=seeds)
+        else:
+            mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
+                                     search_radius=search_radius, levels=levels, confidence=True,
+                                     sad_floor=sad_floor, thsad=th)
         acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
                                   confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
                                   c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
@@ -411,9 +444,23 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         zeroed[slot] = True
         return out
 
+    pairs = {i: (np.zeros((bx * by, 2), np.int32), np.zeros((bx * by, 2), np.int32)) for i in range(2 * d)}
+
+    def pair_analyse(newer):
+        # nlmeans/denoiser/stages.rs:146-197: both directions into pair slot head mod 2d.
+        if not chained or st["head"] == 0:
+            return
+        older = (newer + tf - 1) % tf
+        pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
+        kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels)
+        fwd, _ = motion_search(pyr, w, h, tf, older, [newer], **kw)
+        bwd, _ = motion_search(pyr, w, h, tf, newer, [older], **kw)
+        pairs[st["head"] % (2 * d)] = (fwd[0], bwd[0])
+
     def push(frame):
         s = st["head"] % tf
         ring[s] = frame
+        pair_analyse(s)
         slot_frames[s] = st["real"]
         st["head"] += 1
         st["loaded"] = min(st["loaded"] + 1, tf)
@@ -440,6 +487,8 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         while st["loaded"] < tf:
             last, nxt = (st["head"] - 1) % tf, st["head"] % tf
             ring[nxt] = ring[last]
+            if chained:
+                pairs[st["head"] % (2 * d)] = (np.zeros((bx * by, 2), np.int32), np.zeros((bx * by, 2), np.int32))
             slot_frames[nxt] = slot_frames[last]
             st["head"] += 1
             st["loaded"] += 1

@@ -84,9 +84,8 @@ def test_gpu_matches_recorded_digest(oracle, label):
     kw = dict(case)
     o_acc, o_ws, o_gw = oracle.collab_fused(kw.pop("ring"), kw.pop("width"), kw.pop("height"), kw.pop("channels"),
                                             **kw)
-    assert np.array_equal(wsum != 0, o_ws != 0)
-    got = np.where(wsum != 0, accum * 5.0 / np.where(wsum != 0, wsum, 1), 0.0)
-    want = np.where(o_ws != 0, o_acc * 5.0 / np.where(o_ws != 0, o_ws, 1), 0.0)
-    close = np.abs(got - want) <= 1e-4
-    print(label, "pixels within 1e-4 of the oracle:", close.mean(), "max diff", np.abs(got - want).max())
-    assert close.mean() >= 0.999
+    # Against the oracle: the kernels round every multiply and add as the restatement does and
+    # aggregate in integers, so the accumulators and group weights are identical.
+    assert np.array_equal(accum, o_acc)
+    assert np.array_equal(wsum, o_ws)
+    assert np.array_equal(gw.view(np.uint32), o_gw.view(np.uint32))

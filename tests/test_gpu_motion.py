@@ -73,3 +73,68 @@ def test_motion_search_matches_oracle_bit_for_bit(lib, oracle, case):
     if confidence:
         assert np.array_equal(conf.view(np.uint32), o_conf.view(np.uint32))
         assert 0.0 <= conf.min() and conf.max() <= 1.0
+
+
+def test_seeded_refine_matches_oracle(lib, oracle):
+    """The seeded search of the chained refine: no coarse pass, the window centred on each block's
+    seed (motion/analyse.rs:273-316), bit for bit."""
+    import torch
+
+    from av_denoise_b200 import _abi
+
+    w, h, frames, levels, blksize, overlap, radius = 120, 80, 3, 2, 16, 8, 2
+    ring = moving_window(w, h, frames, seed=77)
+    o_pyr = oracle.motion_pyramid(ring, 1, w, h, levels)
+    step = blksize - overlap
+    bx, by = -(-w // step), -(-h // step)
+    rng = np.random.default_rng(5)
+    seeds = rng.integers(-6, 7, (2, bx * by, 2)).astype(np.int32)
+    floor, th = oracle.sad_noise_floor(blksize, 0.02), oracle.thsad(blksize, 1.0)
+    o_mv, o_conf = oracle.motion_search(o_pyr, w, h, frames, 1, [0, 2], blksize=blksize, overlap=overlap,
+                                        search_radius=radius, levels=levels, confidence=True, sad_floor=floor,
+                                        thsad=th, seeds=seeds)
+    pyr = torch.from_numpy(o_pyr).cuda()
+    slots = torch.tensor([0, 2], dtype=torch.int32, device="cuda")
+    mv = torch.from_numpy(seeds.reshape(-1).copy()).cuda()
+    conf = torch.zeros(2 * bx * by, device="cuda")
+    noise = torch.tensor([floor], device="cuda")
+    p = _abi.AvdMotionPass()
+    p.pyramid, p.neighbour_slots, p.mv_field, p.confidence, p.noise = (pyr.data_ptr(), slots.data_ptr(),
+                                                                         mv.data_ptr(), conf.data_ptr(),
+                                                                         noise.data_ptr())
+    p.width, p.height, p.frame_count, p.centre_slot, p.neighbours = w, h, frames, 1, 2
+    p.blksize, p.overlap, p.search_radius, p.levels = blksize, overlap, radius, levels
+    p.mv_stride, p.conf_stride, p.sad_floor_word, p.thsad, p.seeded = bx * by * 2, bx * by, 0, th, 1
+    assert lib.avd_motion_search(C.byref(p), C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(mv.cpu().numpy().reshape(2, -1, 2), o_mv)
+    assert np.array_equal(conf.cpu().numpy().view(np.uint32), o_conf.reshape(-1).view(np.uint32))
+
+
+@pytest.mark.parametrize("w,h,d,centre,head_mod", [(96, 64, 2, 2, 0), (96, 64, 2, 0, 3), (96, 64, 2, 4, 1),
+                                                   (61, 37, 3, 5, 2), (61, 37, 3, 1, 5)])
+def test_chain_compose_matches_oracle(lib, oracle, w, h, d, centre, head_mod):
+    """The chained seeds: every neighbour's walk through the pair ring (motion/kernels/chain.rs), with
+    pair vectors large enough to leave the frame."""
+    import torch
+
+    blksize, overlap = 16, 8
+    step = blksize - overlap
+    bx, by = -(-w // step), -(-h // step)
+    rng = np.random.default_rng(w + d + centre)
+    pairs = {i: (rng.integers(-9, 10, (bx * by, 2)).astype(np.int32),
+                 rng.integers(-9, 10, (bx * by, 2)).astype(np.int32)) for i in range(2 * d)}
+    stride = bx * by * 2 + 6
+    ring = np.zeros((2 * d, 2, stride), np.int32)
+    for i in range(2 * d):
+        ring[i, 0, :bx * by * 2] = pairs[i][0].reshape(-1)
+        ring[i, 1, :bx * by * 2] = pairs[i][1].reshape(-1)
+    dev = torch.from_numpy(ring.reshape(-1)).cuda()
+    mv = torch.zeros(2 * d * stride, dtype=torch.int32, device="cuda")
+    st = lib.avd_chain_compose(dev.data_ptr(), mv.data_ptr(), stride, centre, d, head_mod, stride, w, h, blksize,
+                               overlap, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0, lib.avd_last_error().decode()
+    torch.cuda.synchronize()
+    got = mv.cpu().numpy().reshape(2 * d, stride)[:, :bx * by * 2].reshape(2 * d, bx * by, 2)
+    want = oracle.chain_compose(pairs, centre, d, head_mod, step, w, h, bx, by)
+    assert np.array_equal(got, want), np.argwhere(got != want)[:5]

@@ -1,10 +1,10 @@
-"""The NL4D engine (pinned sigma, Direct motion) on the GPU through the C ABI against the oracle's
-stream restatement: the same ring, pass schedule, motion search, group filter and normalise.
+"""The NL4D engine (pinned sigma; Direct and Chained motion) on the GPU through the C ABI against the
+oracle's stream restatement: the same ring, pass schedule, motion search, pair fields and chains,
+group filter and normalise.
 
-Motion vectors and confidences are bit-exact between the two; the group filter's f32 transforms
-differ in the last bits, which the fixed-point accumulators carry into outputs within about 3e-5
-(normalised) of each other. So a sample whose oracle value sits within 1e-4 of a rounding boundary
-is a tie, and the bar is the engine's: no sample more than 1 LSB apart, 99.9% of the rest identical."""
+Every stage is bit-exact between the two (the motion sums in the reference's order, the filter with
+every multiply and add rounded as the restatement rounds them, integer aggregation, the same
+normalise), so every output sample is identical."""
 
 import numpy as np
 import pytest
@@ -46,7 +46,8 @@ def check(oracle, got_planes, frames, fmt, d, sigma, chroma=False, context=0, **
     for g, wn, ex in zip(got_planes, want, exact):
         for c in range(len(wn)):
             par.add(g[c], wn[c], ex[..., c], fmt.max_value(), tie_band=NL4D_TIE_BAND)
-    st = par.check(min_raw=0.995)
+    st = par.check(min_identical=1.0, min_raw=1.0)
+    assert st["max_lsb"] == 0, st
     print(st)
     return st
 
@@ -116,6 +117,29 @@ def test_nl4d_options_this_build_rejects():
     g = avd.Geometry(64, 48, avd.ChromaLayout.GRAY, fmt, fmt)
     with pytest.raises(avd.InvalidOptions, match="automatic noise estimate"):
         avd.build_engine(avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=1), None, g))
-    chained = avd.Nl4dOptions(sigma=0.03, temporal_radius=3)
-    with pytest.raises(avd.InvalidOptions, match="chained"):
-        avd.build_engine(avd.EngineSpec.nl4d(chained, None, g))
+    escalating = avd.Nl4dOptions(sigma=0.03, temporal_radius=1, motion=avd.MotionSearch(max_search_escalation=8))
+    with pytest.raises(avd.InvalidOptions, match="escalation"):
+        avd.build_engine(avd.EngineSpec.nl4d(escalating, None, g))
+
+
+@pytest.mark.parametrize("n,d,estimation,refine_radius,context", [
+    (9, 3, avd.MotionEstimation.AUTO, 2, 0),      # Auto resolves to Chained { refine_radius: 2 } at d >= 3
+    (7, 2, avd.MotionEstimation.CHAINED, 1, 0),
+    (4, 3, avd.MotionEstimation.AUTO, 2, 0),      # shorter than the ring: duplicated frames' pairs are zero
+    (8, 2, avd.MotionEstimation.CHAINED, 3, 2),   # continuation
+    (8, 2, avd.MotionEstimation.CHAINED, 3, 0),
+    (8, 2, avd.MotionEstimation.CHAINED, 2, 2),
+])
+def test_nl4d_chained_matches_oracle(oracle, n, d, estimation, refine_radius, context):
+    """Chained estimation: pair fields between adjacent frames on every push, every neighbour's seed
+    walked from the centre through them, then refined with confidence (motion/chain.rs,
+    kernels/chain.rs, analyse.rs:273-316)."""
+    w, h, sigma = 96, 64, 10.0 / 255
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, n, seed=40 + n + d)
+    o = avd.Nl4dOptions(sigma=sigma, temporal_radius=d, spatial_radius=4,
+                        motion=avd.MotionSearch(estimation=estimation, refine_radius=refine_radius))
+    spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames, context=context)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, context=context, spatial_radius=4,
+          chained=True, refine_radius=refine_radius)
