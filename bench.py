@@ -501,6 +501,65 @@ def run_nl4d(pushes: int, size: str) -> None:
                       "push_ms": [round(t, 3) for t in times]}))
 
 
+def run_nl4d_4k(pushes: int) -> None:
+    """NL4D on the 4K workload: 3840x2160 4:2:0 10-bit, luma and chroma in one engine, 7-frame window
+    (d=3, Auto estimation resolves to Chained), spatial radius 16, hard threshold 2.7 (lambda_ht 2.7,
+    scale 1, pooled threshold and noise map off), motion at its defaults. Synthetic frames: the
+    gratings/rectangles/texture base in 10-bit codes, 12 sprites at integer velocities up to 8
+    px/frame, Gaussian noise of 20 codes plus signal-dependent variance 0.02 * value; sigma pinned
+    at 20 codes (the automatic estimate is not built). Eight generated frames are cycled. Prints
+    the device time of every push and the steady-state median as one JSON line."""
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import synth
+
+    w, h, depth, d = 3840, 2160, 10, 3
+    fmt = avd.SampleFormat.u16(depth)
+    sigma = 20.0 / 1023.0
+    o = avd.Nl4dOptions(sigma=sigma, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
+                        pooled_threshold=False, noise_map=False)
+    geo = avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt)
+    eng = avd.build_engine(avd.EngineSpec.nl4d(o, o, geo))
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    clip = synth.make_clip(w, h, 8, depth=depth, chroma="420", sigma_luma=20.0 / 4.0, sigma_chroma=20.0 / 4.0,
+                           sprites=12, sprite_speed=8, signal_dependent=0.02, seed=2000)
+    dims = [geo.plane_dims(i) for i in range(3)]
+    bufs = []
+    for f in clip:
+        planes = []
+        for p, (pw, ph) in zip(f, dims):
+            flat = p.reshape(-1).astype(np.uint16)
+            planes.append(torch.from_numpy(np.concatenate([flat, np.zeros(flat.size % 2, np.uint16)]).view(np.int32)).cuda())
+        bufs.append(planes)
+    outs = [torch.zeros_like(b) for b in bufs[0]]
+
+    def dp(ts):
+        return [avd.DevicePlane.from_tensor(t, pw, ph) for t, (pw, ph) in zip(ts, dims)]
+
+    times = []
+    for i in range(pushes):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ready = eng.push(dp(bufs[i % len(bufs)]))
+        for _ in range(ready):
+            eng.emit_into(dp(outs))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    eng.close()
+    steady = times[2 * d + 1:]
+    ms = float(np.median(steady))
+    print(json.dumps({"workload": "NL4D 3840x2160 4:2:0 10-bit luma+chroma, d=3 (Chained), spatial_radius 16, "
+                                  "lambda_ht 2.7, plain threshold, sigma pinned at 20 codes",
+                      "ms_per_frame": round(ms, 3), "frames_per_s": round(1000.0 / ms, 2),
+                      "push_ms": [round(t, 2) for t in times]}))
+
+
 def run_adjoint(reps: int) -> None:
     """The NLMeans adjoint (`avd_nlm_backward`) against its forward on the same window: 1920x1080
     luma, d=2, a=5, s=2, strength 8, fast variant. The forward is the engine's push (ingest + the
@@ -675,6 +734,8 @@ def main() -> None:
     ap.add_argument("--nl4d", type=int, default=0, metavar="PUSHES",
                     help="time PUSHES pushes of the NL4D engine (secondary workload) and exit")
     ap.add_argument("--nl4d-size", default="1080", choices=["1080", "2160"])
+    ap.add_argument("--nl4d-4k", type=int, default=0, metavar="PUSHES",
+                    help="time PUSHES pushes of the 4K 4:2:0 10-bit NL4D workload (d=3) and exit")
     ap.add_argument("--adjoint", type=int, default=0, metavar="REPS",
                     help="time the NLMeans adjoint against its forward REPS times and exit")
     ap.add_argument("--batch", type=int, default=0, metavar="REPS",
@@ -690,6 +751,8 @@ def main() -> None:
         run_once()
     elif args.nl4d:
         run_nl4d(args.nl4d, args.nl4d_size)
+    elif args.nl4d_4k:
+        run_nl4d_4k(args.nl4d_4k)
     elif args.adjoint:
         run_adjoint(args.adjoint)
     elif args.batch:
