@@ -89,3 +89,31 @@ def test_gpu_matches_recorded_digest(oracle, label):
     assert np.array_equal(accum, o_acc)
     assert np.array_equal(wsum, o_ws)
     assert np.array_equal(gw.view(np.uint32), o_gw.view(np.uint32))
+
+
+@pytest.mark.parametrize("w,h,radius,sr,seed", [(96, 64, 2, 4, 1), (61, 45, 1, 9, 2), (80, 56, 2, 6, 3),
+                                                (96, 64, 0, 4, 4), (72, 40, 3, 5, 5)])
+def test_gpu_matches_oracle_on_random_passes(oracle, w, h, radius, sr, seed):
+    """Random textured frames, motion fields and confidences: the accumulators, weights and group
+    weights equal the oracle's exactly."""
+    rng = np.random.default_rng(seed)
+    frames = 2 * radius + 1
+    y, x = np.mgrid[0:h * frames, 0:w].astype(np.float32)
+    ring = np.clip(0.5 + 0.2 * np.sin(x * 0.3 + y * 0.11) + rng.normal(0, 0.05, (h * frames, w)), 0, 1)
+    case = dict(ring=ring.astype(np.float32).reshape(-1), width=w, height=h, channels=1, centre_slot=radius,
+                radius=radius, c_min=0.3, refine=2, spatial_radius=sr, k_max=8, sigma=(0.03,), lambda_ht=3.0,
+                rho=0.0, kaiser_beta=2.0)
+    if radius:
+        bx, by = -(-w // 8), -(-h // 8)
+        case.update(mv_field=rng.integers(-6, 7, 2 * radius * bx * by * 2).astype(np.int32),
+                    confidence=rng.uniform(0, 1, 2 * radius * bx * by).astype(np.float32),
+                    neighbour_slots=np.array([s for s in range(frames) if s != radius], np.uint32),
+                    mv_stride=bx * by * 2, conf_stride=bx * by, blocks_x=bx, blocks_y=by)
+    case["pooled"] = 2.42 / 4.158 if seed % 2 else None
+    accum, wsum, gw = run_gpu(case)
+    kw = dict(case)
+    o_acc, o_ws, o_gw = oracle.collab_fused(kw.pop("ring"), kw.pop("width"), kw.pop("height"), kw.pop("channels"),
+                                            **kw)
+    assert np.array_equal(wsum, o_ws)
+    assert np.array_equal(accum, o_acc)
+    assert np.array_equal(gw.view(np.uint32), o_gw.view(np.uint32))
