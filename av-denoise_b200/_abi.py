@@ -178,8 +178,16 @@ class AvdBatchJob(C.Structure):
                [(n, f32) for n in ("strength", "pair_offset", "spatial_offset")]
 
 
+class AvdHostTiming(C.Structure):
+    _fields_ = [("blocked", C.c_double), ("submit", C.c_double), ("frames", u64), ("has_luma", u32),
+                ("has_chroma", u32), ("luma_device_busy", C.c_double), ("chroma_device_busy", C.c_double)]
+
+
 _P = C.POINTER
 _E = C.c_void_p  # AvdEngine*
+_H = C.c_void_p  # AvdHost*
+# void (*AvdHostSink)(void* user, const void* const* planes, size_t n)
+AvdHostSink = C.CFUNCTYPE(None, C.c_void_p, _P(C.c_void_p), C.c_size_t)
 
 # name -> (restype, argtypes); the exact set of entry points include/avd.h declares.
 PROTOTYPES: dict[str, tuple] = {
@@ -210,6 +218,18 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_engine_last_error": (C.c_char_p, [_E]),
     "avd_engine_fail_for_test": (C.c_int, [_E]),
     "avd_last_error": (C.c_char_p, []),
+    "avd_host_create": (C.c_int, [_P(AvdEngineSpec), _P(AvdTuning), _P(_H)]),
+    "avd_host_destroy": (None, [_H]),
+    "avd_host_plane_bytes": (u64, [_H, C.c_size_t]),
+    "avd_host_push": (C.c_int, [_H, _P(C.c_void_p), _P(u64), C.c_size_t]),
+    "avd_host_push_priming": (C.c_int, [_H, _P(C.c_void_p), _P(u64), C.c_size_t]),
+    "avd_host_recv": (C.c_int, [_H, _P(C.c_void_p), C.c_size_t, _P(C.c_int)]),
+    "avd_host_flush": (C.c_int, [_H, AvdHostSink, C.c_void_p]),
+    "avd_host_reset": (None, [_H]),
+    "avd_host_last_error": (C.c_char_p, [_H]),
+    "avd_host_poison_for_test": (None, [_H]),
+    "avd_host_timing": (C.c_int, [_H, _P(AvdHostTiming)]),
+    "avd_host_sample_device_time": (None, [_H, u32]),
     "avd_collab_pass": (C.c_int, [_P(AvdCollabPass), C.c_void_p]),
     "avd_collab_member_bytes": (u64, [u32, u32]),
     "avd_dct_noise_profile": (None, [f32, _P(f32)]),

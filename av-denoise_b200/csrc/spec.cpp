@@ -424,6 +424,8 @@ const char* avd_status_message(AvdStatus status) {
         case AVD_ERR_NEEDS_RESET: return "an earlier call failed, reset the engine before using it again";
         case AVD_ERR_GPU: return "gpu error";
         case AVD_ERR_NULL_ARG: return "null argument";
+        case AVD_ERR_QUEUE_FULL: return "frames in flight must be collected before the next push";
+        case AVD_ERR_POISONED: return "an earlier call failed, reset the stream before using it again";
     }
     return "unknown status";
 }

@@ -453,6 +453,107 @@ def run_once() -> None:
     print("one luma NLM launch done")
 
 
+def run_host(frames: int) -> None:
+    """The host denoiser (wire bytes in, wire bytes out) against the same engine fed from HBM:
+    1920x1080 4:2:0 u8, luma NLMeans d=2 a=5 s=2 strength 8, chroma passed through. Pushes
+    `frames` frames with the push/recv pattern of the reference's host API and a flush, timed by the
+    host clock from the first push to the last frame handed back; the resident run times the same
+    pushes and emits with CUDA events. Prints one JSON line."""
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import synth
+
+    clip = synth.temporal_1080p_clip(frames=8, seed=11)
+    fmt = avd.SampleFormat.u8()
+    t = avd.NlmTuning(search_radius=LUMA["a"], patch_radius=LUMA["s"], strength=LUMA["strength"])
+    alg = avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(tuning=t, mode=avd.DenoisingMode.temporal(LUMA["d"])))
+    spec = avd.EngineSpec.nlmeans(alg, None, avd.Geometry(W, H, avd.ChromaLayout.YUV420, fmt, fmt))
+    wire = [[np.ascontiguousarray(p).tobytes() for p in f] for f in clip]
+
+    sinks = [bytearray(len(b)) for b in wire[0]]
+
+    def host_pass(den, lockstep):
+        """lockstep: `recv` (a fresh buffer set) after every push, the reference's doc example;
+        pipelined: `recv_into` caller-owned buffers only when the queue is full, keeping
+        MAX_PENDING frames in flight."""
+        got = 0
+        for k in range(frames):
+            planes = wire[k % len(wire)]
+            try:
+                den.push(planes)
+            except avd.QueueFull:
+                got += den.recv() is not None if lockstep else den.recv_into(sinks)
+                den.push(planes)
+            if lockstep and den.recv() is not None:
+                got += 1
+        out = []
+        den.flush(out.append)
+        return got + len(out)
+
+    host_times, host_split = {}, {}
+    for lockstep in (False, True):
+        den = avd.HostDenoiser(spec)
+        host_pass(den, lockstep)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            n = host_pass(den, lockstep)
+            ts.append(time.perf_counter() - t0)
+            assert n == frames
+        name = "lockstep" if lockstep else "pipelined"
+        host_times[name] = ts
+        tm = den.timing()
+        per = 1e3 / max(1, tm.frames)
+        host_split[name] = {"blocked_ms_per_frame": round(tm.blocked * per, 4),
+                            "submit_ms_per_frame": round(tm.submit * per, 4),
+                            "outside_calls_ms_per_frame": round((4 * sum(ts) / 3 * 1e3) / max(1, tm.frames)
+                                                                - (tm.blocked + tm.submit) * per, 4)}
+        den.close()
+
+    dims = [spec.geometry.plane_dims(i) for i in range(3)]
+    eng = avd.build_engine(spec)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    dev = [[torch.from_numpy(np.frombuffer(b + bytes((-len(b)) % 4), np.int32).copy()).cuda() for b in f]
+           for f in wire]
+    outb = [torch.zeros(plane_words(fmt, w, h), dtype=torch.int32, device="cuda") for (w, h) in dims]
+    planes = [[avd.DevicePlane.from_tensor(b, w, h) for b, (w, h) in zip(f, dims)] for f in dev]
+    out_planes = [avd.DevicePlane.from_tensor(b, w, h) for b, (w, h) in zip(outb, dims)]
+
+    def device_pass():
+        for k in range(frames):
+            for _ in range(eng.push(planes[k % len(planes)])):
+                eng.emit_into(out_planes)
+        for _ in range(eng.finish()):
+            eng.emit_into(out_planes)
+
+    device_pass()
+    torch.cuda.synchronize()
+    dev_times = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        device_pass()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dev_times.append(e0.elapsed_time(e1) / 1e3)
+    eng.close()
+    wire_bytes = sum(len(b) for b in wire[0])
+    dev_fps = frames / statistics.median(dev_times)
+    line = {"workload": "host denoiser: 1920x1080 4:2:0 u8, luma NLMeans d=2 a=5 s=2 strength 8, chroma passthrough",
+            "frames": frames, "resident_frames_per_s": round(dev_fps, 2),
+            "wire_bytes_per_frame_each_way": wire_bytes, "resident_ms": [round(x * 1e3, 2) for x in dev_times]}
+    for name, ts in host_times.items():
+        fps = frames / statistics.median(ts)
+        line[name] = {"frames_per_s": round(fps, 2), "over_resident": round(fps / dev_fps, 4),
+                      "ms": [round(x * 1e3, 2) for x in ts], **host_split[name]}
+    print(json.dumps(line))
+
+
 def run_nl4d(pushes: int, size: str) -> None:
     """The NL4D engine on one plane of synthetic content with a pinned sigma and Direct motion:
     1920x1080 u8 or 3840x2160 10-bit luma, d=2, spatial radius 9, defaults otherwise. Prints the
@@ -740,6 +841,8 @@ def main() -> None:
                     help="time the NLMeans adjoint against its forward REPS times and exit")
     ap.add_argument("--batch", type=int, default=0, metavar="REPS",
                     help="time the batched launch against the per-frame loop REPS times and exit")
+    ap.add_argument("--host", type=int, default=0, metavar="FRAMES",
+                    help="time FRAMES frames through the host denoiser against the resident engine and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -757,6 +860,8 @@ def main() -> None:
         run_adjoint(args.adjoint)
     elif args.batch:
         run_batch(args.batch)
+    elif args.host:
+        run_host(args.host)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -46,7 +46,10 @@ typedef enum AvdStatus {
     AVD_ERR_CONTEXT_AFTER_PUSH = 6,
     AVD_ERR_NEEDS_RESET = 7,
     AVD_ERR_GPU = 8, /* Error::Gpu: any CUDA failure, which poisons the engine */
-    AVD_ERR_NULL_ARG = 9
+    AVD_ERR_NULL_ARG = 9,
+    /* av-denoise/src/host/mod.rs:37-57 (`DenoiserError`) for the host denoiser below: */
+    AVD_ERR_QUEUE_FULL = 10, /* QueueFull: MAX_PENDING frames wait to be collected; not poisoning */
+    AVD_ERR_POISONED = 11    /* Poisoned: an earlier call failed; reset the stream */
 } AvdStatus;
 
 /* ---- geometry ------------------------------------------------------------------------------ */
@@ -341,6 +344,68 @@ AVD_API const char* avd_engine_last_error(const AvdEngine* engine);
 /* Test hook mirroring `fail_through_guard_for_test` (av-denoise-core/src/nlmeans/engine.rs:194-199):
  * forces a GPU-class failure through the poison guard, with no GPU work. */
 AVD_API AvdStatus avd_engine_fail_for_test(AvdEngine* engine);
+
+/* ---- host denoiser ------------------------------------------------------------------------ */
+
+/* av-denoise/src/host/mod.rs:111-420 (`HostDenoiser`): an engine fed from host memory. Frames go
+ * in as wire planes (width x height samples: 1 byte for U8, 2 little-endian bytes for U16, 4 for
+ * F32, each plane at its own size), are staged in pinned memory and uploaded on a copy stream that
+ * overlaps the engine's stream; denoised frames are read back on a third stream into pinned
+ * memory, at most MAX_PENDING = 2 in flight (mod.rs:27-33). The denoiser owns its streams and
+ * buffers. */
+typedef struct AvdHost AvdHost;
+
+/* `HostDenoiser::create` without the accelerator choice: the CUDA device current at the call. */
+AVD_API AvdStatus avd_host_create(const AvdEngineSpec* spec, const AvdTuning* tuning, AvdHost** out);
+AVD_API void avd_host_destroy(AvdHost* host);
+
+/* The wire byte length of plane `index` (`plane_lengths`, mod.rs:124). */
+AVD_API uint64_t avd_host_plane_bytes(const AvdHost* host, size_t index);
+
+/* mod.rs:256-290 (`push`): uploads one frame and starts denoising every frame it completes.
+ * AVD_ERR_QUEUE_FULL once 2 frames wait in flight (the call changes nothing); a rejected plane
+ * (AVD_ERR_PLANE_MISMATCH) leaves the denoiser usable; any other failure poisons it. */
+AVD_API AvdStatus avd_host_push(AvdHost* host, const void* const* planes, const uint64_t* bytes, size_t n);
+
+/* mod.rs:302-322 (`push_priming`): uploads one frame as context only. */
+AVD_API AvdStatus avd_host_push_priming(AvdHost* host, const void* const* planes, const uint64_t* bytes, size_t n);
+
+/* mod.rs:324-343 (`recv`): blocks until the oldest frame in flight lands and copies its planes into
+ * `out` (avd_host_plane_bytes each); `*got` is 0 when nothing was in flight. */
+AVD_API AvdStatus avd_host_recv(AvdHost* host, void* const* out, size_t n, int* got);
+
+/* mod.rs:345-373 (`flush`): drains the frames in flight and the temporal tail, handing each to
+ * `sink` in order; the denoiser is ready for a fresh stream afterwards. */
+typedef void (*AvdHostSink)(void* user, const void* const* planes, size_t n);
+AVD_API AvdStatus avd_host_flush(AvdHost* host, AvdHostSink sink, void* user);
+
+/* mod.rs:375-381 (`reset_stream`): drops the frames in flight and clears any poison. */
+AVD_API void avd_host_reset(AvdHost* host);
+
+/* The message of the host denoiser's last failed call; with a null host, of the last failed create. */
+AVD_API const char* avd_host_last_error(const AvdHost* host);
+
+/* av-denoise/src/host/timing.rs:20-56 (`PlanarTiming`): where the denoiser's time went since it
+ * was built. `blocked` is host time waiting for readbacks to land, `submit` the rest of the time
+ * spent inside its calls (the flush sink's time excluded); each denoised plane group's device time
+ * is scaled from its sampled frames to every emitted frame, or -1 when nothing was sampled. */
+typedef struct AvdHostTiming {
+    double blocked;
+    double submit;
+    uint64_t frames;
+    uint32_t has_luma;
+    uint32_t has_chroma;
+    double luma_device_busy;
+    double chroma_device_busy;
+} AvdHostTiming;
+
+/* mod.rs:383-398 (`timing`; waits for device spans in flight) and `sample_device_time`. */
+AVD_API AvdStatus avd_host_timing(AvdHost* host, AvdHostTiming* out);
+AVD_API void avd_host_sample_device_time(AvdHost* host, uint32_t every);
+
+/* Marks the stream failed, as a failure inside a call would, so that tests can exercise the
+ * Poisoned path without a device fault (av-denoise/src/host/mod.rs:392-395, `poison_for_test`). */
+AVD_API void avd_host_poison_for_test(AvdHost* host);
 
 /* ---- NL4D kernel-level entry points ------------------------------------------------------- */
 
