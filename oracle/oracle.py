@@ -537,6 +537,139 @@ def immerkaer_sigma_low_from_partials(partials: np.ndarray, channels: int, width
     return low
 
 
+# ---- automatic noise estimate (noise_estimate_oracle.cpp) ------------------------------------------
+
+READING_WORDS = 30
+STATE_WORDS = 32
+DERIVED_WORDS = 11
+NOISE_WINDOW_RADIUS = 8
+LOOKAHEAD_FRAMES = 8
+RECIPROCAL_FLOOR = 1e-12
+
+
+def _noise_lib():
+    l = lib()
+    l.orc_noise_record_len.argtypes = [C.c_int]
+    l.orc_noise_record_len.restype = C.c_int
+    l.orc_min_static_blocks.argtypes = [C.c_uint32]
+    l.orc_min_static_blocks.restype = C.c_uint32
+    l.orc_temporal_stats.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, _fp]
+    l.orc_noise_reading.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
+    l.orc_fold_words.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, C.c_int, C.c_float,
+                                 C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, C.c_float, _fp]
+    l.orc_noise_fold.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, _fp, C.c_int, C.c_int, _fp, _fp, _fp, _fp]
+    l.orc_correlation_factor.argtypes = [C.c_float, _fp]
+    l.orc_correlation_factor.restype = C.c_float
+    return l
+
+
+def noise_record_len(channels: int) -> int:
+    return _noise_lib().orc_noise_record_len(channels)
+
+
+def stats_blocks(width: int, height: int) -> tuple[int, int]:
+    return -(-width // 16), -(-height // 16)
+
+
+def min_static_blocks(total: int) -> int:
+    return int(_noise_lib().orc_min_static_blocks(total))
+
+
+def temporal_stats(new: np.ndarray, prev: np.ndarray, channels: int, width: int, height: int) -> np.ndarray:
+    """The temporal residual records of `new` against `prev`, (H, W, C) f32 frames."""
+    bx, by = stats_blocks(width, height)
+    out = np.zeros(bx * by * noise_record_len(channels), np.float32)
+    _noise_lib().orc_temporal_stats(_f(np.ascontiguousarray(new, np.float32)),
+                                    _f(np.ascontiguousarray(prev, np.float32)), channels, width, height, _f(out))
+    return out
+
+
+def noise_reading(records: np.ndarray | None, imm_low, channels: int, width: int, height: int,
+                  temporal: bool) -> np.ndarray:
+    """One slot's READING_WORDS reading from its records (None without temporal stats) and its two
+    Immerkaer lower quartiles."""
+    out = np.zeros(READING_WORDS, np.float32)
+    low = np.ascontiguousarray(np.asarray(imm_low, np.float32).reshape(2))
+    rec = _f(np.ascontiguousarray(records, np.float32)) if records is not None else None
+    _noise_lib().orc_noise_reading(rec, _f(low), channels, width, height, int(temporal), _f(out))
+    return out
+
+
+def fold_words(width: int, height: int, *, sigma_scale=1.0, curve_applies=False, g_max=0.0,
+               weight_floor=RECIPROCAL_FLOOR, h2_per_inverse_variance=None, h2_fixed=0.0, pilot_h2_factor=1.0,
+               offset_per_variance=0.0, main_offset=True, sad_per_sigma=0.0,
+               confidence_sad_per_sigma=0.0) -> np.ndarray:
+    """noise/fold.rs:118-146: the 16 fold settings words."""
+    out = np.zeros(16, np.float32)
+    _noise_lib().orc_fold_words(width, height, sigma_scale, int(curve_applies), g_max, weight_floor,
+                                int(h2_per_inverse_variance is not None), h2_per_inverse_variance or 0.0, h2_fixed,
+                                pilot_h2_factor, offset_per_variance, int(main_offset), sad_per_sigma,
+                                confidence_sad_per_sigma, immerkaer_scale(), _f(out))
+    return out
+
+
+def correlation_factor(rho: float, settings: np.ndarray) -> float:
+    return float(_noise_lib().orc_correlation_factor(rho, _f(np.ascontiguousarray(settings, np.float32))))
+
+
+def noise_fold(records: np.ndarray, results: np.ndarray, capacity: int, first: int, last: int,
+               settings: np.ndarray, channels: int, table_radius: int = 0):
+    """One window fold over history frames first..=last (frame f in slot f % capacity). Returns
+    (state, derived, spatial_table, pilot_table)."""
+    side = 2 * table_radius + 1
+    state = np.zeros(STATE_WORDS, np.float32)
+    derived = np.zeros(DERIVED_WORDS, np.float32)
+    spatial = np.zeros(side * side, np.float32)
+    pilot = np.zeros(side * side, np.float32)
+    _noise_lib().orc_noise_fold(_f(np.ascontiguousarray(records, np.float32)),
+                                _f(np.ascontiguousarray(results, np.float32)), capacity, first, last,
+                                _f(np.ascontiguousarray(settings, np.float32)), channels, table_radius, _f(state),
+                                _f(derived), _f(spatial), _f(pilot))
+    return state, derived, spatial, pilot
+
+
+def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: int, temporal: bool):
+    """Every frame's reading and Immerkaer totals, each read against the frame before it (the first
+    frame's records are zero), as the look-ahead reads them without motion compensation
+    (nlmeans/denoiser/lookahead.rs:425-444)."""
+    readings, totals = [], []
+    for i, f in enumerate(frames):
+        _, tot, low = immerkaer(f, channels, width, height)
+        rec = None
+        if temporal:
+            if i == 0:
+                rec = np.zeros(stats_blocks(width, height)[0] * stats_blocks(width, height)[1]
+                               * noise_record_len(channels), np.float32)
+            else:
+                rec = temporal_stats(f, frames[i - 1], channels, width, height)
+        readings.append(noise_reading(rec, low, channels, width, height, temporal))
+        totals.append(tot)
+    return readings, totals
+
+
+def noise_window(centre: int, newest: int) -> tuple[int, int]:
+    """noise/history.rs:31-44 (`WindowBounds::around`)."""
+    return max(centre - NOISE_WINDOW_RADIUS, 0), min(centre + NOISE_WINDOW_RADIUS, newest)
+
+
+def fold_stream(readings, totals, settings, channels: int, table_radius: int, temporal_radius: int):
+    """The fold of every centre frame of a stream of n frames: window around(c, n - 1) over a
+    history of 17 + d slots, as the NLMeans front folds before each pass. Returns a list of
+    (state, derived, spatial_table, pilot_table)."""
+    n = len(readings)
+    cap = 2 * NOISE_WINDOW_RADIUS + 1 + temporal_radius
+    out = []
+    for c in range(n):
+        first, last = noise_window(c, n - 1)
+        records = np.zeros(cap * READING_WORDS, np.float32)
+        results = np.zeros(cap * 2, np.float32)
+        for f in range(first, last + 1):
+            records[(f % cap) * READING_WORDS:(f % cap + 1) * READING_WORDS] = readings[f]
+            results[(f % cap) * 2:(f % cap) * 2 + 2] = totals[f]
+        out.append(noise_fold(records, results, cap, first, last, settings, channels, table_radius))
+    return out
+
+
 # ---- NLMeans adjoint (nlm_backward_oracle.cpp) -----------------------------------------------------
 
 def nlm_backward(window: list[np.ndarray], d: int, a: int, s: int, strength: float, grad_out: np.ndarray,
