@@ -92,4 +92,23 @@ void plane_dims(const AvdGeometry& g, size_t index, uint32_t* w, uint32_t* h);
 // Full spec validation with the per-pass build checks; writes the message.
 AvdStatus validate_spec(const AvdEngineSpec& spec, std::string* message);
 
+// Automatic noise estimate (noise_host.cpp): noise/temporal.rs:83-100 and noise/fold.rs:118-146.
+struct FoldCoefficients {
+    float sigma_scale = 1.0f;
+    bool curve_applies = false;
+    float weight_g_max = 0.0f;
+    float weight_floor = 1e-12f;
+    bool h2_auto = false;
+    float h2_per_inverse_variance = 0.0f;
+    float h2_fixed = 0.0f;
+    float pilot_h2_factor = 1.0f;
+    float offset_per_variance = 0.0f;
+    bool main_offset = true;
+    float sad_per_sigma = 0.0f;
+    float confidence_sad_per_sigma = 0.0f;
+};
+uint32_t min_static_blocks(uint32_t total);
+float immerkaer_sigma_scale();
+void noise_fold_words(uint32_t width, uint32_t height, const FoldCoefficients& k, float* words);
+
 }  // namespace avd

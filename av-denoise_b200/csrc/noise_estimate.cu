@@ -1,0 +1,619 @@
+// The automatic noise estimate on sm_100a, without motion compensation: per-block temporal residual
+// statistics, one frame's reading and the window fold into the derived words and offset tables.
+//
+// Reference behaviour (av-denoise-core/src/noise):
+//   kernels/stats.rs:141-420   `nlm_temporal_noise_stats`: per 16x16 block the per-channel sums of
+//                              d = new - prev and d^2 and the lag-1 channel-0 product, each summed
+//                              over the block's 256 threads in thread order; each channel's texture
+//                              from 4x4 cell means (stats.rs:599-650). No luma quarter fields.
+//   kernels/sample.rs:143-803  `noise_block_derive`, `noise_block_accept`, `noise_sample_finish`:
+//                              the static gate, the outlier ceiling, the moved-texture threshold, the
+//                              kept sigmas' median and lower quartile, the median correlation.
+//   kernels/window.rs:1-498, kernels/derive.rs:1-192
+//                              `noise_window_fold`: four chains' medians over the window, the stream
+//                              state, the derived words and both NLM offset tables.
+//
+// Design. The reference runs the reading as 9 launches over three tagged radix-select batches. Here
+// one CTA of 1024 threads builds the whole reading: it derives every block's values into a small
+// global scratch (L2-resident: at 3840x2160 that is 32,400 blocks), answers each order statistic
+// with an exact 4-pass 8-bit radix select (one warp scans each query's histogram), and writes the
+// reading words into the frame's history slot. The fold is one CTA as well. Order statistics are
+// exact, so the results equal the reference's tagged selects; every other step rounds each multiply
+// and add on its own (this file is built with -fmad=false), as the oracle does.
+
+#include <cstdint>
+
+#include "kernels.h"
+
+namespace avd {
+namespace {
+
+constexpr int kNB = 16;
+constexpr int kNoiseChannels = 2;
+constexpr int kReadingThreads = 1024;
+constexpr int kReadingWords = 30;
+constexpr uint32_t kExcluded = 0xFFFFFFFFu;
+constexpr float kStaticGate = 1.5f / 255.0f;
+constexpr float kRhoSigmaGate = 0.3f / 255.0f;
+constexpr float kOutlierFactor = 5.0f;
+constexpr float kSigmaFloor = 0.1f / 255.0f;
+constexpr float kSqrt2 = 1.41421356237309504880f;
+
+// Reading, fold-settings, state and derived word layouts (noise/reading.rs, fold.rs, derived.rs).
+constexpr int R_VALID = 2, R_SIGMA = 4, R_SIGMA_LOW = 6, R_RHO = 8, R_STATIC = 9, R_ACCEPTED = 10,
+              R_CURVE_VALID = 11, R_QUARTER_MEDIAN = 12, R_RATIOS = 14;
+constexpr int F_SIGMA_SCALE = 0, F_CURVE_APPLIES = 1, F_G_MAX = 2, F_W_FLOOR = 3, F_H2_AUTO = 4, F_H2_PIV = 5,
+              F_H2_FIXED = 6, F_PILOT = 7, F_OFFSET_PV = 8, F_MAIN_OFFSET = 9, F_SAD = 10, F_CONF_SAD = 11,
+              F_IMM = 12, F_SEG = 13;
+constexpr int S_MEDIAN = 0, S_LOW = 3, S_LOW_UNB = 6, S_TEMPORAL = 9, S_RHO_VALID = 12, S_RHO = 13, S_CURVE = 14,
+              S_QUARTER = 15, S_RATIOS = 16;
+constexpr int D_SIGMA = 0, D_WEIGHT = 2, D_CURVE = 3, D_SAD = 4, D_CONF_SAD = 5, D_H2 = 6, D_PILOT_H2 = 7,
+              D_OFFSET = 8, D_INPUT_OFFSET = 9, D_RHO = 10;
+
+__host__ __device__ constexpr int record_len(int c) { return 3 * c + 26; }
+__host__ __device__ constexpr int texture_lane(int channels, int c) {
+    return c == 0 ? 2 * channels + 1 : 2 * channels + 3 + 24 + c - 1;
+}
+
+// kernels/select.rs:31-46: a float's order-preserving key and back.
+__device__ __forceinline__ uint32_t order_key(float v) {
+    const uint32_t b = __float_as_uint(v);
+    return b >= 0x80000000u ? b ^ 0xFFFFFFFFu : b ^ 0x80000000u;
+}
+__device__ __forceinline__ float key_value(uint32_t k) {
+    return __uint_as_float(k >= 0x80000000u ? k ^ 0x80000000u : k ^ 0xFFFFFFFFu);
+}
+
+// ---- temporal stats ---------------------------------------------------------------------------
+
+template <int C>
+__global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __restrict__ next,
+                                                             const float* __restrict__ prev, int width, int height,
+                                                             float* __restrict__ records) {
+    constexpr int L = 2 * C + 1;
+    __shared__ float scratch[256 * L];
+    __shared__ float tile[256];
+    __shared__ float cells[16];
+    const int t = threadIdx.x, lx = t % kNB, ly = t / kNB;
+    const int x0 = blockIdx.x * kNB, y0 = blockIdx.y * kNB;
+    const int gx = x0 + lx, gy = y0 + ly;
+    const int bw = min(kNB, width - x0), bh = min(kNB, height - y0);
+    const bool valid = gx < width && gy < height;
+    float* out = records + (static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x) * record_len(C);
+
+    float nv[C], d[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        nv[c] = 0.0f;
+        d[c] = 0.0f;
+        if (valid) {
+            const int64_t at = (static_cast<int64_t>(gy) * width + gx) * C + c;
+            nv[c] = next[at];
+            d[c] = nv[c] - prev[at];
+        }
+        scratch[t * L + c] = d[c];
+        scratch[t * L + C + c] = d[c] * d[c];
+    }
+    __syncthreads();
+    // The lag pair never crosses the block's in-frame edge (lx + 1 < bw <= 16 keeps t + 1 in range).
+    const float lag = (valid && lx + 1 < bw) ? d[0] * scratch[(t + 1) * L] : 0.0f;
+    scratch[t * L + 2 * C] = lag;
+    __syncthreads();
+    if (t < L) {
+        float total = 0.0f;
+        for (int i = 0; i < 256; ++i) total += scratch[i * L + t];
+        out[t] = total;
+    }
+    // The moved lane and the quarter lanes are written as zero (no motion, no luma fields).
+    if (t >= 2 * C + 2 && t < 2 * C + 27) out[t] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        __syncthreads();
+        tile[t] = valid ? nv[c] : 0.0f;
+        __syncthreads();
+        if (t < 16) {
+            const int cx = t % 4, cy = t / 4;
+            float cell = 0.0f;
+#pragma unroll
+            for (int dy = 0; dy < 4; ++dy)
+#pragma unroll
+                for (int dx = 0; dx < 4; ++dx) cell += tile[(4 * cy + dy) * kNB + 4 * cx + dx];
+            cells[t] = cell / 16.0f;
+        }
+        __syncthreads();
+        if (t == 0) {
+            const int cols = bw / 4, rows = bh / 4;
+            float energy = 0.0f;
+            uint32_t pairs = 0;
+            for (int cy = 0; cy < rows; ++cy)
+                for (int cx = 0; cx < cols; ++cx) {
+                    const float here = cells[cy * 4 + cx];
+                    if (cx + 1 < cols) {
+                        const float s = here - cells[cy * 4 + cx + 1];
+                        energy += s * s;
+                        ++pairs;
+                    }
+                    if (cy + 1 < rows) {
+                        const float s = here - cells[(cy + 1) * 4 + cx];
+                        energy += s * s;
+                        ++pairs;
+                    }
+                }
+            out[texture_lane(C, c)] = pairs ? energy / static_cast<float>(pairs) : 0.0f;
+        }
+    }
+}
+
+// ---- the reading ------------------------------------------------------------------------------
+
+// The per-block values the reading works from (global scratch, one array per field).
+struct BlockScratch {
+    float* sigma[kNoiseChannels];
+    float* texture[kNoiseChannels];
+    float* mean0;
+    float* var0;
+    float* mean_lag;
+    float* pairs;
+    float* rho;
+    uint32_t* flags;  // per channel: bit 0 candidate, bit 1 measurable, bit 2 kept, bit 3 accepted; bit 8 moved,
+                      // bit 9 has_rho
+};
+
+enum SetKind : int { kSetReference, kSetTexture, kSetKept, kSetRho };
+
+struct ReadingShared {
+    uint32_t hist[4][256];
+    uint32_t prefix[4], rank[4];
+    uint32_t ref_n[kNoiseChannels], excl_n[kNoiseChannels], tex_n[kNoiseChannels], kept_n[kNoiseChannels],
+        acc_n[kNoiseChannels], rho_n;
+    uint32_t ref_min[kNoiseChannels], ref_max[kNoiseChannels];
+    float ceiling[kNoiseChannels], threshold[kNoiseChannels];
+    uint32_t trusted[kNoiseChannels];
+    uint32_t result[4];
+};
+
+__device__ __forceinline__ uint32_t set_key(const BlockScratch& s, int kind, int c, int i) {
+    const uint32_t f = s.flags[i] >> (4 * c);
+    switch (kind) {
+        case kSetReference: return ((f & 3u) == 3u) ? order_key(s.sigma[c][i]) : kExcluded;
+        case kSetTexture:
+            return ((f & 3u) == 3u && (s.flags[i] & 0x100u)) ? order_key(s.texture[c][i]) : kExcluded;
+        case kSetKept: return (f & 4u) ? order_key(s.sigma[c][i]) : kExcluded;
+        default: return (s.flags[i] & 0x200u) ? order_key(s.rho[i]) : kExcluded;
+    }
+}
+
+// The keys of ranks[0..nq) among the set's elements (all ranks below the set's count), exactly:
+// four 8-bit radix passes, one histogram per query, one warp scanning each query's histogram.
+__device__ void select_ranks(const BlockScratch& s, int kind, int c, int n, const uint32_t* ranks, int nq,
+                             ReadingShared& sh) {
+    const int t = threadIdx.x;
+    if (t < nq) {
+        sh.prefix[t] = 0;
+        sh.rank[t] = ranks[t];
+    }
+    uint32_t mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = t; i < 4 * 256; i += blockDim.x) (&sh.hist[0][0])[i] = 0;
+        __syncthreads();
+        for (int i = t; i < n; i += blockDim.x) {
+            const uint32_t key = set_key(s, kind, c, i);
+            if (key == kExcluded) continue;
+            for (int q = 0; q < nq; ++q)
+                if ((key & mask) == sh.prefix[q]) atomicAdd(&sh.hist[q][(key >> shift) & 0xFFu], 1u);
+        }
+        __syncthreads();
+        const int warp = t / 32, lane = t % 32;
+        if (warp < nq) {
+            const uint32_t* h = sh.hist[warp];
+            uint32_t mine = 0;
+            for (int b = 0; b < 8; ++b) mine += h[lane * 8 + b];
+            uint32_t incl = mine;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const uint32_t below = incl - mine, rank = sh.rank[warp];
+            if (rank >= below && rank < incl) {
+                uint32_t seen = below, b = 0;
+                for (; b < 8; ++b) {
+                    if (rank < seen + h[lane * 8 + b]) break;
+                    seen += h[lane * 8 + b];
+                }
+                sh.prefix[warp] |= static_cast<uint32_t>(lane * 8 + b) << shift;
+                sh.rank[warp] = rank - seen;
+            }
+        }
+        mask |= 0xFFu << shift;
+        __syncthreads();
+    }
+    if (t < nq) sh.result[t] = sh.prefix[t];
+    __syncthreads();
+}
+
+__device__ __forceinline__ float quartile_from_pair(float low, float high, uint32_t count) {
+    const uint32_t last = max(count, 1u) - 1u;
+    const float fraction = static_cast<float>(last % 4u) * 0.25f;
+    return low + fraction * (high - low);
+}
+__device__ __forceinline__ float median_from_pair(float low, float high) { return (low + high) * 0.5f; }
+
+// The median pair and quartile pair of a set of n elements (all four zero for an empty set).
+__device__ void set_pairs(const BlockScratch& s, int kind, int c, int nb, uint32_t n, float out[4],
+                          ReadingShared& sh) {
+    if (n == 0) {
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+        return;
+    }
+    const uint32_t ranks[4] = {(n - 1) / 2, n / 2, (n - 1) / 4, (n + 2) / 4};
+    select_ranks(s, kind, c, nb, ranks, 4, sh);
+    for (int q = 0; q < 4; ++q) out[q] = key_value(sh.result[q]);
+    __syncthreads();
+}
+
+template <int C>
+__global__ void __launch_bounds__(kReadingThreads) noise_reading_kernel(const float* __restrict__ records, int width,
+                                                                       int height, BlockScratch s, uint32_t min_accepted,
+                                                                       float* __restrict__ reading) {
+    __shared__ ReadingShared sh;
+    const int t = threadIdx.x;
+    const int bxn = (width + kNB - 1) / kNB, byn = (height + kNB - 1) / kNB, nb = bxn * byn;
+    if (t < kNoiseChannels) {
+        sh.ref_n[t] = sh.excl_n[t] = sh.tex_n[t] = sh.kept_n[t] = sh.acc_n[t] = 0;
+        sh.ref_min[t] = 0xFFFFFFFFu;
+        sh.ref_max[t] = 0u;
+    }
+    if (t == 0) sh.rho_n = 0;
+    __syncthreads();
+
+    // Block derive (sample.rs:143-276).
+    for (int i = t; i < nb; i += blockDim.x) {
+        const int bx = i % bxn, by = i / bxn;
+        const int bw = min(kNB, width - bx * kNB), bh = min(kNB, height - by * kNB);
+        const float pixels = static_cast<float>(bw * bh), pairs = static_cast<float>(bh * (bw - 1));
+        const float* r = records + static_cast<int64_t>(i) * record_len(C);
+        const bool moved = r[2 * C + 2] != 0.0f;
+        uint32_t flags = moved ? 0x100u : 0u;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const float mean = r[c] / pixels;
+            const float ms = r[C + c] / pixels;
+            const float var = fmaxf(ms - mean * mean, 0.0f);
+            const float sigma = sqrtf(var) / kSqrt2;
+            const bool candidate = fabsf(mean) < kStaticGate;
+            const bool measurable = sigma > kRhoSigmaGate;
+            s.sigma[c][i] = sigma;
+            s.texture[c][i] = r[texture_lane(C, c)];
+            flags |= ((candidate ? 1u : 0u) | (measurable ? 2u : 0u)) << (4 * c);
+            if (candidate && measurable) {
+                atomicAdd(&sh.ref_n[c], 1u);
+                const uint32_t k = order_key(sigma);
+                atomicMin(&sh.ref_min[c], k);
+                atomicMax(&sh.ref_max[c], k);
+                if (moved) atomicAdd(&sh.tex_n[c], 1u);
+            } else if (candidate) {
+                atomicAdd(&sh.excl_n[c], 1u);
+            }
+            if (c == 0) {
+                s.mean0[i] = mean;
+                s.var0[i] = var;
+            }
+        }
+        s.pairs[i] = pairs;
+        s.mean_lag[i] = pairs > 0.0f ? r[2 * C] / pairs : 0.0f;
+        s.flags[i] = flags;
+    }
+    __threadfence_block();
+    __syncthreads();
+
+    // The outlier ceilings and moved-texture thresholds (sample.rs:310-360).
+    for (int c = 0; c < C; ++c) {
+        const uint32_t n = sh.ref_n[c];
+        float ql = 0.0f, qh = 0.0f;
+        if (n > 0) {
+            const uint32_t ranks[2] = {(n - 1) / 4, (n + 2) / 4};
+            select_ranks(s, kSetReference, c, nb, ranks, 2, sh);
+            ql = key_value(sh.result[0]);
+            qh = key_value(sh.result[1]);
+        }
+        float threshold = 0.0f;
+        const uint32_t tn = sh.tex_n[c];
+        if (tn > 0) {
+            const uint32_t ranks[1] = {(tn - 1) * 2 / 5};
+            select_ranks(s, kSetTexture, c, nb, ranks, 1, sh);
+            threshold = key_value(sh.result[0]);
+        }
+        if (t == 0) {
+            const float q = quartile_from_pair(ql, qh, n);
+            sh.ceiling[c] = n > 0 ? q * kOutlierFactor : 0.0f;
+            const bool spread = n > 0 && key_value(sh.ref_max[c]) > key_value(sh.ref_min[c]);
+            sh.trusted[c] = (sh.excl_n[c] == 0 || spread) ? 1u : 0u;
+            sh.threshold[c] = threshold;
+        }
+        __syncthreads();
+    }
+
+    // Block accept (sample.rs:362-500).
+    for (int i = t; i < nb; i += blockDim.x) {
+        uint32_t flags = s.flags[i];
+        const bool moved = flags & 0x100u;
+        bool accepted0 = false;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const float sigma = s.sigma[c][i];
+            const bool candidate = (flags >> (4 * c)) & 1u;
+            const bool acc = sh.trusted[c] && candidate && sigma <= sh.ceiling[c] && sigma > kRhoSigmaGate;
+            const bool textured = moved && sh.tex_n[c] > 0 && s.texture[c][i] > sh.threshold[c];
+            if (acc) {
+                flags |= 8u << (4 * c);
+                atomicAdd(&sh.acc_n[c], 1u);
+            }
+            if (acc && !textured) {
+                flags |= 4u << (4 * c);
+                atomicAdd(&sh.kept_n[c], 1u);
+            }
+            if (c == 0) accepted0 = acc;
+        }
+        const bool has_rho = accepted0 && s.pairs[i] > 0.0f;
+        const float variance = has_rho ? s.var0[i] : 1.0f;
+        const float mean0 = s.mean0[i];
+        const float rho = (s.mean_lag[i] - mean0 * mean0) / variance;
+        if (has_rho) {
+            flags |= 0x200u;
+            s.rho[i] = fminf(fmaxf(rho, 0.0f), 1.0f);
+            atomicAdd(&sh.rho_n, 1u);
+        }
+        s.flags[i] = flags;
+    }
+    __threadfence_block();
+    __syncthreads();
+
+    // The sample (sample.rs:562-710).
+    float kept[kNoiseChannels][4] = {};
+    for (int c = 0; c < C; ++c) set_pairs(s, kSetKept, c, nb, sh.kept_n[c], kept[c], sh);
+    float rho_pair[4];
+    set_pairs(s, kSetRho, 0, nb, sh.rho_n, rho_pair, sh);
+    if (t == 0) {
+        auto channel_valid = [&](int c) { return c < C && sh.acc_n[c] >= min_accepted && sh.kept_n[c] > 0; };
+        const bool valid0 = sh.rho_n > 0 && channel_valid(0);
+        const float static_fraction = static_cast<float>(sh.acc_n[0]) / static_cast<float>(nb);
+        for (int c = 0; c < kNoiseChannels; ++c) {
+            const bool k = c == 0 ? valid0 : channel_valid(c);
+            const float sigma = median_from_pair(kept[c][0], kept[c][1]);
+            const float low = quartile_from_pair(kept[c][2], kept[c][3], c < C ? sh.kept_n[c] : 0u);
+            reading[R_VALID + c] = k ? 1.0f : 0.0f;
+            reading[R_SIGMA + c] = k ? sigma : 0.0f;
+            reading[R_SIGMA_LOW + c] = k ? low : 0.0f;
+        }
+        reading[R_RHO] = valid0 ? median_from_pair(rho_pair[0], rho_pair[1]) : 0.0f;
+        reading[R_STATIC] = valid0 ? static_fraction : 0.0f;
+        reading[R_ACCEPTED] = static_cast<float>(sh.acc_n[0]);
+        for (int w = R_ACCEPTED + 1; w < kReadingWords; ++w) reading[w] = 0.0f;
+    }
+}
+
+// A reading without temporal stats: the Immerkaer words (already written) and zeros.
+__global__ void spatial_reading_kernel(float* __restrict__ reading) {
+    const int w = threadIdx.x + 2;
+    if (w < kReadingWords) reading[w] = 0.0f;
+}
+
+// ---- the window fold --------------------------------------------------------------------------
+
+__device__ float fold_correlation_factor(float rho, const float* settings) {
+    const float r0 = 0.0f, r1 = 0.3f, r2 = 0.5f, r3 = 0.65f;
+    const float a0 = 1.0f, a1 = 1.05f, a2 = 1.25f, a3 = 1.45f;
+    const float x = fminf(fmaxf(rho, r0), r3);
+    const float f0 = (x - r0) * settings[F_SEG];
+    const float f1 = (x - r1) * settings[F_SEG + 1];
+    const float f2 = (x - r2) * settings[F_SEG + 2];
+    const float first = a0 + f0 * (a1 - a0);
+    const float second = a1 + f1 * (a2 - a1);
+    const float third = a2 + f2 * (a3 - a2);
+    const float later = x <= r2 ? second : third;
+    return x <= r1 ? first : later;
+}
+
+// exp and ln in double precision, rounded to float, as the oracle evaluates them.
+__device__ float spatial_offset_factor(int dx, int dy, float rho) {
+    const int sq = dx * dx + dy * dy;
+    if (sq == 0) return 0.0f;
+    if (rho <= 0.0f) return 1.0f;
+    const float distance = sqrtf(static_cast<float>(sq));
+    const float log_rho = static_cast<float>(log(static_cast<double>(rho)));
+    const float shared = static_cast<float>(exp(static_cast<double>(distance * log_rho)));
+    return 1.0f - shared;
+}
+
+__device__ float sorted_median(float* v, int n) {
+    for (int i = 1; i < n; ++i) {
+        const float key = v[i];
+        int p = i;
+        while (p > 0 && v[p - 1] > key) {
+            v[p] = v[p - 1];
+            --p;
+        }
+        v[p] = key;
+    }
+    return n > 0 ? (v[(n - 1) / 2] + v[n / 2]) * 0.5f : 0.0f;
+}
+
+__global__ void __launch_bounds__(256) noise_fold_kernel(const float* __restrict__ records,
+                                                         const float* __restrict__ results, int capacity, int first,
+                                                         int last, const float* __restrict__ settings, int channels,
+                                                         int table_radius, float* __restrict__ state,
+                                                         float* __restrict__ derived, float* __restrict__ spatial,
+                                                         float* __restrict__ pilot) {
+    __shared__ float medians[26];
+    __shared__ float inputs[3];
+    const int t = threadIdx.x;
+    auto rec = [&](int frame) { return records + static_cast<int64_t>(frame % capacity) * kReadingWords; };
+    auto has_sample = [&](int frame, int c) { return rec(frame)[R_VALID + c] != 0.0f; };
+    auto has_curve = [&](int frame) { return rec(frame)[R_CURVE_VALID] != 0.0f; };
+    if (t < 26) {
+        float v[17];
+        int n = 0;
+        if (t < 8) {
+            const int chain = t / 2, c = t % 2;
+            float m = 0.0f;
+            if (c < channels) {
+                const float sigma_scale = settings[F_SIGMA_SCALE], imm_factor = settings[F_IMM];
+                for (int f = first; f <= last; ++f) {
+                    if (chain == 3 && !has_sample(f, c)) continue;
+                    const float* r = rec(f);
+                    const bool has = has_sample(f, c);
+                    const float factor = fold_correlation_factor(r[R_RHO], settings);
+                    const float immerkaer = imm_factor * results[static_cast<int64_t>(f % capacity) * 2 + c];
+                    const float imm_low = r[c], sigma = r[R_SIGMA + c], sigma_low = r[R_SIGMA_LOW + c];
+                    float x;
+                    if (chain == 0) x = (has ? fmaxf(immerkaer, sigma * factor) : immerkaer) * sigma_scale;
+                    else if (chain == 1) x = (has ? fmaxf(imm_low, sigma_low * factor) : imm_low) * sigma_scale;
+                    else if (chain == 2) x = (has ? fmaxf(imm_low, sigma_low) : imm_low) * sigma_scale;
+                    else x = sigma * sigma_scale;
+                    v[n++] = x;
+                }
+                const float med = sorted_median(v, n);
+                m = n > 0 ? fmaxf(med, kSigmaFloor) : 0.0f;
+            }
+            medians[t] = m;
+        } else {
+            const int word = t == 8 ? R_RHO : (t == 9 ? R_QUARTER_MEDIAN : R_RATIOS + t - 10);
+            const bool curve_gate = t != 8;
+            for (int f = first; f <= last; ++f)
+                if (has_sample(f, 0) && (!curve_gate || has_curve(f))) v[n++] = rec(f)[word];
+            medians[t] = sorted_median(v, n);
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        uint32_t sampled = 0, curved = 0;
+        for (int f = first; f <= last; ++f) {
+            sampled += has_sample(f, 0) ? 1u : 0u;
+            curved += (has_sample(f, 0) && has_curve(f)) ? 1u : 0u;
+        }
+        const bool curve_present = sampled > 0 && 2 * curved >= sampled;
+        uint32_t mask = sampled > 0 ? 1u : 0u;
+        for (int c = 1; c < channels; ++c) {
+            bool any = false;
+            for (int f = first; f <= last; ++f) any = any || has_sample(f, c);
+            if (any) mask |= 1u << c;
+        }
+        const bool rho_valid = mask & 1u, any_sampled = mask != 0;
+        for (int c = 0; c < kNoiseChannels; ++c) {
+            const bool sampled_c = mask & (1u << c);
+            const float unb = medians[4 + c], temporal = medians[6 + c];
+            state[S_MEDIAN + 1 + c] = medians[c];
+            state[S_LOW + 1 + c] = medians[2 + c];
+            state[S_LOW_UNB + 1 + c] = unb;
+            state[S_TEMPORAL + 1 + c] = sampled_c ? temporal : (any_sampled ? unb : 0.0f);
+            derived[D_SIGMA + c] = sampled_c ? temporal : unb;
+        }
+        float median_sum = 0.0f, low_sum = 0.0f;
+        for (int c = 0; c < channels; ++c) {
+            median_sum += medians[c] * medians[c];
+            low_sum += medians[2 + c] * medians[2 + c];
+        }
+        const float rho = rho_valid ? medians[8] : 0.0f;
+        state[S_MEDIAN] = 1.0f;
+        state[S_LOW] = 1.0f;
+        state[S_LOW_UNB] = 1.0f;
+        state[S_TEMPORAL] = any_sampled ? 1.0f : 0.0f;
+        state[S_RHO_VALID] = rho_valid ? 1.0f : 0.0f;
+        state[S_RHO] = rho;
+        state[S_CURVE] = curve_present ? 1.0f : 0.0f;
+        state[S_QUARTER] = curve_present ? medians[9] : 0.0f;
+        const bool curve_valid = curve_present && settings[F_CURVE_APPLIES] != 0.0f;
+        for (int b = 0; b < 16; ++b) state[S_RATIOS + b] = curve_present ? medians[10 + b] : 0.0f;
+        const float sigma0 = derived[D_SIGMA];
+        const float g_max = settings[F_G_MAX], floor = settings[F_W_FLOOR];
+        const float norm = sigma0 * sigma0 * g_max * g_max;
+        const bool usable = isfinite(norm) && norm > floor;
+        const float h2_measured = settings[F_H2_PIV] * static_cast<float>(channels) / median_sum;
+        const float h2 = settings[F_H2_AUTO] != 0.0f ? h2_measured : settings[F_H2_FIXED];
+        const float input_offset = settings[F_OFFSET_PV] * low_sum;
+        const float noise_offset = settings[F_MAIN_OFFSET] != 0.0f ? input_offset : 0.0f;
+        derived[D_WEIGHT] = usable ? norm : floor;
+        derived[D_CURVE] = curve_valid ? 1.0f : 0.0f;
+        derived[D_SAD] = settings[F_SAD] * medians[0];
+        derived[D_CONF_SAD] = settings[F_CONF_SAD] * medians[0];
+        derived[D_H2] = h2;
+        derived[D_PILOT_H2] = h2 * settings[F_PILOT];
+        derived[D_OFFSET] = noise_offset;
+        derived[D_INPUT_OFFSET] = input_offset;
+        derived[D_RHO] = rho;
+        inputs[0] = noise_offset;
+        inputs[1] = input_offset;
+        inputs[2] = rho;
+    }
+    __syncthreads();
+    if (table_radius > 0) {
+        const int side = 2 * table_radius + 1;
+        for (int i = t; i < side * side; i += blockDim.x) {
+            const int dx = i % side - table_radius, dy = i / side - table_radius;
+            spatial[i] = inputs[0] * spatial_offset_factor(dx, dy, inputs[2]);
+            pilot[i] = inputs[1] * spatial_offset_factor(dx, dy, 0.0f);
+        }
+    }
+}
+
+}  // namespace
+
+size_t noise_scratch_floats(int width, int height) {
+    const size_t nb = static_cast<size_t>((width + kNB - 1) / kNB) * ((height + kNB - 1) / kNB);
+    return nb * 10;  // sigma x2, texture x2, mean0, var0, mean_lag, pairs, rho, flags
+}
+
+size_t noise_records_floats(int width, int height, int channels) {
+    return static_cast<size_t>((width + kNB - 1) / kNB) * ((height + kNB - 1) / kNB) * record_len(channels);
+}
+
+cudaError_t launch_temporal_stats(const float* next, const float* prev, int channels, int width, int height,
+                                  float* records, cudaStream_t s) {
+    if (channels < 1 || channels > 2 || width < 1 || height < 1) return cudaErrorInvalidValue;
+    dim3 grid((width + kNB - 1) / kNB, (height + kNB - 1) / kNB);
+    if (!prev)  // the first frame of a stream has no previous frame: its records are zero
+        return cudaMemsetAsync(records, 0, noise_records_floats(width, height, channels) * sizeof(float), s);
+    if (channels == 1)
+        temporal_stats_kernel<1><<<grid, 256, 0, s>>>(next, prev, width, height, records);
+    else
+        temporal_stats_kernel<2><<<grid, 256, 0, s>>>(next, prev, width, height, records);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_noise_reading(const float* records, int channels, int width, int height, float* scratch,
+                                 uint32_t min_accepted, float* reading, cudaStream_t s) {
+    if (channels < 1 || channels > 2 || width < 1 || height < 1) return cudaErrorInvalidValue;
+    if (!records) {
+        spatial_reading_kernel<<<1, 32, 0, s>>>(reading);
+        return cudaGetLastError();
+    }
+    const size_t nb = static_cast<size_t>((width + kNB - 1) / kNB) * ((height + kNB - 1) / kNB);
+    BlockScratch b{};
+    b.sigma[0] = scratch;
+    b.sigma[1] = scratch + nb;
+    b.texture[0] = scratch + 2 * nb;
+    b.texture[1] = scratch + 3 * nb;
+    b.mean0 = scratch + 4 * nb;
+    b.var0 = scratch + 5 * nb;
+    b.mean_lag = scratch + 6 * nb;
+    b.pairs = scratch + 7 * nb;
+    b.rho = scratch + 8 * nb;
+    b.flags = reinterpret_cast<uint32_t*>(scratch + 9 * nb);
+    if (channels == 1)
+        noise_reading_kernel<1><<<1, kReadingThreads, 0, s>>>(records, width, height, b, min_accepted, reading);
+    else
+        noise_reading_kernel<2><<<1, kReadingThreads, 0, s>>>(records, width, height, b, min_accepted, reading);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_noise_fold(const float* records, const float* results, int capacity, int first, int last,
+                              const float* settings, int channels, int table_radius, float* state, float* derived,
+                              float* spatial, float* pilot, cudaStream_t s) {
+    if (last < first || last - first + 1 > 17 || last - first + 1 > capacity || channels < 1 || channels > 2)
+        return cudaErrorInvalidValue;
+    noise_fold_kernel<<<1, 256, 0, s>>>(records, results, capacity, first, last, settings, channels, table_radius,
+                                        state, derived, spatial, pilot);
+    return cudaGetLastError();
+}
+
+}  // namespace avd

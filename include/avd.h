@@ -513,6 +513,49 @@ AVD_API uint64_t avd_immerkaer_partials_len(uint32_t width, uint32_t height);
 AVD_API AvdStatus avd_immerkaer(uint64_t frame, uint32_t channels, uint32_t width, uint32_t height, uint64_t partials,
                                 uint64_t results, uint64_t sigma_low, void* stream);
 
+/* The floats of one frame's temporal residual records: 3 * channels + 26 per 16x16 block
+ * (av-denoise-core/src/noise/temporal.rs:98-123), and of the reading's per-block scratch. */
+AVD_API uint64_t avd_noise_records_floats(uint32_t width, uint32_t height, uint32_t channels);
+AVD_API uint64_t avd_noise_scratch_floats(uint32_t width, uint32_t height);
+
+/* The temporal residual records of f32 frame `next` against `prev` (kernels/stats.rs:141-420,
+ * `nlm_temporal_noise_stats` without motion compensation and without the luma quarter fields);
+ * `prev` = 0 zeroes them, as a stream's first frame reads (noise/slot.rs:40-60). */
+AVD_API AvdStatus avd_noise_temporal_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width,
+                                           uint32_t height, uint64_t records, void* stream);
+
+/* One frame's reading, AVD_NOISE_READING_WORDS floats (noise/reading.rs:7-33), from its records
+ * (0 without temporal stats: the reading is then the Immerkaer words alone) through
+ * kernels/sample.rs:143-803. Words 0 and 1 must already hold the frame's Immerkaer lower quartiles
+ * (`sigma_low` of avd_immerkaer); the call writes the rest. `scratch` holds
+ * avd_noise_scratch_floats floats. */
+#define AVD_NOISE_READING_WORDS 30
+#define AVD_NOISE_STATE_WORDS 32
+#define AVD_NOISE_DERIVED_WORDS 11
+#define AVD_NOISE_FOLD_WORDS 16
+AVD_API AvdStatus avd_noise_reading(uint64_t records, uint32_t channels, uint32_t width, uint32_t height,
+                                    uint64_t scratch, uint64_t reading, void* stream);
+
+/* The fold settings words for a plane of width x height (noise/fold.rs:118-146, `fold_words`):
+ * sigma_scale, whether the consumer applies the curve, the weight-scale gain and floor, the h2
+ * coefficient (`h2_auto` 0 for a fixed strength `h2_fixed`), the pilot factor, the noise-offset
+ * coefficient and whether the main pass subtracts it, and the two SAD-floor coefficients. */
+AVD_API void avd_noise_fold_words(uint32_t width, uint32_t height, float sigma_scale, uint32_t curve_applies,
+                                  float weight_g_max, float weight_floor, uint32_t h2_auto,
+                                  float h2_per_inverse_variance, float h2_fixed, float pilot_h2_factor,
+                                  float offset_per_variance, uint32_t main_offset, float sad_per_sigma,
+                                  float confidence_sad_per_sigma, float* out16);
+
+/* One window fold over history frames first..=last, frame f in slot f % capacity of `records`
+ * (READING_WORDS each) and `results` (the two Immerkaer abs totals each): kernels/window.rs:414-498
+ * (`noise_window_fold`). Writes the stream state (STATE_WORDS), the derived words
+ * (DERIVED_WORDS: sigma[2], weight scale, curve flag, SAD floor, confidence SAD floor, h2, pilot h2,
+ * noise offset, input noise offset, rho) and, with table_radius > 0, both (2r+1)^2 offset tables. */
+AVD_API AvdStatus avd_noise_fold(uint64_t records, uint64_t results, uint32_t capacity, uint32_t first,
+                                 uint32_t last, uint64_t settings, uint32_t channels, uint32_t table_radius,
+                                 uint64_t state, uint64_t derived, uint64_t spatial_table, uint64_t pilot_table,
+                                 void* stream);
+
 /* ---- adjoint -------------------------------------------------------------------------------- */
 
 /* No Rust item in the reference: the adjoint the hot-path contract adds to the boundary
