@@ -40,10 +40,8 @@ class NlmPass final : public Pass {
         pass->in_ = in;
         pass->out_ = out;
         const NlmParams& p = pass->params_;
-        if (p.hq && !p.hq_params.has_sigma_override)
-            return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "NLMeans-HQ with the automatic noise estimate is not available in this build yet; set "
-                           "hq.sigma_override"};
+        // nlmeans/denoiser/noise.rs:50-52 (`measures_noise`): HQ without a pinned sigma measures it.
+        pass->measures_ = p.hq && !p.hq_params.has_sigma_override;
         if (p.prefilter.kind != AVD_PREFILTER_NONE)
             return Failure{AVD_ERR_INVALID_OPTIONS, "prefilters are not available in this build"};
         if (p.motion.active && p.temporal_radius > 0)
@@ -102,8 +100,8 @@ class NlmPass final : public Pass {
         if (poisoned_) return Failure{AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET)};
         if (ready_slot_ >= 0 || tail_remaining_ > 0)
             return Failure{AVD_ERR_OUTPUTS_PENDING, avd_status_message(AVD_ERR_OUTPUTS_PENDING)};
-        // nlmeans/denoiser/mod.rs:538-545 (`flush_target`).
-        tail_remaining_ = std::min<size_t>(real_pushes_, params_.temporal_radius);
+        // nlmeans/denoiser/mod.rs:534-545 (`flush_target`): the look-ahead's frames, then the ring's.
+        tail_remaining_ = held() + std::min<size_t>(real_pushes_, params_.temporal_radius);
         if (tail_remaining_ == 0) restart_stream();
         *tail = tail_remaining_;
         return std::nullopt;
@@ -127,7 +125,8 @@ class NlmPass final : public Pass {
         return s;
     }
 
-    uint32_t next_frame() const override { return static_cast<uint32_t>(real_pushes_); }
+    // The stream frame the next push takes: frames in the look-ahead count (nlmeans/edges.rs:26-31).
+    uint32_t next_frame() const override { return static_cast<uint32_t>(real_pushes_ + held()); }
     std::optional<uint32_t> emitted_frame() const override { return emitted_; }
     AvdEngineTiming timing() override { return timer_.collect(); }
     void sample_device_time(uint32_t every) override { timer_.every = every; }
@@ -195,6 +194,54 @@ class NlmPass final : public Pass {
                 return gpu_failure("offset table upload", e);
         }
         slot_frames_.assign(total_frames(), 0u);
+        if (measures_) return allocate_noise();
+        return std::nullopt;
+    }
+
+    // The measured noise state (noise/state.rs:172-330 `measurement_buffers`, lookahead.rs:53-112):
+    // the 8-frame look-ahead ring, one frame's Immerkaer partials and temporal records, the reading
+    // scratch, a history of 17 + d readings, the fold settings and state, the derived words and the
+    // two offset tables of the search window.
+    std::optional<Failure> allocate_noise() {
+        const size_t fe = frame_elems();
+        const int w = static_cast<int>(width_), h = static_cast<int>(height_);
+        const int c = static_cast<int>(params_.channel_count());
+        history_capacity_ = 2 * kNoiseWindowRadius + 1 + params_.temporal_radius;
+        const uint32_t side = 2 * params_.search_radius + 1;
+        cudaError_t e;
+        if ((e = lookahead_.alloc(fe * kLookaheadFrames * sizeof(float))) != cudaSuccess)
+            return gpu_failure("look-ahead ring", e);
+        if ((e = partials_.alloc(immerkaer_partials_len(w, h) * sizeof(float))) != cudaSuccess)
+            return gpu_failure("noise partials", e);
+        if (params_.temporal_radius > 0) {
+            if ((e = records_.alloc(noise_records_floats(w, h, c) * sizeof(float))) != cudaSuccess)
+                return gpu_failure("noise records", e);
+            if ((e = noise_scratch_.alloc(noise_scratch_floats(w, h) * sizeof(float))) != cudaSuccess)
+                return gpu_failure("noise scratch", e);
+        }
+        if ((e = history_records_.alloc(history_capacity_ * kReadingWords * sizeof(float))) != cudaSuccess)
+            return gpu_failure("noise history", e);
+        if ((e = history_results_.alloc(history_capacity_ * 2 * sizeof(float))) != cudaSuccess)
+            return gpu_failure("noise history", e);
+        if ((e = fold_settings_.alloc(16 * sizeof(float))) != cudaSuccess) return gpu_failure("fold settings", e);
+        if ((e = fold_state_.alloc(32 * sizeof(float))) != cudaSuccess) return gpu_failure("fold state", e);
+        if ((e = noise_derived_.alloc(16 * sizeof(float))) != cudaSuccess) return gpu_failure("derived words", e);
+        if ((e = pilot_lut_.alloc(side * side * sizeof(float))) != cudaSuccess) return gpu_failure("pilot table", e);
+        for (DeviceBuffer* b : {&history_records_, &history_results_, &fold_state_, &noise_derived_})
+            if ((e = cudaMemset(b->ptr, 0, b->bytes)) != cudaSuccess) return gpu_failure("noise state clear", e);
+        // nlmeans/denoiser/noise.rs:200-246 (`derived_coefficients`): each factor at a sigma of 1.
+        FoldCoefficients k;
+        k.sigma_scale = params_.hq_params.sigma_scale;
+        k.h2_auto = params_.hq_params.auto_strength;
+        k.h2_per_inverse_variance = h2_inv_norm_with(params_, true, 1.0f);
+        k.h2_fixed = h2_inv_norm_with(params_, false, 0.0f);
+        const float unit[1] = {1.0f};
+        k.offset_per_variance = noise_offset_with(params_, unit, 1);
+        k.confidence_sad_per_sigma = conf_pass_ ? avd_sad_noise_floor(kConfBlk, 1.0f) : 0.0f;
+        float words[16];
+        noise_fold_words(width_, height_, k, words);
+        if ((e = cudaMemcpy(fold_settings_.ptr, words, sizeof(words), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return gpu_failure("fold settings upload", e);
         return std::nullopt;
     }
 
@@ -230,18 +277,103 @@ class NlmPass final : public Pass {
 
     float* slot_ptr(size_t slot) const { return ring_.as<float>() + slot * frame_elems(); }
 
-    // nlmeans/denoiser/mod.rs:484-512 (`push_planes`) without look-ahead, then stages.rs:15-26.
+    // nlmeans/denoiser/mod.rs:484-512 (`push_planes`): a front that measures the noise reads the
+    // frame in the look-ahead first; otherwise the frame goes straight into the next ring slot.
     std::optional<Failure> push_planes(const AvdPlane* planes) {
+        if (measures_) return push_into_lookahead(planes);
         const size_t slot = ring_head_ % total_frames();
+        if (auto f = ingest_into(planes, slot_ptr(slot))) return f;
+        return enter_ring(slot);
+    }
+
+    std::optional<Failure> ingest_into(const AvdPlane* planes, float* dst) {
         const void* p0 = reinterpret_cast<const void*>(planes[0].ptr);
         const void* p1 = params_.channel_count() > 1 ? reinterpret_cast<const void*>(planes[1].ptr) : nullptr;
-        cudaError_t e = launch_ingest(p0, p1, slot_ptr(slot), static_cast<int64_t>(pixels()),
+        cudaError_t e = launch_ingest(p0, p1, dst, static_cast<int64_t>(pixels()),
                                       static_cast<int>(params_.channel_count()), plane_format(in_), bias(), stream);
         if (e != cudaSuccess) return gpu_failure("ingest launch", e);
+        return std::nullopt;
+    }
+
+    // nlmeans/denoiser/stages.rs:15-26: the per-frame stages of a frame entering ring slot `slot`.
+    std::optional<Failure> enter_ring(size_t slot) {
         if (auto f = slot_written(slot)) return f;
         slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
         advance_ring();
         return prime_leading_edge_if_first();
+    }
+
+    // ---- the noise look-ahead (nlmeans/denoiser/lookahead.rs:182-259, 425-444) ----
+    size_t held() const { return measures_ ? la_pushed_ - la_released_ : 0; }
+    float* lookahead_slot(size_t frame) const { return lookahead_.as<float>() + (frame % kLookaheadFrames) * frame_elems(); }
+
+    std::optional<Failure> push_into_lookahead(const AvdPlane* planes) {
+        if (held() == kLookaheadFrames) {
+            bool released = false;
+            if (auto f = release_held_frame(&released)) return f;
+        }
+        const size_t frame = la_pushed_;
+        if (auto f = ingest_into(planes, lookahead_slot(frame))) return f;
+        if (auto f = read_lookahead_noise(frame)) return f;
+        la_pushed_ += 1;
+        return std::nullopt;
+    }
+
+    // Reads stream frame `frame` against the frame before it and records the reading in history slot
+    // frame % capacity (noise/slot.rs:32-60, 158-175; noise/history.rs:131-160). A stream's first
+    // frame has nothing before it: its records are zero.
+    std::optional<Failure> read_lookahead_noise(size_t frame) {
+        const int w = static_cast<int>(width_), h = static_cast<int>(height_);
+        const int c = static_cast<int>(params_.channel_count());
+        const size_t hs = frame % history_capacity_;
+        float* reading = history_records_.as<float>() + hs * kReadingWords;
+        float* results = history_results_.as<float>() + hs * 2;
+        cudaError_t e = launch_immerkaer(lookahead_slot(frame), c, w, h, immerkaer_sigma_scale(), partials_.as<float>(),
+                                         results, reading, stream);
+        if (e != cudaSuccess) return gpu_failure("noise estimate launch", e);
+        const float* records = nullptr;
+        if (params_.temporal_radius > 0) {
+            const float* prev = frame > 0 ? lookahead_slot(frame - 1) : nullptr;
+            e = launch_temporal_stats(lookahead_slot(frame), prev, c, w, h, records_.as<float>(), stream);
+            if (e != cudaSuccess) return gpu_failure("temporal noise stats launch", e);
+            records = records_.as<float>();
+        }
+        const uint32_t blocks = static_cast<uint32_t>(((width_ + 15) / 16) * ((height_ + 15) / 16));
+        e = launch_noise_reading(records, c, w, h, noise_scratch_.as<float>(), min_static_blocks(blocks), reading,
+                                 stream);
+        if (e != cudaSuccess) return gpu_failure("noise reading launch", e);
+        recorded_ = std::max(recorded_, frame + 1);
+        return std::nullopt;
+    }
+
+    // lookahead.rs:226-259 (`release_held_frame`): the oldest held frame enters the next ring slot.
+    std::optional<Failure> release_held_frame(bool* released) {
+        *released = false;
+        if (held() == 0) return std::nullopt;
+        const size_t frame = la_released_;
+        const size_t slot = ring_head_ % total_frames();
+        cudaError_t e = cudaMemcpyAsync(slot_ptr(slot), lookahead_slot(frame), frame_elems() * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return gpu_failure("look-ahead release", e);
+        la_released_ += 1;
+        *released = true;
+        return enter_ring(slot);
+    }
+
+    // nlmeans/denoiser/noise.rs:171-185 (`update_noise_estimate`): the fold of the window around the
+    // centre frame, reaching every recorded frame ahead up to the window radius.
+    std::optional<Failure> update_noise_estimate() {
+        const int64_t centre = centre_frame();
+        const int64_t newest = static_cast<int64_t>(recorded_) - 1;
+        const int first = static_cast<int>(std::max<int64_t>(centre - kNoiseWindowRadius, 0));
+        const int last = static_cast<int>(std::min<int64_t>(centre + kNoiseWindowRadius, newest));
+        cudaError_t e = launch_noise_fold(history_records_.as<float>(), history_results_.as<float>(),
+                                          static_cast<int>(history_capacity_), first, last, fold_settings_.as<float>(),
+                                          static_cast<int>(params_.channel_count()),
+                                          static_cast<int>(params_.search_radius), fold_state_.as<float>(),
+                                          noise_derived_.as<float>(), lut_.as<float>(), pilot_lut_.as<float>(), stream);
+        if (e != cudaSuccess) return gpu_failure("noise fold launch", e);
+        return std::nullopt;
     }
 
     // ring.rs:12-20.
@@ -299,7 +431,7 @@ class NlmPass final : public Pass {
             if (l != d) m.inline_slots[n++] = static_cast<uint32_t>(phys_frame(l));
         m.mv_field = mv_scratch_.as<int32_t>();
         m.confidence = conf_.as<float>();
-        m.noise = derived_.as<float>();
+        m.noise = measures_ ? noise_derived_.as<float>() : derived_.as<float>();
         m.width = static_cast<int>(width_);
         m.height = static_cast<int>(height_);
         m.frame_count = static_cast<int>(total_frames());
@@ -313,7 +445,7 @@ class NlmPass final : public Pass {
         m.levels = 1;
         m.mv_stride = static_cast<int>(conf_bx_ * conf_by_ * 2);
         m.conf_stride = static_cast<int>(conf_bx_ * conf_by_);
-        m.sad_floor_word = 2;
+        m.sad_floor_word = measures_ ? kDerivedConfidenceSadFloor : 2;
         m.thsad = thsad_;
         cudaError_t e = launch_motion_search(m, stream);
         if (e != cudaSuccess) return gpu_failure("confidence launch", e);
@@ -338,6 +470,10 @@ class NlmPass final : public Pass {
 
         cudaEvent_t start{};
         bool timed = timer_.begin(stream, &start);
+        // dispatch/mod.rs:640-644: the look-ahead has read every frame the window reaches, so the fold
+        // runs first and the confidence pass reads this centre's own derived words.
+        if (measures_)
+            if (auto f = update_noise_estimate()) return f;
         const int d = static_cast<int>(params_.temporal_radius);
         NlmLaunch a{};
         a.ring = ring_.as<float>();
@@ -354,9 +490,9 @@ class NlmPass final : public Pass {
         }
         a.patch_radius = static_cast<int>(params_.patch_radius);
         a.search_radius = static_cast<int>(params_.search_radius);
-        a.derived = derived_.as<float>();
-        a.h2_word = 0;
-        a.offset_word = 1;
+        a.derived = measures_ ? noise_derived_.as<float>() : derived_.as<float>();
+        a.h2_word = measures_ ? kDerivedH2 : 0;
+        a.offset_word = measures_ ? kDerivedNoiseOffset : 1;
         a.spatial_lut = params_.hq ? lut_.as<float>() : nullptr;
         a.conf = nullptr;
         if (conf_pass_) {
@@ -384,10 +520,15 @@ class NlmPass final : public Pass {
     }
 
     // nlmeans/denoiser/mod.rs:557-573 (`flush_step_gpu`) without look-ahead.
+    // nlmeans/denoiser/mod.rs:551-573 (`flush_step_gpu`): release a held frame, else duplicate the last.
     std::optional<Failure> next_tail_frame(int* slot) {
         for (;;) {
-            if (auto f = duplicate_last_frame()) return f;
-            if (frames_loaded_ < total_frames()) frames_loaded_ += 1;
+            bool released = false;
+            if (auto f = release_held_frame(&released)) return f;
+            if (!released) {
+                if (auto f = duplicate_last_frame()) return f;
+                if (frames_loaded_ < total_frames()) frames_loaded_ += 1;
+            }
             if (auto f = denoise_submit(slot)) return f;
             if (*slot >= 0) return std::nullopt;
         }
@@ -409,7 +550,18 @@ class NlmPass final : public Pass {
         next_output_slot_ = 0;
         real_pushes_ = 0;
         pushed_ = false;
+        la_pushed_ = 0;
+        la_released_ = 0;
+        recorded_ = 0;
     }
+
+    static constexpr int kNoiseWindowRadius = 8;  // noise/history.rs:10
+    static constexpr int kReadingWords = 30;      // noise/reading.rs:33
+    static constexpr int kDerivedConfidenceSadFloor = 5, kDerivedH2 = 6, kDerivedNoiseOffset = 8;  // derived.rs:9-31
+    bool measures_ = false;
+    size_t la_pushed_ = 0, la_released_ = 0, recorded_ = 0, history_capacity_ = 0;
+    DeviceBuffer lookahead_, partials_, records_, noise_scratch_, history_records_, history_results_, fold_settings_,
+        fold_state_, noise_derived_, pilot_lut_;
 
     NlmParams params_;
     size_t held_ = 0;

@@ -159,7 +159,8 @@ def nlm_stream_repeat(frames: list[np.ndarray], d: int, a: int, s: int, h2: floa
     return outs
 
 
-def hq_confidence(window: list[np.ndarray], d: int, sigma: float, thsad_scale: float = 1.0):
+def hq_confidence(window: list[np.ndarray], d: int, sigma: float, thsad_scale: float = 1.0,
+                  sad_floor: float | None = None):
     """The HQ confidence pass over one window (nlmeans/dispatch/motion.rs:554-613): lane 0 of every
     frame, 16x16 blocks at step 8 scored where they stand against the centre, floor
     sad_noise_floor(16, sigma), thsad(16, thsad_scale). Returns the (forward, backward) block
@@ -169,7 +170,8 @@ def hq_confidence(window: list[np.ndarray], d: int, sigma: float, thsad_scale: f
     pyr = motion_pyramid(ring, c, w, h, 1)
     slots = [l for l in range(2 * d + 1) if l != d]
     _, conf = motion_search(pyr, w, h, 2 * d + 1, d, slots, blksize=16, overlap=8, search_radius=0, levels=1,
-                            confidence=True, sad_floor=sad_noise_floor(16, sigma), thsad=thsad(16, thsad_scale))
+                            confidence=True, sad_floor=sad_noise_floor(16, sigma) if sad_floor is None else sad_floor,
+                            thsad=thsad(16, thsad_scale))
     blocks = (max(-(-w // 8), 1), max(-(-h // 8), 1))
     return [(conf[k], conf[2 * d - 1 - k]) for k in range(d)], blocks
 
@@ -668,6 +670,40 @@ def fold_stream(readings, totals, settings, channels: int, table_radius: int, te
             results[(f % cap) * 2:(f % cap) * 2 + 2] = totals[f]
         out.append(noise_fold(records, results, cap, first, last, settings, channels, table_radius))
     return out
+
+
+def nlm_stream_hq_auto(frames: list[np.ndarray], d: int, a: int, s: int, strength: float, *, wref: float = 1.0,
+                       auto_strength: bool = True, noise_floor: bool = True, temporal_confidence: bool = True,
+                       thsad_scale: float = 1.0, sigma_scale: float = 1.0, fp64: bool = False):
+    """NLMeans-HQ with the automatic noise estimate over a stream with repeat edges: every frame is
+    read against the one before it (nlmeans/denoiser/lookahead.rs:425-444), each output frame's
+    window of readings is folded around its centre (nlmeans/denoiser/noise.rs:171-185) into h2, the
+    offset table at the folded correlation and the confidence SAD floor (noise/fold.rs, derived.rs),
+    and the frame is denoised with them. Returns (outputs, folds)."""
+    h, w, c = frames[0].shape
+    f = np.float32
+    area = f((2 * s + 1) ** 2)
+    readings, totals = noise_readings(frames, c, w, h, d >= 1)
+    # nlmeans/denoiser/noise.rs:200-246: each coefficient at a sigma of 1.
+    h2_unit = h2_inv_norm(float(f(strength) * f(1.0) * f(255.0)), s)
+    scale = f(3.0) if c == 1 else f(1.5)
+    offset_unit = float(((f(2.0) * scale) * f(1.0)) * area) if noise_floor else 0.0
+    conf = temporal_confidence and d > 0
+    settings = fold_words(w, h, sigma_scale=sigma_scale, h2_per_inverse_variance=h2_unit if auto_strength else None,
+                          h2_fixed=h2_inv_norm(strength, s), offset_per_variance=offset_unit,
+                          confidence_sad_per_sigma=sad_noise_floor(16, 1.0) if conf else 0.0)
+    folds = fold_stream(readings, totals, settings, c, a, d)
+    n = len(frames)
+    outs = []
+    for i in range(n):
+        window = [frames[min(max(i + k, 0), n - 1)] for k in range(-d, d + 1)]
+        derived, lut = folds[i][1], folds[i][2]
+        cf, blocks = None, (1, 1)
+        if conf:
+            cf, blocks = hq_confidence(window, d, 0.0, thsad_scale, sad_floor=float(derived[5]))
+        outs.append(nlm_frame(window, d, a, s, float(derived[6]), noise_offset=float(derived[8]), lut=lut, conf=cf,
+                              conf_step=8, blocks=blocks, wref=wref, fp64=fp64))
+    return outs, folds
 
 
 # ---- NLMeans adjoint (nlm_backward_oracle.cpp) -----------------------------------------------------
