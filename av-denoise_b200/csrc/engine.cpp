@@ -198,39 +198,16 @@ class NlmPass final : public Pass {
         return std::nullopt;
     }
 
-    // The measured noise state (noise/state.rs:172-330 `measurement_buffers`, lookahead.rs:53-112):
-    // the 8-frame look-ahead ring, one frame's Immerkaer partials and temporal records, the reading
-    // scratch, a history of 17 + d readings, the fold settings and state, the derived words and the
-    // two offset tables of the search window.
+    // The measured noise state (noise/state.rs:172-330 `measurement_buffers`, lookahead.rs:53-112)
+    // with the fold coefficients of nlmeans/denoiser/noise.rs:200-246 (each factor at a sigma of 1).
     std::optional<Failure> allocate_noise() {
-        const size_t fe = frame_elems();
-        const int w = static_cast<int>(width_), h = static_cast<int>(height_);
-        const int c = static_cast<int>(params_.channel_count());
-        history_capacity_ = 2 * kNoiseWindowRadius + 1 + params_.temporal_radius;
-        const uint32_t side = 2 * params_.search_radius + 1;
-        cudaError_t e;
-        if ((e = lookahead_.alloc(fe * kLookaheadFrames * sizeof(float))) != cudaSuccess)
-            return gpu_failure("look-ahead ring", e);
-        if ((e = partials_.alloc(immerkaer_partials_len(w, h) * sizeof(float))) != cudaSuccess)
-            return gpu_failure("noise partials", e);
-        if (params_.temporal_radius > 0) {
-            if ((e = records_.alloc(noise_records_floats(w, h, c) * sizeof(float))) != cudaSuccess)
-                return gpu_failure("noise records", e);
-            if ((e = noise_scratch_.alloc(noise_scratch_floats(w, h) * sizeof(float))) != cudaSuccess)
-                return gpu_failure("noise scratch", e);
-        }
-        if ((e = history_records_.alloc(history_capacity_ * kReadingWords * sizeof(float))) != cudaSuccess)
-            return gpu_failure("noise history", e);
-        if ((e = history_results_.alloc(history_capacity_ * 2 * sizeof(float))) != cudaSuccess)
-            return gpu_failure("noise history", e);
-        if ((e = fold_settings_.alloc(16 * sizeof(float))) != cudaSuccess) return gpu_failure("fold settings", e);
-        if ((e = fold_state_.alloc(32 * sizeof(float))) != cudaSuccess) return gpu_failure("fold state", e);
-        if ((e = noise_derived_.alloc(16 * sizeof(float))) != cudaSuccess) return gpu_failure("derived words", e);
-        if ((e = pilot_lut_.alloc(side * side * sizeof(float))) != cudaSuccess) return gpu_failure("pilot table", e);
-        for (DeviceBuffer* b : {&history_records_, &history_results_, &fold_state_, &noise_derived_})
-            if ((e = cudaMemset(b->ptr, 0, b->bytes)) != cudaSuccess) return gpu_failure("noise state clear", e);
-        // nlmeans/denoiser/noise.rs:200-246 (`derived_coefficients`): each factor at a sigma of 1.
-        FoldCoefficients k;
+        NoiseFrontConfig cfg;
+        cfg.width = width_;
+        cfg.height = height_;
+        cfg.channels = params_.channel_count();
+        cfg.temporal_radius = params_.temporal_radius;
+        cfg.table_radius = params_.search_radius;
+        FoldCoefficients& k = cfg.coefficients;
         k.sigma_scale = params_.hq_params.sigma_scale;
         k.h2_auto = params_.hq_params.auto_strength;
         k.h2_per_inverse_variance = h2_inv_norm_with(params_, true, 1.0f);
@@ -238,11 +215,7 @@ class NlmPass final : public Pass {
         const float unit[1] = {1.0f};
         k.offset_per_variance = noise_offset_with(params_, unit, 1);
         k.confidence_sad_per_sigma = conf_pass_ ? avd_sad_noise_floor(kConfBlk, 1.0f) : 0.0f;
-        float words[16];
-        noise_fold_words(width_, height_, k, words);
-        if ((e = cudaMemcpy(fold_settings_.ptr, words, sizeof(words), cudaMemcpyHostToDevice)) != cudaSuccess)
-            return gpu_failure("fold settings upload", e);
-        return std::nullopt;
+        return noise_.allocate(cfg);
     }
 
     static Failure gpu_failure(const char* what, cudaError_t e) { return Failure{AVD_ERR_GPU, cuda_message(what, e)}; }
@@ -303,77 +276,30 @@ class NlmPass final : public Pass {
         return prime_leading_edge_if_first();
     }
 
-    // ---- the noise look-ahead (nlmeans/denoiser/lookahead.rs:182-259, 425-444) ----
-    size_t held() const { return measures_ ? la_pushed_ - la_released_ : 0; }
-    float* lookahead_slot(size_t frame) const { return lookahead_.as<float>() + (frame % kLookaheadFrames) * frame_elems(); }
+    // ---- the noise look-ahead (nlmeans/denoiser/lookahead.rs:182-259) ----
+    size_t held() const { return measures_ ? noise_.held() : 0; }
 
     std::optional<Failure> push_into_lookahead(const AvdPlane* planes) {
-        if (held() == kLookaheadFrames) {
+        if (noise_.held() == NoiseFront::kFrames) {
             bool released = false;
             if (auto f = release_held_frame(&released)) return f;
         }
-        const size_t frame = la_pushed_;
-        if (auto f = ingest_into(planes, lookahead_slot(frame))) return f;
-        if (auto f = read_lookahead_noise(frame)) return f;
-        la_pushed_ += 1;
-        return std::nullopt;
-    }
-
-    // Reads stream frame `frame` against the frame before it and records the reading in history slot
-    // frame % capacity (noise/slot.rs:32-60, 158-175; noise/history.rs:131-160). A stream's first
-    // frame has nothing before it: its records are zero.
-    std::optional<Failure> read_lookahead_noise(size_t frame) {
-        const int w = static_cast<int>(width_), h = static_cast<int>(height_);
-        const int c = static_cast<int>(params_.channel_count());
-        const size_t hs = frame % history_capacity_;
-        float* reading = history_records_.as<float>() + hs * kReadingWords;
-        float* results = history_results_.as<float>() + hs * 2;
-        cudaError_t e = launch_immerkaer(lookahead_slot(frame), c, w, h, immerkaer_sigma_scale(), partials_.as<float>(),
-                                         results, reading, stream);
-        if (e != cudaSuccess) return gpu_failure("noise estimate launch", e);
-        const float* records = nullptr;
-        if (params_.temporal_radius > 0) {
-            const float* prev = frame > 0 ? lookahead_slot(frame - 1) : nullptr;
-            e = launch_temporal_stats(lookahead_slot(frame), prev, c, w, h, records_.as<float>(), stream);
-            if (e != cudaSuccess) return gpu_failure("temporal noise stats launch", e);
-            records = records_.as<float>();
-        }
-        const uint32_t blocks = static_cast<uint32_t>(((width_ + 15) / 16) * ((height_ + 15) / 16));
-        e = launch_noise_reading(records, c, w, h, noise_scratch_.as<float>(), min_static_blocks(blocks), reading,
-                                 stream);
-        if (e != cudaSuccess) return gpu_failure("noise reading launch", e);
-        recorded_ = std::max(recorded_, frame + 1);
-        return std::nullopt;
+        if (auto f = ingest_into(planes, noise_.slot(noise_.pushed()))) return f;
+        return noise_.read_pushed(stream);
     }
 
     // lookahead.rs:226-259 (`release_held_frame`): the oldest held frame enters the next ring slot.
     std::optional<Failure> release_held_frame(bool* released) {
         *released = false;
-        if (held() == 0) return std::nullopt;
-        const size_t frame = la_released_;
+        if (!measures_) return std::nullopt;
+        const std::optional<size_t> frame = noise_.take_oldest();
+        if (!frame) return std::nullopt;
         const size_t slot = ring_head_ % total_frames();
-        cudaError_t e = cudaMemcpyAsync(slot_ptr(slot), lookahead_slot(frame), frame_elems() * sizeof(float),
+        cudaError_t e = cudaMemcpyAsync(slot_ptr(slot), noise_.slot(*frame), frame_elems() * sizeof(float),
                                         cudaMemcpyDeviceToDevice, stream);
         if (e != cudaSuccess) return gpu_failure("look-ahead release", e);
-        la_released_ += 1;
         *released = true;
         return enter_ring(slot);
-    }
-
-    // nlmeans/denoiser/noise.rs:171-185 (`update_noise_estimate`): the fold of the window around the
-    // centre frame, reaching every recorded frame ahead up to the window radius.
-    std::optional<Failure> update_noise_estimate() {
-        const int64_t centre = centre_frame();
-        const int64_t newest = static_cast<int64_t>(recorded_) - 1;
-        const int first = static_cast<int>(std::max<int64_t>(centre - kNoiseWindowRadius, 0));
-        const int last = static_cast<int>(std::min<int64_t>(centre + kNoiseWindowRadius, newest));
-        cudaError_t e = launch_noise_fold(history_records_.as<float>(), history_results_.as<float>(),
-                                          static_cast<int>(history_capacity_), first, last, fold_settings_.as<float>(),
-                                          static_cast<int>(params_.channel_count()),
-                                          static_cast<int>(params_.search_radius), fold_state_.as<float>(),
-                                          noise_derived_.as<float>(), lut_.as<float>(), pilot_lut_.as<float>(), stream);
-        if (e != cudaSuccess) return gpu_failure("noise fold launch", e);
-        return std::nullopt;
     }
 
     // ring.rs:12-20.
@@ -431,7 +357,7 @@ class NlmPass final : public Pass {
             if (l != d) m.inline_slots[n++] = static_cast<uint32_t>(phys_frame(l));
         m.mv_field = mv_scratch_.as<int32_t>();
         m.confidence = conf_.as<float>();
-        m.noise = measures_ ? noise_derived_.as<float>() : derived_.as<float>();
+        m.noise = measures_ ? noise_.derived() : derived_.as<float>();
         m.width = static_cast<int>(width_);
         m.height = static_cast<int>(height_);
         m.frame_count = static_cast<int>(total_frames());
@@ -473,7 +399,7 @@ class NlmPass final : public Pass {
         // dispatch/mod.rs:640-644: the look-ahead has read every frame the window reaches, so the fold
         // runs first and the confidence pass reads this centre's own derived words.
         if (measures_)
-            if (auto f = update_noise_estimate()) return f;
+            if (auto f = noise_.fold(centre_frame(), stream)) return f;
         const int d = static_cast<int>(params_.temporal_radius);
         NlmLaunch a{};
         a.ring = ring_.as<float>();
@@ -490,10 +416,10 @@ class NlmPass final : public Pass {
         }
         a.patch_radius = static_cast<int>(params_.patch_radius);
         a.search_radius = static_cast<int>(params_.search_radius);
-        a.derived = measures_ ? noise_derived_.as<float>() : derived_.as<float>();
+        a.derived = measures_ ? noise_.derived() : derived_.as<float>();
         a.h2_word = measures_ ? kDerivedH2 : 0;
         a.offset_word = measures_ ? kDerivedNoiseOffset : 1;
-        a.spatial_lut = params_.hq ? lut_.as<float>() : nullptr;
+        a.spatial_lut = measures_ ? noise_.spatial_table() : (params_.hq ? lut_.as<float>() : nullptr);
         a.conf = nullptr;
         if (conf_pass_) {
             if (auto f = run_confidence_pass()) return f;
@@ -550,18 +476,12 @@ class NlmPass final : public Pass {
         next_output_slot_ = 0;
         real_pushes_ = 0;
         pushed_ = false;
-        la_pushed_ = 0;
-        la_released_ = 0;
-        recorded_ = 0;
+        if (measures_) noise_.reset();
     }
 
-    static constexpr int kNoiseWindowRadius = 8;  // noise/history.rs:10
-    static constexpr int kReadingWords = 30;      // noise/reading.rs:33
     static constexpr int kDerivedConfidenceSadFloor = 5, kDerivedH2 = 6, kDerivedNoiseOffset = 8;  // derived.rs:9-31
     bool measures_ = false;
-    size_t la_pushed_ = 0, la_released_ = 0, recorded_ = 0, history_capacity_ = 0;
-    DeviceBuffer lookahead_, partials_, records_, noise_scratch_, history_records_, history_results_, fold_settings_,
-        fold_state_, noise_derived_, pilot_lut_;
+    NoiseFront noise_;
 
     NlmParams params_;
     size_t held_ = 0;

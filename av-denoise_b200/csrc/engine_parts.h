@@ -117,6 +117,44 @@ class Pass {
     cudaStream_t stream = nullptr;
 };
 
+// The noise look-ahead of a front that measures the noise (noise_front.cpp).
+struct NoiseFrontConfig {
+    uint32_t width = 0, height = 0, channels = 1, temporal_radius = 0;
+    uint32_t table_radius = 0;  // the NLM offset tables' search radius, 0 for none
+    FoldCoefficients coefficients;
+    bool motion = false;  // read each frame along the motion to the frame before it
+    int blksize = 16, overlap = 8, search_radius = 4, levels = 2;
+    float thsad = 0.0f;
+};
+
+class NoiseFront {
+   public:
+    static constexpr size_t kFrames = 8;  // nlmeans/denoiser/lookahead.rs:30
+    std::optional<Failure> allocate(const NoiseFrontConfig& cfg);
+    // The look-ahead slot of stream frame `frame`.
+    float* slot(size_t frame) const;
+    size_t held() const { return pushed_ - released_; }
+    size_t pushed() const { return pushed_; }
+    // Reads stream frame pushed(), which the caller has just ingested into slot(pushed()).
+    std::optional<Failure> read_pushed(cudaStream_t s);
+    // The oldest held stream frame, now released, or none when nothing is held.
+    std::optional<size_t> take_oldest();
+    // Folds the window around stream frame `centre` into the derived words and tables.
+    std::optional<Failure> fold(uint32_t centre, cudaStream_t s);
+    float* derived() const { return derived_.as<float>(); }
+    float* spatial_table() const { return spatial_.as<float>(); }
+    void reset();
+
+   private:
+    std::optional<Failure> search(size_t centre_frame, size_t neighbour_frame, int direction, cudaStream_t s);
+    std::optional<Failure> read_against(size_t frame, std::optional<size_t> prev, int direction, cudaStream_t s);
+    NoiseFrontConfig cfg_;
+    size_t capacity_ = 0, pushed_ = 0, released_ = 0, recorded_ = 0;
+    int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2;
+    DeviceBuffer lookahead_, partials_, records_, scratch_, history_records_, history_results_, settings_, state_,
+        derived_, spatial_, pilot_, pyramid_, pair_;
+};
+
 // NL4D pass over one plane group (nl4d_pass.cpp).
 std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels channels, uint32_t width,
                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,

@@ -129,7 +129,9 @@ size_t immerkaer_partials_len(int width, int height);
 // Automatic noise estimate without motion compensation (noise_estimate.cu).
 size_t noise_scratch_floats(int width, int height);
 size_t noise_records_floats(int width, int height, int channels);
+// With `mv_field` (null for none) each block reads `prev` along its motion block's vector.
 cudaError_t launch_temporal_stats(const float* next, const float* prev, int channels, int width, int height,
+                                  const int32_t* mv_field, int mv_blocks_x, int mv_blocks_y, int mv_step,
                                   float* records, cudaStream_t s);
 cudaError_t launch_noise_reading(const float* records, int channels, int width, int height, float* scratch,
                                  uint32_t min_accepted, float* reading, cudaStream_t s);

@@ -1,5 +1,5 @@
 // NL4D pass over one plane group: the collaborative denoiser of av-denoise-core/src/nl4d with its
-// NLMeans-HQ front end, for a pinned sigma.
+// NLMeans-HQ front end, for a pinned sigma or (luma without the noise map) the automatic estimate.
 //
 //   engine       <- nl4d/engine.rs:208-410 (push, push_context, emit_into, finish, reset, pending
 //                   regions, the lazily queued tail)
@@ -47,9 +47,16 @@ class Nl4dPass final : public Pass {
     static std::optional<Failure> create(const AvdNl4dOptions& o, Channels channels, uint32_t width,
                                          uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
                                          std::unique_ptr<Pass>* result) {
-        if (!o.has_sigma)
+        // nl4d/denoiser.rs:228-233: without a pinned sigma the front measures the noise; luma applies
+        // the noise map and chroma the colour gains, neither of which is built.
+        if (!o.has_sigma && channels == Channels::Chroma)
             return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "NL4D with the automatic noise estimate is not available in this build yet; set sigma"};
+                           "NL4D chroma with the automatic noise estimate needs the colour grain gains, which are "
+                           "not available in this build; set sigma"};
+        if (!o.has_sigma && o.noise_map)
+            return Failure{AVD_ERR_INVALID_OPTIONS,
+                           "the NL4D luma noise map of the automatic noise estimate is not available in this build; "
+                           "set noise_map to false or set sigma"};
         const AvdMotionSearch& m = o.motion;
         if (m.max_search_escalation > m.search_radius)
             return Failure{AVD_ERR_INVALID_OPTIONS,
@@ -86,6 +93,7 @@ class Nl4dPass final : public Pass {
         p->thsad_ = avd_thsad(m.blksize, o.thsad_scale);
         p->chained_ = chained;
         p->refine_radius_ = static_cast<int>(refine_radius);
+        p->measures_ = !o.has_sigma;
         if (auto f = p->allocate()) return f;
         *result = std::move(p);
         return std::nullopt;
@@ -142,11 +150,12 @@ class Nl4dPass final : public Pass {
         return std::nullopt;
     }
 
-    // nl4d/engine.rs:368-381 with nl4d/denoiser.rs:496-505 (no look-ahead with a pinned sigma).
+    // nl4d/engine.rs:368-381 with nl4d/denoiser.rs:496-545 (`finish_count`): the regions the held
+    // frames' passes complete, then the tail's.
     std::optional<Failure> finish(size_t* tail) override {
         if (poisoned_) return status(AVD_ERR_NEEDS_RESET);
         if (!pending_.empty() || tail_remaining_ > 0) return status(AVD_ERR_OUTPUTS_PENDING);
-        const size_t count = std::min<size_t>(real_pushes_, 2 * d_);
+        const size_t count = drained_region_count() + std::min<size_t>(real_pushes_ + held(), 2 * d_);
         if (count == 0)
             restart_stream();
         else
@@ -170,7 +179,8 @@ class Nl4dPass final : public Pass {
         s.edges = 1;  // EdgePadding::Shifted
         return s;
     }
-    uint32_t next_frame() const override { return static_cast<uint32_t>(real_pushes_); }
+    // nlmeans/edges.rs:26-31: the stream frame the next push takes, held frames included.
+    uint32_t next_frame() const override { return static_cast<uint32_t>(real_pushes_ + held()); }
     std::optional<uint32_t> emitted_frame() const override { return emitted_; }
     AvdEngineTiming timing() override { return timer_.collect(); }
     void sample_device_time(uint32_t every) override { timer_.every = every; }
@@ -263,10 +273,38 @@ class Nl4dPass final : public Pass {
             return gpu_failure("slot tables upload", e);
         slot_frames_.assign(t, 0u);
         zeroed_.assign(t, false);
+        if (measures_) {
+            // nl4d/denoiser.rs:268-284 and nlmeans/denoiser/noise.rs:200-246: the front's fold
+            // coefficients (its own NLMeans defaults, strength 1.2 and patch radius 4, at a sigma of
+            // 1), the consumer's DCT gain and the motion SAD floor per unit sigma.
+            NoiseFrontConfig cfg;
+            cfg.width = width_;
+            cfg.height = height_;
+            cfg.channels = C();
+            cfg.temporal_radius = d_;
+            FoldCoefficients& k = cfg.coefficients;
+            k.sigma_scale = opts_.sigma_scale;
+            k.weight_g_max = g_max;
+            k.h2_auto = true;
+            const float area = 81.0f, unit_strength = 1.2f * 1.0f * 255.0f;
+            k.h2_per_inverse_variance = (255.0f * 255.0f) / (3.0f * unit_strength * unit_strength * area);
+            k.h2_fixed = (255.0f * 255.0f) / (3.0f * 1.2f * 1.2f * area);
+            k.offset_per_variance = 2.0f * (channels_ == Channels::Luma ? 3.0f : 1.5f) * 1.0f * area;
+            k.sad_per_sigma = avd_sad_noise_floor(opts_.motion.blksize, 1.0f);
+            cfg.motion = true;
+            cfg.blksize = static_cast<int>(opts_.motion.blksize);
+            cfg.overlap = static_cast<int>(opts_.motion.overlap);
+            cfg.search_radius = static_cast<int>(opts_.motion.search_radius);
+            cfg.levels = static_cast<int>(opts_.motion.pyramid_levels);
+            cfg.thsad = thsad_;
+            if (auto f = noise_.allocate(cfg)) return f;
+        }
         return std::nullopt;
     }
 
-    const float* noise_words() const { return tables_.as<float>(); }
+    // The derived words a pass reads (sigma per channel, weight scale, curve flag, motion SAD floor):
+    // the measured front's, or the pinned sigma's.
+    const float* noise_words() const { return measures_ ? noise_.derived() : tables_.as<float>(); }
     const float* noise_curve() const { return tables_.as<float>() + 8; }
     const float* dct_profile() const { return tables_.as<float>() + 24; }
     const float* kaiser_taps() const { return tables_.as<float>() + 32; }
@@ -306,13 +344,33 @@ class Nl4dPass final : public Pass {
         return std::nullopt;
     }
 
+    // nlmeans/denoiser/mod.rs:484-512: a measured front reads the frame in the look-ahead and
+    // releases the frame pushed 8 pushes earlier into the ring.
     std::optional<Failure> push_planes(const AvdPlane* planes) {
+        if (measures_) {
+            if (noise_.held() == NoiseFront::kFrames) {
+                bool released = false;
+                if (auto f = release_held_frame(&released)) return f;
+            }
+            if (auto f = ingest_into(planes, noise_.slot(noise_.pushed()))) return f;
+            return noise_.read_pushed(stream);
+        }
         const size_t slot = ring_head_ % tf();
+        if (auto f = ingest_into(planes, slot_ptr(slot))) return f;
+        return enter_ring(slot);
+    }
+
+    std::optional<Failure> ingest_into(const AvdPlane* planes, float* dst) {
         const void* p0 = reinterpret_cast<const void*>(planes[0].ptr);
         const void* p1 = C() > 1 ? reinterpret_cast<const void*>(planes[1].ptr) : nullptr;
-        cudaError_t e = launch_ingest(p0, p1, slot_ptr(slot), static_cast<int64_t>(pixels()), static_cast<int>(C()),
+        cudaError_t e = launch_ingest(p0, p1, dst, static_cast<int64_t>(pixels()), static_cast<int>(C()),
                                       plane_format(in_), bias(), stream);
         if (e != cudaSuccess) return gpu_failure("ingest launch", e);
+        return std::nullopt;
+    }
+
+    // nlmeans/denoiser/stages.rs:15-40: the per-frame stages of a frame entering ring slot `slot`.
+    std::optional<Failure> enter_ring(size_t slot) {
         if (auto f = build_pyramid(slot)) return f;
         if (auto f = pair_analyse(slot)) return f;
         slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
@@ -320,6 +378,36 @@ class Nl4dPass final : public Pass {
         if (frames_loaded_ < tf()) frames_loaded_ += 1;
         real_pushes_ += 1;
         return std::nullopt;
+    }
+
+    size_t held() const { return measures_ ? noise_.held() : 0; }
+
+    // nlmeans/denoiser/lookahead.rs:226-259 (`release_held_frame`).
+    std::optional<Failure> release_held_frame(bool* released) {
+        *released = false;
+        if (!measures_) return std::nullopt;
+        const std::optional<size_t> frame = noise_.take_oldest();
+        if (!frame) return std::nullopt;
+        const size_t slot = ring_head_ % tf();
+        cudaError_t e = cudaMemcpyAsync(slot_ptr(slot), noise_.slot(*frame), frame_elems() * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return gpu_failure("look-ahead release", e);
+        *released = true;
+        return enter_ring(slot);
+    }
+
+    // nl4d/denoiser.rs:511-538 (`drained_region_count`): the regions the passes of the held frames
+    // complete, following the pass count submit_passes keeps.
+    size_t drained_region_count() const {
+        uint64_t passes = passes_run_;
+        size_t regions = 0;
+        for (size_t taken = real_pushes_ + 1; taken <= real_pushes_ + held(); ++taken) {
+            if (taken < tf()) continue;
+            if (passes == 0 && !continuation_) passes += d_;
+            passes += 1;
+            if (passes > d_) regions += 1;
+        }
+        return regions;
     }
 
     // nlmeans/denoiser/ring.rs:128-146 and nlmeans/edges.rs:41-48.
@@ -392,6 +480,10 @@ class Nl4dPass final : public Pass {
 
     // nlmeans/denoiser/machinery.rs:45-102 then dispatch/motion.rs:173-229.
     std::optional<Failure> machinery_at(uint32_t centre) {
+        // machinery.rs:60-66: the look-ahead has read every frame the window reaches, so the fold
+        // around the pass's centre frame runs first and the match scores confidence against it.
+        if (measures_)
+            if (auto f = noise_.fold(slot_frames_[phys(centre)], stream)) return f;
         if (chained_) {
             // nlmeans/dispatch/motion.rs:138-171 then analyse.rs:273-316: every neighbour's seed
             // chained from the pair ring, then refined `refine_radius` around it with confidence.
@@ -523,8 +615,25 @@ class Nl4dPass final : public Pass {
         return std::nullopt;
     }
 
-    // nl4d/denoiser.rs:544-596 (`finish_passes`).
+    // nl4d/engine.rs:181-196 (`queue_tail_regions`): the look-ahead drains one region at a time
+    // (nl4d/denoiser.rs:478-494, `drain_lookahead`), then the tail passes run.
     std::optional<Failure> queue_tail_regions() {
+        for (;;) {
+            bool released = false;
+            if (auto f = release_held_frame(&released)) return f;
+            if (!released) break;
+            std::optional<uint32_t> region;
+            if (auto f = submit_passes(&region)) return f;
+            if (region) {
+                pending_.push_back(*region);
+                return std::nullopt;
+            }
+        }
+        return finish_passes();
+    }
+
+    // nl4d/denoiser.rs:544-596 (`finish_passes`).
+    std::optional<Failure> finish_passes() {
         const uint32_t emit = static_cast<uint32_t>(std::min<size_t>(real_pushes_, 2 * d_));
         if (emit == 0) return std::nullopt;
         const bool short_stream = real_pushes_ < tf();
@@ -583,6 +692,7 @@ class Nl4dPass final : public Pass {
         tail_remaining_ = 0;
         pushes_ = 0;
         pushed_ = false;
+        if (measures_) noise_.reset();
     }
 
     AvdNl4dOptions opts_{};
@@ -597,6 +707,8 @@ class Nl4dPass final : public Pass {
     DeviceBuffer pair_ring_;
     bool chained_ = false;
     int refine_radius_ = 2;
+    bool measures_ = false;
+    NoiseFront noise_;
     DeviceBuffer outputs_[2];
 
     size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;

@@ -5,7 +5,8 @@
 //   kernels/stats.rs:141-420   `nlm_temporal_noise_stats`: per 16x16 block the per-channel sums of
 //                              d = new - prev and d^2 and the lag-1 channel-0 product, each summed
 //                              over the block's 256 threads in thread order; each channel's texture
-//                              from 4x4 cell means (stats.rs:599-650). No luma quarter fields.
+//                              from 4x4 cell means (stats.rs:599-650); with a motion field, the
+//                              compensated variant's vector check. No luma quarter fields.
 //   kernels/sample.rs:143-803  `noise_block_derive`, `noise_block_accept`, `noise_sample_finish`:
 //                              the static gate, the outlier ceiling, the moved-texture threshold, the
 //                              kept sigmas' median and lower quartile, the median correlation.
@@ -66,20 +67,79 @@ __device__ __forceinline__ float key_value(uint32_t k) {
 
 // ---- temporal stats ---------------------------------------------------------------------------
 
-template <int C>
+// The motion field a compensated read follows: (dx, dy) per block of a blocks_x x blocks_y grid at
+// `step`, each noise block taking the vector of the motion block covering its origin.
+struct StatsMotion {
+    const int32_t* field;
+    int blocks_x, blocks_y, step;
+};
+
+template <int C, bool COMP>
 __global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __restrict__ next,
                                                              const float* __restrict__ prev, int width, int height,
-                                                             float* __restrict__ records) {
+                                                             StatsMotion motion, float* __restrict__ records) {
     constexpr int L = 2 * C + 1;
-    __shared__ float scratch[256 * L];
-    __shared__ float tile[256];
+    // The lane scratch, then the cell tile; the compensated variant's four variance runs of 256
+    // threads each alias the start of it before the lanes are written.
+    constexpr int kScratch = 256 * L + 256 > 1024 ? 256 * L + 256 : 1024;
+    __shared__ float smem[kScratch];
     __shared__ float cells[16];
+    float* scratch = smem;
+    float* tile = smem + 256 * L;
     const int t = threadIdx.x, lx = t % kNB, ly = t / kNB;
     const int x0 = blockIdx.x * kNB, y0 = blockIdx.y * kNB;
     const int gx = x0 + lx, gy = y0 + ly;
     const int bw = min(kNB, width - x0), bh = min(kNB, height - y0);
-    const bool valid = gx < width && gy < height;
     float* out = records + (static_cast<int64_t>(blockIdx.y) * gridDim.x + blockIdx.x) * record_len(C);
+    auto at = [&](int x, int y, int c) { return (static_cast<int64_t>(y) * width + x) * C + c; };
+
+    int sx = 0, sy = 0;
+    bool matched = true, moved = false;
+    if (COMP) {
+        // kernels/stats.rs:224-330: the block follows its vector only when the channel-0 residual
+        // variance along it is at most half the zero-vector variance (or nothing of it matches).
+        const int col = min(x0 / motion.step, motion.blocks_x - 1), row = min(y0 / motion.step, motion.blocks_y - 1);
+        const int vx = motion.field[(row * motion.blocks_x + col) * 2];
+        const int vy = motion.field[(row * motion.blocks_x + col) * 2 + 1];
+        float zr = 0.0f, vr = 0.0f;
+        if (gx < width && gy < height) {
+            const float nl = next[at(gx, gy, 0)];
+            zr = nl - prev[at(gx, gy, 0)];
+            const int mx = gx + vx, my = gy + vy;
+            if (mx >= 0 && mx < width && my >= 0 && my < height) vr = nl - prev[at(mx, my, 0)];
+        }
+        smem[t] = zr;
+        smem[256 + t] = zr * zr;
+        smem[512 + t] = vr;
+        smem[768 + t] = vr * vr;
+        __syncthreads();
+#pragma unroll
+        for (int stride = 128; stride >= 1; stride >>= 1) {
+            if (t < stride) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) smem[r * 256 + t] += smem[r * 256 + t + stride];
+            }
+            __syncthreads();
+        }
+        const float zero_sum = smem[0], zero_sq = smem[256], vec_sum = smem[512], vec_sq = smem[768];
+        __syncthreads();
+        const int left = x0 + vx, top = y0 + vy, right = left + bw, bottom = top + bh;
+        const int ow = max(min(right, width) - max(left, 0), 0), oh = max(min(bottom, height) - max(top, 0), 0);
+        const float matched_pixels = static_cast<float>(ow * oh), block_pixels = static_cast<float>(bw * bh);
+        const float zero_mean = zero_sum / block_pixels;
+        const float zero_var = zero_sq / block_pixels - zero_mean * zero_mean;
+        const float safe = fmaxf(matched_pixels, 1.0f);
+        const float vec_mean = vec_sum / safe;
+        const float vec_var = vec_sq / safe - vec_mean * vec_mean;
+        const bool follows = (vx != 0 || vy != 0) && (matched_pixels == 0.0f || vec_var <= 0.5f * zero_var);
+        if (follows) {
+            sx = vx;
+            sy = vy;
+            matched = left >= 0 && right <= width && top >= 0 && bottom <= height;
+        }
+        moved = follows && matched;
+    }
+    const bool valid = gx < width && gy < height && matched;
 
     float nv[C], d[C];
 #pragma unroll
@@ -87,9 +147,8 @@ __global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __rest
         nv[c] = 0.0f;
         d[c] = 0.0f;
         if (valid) {
-            const int64_t at = (static_cast<int64_t>(gy) * width + gx) * C + c;
-            nv[c] = next[at];
-            d[c] = nv[c] - prev[at];
+            nv[c] = next[at(gx, gy, c)];
+            d[c] = nv[c] - prev[at(gx + sx, gy + sy, c)];
         }
         scratch[t * L + c] = d[c];
         scratch[t * L + C + c] = d[c] * d[c];
@@ -104,8 +163,9 @@ __global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __rest
         for (int i = 0; i < 256; ++i) total += scratch[i * L + t];
         out[t] = total;
     }
-    // The moved lane and the quarter lanes are written as zero (no motion, no luma fields).
-    if (t >= 2 * C + 2 && t < 2 * C + 27) out[t] = 0.0f;
+    // The moved lane, then the quarter lanes as zero (no luma fields).
+    if (t == 2 * C + 2) out[t] = moved ? 1.0f : 0.0f;
+    if (t > 2 * C + 2 && t < 2 * C + 27) out[t] = 0.0f;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         __syncthreads();
@@ -568,15 +628,25 @@ size_t noise_records_floats(int width, int height, int channels) {
 }
 
 cudaError_t launch_temporal_stats(const float* next, const float* prev, int channels, int width, int height,
+                                  const int32_t* mv_field, int mv_blocks_x, int mv_blocks_y, int mv_step,
                                   float* records, cudaStream_t s) {
     if (channels < 1 || channels > 2 || width < 1 || height < 1) return cudaErrorInvalidValue;
+    if (mv_field && (mv_blocks_x < 1 || mv_blocks_y < 1 || mv_step < 1)) return cudaErrorInvalidValue;
     dim3 grid((width + kNB - 1) / kNB, (height + kNB - 1) / kNB);
     if (!prev)  // the first frame of a stream has no previous frame: its records are zero
         return cudaMemsetAsync(records, 0, noise_records_floats(width, height, channels) * sizeof(float), s);
-    if (channels == 1)
-        temporal_stats_kernel<1><<<grid, 256, 0, s>>>(next, prev, width, height, records);
-    else
-        temporal_stats_kernel<2><<<grid, 256, 0, s>>>(next, prev, width, height, records);
+    const StatsMotion m{mv_field, mv_blocks_x, mv_blocks_y, mv_step};
+    if (channels == 1) {
+        if (mv_field)
+            temporal_stats_kernel<1, true><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
+        else
+            temporal_stats_kernel<1, false><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
+    } else {
+        if (mv_field)
+            temporal_stats_kernel<2, true><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
+        else
+            temporal_stats_kernel<2, false><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
+    }
     return cudaGetLastError();
 }
 

@@ -79,9 +79,26 @@ AvdStatus avd_noise_temporal_stats(uint64_t next, uint64_t prev, uint32_t channe
         return fail(AVD_ERR_INVALID_GEOMETRY, "noise temporal stats: bad geometry");
     cudaError_t e = avd::launch_temporal_stats(reinterpret_cast<const float*>(next), reinterpret_cast<const float*>(prev),
                                                static_cast<int>(channels), static_cast<int>(width),
-                                               static_cast<int>(height), reinterpret_cast<float*>(records),
-                                               static_cast<cudaStream_t>(stream));
+                                               static_cast<int>(height), nullptr, 0, 0, 0,
+                                               reinterpret_cast<float*>(records), static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("noise temporal stats launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+AvdStatus avd_noise_compensated_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width, uint32_t height,
+                                      uint64_t mv_field, uint32_t mv_blocks_x, uint32_t mv_blocks_y, uint32_t mv_step,
+                                      uint64_t records, void* stream) {
+    if (!next || !prev || !records || !mv_field) return fail(AVD_ERR_NULL_ARG, "noise compensated stats: null buffer");
+    if (channels < 1 || channels > 2 || width == 0 || height == 0 || mv_blocks_x == 0 || mv_blocks_y == 0 ||
+        mv_step == 0)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "noise compensated stats: bad geometry");
+    cudaError_t e = avd::launch_temporal_stats(
+        reinterpret_cast<const float*>(next), reinterpret_cast<const float*>(prev), static_cast<int>(channels),
+        static_cast<int>(width), static_cast<int>(height), reinterpret_cast<const int32_t*>(mv_field),
+        static_cast<int>(mv_blocks_x), static_cast<int>(mv_blocks_y), static_cast<int>(mv_step),
+        reinterpret_cast<float*>(records), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess)
+        return fail(AVD_ERR_GPU, std::string("noise compensated stats launch: ") + cudaGetErrorString(e));
     return AVD_OK;
 }
 

@@ -524,6 +524,15 @@ AVD_API uint64_t avd_noise_scratch_floats(uint32_t width, uint32_t height);
 AVD_API AvdStatus avd_noise_temporal_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width,
                                            uint32_t height, uint64_t records, void* stream);
 
+/* The records of `next` against `prev` along a motion field (kernels/stats.rs:224-330, the compensated
+ * variant): `mv_field` holds an int32 (dx, dy) per block of an mv_blocks_x x mv_blocks_y grid at
+ * `mv_step`; each 16x16 block follows the vector of the motion block covering its origin when its
+ * channel-0 residual variance along it is at most half the zero-vector variance, and a followed block
+ * that leaves the frame writes an all-zero record. The moved lane records each followed block. */
+AVD_API AvdStatus avd_noise_compensated_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width,
+                                              uint32_t height, uint64_t mv_field, uint32_t mv_blocks_x,
+                                              uint32_t mv_blocks_y, uint32_t mv_step, uint64_t records, void* stream);
+
 /* One frame's reading, AVD_NOISE_READING_WORDS floats (noise/reading.rs:7-33), from its records
  * (0 without temporal stats: the reading is then the Immerkaer words alone) through
  * kernels/sample.rs:143-803. Words 0 and 1 must already hold the frame's Immerkaer lower quartiles

@@ -172,6 +172,116 @@ void orc_temporal_stats(const float* next, const float* prev, int channels, int 
         }
 }
 
+// The records of `next` against `prev` along a motion field (kernels/stats.rs:224-330, the
+// `compensated` variant): each block reads the whole-pixel vector of the motion block covering its
+// origin (`mv`: (dx, dy) per block of an mv_bx x mv_by grid at `step`), follows it only when its
+// channel-0 residual variance along it is at most 0.5 of the zero-vector variance (or nothing of
+// it matches inside the frame), and writes an all-zero record when the followed block leaves the
+// frame. The four variance sums are halving-tree reductions over the block's 256 threads.
+void orc_temporal_stats_mc(const float* next, const float* prev, int channels, int w, int h, const int32_t* mv,
+                           int mv_bx, int mv_by, int step, float* records) {
+    const int bxn = (w + NB - 1) / NB, byn = (h + NB - 1) / NB, rl = record_len(channels);
+    const int lanes = 2 * channels + 1;
+    auto value = [&](const float* f, int x, int y, int c) { return f[(static_cast<int64_t>(y) * w + x) * channels + c]; };
+    std::vector<float> runs(4 * 256), scratch(256 * lanes), tile(256), cells(16), d0(256);
+    for (int by = 0; by < byn; ++by)
+        for (int bx = 0; bx < bxn; ++bx) {
+            const int x0 = bx * NB, y0 = by * NB;
+            const int bw = std::min(NB, w - x0), bh = std::min(NB, h - y0);
+            float* out = records + static_cast<int64_t>(by * bxn + bx) * rl;
+            const int col = std::min(x0 / step, mv_bx - 1), row = std::min(y0 / step, mv_by - 1);
+            const int vx = mv[(row * mv_bx + col) * 2], vy = mv[(row * mv_bx + col) * 2 + 1];
+            for (int t = 0; t < 256; ++t) {
+                const int gx = x0 + t % NB, gy = y0 + t / NB;
+                float zr = 0.0f, vr = 0.0f;
+                if (gx < w && gy < h) {
+                    const float nl = value(next, gx, gy, 0);
+                    zr = nl - value(prev, gx, gy, 0);
+                    const int mx = gx + vx, my = gy + vy;
+                    if (mx >= 0 && mx < w && my >= 0 && my < h) vr = nl - value(prev, mx, my, 0);
+                }
+                runs[t] = zr;
+                runs[256 + t] = zr * zr;
+                runs[512 + t] = vr;
+                runs[768 + t] = vr * vr;
+            }
+            for (int stride = 128; stride >= 1; stride >>= 1)
+                for (int t = 0; t < stride; ++t)
+                    for (int r = 0; r < 4; ++r) runs[r * 256 + t] += runs[r * 256 + t + stride];
+            const int left = x0 + vx, top = y0 + vy, right = left + bw, bottom = top + bh;
+            const int ow = std::max(std::min(right, w) - std::max(left, 0), 0);
+            const int oh = std::max(std::min(bottom, h) - std::max(top, 0), 0);
+            const float matched_pixels = static_cast<float>(ow * oh), block_pixels = static_cast<float>(bw * bh);
+            const float zero_mean = runs[0] / block_pixels;
+            const float zero_var = runs[256] / block_pixels - zero_mean * zero_mean;
+            const float safe = std::max(matched_pixels, 1.0f);
+            const float vec_mean = runs[512] / safe;
+            const float vec_var = runs[768] / safe - vec_mean * vec_mean;
+            const bool has_vector = vx != 0 || vy != 0;
+            const bool follows = has_vector && (matched_pixels == 0.0f || vec_var <= 0.5f * zero_var);
+            int sx = 0, sy = 0;
+            bool matched = true;
+            if (follows) {
+                sx = vx;
+                sy = vy;
+                matched = left >= 0 && right <= w && top >= 0 && bottom <= h;
+            }
+            std::fill(out, out + rl, 0.0f);
+            for (int t = 0; t < 256; ++t) {
+                const int lx = t % NB, gx = x0 + lx, gy = y0 + t / NB;
+                const bool valid = gx < w && gy < h && matched;
+                for (int c = 0; c < channels; ++c) {
+                    const float r = valid ? value(next, gx, gy, c) - value(prev, gx + sx, gy + sy, c) : 0.0f;
+                    scratch[t * lanes + c] = r;
+                    scratch[t * lanes + channels + c] = r * r;
+                    if (c == 0) d0[t] = r;
+                }
+            }
+            for (int t = 0; t < 256; ++t) {
+                const int lx = t % NB, gx = x0 + lx, gy = y0 + t / NB;
+                const bool valid = gx < w && gy < h && matched;
+                scratch[t * lanes + 2 * channels] = (valid && lx + 1 < bw) ? d0[t] * d0[t + 1] : 0.0f;
+            }
+            for (int lane = 0; lane < lanes; ++lane) {
+                float total = 0.0f;
+                for (int t = 0; t < 256; ++t) total += scratch[t * lanes + lane];
+                out[lane] = total;
+            }
+            for (int c = 0; c < channels; ++c) {
+                for (int t = 0; t < 256; ++t) {
+                    const int gx = x0 + t % NB, gy = y0 + t / NB;
+                    tile[t] = (gx < w && gy < h && matched) ? value(next, gx, gy, c) : 0.0f;
+                }
+                for (int i = 0; i < 16; ++i) {
+                    const int cx = i % 4, cy = i / 4;
+                    float cell = 0.0f;
+                    for (int dy = 0; dy < 4; ++dy)
+                        for (int dx = 0; dx < 4; ++dx) cell += tile[(4 * cy + dy) * NB + 4 * cx + dx];
+                    cells[i] = cell / 16.0f;
+                }
+                const int cols = bw / 4, rows = bh / 4;
+                float energy = 0.0f;
+                uint32_t pairs = 0;
+                for (int cy = 0; cy < rows; ++cy)
+                    for (int cx = 0; cx < cols; ++cx) {
+                        const float here = cells[cy * 4 + cx];
+                        if (cx + 1 < cols) {
+                            const float s = here - cells[cy * 4 + cx + 1];
+                            energy += s * s;
+                            ++pairs;
+                        }
+                        if (cy + 1 < rows) {
+                            const float s = here - cells[(cy + 1) * 4 + cx];
+                            energy += s * s;
+                            ++pairs;
+                        }
+                    }
+                out[texture_lane(channels, c)] = pairs ? energy / static_cast<float>(pairs) : 0.0f;
+            }
+            out[2 * channels + 2] = (follows && matched) ? 1.0f : 0.0f;
+        }
+}
+
 // One slot's reading (READING_WORDS floats). `records` may be null without temporal stats;
 // `imm_low` holds the two Immerkaer lower quartiles (the quartile of the cube sigmas).
 void orc_noise_reading(const float* records, const float* imm_low, int channels, int w, int h, int temporal,

@@ -379,7 +379,7 @@ def chain_compose(pairs: dict, centre: int, d: int, head_mod: int, step: int, wi
 def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, overlap=8, search_radius=4,
                 levels=2, refine=2, spatial_radius=9, lambda_ht=4.158, c_min=0.05, kaiser_beta=2.0,
                 pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0, chained: bool = False,
-                refine_radius: int = 2) -> list[np.ndarray]:
+                refine_radius: int = 2, noise=None) -> list[np.ndarray]:
     """The NL4D engine with a pinned sigma and Direct motion (no camera model, no truemotion) over a
     stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order.
 
@@ -388,7 +388,9 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     one pass centred on the middle slot per push; after more than d passes each middle pass
     completes the region d slots behind it; at the end, tail passes centred on d+1..2d (or, for a
     stream shorter than the ring, on every real frame after padding with the last frame). The
-    first `context` frames are priming pushes (no head passes)."""
+    first `context` frames are priming pushes (no head passes). With `noise`, a function of a pass's
+    centre stream frame returning (sigma, weight_scale, sad_floor), each pass reads those (the
+    automatic estimate's fold around that frame) instead of the pinned sigma's."""
     h, w, c = frames[0].shape
     tf = 2 * d + 1
     step = blksize - overlap
@@ -420,20 +422,24 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
             zeroed[i] = False
         st["passes"] += 1
         slots = [phys(l) for l in range(tf) if l != centre]
+        p_sigma, p_weight, p_floor = sigma, None, sad_floor
+        if noise is not None:
+            p_sigma, p_weight, p_floor = noise(slot_frames[cs])
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
         if chained:
             seeds = chain_compose(pairs, centre, d, st["head"] % (2 * d), step, w, h, bx, by)
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=refine_radius, levels=levels, confidence=True,
-                                     sad_floor=sad_floor, thsad=th, seeds=seeds)
+                                     sad_floor=p_floor, thsad=th, seeds=seeds)
         else:
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=search_radius, levels=levels, confidence=True,
-                                     sad_floor=sad_floor, thsad=th)
+                                     sad_floor=p_floor, thsad=th)
         acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
                                   confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
                                   c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
-                                  sigma=(sigma,) * c, lambda_ht=lambda_ht, kaiser_beta=kaiser_beta,
+                                  sigma=(p_sigma,) * c, weight_scale_override=p_weight, lambda_ht=lambda_ht,
+                                  kaiser_beta=kaiser_beta,
                                   pooled=pool_ratio, blksize=blksize, blk_step=step, blocks_x=bx, blocks_y=by,
                                   mv_stride=bx * by * 2, conf_stride=bx * by)
         accum[:] += acc.reshape(tf, -1)
@@ -557,6 +563,8 @@ def _noise_lib():
     l.orc_min_static_blocks.restype = C.c_uint32
     l.orc_temporal_stats.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, _fp]
     l.orc_noise_reading.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
+    l.orc_temporal_stats_mc.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int,
+                                        C.c_int, _fp]
     l.orc_fold_words.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, C.c_int, C.c_float,
                                  C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, C.c_float, _fp]
     l.orc_noise_fold.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, _fp, C.c_int, C.c_int, _fp, _fp, _fp, _fp]
@@ -583,6 +591,19 @@ def temporal_stats(new: np.ndarray, prev: np.ndarray, channels: int, width: int,
     out = np.zeros(bx * by * noise_record_len(channels), np.float32)
     _noise_lib().orc_temporal_stats(_f(np.ascontiguousarray(new, np.float32)),
                                     _f(np.ascontiguousarray(prev, np.float32)), channels, width, height, _f(out))
+    return out
+
+
+def temporal_stats_mc(new: np.ndarray, prev: np.ndarray, channels: int, width: int, height: int, mv: np.ndarray,
+                      mv_blocks: tuple[int, int], step: int) -> np.ndarray:
+    """The records of `new` against `prev` along the motion field `mv` ((bx * by, 2) int32)."""
+    bx, by = stats_blocks(width, height)
+    out = np.zeros(bx * by * noise_record_len(channels), np.float32)
+    field = np.ascontiguousarray(mv, np.int32).reshape(-1)
+    _noise_lib().orc_temporal_stats_mc(_f(np.ascontiguousarray(new, np.float32)),
+                                       _f(np.ascontiguousarray(prev, np.float32)), channels, width, height,
+                                       field.ctypes.data_as(C.POINTER(C.c_int32)), mv_blocks[0], mv_blocks[1], step,
+                                       _f(out))
     return out
 
 
@@ -646,6 +667,38 @@ def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: 
                 rec = temporal_stats(f, frames[i - 1], channels, width, height)
         readings.append(noise_reading(rec, low, channels, width, height, temporal))
         totals.append(tot)
+    return readings, totals
+
+
+def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, height: int, *, blksize: int,
+                      overlap: int, search_radius: int, levels: int):
+    """Every frame's reading as a motion-compensated look-ahead takes it
+    (nlmeans/denoiser/lookahead.rs:283-319, 425-458, 543-605): frame i >= 1 is searched against
+    frame i - 1 (newer to older) and read along that field; frame 1 is also searched older to newer
+    and frame 0 re-read along it. Frame 0 keeps its Immerkaer words from its own read. Returns
+    (readings, Immerkaer totals)."""
+    step = blksize - overlap
+    mb = (max(-(-width // step), 1), max(-(-height // step), 1))
+    kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels)
+    rec_len = stats_blocks(width, height)[0] * stats_blocks(width, height)[1] * noise_record_len(channels)
+    readings, totals, lows = [], [], []
+    for i, f in enumerate(frames):
+        _, tot, low = immerkaer(f, channels, width, height)
+        totals.append(tot)
+        lows.append(low)
+        if i == 0:
+            readings.append(noise_reading(np.zeros(rec_len, np.float32), low, channels, width, height, True))
+            continue
+        pair = np.stack([np.ascontiguousarray(frames[i - 1], np.float32),
+                         np.ascontiguousarray(f, np.float32)]).reshape(-1)
+        pyr = motion_pyramid(pair, channels, width, height, levels)
+        newer_to_older, _ = motion_search(pyr, width, height, 2, 1, [0], **kw)
+        rec = temporal_stats_mc(f, frames[i - 1], channels, width, height, newer_to_older[0], mb, step)
+        readings.append(noise_reading(rec, low, channels, width, height, True))
+        if i == 1:
+            older_to_newer, _ = motion_search(pyr, width, height, 2, 0, [1], **kw)
+            rec0 = temporal_stats_mc(frames[0], f, channels, width, height, older_to_newer[0], mb, step)
+            readings[0] = noise_reading(rec0, lows[0], channels, width, height, True)
     return readings, totals
 
 

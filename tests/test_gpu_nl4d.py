@@ -115,8 +115,12 @@ def test_nl4d_continuation_skips_head_passes(oracle):
 def test_nl4d_options_this_build_rejects():
     fmt = avd.SampleFormat.u8()
     g = avd.Geometry(64, 48, avd.ChromaLayout.GRAY, fmt, fmt)
-    with pytest.raises(avd.InvalidOptions, match="automatic noise estimate"):
+    # The automatic estimate is built for luma without the noise map (tests/test_gpu_nl4d_auto.py).
+    with pytest.raises(avd.InvalidOptions, match="noise map"):
         avd.build_engine(avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=1), None, g))
+    g420 = avd.Geometry(64, 48, avd.ChromaLayout.YUV420, fmt, fmt)
+    with pytest.raises(avd.InvalidOptions, match="colour grain gains"):
+        avd.build_engine(avd.EngineSpec.nl4d(None, avd.Nl4dOptions(temporal_radius=1, noise_map=False), g420))
     escalating = avd.Nl4dOptions(sigma=0.03, temporal_radius=1, motion=avd.MotionSearch(max_search_escalation=8))
     with pytest.raises(avd.InvalidOptions, match="escalation"):
         avd.build_engine(avd.EngineSpec.nl4d(escalating, None, g))

@@ -1,0 +1,71 @@
+"""NL4D with the automatic noise estimate (luma, no sigma, noise map off) on the GPU through the C
+ABI against the oracle's stream restatement: the 8-frame look-ahead searches each frame against the
+one before it, reads the noise along that motion (the first frame again along the motion to the
+second), and every pass folds the window around its centre frame into the sigma, weight scale and
+motion SAD floor it filters with (nlmeans/denoiser/lookahead.rs, nl4d/denoiser.rs, noise/*).
+
+Every stage is bit-exact, so every output sample is identical to the oracle's."""
+
+import numpy as np
+import pytest
+
+from conftest import avd
+from gpu_util import Runner
+from test_gpu_nl4d import check, clip
+
+pytestmark = pytest.mark.gpu
+
+
+def auto_noise(oracle, frames, fmt, d, *, blksize=16, overlap=8, search_radius=4, levels=2, sigma_scale=1.0):
+    """The per-pass (sigma, weight scale, SAD floor) of the measured front, by centre frame."""
+    f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), 0.0) for p in frames]
+    h, w, c = f32[0].shape
+    readings, totals = oracle.noise_readings_mc(f32, c, w, h, blksize=blksize, overlap=overlap,
+                                                search_radius=search_radius, levels=levels)
+    f = np.float32
+    area, unit = f(81.0), f(1.2) * f(1.0) * f(255.0)
+    settings = oracle.fold_words(w, h, sigma_scale=sigma_scale, g_max=float(oracle.dct_noise_profile(0.0).max()),
+                                 h2_per_inverse_variance=float(f(65025.0) / (f(3.0) * unit * unit * area)),
+                                 h2_fixed=float(f(65025.0) / (f(3.0) * f(1.2) * f(1.2) * area)),
+                                 offset_per_variance=float(f(2.0) * f(3.0) * f(1.0) * area),
+                                 sad_per_sigma=oracle.sad_noise_floor(blksize, 1.0))
+    folds = oracle.fold_stream(readings, totals, settings, c, 0, d)
+    derived = [fd[1] for fd in folds]
+    return (lambda frame: (float(derived[frame][0]), float(derived[frame][2]), float(derived[frame][4]))), derived
+
+
+@pytest.mark.parametrize("w,h,n,d,estimation,context", [
+    (96, 64, 12, 2, avd.MotionEstimation.DIRECT, 0),
+    (96, 64, 14, 3, avd.MotionEstimation.AUTO, 0),    # Chained at d >= 3
+    (80, 48, 5, 2, avd.MotionEstimation.DIRECT, 0),   # shorter than the look-ahead
+    (72, 56, 11, 1, avd.MotionEstimation.DIRECT, 2),  # continuation
+    (88, 40, 20, 2, avd.MotionEstimation.CHAINED, 0),  # the history wraps
+])
+def test_nl4d_auto_sigma_matches_oracle(oracle, w, h, n, d, estimation, context):
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, n, seed=w + n + d, sigma=9.0)
+    o = avd.Nl4dOptions(sigma=None, noise_map=False, temporal_radius=d, spatial_radius=4,
+                        motion=avd.MotionSearch(estimation=estimation))
+    spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    assert spec.max_held_frames() == 2 * d + 8
+    got = Runner(spec).run(frames, context=context)
+    noise, derived = auto_noise(oracle, [[f[0]] for f in frames], fmt, d)
+    chained = estimation == avd.MotionEstimation.CHAINED or (estimation == avd.MotionEstimation.AUTO and d >= 3)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 0.0, context=context, spatial_radius=4,
+          chained=chained, noise=noise)
+    # Along the motion the estimate finds the synthetic 9-code noise.
+    sig = derived[n // 2][0] * 255
+    assert 6.5 < sig < 11.0, sig
+
+
+def test_nl4d_auto_10bit_sigma_scale(oracle):
+    w, h, n, d = 96, 64, 10, 1
+    fmt = avd.SampleFormat.u16(10)
+    frames = clip(w, h, n, depth=10, seed=77, sigma=12.0)
+    o = avd.Nl4dOptions(sigma=None, noise_map=False, sigma_scale=1.2, temporal_radius=d, spatial_radius=3,
+                        pooled_threshold=False, lambda_ht=2.7)
+    spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    noise, _ = auto_noise(oracle, [[f[0]] for f in frames], fmt, d, sigma_scale=1.2)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 0.0, spatial_radius=3, noise=noise,
+          pooled_threshold=False, lambda_ht=2.7)
