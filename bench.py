@@ -602,14 +602,19 @@ def run_nl4d(pushes: int, size: str) -> None:
                       "push_ms": [round(t, 3) for t in times]}))
 
 
-def run_nl4d_4k(pushes: int) -> None:
-    """NL4D on the 4K workload: 3840x2160 4:2:0 10-bit, luma and chroma in one engine, 7-frame window
-    (d=3, Auto estimation resolves to Chained), spatial radius 16, hard threshold 2.7 (lambda_ht 2.7,
-    scale 1, pooled threshold and noise map off), motion at its defaults. Synthetic frames: the
-    gratings/rectangles/texture base in 10-bit codes, 12 sprites at integer velocities up to 8
-    px/frame, Gaussian noise of 20 codes plus signal-dependent variance 0.02 * value; sigma pinned
-    at 20 codes (the automatic estimate is not built). Eight generated frames are cycled. Prints
-    the device time of every push and the steady-state median as one JSON line."""
+def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
+    """NL4D on the 4K workload: 3840x2160 4:2:0 10-bit, 7-frame window (d=3, Auto estimation resolves
+    to Chained), spatial radius 16, hard threshold 2.7 (lambda_ht 2.7, scale 1, pooled threshold and
+    noise map off), motion at its defaults. Synthetic frames: the gratings/rectangles/texture base in
+    10-bit codes, 12 sprites at integer velocities up to 8 px/frame, Gaussian noise of 20 codes plus
+    signal-dependent variance 0.02 * value. Eight generated frames are cycled.
+
+    Default: luma and chroma in one engine with sigma pinned at 20 codes. With `auto`, luma takes its
+    sigma from the automatic noise estimate (motion-compensated look-ahead, noise map off) and chroma
+    keeps the pinned sigma (its colour gains are not built); the two plane groups' window spans then
+    differ, which one engine rejects, so a luma engine and a chroma engine run side by side, as a
+    caller of the reference must. Prints the device time of every push and the steady-state median
+    as one JSON line."""
     import numpy as np
     import torch
 
@@ -621,12 +626,20 @@ def run_nl4d_4k(pushes: int) -> None:
     w, h, depth, d = 3840, 2160, 10, 3
     fmt = avd.SampleFormat.u16(depth)
     sigma = 20.0 / 1023.0
-    o = avd.Nl4dOptions(sigma=sigma, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
-                        pooled_threshold=False, noise_map=False)
+
+    def options(sig):
+        return avd.Nl4dOptions(sigma=sig, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
+                               pooled_threshold=False, noise_map=False)
+
     geo = avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt)
-    eng = avd.build_engine(avd.EngineSpec.nl4d(o, o, geo))
+    if auto:
+        engines = [avd.build_engine(avd.EngineSpec.nl4d(options(None), None, geo)),
+                   avd.build_engine(avd.EngineSpec.nl4d(None, options(sigma), geo))]
+    else:
+        engines = [avd.build_engine(avd.EngineSpec.nl4d(options(sigma), options(sigma), geo))]
     stream = torch.cuda.current_stream()
-    eng.set_stream(stream.cuda_stream)
+    for eng in engines:
+        eng.set_stream(stream.cuda_stream)
     clip = synth.make_clip(w, h, 8, depth=depth, chroma="420", sigma_luma=20.0 / 4.0, sigma_chroma=20.0 / 4.0,
                            sprites=12, sprite_speed=8, signal_dependent=0.02, seed=2000)
     dims = [geo.plane_dims(i) for i in range(3)]
@@ -646,17 +659,22 @@ def run_nl4d_4k(pushes: int) -> None:
     for i in range(pushes):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        ready = eng.push(dp(bufs[i % len(bufs)]))
-        for _ in range(ready):
-            eng.emit_into(dp(outs))
+        for eng in engines:
+            ready = eng.push(dp(bufs[i % len(bufs)]))
+            for _ in range(ready):
+                eng.emit_into(dp(outs))
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
-    eng.close()
-    steady = times[2 * d + 1:]
+    for eng in engines:
+        eng.close()
+    warm = 2 * d + 1 + (8 if auto else 0)
+    steady = times[warm:]
     ms = float(np.median(steady))
+    what = ("luma sigma from the automatic noise estimate, chroma sigma pinned at 20 codes (two engines)" if auto
+            else "sigma pinned at 20 codes")
     print(json.dumps({"workload": "NL4D 3840x2160 4:2:0 10-bit luma+chroma, d=3 (Chained), spatial_radius 16, "
-                                  "lambda_ht 2.7, plain threshold, sigma pinned at 20 codes",
+                                  "lambda_ht 2.7, plain threshold, " + what,
                       "ms_per_frame": round(ms, 3), "frames_per_s": round(1000.0 / ms, 2),
                       "push_ms": [round(t, 2) for t in times]}))
 
@@ -837,6 +855,8 @@ def main() -> None:
     ap.add_argument("--nl4d-size", default="1080", choices=["1080", "2160"])
     ap.add_argument("--nl4d-4k", type=int, default=0, metavar="PUSHES",
                     help="time PUSHES pushes of the 4K 4:2:0 10-bit NL4D workload (d=3) and exit")
+    ap.add_argument("--auto-sigma", action="store_true",
+                    help="with --nl4d-4k: luma sigma from the automatic noise estimate")
     ap.add_argument("--adjoint", type=int, default=0, metavar="REPS",
                     help="time the NLMeans adjoint against its forward REPS times and exit")
     ap.add_argument("--batch", type=int, default=0, metavar="REPS",
@@ -855,7 +875,7 @@ def main() -> None:
     elif args.nl4d:
         run_nl4d(args.nl4d, args.nl4d_size)
     elif args.nl4d_4k:
-        run_nl4d_4k(args.nl4d_4k)
+        run_nl4d_4k(args.nl4d_4k, auto=args.auto_sigma)
     elif args.adjoint:
         run_adjoint(args.adjoint)
     elif args.batch:
