@@ -284,6 +284,7 @@ class NlmPass final : public Pass {
             bool released = false;
             if (auto f = release_held_frame(&released)) return f;
         }
+        if (auto f = noise_.before_ingest(stream)) return f;
         if (auto f = ingest_into(planes, noise_.slot(noise_.pushed()))) return f;
         return noise_.read_pushed(stream);
     }

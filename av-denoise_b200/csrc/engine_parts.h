@@ -130,17 +130,25 @@ struct NoiseFrontConfig {
 class NoiseFront {
    public:
     static constexpr size_t kFrames = 8;  // nlmeans/denoiser/lookahead.rs:30
+    NoiseFront() = default;
+    NoiseFront(const NoiseFront&) = delete;
+    NoiseFront& operator=(const NoiseFront&) = delete;
+    ~NoiseFront();
     std::optional<Failure> allocate(const NoiseFrontConfig& cfg);
+    // Orders a write into a look-ahead slot on `main` after the reads queued on the side stream.
+    std::optional<Failure> before_ingest(cudaStream_t main);
     // The look-ahead slot of stream frame `frame`.
     float* slot(size_t frame) const;
     size_t held() const { return pushed_ - released_; }
     size_t pushed() const { return pushed_; }
-    // Reads stream frame pushed(), which the caller has just ingested into slot(pushed()).
-    std::optional<Failure> read_pushed(cudaStream_t s);
+    // Reads stream frame pushed(), which the caller has just ingested into slot(pushed()) on `main`.
+    // The reads run on the front's own high-priority stream, overlapping the pass's work on `main`.
+    std::optional<Failure> read_pushed(cudaStream_t main);
     // The oldest held stream frame, now released, or none when nothing is held.
     std::optional<size_t> take_oldest();
-    // Folds the window around stream frame `centre` into the derived words and tables.
-    std::optional<Failure> fold(uint32_t centre, cudaStream_t s);
+    // Folds the window around stream frame `centre` into the derived words and tables, on `main`
+    // after the reads.
+    std::optional<Failure> fold(uint32_t centre, cudaStream_t main);
     float* derived() const { return derived_.as<float>(); }
     float* spatial_table() const { return spatial_.as<float>(); }
     void reset();
@@ -149,6 +157,9 @@ class NoiseFront {
     std::optional<Failure> search(size_t centre_frame, size_t neighbour_frame, int direction, cudaStream_t s);
     std::optional<Failure> read_against(size_t frame, std::optional<size_t> prev, int direction, cudaStream_t s);
     NoiseFrontConfig cfg_;
+    cudaStream_t side_ = nullptr;
+    cudaEvent_t ingested_ = nullptr, read_done_ = nullptr;
+    bool reads_queued_ = false;
     size_t capacity_ = 0, pushed_ = 0, released_ = 0, recorded_ = 0;
     int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2;
     DeviceBuffer lookahead_, partials_, records_, scratch_, history_records_, history_results_, settings_, state_,

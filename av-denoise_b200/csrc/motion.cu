@@ -382,6 +382,46 @@ __global__ void __launch_bounds__(Blocked<BLK, R>::kWarps * 32) blocked_kernel(S
     }
 }
 
+// The fine pass at radius 0 (the HQ confidence pass scores every block where it stands): one thread
+// per (block, neighbour). The single candidate's SAD is the same sequential row-major sum the
+// windowed kernels take, so vectors, SADs and confidences are theirs bit for bit; a SAD that is not
+// below the 1e30 start leaves the search's 1e30 (block_match.rs:735-742).
+__global__ void __launch_bounds__(128) zero_radius_fine_kernel(SearchArgs a) {
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y, n = blockIdx.z;
+    if (bx >= a.L.blocks_x) return;
+    int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
+    const int cdx = a.use_seed ? mv[0] : 0;
+    const int cdy = a.use_seed ? mv[1] : 0;
+    const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
+    const uint32_t nbr_slot = a.neighbour_slots ? a.neighbour_slots[n] : a.slots[n];
+    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(nbr_slot) * a.L.slot_pixels;
+    const int ox = bx * a.L.step, oy = by * a.L.step, b = a.L.blksize;
+    float sad = 0.0f;
+    for (int iy = 0; iy < b; ++iy) {
+        const int64_t crow = centre_base + static_cast<int64_t>(clamp_to(oy + iy, a.L.height)) * a.L.width;
+        const int64_t wrow = nbr_base + static_cast<int64_t>(clamp_to(oy + cdy + iy, a.L.height)) * a.L.width;
+#pragma unroll 8
+        for (int ix = 0; ix < b; ++ix) {
+            const float c = __ldg(a.L.pyramid + crow + clamp_to(ox + ix, a.L.width));
+            const float w = __ldg(a.L.pyramid + wrow + clamp_to(ox + cdx + ix, a.L.width));
+            sad = __fadd_rn(sad, fabsf(__fsub_rn(c, w)));
+        }
+    }
+    if (!(sad <= kNoSad)) sad = kNoSad;
+    mv[0] = cdx;
+    mv[1] = cdy;
+    if (a.confidence) {
+        const float floor = a.noise[a.sad_floor_word];
+        float excess = __fsub_rn(sad, floor);
+        if (excess < 0.0f) excess = 0.0f;
+        const float t2 = __fmul_rn(a.thsad, a.thsad);
+        const float e2 = __fmul_rn(excess, excess);
+        float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
+        if (c < 0.0f) c = 0.0f;
+        a.confidence[static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx] = c;
+    }
+}
+
 template <int BLK, int R>
 cudaError_t launch_blocked(bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
     using B = Blocked<BLK, R>;
@@ -402,6 +442,10 @@ cudaError_t launch_search(bool coarse, const SearchArgs& a, dim3 grid, cudaStrea
             case 32: return launch_blocked<32, R>(coarse, a, grid, s);
             default: break;
         }
+    }
+    if (R == 0 && !coarse) {
+        zero_radius_fine_kernel<<<dim3((grid.x + 127) / 128, grid.y, grid.z), 128, 0, s>>>(a);
+        return cudaGetLastError();
     }
     constexpr int kCand = (2 * R + 1) * (2 * R + 1);
     const int threads = ((kCand + 31) / 32) * 32;

@@ -7,7 +7,9 @@
 // the front follows motion) and its reading, recorded in history slot frame % (17 + d). The frame
 // enters the pass's ring 8 pushes later, so every window a pass folds is recorded by then. Before
 // each pass the window around the pass's centre frame is folded into the derived words and, for
-// NLMeans, the offset tables. Every launch is queued on the pass's stream.
+// NLMeans, the offset tables. The reads run on the front's own high-priority stream, ordered after
+// the ingest by an event, so they overlap the pass's work; the fold and the next ingest into a
+// look-ahead slot wait for them on the pass's stream.
 
 #include <cuda_runtime.h>
 
@@ -26,6 +28,13 @@ constexpr int kOlderToNewer = 0, kNewerToOlder = 1;  // lookahead.rs:43-46
 
 int64_t pad8(int64_t n) { return (n + 7) / 8 * 8; }
 }  // namespace
+
+NoiseFront::~NoiseFront() {
+    if (side_) cudaStreamSynchronize(side_);
+    if (ingested_) cudaEventDestroy(ingested_);
+    if (read_done_) cudaEventDestroy(read_done_);
+    if (side_) cudaStreamDestroy(side_);
+}
 
 std::optional<Failure> NoiseFront::allocate(const NoiseFrontConfig& cfg) {
     cfg_ = cfg;
@@ -55,6 +64,15 @@ std::optional<Failure> NoiseFront::allocate(const NoiseFrontConfig& cfg) {
     if ((e = pilot_.alloc(side * side * sizeof(float))) != cudaSuccess) return fail("pilot table", e);
     for (DeviceBuffer* b : {&history_records_, &history_results_, &state_, &derived_, &spatial_, &pilot_})
         if ((e = cudaMemset(b->ptr, 0, b->bytes)) != cudaSuccess) return fail("noise state clear", e);
+    // The reads of each pushed frame run on a stream of their own, at the highest priority so their
+    // small grids start between the pass's tiles.
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if ((e = cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, greatest)) != cudaSuccess)
+        return fail("noise stream", e);
+    if ((e = cudaEventCreateWithFlags(&ingested_, cudaEventDisableTiming)) != cudaSuccess) return fail("noise event", e);
+    if ((e = cudaEventCreateWithFlags(&read_done_, cudaEventDisableTiming)) != cudaSuccess)
+        return fail("noise event", e);
     float words[16];
     noise_fold_words(cfg.width, cfg.height, cfg.coefficients, words);
     if ((e = cudaMemcpy(settings_.ptr, words, sizeof(words), cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -137,10 +155,21 @@ std::optional<Failure> NoiseFront::read_against(size_t frame, std::optional<size
     return std::nullopt;
 }
 
+std::optional<Failure> NoiseFront::before_ingest(cudaStream_t main) {
+    if (!reads_queued_) return std::nullopt;
+    cudaError_t e = cudaStreamWaitEvent(main, read_done_, 0);
+    if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise read wait", e)};
+    return std::nullopt;
+}
+
 // lookahead.rs:182-216 and 283-458: the new frame's pyramid and pair search (with motion), then its
 // noise read against the frame before it, and, at the stream's second frame, the first frame read
 // again along the motion to it.
-std::optional<Failure> NoiseFront::read_pushed(cudaStream_t s) {
+std::optional<Failure> NoiseFront::read_pushed(cudaStream_t main) {
+    cudaError_t ev = cudaEventRecord(ingested_, main);
+    if (ev == cudaSuccess) ev = cudaStreamWaitEvent(side_, ingested_, 0);
+    if (ev != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise read order", ev)};
+    const cudaStream_t s = side_;
     const size_t frame = pushed_;
     const int w = static_cast<int>(cfg_.width), h = static_cast<int>(cfg_.height);
     const int c = static_cast<int>(cfg_.channels);
@@ -164,6 +193,8 @@ std::optional<Failure> NoiseFront::read_pushed(cudaStream_t s) {
     if (auto f = read_against(frame, prev, kNewerToOlder, s)) return f;
     if (cfg_.motion && frame == 1)
         if (auto f = read_against(0, std::optional<size_t>(1), kOlderToNewer, s)) return f;
+    if ((e = cudaEventRecord(read_done_, s)) != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise read", e)};
+    reads_queued_ = true;
     pushed_ += 1;
     recorded_ = std::max(recorded_, frame + 1);
     return std::nullopt;
@@ -171,6 +202,7 @@ std::optional<Failure> NoiseFront::read_pushed(cudaStream_t s) {
 
 // nlmeans/denoiser/noise.rs:171-185 (`update_noise_estimate`).
 std::optional<Failure> NoiseFront::fold(uint32_t centre, cudaStream_t s) {
+    if (auto f = before_ingest(s)) return f;  // every recorded frame's reading has landed
     const int64_t newest = static_cast<int64_t>(recorded_) - 1;
     const int first = static_cast<int>(std::max<int64_t>(static_cast<int64_t>(centre) - kNoiseWindowRadius, 0));
     const int last = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(centre) + kNoiseWindowRadius, newest));

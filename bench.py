@@ -554,6 +554,51 @@ def run_host(frames: int) -> None:
     print(json.dumps(line))
 
 
+def run_hq_auto(pushes: int) -> None:
+    """NLMeans-HQ with the automatic noise estimate: 1920x1080 u8 luma, d=2, a=5, s=2, default HQ
+    strength and temporal confidence, on the 1080p temporal clip. Each push reads one frame's noise
+    in the look-ahead (Immerkaer, temporal records, reading) and, once the look-ahead and the ring
+    are full, folds the window and denoises one frame. Prints the device time of every push (CUDA
+    events) and the steady-state median as one JSON line."""
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import synth
+
+    clip = synth.temporal_1080p_clip(frames=8, seed=21)
+    fmt = avd.SampleFormat.u8()
+    t = avd.NlmTuning(search_radius=LUMA["a"], patch_radius=LUMA["s"])
+    hq = avd.HqParams(sigma_override=None)
+    alg = avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(
+        nlm=avd.NlmeansOptions(tuning=t, mode=avd.DenoisingMode.temporal(LUMA["d"])), hq=hq))
+    eng = avd.build_engine(avd.EngineSpec.nlmeans(alg, None, avd.Geometry(W, H, avd.ChromaLayout.GRAY, fmt, fmt)))
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    bufs = []
+    for f in clip:
+        flat = f[0].reshape(-1)
+        bufs.append(torch.from_numpy(np.concatenate([flat, np.zeros((-flat.size) % 4, np.uint8)]).view(np.int32)).cuda())
+    out = torch.zeros_like(bufs[0])
+    times = []
+    for i in range(pushes):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if eng.push([avd.DevicePlane.from_tensor(bufs[i % len(bufs)], W, H)]):
+            eng.emit_into([avd.DevicePlane.from_tensor(out, W, H)])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    eng.close()
+    steady = times[8 + 2 * LUMA["d"] + 1:]
+    ms = float(np.median(steady)) if steady else float("nan")
+    print(json.dumps({"workload": "NLMeans-HQ automatic sigma, 1920x1080 u8 luma, d=2 a=5 s=2, temporal confidence",
+                      "ms_per_frame": round(ms, 4), "frames_per_s": round(1000.0 / ms, 2),
+                      "push_ms": [round(x, 3) for x in times]}))
+
+
 def run_nl4d(pushes: int, size: str) -> None:
     """The NL4D engine on one plane of synthetic content with a pinned sigma and Direct motion:
     1920x1080 u8 or 3840x2160 10-bit luma, d=2, spatial radius 9, defaults otherwise. Prints the
@@ -863,6 +908,8 @@ def main() -> None:
                     help="time the batched launch against the per-frame loop REPS times and exit")
     ap.add_argument("--host", type=int, default=0, metavar="FRAMES",
                     help="time FRAMES frames through the host denoiser against the resident engine and exit")
+    ap.add_argument("--hq-auto", type=int, default=0, metavar="PUSHES",
+                    help="time PUSHES pushes of NLMeans-HQ with the automatic noise estimate and exit")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -882,6 +929,8 @@ def main() -> None:
         run_batch(args.batch)
     elif args.host:
         run_host(args.host)
+    elif args.hq_auto:
+        run_hq_auto(args.hq_auto)
     elif args.impl == "reference":
         run_reference(args)
     else:
