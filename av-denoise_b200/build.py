@@ -47,7 +47,7 @@ def _sources() -> list[Path]:
 
 
 def _headers() -> list[Path]:
-    return sorted(list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h")))
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h")))
 
 
 def _needs(obj: Path, src: Path, headers: list[Path]) -> bool:
