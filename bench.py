@@ -98,6 +98,25 @@ def build_specs(avd):
     return avd.EngineSpec.nlmeans(alg(LUMA), None, geo), avd.EngineSpec.nlmeans(None, alg(CHROMA), geo)
 
 
+def replica_seed(rank: int) -> int:
+    """Each rank denoises its own clip (independent units, no data-path collective)."""
+    return 1000 + rank
+
+
+def replica_throughput(local_times: list[float], frames_per_rank: int, world: int, device: str = "cuda"):
+    """Whole-job throughput of N replicas: every rank's timings are reduced to the max over ranks
+    (the one collective, on timings only), and value = frames of all ranks / that time. Returns
+    (max-over-ranks times, values)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(local_times, device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    times = [float(x) for x in t]
+    return times, [frames_per_rank * world / x for x in times]
+
+
 def plane_words(fmt, w, h):
     return fmt.plane_bytes(w * h) // 4
 
@@ -123,7 +142,7 @@ def run_gpu(args) -> None:
         if world > 1:
             dist.barrier()
 
-    clip = synth.temporal_1080p_clip(frames=FRAMES, seed=1000 + rank)
+    clip = synth.temporal_1080p_clip(frames=FRAMES, seed=replica_seed(rank))
     spec_l, spec_c = build_specs(avd)
     fmt = spec_l.geometry.input
     dims = [spec_l.geometry.plane_dims(i) for i in range(3)]
@@ -286,15 +305,8 @@ def run_gpu(args) -> None:
     torch.cuda.synchronize()
     same = all(torch.equal(host_out[FRAMES - 1][i], out[i].cpu()) for i in range(3))
 
-    t_step = sum(times) / len(times)
-    t_e2e = sum(e2e_times) / len(e2e_times)
-    if world > 1:
-        t = torch.tensor([t_step, t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_step, t_e2e = float(t[0]), float(t[1])
-
-    fps = FRAMES * world / t_step
-    fps_e2e = FRAMES * world / t_e2e
+    (t_step, t_e2e), (fps, fps_e2e) = replica_throughput(
+        [sum(times) / len(times), sum(e2e_times) / len(e2e_times)], FRAMES, world)
     peaks = read_peaks()
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     luma_px = W * H
