@@ -228,6 +228,10 @@ def hq_default_strength(channels: int, temporal_radius: int) -> float:
     return float(_abi.load().avd_hq_default_strength(channels, temporal_radius))
 
 
+# nlmeans/prefilter/mod.rs:28-32: the pilot strength as a multiplier on the main pass strength.
+DEFAULT_PILOT_STRENGTH_SCALE = 0.4
+
+
 @dataclass
 class PrefilterMode:
     """nlmeans/prefilter/mod.rs:15-26: kind 0 None, 1 Bilateral, 2 NlmSpatial."""
@@ -246,11 +250,53 @@ class PrefilterMode:
         return PrefilterMode(1, sigma_s, sigma_r, 0.0)
 
     @staticmethod
-    def nlm_spatial(strength_scale: float = 0.4) -> "PrefilterMode":
+    def nlm_spatial(strength_scale: float = DEFAULT_PILOT_STRENGTH_SCALE) -> "PrefilterMode":
         return PrefilterMode(2, 0.0, 0.0, strength_scale)
+
+    def needs_reference_buf(self) -> bool:
+        """nlmeans/prefilter/mod.rs:36-39: every prefilter keeps a reference ring."""
+        return self.kind != 0
+
+    def is_gpu_internal(self) -> bool:
+        """nlmeans/prefilter/mod.rs:41-44: both prefilters build their reference on the GPU."""
+        return self.kind in (1, 2)
 
     def _c(self) -> _abi.AvdPrefilter:
         return _abi.AvdPrefilter(self.kind, self.sigma_s, self.sigma_r, self.strength_scale)
+
+
+def bilateral_radius(sigma_s: float) -> int:
+    """nlmeans/prefilter/bilateral.rs:7-13: max(ceil(2 sigma_s), 1), evaluated in f32."""
+    import numpy as np
+
+    return max(int(np.ceil(np.float32(2.0) * np.float32(sigma_s))), 1)
+
+
+def parse_prefilter(value: str) -> PrefilterMode:
+    """nlmeans/prefilter/mod.rs:46-94 (`parse_prefilter`): "none" or "" -> None, "nlm" or
+    "nlm:<strength_scale>" -> NlmSpatial, "bilateral:<sigma_s>,<sigma_r>" -> Bilateral. Raises
+    ValueError on anything else, naming the form it expected."""
+    if value in ("none", ""):
+        return PrefilterMode.none()
+    if value == "nlm":
+        return PrefilterMode.nlm_spatial(DEFAULT_PILOT_STRENGTH_SCALE)
+    if value.startswith("nlm:"):
+        try:
+            scale = float(value[4:].strip())
+        except ValueError:
+            raise ValueError("--prefilter nlm expects a number: nlm:<strength_scale>") from None
+        return PrefilterMode.nlm_spatial(scale)
+    if value.startswith("bilateral:"):
+        parts = value[len("bilateral:"):].split(",")
+        if len(parts) != 2:
+            raise ValueError("--prefilter bilateral expects two values: bilateral:<sigma_s>,<sigma_r>")
+        try:
+            sigma_s, sigma_r = float(parts[0].strip()), float(parts[1].strip())
+        except ValueError:
+            raise ValueError("--prefilter bilateral expects two numbers: bilateral:<sigma_s>,<sigma_r>") from None
+        return PrefilterMode.bilateral(sigma_s, sigma_r)
+    raise ValueError(
+        f"unknown prefilter '{value}', expected `none`, `nlm[:<strength_scale>]`, or `bilateral:<sigma_s>,<sigma_r>`")
 
 
 class MotionEstimation(enum.IntEnum):

@@ -70,6 +70,11 @@ float h2_inv_norm_with(const NlmParams& p, bool has_sigma, float sigma);
 // `NlmParams::noise_offset_with` for equal sigmas on every active channel (params.rs:245-268).
 float noise_offset_with(const NlmParams& p, const float* sigmas, int n);
 
+// The bilateral prefilter's kernel radius, max(ceil(2 sigma_s), 1), and its Gaussian factor
+// 1 / (2 sigma^2) (nlmeans/prefilter/bilateral.rs:11-22).
+uint32_t bilateral_radius(float sigma_s);
+float inv_two_sigma_sq(float sigma);
+
 // The frames a pass holds before it emits one (nlmeans/engine.rs:24-26, 187-192;
 // nl4d/engine.rs:217-222).
 size_t nlm_held_frames(const AvdNlmeansAlgorithm& algorithm, Channels channels);

@@ -42,8 +42,6 @@ class NlmPass final : public Pass {
         const NlmParams& p = pass->params_;
         // nlmeans/denoiser/noise.rs:50-52 (`measures_noise`): HQ without a pinned sigma measures it.
         pass->measures_ = p.hq && !p.hq_params.has_sigma_override;
-        if (p.prefilter.kind != AVD_PREFILTER_NONE)
-            return Failure{AVD_ERR_INVALID_OPTIONS, "prefilters are not available in this build"};
         if (p.motion.active && p.temporal_radius > 0)
             return Failure{AVD_ERR_INVALID_OPTIONS, "NLMeans motion compensation is not available in this build"};
         // nlmeans/denoiser/mod.rs:340-370: confidence without motion compensation scores every
@@ -153,6 +151,9 @@ class NlmPass final : public Pass {
         const size_t fe = frame_elems();
         cudaError_t e;
         if ((e = ring_.alloc(fe * total_frames() * sizeof(float))) != cudaSuccess) return gpu_failure("ring", e);
+        // nlmeans/denoiser/mod.rs:225 (`needs_reference_buf`): every prefilter keeps a reference ring.
+        if (has_reference() && (e = ref_.alloc(fe * total_frames() * sizeof(float))) != cudaSuccess)
+            return gpu_failure("reference ring", e);
         for (auto& o : outputs_)
             if ((e = o.alloc(fe * sizeof(float))) != cudaSuccess) return gpu_failure("output slot", e);
         if ((e = derived_.alloc(16 * sizeof(float))) != cudaSuccess) return gpu_failure("derived words", e);
@@ -163,7 +164,14 @@ class NlmPass final : public Pass {
         const float sigma = params_.hq_params.sigma_override;
         words[0] = h2_inv_norm_with(params_, has_sigma, sigma);
         float sig[2] = {sigma, sigma};
-        words[1] = has_sigma ? noise_offset_with(params_, sig, 2) : 0.0f;
+        const float input_offset = has_sigma ? noise_offset_with(params_, sig, 2) : 0.0f;
+        // noise.rs:343-390: under the NLM pilot the main pass compares pilot outputs, which carry
+        // no noise floor, and the pilot (word 3) runs at h2 / strength_scale^2 (dispatch/mod.rs:40-43).
+        words[1] = runs_pilot() ? 0.0f : input_offset;
+        if (runs_pilot()) {
+            const float sc = params_.prefilter.strength_scale;
+            words[3] = words[0] / (sc * sc);
+        }
         if (conf_pass_) {
             // motion/confidence.rs:17-30; nlmeans/denoiser/noise.rs:365-368: the confidence floor
             // uses the pinned sigma unscaled by any prefilter.
@@ -184,14 +192,22 @@ class NlmPass final : public Pass {
             return gpu_failure("derived upload", e);
         if (params_.hq) {
             // noise/correlation.rs:71-88 (`build_spatial_offset_lut`): with no measured grain
-            // correlation (rho = 0) every candidate but the centre takes the flat noise offset.
+            // correlation (rho = 0) every candidate but the centre takes the flat noise offset; the
+            // main pass's table holds its own offset, the pilot's the input's (noise/fold.rs:96-109).
             const uint32_t side = 2 * params_.search_radius + 1;
-            std::vector<float> lut(side * side, words[1]);
-            lut[params_.search_radius * side + params_.search_radius] = 0.0f;
-            if ((e = lut_.alloc(lut.size() * sizeof(float))) != cudaSuccess) return gpu_failure("offset table", e);
-            if ((e = cudaMemcpy(lut_.ptr, lut.data(), lut.size() * sizeof(float), cudaMemcpyHostToDevice)) !=
-                cudaSuccess)
-                return gpu_failure("offset table upload", e);
+            auto upload = [&](DeviceBuffer& dst, float offset, const char* what) -> std::optional<Failure> {
+                std::vector<float> lut(side * side, offset);
+                lut[params_.search_radius * side + params_.search_radius] = 0.0f;
+                cudaError_t err;
+                if ((err = dst.alloc(lut.size() * sizeof(float))) != cudaSuccess) return gpu_failure(what, err);
+                if ((err = cudaMemcpy(dst.ptr, lut.data(), lut.size() * sizeof(float), cudaMemcpyHostToDevice)) !=
+                    cudaSuccess)
+                    return gpu_failure(what, err);
+                return std::nullopt;
+            };
+            if (auto f = upload(lut_, words[1], "offset table")) return f;
+            if (runs_pilot())
+                if (auto f = upload(pilot_lut_, input_offset, "pilot offset table")) return f;
         }
         slot_frames_.assign(total_frames(), 0u);
         if (measures_) return allocate_noise();
@@ -214,6 +230,12 @@ class NlmPass final : public Pass {
         k.h2_fixed = h2_inv_norm_with(params_, false, 0.0f);
         const float unit[1] = {1.0f};
         k.offset_per_variance = noise_offset_with(params_, unit, 1);
+        if (runs_pilot()) {
+            // noise.rs:218-224: the pilot's strength factor at h2 = 1; the main pass takes no offset.
+            const float sc = params_.prefilter.strength_scale;
+            k.pilot_h2_factor = 1.0f / (sc * sc);
+            k.main_offset = false;
+        }
         k.confidence_sad_per_sigma = conf_pass_ ? avd_sad_noise_floor(kConfBlk, 1.0f) : 0.0f;
         return noise_.allocate(cfg);
     }
@@ -269,7 +291,12 @@ class NlmPass final : public Pass {
     }
 
     // nlmeans/denoiser/stages.rs:15-26: the per-frame stages of a frame entering ring slot `slot`.
+    // noise.rs:147-165: with the pilot, the stream's first frame folds the window around frame 0
+    // first, since the pilot reads the derived words and no pass has folded any yet.
     std::optional<Failure> enter_ring(size_t slot) {
+        if (runs_pilot() && measures_ && frames_loaded_ == 0)
+            if (auto f = noise_.fold(0, stream)) return f;
+        if (auto f = run_prefilter(slot)) return f;
         if (auto f = slot_written(slot)) return f;
         slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
         advance_ring();
@@ -321,7 +348,8 @@ class NlmPass final : public Pass {
         return std::nullopt;
     }
 
-    // ring.rs:128-146.
+    // ring.rs:128-180: the input slot (and a bilateral reference slot) copied; the pilot rebuilds
+    // the duplicated slot's reference instead.
     std::optional<Failure> duplicate_last_frame() {
         const size_t tf = total_frames();
         const size_t last = (ring_head_ - 1) % tf;
@@ -329,9 +357,61 @@ class NlmPass final : public Pass {
         cudaError_t e = cudaMemcpyAsync(slot_ptr(next), slot_ptr(last), frame_elems() * sizeof(float),
                                         cudaMemcpyDeviceToDevice, stream);
         if (e != cudaSuccess) return gpu_failure("slot copy", e);
+        if (has_reference() && !runs_pilot()) {
+            e = cudaMemcpyAsync(ref_slot_ptr(next), ref_slot_ptr(last), frame_elems() * sizeof(float),
+                                cudaMemcpyDeviceToDevice, stream);
+            if (e != cudaSuccess) return gpu_failure("reference slot copy", e);
+        }
+        if (runs_pilot())
+            if (auto f = run_pilot(next)) return f;
         if (auto f = slot_written(next)) return f;
         slot_frames_[next] = slot_frames_[last];
         ring_head_ += 1;
+        return std::nullopt;
+    }
+
+    // ---- prefilters (nlmeans/prefilter/mod.rs, denoiser/stages.rs:29-59) ----
+    bool has_reference() const { return params_.prefilter.kind != AVD_PREFILTER_NONE; }
+    bool runs_pilot() const { return params_.prefilter.kind == AVD_PREFILTER_NLM_SPATIAL; }
+    float* ref_slot_ptr(size_t slot) const { return ref_.as<float>() + slot * frame_elems(); }
+
+    // stages.rs:29-59: the reference of a frame just written to ring slot `slot`.
+    std::optional<Failure> run_prefilter(size_t slot) {
+        if (runs_pilot()) return run_pilot(slot);
+        if (params_.prefilter.kind != AVD_PREFILTER_BILATERAL) return std::nullopt;
+        // prefilter/bilateral.rs:11-22, 24-61.
+        const float ss = params_.prefilter.sigma_s, sr = params_.prefilter.sigma_r;
+        const int radius = static_cast<int>(bilateral_radius(ss));
+        cudaError_t e = launch_bilateral(slot_ptr(slot), ref_slot_ptr(slot), static_cast<int>(width_),
+                                         static_cast<int>(height_), static_cast<int>(params_.channel_count()), radius,
+                                         inv_two_sigma_sq(ss), inv_two_sigma_sq(sr), stream);
+        if (e != cudaSuccess) return gpu_failure("bilateral prefilter launch", e);
+        return std::nullopt;
+    }
+
+    // dispatch/mod.rs:598-620 (`run_nlm_spatial_pilot`): the single-frame windowed pass over the
+    // noisy input of `slot` at the pilot strength with the pilot's offset table, finished into the
+    // slot's reference.
+    std::optional<Failure> run_pilot(size_t slot) {
+        NlmLaunch a{};
+        a.ring = ring_.as<float>();
+        a.width = static_cast<int>(width_);
+        a.height = static_cast<int>(height_);
+        a.channels = static_cast<int>(params_.channel_count());
+        a.frame_elems = static_cast<int64_t>(frame_elems());
+        a.slot_centre = static_cast<int>(slot);
+        a.pairs = 0;
+        a.patch_radius = static_cast<int>(params_.patch_radius);
+        a.search_radius = static_cast<int>(params_.search_radius);
+        a.derived = measures_ ? noise_.derived() : derived_.as<float>();
+        a.h2_word = measures_ ? kDerivedPilotH2 : 3;
+        a.offset_word = measures_ ? kDerivedNoiseOffset : 1;
+        a.spatial_lut = measures_ ? noise_.pilot_table() : (params_.hq ? pilot_lut_.as<float>() : nullptr);
+        a.wref = params_.self_weight;
+        a.fast = params_.hq ? 0 : 1;
+        a.out = ref_slot_ptr(slot);
+        cudaError_t e = launch_nlm(a, stream);
+        if (e != cudaSuccess) return gpu_failure("nlm pilot launch", e);
         return std::nullopt;
     }
 
@@ -439,6 +519,7 @@ class NlmPass final : public Pass {
         a.wref = params_.self_weight;
         a.fast = params_.hq ? 0 : 1;
         a.out = outputs_[slot].as<float>();
+        a.ref_ring = has_reference() ? ref_.as<float>() : nullptr;
         cudaError_t e = launch_nlm(a, stream);
         if (e != cudaSuccess) return gpu_failure("nlm launch", e);
         if (timed) timer_.end(stream, start);
@@ -480,7 +561,8 @@ class NlmPass final : public Pass {
         if (measures_) noise_.reset();
     }
 
-    static constexpr int kDerivedConfidenceSadFloor = 5, kDerivedH2 = 6, kDerivedNoiseOffset = 8;  // derived.rs:9-31
+    static constexpr int kDerivedConfidenceSadFloor = 5, kDerivedH2 = 6, kDerivedPilotH2 = 7,
+                         kDerivedNoiseOffset = 8;  // derived.rs:9-31
     bool measures_ = false;
     NoiseFront noise_;
 
@@ -491,7 +573,8 @@ class NlmPass final : public Pass {
     DeviceBuffer ring_;
     DeviceBuffer outputs_[2];
     DeviceBuffer derived_;
-    DeviceBuffer lut_;
+    DeviceBuffer lut_, pilot_lut_;
+    DeviceBuffer ref_;  // the prefilter's reference ring, slot for slot beside `ring_`
     std::vector<uint32_t> slot_frames_;
     size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;
     int next_output_slot_ = 0;

@@ -151,6 +151,7 @@ class NoiseFront {
     std::optional<Failure> fold(uint32_t centre, cudaStream_t main);
     float* derived() const { return derived_.as<float>(); }
     float* spatial_table() const { return spatial_.as<float>(); }
+    float* pilot_table() const { return pilot_.as<float>(); }
     void reset();
 
    private:

@@ -46,9 +46,19 @@ struct NlmLaunch {
     float wref;
     int fast;  // 1: no noise offsets and no confidence, so one strength weighs every lane
     float* out;  // width*height*channels
+    const float* ref_ring;  // a prefilter's reference ring (same slots as `ring`) the distances
+                            // compare, or null to compare `ring` itself
 };
 
 cudaError_t launch_nlm(const NlmLaunch& args, cudaStream_t stream);
+// The same launch with `args.ref_ring` set (prefilter.cu).
+cudaError_t launch_nlm_ref(const NlmLaunch& args, cudaStream_t stream);
+
+// The bilateral prefilter (nlmeans/kernels/bilateral.rs:16-107) of one frame `in` into `out`
+// (both width*height*channels f32): kernel radius `radius`, with the spatial and range factors
+// 1 / (2 sigma^2) of prefilter/bilateral.rs:20-22.
+cudaError_t launch_bilateral(const float* in, float* out, int width, int height, int channels, int radius,
+                             float inv_two_sigma_s_sq, float inv_two_sigma_r_sq, cudaStream_t stream);
 
 // A batch of NLM launches (device array `jobs`, all with `channels`, `patch_radius` and `fast`) as one
 // persistent launch: `prefix` holds njobs + 1 running tile counts, `counter` one zeroed int.

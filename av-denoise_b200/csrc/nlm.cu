@@ -75,17 +75,6 @@ __global__ void __launch_bounds__(kThreads, C == 1 && FAST ? 5 : 4)
     }
 }
 
-template <int C, int S>
-size_t smem_bytes(int A, int pairs) {
-    using K = Cfg<C, S>;
-    int nrows = K::TY + 2 * S + 2 * A;
-    int ncols = kTX + 2 * S + 2 * A;
-    int nstride = nbr_stride(ncols, C);
-    size_t floats = (size_t)round_up4(K::CROWS * K::CSTRIDE) + (size_t)round_up4((pairs > 0 ? 2 : 1) * nrows * nstride) +
-                    (size_t)2 * K::HS_BUF;
-    return floats * sizeof(float);
-}
-
 template <int C, int S, bool FAST>
 cudaError_t launch_csf(const NlmLaunch& a, cudaStream_t stream) {
     using K = Cfg<C, S>;
@@ -97,7 +86,7 @@ cudaError_t launch_csf(const NlmLaunch& a, cudaStream_t stream) {
     });
     if (attr_err != cudaSuccess) return attr_err;
     dim3 grid((a.width + kTX - 1) / kTX, (a.height + K::TY - 1) / K::TY);
-    size_t smem = smem_bytes<C, S>(a.search_radius, a.pairs);
+    size_t smem = nlm_smem_bytes<C, S>(a.search_radius, a.pairs, false);
     nlm_window_kernel<C, S, FAST><<<grid, kThreads, smem, stream>>>(a);
     return cudaGetLastError();
 }
@@ -122,7 +111,7 @@ cudaError_t batch_csf(const NlmLaunch* jobs, const int* prefix, int njobs, int* 
                                         200 * 1024);
     });
     if (attr_err != cudaSuccess) return attr_err;
-    const size_t smem = smem_bytes<C, S>(max_a, max_pairs);
+    const size_t smem = nlm_smem_bytes<C, S>(max_a, max_pairs, false);
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -170,6 +159,7 @@ cudaError_t launch_nlm(const NlmLaunch& a, cudaStream_t stream) {
     if (a.pairs < 0 || a.pairs > kMaxPairs || a.search_radius < 0 || a.search_radius > 8 || a.patch_radius < 0 ||
         a.patch_radius > 16)
         return cudaErrorInvalidValue;
+    if (a.ref_ring) return launch_nlm_ref(a, stream);
     if (a.channels == 1) return dispatch_s<1, 0>(a, stream);
     if (a.channels == 2) return dispatch_s<2, 0>(a, stream);
     return cudaErrorInvalidValue;

@@ -150,13 +150,29 @@ __device__ __forceinline__ void row_run(const CentreRun<C, S>& c, const float* _
         *reinterpret_cast<float4*>(hs_out + 4 * m) = make_float4(h[2 * m].x, h[2 * m].y, h[2 * m + 1].x, h[2 * m + 1].y);
 }
 
-// Shared-memory layout of one CTA.
+// Shared-memory layout of one CTA. With a reference ring (a prefilter), `ctr` and `nbr` hold the
+// reference frames the distances compare and `val` the input frames whose values are averaged;
+// without one, `val` is unused and the values come from `nbr`.
 struct Smem {
     float* ctr;     // centre frame, s halo, rows of CSTRIDE floats
     float* nbr[2];  // neighbour tiles, s + a halo, rows of `nstride` floats
+    float* val[2];  // input neighbour tiles beside reference `nbr` tiles, same geometry
     float* hs;      // [2 buffers][HR][kTX lane pairs], rows of kHsStride floats
     int nstride, nrows, ncols;
 };
+
+// Dynamic shared memory of one tile CTA for search radius A, `pairs` temporal pair passes and,
+// with `ref`, the input value tiles beside the reference tiles.
+template <int C, int S>
+inline size_t nlm_smem_bytes(int A, int pairs, bool ref) {
+    using K = Cfg<C, S>;
+    const int nrows = K::TY + 2 * S + 2 * A;
+    const int ncols = kTX + 2 * S + 2 * A;
+    const int nstride = nbr_stride(ncols, C);
+    const size_t tiles = (size_t)round_up4((pairs > 0 ? 2 : 1) * nrows * nstride);
+    const size_t floats = (size_t)round_up4(K::CROWS * K::CSTRIDE) + (ref ? 2 : 1) * tiles + (size_t)2 * K::HS_BUF;
+    return floats * sizeof(float);
+}
 
 // Per-thread accumulators: lane pairs, summed at the finish.
 template <int C, int V>
@@ -169,18 +185,22 @@ struct Acc {
 
 // The lanes of one step: neighbour tiles and offsets (the neighbour of pixel p is p + (dx, dy)),
 // and each lane's offset id in the forward's order (fused.rs: for each pair pass k and q, the
-// forward frame then the backward frame; then the single-frame pass's q != 0, row-major).
+// forward frame then the backward frame; then the single-frame pass's q != 0, row-major). With a
+// reference ring, v0 and v1 are the input tiles whose values the lanes average.
 struct Lanes {
     const float* t0;
     const float* t1;
     int dx0, dy0, dx1, dy1;
     int id0, id1;
+    const float* v0;
+    const float* v1;
 };
 
 // One two-lane step: phase 1, barrier, phase 2. FAST: one strength, no offsets, no confidence.
 // TRACK: keep the id of the first offset reaching the max weight (the adjoint's records); lane 0's
 // id is below lane 1's and steps run in id order, so strict comparisons keep the first.
-template <int C, int S, bool FAST, bool CONF, bool TRACK = false>
+// REF: distances on the reference tiles t0/t1, values from the input tiles v0/v1.
+template <int C, int S, bool FAST, bool CONF, bool TRACK = false, bool REF = false>
 __device__ __forceinline__ void step(const Smem& sm, int A, const Lanes& ln, int& buf, const CentreRun<C, S>& crun,
                                      float2 kk, float2 scale2, float2 negoff, const float2* conf,
                                      Acc<C, Cfg<C, S>::V>& acc) {
@@ -213,8 +233,8 @@ __device__ __forceinline__ void step(const Smem& sm, int A, const Lanes& ln, int
     float2 dist = hv[0];
 #pragma unroll
     for (int i = 1; i <= 2 * S; ++i) dist = add2(dist, hv[i]);
-    const float* p0 = ln.t0 + (y0 + S + ln.dy0 + A) * sm.nstride + (col + S + ln.dx0 + A) * C;
-    const float* p1 = ln.t1 + (y0 + S + ln.dy1 + A) * sm.nstride + (col + S + ln.dx1 + A) * C;
+    const float* p0 = (REF ? ln.v0 : ln.t0) + (y0 + S + ln.dy0 + A) * sm.nstride + (col + S + ln.dx0 + A) * C;
+    const float* p1 = (REF ? ln.v1 : ln.t1) + (y0 + S + ln.dy1 + A) * sm.nstride + (col + S + ln.dx1 + A) * C;
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         if (k > 0) dist = sub2(add2(dist, hv[k + 2 * S]), hv[k - 1]);
@@ -281,11 +301,14 @@ struct RecordOut {
 constexpr int kRecordWords = 5;
 
 // One output tile (tile_x, tile_y) of the launch `a`; the whole CTA calls it. REC: the adjoint's
-// records instead of the output (the max weight tracked with its first offset id).
-template <int C, int S, bool FAST, bool REC = false>
+// records instead of the output (the max weight tracked with its first offset id). REF: the
+// distances compare the reference ring `a.ref_ring` (the `_ref` kernels of fused.rs:532-900) while
+// the averaged values and the finish's centre value come from the input ring `a.ring`.
+template <int C, int S, bool FAST, bool REC = false, bool REF = false>
 __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int tile_y, const RecordOut* rec = nullptr) {
     using K = Cfg<C, S>;
     constexpr int V = K::V;
+    static_assert(!(REC && REF), "the adjoint records have no reference-ring form");
 
     const int A = a.search_radius;
     const int W = a.width, H = a.height;
@@ -303,7 +326,10 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
     sm.ctr = smem_raw;
     sm.nbr[0] = sm.ctr + round_up4(K::CROWS * K::CSTRIDE);
     sm.nbr[1] = sm.nbr[0] + sm.nrows * sm.nstride;
-    sm.hs = sm.nbr[0] + round_up4((a.pairs > 0 ? 2 : 1) * sm.nrows * sm.nstride);
+    const int tile_floats = round_up4((a.pairs > 0 ? 2 : 1) * sm.nrows * sm.nstride);
+    sm.val[0] = sm.nbr[0] + tile_floats;
+    sm.val[1] = sm.val[0] + sm.nrows * sm.nstride;
+    sm.hs = sm.nbr[0] + (REF ? 2 : 1) * tile_floats;
 
     const float h2 = __ldg(a.derived + a.h2_word);
     const float off_pair = __ldg(a.derived + a.offset_word);
@@ -313,7 +339,9 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
     const float2 scale2 = f2(scale, scale);
 
     const float* centre = a.ring + a.slot_centre * a.frame_elems;
-    load_tile<C>(sm.ctr, K::CSTRIDE, K::CROWS, K::CW, centre, X0 - S, Y0 - S, W, H);
+    const float* dist_ring = REF ? a.ref_ring : a.ring;
+    const float* dist_centre = dist_ring + a.slot_centre * a.frame_elems;
+    load_tile<C>(sm.ctr, K::CSTRIDE, K::CROWS, K::CW, dist_centre, X0 - S, Y0 - S, W, H);
     __syncthreads();
 
     CentreRun<C, S> crun;
@@ -337,10 +365,16 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
     float2 conf[V];
     for (int p = 0; p < a.pairs; ++p) {
         __syncthreads();  // every thread is done with the previous pass's tiles
-        load_tile<C>(sm.nbr[0], sm.nstride, sm.nrows, sm.ncols, a.ring + a.slot_fwd[p] * a.frame_elems, X0 - S - A,
-                     Y0 - S - A, W, H);
-        load_tile<C>(sm.nbr[1], sm.nstride, sm.nrows, sm.ncols, a.ring + a.slot_bwd[p] * a.frame_elems, X0 - S - A,
-                     Y0 - S - A, W, H);
+        load_tile<C>(sm.nbr[0], sm.nstride, sm.nrows, sm.ncols, dist_ring + a.slot_fwd[p] * a.frame_elems,
+                     X0 - S - A, Y0 - S - A, W, H);
+        load_tile<C>(sm.nbr[1], sm.nstride, sm.nrows, sm.ncols, dist_ring + a.slot_bwd[p] * a.frame_elems,
+                     X0 - S - A, Y0 - S - A, W, H);
+        if (REF) {
+            load_tile<C>(sm.val[0], sm.nstride, sm.nrows, sm.ncols, a.ring + a.slot_fwd[p] * a.frame_elems,
+                         X0 - S - A, Y0 - S - A, W, H);
+            load_tile<C>(sm.val[1], sm.nstride, sm.nrows, sm.ncols, a.ring + a.slot_bwd[p] * a.frame_elems,
+                         X0 - S - A, Y0 - S - A, W, H);
+        }
         const bool use_conf = !FAST && a.conf != nullptr;
 #pragma unroll
         for (int k = 0; k < V; ++k) {
@@ -354,7 +388,7 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
             }
         }
         __syncthreads();
-        Lanes ln{sm.nbr[0], sm.nbr[1], 0, 0, 0, 0, 0, 0};
+        Lanes ln{sm.nbr[0], sm.nbr[1], 0, 0, 0, 0, 0, 0, sm.val[0], sm.val[1]};
         const float2 negoff = f2(-off_pair, -off_pair);
         for (int qy = -A; qy <= A; ++qy) {
             for (int qx = -A; qx <= A; ++qx) {
@@ -365,19 +399,20 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
                 ln.id0 = 2 * ((p * side + qy + A) * side + qx + A);
                 ln.id1 = ln.id0 + 1;
                 if (use_conf)
-                    step<C, S, FAST, true, REC>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
+                    step<C, S, FAST, true, REC, REF>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
                 else
-                    step<C, S, FAST, false, REC>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
+                    step<C, S, FAST, false, REC, REF>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
             }
         }
     }
 
     // The single-frame pass: the window without its centre, two consecutive offsets per step.
     __syncthreads();
-    load_tile<C>(sm.nbr[0], sm.nstride, sm.nrows, sm.ncols, centre, X0 - S - A, Y0 - S - A, W, H);
+    load_tile<C>(sm.nbr[0], sm.nstride, sm.nrows, sm.ncols, dist_centre, X0 - S - A, Y0 - S - A, W, H);
+    if (REF) load_tile<C>(sm.val[0], sm.nstride, sm.nrows, sm.ncols, centre, X0 - S - A, Y0 - S - A, W, H);
     __syncthreads();
     {
-        Lanes ln{sm.nbr[0], sm.nbr[0], 0, 0, 0, 0, 0, 0};
+        Lanes ln{sm.nbr[0], sm.nbr[0], 0, 0, 0, 0, 0, 0, sm.val[0], sm.val[0]};
         const int n = side * side - 1;
         const int mid = A * side + A;
         const int spatial_base = 2 * a.pairs * side * side;
@@ -392,7 +427,7 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
             ln.dy1 = l1 / side - A;
             float2 negoff = f2(0.0f, 0.0f);
             if (!FAST && a.spatial_lut) negoff = f2(-__ldg(a.spatial_lut + l0), -__ldg(a.spatial_lut + l1));
-            step<C, S, FAST, false, REC>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
+            step<C, S, FAST, false, REC, REF>(sm, A, ln, buf, crun, kk, scale2, negoff, conf, acc);
         }
     }
 
@@ -451,7 +486,9 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
         if (gx >= W || gy >= H) continue;
         const float max_w = FAST ? ex2_approx(acc.m[k] * kk.x) : acc.m[k];
         const float wsum = acc.ws[k].x + acc.ws[k].y;
-        const float* orig = sm.ctr + (y0 + k + S) * K::CSTRIDE + (col + S) * C;
+        // The centre value: the input's own (accumulate.rs:175-201 reads the input ring), which the
+        // reference-ring tile does not hold.
+        const float* orig = REF ? centre + ((int64_t)gy * W + gx) * C : sm.ctr + (y0 + k + S) * K::CSTRIDE + (col + S) * C;
         const float self_weight = __fmul_rn(a.wref, max_w);
         const float denom = __fadd_rn(self_weight, wsum);
         float* dst = a.out + ((int64_t)gy * W + gx) * C;

@@ -30,14 +30,6 @@ std::string fmt(const char* f, ...) {
 
 bool finite(float v) { return std::isfinite(v); }
 
-// av-denoise-core/src/nlmeans/prefilter/bilateral.rs:11-22.
-uint32_t bilateral_radius(float sigma_s) {
-    float r = std::ceil(2.0f * sigma_s);
-    uint32_t radius = r > 0.0f ? static_cast<uint32_t>(r) : 0u;
-    return std::max(radius, 1u);
-}
-float inv_two_sigma_sq(float sigma) { return 1.0f / (2.0f * sigma * sigma); }
-
 // av-denoise-core/src/motion/search.rs:229-290 (`MotionCompensationMode::validate`) and
 // :143-156 (`MotionEstimation::validate`).
 std::string validate_motion(const AvdMotionCompensation& m) {
@@ -132,6 +124,14 @@ std::string validate_nl4d(const AvdNl4dOptions& o, Channels c) {
 }
 
 }  // namespace
+
+// av-denoise-core/src/nlmeans/prefilter/bilateral.rs:11-22.
+uint32_t bilateral_radius(float sigma_s) {
+    float r = std::ceil(2.0f * sigma_s);
+    uint32_t radius = r > 0.0f ? static_cast<uint32_t>(r) : 0u;
+    return std::max(radius, 1u);
+}
+float inv_two_sigma_sq(float sigma) { return 1.0f / (2.0f * sigma * sigma); }
 
 float sample_max_value(const AvdSampleFormat& f) {
     switch (f.kind) {

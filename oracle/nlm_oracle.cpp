@@ -87,12 +87,15 @@ struct Conf {
 // (dispatch/mod.rs:665-679): zeroed accumulators, one pair launch per q_k in -d..-1
 // (`nlm_fused_pair_accumulate_window`, fused.rs:138-347), then the single-frame launch
 // (`nlm_fused_single_window`, fused.rs:364-530), then `nlm_finish` (accumulate.rs:152-202).
-// Each launch keeps register sums and adds them to the buffers once at its end.
+// Each launch keeps register sums and adds them to the buffers once at its end. `refs` is the
+// window the distances compare: the window itself, or a prefilter's reference frames (the `_ref`
+// launches, fused.rs:532-900, which average the input's values all the same).
 template <typename T>
-void nlm_pixel(const std::vector<Frame<T>>& window, int d, int px, int py, int a, int s, T h2,
-               T noise_offset, const T* lut, const std::vector<Conf>& conf, T wref, T* out) {
+void nlm_pixel(const std::vector<Frame<T>>& window, const std::vector<Frame<T>>& refs, int d, int px, int py,
+               int a, int s, T h2, T noise_offset, const T* lut, const std::vector<Conf>& conf, T wref, T* out) {
     const int C = window[d].channels;
     const Frame<T>& ctr = window[d];
+    const Frame<T>& rctr = refs[d];
     const T scale = channel_scale<T>(C);
     T accum[2] = {T(0), T(0)};
     T weight_sum = T(0);
@@ -102,13 +105,15 @@ void nlm_pixel(const std::vector<Frame<T>>& window, int d, int px, int py, int a
         // q_k = -d + k: the forward frame is centre + q_k, the backward frame centre - q_k.
         const Frame<T>& fwd = window[k];
         const Frame<T>& bwd = window[2 * d - k];
+        const Frame<T>& rfwd = refs[k];
+        const Frame<T>& rbwd = refs[2 * d - k];
         const Conf* cf = conf.empty() ? nullptr : &conf[k];
         T acc[2] = {T(0), T(0)};
         T ws = T(0), wm = T(0);
         for (int qy = -a; qy <= a; ++qy) {
             for (int qx = -a; qx <= a; ++qx) {
-                T sum_f = patch_distance(ctr, fwd, px, py, qx, qy, s, scale);
-                T sum_b = patch_distance(ctr, bwd, px, py, -qx, -qy, s, scale);
+                T sum_f = patch_distance(rctr, rfwd, px, py, qx, qy, s, scale);
+                T sum_b = patch_distance(rctr, rbwd, px, py, -qx, -qy, s, scale);
                 T w_f = welsch(sum_f, h2, noise_offset);
                 T w_b = welsch(sum_b, h2, noise_offset);
                 if (cf && cf->fwd) {
@@ -141,7 +146,7 @@ void nlm_pixel(const std::vector<Frame<T>>& window, int d, int px, int py, int a
         for (int qy = -a; qy <= a; ++qy) {
             for (int qx = -a; qx <= a; ++qx) {
                 if (qx == 0 && qy == 0) continue;
-                T dist = patch_distance(ctr, ctr, px, py, qx, qy, s, scale);
+                T dist = patch_distance(rctr, rctr, px, py, qx, qy, s, scale);
                 T off = lut ? lut[(qy + a) * side + (qx + a)] : T(0);
                 T w = welsch(dist, h2, off);
                 const T* np = ctr.at_clamped(px + qx, py + qy);
@@ -174,12 +179,14 @@ void nlm_pixel(const std::vector<Frame<T>>& window, int d, int px, int py, int a
 }
 
 template <typename T>
-void nlm_window_frame(const T* const* frames, int width, int height, int channels, int d, int a, int s,
-                      T h2, T noise_offset, const T* lut, const float* const* conf_fwd,
+void nlm_window_frame(const T* const* frames, const T* const* ref_frames, int width, int height, int channels, int d,
+                      int a, int s, T h2, T noise_offset, const T* lut, const float* const* conf_fwd,
                       const float* const* conf_bwd, int conf_step, int blocks_x, int blocks_y, T wref,
                       T* out) {
-    std::vector<Frame<T>> window;
+    std::vector<Frame<T>> window, refs;
     for (int i = 0; i < 2 * d + 1; ++i) window.push_back(Frame<T>{frames[i], width, height, channels});
+    for (int i = 0; i < 2 * d + 1; ++i)
+        refs.push_back(Frame<T>{ref_frames ? ref_frames[i] : frames[i], width, height, channels});
     std::vector<Conf> conf;
     if (conf_fwd) {
         for (int k = 0; k < d; ++k) conf.push_back(Conf{conf_fwd[k], conf_bwd[k], conf_step, blocks_x, blocks_y});
@@ -187,7 +194,7 @@ void nlm_window_frame(const T* const* frames, int width, int height, int channel
 #pragma omp parallel for schedule(dynamic, 4)
     for (int y = 0; y < height; ++y) {
         for (int x = 0; x < width; ++x) {
-            nlm_pixel<T>(window, d, x, y, a, s, h2, noise_offset, lut, conf, wref,
+            nlm_pixel<T>(window, refs, d, x, y, a, s, h2, noise_offset, lut, conf, wref,
                          out + ((size_t)y * width + x) * channels);
         }
     }
@@ -272,37 +279,100 @@ float orc_h2_inv_norm(float strength, int patch_radius) {
 float orc_welsch_weight(float sum, float h2, float off) { return welsch<float>(sum, h2, off); }
 
 // One denoised frame of the windowed NLM path, FP32 mirror. `frames` holds the 2d+1 window
-// frames (normalised f32, interleaved), the centre at index d. `lut` is the (2a+1)^2 spatial
-// offset table (null = zeros). `conf_fwd`/`conf_bwd` (null = off) hold, for pair k (q_k = -d+k),
-// the per-block confidence of the forward and backward neighbour.
+// frames (normalised f32, interleaved), the centre at index d; `refs` (null = `frames`) the
+// window's reference frames the distances compare. `lut` is the (2a+1)^2 spatial offset table
+// (null = zeros). `conf_fwd`/`conf_bwd` (null = off) hold, for pair k (q_k = -d+k), the per-block
+// confidence of the forward and backward neighbour.
+void orc_nlm_frame_ref_f32(const float* const* frames, const float* const* refs, int width, int height, int channels,
+                           int d, int a, int s, float h2, float noise_offset, const float* lut,
+                           const float* const* conf_fwd, const float* const* conf_bwd, int conf_step, int blocks_x,
+                           int blocks_y, float wref, float* out) {
+    nlm_window_frame<float>(frames, refs, width, height, channels, d, a, s, h2, noise_offset, lut, conf_fwd,
+                            conf_bwd, conf_step, blocks_x, blocks_y, wref, out);
+}
+
 void orc_nlm_frame_f32(const float* const* frames, int width, int height, int channels, int d, int a, int s,
                        float h2, float noise_offset, const float* lut, const float* const* conf_fwd,
                        const float* const* conf_bwd, int conf_step, int blocks_x, int blocks_y, float wref,
                        float* out) {
-    nlm_window_frame<float>(frames, width, height, channels, d, a, s, h2, noise_offset, lut, conf_fwd, conf_bwd,
-                            conf_step, blocks_x, blocks_y, wref, out);
+    orc_nlm_frame_ref_f32(frames, nullptr, width, height, channels, d, a, s, h2, noise_offset, lut, conf_fwd,
+                          conf_bwd, conf_step, blocks_x, blocks_y, wref, out);
 }
 
 // The same maths in FP64 (inputs widened from f32).
-void orc_nlm_frame_f64(const float* const* frames, int width, int height, int channels, int d, int a, int s,
-                       double h2, double noise_offset, const float* lut, const float* const* conf_fwd,
-                       const float* const* conf_bwd, int conf_step, int blocks_x, int blocks_y, double wref,
-                       double* out) {
+void orc_nlm_frame_ref_f64(const float* const* frames, const float* const* refs, int width, int height, int channels,
+                           int d, int a, int s, double h2, double noise_offset, const float* lut,
+                           const float* const* conf_fwd, const float* const* conf_bwd, int conf_step, int blocks_x,
+                           int blocks_y, double wref, double* out) {
     const size_t n = (size_t)width * height * channels;
-    std::vector<std::vector<double>> wide(2 * d + 1, std::vector<double>(n));
-    std::vector<const double*> ptrs;
-    for (int i = 0; i < 2 * d + 1; ++i) {
-        for (size_t j = 0; j < n; ++j) wide[i][j] = frames[i][j];
-        ptrs.push_back(wide[i].data());
-    }
+    auto widen = [&](const float* const* src, std::vector<std::vector<double>>& wide, std::vector<const double*>& ptrs) {
+        wide.assign(2 * d + 1, std::vector<double>(n));
+        for (int i = 0; i < 2 * d + 1; ++i) {
+            for (size_t j = 0; j < n; ++j) wide[i][j] = src[i][j];
+            ptrs.push_back(wide[i].data());
+        }
+    };
+    std::vector<std::vector<double>> wide, wide_ref;
+    std::vector<const double*> ptrs, ref_ptrs;
+    widen(frames, wide, ptrs);
+    if (refs) widen(refs, wide_ref, ref_ptrs);
     std::vector<double> lut64;
     if (lut) {
         int side = 2 * a + 1;
         lut64.assign(lut, lut + side * side);
     }
-    nlm_window_frame<double>(ptrs.data(), width, height, channels, d, a, s, h2, noise_offset,
-                             lut ? lut64.data() : nullptr, conf_fwd, conf_bwd, conf_step, blocks_x, blocks_y,
-                             wref, out);
+    nlm_window_frame<double>(ptrs.data(), refs ? ref_ptrs.data() : nullptr, width, height, channels, d, a, s, h2,
+                             noise_offset, lut ? lut64.data() : nullptr, conf_fwd, conf_bwd, conf_step, blocks_x,
+                             blocks_y, wref, out);
+}
+
+void orc_nlm_frame_f64(const float* const* frames, int width, int height, int channels, int d, int a, int s,
+                       double h2, double noise_offset, const float* lut, const float* const* conf_fwd,
+                       const float* const* conf_bwd, int conf_step, int blocks_x, int blocks_y, double wref,
+                       double* out) {
+    orc_nlm_frame_ref_f64(frames, nullptr, width, height, channels, d, a, s, h2, noise_offset, lut, conf_fwd,
+                          conf_bwd, conf_step, blocks_x, blocks_y, wref, out);
+}
+
+// av-denoise-core/src/nlmeans/kernels/bilateral.rs:16-107 (`nlm_bilateral`), FP32 mirror: the
+// (2r+1)^2 clamped neighbours in row-major order, each weight
+// exp(-((dx^2 + dy^2) * inv_s + sum_c (n_c - c_c)^2 * inv_r)), and the weighted sum times the
+// reciprocal of the weight sum. `radius` is max(ceil(2 sigma_s), 1) and inv_s, inv_r are
+// 1 / (2 sigma^2) (prefilter/bilateral.rs:11-22).
+void orc_bilateral_f32(const float* frame, int width, int height, int channels, int radius, float inv_s,
+                       float inv_r, float* out) {
+    const Frame<float> f{frame, width, height, channels};
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int y = 0; y < height; ++y) {
+        for (int x = 0; x < width; ++x) {
+            const float* c = f.at_clamped(x, y);
+            float acc[2] = {0.0f, 0.0f};
+            float wsum = 0.0f;
+            for (int oy = 0; oy <= 2 * radius; ++oy) {
+                for (int ox = 0; ox <= 2 * radius; ++ox) {
+                    const int dy = oy - radius, dx = ox - radius;
+                    const float* n = f.at_clamped(x + dx, y + dy);
+                    float range_sq = 0.0f;
+                    for (int ch = 0; ch < channels; ++ch) {
+                        float lane = n[ch] - c[ch];
+                        float sq = lane * lane;
+                        range_sq = range_sq + sq;
+                    }
+                    float spatial = (float)(dx * dx + dy * dy) * inv_s;
+                    float r = range_sq * inv_r;
+                    float w = std::exp(-(spatial + r));
+                    for (int ch = 0; ch < channels; ++ch) {
+                        float t = n[ch] * w;
+                        acc[ch] = acc[ch] + t;
+                    }
+                    wsum = wsum + w;
+                }
+            }
+            const float inv = 1.0f / wsum;
+            float* o = out + ((size_t)y * width + x) * channels;
+            for (int ch = 0; ch < channels; ++ch) o[ch] = acc[ch] * inv;
+        }
+    }
 }
 
 }  // extern "C"

@@ -51,6 +51,9 @@ def lib():
                                         C.c_float, _fp, _fpp, _fpp, C.c_int, C.c_int, C.c_int, C.c_float, _fp]
         l.orc_nlm_frame_f64.argtypes = [_fpp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                         C.c_double, _fp, _fpp, _fpp, C.c_int, C.c_int, C.c_int, C.c_double, _dp]
+        l.orc_nlm_frame_ref_f32.argtypes = [_fpp, _fpp] + l.orc_nlm_frame_f32.argtypes[1:]
+        l.orc_nlm_frame_ref_f64.argtypes = [_fpp, _fpp] + l.orc_nlm_frame_f64.argtypes[1:]
+        l.orc_bilateral_f32.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _fp]
         _lib = l
     return _lib
 
@@ -115,13 +118,16 @@ def egress(frame: np.ndarray, fmt_kind: int, max_value: float, bias: float = 0.0
 def nlm_frame(window: list[np.ndarray], d: int, a: int, s: int, h2: float, noise_offset: float = 0.0,
               lut: np.ndarray | None = None, conf: list[tuple[np.ndarray, np.ndarray]] | None = None,
               conf_step: int = 8, blocks: tuple[int, int] = (1, 1), wref: float = 1.0,
-              fp64: bool = False) -> np.ndarray:
+              fp64: bool = False, refs: list[np.ndarray] | None = None) -> np.ndarray:
     """One windowed NLM output frame (FP32 mirror, or FP64). `window` holds 2d+1 (H, W, C) f32
-    frames, the centre at index d."""
+    frames, the centre at index d; `refs`, when given, the prefilter's reference frames of the same
+    window, which the patch distances compare instead."""
     assert len(window) == 2 * d + 1
     h, w, c = window[0].shape
     frames = [np.ascontiguousarray(f, np.float32) for f in window]
     arr = (_fp * len(frames))(*[_f(f) for f in frames])
+    rframes = [np.ascontiguousarray(f, np.float32) for f in refs] if refs is not None else None
+    rarr = (_fp * len(rframes))(*[_f(f) for f in rframes]) if rframes is not None else None
     lut_p = _f(np.ascontiguousarray(lut, np.float32)) if lut is not None else None
     cf = cb = None
     keep = []
@@ -133,29 +139,82 @@ def nlm_frame(window: list[np.ndarray], d: int, a: int, s: int, h2: float, noise
         cb = (_fp * d)(*[_f(x) for x in bw])
     if fp64:
         out = np.empty((h, w, c), np.float64)
-        lib().orc_nlm_frame_f64(arr, w, h, c, d, a, s, h2, noise_offset, lut_p, cf, cb, conf_step, blocks[0],
-                                blocks[1], wref, out.ctypes.data_as(_dp))
+        lib().orc_nlm_frame_ref_f64(arr, rarr, w, h, c, d, a, s, h2, noise_offset, lut_p, cf, cb, conf_step,
+                                    blocks[0], blocks[1], wref, out.ctypes.data_as(_dp))
     else:
         out = np.empty((h, w, c), np.float32)
-        lib().orc_nlm_frame_f32(arr, w, h, c, d, a, s, h2, noise_offset, lut_p, cf, cb, conf_step, blocks[0],
-                                blocks[1], wref, _f(out))
+        lib().orc_nlm_frame_ref_f32(arr, rarr, w, h, c, d, a, s, h2, noise_offset, lut_p, cf, cb, conf_step,
+                                    blocks[0], blocks[1], wref, _f(out))
     return out
+
+
+def bilateral_radius(sigma_s: float) -> int:
+    """nlmeans/prefilter/bilateral.rs:11-13: max(ceil(2 sigma_s), 1), in f32."""
+    return max(int(np.ceil(np.float32(2.0) * np.float32(sigma_s))), 1)
+
+
+def inv_two_sigma_sq(sigma: float) -> float:
+    """nlmeans/prefilter/bilateral.rs:20-22: 1 / (2 sigma^2), in f32."""
+    f = np.float32
+    return float(f(1.0) / ((f(2.0) * f(sigma)) * f(sigma)))
+
+
+def bilateral(frame: np.ndarray, sigma_s: float, sigma_r: float) -> np.ndarray:
+    """The bilateral prefilter of one (H, W, C) f32 frame (nlmeans/kernels/bilateral.rs:16-107)."""
+    h, w, c = frame.shape
+    src = np.ascontiguousarray(frame, np.float32)
+    out = np.empty_like(src)
+    lib().orc_bilateral_f32(_f(src), w, h, c, bilateral_radius(sigma_s), inv_two_sigma_sq(sigma_s),
+                            inv_two_sigma_sq(sigma_r), _f(out))
+    return out
+
+
+def pilot_h2(h2: float, strength_scale: float) -> float:
+    """nlmeans/dispatch/mod.rs:40-43: h2 / strength_scale^2, in f32."""
+    f = np.float32
+    return float(f(h2) / (f(strength_scale) * f(strength_scale)))
+
+
+def flat_offset_lut(a: int, offset: float) -> np.ndarray:
+    """noise/correlation.rs:71-88 at rho 0: `offset` for every candidate but the centre."""
+    side = 2 * a + 1
+    lut = np.full(side * side, offset, np.float32)
+    lut[a * side + a] = 0.0
+    return lut
+
+
+def prefilter_refs(frames: list[np.ndarray], prefilter, a: int, s: int, wref: float = 1.0) -> list[np.ndarray]:
+    """The reference frame of every stream frame under a fixed-strength prefilter
+    (nlmeans/denoiser/stages.rs:29-59): ("bilateral", sigma_s, sigma_r) blurs each frame;
+    ("nlm", pilot_h2, pilot_lut) denoises each frame alone with the windowed spatial pass at the
+    pilot strength and offset table (dispatch/mod.rs:598-620). The references are a function of
+    their own frame only, so an edge duplicate's reference is its frame's."""
+    kind = prefilter[0]
+    if kind == "bilateral":
+        return [bilateral(f, prefilter[1], prefilter[2]) for f in frames]
+    assert kind == "nlm"
+    return [nlm_frame([f], 0, a, s, prefilter[1], lut=prefilter[2], wref=wref) for f in frames]
 
 
 def nlm_stream_repeat(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, wref: float = 1.0,
                       noise_offset: float = 0.0, fp64: bool = False, lut: np.ndarray | None = None,
-                      conf_sigma: float | None = None, thsad_scale: float = 1.0) -> list[np.ndarray]:
+                      conf_sigma: float | None = None, thsad_scale: float = 1.0, prefilter=None) -> list[np.ndarray]:
     """The NLMeans engine over a whole stream with repeat edges: one output per input. With
-    `conf_sigma`, every temporal weight is scaled by the HQ confidence pass at that pinned sigma."""
+    `conf_sigma`, every temporal weight is scaled by the HQ confidence pass at that pinned sigma.
+    With `prefilter` (see `prefilter_refs`) the distances compare the reference frames; the
+    references themselves are always the FP32 mirror's, as the engine keeps them in f32."""
     n = len(frames)
+    refs = prefilter_refs(frames, prefilter, a, s, wref) if prefilter is not None else None
     outs = []
     for i in range(n):
-        window = [frames[min(max(i + k, 0), n - 1)] for k in range(-d, d + 1)]
+        idx = [min(max(i + k, 0), n - 1) for k in range(-d, d + 1)]
+        window = [frames[j] for j in idx]
         conf, blocks = None, (1, 1)
         if conf_sigma is not None and d > 0:
             conf, blocks = hq_confidence(window, d, conf_sigma, thsad_scale)
         outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, lut=lut, conf=conf, conf_step=8,
-                              blocks=blocks, wref=wref, fp64=fp64))
+                              blocks=blocks, wref=wref, fp64=fp64,
+                              refs=[refs[j] for j in idx] if refs is not None else None))
     return outs
 
 
@@ -757,6 +816,102 @@ def nlm_stream_hq_auto(frames: list[np.ndarray], d: int, a: int, s: int, strengt
         outs.append(nlm_frame(window, d, a, s, float(derived[6]), noise_offset=float(derived[8]), lut=lut, conf=cf,
                               conf_step=8, blocks=blocks, wref=wref, fp64=fp64))
     return outs, folds
+
+
+def fold_at(readings, totals, settings, channels: int, table_radius: int, temporal_radius: int, centre: int,
+            newest: int):
+    """The fold of the window around stream frame `centre` when frames 0..=newest are recorded
+    (noise/history.rs:31-44 over a history of 17 + d slots). Returns (state, derived, spatial, pilot)."""
+    cap = 2 * NOISE_WINDOW_RADIUS + 1 + temporal_radius
+    first, last = noise_window(centre, newest)
+    records = np.zeros(cap * READING_WORDS, np.float32)
+    results = np.zeros(cap * 2, np.float32)
+    for f in range(first, last + 1):
+        records[(f % cap) * READING_WORDS:(f % cap + 1) * READING_WORDS] = readings[f]
+        results[(f % cap) * 2:(f % cap) * 2 + 2] = totals[f]
+    return noise_fold(records, results, cap, first, last, settings, channels, table_radius)
+
+
+LOOKAHEAD_FRAMES = 8
+
+
+def nlm_stream_hq_auto_pilot(frames: list[np.ndarray], d: int, a: int, s: int, strength: float,
+                             strength_scale: float, *, wref: float = 1.0, auto_strength: bool = True,
+                             noise_floor: bool = True, temporal_confidence: bool = True, thsad_scale: float = 1.0,
+                             sigma_scale: float = 1.0, fp64: bool = False):
+    """NLMeans-HQ with the automatic noise estimate and the spatial-NLM pilot, replayed event by
+    event as the front runs it, since each pilot reads the derived words of the latest fold:
+      - a push first releases the oldest of 8 look-ahead frames into the ring (lookahead.rs:226-259),
+        then reads the pushed frame (recorded = pushes so far), then denoises the window centre if
+        the ring is full, folding around it first (dispatch/mod.rs:640-644);
+      - a frame entering the ring is piloted with the current derived words (stages.rs:29-40); the
+        stream's first frame folds the window around frame 0 first (noise.rs:147-165) and its d
+        leading-edge copies are piloted with the same words (ring.rs:103-180);
+      - the tail releases the held frames, then duplicates the last frame, each re-piloted with the
+        words of that moment, one output per step (denoiser/mod.rs:534-573).
+    The pilot uses derived word 7 and the fold's pilot table; the main pass word 6, offset word 8
+    (0 under the pilot) and the spatial table. Returns (outputs, [(centre, derived) per output])."""
+    h, w, c = frames[0].shape
+    f = np.float32
+    area = f((2 * s + 1) ** 2)
+    n = len(frames)
+    readings, totals = noise_readings(frames, c, w, h, d >= 1)
+    h2_unit = h2_inv_norm(float(f(strength) * f(1.0) * f(255.0)), s)
+    scale = f(3.0) if c == 1 else f(1.5)
+    offset_unit = float(((f(2.0) * scale) * f(1.0)) * area) if noise_floor else 0.0
+    conf = temporal_confidence and d > 0
+    sc = f(strength_scale)
+    settings = fold_words(w, h, sigma_scale=sigma_scale, h2_per_inverse_variance=h2_unit if auto_strength else None,
+                          h2_fixed=h2_inv_norm(strength, s), pilot_h2_factor=float(f(1.0) / (sc * sc)),
+                          offset_per_variance=offset_unit, main_offset=False,
+                          confidence_sad_per_sigma=sad_noise_floor(16, 1.0) if conf else 0.0)
+    state = {"fold": None, "recorded": 0}
+    entries = []  # (stream frame, reference) per ring entry, oldest first
+    outs, used = [], []
+
+    def pilot(frame_idx):
+        derived, pilot_table = state["fold"][1], state["fold"][3]
+        return nlm_frame([frames[frame_idx]], 0, a, s, float(derived[7]), lut=pilot_table, wref=wref)
+
+    def enter(frame_idx):
+        if not entries:
+            state["fold"] = fold_at(readings, totals, settings, c, a, d, 0, state["recorded"] - 1)
+        entries.append((frame_idx, pilot(frame_idx)))
+        if len(entries) == 1:
+            entries.extend([entries[0]] * d)
+
+    def denoise(newest):
+        if len(entries) < 2 * d + 1:
+            return
+        window = entries[-(2 * d + 1):]
+        centre = window[d][0]
+        fold = fold_at(readings, totals, settings, c, a, d, centre, newest)
+        state["fold"] = fold
+        derived, lut = fold[1], fold[2]
+        inputs = [frames[e[0]] for e in window]
+        cf, blocks = None, (1, 1)
+        if conf:
+            cf, blocks = hq_confidence(inputs, d, 0.0, thsad_scale, sad_floor=float(derived[5]))
+        outs.append(nlm_frame(inputs, d, a, s, float(derived[6]), noise_offset=float(derived[8]), lut=lut, conf=cf,
+                              conf_step=8, blocks=blocks, wref=wref, fp64=fp64, refs=[e[1] for e in window]))
+        used.append((centre, derived))
+
+    for i in range(n):
+        if i >= LOOKAHEAD_FRAMES:
+            enter(i - LOOKAHEAD_FRAMES)
+        state["recorded"] = i + 1
+        denoise(i)
+    held = list(range(max(n - LOOKAHEAD_FRAMES, 0), n))
+    while len(outs) < n:
+        before = len(outs)
+        while len(outs) == before:
+            if held:
+                enter(held.pop(0))
+            else:
+                last = entries[-1][0]
+                entries.append((last, pilot(last)))
+            denoise(n - 1)
+    return outs, used
 
 
 # ---- NLMeans adjoint (nlm_backward_oracle.cpp) -----------------------------------------------------

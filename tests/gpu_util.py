@@ -116,26 +116,35 @@ def hq_fixed_words(strength: float, sigma: float, s: int, channels: int, a: int)
 
 
 def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, wref=1.0, chroma=False,
-                out_fmt=None, exact=False, hq_sigma=None, hq_confidence=False, thsad_scale=1.0):
+                out_fmt=None, exact=False, hq_sigma=None, hq_confidence=False, thsad_scale=1.0, prefilter=None):
     """The oracle's output planes for one plane group over a stream (repeat edges).
 
-    Returns the FP32-mirror output planes; with `exact`, also the FP64 outputs as (H, W, C)
-    normalised floats, which mark the samples that sit on a rounding tie."""
+    `prefilter` is an `avd.PrefilterMode` (or None). Returns the FP32-mirror output planes; with
+    `exact`, also the FP64 outputs as (H, W, C) normalised floats, which mark the samples that sit
+    on a rounding tie."""
     out_fmt = out_fmt or fmt
     bias = 0.5 if (chroma and fmt.kind == 2) else 0.0
     f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), bias) for p in frames]
     h2, off, lut = oracle.h2_inv_norm(strength, s), 0.0, None
     if hq_sigma is not None:
         h2, off, lut = hq_fixed_words(strength, hq_sigma, s, 2 if chroma else 1, a)
+    pf = None
+    if prefilter is not None and prefilter.kind == 1:
+        pf = ("bilateral", prefilter.sigma_s, prefilter.sigma_r)
+    elif prefilter is not None and prefilter.kind == 2:
+        # nlmeans/denoiser/noise.rs:343-390: the pilot runs at h2 / scale^2 with the input's offset
+        # table; the main pass compares pilot outputs with no offset at all.
+        pf = ("nlm", oracle.pilot_h2(h2, prefilter.strength_scale), lut)
+        off, lut = 0.0, None
     cs = hq_sigma if hq_confidence else None
     outs = oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, conf_sigma=cs,
-                                    thsad_scale=thsad_scale)
+                                    thsad_scale=thsad_scale, prefilter=pf)
     obias = 0.5 if (chroma and out_fmt.kind == 2) else 0.0
     planes = [oracle.egress(o, out_fmt.kind, out_fmt.max_value(), obias) for o in outs]
     if not exact:
         return planes
     return planes, oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, fp64=True,
-                                            conf_sigma=cs, thsad_scale=thsad_scale)
+                                            conf_sigma=cs, thsad_scale=thsad_scale, prefilter=pf)
 
 
 # A sample whose exact (FP64) value lies within this distance, in normalised units, of a rounding

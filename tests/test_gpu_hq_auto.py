@@ -117,3 +117,36 @@ def test_hq_auto_reset_and_reuse(oracle):
     third = r.run(frames)
     for x, y in zip(first, third):
         assert np.array_equal(x[0], y[0])
+
+
+def hq_auto_pilot(d, a, s, scale, confidence=True):
+    mode = avd.DenoisingMode.temporal(d) if d else avd.DenoisingMode.spacial()
+    tuning = avd.NlmTuning(search_radius=a, patch_radius=s)
+    params = avd.HqParams(sigma_override=None, temporal_confidence=confidence)
+    opts = avd.NlmeansOptions(prefilter=avd.PrefilterMode.nlm_spatial(scale), tuning=tuning, mode=mode)
+    return avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(nlm=opts, hq=params))
+
+
+@pytest.mark.parametrize("w,h,n,d,a,s,scale,conf", [(96, 64, 12, 1, 3, 2, 0.4, True), (80, 48, 5, 2, 2, 1, 1.0, True),
+                                                    (72, 40, 11, 0, 4, 2, 0.6, False)])
+def test_hq_auto_with_the_pilot(oracle, w, h, n, d, a, s, scale, conf):
+    """The pilot reads the derived words of the latest fold as each frame enters the ring, the first
+    frame's after a fold around frame 0 (nlmeans/denoiser/noise.rs:147-165); the main pass compares
+    pilot outputs with no noise offset. The oracle replays the front event by event."""
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, n, seed=500 + n + d, sigma=7.0)
+    spec = avd.EngineSpec.nlmeans(hq_auto_pilot(d, a, s, scale, conf), None,
+                                  avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    strength = avd.hq_default_strength(1, d)
+    f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
+    outs, used = oracle.nlm_stream_hq_auto_pilot(f32, d, a, s, strength, scale, temporal_confidence=conf)
+    exact, _ = oracle.nlm_stream_hq_auto_pilot(f32, d, a, s, strength, scale, temporal_confidence=conf, fp64=True)
+    assert [u[0] for u in used] == list(range(n))
+    assert all(u[1][8] == 0.0 for u in used)
+    want = [oracle.egress(o, fmt.kind, fmt.max_value(), 0.0) for o in outs]
+    assert len(got) == len(want)
+    par = Parity()
+    for g, wn, ex in zip(got, want, exact):
+        par.add(g[0], wn[0], ex[..., 0], fmt.max_value())
+    print(par.check(min_raw=0.95))
