@@ -162,7 +162,15 @@ class AvdMotionPass(C.Structure):
     _fields_ = [(n, u64) for n in ("pyramid", "neighbour_slots", "mv_field", "confidence", "noise")] + \
                [(n, u32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize", "overlap",
                                    "search_radius", "levels", "mv_stride", "conf_stride", "sad_floor_word")] + \
-               [("thsad", f32), ("seeded", u32)]
+               [("thsad", f32), ("seeded", u32), ("keep_seeds", u64)]
+
+
+class AvdTruemotionPass(C.Structure):
+    _fields_ = [(n, u64) for n in ("pyramid", "neighbour_slots", "mv_in", "seeds", "mv_out", "confidence",
+                                   "noise")] + \
+               [(n, u32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize", "overlap",
+                                   "mv_stride", "conf_stride", "sad_field", "reads_floor")] + \
+               [("field_lambda", f32), ("thsad", f32)]
 
 
 class AvdNlmBackward(C.Structure):
@@ -238,6 +246,7 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_motion_pyramid_floats": (u64, [u32, u32, u32, u32]),
     "avd_motion_pyramid_build": (C.c_int, [u64, u32, u32, u32, u32, u32, u32, u64, u32, C.c_void_p]),
     "avd_motion_search": (C.c_int, [_P(AvdMotionPass), C.c_void_p]),
+    "avd_truemotion_pass": (C.c_int, [_P(AvdTruemotionPass), C.c_void_p]),
     "avd_chain_compose": (C.c_int, [u64, u64, u32, u32, u32, u32, u32, u32, u32, u32, u32, C.c_void_p]),
     "avd_sad_noise_floor": (f32, [u32, f32]),
     "avd_thsad": (f32, [u32, f32]),

@@ -38,8 +38,8 @@ COMMON = [
 # Per-file flags. The NL4D collaborative filter rounds every multiply and add on its own, as its CPU
 # restatement does (built with -ffp-contract=off), so its member choices and threshold decisions
 # agree bit for bit; -fmad=false keeps nvcc from fusing any of them. The noise estimate does the same
-# for its reading and fold words.
-PER_FILE = {"collab.cu": ["-fmad=false"], "noise_estimate.cu": ["-fmad=false"]}
+# for its reading and fold words, and the truemotion stage for its costs and confidences.
+PER_FILE = {"collab.cu": ["-fmad=false"], "noise_estimate.cu": ["-fmad=false"], "truemotion.cu": ["-fmad=false"]}
 
 
 def _sources() -> list[Path]:

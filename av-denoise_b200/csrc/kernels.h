@@ -114,6 +114,8 @@ struct MotionLaunch {
     int mv_stride, conf_stride, sad_floor_word;
     float thsad;
     int seeded;  // 1: the field already holds every block's seed; no coarse pass
+    int32_t* keep_seeds;  // non-null: the field after the coarse pass is copied here (the truemotion
+                          // stage's seed candidates)
 };
 
 int64_t pyramid_slot_pixels(int width, int height, int level);
@@ -123,6 +125,27 @@ int64_t pyramid_floats(int width, int height, int frame_count, int levels);
 cudaError_t launch_pyramid_build(const float* ring, int channels, int width, int height, int frame_count,
                                  int ring_slot, int levels, float* pyramid, int pyramid_slot, cudaStream_t stream);
 cudaError_t launch_motion_search(const MotionLaunch& args, cudaStream_t stream);
+
+// One truemotion pass (truemotion.cu, motion/truemotion/kernels/truemotion/mod.rs:560-763) over the
+// field `mv_in` into `mv_out` (a separate buffer), with `seeds` (or null) as extra candidates and
+// the confidence written when `confidence` is set. lambda_base = field_lambda * blksize^2 * 0.02,
+// lambda_noise = field_lambda, fade_level = 2 * thsad (truemotion/stage.rs:52-62).
+struct TruemotionLaunch {
+    static constexpr int kMaxInlineSlots = 16;
+    const float* pyramid;  // level 0: slot s starts s * slot_pixels values in
+    int64_t slot_pixels;
+    const uint32_t* neighbour_slots;  // device table, or null to read `inline_slots`
+    uint32_t inline_slots[kMaxInlineSlots];
+    const int32_t* mv_in;
+    const int32_t* seeds;
+    int32_t* mv_out;
+    float* confidence;
+    const float* noise;
+    int width, height, centre_slot, neighbours, blksize, step, blocks_x, blocks_y, mv_stride, conf_stride;
+    int sad_field, reads_floor, refine_radius;
+    float lambda_base, lambda_noise, surcharge, fade_level, thsad;
+};
+cudaError_t launch_truemotion(const TruemotionLaunch& args, cudaStream_t stream);
 
 // motion/kernels/chain.rs (`mc_chain_compose`): every neighbour's seed as the walk of pair vectors
 // from the centre. Neighbour n is logical position n (n < centre) or n + 1 of a 2d+1 window; the pair

@@ -553,6 +553,12 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
         if (a.L.blksize > kMaxBlk) return cudaErrorInvalidValue;
         dim3 grid(a.L.blocks_x, a.L.blocks_y, m.neighbours);
         if (cudaError_t e = dispatch_search(m.coarse_radius, true, a, grid, s)) return e;
+        // analyse.rs:268-277 (`keep_seeds`): the coarse field, before the fine pass overwrites it.
+        if (m.keep_seeds)
+            if (cudaError_t e = cudaMemcpyAsync(m.keep_seeds, m.mv_field,
+                                                static_cast<size_t>(m.neighbours) * m.mv_stride * sizeof(int32_t),
+                                                cudaMemcpyDeviceToDevice, s))
+                return e;
     }
     SearchArgs a{};
     a.L.pyramid = m.pyramid;

@@ -80,8 +80,57 @@ AvdStatus avd_motion_search(const AvdMotionPass* p, void* stream) {
     m.sad_floor_word = static_cast<int>(p->sad_floor_word);
     m.thsad = p->thsad;
     m.seeded = p->seeded ? 1 : 0;
+    m.keep_seeds = reinterpret_cast<int32_t*>(p->keep_seeds);
     cudaError_t e = avd::launch_motion_search(m, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("motion search launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+AvdStatus avd_truemotion_pass(const AvdTruemotionPass* p, void* stream) {
+    if (!p || !p->pyramid || !p->neighbour_slots || !p->mv_in || !p->mv_out || !p->noise)
+        return fail(AVD_ERR_NULL_ARG, "truemotion: null buffer");
+    if (p->mv_in == p->mv_out) return fail(AVD_ERR_INVALID_OPTIONS, "truemotion: mv_out must not be mv_in");
+    if (p->width == 0 || p->height == 0 || p->neighbours == 0 || p->centre_slot >= p->frame_count)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "truemotion: bad geometry");
+    if (p->blksize < 2 || p->blksize > 32 || p->overlap >= p->blksize)
+        return fail(AVD_ERR_INVALID_OPTIONS, "truemotion: blksize must be in 2..=32 and overlap below it");
+    if (!(p->field_lambda > 0.0f) || !std::isfinite(p->field_lambda) || !(p->thsad >= 0.0f))
+        return fail(AVD_ERR_INVALID_OPTIONS, "truemotion: field_lambda must be finite and positive");
+    const uint32_t step = p->blksize - p->overlap;
+    const uint32_t bx = std::max<uint32_t>((p->width + step - 1) / step, 1);
+    const uint32_t by = std::max<uint32_t>((p->height + step - 1) / step, 1);
+    if (p->mv_stride < 2 * bx * by || (p->confidence && p->conf_stride < bx * by))
+        return fail(AVD_ERR_INVALID_OPTIONS, "truemotion: field strides below the block count");
+    avd::TruemotionLaunch t{};
+    t.pyramid = reinterpret_cast<const float*>(p->pyramid);
+    t.slot_pixels = avd::pyramid_slot_pixels(static_cast<int>(p->width), static_cast<int>(p->height), 0);
+    t.neighbour_slots = reinterpret_cast<const uint32_t*>(p->neighbour_slots);
+    t.mv_in = reinterpret_cast<const int32_t*>(p->mv_in);
+    t.seeds = reinterpret_cast<const int32_t*>(p->seeds);
+    t.mv_out = reinterpret_cast<int32_t*>(p->mv_out);
+    t.confidence = reinterpret_cast<float*>(p->confidence);
+    t.noise = reinterpret_cast<const float*>(p->noise);
+    t.width = static_cast<int>(p->width);
+    t.height = static_cast<int>(p->height);
+    t.centre_slot = static_cast<int>(p->centre_slot);
+    t.neighbours = static_cast<int>(p->neighbours);
+    t.blksize = static_cast<int>(p->blksize);
+    t.step = static_cast<int>(step);
+    t.blocks_x = static_cast<int>(bx);
+    t.blocks_y = static_cast<int>(by);
+    t.mv_stride = static_cast<int>(p->mv_stride);
+    t.conf_stride = static_cast<int>(p->conf_stride);
+    t.sad_field = static_cast<int>(p->sad_field);
+    t.reads_floor = p->reads_floor ? 1 : 0;
+    t.refine_radius = 1;
+    // motion/truemotion/stage.rs:52-62 with params.rs:4-33.
+    t.lambda_base = p->field_lambda * static_cast<float>(p->blksize * p->blksize) * 0.02f;
+    t.lambda_noise = p->field_lambda * 1.0f;
+    t.surcharge = 0.125f;
+    t.fade_level = 2.0f * std::max(p->thsad, 0.0f);
+    t.thsad = p->thsad;
+    cudaError_t e = avd::launch_truemotion(t, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("truemotion launch: ") + cudaGetErrorString(e));
     return AVD_OK;
 }
 

@@ -218,6 +218,13 @@ class Nl4dPass final : public Pass {
         const size_t nbrs = 2 * d_;
         if ((e = mv_.alloc(nbrs * mv_stride_ * sizeof(int32_t))) != cudaSuccess) return gpu_failure("motion field", e);
         if ((e = conf_.alloc(nbrs * conf_stride_ * sizeof(float))) != cudaSuccess) return gpu_failure("confidence", e);
+        if (truemotion()) {
+            // motion/truemotion/stage.rs:14-27: the search's seeds and the field between passes.
+            if ((e = tm_seeds_.alloc(nbrs * mv_stride_ * sizeof(int32_t))) != cudaSuccess)
+                return gpu_failure("truemotion seeds", e);
+            if ((e = tm_field_.alloc(nbrs * mv_stride_ * sizeof(int32_t))) != cudaSuccess)
+                return gpu_failure("truemotion field", e);
+        }
         if (chained_) {
             // motion/context.rs:110-140: 2d pair slots of two directions, each a padded field.
             if ((e = pair_ring_.alloc(nbrs * 2 * mv_stride_ * sizeof(int32_t))) != cudaSuccess)
@@ -447,9 +454,57 @@ class Nl4dPass final : public Pass {
             m.neighbours = 1;
             m.mv_field = pair + dir * mv_stride_;
             m.confidence = nullptr;
-            cudaError_t e = launch_motion_search(m, stream);
-            if (e != cudaSuccess) return gpu_failure("pair analyse launch", e);
+            // motion/chain.rs:54-62: each direction ends with the stage at the unscaled penalty.
+            if (auto f = search_then_truemotion(m, false)) return f;
         }
+        return std::nullopt;
+    }
+
+    // ---- the truemotion stage (motion/analyse.rs:175-312, truemotion/stage.rs) ----
+    bool truemotion() const { return opts_.field_lambda > 0.0f; }
+
+    // The search `m`, then, with the stage on, one truemotion pass over its field with the coarse
+    // pass's field as the seed candidates; the pass's field lands back in `m.mv_field`.
+    std::optional<Failure> search_then_truemotion(MotionLaunch m, bool reads_floor) {
+        const bool coarse = m.levels > 1 && !m.seeded;
+        if (truemotion() && coarse) m.keep_seeds = tm_seeds_.as<int32_t>();
+        cudaError_t e = launch_motion_search(m, stream);
+        if (e != cudaSuccess) return gpu_failure("motion search launch", e);
+        if (!truemotion()) return std::nullopt;
+        TruemotionLaunch t{};
+        t.pyramid = m.pyramid;
+        t.slot_pixels = pyramid_slot_pixels(m.width, m.height, 0);
+        t.neighbour_slots = m.neighbour_slots;
+        for (int i = 0; i < TruemotionLaunch::kMaxInlineSlots; ++i) t.inline_slots[i] = m.inline_slots[i];
+        t.mv_in = m.mv_field;
+        t.seeds = coarse ? tm_seeds_.as<int32_t>() : nullptr;
+        t.mv_out = tm_field_.as<int32_t>();
+        t.confidence = m.confidence;
+        t.noise = m.noise;
+        t.width = m.width;
+        t.height = m.height;
+        t.centre_slot = m.centre_slot;
+        t.neighbours = m.neighbours;
+        t.blksize = m.blksize;
+        t.step = step_;
+        t.blocks_x = blocks_x_;
+        t.blocks_y = blocks_y_;
+        t.mv_stride = mv_stride_;
+        t.conf_stride = conf_stride_;
+        t.sad_field = kSadFloorWord;
+        t.reads_floor = reads_floor ? 1 : 0;
+        t.refine_radius = 1;  // truemotion/params.rs:15
+        // truemotion/stage.rs:52-62 with params.rs:4-33 (noise weight 1, surcharge 1/8, fade 2 thsad).
+        const float lambda = opts_.field_lambda;
+        t.lambda_base = lambda * static_cast<float>(m.blksize * m.blksize) * 0.02f;
+        t.lambda_noise = lambda * 1.0f;
+        t.surcharge = 0.125f;
+        t.fade_level = 2.0f * std::max(m.thsad, 0.0f);
+        t.thsad = m.thsad;
+        if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
+        e = cudaMemcpyAsync(m.mv_field, t.mv_out, static_cast<size_t>(m.neighbours) * mv_stride_ * sizeof(int32_t),
+                            cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return gpu_failure("truemotion field copy", e);
         return std::nullopt;
     }
 
@@ -528,9 +583,8 @@ class Nl4dPass final : public Pass {
         m.conf_stride = conf_stride_;
         m.sad_floor_word = kSadFloorWord;
         m.thsad = thsad_;
-        cudaError_t e = launch_motion_search(m, stream);
-        if (e != cudaSuccess) return gpu_failure("motion search launch", e);
-        return std::nullopt;
+        // nlmeans/dispatch/motion.rs:201-206: the window's floor scales the stage's penalty.
+        return search_then_truemotion(m, true);
     }
 
     enum class Clear { WholeRing, NewestRegion, Nothing };
@@ -706,6 +760,7 @@ class Nl4dPass final : public Pass {
 
     DeviceBuffer ring_, pyramid_, mv_, conf_, accum_, wsum_, group_weight_, members_, tables_, slot_tables_;
     DeviceBuffer pair_ring_;
+    DeviceBuffer tm_seeds_, tm_field_;  // the truemotion stage's seeds and output field
     bool chained_ = false;
     int refine_radius_ = 2;
     bool measures_ = false;

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kBx * kBy) bilateral_kernel(const float* __res
 }
 
 template <int C, int S, bool FAST>
-__global__ void __launch_bounds__(kThreads, 3) nlm_ref_window_kernel(NlmLaunch a) {
+__global__ void __launch_bounds__(kThreads, C == 1 ? 4 : 3) nlm_ref_window_kernel(NlmLaunch a) {
     nlm_tile<C, S, FAST, false, true>(a, blockIdx.x, blockIdx.y);
 }
 

@@ -566,7 +566,54 @@ def run_host(frames: int) -> None:
     print(json.dumps(line))
 
 
-def run_hq_auto(pushes: int) -> None:
+def run_prefilters(pushes: int) -> None:
+    """The NLMeans prefilters on the headline luma pass: 1920x1080 u8 luma, d=2, a=5, s=2,
+    strength 8, once with no prefilter, once with the bilateral reference ring (sigma_s 1.5, sigma_r
+    0.05: a 7x7 kernel) and once with the spatial-NLM pilot (strength scale 0.4). Each push writes one
+    ring slot (and its reference) and denoises one frame; prints the steady-state device time per
+    frame of each (CUDA events around every push) as one JSON line."""
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import synth
+
+    clip = synth.temporal_1080p_clip(frames=8, seed=21)
+    fmt = avd.SampleFormat.u8()
+    stream = torch.cuda.current_stream()
+    bufs = []
+    for f in clip:
+        flat = f[0].reshape(-1)
+        bufs.append(torch.from_numpy(np.concatenate([flat, np.zeros((-flat.size) % 4, np.uint8)]).view(np.int32)).cuda())
+    out = torch.zeros_like(bufs[0])
+    res = {}
+    for name, pf in (("none", avd.PrefilterMode.none()), ("bilateral:1.5,0.05", avd.PrefilterMode.bilateral(1.5, 0.05)),
+                     ("nlm:0.4", avd.PrefilterMode.nlm_spatial(0.4))):
+        t = avd.NlmTuning(search_radius=LUMA["a"], patch_radius=LUMA["s"], strength=LUMA["strength"])
+        alg = avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(prefilter=pf, tuning=t,
+                                                           mode=avd.DenoisingMode.temporal(LUMA["d"])))
+        eng = avd.build_engine(avd.EngineSpec.nlmeans(alg, None, avd.Geometry(W, H, avd.ChromaLayout.GRAY, fmt, fmt)))
+        eng.set_stream(stream.cuda_stream)
+        times = []
+        for i in range(pushes):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if eng.push([avd.DevicePlane.from_tensor(bufs[i % len(bufs)], W, H)]):
+                eng.emit_into([avd.DevicePlane.from_tensor(out, W, H)])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        eng.close()
+        steady = times[2 * LUMA["d"] + 1:]
+        res[name] = round(float(np.median(steady)), 4)
+    print(json.dumps({"workload": "NLMeans 1920x1080 u8 luma d=2 a=5 s=2 strength 8, per prefilter",
+                      "ms_per_frame": res,
+                      "over_plain": {k: round(v / res["none"], 4) for k, v in res.items()}}))
+
+
+def run_hq_auto(pushes: int, prefilter: str = "none") -> None:
     """NLMeans-HQ with the automatic noise estimate: 1920x1080 u8 luma, d=2, a=5, s=2, default HQ
     strength and temporal confidence, on the 1080p temporal clip. Each push reads one frame's noise
     in the look-ahead (Immerkaer, temporal records, reading) and, once the look-ahead and the ring
@@ -585,7 +632,8 @@ def run_hq_auto(pushes: int) -> None:
     t = avd.NlmTuning(search_radius=LUMA["a"], patch_radius=LUMA["s"])
     hq = avd.HqParams(sigma_override=None)
     alg = avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(
-        nlm=avd.NlmeansOptions(tuning=t, mode=avd.DenoisingMode.temporal(LUMA["d"])), hq=hq))
+        nlm=avd.NlmeansOptions(prefilter=avd.parse_prefilter(prefilter), tuning=t,
+                               mode=avd.DenoisingMode.temporal(LUMA["d"])), hq=hq))
     eng = avd.build_engine(avd.EngineSpec.nlmeans(alg, None, avd.Geometry(W, H, avd.ChromaLayout.GRAY, fmt, fmt)))
     stream = torch.cuda.current_stream()
     eng.set_stream(stream.cuda_stream)
@@ -607,6 +655,7 @@ def run_hq_auto(pushes: int) -> None:
     steady = times[8 + 2 * LUMA["d"] + 1:]
     ms = float(np.median(steady)) if steady else float("nan")
     print(json.dumps({"workload": "NLMeans-HQ automatic sigma, 1920x1080 u8 luma, d=2 a=5 s=2, temporal confidence",
+                      "prefilter": prefilter,
                       "ms_per_frame": round(ms, 4), "frames_per_s": round(1000.0 / ms, 2),
                       "push_ms": [round(x, 3) for x in times]}))
 
@@ -922,6 +971,9 @@ def main() -> None:
                     help="time FRAMES frames through the host denoiser against the resident engine and exit")
     ap.add_argument("--hq-auto", type=int, default=0, metavar="PUSHES",
                     help="time PUSHES pushes of NLMeans-HQ with the automatic noise estimate and exit")
+    ap.add_argument("--prefilters", type=int, default=0, metavar="PUSHES",
+                    help="time the headline luma pass with no prefilter, the bilateral and the NLM pilot")
+    ap.add_argument("--prefilter", default="none", help="prefilter of --hq-auto (none, nlm[:scale], bilateral:ss,sr)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -942,7 +994,9 @@ def main() -> None:
     elif args.host:
         run_host(args.host)
     elif args.hq_auto:
-        run_hq_auto(args.hq_auto)
+        run_hq_auto(args.hq_auto, args.prefilter)
+    elif args.prefilters:
+        run_prefilters(args.prefilters)
     elif args.impl == "reference":
         run_reference(args)
     else:

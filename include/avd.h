@@ -464,7 +464,7 @@ AVD_API AvdStatus avd_motion_pyramid_build(uint64_t ring, uint32_t channels, uin
                                            uint64_t pyramid, uint32_t pyramid_slot, void* stream);
 
 /* One block-matching motion search over a built pyramid, as `run_analyse` runs it without the
- * camera-model candidate and the truemotion stage (av-denoise-core/src/motion/analyse.rs:170-258),
+ * camera-model candidate, before its truemotion stage (av-denoise-core/src/motion/analyse.rs:170-266),
  * and as `run_confidence` runs it with `search_radius` 0 and one level (motion/confidence.rs:39-66). */
 typedef struct AvdMotionPass {
     uint64_t pyramid;         /* f32, avd_motion_pyramid_floats(width, height, frame_count, levels) */
@@ -478,9 +478,36 @@ typedef struct AvdMotionPass {
     float thsad; /* av-denoise-core/src/motion/confidence.rs:27-30; must be > 0 with confidence */
     uint32_t seeded; /* 1: `mv_field` already holds each block's seed and the search skips the coarse
                       * pass, as `run_seeded_refine` does (motion/analyse.rs:273-316) */
+    uint64_t keep_seeds; /* i32 like `mv_field`: the field after the coarse pass, the truemotion stage's
+                          * seed candidates (analyse.rs:268-277); 0 = not kept */
 } AvdMotionPass;
 
 AVD_API AvdStatus avd_motion_search(const AvdMotionPass* pass, void* stream);
+
+/* One pass of the truemotion stage that ends a search (av-denoise-core/src/motion/truemotion/
+ * stage.rs:29-145 with kernels/truemotion/mod.rs:560-763), without the camera-model candidate:
+ * every block of every neighbour picks its vector in `mv_in` again from its own vector, its 3x3
+ * lower median, its four adjacent blocks' vectors, zero and, with `seeds`, its own and its four
+ * diagonal blocks' seeds, at cost SAD + lambda * |v - median|_1 (+ SAD / 8 off the median), with
+ * lambda = field_lambda * blksize^2 * 0.02 + field_lambda * floor faded by the median's excess SAD
+ * over 2 * thsad, then the ring of radius 1 around a new winner. The floor is noise word
+ * `sad_field` when `reads_floor` and positive, else 0. Writes `mv_out` (a buffer apart from
+ * `mv_in`) and, when set, `confidence` scored against noise word `sad_field`. Queued on `stream`. */
+typedef struct AvdTruemotionPass {
+    uint64_t pyramid;         /* f32 pyramid; level 0 is read */
+    uint64_t neighbour_slots; /* u32 pyramid slot of each neighbour */
+    uint64_t mv_in;           /* i32 (dx, dy) per block per neighbour, `mv_stride` apart */
+    uint64_t seeds;           /* i32 like `mv_in`, the coarse pass's field; 0 = no seed candidates */
+    uint64_t mv_out;          /* i32 like `mv_in`; written */
+    uint64_t confidence;      /* f32 per block per neighbour, `conf_stride` apart; 0 = not written */
+    uint64_t noise;           /* f32 words */
+    uint32_t width, height, frame_count, centre_slot, neighbours;
+    uint32_t blksize, overlap, mv_stride, conf_stride, sad_field, reads_floor;
+    float field_lambda; /* > 0 */
+    float thsad;
+} AvdTruemotionPass;
+
+AVD_API AvdStatus avd_truemotion_pass(const AvdTruemotionPass* pass, void* stream);
 
 /* av-denoise-core/src/nlmeans/dispatch/motion.rs:619-690 (`run_chain_compose`) with
  * motion/kernels/chain.rs:20-72: every neighbour's seed of a pass centred on logical `centre` of a

@@ -1,7 +1,7 @@
 // CPU ORACLE - test infrastructure only (see nlm_oracle.cpp for the rules it follows).
 //
 // A C++17 restatement of av-denoise's block-matching motion search without the camera-model
-// candidate and the truemotion stage:
+// candidate, and of the truemotion stage that can end it:
 //   pyramid: av-denoise-core/src/motion/kernels/pyramid.rs:10-61 (lane-0 extract, 2x2 average,
 //            odd edge repeated) and motion/pyramid.rs:82-107 (levels built one after another);
 //   coarse:  motion/kernels/block_match.rs:117-215 and motion/analyse.rs:100-150 (the smallest
@@ -12,7 +12,13 @@
 //            refine of chained seeds);
 //   window:  block_match.rs:656-849 (clamped staging, SAD summed row by row left to right, lowest
 //            SAD with the first row-major index, the window's centre winning a tie, SADs at or
-//            above 1e30 never chosen).
+//            above 1e30 never chosen);
+//   truemotion: motion/truemotion/kernels/truemotion/{mod.rs,candidates.rs,score.rs} and
+//            truemotion/stage.rs (one pass: candidates own, 3x3 lower median, left/right/up/down,
+//            zero, the block's coarse seed and its four diagonal seeds; SAD + lambda per pixel of
+//            L1 distance from the median, a surcharge off the median, the early settle, the refine
+//            ring around a new best; each candidate's SAD summed per row left to right, then the
+//            rows top to bottom).
 // Every f32 operation is one rounded operation in the reference's order (the build turns off
 // contraction), so the vectors and confidences are expected to match the CUDA path bit for bit.
 //
@@ -111,6 +117,7 @@ struct OrcMotionArgs {
     uint32_t mv_stride, conf_stride, sad_floor_word;
     float thsad;
     uint32_t seeded;  // 1: mv_field holds the seeds; no coarse pass (motion/analyse.rs:273-316)
+    int32_t* keep_seeds;  // non-null: the field after the coarse pass is copied here (analyse.rs:268-277)
 };
 
 int64_t orc_motion_pyramid_floats(int w, int h, int frames, int levels) { return level_base(w, h, frames, levels); }
@@ -173,6 +180,8 @@ void orc_motion_search(const OrcMotionArgs* a) {
                             mv[(r * bx_n + c) * 2 + 1] = b.dy * scale;
                         }
                 }
+        if (a->keep_seeds)
+            std::copy(a->mv_field, a->mv_field + static_cast<int64_t>(a->neighbours) * a->mv_stride, a->keep_seeds);
     }
     Level L{a->pyramid, slot_pixels(w, h, 0), w, h, static_cast<int>(a->blksize), step, bx_n, by_n};
 #pragma omp parallel for collapse(2) schedule(dynamic)
@@ -195,6 +204,205 @@ void orc_motion_search(const OrcMotionArgs* a) {
                     a->confidence[static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx] = c;
                 }
             }
+}
+
+// One truemotion pass (motion/truemotion/kernels/truemotion/mod.rs:560-763, `mc_truemotion` with
+// the serial scoring of score.rs:7-61) over level 0 of `pyramid`: every block of every neighbour
+// picks its vector from `mv_in` (and `seeds`, when given) into `mv_out`, with its confidence when
+// `confidence` is given. No camera model (no prediction candidate), no change flags.
+struct OrcTruemotionArgs {
+    const float* pyramid;
+    const uint32_t* neighbour_slots;
+    const int32_t* mv_in;
+    const int32_t* seeds;  // null: no seed candidates
+    int32_t* mv_out;
+    float* confidence;  // null: not written
+    const float* noise;
+    uint32_t width, height, frame_count, centre_slot, neighbours, blksize, overlap, mv_stride, conf_stride;
+    uint32_t sad_field, reads_floor, refine_radius;
+    float lambda_base, lambda_noise, surcharge, fade_level, thsad;
+};
+
+namespace {
+
+struct Vec2 {
+    int dx, dy;
+};
+
+bool on_grid(int c, int r, int bx, int by) { return c >= 0 && r >= 0 && c < bx && r < by; }
+
+// candidates.rs:83-108 (`push_unique`).
+void push_unique(std::vector<Vec2>& list, Vec2 v) {
+    for (const Vec2& e : list)
+        if (e.dx == v.dx && e.dy == v.dy) return;
+    list.push_back(v);
+}
+
+// truemotion/kernels/truemotion/mod.rs:230-248 (`penalised_cost`).
+float penalised_cost(float sad, Vec2 v, Vec2 median, float lambda, float surcharge) {
+    const int deviation = std::abs(v.dx - median.dx) + std::abs(v.dy - median.dy);
+    float cost = sad + lambda * static_cast<float>(deviation);
+    if (deviation != 0 && surcharge > 0.0f) cost += surcharge * sad;
+    return cost;
+}
+
+// mod.rs:448-463 (`pass_confidence`).
+float pass_confidence(float sad, float floor, float thsad) {
+    float excess = sad - floor;
+    if (excess < 0.0f) excess = 0.0f;
+    const float t2 = thsad * thsad, e2 = excess * excess;
+    float c = (t2 - e2) / (t2 + e2);
+    if (c < 0.0f) c = 0.0f;
+    return c;
+}
+
+}  // namespace
+
+void orc_truemotion_pass(const OrcTruemotionArgs* a) {
+    const int w = static_cast<int>(a->width), h = static_cast<int>(a->height);
+    const int b = static_cast<int>(a->blksize), step = static_cast<int>(a->blksize - a->overlap);
+    const int bx_n = (w + step - 1) / step > 1 ? (w + step - 1) / step : 1;
+    const int by_n = (h + step - 1) / step > 1 ? (h + step - 1) / step : 1;
+    const int64_t slot = slot_pixels(w, h, 0);
+#pragma omp parallel for collapse(2) schedule(dynamic, 16)
+    for (int n = 0; n < static_cast<int>(a->neighbours); ++n)
+        for (int blk = 0; blk < bx_n * by_n; ++blk) {
+            const int col = blk % bx_n, row = blk / bx_n;
+            const int ox = col * step, oy = row * step;
+            const int64_t mv_base = static_cast<int64_t>(n) * a->mv_stride;
+            const float* cf = a->pyramid + a->centre_slot * slot;
+            const float* nf = a->pyramid + a->neighbour_slots[n] * slot;
+            auto field = [&](const int32_t* f, int c, int r) -> Vec2 {
+                if (!f || !on_grid(c, r, bx_n, by_n)) return Vec2{0, 0};
+                const int32_t* v = f + mv_base + (static_cast<int64_t>(r) * bx_n + c) * 2;
+                return Vec2{v[0], v[1]};
+            };
+            const Vec2 own = field(a->mv_in, col, row);
+            // candidates.rs:124-176 (`neighbourhood_median`): the component-wise lower median of the
+            // on-grid blocks of the 3x3 neighbourhood, the block's own vector without any.
+            std::vector<int> xs, ys;
+            for (int pos = 0; pos < 9; ++pos) {
+                if (pos == 4) continue;
+                const int c = col + pos % 3 - 1, r = row + pos / 3 - 1;
+                if (!on_grid(c, r, bx_n, by_n)) continue;
+                const Vec2 v = field(a->mv_in, c, r);
+                xs.push_back(v.dx);
+                ys.push_back(v.dy);
+            }
+            Vec2 median = own;
+            if (!xs.empty()) {
+                std::sort(xs.begin(), xs.end());
+                std::sort(ys.begin(), ys.end());
+                median = Vec2{xs[(xs.size() - 1) / 2], ys[(ys.size() - 1) / 2]};
+            }
+            // candidates.rs:178-306 (`gather_candidates`), without the model's prediction.
+            std::vector<Vec2> list;
+            push_unique(list, own);
+            push_unique(list, median);
+            const int side_dx[4] = {-1, 1, 0, 0}, side_dy[4] = {0, 0, -1, 1};
+            for (int sd = 0; sd < 4; ++sd)
+                if (on_grid(col + side_dx[sd], row + side_dy[sd], bx_n, by_n))
+                    push_unique(list, field(a->mv_in, col + side_dx[sd], row + side_dy[sd]));
+            push_unique(list, Vec2{0, 0});
+            if (a->seeds) {
+                push_unique(list, field(a->seeds, col, row));
+                for (int corner = 0; corner < 4; ++corner) {
+                    const int cc = col + (corner % 2) * 2 - 1, rr = row + (corner / 2) * 2 - 1;
+                    if (on_grid(cc, rr, bx_n, by_n)) push_unique(list, field(a->seeds, cc, rr));
+                }
+            }
+            int median_entry = 0;
+            for (int e = static_cast<int>(list.size()) - 1; e >= 0; --e)
+                if (list[e].dx == median.dx && list[e].dy == median.dy) median_entry = e;
+            // score.rs:7-61: each row summed left to right, then the rows top to bottom.
+            std::vector<float> centre(static_cast<size_t>(b) * b);
+            for (int py = 0; py < b; ++py)
+                for (int px = 0; px < b; ++px)
+                    centre[py * b + px] = cf[static_cast<int64_t>(clamp_to(oy + py, h)) * w + clamp_to(ox + px, w)];
+            auto sad_of = [&](Vec2 v) {
+                float sad = 0.0f;
+                for (int iy = 0; iy < b; ++iy) {
+                    const int ny = clamp_to(oy + iy + v.dy, h);
+                    float row_sum = 0.0f;
+                    for (int ix = 0; ix < b; ++ix) {
+                        const float diff = centre[iy * b + ix] - nf[static_cast<int64_t>(ny) * w + clamp_to(ox + ix + v.dx, w)];
+                        row_sum += diff < 0.0f ? -diff : diff;
+                    }
+                    sad += row_sum;
+                }
+                return sad;
+            };
+            std::vector<float> sads(list.size());
+            for (size_t e = 0; e < list.size(); ++e) sads[e] = sad_of(list[e]);
+            // mod.rs:250-276 (`block_lambda`).
+            const float median_sad = sads[median_entry];
+            float floor = 0.0f;
+            if (a->reads_floor) {
+                const float reading = a->noise[a->sad_field];
+                if (reading > 0.0f) floor = reading;
+            }
+            float lambda = a->lambda_base + a->lambda_noise * floor;
+            if (a->fade_level > 0.0f) {
+                const float excess = std::max(median_sad - floor, 0.0f);
+                const float level_sq = a->fade_level * a->fade_level;
+                const float fade = level_sq / (level_sq + excess * excess);
+                lambda *= fade;
+            }
+            // mod.rs:292-345 (`settle_early`).
+            const float own_cost = penalised_cost(sads[0], list[0], median, lambda, a->surcharge);
+            const float median_cost = penalised_cost(median_sad, median, median, lambda, a->surcharge);
+            int outcome = 0;  // 0 unsettled, 1 own wins, 2 median wins
+            if (list.size() == 1 || (median_entry == 0 && own_cost <= lambda)) {
+                outcome = 1;
+            } else if (median_entry == 1) {
+                if (own_cost <= median_cost && own_cost <= lambda) outcome = 1;
+                else if (median_cost < own_cost && median_cost <= lambda) outcome = 2;
+            }
+            Vec2 best = list[0];
+            float best_cost = own_cost, best_sad = sads[0];
+            if (outcome == 2) {
+                best = list[1];
+                best_cost = median_cost;
+                best_sad = sads[1];
+            }
+            if (outcome == 0) {
+                // mod.rs:347-387 (`pick_listed`): the lowest cost, a tie keeping the earlier entry.
+                size_t bi = 0;
+                for (size_t e = 1; e < list.size(); ++e) {
+                    const float cost = penalised_cost(sads[e], list[e], median, lambda, a->surcharge);
+                    if (cost < best_cost) {
+                        best_cost = cost;
+                        bi = e;
+                    }
+                }
+                best = list[bi];
+                best_sad = sads[bi];
+            }
+            const bool kept = best.dx == own.dx && best.dy == own.dy;
+            if (outcome != 1 && a->refine_radius > 0 && !kept) {
+                // mod.rs:389-441: the ring around the best, each replacing it only when cheaper.
+                const int reach = static_cast<int>(a->refine_radius);
+                const Vec2 centre_vec = best;
+                for (int ry = -reach; ry <= reach; ++ry)
+                    for (int rx = -reach; rx <= reach; ++rx) {
+                        if (rx == 0 && ry == 0) continue;
+                        const Vec2 v{centre_vec.dx + rx, centre_vec.dy + ry};
+                        const float sad = sad_of(v);
+                        const float cost = penalised_cost(sad, v, median, lambda, a->surcharge);
+                        if (cost < best_cost) {
+                            best_cost = cost;
+                            best_sad = sad;
+                            best = v;
+                        }
+                    }
+            }
+            int32_t* out = a->mv_out + mv_base + static_cast<int64_t>(blk) * 2;
+            out[0] = best.dx;
+            out[1] = best.dy;
+            if (a->confidence)
+                a->confidence[static_cast<int64_t>(n) * a->conf_stride + blk] =
+                    pass_confidence(best_sad, a->noise[a->sad_field], a->thsad);
+        }
 }
 
 }  // extern "C"

@@ -343,7 +343,63 @@ class MotionArgs(C.Structure):
         ("confidence", _fp), ("noise", _fp),
     ] + [(n, C.c_uint32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize",
                                    "overlap", "search_radius", "levels", "mv_stride", "conf_stride",
-                                   "sad_floor_word")] + [("thsad", C.c_float), ("seeded", C.c_uint32)]
+                                   "sad_floor_word")] + [("thsad", C.c_float), ("seeded", C.c_uint32),
+                                                         ("keep_seeds", C.POINTER(C.c_int32))]
+
+
+class TruemotionArgs(C.Structure):
+    _fields_ = [
+        ("pyramid", _fp), ("neighbour_slots", C.POINTER(C.c_uint32)), ("mv_in", C.POINTER(C.c_int32)),
+        ("seeds", C.POINTER(C.c_int32)), ("mv_out", C.POINTER(C.c_int32)), ("confidence", _fp), ("noise", _fp),
+    ] + [(n, C.c_uint32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize",
+                                   "overlap", "mv_stride", "conf_stride", "sad_field", "reads_floor",
+                                   "refine_radius")] + [(n, C.c_float) for n in ("lambda_base", "lambda_noise",
+                                                                                 "surcharge", "fade_level", "thsad")]
+
+
+# motion/truemotion/params.rs:4-33 and motion/confidence.rs:10.
+TRUEMOTION = dict(noise_weight=1.0, surcharge=0.125, fade_scale=2.0, refine_radius=1)
+THSAD_PIXEL = 0.02
+
+
+def truemotion_values(field_lambda: float, blksize: int, thsad_value: float) -> tuple[float, float, float]:
+    """motion/truemotion/stage.rs:52-62 in f32: (lambda_base, lambda_noise, fade_level)."""
+    f = np.float32
+    base = f(f(f(field_lambda) * f(blksize * blksize)) * f(THSAD_PIXEL))
+    noise = f(f(field_lambda) * f(TRUEMOTION["noise_weight"]))
+    fade = f(f(TRUEMOTION["fade_scale"]) * f(max(thsad_value, 0.0)))
+    return float(base), float(noise), float(fade)
+
+
+def truemotion_pass(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
+                    mv_in: np.ndarray, seeds: np.ndarray | None, *, blksize=16, overlap=8, field_lambda=1.0,
+                    thsad=0.0, sad_floor=0.0, reads_floor=True, confidence=False):
+    """One truemotion pass (no camera model): returns (mv (n, blocks, 2), conf (n, blocks))."""
+    step = blksize - overlap
+    bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
+    slots = np.ascontiguousarray(neighbour_slots, np.uint32)
+    n = slots.size
+    mv_in = np.ascontiguousarray(mv_in, np.int32).reshape(-1)
+    sd = np.ascontiguousarray(seeds, np.int32).reshape(-1) if seeds is not None else None
+    out = np.zeros_like(mv_in)
+    conf = np.zeros(n * bx * by, np.float32)
+    noise = np.array([sad_floor], np.float32)
+    lb, ln, fade = truemotion_values(field_lambda, blksize, thsad)
+    a = TruemotionArgs()
+    a.pyramid, a.neighbour_slots = _f(pyramid), slots.ctypes.data_as(C.POINTER(C.c_uint32))
+    a.mv_in = mv_in.ctypes.data_as(C.POINTER(C.c_int32))
+    a.seeds = sd.ctypes.data_as(C.POINTER(C.c_int32)) if sd is not None else None
+    a.mv_out = out.ctypes.data_as(C.POINTER(C.c_int32))
+    a.confidence = _f(conf) if confidence else None
+    a.noise = _f(noise)
+    a.width, a.height, a.frame_count, a.centre_slot, a.neighbours = width, height, frames, centre_slot, n
+    a.blksize, a.overlap, a.mv_stride, a.conf_stride = blksize, overlap, bx * by * 2, bx * by
+    a.sad_field, a.reads_floor, a.refine_radius = 0, int(reads_floor), TRUEMOTION["refine_radius"]
+    a.lambda_base, a.lambda_noise, a.surcharge, a.fade_level, a.thsad = lb, ln, TRUEMOTION["surcharge"], fade, thsad
+    l = lib()
+    l.orc_truemotion_pass.argtypes = [C.POINTER(TruemotionArgs)]
+    l.orc_truemotion_pass(C.byref(a))
+    return out.reshape(n, bx * by, 2), conf.reshape(n, bx * by)
 
 
 def motion_pyramid(ring: np.ndarray, channels: int, width: int, height: int, levels: int) -> np.ndarray:
@@ -362,9 +418,11 @@ def motion_pyramid(ring: np.ndarray, channels: int, width: int, height: int, lev
 
 def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
                   *, blksize=16, overlap=8, search_radius=4, levels=2, confidence=False, sad_floor=0.0,
-                  thsad=0.0, seeds: np.ndarray | None = None):
-    """One block-matching search (no camera model, no truemotion). Returns (mv (n, blocks, 2), conf).
-    With `seeds` (n, blocks, 2) the search refines around them and skips the coarse pass."""
+                  thsad=0.0, seeds: np.ndarray | None = None, field_lambda: float = 0.0, reads_floor: bool = True):
+    """One block-matching search (no camera model). Returns (mv (n, blocks, 2), conf).
+    With `seeds` (n, blocks, 2) the search refines around them and skips the coarse pass. With
+    `field_lambda` > 0 the truemotion stage ends the search (motion/analyse.rs:175-312): its seed
+    candidates are the coarse pass's field, when a coarse pass ran."""
     step = blksize - overlap
     bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
     slots = np.ascontiguousarray(neighbour_slots, np.uint32)
@@ -381,9 +439,16 @@ def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, cen
     a.blksize, a.overlap, a.search_radius, a.levels = blksize, overlap, search_radius, levels
     a.mv_stride, a.conf_stride, a.sad_floor_word, a.thsad = bx * by * 2, bx * by, 0, thsad
     a.seeded = int(seeds is not None)
+    coarse = levels > 1 and seeds is None
+    kept = np.zeros_like(mv) if (field_lambda > 0.0 and coarse) else None
+    a.keep_seeds = kept.ctypes.data_as(C.POINTER(C.c_int32)) if kept is not None else None
     l = lib()
     l.orc_motion_search.argtypes = [C.POINTER(MotionArgs)]
     l.orc_motion_search(C.byref(a))
+    if field_lambda > 0.0:
+        return truemotion_pass(pyramid, width, height, frames, centre_slot, slots, mv, kept, blksize=blksize,
+                               overlap=overlap, field_lambda=field_lambda, thsad=thsad, sad_floor=sad_floor,
+                               reads_floor=reads_floor, confidence=confidence)
     return mv.reshape(n, bx * by, 2), conf.reshape(n, bx * by)
 
 
@@ -438,9 +503,12 @@ def chain_compose(pairs: dict, centre: int, d: int, head_mod: int, step: int, wi
 def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, overlap=8, search_radius=4,
                 levels=2, refine=2, spatial_radius=9, lambda_ht=4.158, c_min=0.05, kaiser_beta=2.0,
                 pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0, chained: bool = False,
-                refine_radius: int = 2, noise=None) -> list[np.ndarray]:
-    """The NL4D engine with a pinned sigma and Direct motion (no camera model, no truemotion) over a
-    stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order.
+                refine_radius: int = 2, noise=None, field_lambda: float = 1.0) -> list[np.ndarray]:
+    """The NL4D engine with a pinned sigma and Direct or Chained motion (no camera model) over a
+    stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order. With
+    `field_lambda` > 0 the truemotion stage ends the Direct window search (reading the window's SAD
+    floor) and each pair search (without it); the chained refine runs none
+    (nlmeans/dispatch/motion.rs:201-206, denoiser/stages.rs:146-197).
 
     It follows nl4d/engine.rs:287-381 and nl4d/denoiser.rs:370-596: a shifted-edge ring of 2d+1
     slots; when the ring first fills at a scene start, head passes centred on logical 0..d-1, then
@@ -493,7 +561,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         else:
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=search_radius, levels=levels, confidence=True,
-                                     sad_floor=p_floor, thsad=th)
+                                     sad_floor=p_floor, thsad=th, field_lambda=field_lambda, reads_floor=True)
         acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
                                   confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
                                   c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
@@ -519,7 +587,8 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
             return
         older = (newer + tf - 1) % tf
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
-        kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels)
+        kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=th,
+                  field_lambda=field_lambda, reads_floor=False)
         fwd, _ = motion_search(pyr, w, h, tf, older, [newer], **kw)
         bwd, _ = motion_search(pyr, w, h, tf, newer, [older], **kw)
         pairs[st["head"] % (2 * d)] = (fwd[0], bwd[0])

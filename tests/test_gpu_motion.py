@@ -138,3 +138,88 @@ def test_chain_compose_matches_oracle(lib, oracle, w, h, d, centre, head_mod):
     got = mv.cpu().numpy().reshape(2 * d, stride)[:, :bx * by * 2].reshape(2 * d, bx * by, 2)
     want = oracle.chain_compose(pairs, centre, d, head_mod, step, w, h, bx, by)
     assert np.array_equal(got, want), np.argwhere(got != want)[:5]
+
+
+TM_CASES = [
+    # width, height, frames, levels, blksize, overlap, radius, field_lambda, reads_floor, sigma
+    (160, 96, 5, 2, 16, 8, 4, 1.0, True, 0.02),
+    (123, 77, 3, 3, 16, 8, 6, 1.0, False, 0.0),
+    (200, 120, 3, 2, 32, 16, 8, 2.5, True, 0.05),
+    (64, 48, 3, 1, 8, 4, 2, 0.5, True, 0.01),  # one level: no seed candidates
+    (33, 17, 3, 2, 8, 0, 3, 1.0, True, 0.03),
+    (16, 8, 3, 2, 16, 8, 2, 1.0, True, 0.02),  # a grid of 2 x 1 blocks
+]
+
+
+@pytest.mark.parametrize("case", TM_CASES, ids=lambda c: "x".join(map(str, c[:8])))
+def test_search_then_truemotion_matches_oracle_bit_for_bit(lib, oracle, case):
+    """The search with its truemotion stage (motion/analyse.rs:175-312): the coarse field kept as the
+    seed candidates, then one pass over the fine field; vectors and confidences bit for bit."""
+    import torch
+
+    from av_denoise_b200 import _abi
+
+    w, h, frames, levels, blksize, overlap, radius, lam, reads_floor, sigma = case
+    ring = moving_window(w, h, frames, seed=w * 3 + h, channels=1)
+    rng = np.random.default_rng(w)
+    ring = (ring + rng.normal(0, sigma, ring.shape)).astype(np.float32) if sigma else ring
+    centre = frames // 2
+    slots = [s for s in range(frames) if s != centre][::-1]
+    floor = oracle.sad_noise_floor(blksize, sigma)
+    th = oracle.thsad(blksize, 1.0)
+    o_pyr = oracle.motion_pyramid(ring, 1, w, h, levels)
+    o_mv, o_conf = oracle.motion_search(o_pyr, w, h, frames, centre, slots, blksize=blksize, overlap=overlap,
+                                        search_radius=radius, levels=levels, confidence=True, sad_floor=floor,
+                                        thsad=th, field_lambda=lam, reads_floor=reads_floor)
+    plain, _ = oracle.motion_search(o_pyr, w, h, frames, centre, slots, blksize=blksize, overlap=overlap,
+                                    search_radius=radius, levels=levels, sad_floor=floor, thsad=th)
+    step = blksize - overlap
+    bx, by = max(-(-w // step), 1), max(-(-h // step), 1)
+    n = len(slots)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    pyr = torch.from_numpy(o_pyr).cuda()
+    slots_t = torch.tensor(np.asarray(slots, np.int32), device="cuda")
+    mv = torch.zeros(n * bx * by * 2, dtype=torch.int32, device="cuda")
+    seeds = torch.zeros_like(mv)
+    out = torch.full_like(mv, 12345)
+    conf = torch.zeros(n * bx * by, dtype=torch.float32, device="cuda")
+    noise = torch.tensor([floor], dtype=torch.float32, device="cuda")
+    p = _abi.AvdMotionPass()
+    p.pyramid, p.neighbour_slots, p.mv_field, p.confidence, p.noise = (pyr.data_ptr(), slots_t.data_ptr(),
+                                                                         mv.data_ptr(), 0, noise.data_ptr())
+    p.width, p.height, p.frame_count, p.centre_slot, p.neighbours = w, h, frames, centre, n
+    p.blksize, p.overlap, p.search_radius, p.levels = blksize, overlap, radius, levels
+    p.mv_stride, p.conf_stride, p.sad_floor_word, p.thsad = bx * by * 2, bx * by, 0, th
+    p.keep_seeds = seeds.data_ptr() if levels > 1 else 0
+    assert lib.avd_motion_search(C.byref(p), stream) == 0, lib.avd_last_error().decode()
+    t = _abi.AvdTruemotionPass()
+    t.pyramid, t.neighbour_slots, t.mv_in = pyr.data_ptr(), slots_t.data_ptr(), mv.data_ptr()
+    t.seeds = seeds.data_ptr() if levels > 1 else 0
+    t.mv_out, t.confidence, t.noise = out.data_ptr(), conf.data_ptr(), noise.data_ptr()
+    t.width, t.height, t.frame_count, t.centre_slot, t.neighbours = w, h, frames, centre, n
+    t.blksize, t.overlap, t.mv_stride, t.conf_stride = blksize, overlap, bx * by * 2, bx * by
+    t.sad_field, t.reads_floor, t.field_lambda, t.thsad = 0, int(reads_floor), lam, th
+    assert lib.avd_truemotion_pass(C.byref(t), stream) == 0, lib.avd_last_error().decode()
+    torch.cuda.synchronize()
+    assert np.array_equal(mv.cpu().numpy().reshape(n, -1, 2), plain)
+    got = out.cpu().numpy().reshape(n, -1, 2)
+    assert np.array_equal(got, o_mv), np.argwhere(got != o_mv)[:5]
+    assert np.array_equal(conf.cpu().numpy().view(np.uint32), o_conf.reshape(-1).view(np.uint32))
+    print("blocks the stage changed:", int((got != plain).any(axis=2).sum()), "of", n * bx * by)
+
+
+def test_truemotion_rejects_bad_passes(lib):
+    from av_denoise_b200 import _abi
+
+    t = _abi.AvdTruemotionPass()
+    assert lib.avd_truemotion_pass(C.byref(t), None) != 0  # null buffers
+    t.pyramid = t.neighbour_slots = t.noise = 256
+    t.mv_in = t.mv_out = 512
+    t.width, t.height, t.frame_count, t.neighbours, t.blksize, t.overlap = 64, 48, 3, 2, 16, 8
+    t.mv_stride, t.conf_stride, t.field_lambda = 2 * 48, 48, 1.0
+    assert lib.avd_truemotion_pass(C.byref(t), None) != 0  # mv_out is mv_in
+    t.mv_out = 1024
+    t.field_lambda = 0.0
+    assert lib.avd_truemotion_pass(C.byref(t), None) != 0  # lambda 0 runs no stage
+    t.field_lambda, t.mv_stride = 1.0, 10
+    assert lib.avd_truemotion_pass(C.byref(t), None) != 0  # stride below the blocks

@@ -80,3 +80,63 @@ def test_pyramid_layout_and_downscale(oracle, lib):
     l1 = pyr[96:96 + 18].reshape(3, 6)
     f = frame
     assert l1[0, 0] == np.float32((((f[0, 0] + f[0, 1]) + f[1, 0]) + f[1, 1]) * np.float32(0.25))
+
+
+# ---- the truemotion stage (motion/truemotion), restated from its behavioural suite ------------------
+
+def _ring(frames):
+    return np.stack([f[..., None] for f in frames]).astype(np.float32)
+
+
+def test_truemotion_keeps_a_static_scene_still(oracle):
+    f = textured(96, 64, 3)
+    ring = _ring([f, f, f])
+    pyr = oracle.motion_pyramid(ring, 1, 96, 64, 2)
+    mv, conf = oracle.motion_search(pyr, 96, 64, 3, 1, [0, 2], confidence=True, sad_floor=0.0,
+                                    thsad=oracle.thsad(16, 1.0), field_lambda=1.0)
+    assert not mv.any()
+    assert np.all(conf == 1.0)
+
+
+def test_truemotion_pulls_a_stray_vector_to_the_consensus_on_flat_content(oracle):
+    """truemotion/tests/stage.rs (`the_penalty_prefers_the_consensus_on_a_flat_noisy_block`): a pan
+    over a flat, grainy frame gives the flat blocks vectors the grain picked; the penalty brings a
+    planted stray vector back to its neighbourhood's."""
+    w, h = 96, 64
+    rng = np.random.default_rng(4)
+    flat = np.full((h, w), 0.5, np.float32)
+    a = flat + rng.normal(0, 0.01, (h, w)).astype(np.float32)
+    b = flat + rng.normal(0, 0.01, (h, w)).astype(np.float32)
+    ring = _ring([a, b])
+    pyr = oracle.motion_pyramid(ring, 1, w, h, 1)
+    step = 8
+    bx, by = -(-w // step), -(-h // step)
+    field = np.tile(np.array([2, 1], np.int32), (1, bx * by, 1))
+    stray = 3 * bx + 4
+    field[0, stray] = (-3, 2)
+    th = oracle.thsad(16, 1.0)
+    out, _ = oracle.truemotion_pass(pyr, w, h, 2, 0, [1], field, None, field_lambda=1.0, thsad=th,
+                                    sad_floor=oracle.sad_noise_floor(16, 0.01), reads_floor=True)
+    assert tuple(out[0, stray]) == (2, 1)
+    assert np.all(out[0] == (2, 1)), "every block keeps or joins the consensus"
+
+
+def test_truemotion_keeps_true_motion_on_texture(oracle):
+    """stage.rs (`the_penalty_keeps_the_true_motion_on_a_textured_block`): a textured frame shifted
+    by (3, -2) keeps that vector through the stage, even from a field seeded off by one."""
+    w, h = 96, 64
+    f = textured(w, h, 8)
+    g = shifted(f, 3, -2)
+    ring = _ring([f, g])
+    pyr = oracle.motion_pyramid(ring, 1, w, h, 2)
+    th = oracle.thsad(16, 1.0)
+    mv, _ = oracle.motion_search(pyr, w, h, 2, 0, [1], search_radius=4, thsad=th, field_lambda=1.0)
+    inner = mv[0].reshape(-(-h // 8), -(-w // 8), 2)[1:-2, 1:-2]
+    assert np.all(inner[..., 0] == 3) and np.all(inner[..., 1] == -2)
+
+
+def test_truemotion_values_follow_the_stage(oracle):
+    """truemotion/stage.rs:52-62: lambda_base = lambda * area * 0.02, fade level 2 thsad."""
+    base, noise, fade = oracle.truemotion_values(1.0, 16, oracle.thsad(16, 1.0))
+    assert base == pytest.approx(256 * 0.02) and noise == 1.0 and fade == pytest.approx(2 * 256 * 0.02)
+    assert oracle.truemotion_values(0.0, 16, 5.0)[:2] == (0.0, 0.0)
