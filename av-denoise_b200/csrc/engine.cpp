@@ -42,11 +42,26 @@ class NlmPass final : public Pass {
         const NlmParams& p = pass->params_;
         // nlmeans/denoiser/noise.rs:50-52 (`measures_noise`): HQ without a pinned sigma measures it.
         pass->measures_ = p.hq && !p.hq_params.has_sigma_override;
-        if (p.motion.active && p.temporal_radius > 0)
-            return Failure{AVD_ERR_INVALID_OPTIONS, "NLMeans motion compensation is not available in this build"};
+        // nlmeans/denoiser/mod.rs:242-246: motion compensation needs a temporal window.
+        pass->mc_ = p.motion.active && p.temporal_radius > 0;
+        if (pass->mc_) {
+            const AvdMotionSearch& m = p.motion.search;
+            if (m.max_search_escalation > m.search_radius)
+                return Failure{AVD_ERR_INVALID_OPTIONS,
+                               "motion search escalation is not available in this build; set max_search_escalation "
+                               "to search_radius"};
+            // motion/search.rs:133-139: Auto resolves to Chained { refine_radius: 2 } at d >= 3.
+            pass->mc_chained_ = m.estimation == AVD_ESTIMATION_CHAINED ||
+                                (m.estimation == AVD_ESTIMATION_AUTO && p.temporal_radius >= kChainedRadiusThreshold);
+            pass->mc_refine_radius_ =
+                static_cast<int>(m.estimation == AVD_ESTIMATION_CHAINED ? m.refine_radius : kDefaultRefineRadius);
+        }
         // nlmeans/denoiser/mod.rs:340-370: confidence without motion compensation scores every
-        // neighbour block where it stands (blksize 16, step 8, radius 0, one level).
-        pass->conf_pass_ = p.hq && p.hq_params.temporal_confidence && p.temporal_radius > 0;
+        // neighbour block where it stands (blksize 16, step 8, radius 0, one level); with it the
+        // window search scores its own blocks.
+        const bool confidence = p.hq && p.hq_params.temporal_confidence && p.temporal_radius > 0;
+        pass->conf_pass_ = confidence && !pass->mc_;
+        pass->mc_conf_ = confidence && pass->mc_;
         if (auto f = pass->allocate()) return f;
         *result = std::move(pass);
         return std::nullopt;
@@ -172,6 +187,13 @@ class NlmPass final : public Pass {
             const float sc = params_.prefilter.strength_scale;
             words[3] = words[0] / (sc * sc);
         }
+        if (mc_ && (e = allocate_motion()) != cudaSuccess) return gpu_failure("motion compensation buffers", e);
+        if (mc_) {
+            // noise.rs:360-363 with dispatch/motion.rs:28-72: the window search's SAD floor (word 4)
+            // at the pinned sigma times the prefilter's residual fraction (0 for both prefilters).
+            const float residual = has_reference() ? 0.0f : 1.0f;
+            words[kFixedSadFloor] = avd_sad_noise_floor(mc_blksize(), (has_sigma ? sigma : 0.0f) * residual);
+        }
         if (conf_pass_) {
             // motion/confidence.rs:17-30; nlmeans/denoiser/noise.rs:365-368: the confidence floor
             // uses the pinned sigma unscaled by any prefilter.
@@ -237,6 +259,17 @@ class NlmPass final : public Pass {
             k.main_offset = false;
         }
         k.confidence_sad_per_sigma = conf_pass_ ? avd_sad_noise_floor(kConfBlk, 1.0f) : 0.0f;
+        if (mc_) {
+            // noise.rs:226-229: the window search's floor per unit sigma, the prefilter's residual
+            // fraction applied; the look-ahead reads each frame along its motion (lookahead.rs).
+            k.sad_per_sigma = avd_sad_noise_floor(mc_blksize(), has_reference() ? 0.0f : 1.0f);
+            cfg.motion = true;
+            cfg.blksize = static_cast<int>(params_.motion.search.blksize);
+            cfg.overlap = static_cast<int>(params_.motion.search.overlap);
+            cfg.search_radius = static_cast<int>(params_.motion.search.search_radius);
+            cfg.levels = static_cast<int>(params_.motion.search.pyramid_levels);
+            cfg.thsad = mc_thsad();
+        }
         return noise_.allocate(cfg);
     }
 
@@ -297,6 +330,7 @@ class NlmPass final : public Pass {
         if (runs_pilot() && measures_ && frames_loaded_ == 0)
             if (auto f = noise_.fold(0, stream)) return f;
         if (auto f = run_prefilter(slot)) return f;
+        if (auto f = mc_slot_written(slot, false)) return f;
         if (auto f = slot_written(slot)) return f;
         slot_frames_[slot] = static_cast<uint32_t>(real_pushes_);
         advance_ring();
@@ -364,6 +398,7 @@ class NlmPass final : public Pass {
         }
         if (runs_pilot())
             if (auto f = run_pilot(next)) return f;
+        if (auto f = mc_slot_written(next, true)) return f;
         if (auto f = slot_written(next)) return f;
         slot_frames_[next] = slot_frames_[last];
         ring_head_ += 1;
@@ -412,6 +447,201 @@ class NlmPass final : public Pass {
         a.out = ref_slot_ptr(slot);
         cudaError_t e = launch_nlm(a, stream);
         if (e != cudaSuccess) return gpu_failure("nlm pilot launch", e);
+        return std::nullopt;
+    }
+
+    // ---- motion compensation (nlmeans/dispatch/motion.rs, denoiser/stages.rs:62-209) ----
+    uint32_t mc_blksize() const { return params_.motion.search.blksize; }
+    int mc_step() const { return static_cast<int>(params_.motion.search.blksize - params_.motion.search.overlap); }
+    float mc_thsad() const {
+        // dispatch/motion.rs:75-79 (`search_thsad`).
+        return avd_thsad(mc_blksize(), params_.hq ? params_.hq_params.thsad_scale : 1.0f);
+    }
+    int mc_levels() const { return static_cast<int>(params_.motion.search.pyramid_levels); }
+    float* mc_search_pyramid() const { return has_reference() ? mc_ref_pyr_.as<float>() : mc_pyr_.as<float>(); }
+
+    cudaError_t allocate_motion() {
+        const int step = mc_step();
+        mc_bx_ = std::max<int>((static_cast<int>(width_) + step - 1) / step, 1);
+        mc_by_ = std::max<int>((static_cast<int>(height_) + step - 1) / step, 1);
+        mc_mv_stride_ = static_cast<int>((2LL * mc_bx_ * mc_by_ + 7) / 8 * 8);
+        mc_conf_stride_ = static_cast<int>((static_cast<int64_t>(mc_bx_) * mc_by_ + 7) / 8 * 8);
+        const size_t nbrs = 2 * params_.temporal_radius, fe = frame_elems(), t = total_frames();
+        const size_t pyr = static_cast<size_t>(
+            pyramid_floats(static_cast<int>(width_), static_cast<int>(height_), static_cast<int>(t), mc_levels()));
+        cudaError_t e;
+        if ((e = mc_pyr_.alloc(pyr * sizeof(float))) != cudaSuccess) return e;
+        if ((e = comp_.alloc(fe * t * sizeof(float))) != cudaSuccess) return e;
+        if (has_reference()) {
+            if ((e = mc_ref_pyr_.alloc(pyr * sizeof(float))) != cudaSuccess) return e;
+            if ((e = comp_ref_.alloc(fe * t * sizeof(float))) != cudaSuccess) return e;
+        }
+        if ((e = mc_mv_.alloc(nbrs * mc_mv_stride_ * sizeof(int32_t))) != cudaSuccess) return e;
+        if ((e = tm_seeds_.alloc(nbrs * mc_mv_stride_ * sizeof(int32_t))) != cudaSuccess) return e;
+        if ((e = tm_field_.alloc(nbrs * mc_mv_stride_ * sizeof(int32_t))) != cudaSuccess) return e;
+        if (mc_conf_ && (e = mc_conf_buf_.alloc(nbrs * mc_conf_stride_ * sizeof(float))) != cudaSuccess) return e;
+        if (mc_chained_) {
+            // motion/context.rs:209-211: 2d pair slots of two directions each.
+            if ((e = pair_ring_.alloc(nbrs * 2 * mc_mv_stride_ * sizeof(int32_t))) != cudaSuccess) return e;
+            if ((e = cudaMemset(pair_ring_.ptr, 0, pair_ring_.bytes)) != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+
+    MotionLaunch mc_launch() const {
+        MotionLaunch m{};
+        m.pyramid = mc_search_pyramid();
+        m.noise = measures_ ? noise_.derived() : derived_.as<float>();
+        m.width = static_cast<int>(width_);
+        m.height = static_cast<int>(height_);
+        m.frame_count = static_cast<int>(total_frames());
+        m.blksize = static_cast<int>(params_.motion.search.blksize);
+        m.overlap = static_cast<int>(params_.motion.search.overlap);
+        m.search_radius = static_cast<int>(params_.motion.search.search_radius);
+        m.coarse_radius = m.search_radius;
+        m.coarse_block_factor = 1;
+        m.levels = mc_levels();
+        m.mv_stride = mc_mv_stride_;
+        m.conf_stride = mc_conf_stride_;
+        m.sad_floor_word = measures_ ? kDerivedSadFloor : kFixedSadFloor;
+        m.thsad = mc_thsad();
+        return m;
+    }
+
+    // stages.rs:62-108 and 146-209: a slot's pyramids (the input's, and the reference's under a
+    // prefilter), then the pair between it and the slot before (both ways, into pair slot ring_head
+    // mod 2d), or, for an edge copy, that pair slot zeroed.
+    std::optional<Failure> mc_slot_written(size_t slot, bool duplicate) {
+        if (!mc_) return std::nullopt;
+        const int t = static_cast<int>(total_frames());
+        cudaError_t e = launch_pyramid_build(ring_.as<float>(), static_cast<int>(params_.channel_count()),
+                                             static_cast<int>(width_), static_cast<int>(height_), t,
+                                             static_cast<int>(slot), mc_levels(), mc_pyr_.as<float>(),
+                                             static_cast<int>(slot), stream);
+        if (e == cudaSuccess && has_reference())
+            e = launch_pyramid_build(ref_.as<float>(), static_cast<int>(params_.channel_count()),
+                                     static_cast<int>(width_), static_cast<int>(height_), t, static_cast<int>(slot),
+                                     mc_levels(), mc_ref_pyr_.as<float>(), static_cast<int>(slot), stream);
+        if (e != cudaSuccess) return gpu_failure("motion pyramid launch", e);
+        if (!mc_chained_) return std::nullopt;
+        const size_t d = params_.temporal_radius;
+        int32_t* pair = pair_ring_.as<int32_t>() + (ring_head_ % (2 * d)) * 2 * mc_mv_stride_;
+        if (duplicate) {
+            if ((e = cudaMemsetAsync(pair, 0, 2 * mc_mv_stride_ * sizeof(int32_t), stream)) != cudaSuccess)
+                return gpu_failure("pair clear", e);
+            return std::nullopt;
+        }
+        if (ring_head_ == 0) return std::nullopt;
+        const size_t older = (slot + total_frames() - 1) % total_frames();
+        for (int dir = 0; dir < 2; ++dir) {
+            MotionLaunch m = mc_launch();
+            m.inline_slots[0] = static_cast<uint32_t>(dir == 0 ? slot : older);
+            m.centre_slot = static_cast<int>(dir == 0 ? older : slot);
+            m.neighbours = 1;
+            m.mv_field = pair + dir * mc_mv_stride_;
+            m.confidence = nullptr;
+            // motion/chain.rs:54-62: each direction ends with the stage at the unscaled penalty.
+            if (auto f = search_then_truemotion(m, false)) return f;
+        }
+        return std::nullopt;
+    }
+
+    // motion/analyse.rs:175-312: the search, then one truemotion pass (field_lambda 1, the NLMeans
+    // front's default) with the coarse pass's field as the seed candidates.
+    std::optional<Failure> search_then_truemotion(MotionLaunch m, bool reads_floor) {
+        const bool coarse = m.levels > 1 && !m.seeded;
+        if (coarse) m.keep_seeds = tm_seeds_.as<int32_t>();
+        cudaError_t e = launch_motion_search(m, stream);
+        if (e != cudaSuccess) return gpu_failure("motion search launch", e);
+        TruemotionLaunch t{};
+        t.pyramid = m.pyramid;
+        t.slot_pixels = pyramid_slot_pixels(m.width, m.height, 0);
+        t.neighbour_slots = nullptr;
+        for (int i = 0; i < TruemotionLaunch::kMaxInlineSlots; ++i) t.inline_slots[i] = m.inline_slots[i];
+        t.mv_in = m.mv_field;
+        t.seeds = coarse ? tm_seeds_.as<int32_t>() : nullptr;
+        t.mv_out = tm_field_.as<int32_t>();
+        t.confidence = m.confidence;
+        t.noise = m.noise;
+        t.width = m.width;
+        t.height = m.height;
+        t.centre_slot = m.centre_slot;
+        t.neighbours = m.neighbours;
+        t.blksize = m.blksize;
+        t.step = mc_step();
+        t.blocks_x = mc_bx_;
+        t.blocks_y = mc_by_;
+        t.mv_stride = mc_mv_stride_;
+        t.conf_stride = mc_conf_stride_;
+        t.sad_field = m.sad_floor_word;
+        t.reads_floor = reads_floor ? 1 : 0;
+        t.refine_radius = 1;  // truemotion/params.rs:15
+        // truemotion/stage.rs:52-62 with params.rs:4-33 at the default field_lambda 1.
+        const float lambda = 1.0f;
+        t.lambda_base = lambda * static_cast<float>(m.blksize * m.blksize) * 0.02f;
+        t.lambda_noise = lambda * 1.0f;
+        t.surcharge = 0.125f;
+        t.fade_level = 2.0f * std::max(m.thsad, 0.0f);
+        t.thsad = m.thsad;
+        if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
+        e = cudaMemcpyAsync(m.mv_field, t.mv_out, static_cast<size_t>(m.neighbours) * mc_mv_stride_ * sizeof(int32_t),
+                            cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return gpu_failure("truemotion field copy", e);
+        return std::nullopt;
+    }
+
+    // dispatch/motion.rs:427-487 then 104-229: the centre copied through, every neighbour's motion
+    // estimated (Chained: the pair walk refined with confidence; Direct: the search with its
+    // truemotion stage reading the window's floor), then each neighbour warped into the
+    // compensated rings (compensate.rs).
+    std::optional<Failure> run_motion_compensation() {
+        const int d = static_cast<int>(params_.temporal_radius);
+        const size_t centre = static_cast<size_t>(phys_frame(d));
+        const size_t bytes = frame_elems() * sizeof(float);
+        cudaError_t e = cudaMemcpyAsync(comp_.as<float>() + centre * frame_elems(), slot_ptr(centre), bytes,
+                                        cudaMemcpyDeviceToDevice, stream);
+        if (e == cudaSuccess && has_reference())
+            e = cudaMemcpyAsync(comp_ref_.as<float>() + centre * frame_elems(), ref_slot_ptr(centre), bytes,
+                                cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return gpu_failure("centre copy", e);
+        MotionLaunch m = mc_launch();
+        int n = 0;
+        for (int l = 0; l <= 2 * d; ++l)
+            if (l != d) m.inline_slots[n++] = static_cast<uint32_t>(phys_frame(l));
+        m.centre_slot = static_cast<int>(centre);
+        m.neighbours = n;
+        m.mv_field = mc_mv_.as<int32_t>();
+        m.confidence = mc_conf_ ? mc_conf_buf_.as<float>() : nullptr;
+        if (mc_chained_) {
+            e = launch_chain_compose(pair_ring_.as<int32_t>(), mc_mv_.as<int32_t>(), mc_mv_stride_, d, d,
+                                     static_cast<int>(ring_head_ % (2 * d)), mc_mv_stride_, 2 * mc_mv_stride_,
+                                     mc_step(), static_cast<int>(width_), static_cast<int>(height_), mc_bx_, mc_by_,
+                                     stream);
+            if (e != cudaSuccess) return gpu_failure("chain compose launch", e);
+            m.search_radius = mc_refine_radius_;
+            m.coarse_radius = mc_refine_radius_;
+            m.seeded = 1;
+            if ((e = launch_motion_search(m, stream)) != cudaSuccess) return gpu_failure("seeded refine launch", e);
+        } else {
+            if (auto f = search_then_truemotion(m, true)) return f;
+        }
+        WarpLaunch w{};
+        w.src_ring = ring_.as<float>();
+        w.dst_ring = comp_.as<float>();
+        w.src_ref = has_reference() ? ref_.as<float>() : nullptr;
+        w.dst_ref = has_reference() ? comp_ref_.as<float>() : nullptr;
+        w.mv_field = mc_mv_.as<int32_t>();
+        w.mv_stride = mc_mv_stride_;
+        for (int i = 0; i < n; ++i) w.slots[i] = m.inline_slots[i];
+        w.neighbours = n;
+        w.frame_elems = static_cast<int64_t>(frame_elems());
+        w.channels = static_cast<int>(params_.channel_count());
+        w.width = static_cast<int>(width_);
+        w.height = static_cast<int>(height_);
+        w.step = mc_step();
+        w.blocks_x = mc_bx_;
+        w.blocks_y = mc_by_;
+        if ((e = launch_warp(w, stream)) != cudaSuccess) return gpu_failure("warp launch", e);
         return std::nullopt;
     }
 
@@ -502,6 +732,22 @@ class NlmPass final : public Pass {
         a.offset_word = measures_ ? kDerivedNoiseOffset : 1;
         a.spatial_lut = measures_ ? noise_.spatial_table() : (params_.hq ? lut_.as<float>() : nullptr);
         a.conf = nullptr;
+        if (mc_) {
+            if (auto f = run_motion_compensation()) return f;
+            // dispatch/mod.rs:141-200: the temporal passes read the compensated rings, weighted by
+            // the window search's confidence per motion block.
+            a.ring = comp_.as<float>();
+            if (mc_conf_) {
+                a.conf = mc_conf_buf_.as<float>();
+                for (int k = 0; k < d; ++k) {
+                    a.conf_fwd_off[k] = static_cast<int64_t>(k) * mc_conf_stride_;
+                    a.conf_bwd_off[k] = static_cast<int64_t>(2 * d - 1 - k) * mc_conf_stride_;
+                }
+                a.conf_step = mc_step();
+                a.blocks_x = mc_bx_;
+                a.blocks_y = mc_by_;
+            }
+        }
         if (conf_pass_) {
             if (auto f = run_confidence_pass()) return f;
             // dispatch/mod.rs:175-200: pair k (q_k = -d + k) weighs its forward frame by neighbour
@@ -519,7 +765,7 @@ class NlmPass final : public Pass {
         a.wref = params_.self_weight;
         a.fast = params_.hq ? 0 : 1;
         a.out = outputs_[slot].as<float>();
-        a.ref_ring = has_reference() ? ref_.as<float>() : nullptr;
+        a.ref_ring = has_reference() ? (mc_ ? comp_ref_.as<float>() : ref_.as<float>()) : nullptr;
         cudaError_t e = launch_nlm(a, stream);
         if (e != cudaSuccess) return gpu_failure("nlm launch", e);
         if (timed) timer_.end(stream, start);
@@ -561,8 +807,13 @@ class NlmPass final : public Pass {
         if (measures_) noise_.reset();
     }
 
-    static constexpr int kDerivedConfidenceSadFloor = 5, kDerivedH2 = 6, kDerivedPilotH2 = 7,
+    static constexpr int kDerivedSadFloor = 4, kDerivedConfidenceSadFloor = 5, kDerivedH2 = 6, kDerivedPilotH2 = 7,
                          kDerivedNoiseOffset = 8;  // derived.rs:9-31
+    static constexpr int kFixedSadFloor = 4;  // the window search's floor among the fixed words
+
+    bool mc_ = false, mc_chained_ = false, mc_conf_ = false;
+    int mc_refine_radius_ = 2, mc_bx_ = 1, mc_by_ = 1, mc_mv_stride_ = 2, mc_conf_stride_ = 1;
+    DeviceBuffer mc_pyr_, mc_ref_pyr_, comp_, comp_ref_, mc_mv_, tm_seeds_, tm_field_, mc_conf_buf_, pair_ring_;
     bool measures_ = false;
     NoiseFront noise_;
 

@@ -147,6 +147,24 @@ struct TruemotionLaunch {
 };
 cudaError_t launch_truemotion(const TruemotionLaunch& args, cudaStream_t stream);
 
+// motion/kernels/compensate.rs (`mc_warp`) for every neighbour of a window in one launch: ring slot
+// slots[n] of `src_ring` (and `src_ref`, when set) warped along neighbour n's field into the same
+// slot of `dst_ring` (and `dst_ref`).
+struct WarpLaunch {
+    static constexpr int kMaxSlots = 16;
+    const float* src_ring;
+    float* dst_ring;
+    const float* src_ref;
+    float* dst_ref;
+    const int32_t* mv_field;
+    int mv_stride;
+    uint32_t slots[kMaxSlots];
+    int neighbours;
+    int64_t frame_elems;
+    int channels, width, height, step, blocks_x, blocks_y;
+};
+cudaError_t launch_warp(const WarpLaunch& args, cudaStream_t stream);
+
 // motion/kernels/chain.rs (`mc_chain_compose`): every neighbour's seed as the walk of pair vectors
 // from the centre. Neighbour n is logical position n (n < centre) or n + 1 of a 2d+1 window; the pair
 // between logical g and g+1 sits in pair slot (head_mod + g) mod 2d, direction 0 older-to-newer and

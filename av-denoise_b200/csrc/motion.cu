@@ -587,6 +587,25 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
 }
 
 namespace {
+// motion/kernels/compensate.rs:6-44 (`mc_warp`): pixel (x, y) of neighbour n takes the vector of
+// block (min(x / step, bx - 1), min(y / step, by - 1)) and copies the source pixel at the clamped
+// (x + dx, y + dy), every channel; the reference ring follows the same vectors when given.
+__global__ void __launch_bounds__(256) warp_kernel(WarpLaunch w) {
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= w.width || y >= w.height) return;
+    const int n = blockIdx.z;
+    const int64_t slot = w.slots[n];
+    const int bc = min(x / w.step, w.blocks_x - 1), br = min(y / w.step, w.blocks_y - 1);
+    const int32_t* mv = w.mv_field + static_cast<int64_t>(n) * w.mv_stride + 2 * (br * w.blocks_x + bc);
+    const int sx = clamp_to(x + mv[0], w.width), sy = clamp_to(y + mv[1], w.height);
+    const int64_t src = slot * w.frame_elems + (static_cast<int64_t>(sy) * w.width + sx) * w.channels;
+    const int64_t dst = slot * w.frame_elems + (static_cast<int64_t>(y) * w.width + x) * w.channels;
+    for (int c = 0; c < w.channels; ++c) w.dst_ring[dst + c] = __ldg(w.src_ring + src + c);
+    if (w.src_ref)
+        for (int c = 0; c < w.channels; ++c) w.dst_ref[dst + c] = __ldg(w.src_ref + src + c);
+}
+
 __global__ void chain_compose_kernel(const int32_t* __restrict__ pair_ring, int32_t* __restrict__ mv_field,
                                      int mv_stride, int centre, int d, int head_mod, int dir_stride,
                                      int slot_stride, int step, int width, int height, int blocks_x, int blocks_y) {
@@ -625,6 +644,16 @@ cudaError_t launch_chain_compose(const int32_t* pair_ring, int32_t* mv_field, in
     dim3 grid((blocks_x + 63) / 64, blocks_y, 2 * d);
     chain_compose_kernel<<<grid, 64, 0, s>>>(pair_ring, mv_field, mv_stride, centre, d, head_mod, dir_stride,
                                              slot_stride, step, width, height, blocks_x, blocks_y);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_warp(const WarpLaunch& w, cudaStream_t s) {
+    if (!w.src_ring || !w.dst_ring || !w.mv_field || (w.src_ref && !w.dst_ref) || w.neighbours < 1 ||
+        w.neighbours > WarpLaunch::kMaxSlots || w.channels < 1 || w.channels > 2 || w.step < 1 || w.blocks_x < 1 ||
+        w.blocks_y < 1)
+        return cudaErrorInvalidValue;
+    dim3 grid((w.width + 31) / 32, (w.height + 7) / 8, w.neighbours);
+    warp_kernel<<<grid, dim3(32, 8), 0, s>>>(w);
     return cudaGetLastError();
 }
 

@@ -218,6 +218,123 @@ def nlm_stream_repeat(frames: list[np.ndarray], d: int, a: int, s: int, h2: floa
     return outs
 
 
+def mc_warp(frame: np.ndarray, mv: np.ndarray, step: int, bx: int, by: int) -> np.ndarray:
+    """motion/kernels/compensate.rs:6-44 (`mc_warp`): pixel (x, y) takes the vector of block
+    (min(x / step, bx - 1), min(y / step, by - 1)) and copies the source pixel at the clamped
+    (x + dx, y + dy)."""
+    h, w, _ = frame.shape
+    ys, xs = np.mgrid[0:h, 0:w]
+    v = np.asarray(mv, np.int32).reshape(by, bx, 2)[np.minimum(ys // step, by - 1), np.minimum(xs // step, bx - 1)]
+    return frame[np.clip(ys + v[..., 1], 0, h - 1), np.clip(xs + v[..., 0], 0, w - 1)]
+
+
+def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *, wref: float = 1.0,
+                  noise_offset: float = 0.0, lut: np.ndarray | None = None, confidence: bool = False,
+                  sad_floor: float = 0.0, thsad_scale: float = 1.0, blksize: int = 16, overlap: int = 8,
+                  search_radius: int = 4, levels: int = 2, chained: bool = False, refine_radius: int = 2,
+                  prefilter=None, fp64: bool = False) -> list[np.ndarray]:
+    """NLMeans with motion compensation over a stream with repeat edges, replayed slot by slot as
+    the ring runs it (nlmeans/denoiser/ring.rs, stages.rs:62-209, dispatch/motion.rs:104-487):
+      - each slot write (and each edge copy) builds the slot's pyramids; with Chained estimation it
+        then searches the pair between the slot and the one before it both ways (each direction
+        ending with the truemotion stage, floor unread) into pair slot ring_head mod 2d, or zeroes
+        that pair slot for an edge copy;
+      - each window matches every neighbour against the centre on the reference's pyramid under a
+        prefilter, else the input's: Chained walks the pair ring and refines `refine_radius` around
+        the walk, Direct searches with its truemotion stage reading the window's floor; with
+        `confidence` (HQ temporal confidence) the search scores each block against `sad_floor`;
+      - every neighbour (and its reference) is warped along its field, the temporal passes compare
+        the warped frames, weighted by the confidence of their motion blocks.
+    `prefilter` is as in `prefilter_refs` (fixed strength). Returns one output per input."""
+    n = len(frames)
+    h, w, c = frames[0].shape
+    tf = 2 * d + 1
+    step = blksize - overlap
+    bx, by = max(-(-w // step), 1), max(-(-h // step), 1)
+    refs_of = prefilter_refs(frames, prefilter, a, s, wref) if prefilter is not None else None
+    th = thsad(blksize, thsad_scale)
+    slot_frame = [0] * tf
+    zero = np.zeros((bx * by, 2), np.int32)
+    pairs = {i: (zero, zero) for i in range(2 * d)}
+    st = dict(head=0, loaded=0)
+    outs = []
+
+    def search_pyramid():
+        src = refs_of if refs_of is not None else frames
+        ring = np.stack([src[f] for f in slot_frame]).astype(np.float32)
+        return motion_pyramid(ring.reshape(-1), c, w, h, levels)
+
+    def write(slot, frame_idx, duplicate):
+        slot_frame[slot] = frame_idx
+        if not chained:
+            return
+        if duplicate:
+            pairs[st["head"] % (2 * d)] = (zero, zero)
+        elif st["head"] > 0:
+            older = (slot + tf - 1) % tf
+            pyr = search_pyramid()
+            kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=th,
+                      field_lambda=1.0, reads_floor=False)
+            fwd, _ = motion_search(pyr, w, h, tf, older, [slot], **kw)
+            bwd, _ = motion_search(pyr, w, h, tf, slot, [older], **kw)
+            pairs[st["head"] % (2 * d)] = (fwd[0], bwd[0])
+
+    def duplicate_last():
+        last, nxt = (st["head"] - 1) % tf, st["head"] % tf
+        write(nxt, slot_frame[last], True)
+        st["head"] += 1
+
+    def enter(frame_idx):
+        write(st["head"] % tf, frame_idx, False)
+        st["head"] += 1
+        st["loaded"] = min(st["loaded"] + 1, tf)
+        if st["loaded"] == 1:
+            for _ in range(d):
+                duplicate_last()
+                st["loaded"] += 1
+
+    def denoise():
+        if st["loaded"] < tf:
+            return
+        phys = [(st["head"] % tf + l) % tf for l in range(tf)]
+        cs = phys[d]
+        slots = [phys[l] for l in range(tf) if l != d]
+        pyr = search_pyramid()
+        if chained:
+            seeds = chain_compose(pairs, d, d, st["head"] % (2 * d), step, w, h, bx, by)
+            mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
+                                   search_radius=refine_radius, levels=levels, confidence=confidence,
+                                   sad_floor=sad_floor, thsad=th, seeds=seeds)
+        else:
+            mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
+                                   search_radius=search_radius, levels=levels, confidence=confidence,
+                                   sad_floor=sad_floor, thsad=th, field_lambda=1.0, reads_floor=True)
+        window, refs = [], []
+        idx = 0
+        for l in range(tf):
+            f = slot_frame[phys[l]]
+            if l == d:
+                window.append(frames[f])
+                refs.append(refs_of[f] if refs_of is not None else None)
+                continue
+            window.append(mc_warp(frames[f], mv[idx], step, bx, by))
+            refs.append(mc_warp(refs_of[f], mv[idx], step, bx, by) if refs_of is not None else None)
+            idx += 1
+        conf = [(cf[k], cf[2 * d - 1 - k]) for k in range(d)] if confidence else None
+        outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, lut=lut, conf=conf, conf_step=step,
+                              blocks=(bx, by), wref=wref, fp64=fp64,
+                              refs=refs if refs_of is not None else None))
+
+    for i in range(n):
+        enter(i)
+        denoise()
+    while len(outs) < n:
+        duplicate_last()
+        st["loaded"] = min(st["loaded"] + 1, tf)
+        denoise()
+    return outs
+
+
 def hq_confidence(window: list[np.ndarray], d: int, sigma: float, thsad_scale: float = 1.0,
                   sad_floor: float | None = None):
     """The HQ confidence pass over one window (nlmeans/dispatch/motion.rs:554-613): lane 0 of every

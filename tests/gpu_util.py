@@ -116,12 +116,13 @@ def hq_fixed_words(strength: float, sigma: float, s: int, channels: int, a: int)
 
 
 def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, wref=1.0, chroma=False,
-                out_fmt=None, exact=False, hq_sigma=None, hq_confidence=False, thsad_scale=1.0, prefilter=None):
+                out_fmt=None, exact=False, hq_sigma=None, hq_confidence=False, thsad_scale=1.0, prefilter=None,
+                motion=None):
     """The oracle's output planes for one plane group over a stream (repeat edges).
 
-    `prefilter` is an `avd.PrefilterMode` (or None). Returns the FP32-mirror output planes; with
-    `exact`, also the FP64 outputs as (H, W, C) normalised floats, which mark the samples that sit
-    on a rounding tie."""
+    `prefilter` is an `avd.PrefilterMode` (or None); `motion` an `avd.MotionSearch` for motion
+    compensation (or None). Returns the FP32-mirror output planes; with `exact`, also the FP64
+    outputs as (H, W, C) normalised floats, which mark the samples that sit on a rounding tie."""
     out_fmt = out_fmt or fmt
     bias = 0.5 if (chroma and fmt.kind == 2) else 0.0
     f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), bias) for p in frames]
@@ -137,14 +138,31 @@ def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, 
         pf = ("nlm", oracle.pilot_h2(h2, prefilter.strength_scale), lut)
         off, lut = 0.0, None
     cs = hq_sigma if hq_confidence else None
-    outs = oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, conf_sigma=cs,
-                                    thsad_scale=thsad_scale, prefilter=pf)
+    if motion is not None and d > 0:
+        # nlmeans/denoiser/noise.rs:360-363: the window search's floor at the pinned sigma times the
+        # prefilter's residual fraction (0 for both prefilters).
+        sigma_y = (hq_sigma or 0.0) * (0.0 if pf is not None else 1.0)
+        chained = motion.estimation == avd.MotionEstimation.CHAINED or (
+            motion.estimation == avd.MotionEstimation.AUTO and d >= 3)
+        refine = motion.refine_radius if motion.estimation == avd.MotionEstimation.CHAINED else 2
+
+        def run(fp64):
+            return oracle.nlm_stream_mc(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut,
+                                        confidence=hq_confidence, sad_floor=oracle.sad_noise_floor(motion.blksize,
+                                                                                                   sigma_y),
+                                        thsad_scale=thsad_scale, blksize=motion.blksize, overlap=motion.overlap,
+                                        search_radius=motion.search_radius, levels=motion.pyramid_levels,
+                                        chained=chained, refine_radius=refine, prefilter=pf, fp64=fp64)
+    else:
+        def run(fp64):
+            return oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, fp64=fp64,
+                                            conf_sigma=cs, thsad_scale=thsad_scale, prefilter=pf)
+    outs = run(False)
     obias = 0.5 if (chroma and out_fmt.kind == 2) else 0.0
     planes = [oracle.egress(o, out_fmt.kind, out_fmt.max_value(), obias) for o in outs]
     if not exact:
         return planes
-    return planes, oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, fp64=True,
-                                            conf_sigma=cs, thsad_scale=thsad_scale, prefilter=pf)
+    return planes, run(True)
 
 
 # A sample whose exact (FP64) value lies within this distance, in normalised units, of a rounding

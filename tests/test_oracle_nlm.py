@@ -138,3 +138,33 @@ def test_stream_repeat_edges(oracle):
     assert np.array_equal(outs[0], first)
     last = oracle.nlm_frame([frames[0], frames[1], frames[2], frames[2], frames[2]], 2, 1, 1, h2)
     assert np.array_equal(outs[2], last)
+
+
+# ---- motion compensation (motion/kernels/compensate.rs, nlmeans/dispatch/motion.rs) ---------------
+
+def test_mc_warp_follows_each_blocks_vector(oracle):
+    rng = np.random.default_rng(1)
+    f = rng.random((20, 28, 2), dtype=np.float32)
+    bx, by, step = 4, 3, 8
+    assert np.array_equal(oracle.mc_warp(f, np.zeros((bx * by, 2), np.int32), step, bx, by), f)
+    mv = np.zeros((bx * by, 2), np.int32)
+    mv[:] = (2, -1)
+    got = oracle.mc_warp(f, mv, step, bx, by)
+    ys, xs = np.mgrid[0:20, 0:28]
+    assert np.array_equal(got, f[np.clip(ys - 1, 0, 19), np.clip(xs + 2, 0, 27)])
+    mv[bx * by - 1] = (-5, 4)  # the last block also covers the ragged right and bottom edges
+    got = oracle.mc_warp(f, mv, step, bx, by)
+    assert np.array_equal(got[16:, 24:], f[np.clip(ys[16:, 24:] + 4, 0, 19), np.clip(xs[16:, 24:] - 5, 0, 27)])
+
+
+@pytest.mark.parametrize("d,chained", [(1, False), (2, False), (3, True)])
+def test_motion_compensation_of_a_still_clip_is_the_plain_pass(oracle, d, chained):
+    """Every block of identical frames matches where it stands, so the warped window is the window
+    and the output is the plain pass's, bit for bit."""
+    rng = np.random.default_rng(2)
+    f = rng.random((40, 48, 1), dtype=np.float32)
+    frames = [f] * 4
+    h2 = oracle.h2_inv_norm(6.0, 1)
+    plain = oracle.nlm_stream_repeat(frames, d, 2, 1, h2)
+    mc = oracle.nlm_stream_mc(frames, d, 2, 1, h2, chained=chained)
+    assert all(np.array_equal(x, y) for x, y in zip(plain, mc))
