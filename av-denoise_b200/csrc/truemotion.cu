@@ -21,10 +21,15 @@
 // a search that escalates).
 //
 // Layout and design: one warp per (block, neighbour), four per CTA, each with its own slice of
-// shared memory: the block's centre pixels, the candidate list and a row-sum tile. A candidate's
-// rows are spread over the lanes (each lane sums one row left to right), then one lane per
-// candidate adds its rows top to bottom, so every SAD is the reference's sum bit for bit. The
-// candidate logic runs on lane 0. The file is built with -fmad=false so no multiply-add is fused.
+// shared memory: the staged 3x3 field and seeds, the candidate list, a |difference| tile and the
+// row sums. Candidates are scored in chunks of 32 / blksize: lane l owns column l mod blksize of
+// candidate l / blksize, keeps that column of the centre block in registers, and walks down the
+// rows (so each load instruction reads whole row segments) writing |centre - neighbour| into the
+// tile (rows padded to an odd stride); then each lane sums one tile row left to right, and one lane
+// per candidate adds its rows top to bottom, so every SAD is the reference's sum bit for bit. The
+// candidate logic runs on lane 0 from the staged words. The block size is a template argument for
+// 8, 16 and 32 (0 = any other, the centre block then read from shared memory). The file is built
+// with -fmad=false so no multiply-add is fused.
 
 #include <cuda_runtime.h>
 
@@ -40,12 +45,22 @@ constexpr int kWarps = 4;
 constexpr int kMaxBlk = 32;
 constexpr int kListCap = 13;  // mod.rs:10-14 (TRUEMOTION_CANDIDATES)
 
+template <int BLK>
 struct WarpSlice {
-    float centre[kMaxBlk * kMaxBlk];
-    float row_sums[kListCap * kMaxBlk];
+    static constexpr int kB = BLK ? BLK : kMaxBlk;
+    float centre[BLK ? 1 : kB * kB];  // the generic block size's centre block
+    float diffs[32 * (kB + 1)];       // 32 rows of |centre - neighbour|, odd stride
+    float row_sums[kListCap * kB];
     float sads[kListCap];
     int list[2 * kListCap];
+    int staged[36];  // the 3x3 field, then the 3x3 seeds, (dx, dy) per block, 0 off the grid
     int count;
+};
+
+// The centre block's column that a lane owns, in registers for the templated block sizes.
+template <int BLK>
+struct CentreColumn {
+    float v[BLK ? BLK : 1];
 };
 
 __device__ __forceinline__ int clamp_to(int v, int limit) { return v < 0 ? 0 : (v >= limit ? limit - 1 : v); }
@@ -69,21 +84,43 @@ __device__ __forceinline__ float penalised_cost(float sad, int vx, int vy, int m
 }
 
 // Scores list entries [first, count) into `sads` with the whole warp.
-__device__ __forceinline__ void score(WarpSlice& w, int first, int count, const TruemotionLaunch& t,
-                                      const float* __restrict__ nbr, int ox, int oy, int lane) {
-    const int B = t.blksize;
-    const int rows = (count - first) * B;
-    for (int item = lane; item < rows; item += 32) {
-        const int e = first + item / B;
-        const int iy = item - (item / B) * B;
-        const int mvx = w.list[2 * e], mvy = w.list[2 * e + 1];
-        const float* row = nbr + static_cast<int64_t>(clamp_to(oy + iy + mvy, t.height)) * t.width;
-        const float* c = w.centre + iy * B;
-        float s = 0.0f;
-        for (int ix = 0; ix < B; ++ix) s += fabsf(c[ix] - __ldg(row + clamp_to(ox + ix + mvx, t.width)));
-        w.row_sums[item] = s;
+template <int BLK>
+__device__ __forceinline__ void score(WarpSlice<BLK>& w, const CentreColumn<BLK>& cc, int first, int count,
+                                      const TruemotionLaunch& t, const float* __restrict__ nbr, int ox, int oy,
+                                      int lane) {
+    const int B = BLK ? BLK : t.blksize;
+    const int stride = B + 1;
+    const int per = 32 / B;  // candidates per chunk of at most 32 rows
+    const int my_cand = lane / B, ix = lane - my_cand * B;
+    for (int c0 = first; c0 < count; c0 += per) {
+        const int nc = min(per, count - c0);
+        if (my_cand < nc) {
+            const int e = c0 + my_cand;
+            const int mvx = w.list[2 * e], mvy = w.list[2 * e + 1];
+            const float* column = nbr + clamp_to(ox + ix + mvx, t.width);
+            float* d = w.diffs + my_cand * B * stride + ix;
+            if (BLK) {
+#pragma unroll
+                for (int r = 0; r < (BLK ? BLK : 1); ++r) {
+                    const float nv = __ldg(column + static_cast<int64_t>(clamp_to(oy + r + mvy, t.height)) * t.width);
+                    d[r * stride] = fabsf(cc.v[r] - nv);
+                }
+            } else {
+                for (int r = 0; r < B; ++r) {
+                    const float nv = __ldg(column + static_cast<int64_t>(clamp_to(oy + r + mvy, t.height)) * t.width);
+                    d[r * stride] = fabsf(w.centre[r * B + ix] - nv);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane < nc * B) {
+            const float* d = w.diffs + lane * stride;
+            float s = 0.0f;
+            for (int ix = 0; ix < B; ++ix) s += d[ix];
+            w.row_sums[(c0 - first) * B + lane] = s;
+        }
+        __syncwarp();
     }
-    __syncwarp();
     for (int e = first + lane; e < count; e += 32) {
         float sad = 0.0f;
         for (int iy = 0; iy < B; ++iy) sad += w.row_sums[(e - first) * B + iy];
@@ -92,42 +129,65 @@ __device__ __forceinline__ void score(WarpSlice& w, int first, int count, const 
     __syncwarp();
 }
 
+template <int BLK>
 __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunch t) {
-    __shared__ WarpSlice slices[kWarps];
+    __shared__ WarpSlice<BLK> slices[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int blocks = t.blocks_x * t.blocks_y;
     const int blk = blockIdx.x * kWarps + warp;
     if (blk >= blocks) return;  // whole warps leave; only warp-level barriers follow
-    WarpSlice& w = slices[warp];
+    WarpSlice<BLK>& w = slices[warp];
     const int n = blockIdx.y;
     const int col = blk % t.blocks_x, row = blk / t.blocks_x;
     const int ox = col * t.step, oy = row * t.step;
-    const int B = t.blksize;
+    const int B = BLK ? BLK : t.blksize;
     const uint32_t nslot = t.neighbour_slots ? t.neighbour_slots[n] : t.inline_slots[n];
     const float* centre = t.pyramid + static_cast<int64_t>(t.centre_slot) * t.slot_pixels;
     const float* nbr = t.pyramid + static_cast<int64_t>(nslot) * t.slot_pixels;
     const int32_t* field = t.mv_in + static_cast<int64_t>(n) * t.mv_stride;
     const int32_t* seeds = t.seeds ? t.seeds + static_cast<int64_t>(n) * t.mv_stride : nullptr;
 
-    for (int p = lane; p < B * B; p += 32) {
-        const int py = p / B, px = p - (p / B) * B;
-        w.centre[p] = __ldg(centre + static_cast<int64_t>(clamp_to(oy + py, t.height)) * t.width +
-                            clamp_to(ox + px, t.width));
+    CentreColumn<BLK> cc;
+    if (BLK) {
+        const int cx = clamp_to(ox + lane % (BLK ? BLK : 1), t.width);
+#pragma unroll
+        for (int r = 0; r < (BLK ? BLK : 1); ++r)
+            cc.v[r] = __ldg(centre + static_cast<int64_t>(clamp_to(oy + r, t.height)) * t.width + cx);
+    } else {
+        for (int p = lane; p < B * B; p += 32) {
+            const int py = p / B, px = p - (p / B) * B;
+            w.centre[p] = __ldg(centre + static_cast<int64_t>(clamp_to(oy + py, t.height)) * t.width +
+                                clamp_to(ox + px, t.width));
+        }
     }
+    // candidates.rs:18-66 (`stage_neighbourhood`): the 3x3 field and seeds, one word per lane.
+    for (int word = lane; word < 36; word += 32) {
+        const bool reads_seeds = word >= 18;
+        const int fw = word % 18, pos = fw / 2, comp = fw % 2;
+        const int c = col + pos % 3 - 1, r = row + pos / 3 - 1;
+        int value = 0;
+        if (on_grid(c, r, t.blocks_x, t.blocks_y) && (!reads_seeds || seeds)) {
+            const int64_t i = 2 * (static_cast<int64_t>(r) * t.blocks_x + c) + comp;
+            value = reads_seeds ? __ldg(seeds + i) : __ldg(field + i);
+        }
+        w.staged[word] = value;
+    }
+    __syncwarp();
 
     // Lane 0: the median and the candidate list (candidates.rs:124-306).
     int own_x = 0, own_y = 0, med_x = 0, med_y = 0, median_entry = 0;
     if (lane == 0) {
-        own_x = field[2 * blk];
-        own_y = field[2 * blk + 1];
+        const int* sf = w.staged;
+        const int* ss = w.staged + 18;
+        own_x = sf[8];
+        own_y = sf[9];
         int xs[8], ys[8], cnt = 0;
         for (int pos = 0; pos < 9; ++pos) {
             if (pos == 4) continue;
             const int c = col + pos % 3 - 1, r = row + pos / 3 - 1;
             if (!on_grid(c, r, t.blocks_x, t.blocks_y)) continue;
-            const int i = r * t.blocks_x + c;
             // insertion into the sorted runs of each component
-            int vx = field[2 * i], vy = field[2 * i + 1];
+            int vx = sf[2 * pos], vy = sf[2 * pos + 1];
             int j = cnt;
             while (j > 0 && xs[j - 1] > vx) {
                 xs[j] = xs[j - 1];
@@ -151,18 +211,18 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
         for (int s = 0; s < 4; ++s) {
             const int c = col + sdx[s], r = row + sdy[s];
             if (on_grid(c, r, t.blocks_x, t.blocks_y)) {
-                const int i = r * t.blocks_x + c;
-                count = push_unique(w.list, count, field[2 * i], field[2 * i + 1]);
+                const int pos = 3 * (sdy[s] + 1) + sdx[s] + 1;
+                count = push_unique(w.list, count, sf[2 * pos], sf[2 * pos + 1]);
             }
         }
         count = push_unique(w.list, count, 0, 0);
         if (seeds) {
-            count = push_unique(w.list, count, seeds[2 * blk], seeds[2 * blk + 1]);
+            count = push_unique(w.list, count, ss[8], ss[9]);
             for (int corner = 0; corner < 4; ++corner) {
-                const int c = col + (corner % 2) * 2 - 1, r = row + (corner / 2) * 2 - 1;
-                if (on_grid(c, r, t.blocks_x, t.blocks_y)) {
-                    const int i = r * t.blocks_x + c;
-                    count = push_unique(w.list, count, seeds[2 * i], seeds[2 * i + 1]);
+                const int ddx = (corner % 2) * 2 - 1, ddy = (corner / 2) * 2 - 1;
+                if (on_grid(col + ddx, row + ddy, t.blocks_x, t.blocks_y)) {
+                    const int pos = 3 * (ddy + 1) + ddx + 1;
+                    count = push_unique(w.list, count, ss[2 * pos], ss[2 * pos + 1]);
                 }
             }
         }
@@ -173,7 +233,7 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
     __syncwarp();
     const int listed = w.count;
     const int head = listed < 2 ? listed : 2;
-    score(w, 0, head, t, nbr, ox, oy, lane);
+    score<BLK>(w, cc, 0, head, t, nbr, ox, oy, lane);
 
     // Lane 0 decides; the lanes follow its broadcast outcome through the remaining scoring.
     int outcome = 0;
@@ -214,7 +274,7 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
     }
     outcome = __shfl_sync(0xffffffffu, outcome, 0);
     if (outcome == 0) {
-        score(w, head, listed, t, nbr, ox, oy, lane);
+        score<BLK>(w, cc, head, listed, t, nbr, ox, oy, lane);
         if (lane == 0) {
             int bi = 0;
             for (int e = 1; e < listed; ++e) {
@@ -249,7 +309,7 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
     refines = __shfl_sync(0xffffffffu, refines, 0);
     if (refines) {
         const int ring = w.count;
-        score(w, 0, ring, t, nbr, ox, oy, lane);
+        score<BLK>(w, cc, 0, ring, t, nbr, ox, oy, lane);
         if (lane == 0) {
             for (int e = 0; e < ring; ++e) {
                 const int vx = w.list[2 * e], vy = w.list[2 * e + 1];
@@ -288,7 +348,10 @@ cudaError_t launch_truemotion(const TruemotionLaunch& t, cudaStream_t s) {
         return cudaErrorInvalidValue;
     const int blocks = t.blocks_x * t.blocks_y;
     dim3 grid((blocks + kWarps - 1) / kWarps, t.neighbours);
-    truemotion_kernel<<<grid, kWarps * 32, 0, s>>>(t);
+    if (t.blksize == 16) truemotion_kernel<16><<<grid, kWarps * 32, 0, s>>>(t);
+    else if (t.blksize == 8) truemotion_kernel<8><<<grid, kWarps * 32, 0, s>>>(t);
+    else if (t.blksize == 32) truemotion_kernel<32><<<grid, kWarps * 32, 0, s>>>(t);
+    else truemotion_kernel<0><<<grid, kWarps * 32, 0, s>>>(t);
     return cudaGetLastError();
 }
 

@@ -613,6 +613,58 @@ def run_prefilters(pushes: int) -> None:
                       "over_plain": {k: round(v / res["none"], 4) for k, v in res.items()}}))
 
 
+def run_motion_compensated(pushes: int) -> None:
+    """NLMeans with motion compensation on the headline luma pass: 1920x1080 u8 luma, d=2, a=5, s=2,
+    strength 8, default motion search (blksize 16, overlap 8, radius 4, 2 levels, Direct at d=2 with
+    the truemotion stage), plain and then NLMeans-HQ with a pinned sigma and temporal confidence.
+    Prints the steady-state device time per frame of each as one JSON line."""
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    avd = av_denoise_b200_loader.load()
+    from av_denoise_b200 import synth
+
+    clip = synth.temporal_1080p_clip(frames=8, seed=21)
+    fmt = avd.SampleFormat.u8()
+    stream = torch.cuda.current_stream()
+    bufs = []
+    for f in clip:
+        flat = f[0].reshape(-1)
+        bufs.append(torch.from_numpy(np.concatenate([flat, np.zeros((-flat.size) % 4, np.uint8)]).view(np.int32)).cuda())
+    out = torch.zeros_like(bufs[0])
+    t = avd.NlmTuning(search_radius=LUMA["a"], patch_radius=LUMA["s"], strength=LUMA["strength"])
+    mode = avd.DenoisingMode.temporal(LUMA["d"])
+    mc = avd.MotionCompensationMode(avd.MotionSearch())
+    cases = {
+        "plain": avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(tuning=t, mode=mode)),
+        "motion compensated": avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(motion_compensation=mc, tuning=t,
+                                                                           mode=mode)),
+        "HQ pinned sigma 8 codes, confidence, motion compensated": avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(
+            nlm=avd.NlmeansOptions(motion_compensation=mc, tuning=avd.NlmTuning(search_radius=LUMA["a"],
+                                                                               patch_radius=LUMA["s"]), mode=mode),
+            hq=avd.HqParams(sigma_override=8.0 / 255.0))),
+    }
+    res = {}
+    for name, alg in cases.items():
+        eng = avd.build_engine(avd.EngineSpec.nlmeans(alg, None, avd.Geometry(W, H, avd.ChromaLayout.GRAY, fmt, fmt)))
+        eng.set_stream(stream.cuda_stream)
+        times = []
+        for i in range(pushes):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if eng.push([avd.DevicePlane.from_tensor(bufs[i % len(bufs)], W, H)]):
+                eng.emit_into([avd.DevicePlane.from_tensor(out, W, H)])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        eng.close()
+        res[name] = round(float(np.median(times[2 * LUMA["d"] + 1:])), 4)
+    print(json.dumps({"workload": "NLMeans 1920x1080 u8 luma d=2 a=5 s=2 strength 8, motion compensation",
+                      "ms_per_frame": res}))
+
+
 def run_hq_auto(pushes: int, prefilter: str = "none") -> None:
     """NLMeans-HQ with the automatic noise estimate: 1920x1080 u8 luma, d=2, a=5, s=2, default HQ
     strength and temporal confidence, on the 1080p temporal clip. Each push reads one frame's noise
@@ -973,6 +1025,8 @@ def main() -> None:
                     help="time PUSHES pushes of NLMeans-HQ with the automatic noise estimate and exit")
     ap.add_argument("--prefilters", type=int, default=0, metavar="PUSHES",
                     help="time the headline luma pass with no prefilter, the bilateral and the NLM pilot")
+    ap.add_argument("--mc", type=int, default=0, metavar="PUSHES",
+                    help="time the headline luma pass with motion compensation (plain and HQ)")
     ap.add_argument("--prefilter", default="none", help="prefilter of --hq-auto (none, nlm[:scale], bilateral:ss,sr)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -997,6 +1051,8 @@ def main() -> None:
         run_hq_auto(args.hq_auto, args.prefilter)
     elif args.prefilters:
         run_prefilters(args.prefilters)
+    elif args.mc:
+        run_motion_compensated(args.mc)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -232,7 +232,7 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
                   noise_offset: float = 0.0, lut: np.ndarray | None = None, confidence: bool = False,
                   sad_floor: float = 0.0, thsad_scale: float = 1.0, blksize: int = 16, overlap: int = 8,
                   search_radius: int = 4, levels: int = 2, chained: bool = False, refine_radius: int = 2,
-                  prefilter=None, fp64: bool = False) -> list[np.ndarray]:
+                  prefilter=None, fp64: bool = False, derived=None) -> list[np.ndarray]:
     """NLMeans with motion compensation over a stream with repeat edges, replayed slot by slot as
     the ring runs it (nlmeans/denoiser/ring.rs, stages.rs:62-209, dispatch/motion.rs:104-487):
       - each slot write (and each edge copy) builds the slot's pyramids; with Chained estimation it
@@ -245,7 +245,9 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
         `confidence` (HQ temporal confidence) the search scores each block against `sad_floor`;
       - every neighbour (and its reference) is warped along its field, the temporal passes compare
         the warped frames, weighted by the confidence of their motion blocks.
-    `prefilter` is as in `prefilter_refs` (fixed strength). Returns one output per input."""
+    `prefilter` is as in `prefilter_refs` (fixed strength). With `derived`, a function of a window's
+    centre stream frame returning (h2, noise_offset, lut, sad_floor) (the automatic estimate's fold
+    around that frame), each window reads those instead. Returns one output per input."""
     n = len(frames)
     h, w, c = frames[0].shape
     tf = 2 * d + 1
@@ -299,16 +301,19 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
         phys = [(st["head"] % tf + l) % tf for l in range(tf)]
         cs = phys[d]
         slots = [phys[l] for l in range(tf) if l != d]
+        w_h2, w_off, w_lut, w_floor = h2, noise_offset, lut, sad_floor
+        if derived is not None:
+            w_h2, w_off, w_lut, w_floor = derived(slot_frame[cs])
         pyr = search_pyramid()
         if chained:
             seeds = chain_compose(pairs, d, d, st["head"] % (2 * d), step, w, h, bx, by)
             mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                    search_radius=refine_radius, levels=levels, confidence=confidence,
-                                   sad_floor=sad_floor, thsad=th, seeds=seeds)
+                                   sad_floor=w_floor, thsad=th, seeds=seeds)
         else:
             mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                    search_radius=search_radius, levels=levels, confidence=confidence,
-                                   sad_floor=sad_floor, thsad=th, field_lambda=1.0, reads_floor=True)
+                                   sad_floor=w_floor, thsad=th, field_lambda=1.0, reads_floor=True)
         window, refs = [], []
         idx = 0
         for l in range(tf):
@@ -321,7 +326,7 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
             refs.append(mc_warp(refs_of[f], mv[idx], step, bx, by) if refs_of is not None else None)
             idx += 1
         conf = [(cf[k], cf[2 * d - 1 - k]) for k in range(d)] if confidence else None
-        outs.append(nlm_frame(window, d, a, s, h2, noise_offset=noise_offset, lut=lut, conf=conf, conf_step=step,
+        outs.append(nlm_frame(window, d, a, s, w_h2, noise_offset=w_off, lut=w_lut, conf=conf, conf_step=step,
                               blocks=(bx, by), wref=wref, fp64=fp64,
                               refs=refs if refs_of is not None else None))
 

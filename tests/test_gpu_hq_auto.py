@@ -150,3 +150,46 @@ def test_hq_auto_with_the_pilot(oracle, w, h, n, d, a, s, scale, conf):
     for g, wn, ex in zip(got, want, exact):
         par.add(g[0], wn[0], ex[..., 0], fmt.max_value())
     print(par.check(min_raw=0.95))
+
+
+@pytest.mark.parametrize("w,h,n,d,est", [(112, 72, 11, 1, "auto"), (96, 64, 12, 3, "auto"),
+                                         (88, 56, 6, 2, "chained")])
+def test_hq_auto_with_motion_compensation(oracle, w, h, n, d, est):
+    """The look-ahead reads each frame along its motion to the frame before it (as NL4D's does);
+    each window's fold gives h2, the offsets and the window search's SAD floor, per unit sigma
+    sad_noise_floor(16, 1) (nlmeans/denoiser/noise.rs:226-229); the search scores confidence against
+    it and the temporal passes compare the warped neighbours."""
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, n, seed=700 + n + d, sigma=7.0)
+    estimation = avd.MotionEstimation.CHAINED if est == "chained" else avd.MotionEstimation.AUTO
+    ms = avd.MotionSearch(estimation=estimation)
+    mode = avd.DenoisingMode.temporal(d)
+    opts = avd.NlmeansOptions(motion_compensation=avd.MotionCompensationMode(ms),
+                              tuning=avd.NlmTuning(search_radius=3, patch_radius=2), mode=mode)
+    alg = avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(nlm=opts, hq=avd.HqParams(sigma_override=None)))
+    spec = avd.EngineSpec.nlmeans(alg, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    strength = avd.hq_default_strength(1, d)
+    f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
+    readings, totals = oracle.noise_readings_mc(f32, 1, w, h, blksize=16, overlap=8, search_radius=4, levels=2)
+    fl = np.float32
+    settings = oracle.fold_words(w, h, h2_per_inverse_variance=oracle.h2_inv_norm(float(fl(strength) * fl(255.0)), 2),
+                                 h2_fixed=oracle.h2_inv_norm(strength, 2),
+                                 offset_per_variance=float(((fl(2.0) * fl(3.0)) * fl(1.0)) * fl(25.0)),
+                                 sad_per_sigma=oracle.sad_noise_floor(16, 1.0))
+    folds = oracle.fold_stream(readings, totals, settings, 1, 3, d)
+
+    def derived(frame):
+        dv = folds[frame][1]
+        return float(dv[6]), float(dv[8]), folds[frame][2], float(dv[4])
+
+    chained = est == "chained" or d >= 3
+    kw = dict(confidence=True, chained=chained, derived=derived)
+    outs = oracle.nlm_stream_mc(f32, d, 3, 2, 0.0, **kw)
+    exact = oracle.nlm_stream_mc(f32, d, 3, 2, 0.0, fp64=True, **kw)
+    want = [oracle.egress(o, fmt.kind, fmt.max_value(), 0.0) for o in outs]
+    assert len(got) == len(want) == n
+    par = Parity()
+    for g, wn, ex in zip(got, want, exact):
+        par.add(g[0], wn[0], ex[..., 0], fmt.max_value())
+    print(par.check(min_raw=0.95), "sigma*255 at the middle:", folds[n // 2][1][0] * 255)
