@@ -1024,6 +1024,14 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
                                              &engine->chroma);
         if (f) return fail_global(f->status, f->message);
     }
+    if (nl4d && engine->luma && engine->chroma) {
+        // engine/spec.rs:350-365: the chroma pass refines the luma pass's motion, mapped through the
+        // chroma subsampling.
+        const int shift_x = g.chroma == AVD_CHROMA_YUV444 ? 0 : 1;
+        const int shift_y = g.chroma == AVD_CHROMA_YUV420 ? 1 : 0;
+        if (auto f = avd::link_nl4d_luma_motion(engine->luma.get(), engine->chroma.get(), shift_x, shift_y))
+            return fail_global(f->status, f->message);
+    }
     const bool gray = g.chroma == AVD_CHROMA_GRAY;
     const bool cleans_luma = engine->luma != nullptr;
     if (!gray && cleans_luma != (engine->chroma != nullptr)) {

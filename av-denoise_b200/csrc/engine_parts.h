@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <memory>
+#include <algorithm>
 #include <optional>
 #include <string>
 #include <utility>
@@ -171,5 +172,24 @@ class NoiseFront {
 std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels channels, uint32_t width,
                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
                                         std::unique_ptr<Pass>* result);
+
+// The luma pass's window motion mapped onto the chroma pass's block grid, shared by the two passes
+// of one engine (motion/luma_ring.rs, motion/chroma_map.rs): one slot of 2d chroma fields per
+// window, keyed by the window's centre stream frame. The chroma pass allocates it at link time with
+// its own block grid; the luma pass writes it after each window search and the chroma pass refines
+// the mapped vectors instead of searching its own.
+struct LumaMotionShare {
+    DeviceBuffer fields;
+    std::vector<int64_t> tags;  // the stream frame each slot holds, -1 for none
+    int slots = 0, neighbours = 0, blocks_x = 1, blocks_y = 1, step = 8, blksize = 16, mv_stride = 2;
+    int shift_x = 0, shift_y = 0;
+    int32_t* slot_ptr(int slot) const { return fields.as<int32_t>() + static_cast<int64_t>(slot) * neighbours * mv_stride; }
+    void clear() { std::fill(tags.begin(), tags.end(), -1); }
+};
+
+// Links an NL4D engine's luma and chroma passes: the chroma pass reads the luma pass's mapped
+// window motion (engine/spec.rs:350-365 `luma_motion_ring`, nlmeans/denoiser/seeds.rs:168-208).
+// `shift_x`/`shift_y` are the chroma subsampling as powers of two.
+std::optional<Failure> link_nl4d_luma_motion(Pass* luma, Pass* chroma, int shift_x, int shift_y);
 
 }  // namespace avd

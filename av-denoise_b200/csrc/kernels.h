@@ -165,6 +165,20 @@ struct WarpLaunch {
 };
 cudaError_t launch_warp(const WarpLaunch& args, cudaStream_t stream);
 
+// motion/kernels/chroma_map.rs (`mc_map_luma_fields`): `fields` luma motion fields mapped onto the
+// chroma block grid, each chroma block the per-component lower median of the luma blocks inside the
+// area it covers (clamped to the luma grid), divided by the subsampling and rounded half away from
+// zero.
+struct MapLaunch {
+    const int32_t* luma;
+    int32_t* chroma;
+    int fields;
+    int luma_bx, luma_by, luma_step, luma_blksize, luma_stride;
+    int chroma_bx, chroma_by, chroma_step, chroma_blksize, chroma_stride;
+    int shift_x, shift_y;
+};
+cudaError_t launch_map_luma_fields(const MapLaunch& args, cudaStream_t stream);
+
 // motion/kernels/chain.rs (`mc_chain_compose`): every neighbour's seed as the walk of pair vectors
 // from the centre. Neighbour n is logical position n (n < centre) or n + 1 of a 2d+1 window; the pair
 // between logical g and g+1 sits in pair slot (head_mod + g) mod 2d, direction 0 older-to-newer and

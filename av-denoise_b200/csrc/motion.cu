@@ -26,6 +26,7 @@
 // (SAD bits, candidate index) into one 64-bit key: non-negative floats order like their bit
 // patterns, so the minimum key is the lowest SAD with the lowest index, found with warp shuffles.
 
+#include <algorithm>
 #include <cstdint>
 
 #include "kernels.h"
@@ -654,6 +655,75 @@ cudaError_t launch_warp(const WarpLaunch& w, cudaStream_t s) {
         return cudaErrorInvalidValue;
     dim3 grid((w.width + 31) / 32, (w.height + 7) / 8, w.neighbours);
     warp_kernel<<<grid, dim3(32, 8), 0, s>>>(w);
+    return cudaGetLastError();
+}
+
+namespace {
+
+// chroma_map.rs:6-18 (`scale_down`): divided by 2^shift, rounding half away from zero.
+__device__ __forceinline__ int scale_down(int v, int shift) {
+    if (shift == 0) return v;
+    const int factor = 1 << shift, half = 1 << (shift - 1);
+    const int rounded = (abs(v) + half) / factor;
+    return v < 0 ? -rounded : rounded;
+}
+
+__global__ void __launch_bounds__(64) map_luma_fields_kernel(MapLaunch m, int covers_x, int covers_y) {
+    const int col = blockIdx.x * 8 + threadIdx.x;
+    const int row = blockIdx.y * 8 + threadIdx.y;
+    if (col >= m.chroma_bx || row >= m.chroma_by) return;
+    const int field = blockIdx.z;
+    const int origin_x = (col * m.chroma_step) << m.shift_x;
+    const int origin_y = (row * m.chroma_step) << m.shift_y;
+    const int start_col = origin_x / m.luma_step, start_row = origin_y / m.luma_step;
+    const int last_col = min(start_col + covers_x - 1, m.luma_bx - 1);
+    const int last_row = min(start_row + covers_y - 1, m.luma_by - 1);
+    const int first_col = min(start_col, last_col), first_row = min(start_row, last_row);
+    const int32_t* luma = m.luma + static_cast<int64_t>(field) * m.luma_stride;
+    const int n = covers_x * covers_y;
+    // chroma_map.rs:20-46 (`lower_median`): the live entry whose rank among the live entries holds
+    // the lower median, per component; entries past the grid repeat the last block but do not count.
+    auto value = [&](int i, int comp) {
+        const int c = first_col + i % covers_x, r = first_row + i / covers_x;
+        return luma[2 * (min(r, last_row) * m.luma_bx + min(c, last_col)) + comp];
+    };
+    auto live = [&](int i) { return first_col + i % covers_x <= last_col && first_row + i / covers_x <= last_row; };
+    int count = 0;
+    for (int i = 0; i < n; ++i) count += live(i) ? 1 : 0;
+    const int middle = (count - 1) / 2;
+    int out[2];
+    for (int comp = 0; comp < 2; ++comp) {
+        int median = value(0, comp);
+        for (int i = 0; i < n; ++i) {
+            const int vi = value(i, comp);
+            int below = 0, equal = 0;
+            for (int j = 0; j < n; ++j) {
+                if (!live(j)) continue;
+                const int vj = value(j, comp);
+                below += vj < vi ? 1 : 0;
+                equal += vj == vi ? 1 : 0;
+            }
+            if (live(i) && below <= middle && middle < below + equal) median = vi;
+        }
+        out[comp] = median;
+    }
+    int32_t* dst = m.chroma + static_cast<int64_t>(field) * m.chroma_stride + 2 * (row * m.chroma_bx + col);
+    dst[0] = scale_down(out[0], m.shift_x);
+    dst[1] = scale_down(out[1], m.shift_y);
+}
+
+}  // namespace
+
+cudaError_t launch_map_luma_fields(const MapLaunch& m, cudaStream_t s) {
+    if (!m.luma || !m.chroma || m.fields < 1 || m.luma_step < 1 || m.chroma_step < 1 || m.shift_x < 0 ||
+        m.shift_x > 1 || m.shift_y < 0 || m.shift_y > 1)
+        return cudaErrorInvalidValue;
+    // chroma_map.rs:65-68: the luma blocks along each axis of the area a chroma block covers.
+    const int area_x = m.chroma_blksize << m.shift_x, area_y = m.chroma_blksize << m.shift_y;
+    const int covers_x = std::max(area_x - m.luma_blksize, 0) / m.luma_step + 1;
+    const int covers_y = std::max(area_y - m.luma_blksize, 0) / m.luma_step + 1;
+    dim3 grid((m.chroma_bx + 7) / 8, (m.chroma_by + 7) / 8, m.fields);
+    map_luma_fields_kernel<<<grid, dim3(8, 8), 0, s>>>(m, covers_x, covers_y);
     return cudaGetLastError();
 }
 

@@ -342,11 +342,14 @@ class Nl4dPass final : public Pass {
     uint32_t phys(uint32_t logical) const { return static_cast<uint32_t>((ring_start() + logical) % tf()); }
     bool window_ready() const { return frames_loaded_ >= tf(); }
 
+    // A pass that refines the luma pass's motion matches on one level (seeds.rs:184-208).
+    int pyramid_levels() const { return reads_share_ ? 1 : static_cast<int>(opts_.motion.pyramid_levels); }
+
     std::optional<Failure> build_pyramid(size_t slot) {
         cudaError_t e = launch_pyramid_build(ring_.as<float>(), static_cast<int>(C()), static_cast<int>(width_),
                                              static_cast<int>(height_), static_cast<int>(tf()),
-                                             static_cast<int>(slot), static_cast<int>(opts_.motion.pyramid_levels),
-                                             pyramid_.as<float>(), static_cast<int>(slot), stream);
+                                             static_cast<int>(slot), pyramid_levels(), pyramid_.as<float>(),
+                                             static_cast<int>(slot), stream);
         if (e != cudaSuccess) return gpu_failure("pyramid launch", e);
         return std::nullopt;
     }
@@ -534,12 +537,102 @@ class Nl4dPass final : public Pass {
         return slot_tables_.as<uint32_t>() + (ring_start() * tf() + centre) * (2 * d_);
     }
 
-    // nlmeans/denoiser/machinery.rs:45-102 then dispatch/motion.rs:173-229.
+    // nlmeans/denoiser/machinery.rs:45-102 then dispatch/motion.rs:104-229.
     std::optional<Failure> machinery_at(uint32_t centre) {
         // machinery.rs:60-66: the look-ahead has read every frame the window reaches, so the fold
         // around the pass's centre frame runs first and the match scores confidence against it.
         if (measures_)
             if (auto f = noise_.fold(slot_frames_[phys(centre)], stream)) return f;
+        if (reads_share_) return refine_luma_motion(centre);
+        if (auto f = estimate_motion(centre)) return f;
+        return share_window_motion(centre);
+    }
+
+    // dispatch/motion.rs:231-253 (`share_window_motion`): the window's fields mapped onto the chroma
+    // block grid, into the shared slot of the centre's stream frame.
+    std::optional<Failure> share_window_motion(uint32_t centre) {
+        if (!writes_share_) return std::nullopt;
+        const uint32_t frame = slot_frames_[phys(centre)];
+        const int slot = static_cast<int>(frame % static_cast<uint32_t>(share_->slots));
+        MapLaunch mp{};
+        mp.luma = mv_.as<int32_t>();
+        mp.chroma = share_->slot_ptr(slot);
+        mp.fields = static_cast<int>(2 * d_);
+        mp.luma_bx = blocks_x_;
+        mp.luma_by = blocks_y_;
+        mp.luma_step = step_;
+        mp.luma_blksize = static_cast<int>(opts_.motion.blksize);
+        mp.luma_stride = mv_stride_;
+        mp.chroma_bx = share_->blocks_x;
+        mp.chroma_by = share_->blocks_y;
+        mp.chroma_step = share_->step;
+        mp.chroma_blksize = share_->blksize;
+        mp.chroma_stride = share_->mv_stride;
+        mp.shift_x = share_->shift_x;
+        mp.shift_y = share_->shift_y;
+        cudaError_t e = launch_map_luma_fields(mp, stream);
+        if (e != cudaSuccess) return gpu_failure("luma motion map launch", e);
+        share_->tags[slot] = frame;
+        return std::nullopt;
+    }
+
+    // dispatch/motion.rs:255-310 (`refine_luma_motion`): the luma pass's mapped vectors of the centre's
+    // stream frame, searched one pixel around on this plane at one level, with confidence.
+    std::optional<Failure> refine_luma_motion(uint32_t centre) {
+        const uint32_t frame = slot_frames_[phys(centre)];
+        const int slot = static_cast<int>(frame % static_cast<uint32_t>(share_->slots));
+        if (share_->tags[slot] != static_cast<int64_t>(frame)) {
+            char m[120];
+            std::snprintf(m, sizeof(m), "the luma pass has not shared the motion of stream frame %u", frame);
+            return Failure{AVD_ERR_GPU, m};
+        }
+        cudaError_t e = cudaMemcpyAsync(mv_.as<int32_t>(), share_->slot_ptr(slot),
+                                        2 * d_ * static_cast<size_t>(mv_stride_) * sizeof(int32_t),
+                                        cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return gpu_failure("mapped motion copy", e);
+        MotionLaunch m = search_launch();
+        m.neighbour_slots = slot_table(centre);
+        m.mv_field = mv_.as<int32_t>();
+        m.confidence = conf_.as<float>();
+        m.centre_slot = static_cast<int>(phys(centre));
+        m.neighbours = static_cast<int>(2 * d_);
+        m.search_radius = 1;  // dispatch/motion.rs:44 (MAPPED_REFINE_RADIUS)
+        m.coarse_radius = 1;
+        m.levels = 1;
+        m.seeded = 1;
+        if ((e = launch_motion_search(m, stream)) != cudaSuccess) return gpu_failure("mapped refine launch", e);
+        return std::nullopt;
+    }
+
+   public:
+    // engine/spec.rs:350-365 and nlmeans/denoiser/seeds.rs:168-208: the chroma pass reads the luma
+    // pass's motion, so it drops its own search (pair ring, truemotion, coarse level).
+    static std::optional<Failure> link(Nl4dPass& luma, Nl4dPass& chroma, int shift_x, int shift_y) {
+        if (luma.d_ != chroma.d_) return Failure{AVD_ERR_INVALID_OPTIONS, "the luma and chroma windows differ"};
+        auto share = std::make_shared<LumaMotionShare>();
+        share->slots = static_cast<int>(chroma.tf());
+        share->neighbours = static_cast<int>(2 * chroma.d_);
+        share->blocks_x = chroma.blocks_x_;
+        share->blocks_y = chroma.blocks_y_;
+        share->step = chroma.step_;
+        share->blksize = static_cast<int>(chroma.opts_.motion.blksize);
+        share->mv_stride = chroma.mv_stride_;
+        share->shift_x = shift_x;
+        share->shift_y = shift_y;
+        share->tags.assign(share->slots, -1);
+        cudaError_t e = share->fields.alloc(static_cast<size_t>(share->slots) * share->neighbours * share->mv_stride *
+                                            sizeof(int32_t));
+        if (e != cudaSuccess) return gpu_failure("luma motion share", e);
+        luma.share_ = share;
+        luma.writes_share_ = true;
+        chroma.share_ = share;
+        chroma.reads_share_ = true;
+        chroma.chained_ = false;
+        return std::nullopt;
+    }
+
+   private:
+    std::optional<Failure> estimate_motion(uint32_t centre) {
         if (chained_) {
             // nlmeans/dispatch/motion.rs:138-171 then analyse.rs:273-316: every neighbour's seed
             // chained from the pair ring, then refined `refine_radius` around it with confidence.
@@ -737,6 +830,7 @@ class Nl4dPass final : public Pass {
 
     // nl4d/engine.rs:166-171 with nl4d/denoiser.rs:598-610.
     void restart_stream() {
+        if (share_) share_->clear();
         ring_head_ = 0;
         frames_loaded_ = 0;
         real_pushes_ = 0;
@@ -761,6 +855,8 @@ class Nl4dPass final : public Pass {
     DeviceBuffer ring_, pyramid_, mv_, conf_, accum_, wsum_, group_weight_, members_, tables_, slot_tables_;
     DeviceBuffer pair_ring_;
     DeviceBuffer tm_seeds_, tm_field_;  // the truemotion stage's seeds and output field
+    std::shared_ptr<LumaMotionShare> share_;
+    bool writes_share_ = false, reads_share_ = false;
     bool chained_ = false;
     int refine_radius_ = 2;
     bool measures_ = false;
@@ -787,6 +883,13 @@ std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels 
                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
                                         std::unique_ptr<Pass>* result) {
     return Nl4dPass::create(options, channels, width, height, in, out, result);
+}
+
+std::optional<Failure> link_nl4d_luma_motion(Pass* luma, Pass* chroma, int shift_x, int shift_y) {
+    auto* l = dynamic_cast<Nl4dPass*>(luma);
+    auto* c = dynamic_cast<Nl4dPass*>(chroma);
+    if (!l || !c) return std::nullopt;
+    return Nl4dPass::link(*l, *c, shift_x, shift_y);
 }
 
 }  // namespace avd

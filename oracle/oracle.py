@@ -622,10 +622,67 @@ def chain_compose(pairs: dict, centre: int, d: int, head_mod: int, step: int, wi
     return seeds
 
 
+def map_luma_fields(luma_mv: np.ndarray, luma_grid: tuple[int, int, int, int], chroma_grid: tuple[int, int, int, int],
+                    shift_x: int, shift_y: int) -> np.ndarray:
+    """motion/kernels/chroma_map.rs (`mc_map_luma_fields`): every field of `luma_mv` (n, blocks, 2)
+    onto the chroma block grid; grids are (blocks_x, blocks_y, step, blksize). Each chroma block
+    takes the per-component lower median of the luma blocks inside the area it covers (clamped to
+    the luma grid), divided by the subsampling and rounded half away from zero."""
+    lbx, lby, lstep, lblk = luma_grid
+    cbx, cby, cstep, cblk = chroma_grid
+    covers_x = max((cblk << shift_x) - lblk, 0) // lstep + 1
+    covers_y = max((cblk << shift_y) - lblk, 0) // lstep + 1
+    n = luma_mv.shape[0]
+    lum = luma_mv.reshape(n, lby, lbx, 2)
+    out = np.zeros((n, cby * cbx, 2), np.int32)
+
+    def scale_down(v, shift):
+        if shift == 0:
+            return v
+        r = (abs(v) + (1 << (shift - 1))) // (1 << shift)
+        return -r if v < 0 else r
+
+    for row in range(cby):
+        for col in range(cbx):
+            ox, oy = (col * cstep) << shift_x, (row * cstep) << shift_y
+            sc, sr = ox // lstep, oy // lstep
+            lc, lr = min(sc + covers_x - 1, lbx - 1), min(sr + covers_y - 1, lby - 1)
+            fc, fr = min(sc, lc), min(sr, lr)
+            live = [(fr + i // covers_x, fc + i % covers_x) for i in range(covers_x * covers_y)
+                    if fc + i % covers_x <= lc and fr + i // covers_x <= lr]
+            for f in range(n):
+                vals = np.array([lum[f, r, c] for r, c in live], np.int64)
+                mx = int(np.sort(vals[:, 0])[(len(vals) - 1) // 2])
+                my = int(np.sort(vals[:, 1])[(len(vals) - 1) // 2])
+                out[f, row * cbx + col] = (scale_down(mx, shift_x), scale_down(my, shift_y))
+    return out
+
+
+class MotionShare:
+    """The luma pass's window fields shared with the chroma pass of one engine (motion/luma_ring.rs):
+    a luma stream writes each window's field, keyed by engine call and by the centre's stream frame
+    modulo the ring size (a later window of the same call overwrites the slot); a chroma stream of
+    the same calls reads the slot of its window's centre frame, mapped onto its own block grid."""
+
+    def __init__(self, luma_grid, chroma_grid, shift_x, shift_y):
+        self.luma_grid, self.chroma_grid = luma_grid, chroma_grid
+        self.shift_x, self.shift_y = shift_x, shift_y
+        self.calls: dict[int, dict[int, tuple[int, np.ndarray]]] = {}
+
+    def write(self, call: int, slot: int, frame: int, mv: np.ndarray):
+        self.calls.setdefault(call, {})[slot] = (frame, mv.copy())
+
+    def read(self, call: int, slot: int, frame: int) -> np.ndarray:
+        held = self.calls.get(call, {}).get(slot)
+        assert held is not None and held[0] == frame, "the luma pass has not shared this frame's motion"
+        return map_luma_fields(held[1], self.luma_grid, self.chroma_grid, self.shift_x, self.shift_y)
+
+
 def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, overlap=8, search_radius=4,
                 levels=2, refine=2, spatial_radius=9, lambda_ht=4.158, c_min=0.05, kaiser_beta=2.0,
                 pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0, chained: bool = False,
-                refine_radius: int = 2, noise=None, field_lambda: float = 1.0) -> list[np.ndarray]:
+                refine_radius: int = 2, noise=None, field_lambda: float = 1.0, share_writes: MotionShare | None = None,
+                share_reads: MotionShare | None = None) -> list[np.ndarray]:
     """The NL4D engine with a pinned sigma and Direct or Chained motion (no camera model) over a
     stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order. With
     `field_lambda` > 0 the truemotion stage ends the Direct window search (reading the window's SAD
@@ -639,7 +696,10 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     stream shorter than the ring, on every real frame after padding with the last frame). The
     first `context` frames are priming pushes (no head passes). With `noise`, a function of a pass's
     centre stream frame returning (sigma, weight_scale, sad_floor), each pass reads those (the
-    automatic estimate's fold around that frame) instead of the pinned sigma's."""
+    automatic estimate's fold around that frame) instead of the pinned sigma's. With `share_writes`
+    each window's field is shared for a chroma stream; with `share_reads` the window's motion is the
+    shared luma field of the centre frame, searched one pixel around at one level with confidence
+    (nlmeans/dispatch/motion.rs:231-310), and no motion of this plane's own is searched."""
     h, w, c = frames[0].shape
     tf = 2 * d + 1
     step = blksize - overlap
@@ -647,7 +707,9 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     ring = np.zeros((tf, h, w, c), np.float32)
     accum = np.zeros((tf, h * w * c), np.int64)
     wsum = np.zeros((tf, h * w), np.int64)
-    st = dict(head=0, loaded=0, real=0, passes=0, cont=context > 0)
+    st = dict(head=0, loaded=0, real=0, passes=0, cont=context > 0, call=0)
+    if share_reads is not None:
+        chained, levels = False, 1
     slot_frames = [0] * tf
     zeroed = [False] * tf
     sad_floor = sad_noise_floor(blksize, sigma)
@@ -675,7 +737,12 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         if noise is not None:
             p_sigma, p_weight, p_floor = noise(slot_frames[cs])
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
-        if chained:
+        if share_reads is not None:
+            mapped = share_reads.read(st["call"], slot_frames[cs] % tf, slot_frames[cs])
+            mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
+                                     search_radius=1, levels=1, confidence=True, sad_floor=p_floor, thsad=th,
+                                     seeds=mapped)
+        elif chained:
             seeds = chain_compose(pairs, centre, d, st["head"] % (2 * d), step, w, h, bx, by)
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=refine_radius, levels=levels, confidence=True,
@@ -684,6 +751,8 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=search_radius, levels=levels, confidence=True,
                                      sad_floor=p_floor, thsad=th, field_lambda=field_lambda, reads_floor=True)
+        if share_writes is not None:
+            share_writes.write(st["call"], slot_frames[cs] % tf, slot_frames[cs], mv)
         acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
                                   confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
                                   c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
@@ -726,6 +795,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
 
     outs = []
     for i, frame in enumerate(frames):
+        st["call"] = i
         push(frame)
         if i < context or st["loaded"] < tf:
             continue
@@ -737,6 +807,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         run_pass(d, clear)
         if st["passes"] > d:
             outs.append(read_region((phys(d) + tf - d) % tf))
+    st["call"] = len(frames)
     emit = min(st["real"], 2 * d)
     if emit == 0:
         return outs

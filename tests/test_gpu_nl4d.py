@@ -147,3 +147,30 @@ def test_nl4d_chained_matches_oracle(oracle, n, d, estimation, refine_radius, co
     got = Runner(spec).run(frames, context=context)
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, context=context, spatial_radius=4,
           chained=True, refine_radius=refine_radius)
+
+
+@pytest.mark.parametrize("layout,shifts,d,est", [("420", (1, 1), 1, avd.MotionEstimation.DIRECT),
+                                                 ("422", (1, 0), 2, avd.MotionEstimation.DIRECT),
+                                                 ("444", (0, 0), 3, avd.MotionEstimation.AUTO)])
+def test_nl4d_chroma_refines_the_luma_motion(oracle, layout, shifts, d, est):
+    """Luma and chroma in one engine: the chroma pass takes the luma pass's window fields mapped onto
+    its block grid (the lower median of the covered luma blocks, divided by the subsampling) and
+    searches one pixel around them at one level (engine/spec.rs:350-365,
+    nlmeans/dispatch/motion.rs:231-310); every sample of both planes matches the oracle."""
+    w, h, n, sigma = 96, 64, 6, 9.0 / 255
+    fmt = avd.SampleFormat.u8()
+    chroma_layout = {"420": avd.ChromaLayout.YUV420, "422": avd.ChromaLayout.YUV422,
+                     "444": avd.ChromaLayout.YUV444}[layout]
+    frames = clip(w, h, n, chroma=layout, seed=31 + d)
+    o = avd.Nl4dOptions(sigma=sigma, temporal_radius=d, spatial_radius=5, motion=avd.MotionSearch(estimation=est))
+    spec = avd.EngineSpec.nl4d(o, o, avd.Geometry(w, h, chroma_layout, fmt, fmt))
+    got = Runner(spec).run(frames)
+    cw, ch = w >> shifts[0], h >> shifts[1]
+    step = 8
+    share = oracle.MotionShare((-(-w // step), -(-h // step), step, 16), (-(-cw // step), -(-ch // step), step, 16),
+                               shifts[0], shifts[1])
+    chained = est == avd.MotionEstimation.AUTO and d >= 3
+    common = dict(spatial_radius=5, chained=chained)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, share_writes=share, **common)
+    check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, sigma, chroma=True,
+          share_reads=share, **common)

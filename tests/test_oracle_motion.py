@@ -140,3 +140,60 @@ def test_truemotion_values_follow_the_stage(oracle):
     base, noise, fade = oracle.truemotion_values(1.0, 16, oracle.thsad(16, 1.0))
     assert base == pytest.approx(256 * 0.02) and noise == 1.0 and fade == pytest.approx(2 * 256 * 0.02)
     assert oracle.truemotion_values(0.0, 16, 5.0)[:2] == (0.0, 0.0)
+
+
+# ---- luma motion mapped onto chroma (motion/kernels/chroma_map.rs), the reference's own cases -------
+# (motion/tests/chroma_map.rs: blksize 16, step 8 on both planes)
+
+def _grid(w, h):
+    return (-(-w // 8), -(-h // 8), 8, 16)
+
+
+def _field(grid, fn):
+    bx, by = grid[0], grid[1]
+    return np.array([[fn(c, r) for r in range(by) for c in range(bx)]], np.int32)
+
+
+def test_map_444_is_the_identity(oracle):
+    g = _grid(48, 40)
+    v = _field(g, lambda c, r: (c * 3 - 7, r * -5 + 2))
+    assert np.array_equal(oracle.map_luma_fields(v, g, g, 0, 0), v)
+
+
+def test_map_420_halves_both_axes_and_422_x_only(oracle):
+    lg = _grid(64, 64)
+    out = oracle.map_luma_fields(_field(lg, lambda c, r: (12, -20)), lg, _grid(32, 32), 1, 1)
+    assert np.all(out[0] == (6, -10))
+    cg = _grid(32, 64)
+    out = oracle.map_luma_fields(_field(lg, lambda c, r: (12, r * 10 - 30)), lg, cg, 1, 0)
+    for r in range(cg[1]):
+        for c in range(cg[0]):
+            assert tuple(out[0, r * cg[0] + c]) == (6, r * 10 - 30)
+
+
+def test_map_takes_the_footprint_median_per_component(oracle):
+    lg, cg = _grid(64, 64), _grid(32, 32)
+    fx = [[2, 4, 6], [8, 10, 12], [14, 16, 18]]
+    fy = [[-40, 4, 8], [-8, 100, 0], [12, -4, 6]]
+    v = _field(lg, lambda c, r: (fx[r][c], fy[r][c]) if c < 3 and r < 3 else (500, 500))
+    assert tuple(oracle.map_luma_fields(v, lg, cg, 1, 1)[0, 0]) == (5, 2)
+
+
+@pytest.mark.parametrize("vector,expected", [((1, -1), (1, -1)), ((3, -3), (2, -2)), ((5, -7), (3, -4)),
+                                             ((0, 2), (0, 1))])
+def test_map_rounds_odd_vectors_half_away_from_zero(oracle, vector, expected):
+    lg, cg = _grid(64, 64), _grid(32, 32)
+    out = oracle.map_luma_fields(_field(lg, lambda c, r: vector), lg, cg, 1, 1)
+    assert tuple(out[0, 1 * cg[0] + 1]) == expected
+
+
+def test_map_ragged_edges_take_in_bounds_vectors(oracle):
+    lg, cg = _grid(37, 35), _grid(19, 18)
+    assert lg[:2] == (5, 5) and cg[:2] == (3, 3)
+    out = oracle.map_luma_fields(_field(lg, lambda c, r: (c * 20, r * 40)), lg, cg, 1, 1)
+    assert tuple(out[0, 2 * 3 + 2]) == (40, 80)
+    assert tuple(out[0, 1 * 3 + 1]) == (30, 60)
+    lg, cg = _grid(29, 16), _grid(15, 8)
+    assert lg[:2] == (4, 2) and cg[:2] == (2, 1)
+    out = oracle.map_luma_fields(_field(lg, lambda c, r: (c * 20, r * 40)), lg, cg, 1, 1)
+    assert tuple(out[0, 1]) == (20, 0)
