@@ -121,6 +121,9 @@ class NlmPass final : public Pass {
     }
 
     void reset() override {
+        // Only a reset forgets the shared motion: a stream that ends on its own restarts the luma pass
+        // before the chroma pass has read the last window's motion.
+        if (share_) share_->clear();
         ready_slot_ = -1;
         emitted_.reset();
         tail_remaining_ = 0;
@@ -457,7 +460,8 @@ class NlmPass final : public Pass {
         // dispatch/motion.rs:75-79 (`search_thsad`).
         return avd_thsad(mc_blksize(), params_.hq ? params_.hq_params.thsad_scale : 1.0f);
     }
-    int mc_levels() const { return static_cast<int>(params_.motion.search.pyramid_levels); }
+    // A pass that refines the luma pass's motion matches on one level (seeds.rs:184-208).
+    int mc_levels() const { return reads_share_ ? 1 : static_cast<int>(params_.motion.search.pyramid_levels); }
     float* mc_search_pyramid() const { return has_reference() ? mc_ref_pyr_.as<float>() : mc_pyr_.as<float>(); }
 
     cudaError_t allocate_motion() {
@@ -612,7 +616,26 @@ class NlmPass final : public Pass {
         m.neighbours = n;
         m.mv_field = mc_mv_.as<int32_t>();
         m.confidence = mc_conf_ ? mc_conf_buf_.as<float>() : nullptr;
-        if (mc_chained_) {
+        const uint32_t frame = slot_frames_[centre];
+        const int share_slot = share_ ? static_cast<int>(frame % static_cast<uint32_t>(share_->slots)) : 0;
+        if (reads_share_) {
+            // dispatch/motion.rs:255-310 (`refine_luma_motion`): the luma pass's mapped vectors,
+            // searched one pixel around at one level, with confidence.
+            if (share_->tags[share_slot] != static_cast<int64_t>(frame)) {
+                char msg[120];
+                std::snprintf(msg, sizeof(msg), "the luma pass has not shared the motion of stream frame %u", frame);
+                return Failure{AVD_ERR_GPU, msg};
+            }
+            e = cudaMemcpyAsync(mc_mv_.as<int32_t>(), share_->slot_ptr(share_slot),
+                                static_cast<size_t>(n) * mc_mv_stride_ * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                stream);
+            if (e != cudaSuccess) return gpu_failure("mapped motion copy", e);
+            m.search_radius = 1;  // dispatch/motion.rs:44 (MAPPED_REFINE_RADIUS)
+            m.coarse_radius = 1;
+            m.levels = 1;
+            m.seeded = 1;
+            if ((e = launch_motion_search(m, stream)) != cudaSuccess) return gpu_failure("mapped refine launch", e);
+        } else if (mc_chained_) {
             e = launch_chain_compose(pair_ring_.as<int32_t>(), mc_mv_.as<int32_t>(), mc_mv_stride_, d, d,
                                      static_cast<int>(ring_head_ % (2 * d)), mc_mv_stride_, 2 * mc_mv_stride_,
                                      mc_step(), static_cast<int>(width_), static_cast<int>(height_), mc_bx_, mc_by_,
@@ -624,6 +647,27 @@ class NlmPass final : public Pass {
             if ((e = launch_motion_search(m, stream)) != cudaSuccess) return gpu_failure("seeded refine launch", e);
         } else {
             if (auto f = search_then_truemotion(m, true)) return f;
+        }
+        if (writes_share_) {
+            // dispatch/motion.rs:231-253 (`share_window_motion`).
+            MapLaunch mp{};
+            mp.luma = mc_mv_.as<int32_t>();
+            mp.chroma = share_->slot_ptr(share_slot);
+            mp.fields = n;
+            mp.luma_bx = mc_bx_;
+            mp.luma_by = mc_by_;
+            mp.luma_step = mc_step();
+            mp.luma_blksize = static_cast<int>(mc_blksize());
+            mp.luma_stride = mc_mv_stride_;
+            mp.chroma_bx = share_->blocks_x;
+            mp.chroma_by = share_->blocks_y;
+            mp.chroma_step = share_->step;
+            mp.chroma_blksize = share_->blksize;
+            mp.chroma_stride = share_->mv_stride;
+            mp.shift_x = share_->shift_x;
+            mp.shift_y = share_->shift_y;
+            if ((e = launch_map_luma_fields(mp, stream)) != cudaSuccess) return gpu_failure("luma motion map launch", e);
+            share_->tags[share_slot] = frame;
         }
         WarpLaunch w{};
         w.src_ring = ring_.as<float>();
@@ -644,6 +688,39 @@ class NlmPass final : public Pass {
         if ((e = launch_warp(w, stream)) != cudaSuccess) return gpu_failure("warp launch", e);
         return std::nullopt;
     }
+
+   public:
+    // engine/spec.rs:350-365 and nlmeans/denoiser/seeds.rs:168-208: with motion compensation on both
+    // passes, the chroma pass reads the luma pass's motion and drops its own search.
+    static std::optional<Failure> link(NlmPass& luma, NlmPass& chroma, int shift_x, int shift_y) {
+        if (!luma.mc_ || !chroma.mc_) return std::nullopt;
+        if (luma.params_.temporal_radius != chroma.params_.temporal_radius)
+            return Failure{AVD_ERR_INVALID_OPTIONS, "the luma and chroma windows differ"};
+        auto share = std::make_shared<LumaMotionShare>();
+        share->slots = static_cast<int>(chroma.total_frames());
+        share->neighbours = static_cast<int>(2 * chroma.params_.temporal_radius);
+        share->blocks_x = chroma.mc_bx_;
+        share->blocks_y = chroma.mc_by_;
+        share->step = chroma.mc_step();
+        share->blksize = static_cast<int>(chroma.mc_blksize());
+        share->mv_stride = chroma.mc_mv_stride_;
+        share->shift_x = shift_x;
+        share->shift_y = shift_y;
+        share->tags.assign(share->slots, -1);
+        cudaError_t e = share->fields.alloc(static_cast<size_t>(share->slots) * share->neighbours * share->mv_stride *
+                                            sizeof(int32_t));
+        if (e != cudaSuccess) return gpu_failure("luma motion share", e);
+        luma.share_ = share;
+        luma.writes_share_ = true;
+        chroma.share_ = share;
+        chroma.reads_share_ = true;
+        chroma.mc_chained_ = false;
+        return std::nullopt;
+    }
+
+   private:
+    std::shared_ptr<LumaMotionShare> share_;
+    bool writes_share_ = false, reads_share_ = false;
 
     // nlmeans/denoiser/stages.rs:110-130: the confidence pyramid follows every ring slot write.
     std::optional<Failure> slot_written(size_t slot) {
@@ -1024,13 +1101,15 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
                                              &engine->chroma);
         if (f) return fail_global(f->status, f->message);
     }
-    if (nl4d && engine->luma && engine->chroma) {
+    if (engine->luma && engine->chroma) {
         // engine/spec.rs:350-365: the chroma pass refines the luma pass's motion, mapped through the
         // chroma subsampling.
         const int shift_x = g.chroma == AVD_CHROMA_YUV444 ? 0 : 1;
         const int shift_y = g.chroma == AVD_CHROMA_YUV420 ? 1 : 0;
-        if (auto f = avd::link_nl4d_luma_motion(engine->luma.get(), engine->chroma.get(), shift_x, shift_y))
-            return fail_global(f->status, f->message);
+        auto f = nl4d ? avd::link_nl4d_luma_motion(engine->luma.get(), engine->chroma.get(), shift_x, shift_y)
+                      : avd::NlmPass::link(*static_cast<avd::NlmPass*>(engine->luma.get()),
+                                           *static_cast<avd::NlmPass*>(engine->chroma.get()), shift_x, shift_y);
+        if (f) return fail_global(f->status, f->message);
     }
     const bool gray = g.chroma == AVD_CHROMA_GRAY;
     const bool cleans_luma = engine->luma != nullptr;

@@ -165,6 +165,9 @@ class Nl4dPass final : public Pass {
     }
 
     void reset() override {
+        // Only a reset forgets the shared motion (a stream that ends on its own keeps it for the
+        // other pass's last reads).
+        if (share_) share_->clear();
         pending_.clear();
         emitted_.reset();
         poisoned_ = false;
@@ -830,7 +833,6 @@ class Nl4dPass final : public Pass {
 
     // nl4d/engine.rs:166-171 with nl4d/denoiser.rs:598-610.
     void restart_stream() {
-        if (share_) share_->clear();
         ring_head_ = 0;
         frames_loaded_ = 0;
         real_pushes_ = 0;

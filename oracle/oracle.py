@@ -232,7 +232,8 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
                   noise_offset: float = 0.0, lut: np.ndarray | None = None, confidence: bool = False,
                   sad_floor: float = 0.0, thsad_scale: float = 1.0, blksize: int = 16, overlap: int = 8,
                   search_radius: int = 4, levels: int = 2, chained: bool = False, refine_radius: int = 2,
-                  prefilter=None, fp64: bool = False, derived=None) -> list[np.ndarray]:
+                  prefilter=None, fp64: bool = False, derived=None, share_writes=None,
+                  share_reads=None) -> list[np.ndarray]:
     """NLMeans with motion compensation over a stream with repeat edges, replayed slot by slot as
     the ring runs it (nlmeans/denoiser/ring.rs, stages.rs:62-209, dispatch/motion.rs:104-487):
       - each slot write (and each edge copy) builds the slot's pyramids; with Chained estimation it
@@ -247,7 +248,9 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
         the warped frames, weighted by the confidence of their motion blocks.
     `prefilter` is as in `prefilter_refs` (fixed strength). With `derived`, a function of a window's
     centre stream frame returning (h2, noise_offset, lut, sad_floor) (the automatic estimate's fold
-    around that frame), each window reads those instead. Returns one output per input."""
+    around that frame), each window reads those instead. `share_writes` / `share_reads` (a
+    `MotionShare`) share each window's field with a chroma pass, or take the luma pass's mapped field
+    and search one pixel around it at one level, as in `nl4d_stream`. Returns one output per input."""
     n = len(frames)
     h, w, c = frames[0].shape
     tf = 2 * d + 1
@@ -258,7 +261,9 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
     slot_frame = [0] * tf
     zero = np.zeros((bx * by, 2), np.int32)
     pairs = {i: (zero, zero) for i in range(2 * d)}
-    st = dict(head=0, loaded=0)
+    st = dict(head=0, loaded=0, call=0)
+    if share_reads is not None:
+        chained, levels = False, 1
     outs = []
 
     def search_pyramid():
@@ -305,7 +310,11 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
         if derived is not None:
             w_h2, w_off, w_lut, w_floor = derived(slot_frame[cs])
         pyr = search_pyramid()
-        if chained:
+        if share_reads is not None:
+            mapped = share_reads.read(st["call"], slot_frame[cs] % tf, slot_frame[cs])
+            mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap, search_radius=1,
+                                   levels=1, confidence=confidence, sad_floor=w_floor, thsad=th, seeds=mapped)
+        elif chained:
             seeds = chain_compose(pairs, d, d, st["head"] % (2 * d), step, w, h, bx, by)
             mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                    search_radius=refine_radius, levels=levels, confidence=confidence,
@@ -314,6 +323,8 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
             mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                    search_radius=search_radius, levels=levels, confidence=confidence,
                                    sad_floor=w_floor, thsad=th, field_lambda=1.0, reads_floor=True)
+        if share_writes is not None:
+            share_writes.write(st["call"], slot_frame[cs] % tf, slot_frame[cs], mv)
         window, refs = [], []
         idx = 0
         for l in range(tf):
@@ -331,9 +342,11 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
                               refs=refs if refs_of is not None else None))
 
     for i in range(n):
+        st["call"] = i
         enter(i)
         denoise()
     while len(outs) < n:
+        st["call"] = n + len(outs)
         duplicate_last()
         st["loaded"] = min(st["loaded"] + 1, tf)
         denoise()

@@ -117,7 +117,7 @@ def hq_fixed_words(strength: float, sigma: float, s: int, channels: int, a: int)
 
 def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, wref=1.0, chroma=False,
                 out_fmt=None, exact=False, hq_sigma=None, hq_confidence=False, thsad_scale=1.0, prefilter=None,
-                motion=None):
+                motion=None, share_writes=None, share_reads=None):
     """The oracle's output planes for one plane group over a stream (repeat edges).
 
     `prefilter` is an `avd.PrefilterMode` (or None); `motion` an `avd.MotionSearch` for motion
@@ -152,7 +152,8 @@ def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, 
                                                                                                    sigma_y),
                                         thsad_scale=thsad_scale, blksize=motion.blksize, overlap=motion.overlap,
                                         search_radius=motion.search_radius, levels=motion.pyramid_levels,
-                                        chained=chained, refine_radius=refine, prefilter=pf, fp64=fp64)
+                                        chained=chained, refine_radius=refine, prefilter=pf, fp64=fp64,
+                                        share_writes=None if fp64 else share_writes, share_reads=share_reads)
     else:
         def run(fp64):
             return oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, fp64=fp64,

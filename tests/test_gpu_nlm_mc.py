@@ -118,3 +118,25 @@ def test_motion_compensation_rejects_escalation():
                                   avd.Geometry(64, 48, avd.ChromaLayout.GRAY, fmt, fmt))
     with pytest.raises(avd.InvalidOptions, match="escalation"):
         avd.build_engine(spec)
+
+
+@pytest.mark.parametrize("layout,shifts,d,est", [("420", (1, 1), 2, avd.MotionEstimation.DIRECT),
+                                                 ("422", (1, 0), 3, avd.MotionEstimation.AUTO)])
+def test_chroma_refines_the_luma_motion(oracle, layout, shifts, d, est):
+    """Motion compensation on both planes of one engine: the chroma pass takes the luma pass's
+    window fields mapped onto its block grid and searches one pixel around them at one level
+    (engine/spec.rs:350-365, nlmeans/dispatch/motion.rs:231-310)."""
+    w, h = 112, 64
+    fmt = avd.SampleFormat.u8()
+    chroma_layout = avd.ChromaLayout.YUV420 if layout == "420" else avd.ChromaLayout.YUV422
+    frames = clip(w, h, 5, chroma=layout, seed=990 + d)
+    ms = search(est)
+    luma = avd.NlmeansAlgorithm.fast(options(d, 3, 2, 8.0, ms))
+    chroma = avd.NlmeansAlgorithm.fast(options(d, 3, 2, 5.0, ms))
+    spec = avd.EngineSpec.nlmeans(luma, chroma, avd.Geometry(w, h, chroma_layout, fmt, fmt))
+    got = Runner(spec).run(frames)
+    cw, ch = w >> shifts[0], h >> shifts[1]
+    share = oracle.MotionShare((-(-w // 8), -(-h // 8), 8, 16), (-(-cw // 8), -(-ch // 8), 8, 16), *shifts)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, 8.0, ms, share_writes=share)
+    check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, 3, 2, 5.0, ms, chroma=True,
+          min_raw=0.95, share_reads=share)
