@@ -967,6 +967,7 @@ struct AvdEngine {
     std::unique_ptr<avd::Pass> luma, chroma;
     std::unique_ptr<avd::PassthroughRing> passthrough;
     bool passthrough_luma = false;  // which group the ring holds
+    bool luma_guides = false;       // `luma` is a chroma-only engine's luma guide, which cleans nothing
     bool poisoned = false;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -1101,6 +1102,14 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
                                              &engine->chroma);
         if (f) return fail_global(f->status, f->message);
     }
+    if (nl4d && !engine->luma && engine->chroma) {
+        // engine/spec.rs:220-236 (`guide_pass`): a chroma-only run searches luma motion with the
+        // chroma pass's settings at the luma plane's size, for its chroma pass to read.
+        auto f = avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Luma, g.width, g.height, g.input, g.output,
+                                       &engine->luma, true);
+        if (f) return fail_global(f->status, f->message);
+        engine->luma_guides = true;
+    }
     if (engine->luma && engine->chroma) {
         // engine/spec.rs:350-365: the chroma pass refines the luma pass's motion, mapped through the
         // chroma subsampling.
@@ -1112,7 +1121,7 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
         if (f) return fail_global(f->status, f->message);
     }
     const bool gray = g.chroma == AVD_CHROMA_GRAY;
-    const bool cleans_luma = engine->luma != nullptr;
+    const bool cleans_luma = engine->luma != nullptr && !engine->luma_guides;
     if (!gray && cleans_luma != (engine->chroma != nullptr)) {
         // planar.rs:210-220: one slot more than the cleaned pass holds frames.
         engine->passthrough = std::make_unique<avd::PassthroughRing>();

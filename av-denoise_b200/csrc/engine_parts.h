@@ -169,9 +169,11 @@ class NoiseFront {
 };
 
 // NL4D pass over one plane group (nl4d_pass.cpp).
+// With `guides_only` the pass is a chroma-only engine's luma guide: it runs the motion machinery on
+// the luma plane for the chroma pass to read, and no filter (engine/spec.rs:220-236).
 std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels channels, uint32_t width,
                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                        std::unique_ptr<Pass>* result);
+                                        std::unique_ptr<Pass>* result, bool guides_only = false);
 
 // The luma pass's window motion mapped onto the chroma pass's block grid, shared by the two passes
 // of one engine (motion/luma_ring.rs, motion/chroma_map.rs): one slot of 2d chroma fields per

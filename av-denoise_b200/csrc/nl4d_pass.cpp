@@ -46,7 +46,7 @@ class Nl4dPass final : public Pass {
    public:
     static std::optional<Failure> create(const AvdNl4dOptions& o, Channels channels, uint32_t width,
                                          uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                         std::unique_ptr<Pass>* result) {
+                                         std::unique_ptr<Pass>* result, bool guides_only = false) {
         // nl4d/denoiser.rs:228-233: without a pinned sigma the front measures the noise; luma applies
         // the noise map and chroma the colour gains, neither of which is built.
         if (!o.has_sigma && channels == Channels::Chroma)
@@ -94,6 +94,7 @@ class Nl4dPass final : public Pass {
         p->chained_ = chained;
         p->refine_radius_ = static_cast<int>(refine_radius);
         p->measures_ = !o.has_sigma;
+        p->guides_ = guides_only;
         if (auto f = p->allocate()) return f;
         *result = std::move(p);
         return std::nullopt;
@@ -234,14 +235,20 @@ class Nl4dPass final : public Pass {
                 return gpu_failure("pair ring", e);
             if ((e = cudaMemset(pair_ring_.ptr, 0, pair_ring_.bytes)) != cudaSuccess) return gpu_failure("pair ring", e);
         }
-        if ((e = accum_.alloc(fe * t * sizeof(int32_t))) != cudaSuccess) return gpu_failure("accumulator ring", e);
-        if ((e = wsum_.alloc(pixels() * t * sizeof(int32_t))) != cudaSuccess) return gpu_failure("weight ring", e);
+        // nl4d/denoiser.rs:257-260: a guide never runs the filter, so its filter buffers are placeholders.
+        const size_t filter = guides_ ? 0 : 1;
+        if ((e = accum_.alloc(filter * fe * t * sizeof(int32_t))) != cudaSuccess)
+            return gpu_failure("accumulator ring", e);
+        if ((e = wsum_.alloc(filter * pixels() * t * sizeof(int32_t))) != cudaSuccess)
+            return gpu_failure("weight ring", e);
         const size_t refs = static_cast<size_t>((width_ - kPatch + 3) / 4 + 1) * ((height_ - kPatch + 3) / 4 + 1);
-        if ((e = group_weight_.alloc(refs * sizeof(float))) != cudaSuccess) return gpu_failure("group weights", e);
+        if ((e = group_weight_.alloc(filter * refs * sizeof(float))) != cudaSuccess)
+            return gpu_failure("group weights", e);
         const size_t member_words = collab_member_words(static_cast<int>(width_), static_cast<int>(height_));
-        if ((e = members_.alloc(member_words * sizeof(uint32_t))) != cudaSuccess) return gpu_failure("group members", e);
+        if ((e = members_.alloc(filter * member_words * sizeof(uint32_t))) != cudaSuccess)
+            return gpu_failure("group members", e);
         for (auto& o : outputs_)
-            if ((e = o.alloc(fe * sizeof(float))) != cudaSuccess) return gpu_failure("output slot", e);
+            if ((e = o.alloc(filter * fe * sizeof(float))) != cudaSuccess) return gpu_failure("output slot", e);
 
         // Fixed tables: derived words, the (unused) noise curve, the white-noise DCT profile
         // (nl4d/denoiser.rs:273-277) and the Kaiser taps.
@@ -687,6 +694,11 @@ class Nl4dPass final : public Pass {
 
     // nl4d/collab_pass.rs:45-130 and 131-190.
     std::optional<Failure> run_pass(uint32_t centre, Clear clear) {
+        if (guides_) {
+            // nl4d/collab_pass.rs:50-55: a guide's pass runs only the front's machinery.
+            passes_run_ += 1;
+            return std::nullopt;
+        }
         const uint32_t centre_slot = phys(centre);
         uint32_t c0 = 0, c1 = 0;
         if (clear == Clear::WholeRing) {
@@ -814,6 +826,10 @@ class Nl4dPass final : public Pass {
     std::optional<Failure> normalise_region(uint32_t slot, int* out_slot) {
         *out_slot = next_output_slot_;
         next_output_slot_ = (next_output_slot_ + 1) % 2;
+        if (guides_) {
+            zeroed_[slot] = true;
+            return std::nullopt;
+        }
         cudaError_t e = launch_collab_normalise(accum_.as<int32_t>() + slot * frame_elems(),
                                                 wsum_.as<int32_t>() + slot * pixels(), outputs_[*out_slot].as<float>(),
                                                 static_cast<int64_t>(pixels()), static_cast<int>(C()), stream);
@@ -823,6 +839,7 @@ class Nl4dPass final : public Pass {
     }
 
     std::optional<Failure> write_out(int slot, const AvdPlane* planes) {
+        if (guides_) return std::nullopt;  // nl4d/engine.rs:318-321: a guide writes nothing
         void* p0 = reinterpret_cast<void*>(planes[0].ptr);
         void* p1 = C() > 1 ? reinterpret_cast<void*>(planes[1].ptr) : nullptr;
         cudaError_t e = launch_egress(outputs_[slot].as<float>(), p0, p1, static_cast<int64_t>(pixels()),
@@ -859,6 +876,7 @@ class Nl4dPass final : public Pass {
     DeviceBuffer tm_seeds_, tm_field_;  // the truemotion stage's seeds and output field
     std::shared_ptr<LumaMotionShare> share_;
     bool writes_share_ = false, reads_share_ = false;
+    bool guides_ = false;  // a chroma-only engine's luma pass: motion only (engine/spec.rs:220-236)
     bool chained_ = false;
     int refine_radius_ = 2;
     bool measures_ = false;
@@ -883,8 +901,8 @@ class Nl4dPass final : public Pass {
 
 std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels channels, uint32_t width,
                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                        std::unique_ptr<Pass>* result) {
-    return Nl4dPass::create(options, channels, width, height, in, out, result);
+                                        std::unique_ptr<Pass>* result, bool guides_only) {
+    return Nl4dPass::create(options, channels, width, height, in, out, result, guides_only);
 }
 
 std::optional<Failure> link_nl4d_luma_motion(Pass* luma, Pass* chroma, int shift_x, int shift_y) {

@@ -74,17 +74,24 @@ def test_nl4d_plain_threshold_10bit(oracle):
           pooled_threshold=False, lambda_ht=2.7, kaiser_beta=0.0, c_min=0.2)
 
 
-def test_nl4d_chroma_with_luma_passthrough(oracle):
-    w, h, d, sigma = 96, 64, 1, 8.0 / 255
+@pytest.mark.parametrize("d,est", [(1, avd.MotionEstimation.DIRECT), (3, avd.MotionEstimation.AUTO)])
+def test_nl4d_chroma_with_luma_passthrough(oracle, d, est):
+    """A chroma-only engine: luma passes through word for word, and a luma guide pass with the
+    chroma pass's settings searches the motion the chroma pass refines (engine/spec.rs:220-236)."""
+    w, h, sigma = 96, 64, 8.0 / 255
     fmt = avd.SampleFormat.u8()
-    frames = clip(w, h, 5, chroma="420", seed=9)
-    spec = avd.EngineSpec.nl4d(None, opts(d, sigma, spatial_radius=4),
-                               avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    frames = clip(w, h, 5, chroma="420", seed=9 + d)
+    o = avd.Nl4dOptions(sigma=sigma, temporal_radius=d, spatial_radius=4, motion=avd.MotionSearch(estimation=est))
+    spec = avd.EngineSpec.nl4d(None, o, avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
     got = Runner(spec).run(frames)
     for g, f in zip(got, frames):
         assert np.array_equal(g[0], f[0])
+    share = oracle.MotionShare((12, 8, 8, 16), (6, 4, 8, 16), 1, 1)
+    chained = d >= 3
+    f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
+    oracle.nl4d_stream(f32, d, sigma, spatial_radius=4, chained=chained, share_writes=share)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, sigma, chroma=True,
-          spatial_radius=4)
+          spatial_radius=4, chained=chained, share_reads=share)
 
 
 @pytest.mark.parametrize("n", [1, 2, 4])
