@@ -29,10 +29,13 @@ namespace {
 // NLMeans pass: nlmeans/engine.rs:29-318 over the ring of nlmeans/denoiser/mod.rs:40-591.
 class NlmPass final : public Pass {
    public:
+    // With `guides_only` the pass is a chroma-only engine's luma guide: it runs the noise estimate
+    // and the window motion for the chroma pass to read, and no denoise (nlmeans/engine.rs:53-100).
     static std::optional<Failure> create(const AvdNlmeansAlgorithm& alg, Channels channels, uint32_t width,
                                          uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                         std::unique_ptr<Pass>* result) {
+                                         std::unique_ptr<Pass>* result, bool guides_only = false) {
         auto pass = std::unique_ptr<NlmPass>(new NlmPass());
+        pass->guides_ = guides_only;
         pass->params_ = resolve_nlm_params(alg, channels);
         pass->held_ = nlm_held_frames(alg, channels);
         pass->width_ = width;
@@ -602,12 +605,15 @@ class NlmPass final : public Pass {
         const int d = static_cast<int>(params_.temporal_radius);
         const size_t centre = static_cast<size_t>(phys_frame(d));
         const size_t bytes = frame_elems() * sizeof(float);
-        cudaError_t e = cudaMemcpyAsync(comp_.as<float>() + centre * frame_elems(), slot_ptr(centre), bytes,
-                                        cudaMemcpyDeviceToDevice, stream);
-        if (e == cudaSuccess && has_reference())
-            e = cudaMemcpyAsync(comp_ref_.as<float>() + centre * frame_elems(), ref_slot_ptr(centre), bytes,
+        cudaError_t e = cudaSuccess;
+        if (!guides_) {
+            e = cudaMemcpyAsync(comp_.as<float>() + centre * frame_elems(), slot_ptr(centre), bytes,
                                 cudaMemcpyDeviceToDevice, stream);
-        if (e != cudaSuccess) return gpu_failure("centre copy", e);
+            if (e == cudaSuccess && has_reference())
+                e = cudaMemcpyAsync(comp_ref_.as<float>() + centre * frame_elems(), ref_slot_ptr(centre), bytes,
+                                    cudaMemcpyDeviceToDevice, stream);
+            if (e != cudaSuccess) return gpu_failure("centre copy", e);
+        }
         MotionLaunch m = mc_launch();
         int n = 0;
         for (int l = 0; l <= 2 * d; ++l)
@@ -669,6 +675,8 @@ class NlmPass final : public Pass {
             if ((e = launch_map_luma_fields(mp, stream)) != cudaSuccess) return gpu_failure("luma motion map launch", e);
             share_->tags[share_slot] = frame;
         }
+        // dispatch/mod.rs:648-651: a front that only guides stops after the window's motion.
+        if (guides_) return std::nullopt;
         WarpLaunch w{};
         w.src_ring = ring_.as<float>();
         w.dst_ring = comp_.as<float>();
@@ -721,6 +729,7 @@ class NlmPass final : public Pass {
    private:
     std::shared_ptr<LumaMotionShare> share_;
     bool writes_share_ = false, reads_share_ = false;
+    bool guides_ = false;
 
     // nlmeans/denoiser/stages.rs:110-130: the confidence pyramid follows every ring slot write.
     std::optional<Failure> slot_written(size_t slot) {
@@ -809,6 +818,12 @@ class NlmPass final : public Pass {
         a.offset_word = measures_ ? kDerivedNoiseOffset : 1;
         a.spatial_lut = measures_ ? noise_.spatial_table() : (params_.hq ? lut_.as<float>() : nullptr);
         a.conf = nullptr;
+        if (guides_) {
+            if (auto f = run_motion_compensation()) return f;
+            if (timed) timer_.end(stream, start);
+            *out_slot = slot;
+            return std::nullopt;
+        }
         if (mc_) {
             if (auto f = run_motion_compensation()) return f;
             // dispatch/mod.rs:141-200: the temporal passes read the compensated rings, weighted by
@@ -866,6 +881,7 @@ class NlmPass final : public Pass {
     }
 
     std::optional<Failure> write_out(int slot, const AvdPlane* planes) {
+        if (guides_) return std::nullopt;  // a guide writes nothing
         void* p0 = reinterpret_cast<void*>(planes[0].ptr);
         void* p1 = params_.channel_count() > 1 ? reinterpret_cast<void*>(planes[1].ptr) : nullptr;
         cudaError_t e = launch_egress(outputs_[slot].as<float>(), p0, p1, static_cast<int64_t>(pixels()),
@@ -1102,13 +1118,19 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
                                              &engine->chroma);
         if (f) return fail_global(f->status, f->message);
     }
-    if (nl4d && !engine->luma && engine->chroma) {
-        // engine/spec.rs:220-236 (`guide_pass`): a chroma-only run searches luma motion with the
-        // chroma pass's settings at the luma plane's size, for its chroma pass to read.
-        auto f = avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Luma, g.width, g.height, g.input, g.output,
-                                       &engine->luma, true);
-        if (f) return fail_global(f->status, f->message);
-        engine->luma_guides = true;
+    if (!engine->luma && engine->chroma) {
+        // engine/spec.rs:220-236 (`guide_pass`): a chroma-only run whose chroma pass compensates
+        // motion searches luma motion with the chroma pass's settings at the luma plane's size.
+        const bool moves = nl4d || (spec->nlm_chroma.motion_compensation.active &&
+                                    avd::resolve_nlm_params(spec->nlm_chroma, avd::Channels::Chroma).temporal_radius > 0);
+        if (moves) {
+            auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Luma, g.width, g.height, g.input,
+                                                  g.output, &engine->luma, true)
+                          : avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Luma, g.width, g.height, g.input,
+                                                 g.output, &engine->luma, true);
+            if (f) return fail_global(f->status, f->message);
+            engine->luma_guides = true;
+        }
     }
     if (engine->luma && engine->chroma) {
         // engine/spec.rs:350-365: the chroma pass refines the luma pass's motion, mapped through the

@@ -99,7 +99,8 @@ def test_prefilter_with_motion_compensation(oracle, prefilter, est):
 
 
 def test_chroma_motion_compensated_10bit(oracle):
-    """A chroma pass matches lane 0 (U) and warps both interleaved lanes."""
+    """A chroma pass refines the luma guide's mapped vectors on lane 0 (U) and warps both
+    interleaved lanes."""
     w, h = 128, 72
     fmt = avd.SampleFormat.u16(10)
     frames = clip(w, h, 4, depth=10, chroma="420", seed=981)
@@ -107,8 +108,11 @@ def test_chroma_motion_compensated_10bit(oracle):
     spec = avd.EngineSpec.nlmeans(None, avd.NlmeansAlgorithm.fast(options(1, 3, 2, 5.0, ms)),
                                   avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
     got = Runner(spec).run(frames)
+    share = oracle.MotionShare((16, 9, 8, 16), (8, 5, 8, 16), 1, 1)
+    f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
+    oracle.nlm_stream_mc(f32, 1, 3, 2, oracle.h2_inv_norm(5.0, 2), share_writes=share)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, 1, 3, 2, 5.0, ms, chroma=True,
-          min_raw=0.95)
+          min_raw=0.95, share_reads=share)
 
 
 def test_motion_compensation_rejects_escalation():
@@ -138,5 +142,27 @@ def test_chroma_refines_the_luma_motion(oracle, layout, shifts, d, est):
     cw, ch = w >> shifts[0], h >> shifts[1]
     share = oracle.MotionShare((-(-w // 8), -(-h // 8), 8, 16), (-(-cw // 8), -(-ch // 8), 8, 16), *shifts)
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, 8.0, ms, share_writes=share)
+    check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, 3, 2, 5.0, ms, chroma=True,
+          min_raw=0.95, share_reads=share)
+
+
+def test_chroma_only_engine_follows_a_luma_guide(oracle):
+    """A chroma-only engine with motion compensation: luma passes through, and a luma guide pass
+    with the chroma pass's settings searches the motion the chroma pass refines
+    (engine/spec.rs:220-236)."""
+    import numpy as np
+
+    w, h, d = 112, 64, 2
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 5, chroma="420", seed=995)
+    ms = search(avd.MotionEstimation.DIRECT)
+    chroma = avd.NlmeansAlgorithm.fast(options(d, 3, 2, 5.0, ms))
+    spec = avd.EngineSpec.nlmeans(None, chroma, avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    for g, f in zip(got, frames):
+        assert np.array_equal(g[0], f[0])
+    share = oracle.MotionShare((-(-w // 8), -(-h // 8), 8, 16), (-(-(w // 2) // 8), -(-(h // 2) // 8), 8, 16), 1, 1)
+    f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
+    oracle.nlm_stream_mc(f32, d, 3, 2, oracle.h2_inv_norm(5.0, 2), share_writes=share)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, 3, 2, 5.0, ms, chroma=True,
           min_raw=0.95, share_reads=share)
