@@ -696,155 +696,6 @@ class HostDenoiser:
 
     @staticmethod
     def _frame(planes: Sequence[bytes]):
-        """Plane pointers without copies: bytes are passed in place, writable buffers by address."""
-        n = len(planes)
-        ptrs = (C.c_void_p * max(1, n))()
-        sizes = (_abi.u64 * max(1, n))()
-        keep = []
-        for i, p in enumerate(planes):
-            if isinstance(p, bytes):
-                ref = C.c_char_p(p)
-                ptrs[i] = C.cast(ref, C.c_void_p)
-                sizes[i] = len(p)
-            else:
-                mv = memoryview(p).cast("B")
-                ref = (C.c_char * len(mv)).from_buffer_copy(mv) if mv.readonly else (C.c_char * len(mv)).from_buffer(mv)
-                ptrs[i] = C.cast(ref, C.c_void_p)
-                sizes[i] = len(mv)
-            keep.append(ref)
-        return ptrs, sizes, n, keep
-
-    def push(self, planes: Sequence[DevicePlane]) -> int:
-        arr, n = _planes(planes)
-        ready = C.c_size_t(0)
-        self._check(self._lib.avd_engine_push(self._h, arr, n, C.byref(ready)))
-        return ready.value
-
-    def push_context(self, planes: Sequence[DevicePlane]) -> None:
-        arr, n = _planes(planes)
-        self._check(self._lib.avd_engine_push_context(self._h, arr, n))
-
-    def emit_into(self, planes: Sequence[DevicePlane]) -> None:
-        arr, n = _planes(planes)
-        self._check(self._lib.avd_engine_emit_into(self._h, arr, n))
-
-    def finish(self) -> int:
-        tail = C.c_size_t(0)
-        self._check(self._lib.avd_engine_finish(self._h, C.byref(tail)))
-        return tail.value
-
-    def reset(self) -> None:
-        self._check(self._lib.avd_engine_reset(self._h))
-
-    def window_span(self) -> WindowSpan:
-        out = _abi.AvdWindowSpan()
-        self._check(self._lib.avd_engine_window_span(self._h, C.byref(out)))
-        return WindowSpan(out.behind, out.ahead, "shifted" if out.edges else "repeat")
-
-    def max_held_frames(self) -> int:
-        out = C.c_size_t(0)
-        self._check(self._lib.avd_engine_max_held_frames(self._h, C.byref(out)))
-        return out.value
-
-    def timing(self) -> PassTimings:
-        out = _abi.AvdPassTimings()
-        self._check(self._lib.avd_engine_timing(self._h, C.byref(out)))
-        luma = EngineTiming(out.luma.device_time, out.luma.frames) if out.has_luma else None
-        chroma = EngineTiming(out.chroma.device_time, out.chroma.frames) if out.has_chroma else None
-        return PassTimings(luma, chroma)
-
-    def sample_device_time(self, every: int) -> None:
-        self._check(self._lib.avd_engine_sample_device_time(self._h, every))
-
-    def fail_for_test(self) -> None:
-        self._check(self._lib.avd_engine_fail_for_test(self._h))
-
-    def close(self) -> None:
-        if self._h:
-            self._lib.avd_engine_destroy(self._h)
-            self._h = None
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
-
-    def __enter__(self):
-        return self
-
-    def __exit__(self, *exc):
-        self.close()
-
-
-@dataclass
-class TuningConfig:
-    """tune/setup.rs (`TuningConfig`): kept for API parity."""
-
-    deterministic: bool = True
-
-
-def build_engine(spec: EngineSpec, tuning: Optional[TuningConfig] = None) -> Engine:
-    """tune/setup.rs:79-91 (`build_engine`): validates, then builds on the current CUDA device."""
-    lib = _abi.load()
-    t = _abi.AvdTuning(int((tuning or TuningConfig()).deterministic), 0)
-    h = C.c_void_p()
-    st = lib.avd_engine_create(C.byref(spec._c()), C.byref(t), C.byref(h))
-    if st:
-        msg = lib.avd_last_error()
-        _raise(st, msg.decode() if msg else "")
-    return Engine(h)
-
-
-# ---- host denoiser (av-denoise/src/host/mod.rs:111-420) ----------------------------------------
-
-MAX_PENDING = 2  # av-denoise/src/host/mod.rs:27-28
-
-
-@dataclass
-class PlanarTiming:
-    """av-denoise/src/host/timing.rs:20-36: host seconds blocked on readbacks and spent submitting,
-    frames emitted, and each denoised plane group's device seconds (None when not sampled or not
-    denoised)."""
-
-    blocked: float
-    submit: float
-    frames: int
-    luma: Optional[float]
-    chroma: Optional[float]
-
-
-class HostDenoiser:
-    """A stateful denoiser over frames held as wire bytes, one buffer per plane (Y, then U and V).
-
-    Mirrors `HostDenoiser` (av-denoise/src/host/mod.rs:111-420): `push` uploads a frame and starts
-    any frame it completes; `recv` blocks for the oldest frame in flight (None when nothing is in
-    flight); `flush` drains the frames in flight and the temporal tail into `sink`; `reset_stream`
-    drops the stream and clears any poison. Raises `QueueFull` once MAX_PENDING frames wait, and
-    `Poisoned` after a failure until `reset_stream`. Uploads and readbacks run natively in
-    libavd_b200 (pinned staging, a copy stream, two output sets).
-    """
-
-    def __init__(self, spec: EngineSpec, tuning: Optional[TuningConfig] = None):
-        self._lib = _abi.load()
-        t = _abi.AvdTuning(int((tuning or TuningConfig()).deterministic), 0)
-        h = C.c_void_p()
-        st = self._lib.avd_host_create(C.byref(spec._c()), C.byref(t), C.byref(h))
-        if st:
-            msg = self._lib.avd_host_last_error(None)
-            _raise(st, msg.decode() if msg else "")
-        self._h = h
-        self.spec = spec
-        n = spec.geometry.plane_count()
-        self.plane_lengths = [int(self._lib.avd_host_plane_bytes(h, i)) for i in range(n)]
-
-    def _check(self, status: int) -> None:
-        if status:
-            msg = self._lib.avd_host_last_error(self._h)
-            _raise(status, msg.decode() if msg else "")
-
-    @staticmethod
-    def _frame(planes: Sequence[bytes]):
         """Plane pointers without copies: bytes are passed in place, writable buffers by address;
         only a read-only buffer of another type is copied."""
         n = len(planes)
