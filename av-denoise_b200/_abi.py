@@ -162,7 +162,8 @@ class AvdMotionPass(C.Structure):
     _fields_ = [(n, u64) for n in ("pyramid", "neighbour_slots", "mv_field", "confidence", "noise")] + \
                [(n, u32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize", "overlap",
                                    "search_radius", "levels", "mv_stride", "conf_stride", "sad_floor_word")] + \
-               [("thsad", f32), ("seeded", u32), ("keep_seeds", u64)]
+               [("thsad", f32), ("seeded", u32), ("keep_seeds", u64), ("escalation", u64), ("ceiling", u32),
+                ("esc_reads_floor", u32)]
 
 
 class AvdTruemotionPass(C.Structure):
@@ -247,6 +248,7 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_motion_pyramid_build": (C.c_int, [u64, u32, u32, u32, u32, u32, u32, u64, u32, C.c_void_p]),
     "avd_motion_search": (C.c_int, [_P(AvdMotionPass), C.c_void_p]),
     "avd_truemotion_pass": (C.c_int, [_P(AvdTruemotionPass), C.c_void_p]),
+    "avd_escalation_state_floats": (u64, [u32, u32]),
     "avd_chain_compose": (C.c_int, [u64, u64, u32, u32, u32, u32, u32, u32, u32, u32, u32, C.c_void_p]),
     "avd_sad_noise_floor": (f32, [u32, f32]),
     "avd_thsad": (f32, [u32, f32]),

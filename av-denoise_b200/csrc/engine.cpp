@@ -49,10 +49,8 @@ class NlmPass final : public Pass {
         pass->mc_ = p.motion.active && p.temporal_radius > 0;
         if (pass->mc_) {
             const AvdMotionSearch& m = p.motion.search;
-            if (m.max_search_escalation > m.search_radius)
-                return Failure{AVD_ERR_INVALID_OPTIONS,
-                               "motion search escalation is not available in this build; set max_search_escalation "
-                               "to search_radius"};
+            // motion/context.rs:55-71: the schedule escalates to max_search_escalation.
+            pass->mc_ceiling_ = m.max_search_escalation > m.search_radius ? static_cast<int>(m.max_search_escalation) : 0;
             // motion/search.rs:133-139: Auto resolves to Chained { refine_radius: 2 } at d >= 3.
             pass->mc_chained_ = m.estimation == AVD_ESTIMATION_CHAINED ||
                                 (m.estimation == AVD_ESTIMATION_AUTO && p.temporal_radius >= kChainedRadiusThreshold);
@@ -486,6 +484,11 @@ class NlmPass final : public Pass {
         if ((e = mc_mv_.alloc(nbrs * mc_mv_stride_ * sizeof(int32_t))) != cudaSuccess) return e;
         if ((e = tm_seeds_.alloc(nbrs * mc_mv_stride_ * sizeof(int32_t))) != cudaSuccess) return e;
         if ((e = tm_field_.alloc(nbrs * mc_mv_stride_ * sizeof(int32_t))) != cudaSuccess) return e;
+        if (mc_ceiling_ && !reads_share_) {
+            const size_t state = escalation_state_floats(static_cast<int>(nbrs), mc_conf_stride_);
+            if ((e = esc_state_.alloc(state * sizeof(float))) != cudaSuccess) return e;
+            if ((e = tm_changes_.alloc(nbrs * mc_conf_stride_ * sizeof(uint32_t))) != cudaSuccess) return e;
+        }
         if (mc_conf_ && (e = mc_conf_buf_.alloc(nbrs * mc_conf_stride_ * sizeof(float))) != cudaSuccess) return e;
         if (mc_chained_) {
             // motion/context.rs:209-211: 2d pair slots of two directions each.
@@ -512,6 +515,12 @@ class NlmPass final : public Pass {
         m.conf_stride = mc_conf_stride_;
         m.sad_floor_word = measures_ ? kDerivedSadFloor : kFixedSadFloor;
         m.thsad = mc_thsad();
+        // analyse.rs:371-380: a search (and a seeded refine below the ceiling) escalates; the
+        // luma-mapped refine runs a fixed schedule.
+        if (mc_ceiling_ && !reads_share_) {
+            m.escalation = esc_state_.as<float>();
+            m.ceiling = mc_ceiling_;
+        }
         return m;
     }
 
@@ -558,6 +567,8 @@ class NlmPass final : public Pass {
     std::optional<Failure> search_then_truemotion(MotionLaunch m, bool reads_floor) {
         const bool coarse = m.levels > 1 && !m.seeded;
         if (coarse) m.keep_seeds = tm_seeds_.as<int32_t>();
+        // truemotion/params.rs:9-12, 79-90: two passes after a search that escalates.
+        const bool two_passes = m.escalation && m.ceiling > m.search_radius;
         cudaError_t e = launch_motion_search(m, stream);
         if (e != cudaSuccess) return gpu_failure("motion search launch", e);
         TruemotionLaunch t{};
@@ -590,6 +601,18 @@ class NlmPass final : public Pass {
         t.surcharge = 0.125f;
         t.fade_level = 2.0f * std::max(m.thsad, 0.0f);
         t.thsad = m.thsad;
+        if (two_passes) {
+            // truemotion/stage.rs:82-142: the second pass reads the first's field back into the
+            // search's and rescores only the blocks next to one the first changed.
+            t.changes_out = tm_changes_.as<uint32_t>();
+            if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
+            t.mv_in = tm_field_.as<int32_t>();
+            t.mv_out = m.mv_field;
+            t.changes_in = tm_changes_.as<uint32_t>();
+            t.changes_out = nullptr;
+            if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
+            return std::nullopt;
+        }
         if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
         e = cudaMemcpyAsync(m.mv_field, t.mv_out, static_cast<size_t>(m.neighbours) * mc_mv_stride_ * sizeof(int32_t),
                             cudaMemcpyDeviceToDevice, stream);
@@ -650,8 +673,11 @@ class NlmPass final : public Pass {
             m.search_radius = mc_refine_radius_;
             m.coarse_radius = mc_refine_radius_;
             m.seeded = 1;
+            // dispatch/motion.rs:197-201: the window's derived noise is the escalation floor.
+            m.esc_reads_floor = 1;
             if ((e = launch_motion_search(m, stream)) != cudaSuccess) return gpu_failure("seeded refine launch", e);
         } else {
+            m.esc_reads_floor = 1;
             if (auto f = search_then_truemotion(m, true)) return f;
         }
         if (writes_share_) {
@@ -906,7 +932,9 @@ class NlmPass final : public Pass {
 
     bool mc_ = false, mc_chained_ = false, mc_conf_ = false;
     int mc_refine_radius_ = 2, mc_bx_ = 1, mc_by_ = 1, mc_mv_stride_ = 2, mc_conf_stride_ = 1;
+    int mc_ceiling_ = 0;  // the escalation ceiling; 0 when the search does not escalate
     DeviceBuffer mc_pyr_, mc_ref_pyr_, comp_, comp_ref_, mc_mv_, tm_seeds_, tm_field_, mc_conf_buf_, pair_ring_;
+    DeviceBuffer esc_state_, tm_changes_;
     bool measures_ = false;
     NoiseFront noise_;
 

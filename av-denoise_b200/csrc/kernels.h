@@ -116,7 +116,15 @@ struct MotionLaunch {
     int seeded;  // 1: the field already holds every block's seed; no coarse pass
     int32_t* keep_seeds;  // non-null: the field after the coarse pass is copied here (the truemotion
                           // stage's seed candidates)
+    // Search escalation (motion/escalate.rs): with `escalation` (escalation_state_floats of scratch)
+    // and ceiling > search_radius, the blocks that fail the first pass search again `ceiling` around
+    // their first window's centre. The floor is the noise word when `esc_reads_floor` and positive,
+    // else measured from the first pass's SADs; `thsad` must be positive.
+    float* escalation;
+    int ceiling, esc_reads_floor;
 };
+
+size_t escalation_state_floats(int neighbours, int conf_stride);
 
 int64_t pyramid_slot_pixels(int width, int height, int level);
 void pyramid_level_dims(int width, int height, int level, int* w, int* h);
@@ -144,6 +152,11 @@ struct TruemotionLaunch {
     int width, height, centre_slot, neighbours, blksize, step, blocks_x, blocks_y, mv_stride, conf_stride;
     int sad_field, reads_floor, refine_radius;
     float lambda_base, lambda_noise, surcharge, fade_level, thsad;
+    // truemotion/kernels/truemotion/mod.rs:483-520: with `changes_in`, a block whose 3x3
+    // neighbourhood changed nothing last pass copies its own vector (its confidence stands);
+    // `changes_out` flags the blocks whose pick left their own vector (conf layout).
+    const uint32_t* changes_in;
+    uint32_t* changes_out;
 };
 cudaError_t launch_truemotion(const TruemotionLaunch& args, cudaStream_t stream);
 

@@ -457,6 +457,298 @@ cudaError_t launch_search(bool coarse, const SearchArgs& a, dim3 grid, cudaStrea
     return cudaGetLastError();
 }
 
+// ---- search escalation (motion/escalate.rs, motion/kernels/escalate.rs) --------------------------
+//
+// With a ceiling above the first radius, blocks that fail their first window search again around
+// the same centre at the ceiling. The state holds four sections of neighbours * conf_stride floats
+// (kept SAD, edge bar then failure flag, first window centre x and y) and the SAD floor after them.
+// Every stage reads only what the launch before it wrote, so the result does not depend on the
+// order blocks run in.
+
+constexpr float kEscalateBelowConfidence = 0.5f;  // escalate.rs:14-17
+constexpr int kNeighbourDisagreement = 4;         // escalate.rs:19-23
+constexpr float kEscalateSadMargin = 0.125f;      // escalate.rs:25-31
+constexpr unsigned kFloorSamples = 4096, kFloorThreads = 256, kFloorRankDivisor = 4;
+constexpr unsigned kFloorBinShift = 16, kInfinityBin = 0x7F80;
+constexpr float kExactMatchSad = 1.0e-6f, kFlatShare = 0.25f;
+enum { kStateSad = 0, kStateFlag = 1, kStateCentreX = 2, kStateCentreY = 3, kStateSections = 4 };
+
+struct EscalateArgs {
+    SearchLevel L;   // level 0
+    SearchLevel Lc;  // the coarse level, when `widen`
+    const uint32_t* neighbour_slots;
+    uint32_t slots[kMaxNeighbours];
+    int centre_slot, neighbours, use_seed, widen, scale;
+    int32_t* mv_field;
+    int mv_stride;
+    float* confidence;
+    int conf_stride;
+    const float* noise;
+    int sad_floor_word, reads_floor;
+    float thsad;
+    float* state;
+};
+
+__device__ __forceinline__ float match_confidence(float sad, float floor, float thsad) {
+    float excess = __fsub_rn(sad, floor);
+    if (excess < 0.0f) excess = 0.0f;
+    const float t2 = __fmul_rn(thsad, thsad);
+    const float e2 = __fmul_rn(excess, excess);
+    const float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
+    return c < 0.0f ? 0.0f : c;
+}
+
+template <int R>
+struct WindowScratch {
+    float centre_tile[kMaxBlk * kMaxBlk];
+    float window[(kMaxBlk + 2 * kMaxRadius) * (kMaxBlk + 2 * kMaxRadius)];
+    float sads[(2 * R + 1) * (2 * R + 1)];
+    unsigned long long warp_keys[((2 * R + 1) * (2 * R + 1) + 31) / 32];
+    int best_index;
+};
+
+// The winner of the window around (cdx, cdy), valid at thread 0; every thread must call it.
+template <int R>
+__device__ __forceinline__ void window_best(const SearchLevel& L, int64_t centre_base, int64_t nbr_base, int ox,
+                                            int oy, int cdx, int cdy, WindowScratch<R>& w, int* out_dx, int* out_dy,
+                                            float* out_sad) {
+    constexpr int kSide = 2 * R + 1;
+    score_window<R>(L, centre_base, nbr_base, ox, oy, cdx, cdy, w.centre_tile, w.window, w.sads);
+    window_argmin<R>(w.sads, w.warp_keys, &w.best_index);
+    if (threadIdx.x == 0) {
+        float best_sad = kNoSad;
+        int bdx = cdx, bdy = cdy;
+        if (w.best_index >= 0) {
+            best_sad = w.sads[w.best_index];
+            bdx = cdx + (w.best_index % kSide) - R;
+            bdy = cdy + (w.best_index / kSide) - R;
+        }
+        const float centre_sad = w.sads[R * kSide + R];
+        if (centre_sad <= best_sad) {
+            best_sad = centre_sad;
+            bdx = cdx;
+            bdy = cdy;
+        }
+        *out_dx = bdx;
+        *out_dy = bdy;
+        *out_sad = best_sad;
+    }
+}
+
+__device__ __forceinline__ uint32_t escalate_slot(const EscalateArgs& e, int n, int bx, int by) {
+    return static_cast<uint32_t>(n) * e.conf_stride + by * e.L.blocks_x + bx;
+}
+
+__device__ __forceinline__ int64_t escalate_section(const EscalateArgs& e) {
+    return static_cast<int64_t>(e.neighbours) * e.conf_stride;
+}
+
+// The first window's centre of every block: its seed, or no motion.
+__global__ void __launch_bounds__(128) record_centres_kernel(EscalateArgs e) {
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y, n = blockIdx.z;
+    if (bx >= e.L.blocks_x) return;
+    const int32_t* mv = e.mv_field + static_cast<int64_t>(n) * e.mv_stride + (by * e.L.blocks_x + bx) * 2;
+    const int64_t sec = escalate_section(e);
+    const uint32_t slot = escalate_slot(e, n, bx, by);
+    e.state[kStateCentreX * sec + slot] = e.use_seed ? static_cast<float>(mv[0]) : 0.0f;
+    e.state[kStateCentreY * sec + slot] = e.use_seed ? static_cast<float>(mv[1]) : 0.0f;
+}
+
+// block_match.rs:783-796 with escalate.rs:84-155: the first window again, for its kept SAD and,
+// when the winner sits on the window's outer ring, its edge bar (the lowest SAD off the ring).
+template <int R>
+__global__ void __launch_bounds__(320) track_kernel(EscalateArgs e) {
+    constexpr int kSide = 2 * R + 1;
+    __shared__ WindowScratch<R> w;
+    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
+    const int64_t sec = escalate_section(e);
+    const uint32_t slot = escalate_slot(e, n, bx, by);
+    const int cdx = static_cast<int>(e.state[kStateCentreX * sec + slot]);
+    const int cdy = static_cast<int>(e.state[kStateCentreY * sec + slot]);
+    const uint32_t nslot = e.neighbour_slots ? e.neighbour_slots[n] : e.slots[n];
+    const int64_t cb = static_cast<int64_t>(e.centre_slot) * e.L.slot_pixels;
+    const int64_t nb = static_cast<int64_t>(nslot) * e.L.slot_pixels;
+    int dx, dy;
+    float sad;
+    window_best<R>(e.L, cb, nb, bx * e.L.step, by * e.L.step, cdx, cdy, w, &dx, &dy, &sad);
+    if (threadIdx.x != 0) return;
+    float bar = 0.0f;
+    if (abs(dx - cdx) == R || abs(dy - cdy) == R) {
+        bar = kNoSad;
+        for (int y = 1; y < kSide - 1; ++y)
+            for (int x = 1; x < kSide - 1; ++x) bar = fminf(bar, w.sads[y * kSide + x]);
+    }
+    e.state[kStateSad * sec + slot] = sad;
+    e.state[kStateFlag * sec + slot] = bar;
+}
+
+__device__ unsigned count_keys(const unsigned* keys, unsigned lo, unsigned hi, unsigned* counter) {
+    if (threadIdx.x == 0) *counter = 0;
+    __syncthreads();
+    unsigned c = 0;
+    for (unsigned i = threadIdx.x; i < kFloorSamples; i += blockDim.x) {
+        const unsigned k = keys[i];
+        c += (k >= lo && k <= hi) ? 1u : 0u;
+    }
+    atomicAdd(counter, c);
+    __syncthreads();
+    const unsigned total = *counter;
+    __syncthreads();
+    return total;
+}
+
+// escalate.rs:259-297 (`ranked_bin`): the lowest bin at or above `lower` that one in `divisor` of
+// the keys from `lower` up fall at or below. Uniform across the CTA; at most 15 halvings.
+__device__ unsigned ranked_bin(const unsigned* keys, unsigned lower, unsigned divisor, unsigned* counter) {
+    const unsigned valid = count_keys(keys, lower, 0xFFFFFFFFu, counter);
+    unsigned low = lower, high = kInfinityBin;
+    while (low < high) {
+        const unsigned middle = low + (high - low) / 2;
+        if (divisor * count_keys(keys, lower, middle, counter) >= valid)
+            high = middle;
+        else
+            low = middle + 1;
+    }
+    return low;
+}
+
+// escalate.rs:168-257 (`mc_measure_floor`): one CTA.
+__global__ void __launch_bounds__(kFloorThreads) floor_kernel(EscalateArgs e) {
+    __shared__ unsigned keys[kFloorSamples];
+    __shared__ unsigned counter;
+    const int64_t sec = escalate_section(e);
+    float* floor_word = e.state + kStateSections * sec;
+    if (e.reads_floor) {
+        const float reading = e.noise[e.sad_floor_word];
+        if (reading > 0.0f) {
+            if (threadIdx.x == 0) *floor_word = reading;
+            return;  // uniform: every thread read the same word
+        }
+    }
+    const unsigned blocks = static_cast<unsigned>(e.L.blocks_x * e.L.blocks_y);
+    const unsigned total = static_cast<unsigned>(e.neighbours) * blocks;
+    const unsigned sample_step = (total + kFloorSamples - 1) / kFloorSamples;
+    const unsigned sample_count = (total + sample_step - 1) / sample_step;
+    for (unsigned s = threadIdx.x; s < kFloorSamples; s += blockDim.x) {
+        const unsigned flat = min(s, sample_count - 1) * sample_step;
+        const unsigned n = flat / blocks, b = flat % blocks;
+        const float kept = e.state[kStateSad * sec + static_cast<int64_t>(n) * e.conf_stride + b];
+        const bool counted = s < sample_count && kept > kExactMatchSad;
+        keys[s] = counted ? (__float_as_uint(kept) >> kFloorBinShift) : 0u;
+    }
+    __syncthreads();
+    const unsigned valid = count_keys(keys, 1u, 0xFFFFFFFFu, &counter);
+    const unsigned median_bin = ranked_bin(keys, 1u, 2u, &counter);
+    const float median = __uint_as_float(median_bin << kFloorBinShift);
+    const float flat_limit = __fmul_rn(median, kFlatShare);
+    const unsigned grainy = max(__float_as_uint(flat_limit) >> kFloorBinShift, 1u);
+    const unsigned floor_bin = ranked_bin(keys, grainy, kFloorRankDivisor, &counter);
+    if (threadIdx.x == 0) *floor_word = valid == 0 ? 0.0f : __uint_as_float(floor_bin << kFloorBinShift);
+}
+
+// escalate.rs:321-395 (`mc_flag_failures`): low confidence, an edge winner that beats its bar by
+// more than the margin, or a vector more than 4 pixels from every grid neighbour's.
+__global__ void __launch_bounds__(64) flag_kernel(EscalateArgs e) {
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y, n = blockIdx.z;
+    if (bx >= e.L.blocks_x) return;
+    const int64_t sec = escalate_section(e);
+    const uint32_t slot = escalate_slot(e, n, bx, by);
+    const float floor = e.state[kStateSections * sec];
+    const float kept = e.state[kStateSad * sec + slot];
+    const bool low = match_confidence(kept, floor, e.thsad) < kEscalateBelowConfidence;
+    const float margin = __fmul_rn(kEscalateSadMargin, floor);
+    const bool on_edge = __fadd_rn(kept, margin) < e.state[kStateFlag * sec + slot];
+    const int32_t* f = e.mv_field + static_cast<int64_t>(n) * e.mv_stride;
+    const int bxn = e.L.blocks_x, byn = e.L.blocks_y;
+    const int own = (by * bxn + bx) * 2;
+    int closest = INT_MAX;
+    auto gap = [&](int o) { closest = min(closest, max(abs(f[o] - f[own]), abs(f[o + 1] - f[own + 1]))); };
+    if (bx > 0) gap(own - 2);
+    if (bx + 1 < bxn) gap(own + 2);
+    if (by > 0) gap(own - 2 * bxn);
+    if (by + 1 < byn) gap(own + 2 * bxn);
+    if (closest == INT_MAX) closest = 0;
+    e.state[kStateFlag * sec + slot] = (low || on_edge || closest > kNeighbourDisagreement) ? 1.0f : 0.0f;
+}
+
+// escalate.rs:400-559 (`mc_escalate_search`), without the camera model's candidate.
+template <int C>
+__global__ void __launch_bounds__(320) escalate_kernel(EscalateArgs e) {
+    __shared__ WindowScratch<C> w;
+    __shared__ int coarse_vec[2];
+    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
+    const int64_t sec = escalate_section(e);
+    const uint32_t slot = escalate_slot(e, n, bx, by);
+    if (e.state[kStateFlag * sec + slot] == 0.0f) return;  // uniform across the CTA
+    const int cdx = static_cast<int>(e.state[kStateCentreX * sec + slot]);
+    const int cdy = static_cast<int>(e.state[kStateCentreY * sec + slot]);
+    const float margin = __fmul_rn(kEscalateSadMargin, e.state[kStateSections * sec]);
+    const uint32_t nslot = e.neighbour_slots ? e.neighbour_slots[n] : e.slots[n];
+    int dx, dy, kx = 0, ky = 0;
+    float sad;
+    if (e.widen) {
+        const int64_t cb = e.Lc.level_base + static_cast<int64_t>(e.centre_slot) * e.Lc.slot_pixels;
+        const int64_t nb = e.Lc.level_base + static_cast<int64_t>(nslot) * e.Lc.slot_pixels;
+        window_best<C>(e.Lc, cb, nb, bx * e.L.step / e.scale, by * e.L.step / e.scale, 0, 0, w, &kx, &ky, &sad);
+        if (threadIdx.x == 0) {
+            coarse_vec[0] = kx * e.scale;
+            coarse_vec[1] = ky * e.scale;
+        }
+        __syncthreads();
+        kx = coarse_vec[0];
+        ky = coarse_vec[1];
+    }
+    const int64_t cb = static_cast<int64_t>(e.centre_slot) * e.L.slot_pixels;
+    const int64_t nb = static_cast<int64_t>(nslot) * e.L.slot_pixels;
+    window_best<C>(e.L, cb, nb, bx * e.L.step, by * e.L.step, cdx, cdy, w, &dx, &dy, &sad);
+    if (e.widen && (kx != cdx || ky != cdy)) {  // uniform: every thread holds the same vectors
+        int dx2, dy2;
+        float sad2;
+        window_best<C>(e.L, cb, nb, bx * e.L.step, by * e.L.step, kx, ky, w, &dx2, &dy2, &sad2);
+        if (threadIdx.x == 0 && __fadd_rn(sad2, margin) < sad) {
+            dx = dx2;
+            dy = dy2;
+            sad = sad2;
+        }
+    }
+    if (threadIdx.x != 0) return;
+    if (__fadd_rn(sad, margin) < e.state[kStateSad * sec + slot]) {
+        int32_t* mv = e.mv_field + static_cast<int64_t>(n) * e.mv_stride + (by * e.L.blocks_x + bx) * 2;
+        mv[0] = dx;
+        mv[1] = dy;
+        e.state[kStateSad * sec + slot] = sad;
+        if (e.confidence) e.confidence[slot] = match_confidence(sad, e.noise[e.sad_floor_word], e.thsad);
+    }
+}
+
+template <template <int> class K, int R>
+cudaError_t launch_radius_kernel(int radius, const EscalateArgs& e, dim3 grid, cudaStream_t s) {
+    if (radius == R) {
+        constexpr int kCand = (2 * R + 1) * (2 * R + 1);
+        K<R>::launch(e, grid, ((kCand + 31) / 32) * 32, s);
+        return cudaGetLastError();
+    }
+    if constexpr (R < kMaxRadius) {
+        return launch_radius_kernel<K, R + 1>(radius, e, grid, s);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+}
+
+template <int R>
+struct TrackLaunch {
+    static void launch(const EscalateArgs& e, dim3 g, int threads, cudaStream_t s) {
+        track_kernel<R><<<g, threads, 0, s>>>(e);
+    }
+};
+
+template <int R>
+struct EscalateLaunch {
+    static void launch(const EscalateArgs& e, dim3 g, int threads, cudaStream_t s) {
+        escalate_kernel<R><<<g, threads, 0, s>>>(e);
+    }
+};
+
 cudaError_t dispatch_search(int radius, bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
     switch (radius) {
         case 0: return launch_search<0>(coarse, a, grid, s);
@@ -584,7 +876,51 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     a.thsad = m.thsad;
     if (a.L.blksize > kMaxBlk) return cudaErrorInvalidValue;
     dim3 grid(blocks_x, blocks_y, m.neighbours);
-    return dispatch_search(m.search_radius, false, a, grid, s);
+    const bool escalates = m.escalation && m.ceiling > m.search_radius;
+    if (!escalates) return dispatch_search(m.search_radius, false, a, grid, s);
+    if (m.ceiling > kMaxRadius || m.thsad <= 0.0f || !m.noise) return cudaErrorInvalidValue;
+    // analyse.rs:234-262 and escalate.rs:19-57: record the first windows' centres, run the first
+    // pass, then keep its SADs and edge bars, measure the floor, flag the failures and search them
+    // again at the ceiling (the coarse level too, when a coarse pass seeded the search).
+    EscalateArgs e{};
+    e.L = a.L;
+    e.neighbour_slots = m.neighbour_slots;
+    for (int i = 0; i < kMaxNeighbours; ++i) e.slots[i] = m.inline_slots[i];
+    e.centre_slot = m.centre_slot;
+    e.neighbours = m.neighbours;
+    e.use_seed = seeded ? 1 : 0;
+    e.widen = coarse ? 1 : 0;
+    e.scale = 1;
+    if (coarse) {
+        const int level = m.levels - 1;
+        e.scale = 1 << level;
+        pyramid_level_dims(m.width, m.height, level, &e.Lc.width, &e.Lc.height);
+        e.Lc.pyramid = m.pyramid;
+        e.Lc.level_base = pyramid_level_base(m.width, m.height, m.frame_count, level);
+        e.Lc.slot_pixels = pyramid_slot_pixels(m.width, m.height, level);
+        e.Lc.blksize = (m.blksize / e.scale > 2 ? m.blksize / e.scale : 2) * m.coarse_block_factor;
+        if (e.Lc.blksize > kMaxBlk) return cudaErrorInvalidValue;
+    }
+    e.mv_field = m.mv_field;
+    e.mv_stride = m.mv_stride;
+    e.confidence = m.confidence;
+    e.conf_stride = m.conf_stride;
+    e.noise = m.noise;
+    e.sad_floor_word = m.sad_floor_word;
+    e.reads_floor = m.esc_reads_floor;
+    e.thsad = m.thsad;
+    e.state = m.escalation;
+    const dim3 rows((blocks_x + 127) / 128, blocks_y, m.neighbours);
+    record_centres_kernel<<<rows, 128, 0, s>>>(e);
+    if (cudaError_t err = dispatch_search(m.search_radius, false, a, grid, s)) return err;
+    if (cudaError_t err = launch_radius_kernel<TrackLaunch, 0>(m.search_radius, e, grid, s)) return err;
+    floor_kernel<<<1, kFloorThreads, 0, s>>>(e);
+    flag_kernel<<<dim3((blocks_x + 63) / 64, blocks_y, m.neighbours), 64, 0, s>>>(e);
+    return launch_radius_kernel<EscalateLaunch, 0>(m.ceiling, e, grid, s);
+}
+
+size_t escalation_state_floats(int neighbours, int conf_stride) {
+    return static_cast<size_t>(kStateSections) * neighbours * conf_stride + 1;
 }
 
 namespace {

@@ -81,9 +81,22 @@ AvdStatus avd_motion_search(const AvdMotionPass* p, void* stream) {
     m.thsad = p->thsad;
     m.seeded = p->seeded ? 1 : 0;
     m.keep_seeds = reinterpret_cast<int32_t*>(p->keep_seeds);
+    if (p->escalation && p->ceiling > p->search_radius) {
+        if (p->ceiling > 8) return fail(AVD_ERR_INVALID_OPTIONS, "motion search: ceiling must be at most 8");
+        if (!p->noise || !(p->thsad > 0.0f) || p->conf_stride < bx * by)
+            return fail(AVD_ERR_INVALID_OPTIONS,
+                        "motion search: escalation needs the noise words, a positive thsad and conf_stride >= blocks");
+        m.escalation = reinterpret_cast<float*>(p->escalation);
+        m.ceiling = static_cast<int>(p->ceiling);
+        m.esc_reads_floor = p->esc_reads_floor ? 1 : 0;
+    }
     cudaError_t e = avd::launch_motion_search(m, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("motion search launch: ") + cudaGetErrorString(e));
     return AVD_OK;
+}
+
+uint64_t avd_escalation_state_floats(uint32_t neighbours, uint32_t conf_stride) {
+    return static_cast<uint64_t>(avd::escalation_state_floats(static_cast<int>(neighbours), static_cast<int>(conf_stride)));
 }
 
 AvdStatus avd_truemotion_pass(const AvdTruemotionPass* p, void* stream) {

@@ -58,10 +58,6 @@ class Nl4dPass final : public Pass {
                            "the NL4D luma noise map of the automatic noise estimate is not available in this build; "
                            "set noise_map to false or set sigma"};
         const AvdMotionSearch& m = o.motion;
-        if (m.max_search_escalation > m.search_radius)
-            return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "motion search escalation is not available in this build; set max_search_escalation "
-                           "to search_radius"};
         // motion/search.rs:133-139: Auto resolves to Chained { refine_radius: 2 } at d >= 3.
         const bool chained = m.estimation == AVD_ESTIMATION_CHAINED ||
                              (m.estimation == AVD_ESTIMATION_AUTO && o.temporal_radius >= kChainedRadiusThreshold);
@@ -93,6 +89,8 @@ class Nl4dPass final : public Pass {
         p->thsad_ = avd_thsad(m.blksize, o.thsad_scale);
         p->chained_ = chained;
         p->refine_radius_ = static_cast<int>(refine_radius);
+        // motion/context.rs:55-71: the schedule escalates to max_search_escalation.
+        p->ceiling_ = m.max_search_escalation > m.search_radius ? static_cast<int>(m.max_search_escalation) : 0;
         p->measures_ = !o.has_sigma;
         p->guides_ = guides_only;
         if (auto f = p->allocate()) return f;
@@ -222,6 +220,13 @@ class Nl4dPass final : public Pass {
         const size_t nbrs = 2 * d_;
         if ((e = mv_.alloc(nbrs * mv_stride_ * sizeof(int32_t))) != cudaSuccess) return gpu_failure("motion field", e);
         if ((e = conf_.alloc(nbrs * conf_stride_ * sizeof(float))) != cudaSuccess) return gpu_failure("confidence", e);
+        if (ceiling_) {
+            if ((e = esc_state_.alloc(escalation_state_floats(static_cast<int>(nbrs), conf_stride_) * sizeof(float))) !=
+                cudaSuccess)
+                return gpu_failure("escalation state", e);
+            if ((e = tm_changes_.alloc(nbrs * conf_stride_ * sizeof(uint32_t))) != cudaSuccess)
+                return gpu_failure("truemotion change flags", e);
+        }
         if (truemotion()) {
             // motion/truemotion/stage.rs:14-27: the search's seeds and the field between passes.
             if ((e = tm_seeds_.alloc(nbrs * mv_stride_ * sizeof(int32_t))) != cudaSuccess)
@@ -481,6 +486,8 @@ class Nl4dPass final : public Pass {
     std::optional<Failure> search_then_truemotion(MotionLaunch m, bool reads_floor) {
         const bool coarse = m.levels > 1 && !m.seeded;
         if (truemotion() && coarse) m.keep_seeds = tm_seeds_.as<int32_t>();
+        // truemotion/params.rs:9-12, 79-90: two passes after a search that escalates.
+        const bool two_passes = m.escalation && m.ceiling > m.search_radius;
         cudaError_t e = launch_motion_search(m, stream);
         if (e != cudaSuccess) return gpu_failure("motion search launch", e);
         if (!truemotion()) return std::nullopt;
@@ -514,6 +521,18 @@ class Nl4dPass final : public Pass {
         t.surcharge = 0.125f;
         t.fade_level = 2.0f * std::max(m.thsad, 0.0f);
         t.thsad = m.thsad;
+        if (two_passes) {
+            // truemotion/stage.rs:82-142: the second pass reads the first's field back into the
+            // search's and rescores only the blocks next to one the first changed.
+            t.changes_out = tm_changes_.as<uint32_t>();
+            if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
+            t.mv_in = tm_field_.as<int32_t>();
+            t.mv_out = m.mv_field;
+            t.changes_in = tm_changes_.as<uint32_t>();
+            t.changes_out = nullptr;
+            if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
+            return std::nullopt;
+        }
         if ((e = launch_truemotion(t, stream)) != cudaSuccess) return gpu_failure("truemotion launch", e);
         e = cudaMemcpyAsync(m.mv_field, t.mv_out, static_cast<size_t>(m.neighbours) * mv_stride_ * sizeof(int32_t),
                             cudaMemcpyDeviceToDevice, stream);
@@ -538,6 +557,10 @@ class Nl4dPass final : public Pass {
         m.conf_stride = conf_stride_;
         m.sad_floor_word = kSadFloorWord;
         m.thsad = thsad_;
+        if (ceiling_) {
+            m.escalation = esc_state_.as<float>();
+            m.ceiling = ceiling_;
+        }
         return m;
     }
 
@@ -610,6 +633,8 @@ class Nl4dPass final : public Pass {
         m.coarse_radius = 1;
         m.levels = 1;
         m.seeded = 1;
+        m.escalation = nullptr;  // motion/context.rs:95-112: the mapped refine runs a fixed schedule
+        m.ceiling = 0;
         if ((e = launch_motion_search(m, stream)) != cudaSuccess) return gpu_failure("mapped refine launch", e);
         return std::nullopt;
     }
@@ -661,6 +686,7 @@ class Nl4dPass final : public Pass {
             m.search_radius = refine_radius_;
             m.coarse_radius = refine_radius_;
             m.seeded = 1;
+            m.esc_reads_floor = 1;  // the window's floor, as the window search reads it
             e = launch_motion_search(m, stream);
             if (e != cudaSuccess) return gpu_failure("seeded refine launch", e);
             return std::nullopt;
@@ -686,6 +712,12 @@ class Nl4dPass final : public Pass {
         m.conf_stride = conf_stride_;
         m.sad_floor_word = kSadFloorWord;
         m.thsad = thsad_;
+        if (ceiling_) {
+            // nlmeans/dispatch/motion.rs:197-201: the window's derived noise is the escalation floor.
+            m.escalation = esc_state_.as<float>();
+            m.ceiling = ceiling_;
+            m.esc_reads_floor = 1;
+        }
         // nlmeans/dispatch/motion.rs:201-206: the window's floor scales the stage's penalty.
         return search_then_truemotion(m, true);
     }
@@ -879,6 +911,8 @@ class Nl4dPass final : public Pass {
     bool guides_ = false;  // a chroma-only engine's luma pass: motion only (engine/spec.rs:220-236)
     bool chained_ = false;
     int refine_radius_ = 2;
+    int ceiling_ = 0;                   // the escalation ceiling; 0 when the search does not escalate
+    DeviceBuffer esc_state_, tm_changes_;  // escalation state, truemotion change flags
     bool measures_ = false;
     NoiseFront noise_;
     DeviceBuffer outputs_[2];

@@ -146,6 +146,25 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
     const float* nbr = t.pyramid + static_cast<int64_t>(nslot) * t.slot_pixels;
     const int32_t* field = t.mv_in + static_cast<int64_t>(n) * t.mv_stride;
     const int32_t* seeds = t.seeds ? t.seeds + static_cast<int64_t>(n) * t.mv_stride : nullptr;
+    // mod.rs:483-520, 656-680: a block whose 3x3 neighbourhood kept every vector last pass would
+    // pick what it holds again, and its confidence from that pass still stands.
+    if (t.changes_in) {
+        bool changed = false;
+        if (lane < 9) {
+            const int c = col + lane % 3 - 1, r = row + lane / 3 - 1;
+            changed = on_grid(c, r, t.blocks_x, t.blocks_y) &&
+                      __ldg(t.changes_in + static_cast<int64_t>(n) * t.conf_stride + r * t.blocks_x + c) != 0u;
+        }
+        if (!__any_sync(0xffffffffu, changed)) {
+            if (lane == 0) {
+                int32_t* out = t.mv_out + static_cast<int64_t>(n) * t.mv_stride + 2 * blk;
+                out[0] = field[2 * blk];
+                out[1] = field[2 * blk + 1];
+                if (t.changes_out) t.changes_out[static_cast<int64_t>(n) * t.conf_stride + blk] = 0u;
+            }
+            return;  // the whole warp leaves together
+        }
+    }
 
     CentreColumn<BLK> cc;
     if (BLK) {
@@ -335,6 +354,9 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
             if (c < 0.0f) c = 0.0f;
             t.confidence[static_cast<int64_t>(n) * t.conf_stride + blk] = c;
         }
+        if (t.changes_out)
+            t.changes_out[static_cast<int64_t>(n) * t.conf_stride + blk] =
+                (best_x == field[2 * blk] && best_y == field[2 * blk + 1]) ? 0u : 1u;
     }
 }
 

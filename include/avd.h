@@ -480,7 +480,18 @@ typedef struct AvdMotionPass {
                       * pass, as `run_seeded_refine` does (motion/analyse.rs:273-316) */
     uint64_t keep_seeds; /* i32 like `mv_field`: the field after the coarse pass, the truemotion stage's
                           * seed candidates (analyse.rs:268-277); 0 = not kept */
+    uint64_t escalation; /* f32 scratch of avd_escalation_state_floats(neighbours, conf_stride) values;
+                          * with ceiling > search_radius the blocks that fail the first pass search again
+                          * `ceiling` around their first window (motion/escalate.rs:19-57, analyse.rs:
+                          * 234-262); 0 = no escalation */
+    uint32_t ceiling;         /* motion/context.rs:55-71: max_search_escalation; at most 8 */
+    uint32_t esc_reads_floor; /* 1: a positive noise word `sad_floor_word` is the escalation floor; else it
+                               * is measured from the first pass's SADs (escalate.rs:168-257) */
 } AvdMotionPass;
+
+/* The f32 values the escalation state of a search over `neighbours` neighbours holds: four
+ * sections of neighbours * conf_stride and the SAD floor (motion/analyse.rs:85-95). */
+AVD_API uint64_t avd_escalation_state_floats(uint32_t neighbours, uint32_t conf_stride);
 
 AVD_API AvdStatus avd_motion_search(const AvdMotionPass* pass, void* stream);
 

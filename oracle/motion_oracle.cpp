@@ -27,6 +27,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <cstdint>
 #include <cstdint>
 #include <vector>
 
@@ -68,8 +70,9 @@ struct Best {
     float sad;
 };
 
-// block_match.rs:674-760 for one centre.
-Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy, int cdx, int cdy, int R) {
+// block_match.rs:674-760 for one centre; `sads_out`, when given, receives every candidate's SAD.
+Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy, int cdx, int cdy, int R,
+                   std::vector<float>* sads_out = nullptr) {
     const int b = L.blksize, side = 2 * R + 1;
     const float* cf = L.base + centre_slot * L.slot;
     const float* nf = L.base + nbr_slot * L.slot;
@@ -99,7 +102,78 @@ Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy
         }
     const float centre_sad = sads[R * side + R];
     if (centre_sad <= best.sad) best = Best{cdx, cdy, centre_sad};
+    if (sads_out) *sads_out = sads;
     return best;
+}
+
+float match_confidence(float sad, float floor, float thsad) {
+    float excess = sad - floor;
+    if (excess < 0.0f) excess = 0.0f;
+    const float t2 = thsad * thsad, e2 = excess * excess;
+    const float c = (t2 - e2) / (t2 + e2);
+    return c < 0.0f ? 0.0f : c;
+}
+
+// motion/kernels/escalate.rs:14-67: the constants of the escalation stage.
+constexpr float kEscalateBelowConfidence = 0.5f;
+constexpr int kNeighbourDisagreement = 4;
+constexpr float kEscalateSadMargin = 0.125f;
+constexpr uint32_t kFloorSamples = 4096, kFloorRankDivisor = 4, kFloorBinShift = 16, kInfinityBin = 0x7F80;
+constexpr float kExactMatchSad = 1.0e-6f, kFlatShare = 0.25f;
+
+uint32_t float_bits(float v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    return u;
+}
+
+float bits_float(uint32_t u) {
+    float v;
+    std::memcpy(&v, &u, 4);
+    return v;
+}
+
+// escalate.rs:259-297 (`ranked_bin`): the lowest bin b >= lower with divisor * |{lower <= key <= b}|
+// >= |{key >= lower}|, found by the same bisection over [lower, infinity's bin].
+uint32_t ranked_bin(const std::vector<uint32_t>& keys, uint32_t lower, uint32_t divisor) {
+    auto count = [&](uint32_t lo, uint32_t hi) {
+        uint32_t c = 0;
+        for (uint32_t k : keys) c += (k >= lo && k <= hi) ? 1u : 0u;
+        return c;
+    };
+    const uint32_t valid = count(lower, 0xFFFFFFFFu);
+    uint32_t low = lower, high = kInfinityBin;
+    while (low < high) {
+        const uint32_t middle = low + (high - low) / 2;
+        if (divisor * count(lower, middle) >= valid)
+            high = middle;
+        else
+            low = middle + 1;
+    }
+    return low;
+}
+
+// escalate.rs:168-257 (`mc_measure_floor`) over the kept SADs `kept` (neighbour n's block b at
+// n * blocks + b).
+float measure_floor(const std::vector<float>& kept, int neighbours, int blocks) {
+    const uint32_t total = static_cast<uint32_t>(neighbours) * static_cast<uint32_t>(blocks);
+    const uint32_t sample_step = (total + kFloorSamples - 1) / kFloorSamples;
+    const uint32_t sample_count = (total + sample_step - 1) / sample_step;
+    std::vector<uint32_t> keys(kFloorSamples);
+    for (uint32_t s = 0; s < kFloorSamples; ++s) {
+        const uint32_t flat = std::min(s, sample_count - 1) * sample_step;
+        const float k = kept[flat];
+        const bool counted = s < sample_count && k > kExactMatchSad;
+        keys[s] = counted ? float_bits(k) >> kFloorBinShift : 0u;
+    }
+    uint32_t valid = 0;
+    for (uint32_t k : keys) valid += k >= 1 ? 1u : 0u;
+    const uint32_t median_bin = ranked_bin(keys, 1, 2);
+    const float median = bits_float(median_bin << kFloorBinShift);
+    const float flat_limit = median * kFlatShare;
+    const uint32_t grainy = std::max(float_bits(flat_limit) >> kFloorBinShift, 1u);
+    const uint32_t floor_bin = ranked_bin(keys, grainy, kFloorRankDivisor);
+    return valid == 0 ? 0.0f : bits_float(floor_bin << kFloorBinShift);
 }
 
 }  // namespace
@@ -118,6 +192,10 @@ struct OrcMotionArgs {
     float thsad;
     uint32_t seeded;  // 1: mv_field holds the seeds; no coarse pass (motion/analyse.rs:273-316)
     int32_t* keep_seeds;  // non-null: the field after the coarse pass is copied here (analyse.rs:268-277)
+    // motion/escalate.rs:19-57: with ceiling > search_radius the blocks that fail the first pass
+    // search again `ceiling` either side of their first window's centre; `esc_reads_floor` takes the
+    // floor from the noise word when it is positive; `widen_coarse` searches the coarse level again.
+    uint32_t ceiling, esc_reads_floor, widen_coarse;
 };
 
 int64_t orc_motion_pyramid_floats(int w, int h, int frames, int levels) { return level_base(w, h, frames, levels); }
@@ -184,14 +262,43 @@ void orc_motion_search(const OrcMotionArgs* a) {
             std::copy(a->mv_field, a->mv_field + static_cast<int64_t>(a->neighbours) * a->mv_stride, a->keep_seeds);
     }
     Level L{a->pyramid, slot_pixels(w, h, 0), w, h, static_cast<int>(a->blksize), step, bx_n, by_n};
+    const int neighbours = static_cast<int>(a->neighbours), blocks = bx_n * by_n;
+    const int C = static_cast<int>(a->ceiling);
+    const bool escalates = C > R;
+    // escalate.rs:60-67: the kept SAD, the edge bar, and the first window's centre of every block.
+    std::vector<float> kept, edge;
+    std::vector<int> centre_x, centre_y;
+    if (escalates) {
+        kept.assign(static_cast<size_t>(neighbours) * blocks, 0.0f);
+        edge = kept;
+        centre_x.assign(kept.size(), 0);
+        centre_y.assign(kept.size(), 0);
+    }
 #pragma omp parallel for collapse(2) schedule(dynamic)
-    for (int n = 0; n < static_cast<int>(a->neighbours); ++n)
+    for (int n = 0; n < neighbours; ++n)
         for (int by = 0; by < by_n; ++by)
             for (int bx = 0; bx < bx_n; ++bx) {
                 int32_t* mv = a->mv_field + static_cast<int64_t>(n) * a->mv_stride + (by * bx_n + bx) * 2;
                 const int sdx = seeded ? mv[0] : 0, sdy = seeded ? mv[1] : 0;
+                std::vector<float> sads;
                 const Best b = search_window(L, static_cast<int>(a->centre_slot), static_cast<int>(a->neighbour_slots[n]),
-                                             bx * step, by * step, sdx, sdy, R);
+                                             bx * step, by * step, sdx, sdy, R, escalates ? &sads : nullptr);
+                if (escalates) {
+                    // block_match.rs:783-796: a winner on the window's outer ring records the lowest
+                    // SAD off that ring as its edge bar, else 0.
+                    const size_t i = static_cast<size_t>(n) * blocks + by * bx_n + bx;
+                    kept[i] = b.sad;
+                    centre_x[i] = sdx;
+                    centre_y[i] = sdy;
+                    float bar = 0.0f;
+                    if (std::abs(b.dx - sdx) == R || std::abs(b.dy - sdy) == R) {
+                        const int side = 2 * R + 1;
+                        bar = 1.0e30f;
+                        for (int y = 1; y < side - 1; ++y)
+                            for (int x = 1; x < side - 1; ++x) bar = std::min(bar, sads[y * side + x]);
+                    }
+                    edge[i] = bar;
+                }
                 mv[0] = b.dx;
                 mv[1] = b.dy;
                 if (a->confidence) {
@@ -204,12 +311,75 @@ void orc_motion_search(const OrcMotionArgs* a) {
                     a->confidence[static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx] = c;
                 }
             }
+    if (!escalates) return;
+    // escalate.rs:168-257: the floor the flags and margins score against.
+    const float reading = a->noise ? a->noise[a->sad_floor_word] : 0.0f;
+    const float floor = a->esc_reads_floor && reading > 0.0f ? reading : measure_floor(kept, neighbours, blocks);
+    const float margin = kEscalateSadMargin * floor;
+    // escalate.rs:335-395 (`mc_flag_failures`), on the field the fine pass left.
+    std::vector<char> failed(kept.size(), 0);
+    for (int n = 0; n < neighbours; ++n)
+        for (int by = 0; by < by_n; ++by)
+            for (int bx = 0; bx < bx_n; ++bx) {
+                const size_t i = static_cast<size_t>(n) * blocks + by * bx_n + bx;
+                const int32_t* f = a->mv_field + static_cast<int64_t>(n) * a->mv_stride;
+                const int own = (by * bx_n + bx) * 2;
+                int closest = INT32_MAX;
+                auto gap = [&](int slot) {
+                    closest = std::min(closest, std::max(std::abs(f[slot] - f[own]), std::abs(f[slot + 1] - f[own + 1])));
+                };
+                if (bx > 0) gap(own - 2);
+                if (bx + 1 < bx_n) gap(own + 2);
+                if (by > 0) gap(own - 2 * bx_n);
+                if (by + 1 < by_n) gap(own + 2 * bx_n);
+                if (closest == INT32_MAX) closest = 0;
+                const bool low = match_confidence(kept[i], floor, a->thsad) < kEscalateBelowConfidence;
+                const bool on_edge = kept[i] + margin < edge[i];
+                failed[i] = low || on_edge || closest > kNeighbourDisagreement;
+            }
+    // escalate.rs:400-559 (`mc_escalate_search`).
+    const bool widen = a->widen_coarse && a->levels > 1 && !a->seeded;
+    Level Lc{};
+    int scale = 1;
+    if (widen) {
+        const int level = static_cast<int>(a->levels) - 1;
+        scale = 1 << level;
+        level_dims(w, h, level, &Lc.width, &Lc.height);
+        Lc.base = a->pyramid + level_base(w, h, frames, level);
+        Lc.slot = slot_pixels(w, h, level);
+        Lc.blksize = static_cast<int>(a->blksize) / scale > 2 ? static_cast<int>(a->blksize) / scale : 2;
+    }
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int n = 0; n < neighbours; ++n)
+        for (int by = 0; by < by_n; ++by)
+            for (int bx = 0; bx < bx_n; ++bx) {
+                const size_t i = static_cast<size_t>(n) * blocks + by * bx_n + bx;
+                if (!failed[i]) continue;
+                const int cs = static_cast<int>(a->centre_slot), ns = static_cast<int>(a->neighbour_slots[n]);
+                Best best = search_window(L, cs, ns, bx * step, by * step, centre_x[i], centre_y[i], C);
+                if (widen) {
+                    const Best cb = search_window(Lc, cs, ns, bx * step / scale, by * step / scale, 0, 0, C);
+                    const int cx = cb.dx * scale, cy = cb.dy * scale;
+                    if (cx != centre_x[i] || cy != centre_y[i]) {
+                        const Best ch = search_window(L, cs, ns, bx * step, by * step, cx, cy, C);
+                        if (ch.sad + margin < best.sad) best = ch;
+                    }
+                }
+                if (best.sad + margin < kept[i]) {
+                    int32_t* mv = a->mv_field + static_cast<int64_t>(n) * a->mv_stride + (by * bx_n + bx) * 2;
+                    mv[0] = best.dx;
+                    mv[1] = best.dy;
+                    if (a->confidence)
+                        a->confidence[static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx] =
+                            match_confidence(best.sad, a->noise[a->sad_floor_word], a->thsad);
+                }
+            }
 }
 
 // One truemotion pass (motion/truemotion/kernels/truemotion/mod.rs:560-763, `mc_truemotion` with
 // the serial scoring of score.rs:7-61) over level 0 of `pyramid`: every block of every neighbour
 // picks its vector from `mv_in` (and `seeds`, when given) into `mv_out`, with its confidence when
-// `confidence` is given. No camera model (no prediction candidate), no change flags.
+// `confidence` is given. No camera model (no prediction candidate).
 struct OrcTruemotionArgs {
     const float* pyramid;
     const uint32_t* neighbour_slots;
@@ -221,6 +391,11 @@ struct OrcTruemotionArgs {
     uint32_t width, height, frame_count, centre_slot, neighbours, blksize, overlap, mv_stride, conf_stride;
     uint32_t sad_field, reads_floor, refine_radius;
     float lambda_base, lambda_noise, surcharge, fade_level, thsad;
+    // truemotion/kernels/truemotion/mod.rs:483-520, 560-575, 656-680: with `changes_in`, a block
+    // whose 3x3 neighbourhood (itself included) changed nothing in the pass before copies its own
+    // vector and keeps its confidence; `changes_out` flags each block whose pick left its own vector.
+    const uint32_t* changes_in;
+    uint32_t* changes_out;
 };
 
 namespace {
@@ -278,6 +453,21 @@ void orc_truemotion_pass(const OrcTruemotionArgs* a) {
                 return Vec2{v[0], v[1]};
             };
             const Vec2 own = field(a->mv_in, col, row);
+            if (a->changes_in) {
+                bool changed = false;
+                for (int pos = 0; pos < 9; ++pos) {
+                    const int c = col + pos % 3 - 1, r = row + pos / 3 - 1;
+                    if (on_grid(c, r, bx_n, by_n) && a->changes_in[static_cast<int64_t>(n) * a->conf_stride + r * bx_n + c])
+                        changed = true;
+                }
+                if (!changed) {
+                    int32_t* out = a->mv_out + mv_base + static_cast<int64_t>(blk) * 2;
+                    out[0] = own.dx;
+                    out[1] = own.dy;
+                    if (a->changes_out) a->changes_out[static_cast<int64_t>(n) * a->conf_stride + blk] = 0;
+                    continue;
+                }
+            }
             // candidates.rs:124-176 (`neighbourhood_median`): the component-wise lower median of the
             // on-grid blocks of the 3x3 neighbourhood, the block's own vector without any.
             std::vector<int> xs, ys;
@@ -402,6 +592,9 @@ void orc_truemotion_pass(const OrcTruemotionArgs* a) {
             if (a->confidence)
                 a->confidence[static_cast<int64_t>(n) * a->conf_stride + blk] =
                     pass_confidence(best_sad, a->noise[a->sad_field], a->thsad);
+            if (a->changes_out)
+                a->changes_out[static_cast<int64_t>(n) * a->conf_stride + blk] =
+                    (best.dx == own.dx && best.dy == own.dy) ? 0u : 1u;
         }
 }
 

@@ -233,7 +233,7 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
                   sad_floor: float = 0.0, thsad_scale: float = 1.0, blksize: int = 16, overlap: int = 8,
                   search_radius: int = 4, levels: int = 2, chained: bool = False, refine_radius: int = 2,
                   prefilter=None, fp64: bool = False, derived=None, share_writes=None,
-                  share_reads=None) -> list[np.ndarray]:
+                  share_reads=None, ceiling: int = 0) -> list[np.ndarray]:
     """NLMeans with motion compensation over a stream with repeat edges, replayed slot by slot as
     the ring runs it (nlmeans/denoiser/ring.rs, stages.rs:62-209, dispatch/motion.rs:104-487):
       - each slot write (and each edge copy) builds the slot's pyramids; with Chained estimation it
@@ -281,7 +281,7 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
             older = (slot + tf - 1) % tf
             pyr = search_pyramid()
             kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=th,
-                      field_lambda=1.0, reads_floor=False)
+                      field_lambda=1.0, reads_floor=False, ceiling=ceiling)
             fwd, _ = motion_search(pyr, w, h, tf, older, [slot], **kw)
             bwd, _ = motion_search(pyr, w, h, tf, slot, [older], **kw)
             pairs[st["head"] % (2 * d)] = (fwd[0], bwd[0])
@@ -318,11 +318,12 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
             seeds = chain_compose(pairs, d, d, st["head"] % (2 * d), step, w, h, bx, by)
             mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                    search_radius=refine_radius, levels=levels, confidence=confidence,
-                                   sad_floor=w_floor, thsad=th, seeds=seeds)
+                                   sad_floor=w_floor, thsad=th, seeds=seeds, ceiling=ceiling, esc_reads_floor=True)
         else:
             mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                    search_radius=search_radius, levels=levels, confidence=confidence,
-                                   sad_floor=w_floor, thsad=th, field_lambda=1.0, reads_floor=True)
+                                   sad_floor=w_floor, thsad=th, field_lambda=1.0, reads_floor=True, ceiling=ceiling,
+                                   esc_reads_floor=True)
         if share_writes is not None:
             share_writes.write(st["call"], slot_frame[cs] % tf, slot_frame[cs], mv)
         window, refs = [], []
@@ -479,7 +480,8 @@ class MotionArgs(C.Structure):
     ] + [(n, C.c_uint32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize",
                                    "overlap", "search_radius", "levels", "mv_stride", "conf_stride",
                                    "sad_floor_word")] + [("thsad", C.c_float), ("seeded", C.c_uint32),
-                                                         ("keep_seeds", C.POINTER(C.c_int32))]
+                                                         ("keep_seeds", C.POINTER(C.c_int32))] + \
+        [(n, C.c_uint32) for n in ("ceiling", "esc_reads_floor", "widen_coarse")]
 
 
 class TruemotionArgs(C.Structure):
@@ -489,7 +491,8 @@ class TruemotionArgs(C.Structure):
     ] + [(n, C.c_uint32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize",
                                    "overlap", "mv_stride", "conf_stride", "sad_field", "reads_floor",
                                    "refine_radius")] + [(n, C.c_float) for n in ("lambda_base", "lambda_noise",
-                                                                                 "surcharge", "fade_level", "thsad")]
+                                                                                 "surcharge", "fade_level", "thsad")] + \
+        [("changes_in", C.POINTER(C.c_uint32)), ("changes_out", C.POINTER(C.c_uint32))]
 
 
 # motion/truemotion/params.rs:4-33 and motion/confidence.rs:10.
@@ -508,8 +511,26 @@ def truemotion_values(field_lambda: float, blksize: int, thsad_value: float) -> 
 
 def truemotion_pass(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
                     mv_in: np.ndarray, seeds: np.ndarray | None, *, blksize=16, overlap=8, field_lambda=1.0,
-                    thsad=0.0, sad_floor=0.0, reads_floor=True, confidence=False):
-    """One truemotion pass (no camera model): returns (mv (n, blocks, 2), conf (n, blocks))."""
+                    thsad=0.0, sad_floor=0.0, reads_floor=True, confidence=False, passes=1):
+    """The truemotion stage (no camera model): returns (mv (n, blocks, 2), conf (n, blocks)). With
+    `passes` 2 (a search that escalates, truemotion/params.rs:9-12, 79-90) the second pass reads the
+    first's field and rescores only the blocks next to one it changed (truemotion/stage.rs:82-142)."""
+    mv = mv_in
+    conf = None
+    changes = None
+    for p in range(passes):
+        out_changes = np.zeros(np.asarray(mv_in).size // 2, np.uint32) if p + 1 < passes else None
+        mv, c = _truemotion_once(pyramid, width, height, frames, centre_slot, neighbour_slots, mv, seeds,
+                                 blksize=blksize, overlap=overlap, field_lambda=field_lambda, thsad=thsad,
+                                 sad_floor=sad_floor, reads_floor=reads_floor, confidence=confidence,
+                                 changes_in=changes, changes_out=out_changes, conf_in=conf)
+        conf, changes = c, out_changes
+    return mv, conf
+
+
+def _truemotion_once(pyramid, width, height, frames, centre_slot, neighbour_slots, mv_in, seeds, *, blksize,
+                     overlap, field_lambda, thsad, sad_floor, reads_floor, confidence, changes_in=None,
+                     changes_out=None, conf_in=None):
     step = blksize - overlap
     bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
     slots = np.ascontiguousarray(neighbour_slots, np.uint32)
@@ -517,7 +538,7 @@ def truemotion_pass(pyramid: np.ndarray, width: int, height: int, frames: int, c
     mv_in = np.ascontiguousarray(mv_in, np.int32).reshape(-1)
     sd = np.ascontiguousarray(seeds, np.int32).reshape(-1) if seeds is not None else None
     out = np.zeros_like(mv_in)
-    conf = np.zeros(n * bx * by, np.float32)
+    conf = np.zeros(n * bx * by, np.float32) if conf_in is None else np.ascontiguousarray(conf_in, np.float32).reshape(-1).copy()
     noise = np.array([sad_floor], np.float32)
     lb, ln, fade = truemotion_values(field_lambda, blksize, thsad)
     a = TruemotionArgs()
@@ -531,6 +552,8 @@ def truemotion_pass(pyramid: np.ndarray, width: int, height: int, frames: int, c
     a.blksize, a.overlap, a.mv_stride, a.conf_stride = blksize, overlap, bx * by * 2, bx * by
     a.sad_field, a.reads_floor, a.refine_radius = 0, int(reads_floor), TRUEMOTION["refine_radius"]
     a.lambda_base, a.lambda_noise, a.surcharge, a.fade_level, a.thsad = lb, ln, TRUEMOTION["surcharge"], fade, thsad
+    a.changes_in = changes_in.ctypes.data_as(C.POINTER(C.c_uint32)) if changes_in is not None else None
+    a.changes_out = changes_out.ctypes.data_as(C.POINTER(C.c_uint32)) if changes_out is not None else None
     l = lib()
     l.orc_truemotion_pass.argtypes = [C.POINTER(TruemotionArgs)]
     l.orc_truemotion_pass(C.byref(a))
@@ -553,11 +576,15 @@ def motion_pyramid(ring: np.ndarray, channels: int, width: int, height: int, lev
 
 def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
                   *, blksize=16, overlap=8, search_radius=4, levels=2, confidence=False, sad_floor=0.0,
-                  thsad=0.0, seeds: np.ndarray | None = None, field_lambda: float = 0.0, reads_floor: bool = True):
+                  thsad=0.0, seeds: np.ndarray | None = None, field_lambda: float = 0.0, reads_floor: bool = True,
+                  ceiling: int = 0, esc_reads_floor: bool = False):
     """One block-matching search (no camera model). Returns (mv (n, blocks, 2), conf).
     With `seeds` (n, blocks, 2) the search refines around them and skips the coarse pass. With
-    `field_lambda` > 0 the truemotion stage ends the search (motion/analyse.rs:175-312): its seed
-    candidates are the coarse pass's field, when a coarse pass ran."""
+    `ceiling` > `search_radius` the blocks that fail search again `ceiling` around their first
+    window (motion/escalate.rs), the coarse level too when a coarse pass ran, and the truemotion
+    stage runs two passes. With `field_lambda` > 0 the truemotion stage ends the search
+    (motion/analyse.rs:175-312): its seed candidates are the coarse pass's field, when a coarse pass
+    ran."""
     step = blksize - overlap
     bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
     slots = np.ascontiguousarray(neighbour_slots, np.uint32)
@@ -574,6 +601,8 @@ def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, cen
     a.blksize, a.overlap, a.search_radius, a.levels = blksize, overlap, search_radius, levels
     a.mv_stride, a.conf_stride, a.sad_floor_word, a.thsad = bx * by * 2, bx * by, 0, thsad
     a.seeded = int(seeds is not None)
+    escalates = ceiling > search_radius
+    a.ceiling, a.esc_reads_floor, a.widen_coarse = ceiling if escalates else 0, int(esc_reads_floor), 1
     coarse = levels > 1 and seeds is None
     kept = np.zeros_like(mv) if (field_lambda > 0.0 and coarse) else None
     a.keep_seeds = kept.ctypes.data_as(C.POINTER(C.c_int32)) if kept is not None else None
@@ -583,7 +612,7 @@ def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, cen
     if field_lambda > 0.0:
         return truemotion_pass(pyramid, width, height, frames, centre_slot, slots, mv, kept, blksize=blksize,
                                overlap=overlap, field_lambda=field_lambda, thsad=thsad, sad_floor=sad_floor,
-                               reads_floor=reads_floor, confidence=confidence)
+                               reads_floor=reads_floor, confidence=confidence, passes=2 if escalates else 1)
     return mv.reshape(n, bx * by, 2), conf.reshape(n, bx * by)
 
 
@@ -695,7 +724,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
                 levels=2, refine=2, spatial_radius=9, lambda_ht=4.158, c_min=0.05, kaiser_beta=2.0,
                 pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0, chained: bool = False,
                 refine_radius: int = 2, noise=None, field_lambda: float = 1.0, share_writes: MotionShare | None = None,
-                share_reads: MotionShare | None = None) -> list[np.ndarray]:
+                share_reads: MotionShare | None = None, ceiling: int = 0) -> list[np.ndarray]:
     """The NL4D engine with a pinned sigma and Direct or Chained motion (no camera model) over a
     stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order. With
     `field_lambda` > 0 the truemotion stage ends the Direct window search (reading the window's SAD
@@ -759,11 +788,12 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
             seeds = chain_compose(pairs, centre, d, st["head"] % (2 * d), step, w, h, bx, by)
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=refine_radius, levels=levels, confidence=True,
-                                     sad_floor=p_floor, thsad=th, seeds=seeds)
+                                     sad_floor=p_floor, thsad=th, seeds=seeds, ceiling=ceiling, esc_reads_floor=True)
         else:
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=search_radius, levels=levels, confidence=True,
-                                     sad_floor=p_floor, thsad=th, field_lambda=field_lambda, reads_floor=True)
+                                     sad_floor=p_floor, thsad=th, field_lambda=field_lambda, reads_floor=True,
+                                     ceiling=ceiling, esc_reads_floor=True)
         if share_writes is not None:
             share_writes.write(st["call"], slot_frames[cs] % tf, slot_frames[cs], mv)
         acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
@@ -792,7 +822,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         older = (newer + tf - 1) % tf
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
         kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=th,
-                  field_lambda=field_lambda, reads_floor=False)
+                  field_lambda=field_lambda, reads_floor=False, ceiling=ceiling)
         fwd, _ = motion_search(pyr, w, h, tf, older, [newer], **kw)
         bwd, _ = motion_search(pyr, w, h, tf, newer, [older], **kw)
         pairs[st["head"] % (2 * d)] = (fwd[0], bwd[0])

@@ -153,7 +153,9 @@ def oracle_pass(oracle, frames: list[list[np.ndarray]], fmt, d, a, s, strength, 
                                         thsad_scale=thsad_scale, blksize=motion.blksize, overlap=motion.overlap,
                                         search_radius=motion.search_radius, levels=motion.pyramid_levels,
                                         chained=chained, refine_radius=refine, prefilter=pf, fp64=fp64,
-                                        share_writes=None if fp64 else share_writes, share_reads=share_reads)
+                                        share_writes=None if fp64 else share_writes, share_reads=share_reads,
+                                        ceiling=motion.max_search_escalation
+                                        if motion.max_search_escalation > motion.search_radius else 0)
     else:
         def run(fp64):
             return oracle.nlm_stream_repeat(f32, d, a, s, h2, wref=wref, noise_offset=off, lut=lut, fp64=fp64,

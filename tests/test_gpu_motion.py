@@ -23,7 +23,7 @@ CASES = [
 
 
 def gpu_search(lib, ring, w, h, frames, levels, blksize, overlap, radius, channels, confidence, centre, slots,
-               sad_floor, thsad):
+               sad_floor, thsad, ceiling=0, esc_reads_floor=False):
     import torch
 
     from av_denoise_b200 import _abi
@@ -48,6 +48,9 @@ def gpu_search(lib, ring, w, h, frames, levels, blksize, overlap, radius, channe
     p.width, p.height, p.frame_count, p.centre_slot, p.neighbours = w, h, frames, centre, n
     p.blksize, p.overlap, p.search_radius, p.levels = blksize, overlap, radius, levels
     p.mv_stride, p.conf_stride, p.sad_floor_word, p.thsad = bx * by * 2, bx * by, 0, thsad
+    if ceiling:
+        state = torch.zeros(lib.avd_escalation_state_floats(n, bx * by), dtype=torch.float32, device="cuda")
+        p.escalation, p.ceiling, p.esc_reads_floor = state.data_ptr(), ceiling, int(esc_reads_floor)
     st = lib.avd_motion_search(C.byref(p), stream)
     assert st == 0, lib.avd_last_error().decode()
     torch.cuda.synchronize()
@@ -223,3 +226,38 @@ def test_truemotion_rejects_bad_passes(lib):
     assert lib.avd_truemotion_pass(C.byref(t), None) != 0  # lambda 0 runs no stage
     t.field_lambda, t.mv_stride = 1.0, 10
     assert lib.avd_truemotion_pass(C.byref(t), None) != 0  # stride below the blocks
+
+
+ESC_CASES = [
+    # width, height, frames, levels, blksize, overlap, radius, ceiling, reads floor, sad-floor sigma
+    (160, 96, 5, 1, 16, 8, 2, 6, False, 0.02),
+    (160, 96, 5, 2, 16, 8, 2, 8, False, 0.02),
+    (123, 77, 3, 3, 16, 8, 3, 8, True, 0.02),
+    (96, 64, 3, 2, 8, 4, 1, 5, True, 0.0),
+    (200, 120, 5, 2, 32, 16, 4, 8, False, 0.05),
+    (40, 24, 3, 1, 16, 8, 0, 3, False, 0.02),
+]
+
+
+@pytest.mark.parametrize("case", ESC_CASES, ids=lambda c: "x".join(map(str, c[:8])))
+def test_escalating_search_matches_oracle_bit_for_bit(lib, oracle, case):
+    """motion/escalate.rs: the first pass's SADs and edge bars, the floor (read or measured), the
+    failure flags and the wider search (coarse level included) give the oracle's vectors and
+    confidences bit for bit."""
+    w, h, frames, levels, blksize, overlap, radius, ceiling, reads, sig = case
+    ring = moving_window(w, h, frames, seed=w * 11 + h, channels=1)
+    centre = frames // 2
+    slots = [s for s in range(frames) if s != centre]
+    floor = oracle.sad_noise_floor(blksize, sig)
+    th = oracle.thsad(blksize, 1.0)
+    _, mv, conf = gpu_search(lib, ring, w, h, frames, levels, blksize, overlap, radius, 1, True, centre, slots,
+                             floor, th, ceiling=ceiling, esc_reads_floor=reads)
+    o_pyr = oracle.motion_pyramid(ring, 1, w, h, levels)
+    o_mv, o_conf = oracle.motion_search(o_pyr, w, h, frames, centre, slots, blksize=blksize, overlap=overlap,
+                                        search_radius=radius, levels=levels, confidence=True, sad_floor=floor,
+                                        thsad=th, ceiling=ceiling, esc_reads_floor=reads)
+    plain, _ = oracle.motion_search(o_pyr, w, h, frames, centre, slots, blksize=blksize, overlap=overlap,
+                                    search_radius=radius, levels=levels, confidence=True, sad_floor=floor, thsad=th)
+    print("blocks escalated to a new vector:", int(np.any(o_mv != plain, axis=-1).sum()), "of", o_mv.shape[0] * o_mv.shape[1])
+    assert np.array_equal(mv, o_mv), np.argwhere(mv != o_mv)[:5]
+    assert np.array_equal(conf.view(np.uint32), o_conf.view(np.uint32))

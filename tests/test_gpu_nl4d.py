@@ -128,9 +128,9 @@ def test_nl4d_options_this_build_rejects():
     g420 = avd.Geometry(64, 48, avd.ChromaLayout.YUV420, fmt, fmt)
     with pytest.raises(avd.InvalidOptions, match="colour grain gains"):
         avd.build_engine(avd.EngineSpec.nl4d(None, avd.Nl4dOptions(temporal_radius=1, noise_map=False), g420))
+    # Search escalation is built (test_nl4d_escalating_motion_matches_oracle).
     escalating = avd.Nl4dOptions(sigma=0.03, temporal_radius=1, motion=avd.MotionSearch(max_search_escalation=8))
-    with pytest.raises(avd.InvalidOptions, match="escalation"):
-        avd.build_engine(avd.EngineSpec.nl4d(escalating, None, g))
+    avd.build_engine(avd.EngineSpec.nl4d(escalating, None, g)).close()
 
 
 @pytest.mark.parametrize("n,d,estimation,refine_radius,context", [
@@ -181,3 +181,20 @@ def test_nl4d_chroma_refines_the_luma_motion(oracle, layout, shifts, d, est):
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, share_writes=share, **common)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, sigma, chroma=True,
           share_reads=share, **common)
+
+
+@pytest.mark.parametrize("d,chained", [(1, False), (3, True)])
+def test_nl4d_escalating_motion_matches_oracle(oracle, d, chained):
+    """NL4D under a search that escalates to 8 from radius 2 (the slow preset's ceiling): the
+    window search, the pair searches and the chained refine widen their failing blocks, and the
+    truemotion stage runs two passes."""
+    w, h, sigma = 96, 64, 10.0 / 255
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 2 * d + 3, seed=1200 + d)
+    est = avd.MotionEstimation.CHAINED if chained else avd.MotionEstimation.DIRECT
+    ms = avd.MotionSearch(search_radius=2, max_search_escalation=8, estimation=est, refine_radius=2)
+    o = avd.Nl4dOptions(sigma=sigma, temporal_radius=d, spatial_radius=4, motion=ms)
+    spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, spatial_radius=4,
+          search_radius=2, chained=chained, refine_radius=2, ceiling=8)

@@ -115,13 +115,31 @@ def test_chroma_motion_compensated_10bit(oracle):
           min_raw=0.95, share_reads=share)
 
 
-def test_motion_compensation_rejects_escalation():
+@pytest.mark.parametrize("d,est,radius,ceiling,hq", [(2, avd.MotionEstimation.DIRECT, 2, 6, False),
+                                                     (3, avd.MotionEstimation.AUTO, 2, 8, False),
+                                                     (1, avd.MotionEstimation.DIRECT, 1, 4, True)])
+def test_escalating_motion_compensation(oracle, d, est, radius, ceiling, hq):
+    """A search whose max_search_escalation exceeds its radius (the slow presets): failing blocks
+    search again up to the ceiling, and the truemotion stage runs a second pass over the blocks
+    next to a changed one (motion/escalate.rs, truemotion/stage.rs:82-142)."""
+    w, h = 128, 80
     fmt = avd.SampleFormat.u8()
-    ms = avd.MotionSearch(search_radius=2, max_search_escalation=4)
-    spec = avd.EngineSpec.nlmeans(avd.NlmeansAlgorithm.fast(options(1, 2, 2, 8.0, ms)), None,
-                                  avd.Geometry(64, 48, avd.ChromaLayout.GRAY, fmt, fmt))
-    with pytest.raises(avd.InvalidOptions, match="escalation"):
-        avd.build_engine(spec)
+    frames = clip(w, h, 5, seed=1010 + d, motion=7)
+    ms = avd.MotionSearch(blksize=16, overlap=8, search_radius=radius, max_search_escalation=ceiling,
+                          pyramid_levels=2, estimation=est, refine_radius=2)
+    if hq:
+        sigma = 8.0 / 255
+        params = avd.HqParams(sigma_override=sigma, temporal_confidence=True)
+        alg = avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(nlm=options(d, 3, 2, None, ms), hq=params))
+    else:
+        alg = avd.NlmeansAlgorithm.fast(options(d, 3, 2, 8.0, ms))
+    spec = avd.EngineSpec.nlmeans(alg, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    if hq:
+        check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, avd.hq_default_strength(1, d),
+              ms, hq_sigma=sigma, hq_confidence=True, min_raw=0.95)
+    else:
+        check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, 8.0, ms)
 
 
 @pytest.mark.parametrize("layout,shifts,d,est", [("420", (1, 1), 2, avd.MotionEstimation.DIRECT),

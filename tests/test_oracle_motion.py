@@ -197,3 +197,88 @@ def test_map_ragged_edges_take_in_bounds_vectors(oracle):
     assert lg[:2] == (4, 2) and cg[:2] == (2, 1)
     out = oracle.map_luma_fields(_field(lg, lambda c, r: (c * 20, r * 40)), lg, cg, 1, 1)
     assert tuple(out[0, 1]) == (20, 0)
+
+
+# ---- search escalation (motion/escalate.rs; restating motion/tests/escalate.rs) ----
+
+def smooth(w, h, seed):
+    """Rows of a horizontal sinusoid, each with its own phase: a SAD surface that falls toward the
+    true horizontal motion from every side (the reference suite's smooth world)."""
+    phase = np.random.default_rng(seed).random(h)[:, None] * 2 * np.pi
+    return (0.5 + 0.3 * np.sin(0.1 * np.arange(w)[None, :] + phase)).astype(np.float32)
+
+
+def _escalate(oracle, dx, dy, first, ceiling, w=96, h=80, seed=31):
+    c = smooth(w, h, seed)
+    n = shifted(c, dx, dy)
+    pyr = oracle.motion_pyramid(pair_ring(c, n), 1, w, h, 1)
+    # A pinned floor and a lenient thsad: only the edge and neighbour rules fail blocks.
+    kw = dict(blksize=16, overlap=8, search_radius=first, levels=1, confidence=True, thsad=200.0, sad_floor=0.5,
+              esc_reads_floor=True)
+    plain, _ = oracle.motion_search(pyr, w, h, 2, 0, [1], **{k: v for k, v in kw.items() if k != "esc_reads_floor"})
+    esc, conf = oracle.motion_search(pyr, w, h, 2, 0, [1], ceiling=ceiling, **kw)
+    bx, by = -(-w // 8), -(-h // 8)
+    inner = lambda f: f[0].reshape(by, bx, 2)[2:-3, 2:-3]  # noqa: E731
+    return inner(plain), inner(esc), conf
+
+
+def test_in_window_motion_needs_no_escalation(oracle):
+    plain, esc, _ = _escalate(oracle, 1, 1, 2, 6)
+    assert np.all(plain == (1, 1)) and np.array_equal(plain, esc)
+
+
+def test_an_edge_winner_escalates_to_the_true_motion(oracle):
+    plain, esc, _ = _escalate(oracle, 3, 0, 2, 4)
+    assert np.all(np.abs(plain[..., 0]) <= 2)  # the first window cannot reach it
+    assert np.all(esc == (3, 0))
+
+
+def test_escalation_stops_at_the_ceiling(oracle):
+    _, within, _ = _escalate(oracle, 4, 0, 2, 4)
+    assert np.all(within == (4, 0))
+    _, beyond, _ = _escalate(oracle, 6, 0, 2, 4)
+    assert np.all(np.abs(beyond[..., 0]) <= 4)
+
+
+def test_escalation_widens_the_coarse_level_too(oracle):
+    # Two levels: the coarse seed reaches 2 * 2 = 4 pixels; escalation to 8 re-searches the coarse
+    # level at 8, whose winner (x2) seeds a second fine window.
+    w, h = 128, 96
+    c = smooth(w, h, 5)
+    n = shifted(c, 12, 0)
+    pyr = oracle.motion_pyramid(pair_ring(c, n), 1, w, h, 2)
+    kw = dict(blksize=16, overlap=8, search_radius=2, levels=2, confidence=True, thsad=200.0, sad_floor=0.5)
+    plain, _ = oracle.motion_search(pyr, w, h, 2, 0, [1], **kw)
+    esc, _ = oracle.motion_search(pyr, w, h, 2, 0, [1], ceiling=8, esc_reads_floor=True, **kw)
+    inner = lambda f: f[0].reshape(h // 8, w // 8, 2)[3:-4, 3:-4]  # noqa: E731
+    assert np.mean(np.all(inner(plain) == (12, 0), axis=-1)) < 0.5
+    assert np.all(inner(esc) == (12, 0))
+
+
+def test_second_truemotion_pass_keeps_quiet_neighbourhoods(oracle):
+    """With change flags in, a block whose 3x3 neighbourhood changed nothing copies its own vector;
+    with none set the pass is a copy of its input."""
+    w, h = 64, 48
+    c = textured(w, h, 9)
+    n = shifted(c, 2, 0)
+    pyr = oracle.motion_pyramid(pair_ring(c, n), 1, w, h, 1)
+    bx, by = w // 8, h // 8
+    rng = np.random.default_rng(3)
+    mv_in = rng.integers(-3, 4, (1, bx * by, 2)).astype(np.int32)
+    out, _ = oracle._truemotion_once(pyr, w, h, 2, 0, [1], mv_in, None, blksize=16, overlap=8, field_lambda=1.0,
+                                     thsad=5.12, sad_floor=0.0, reads_floor=True, confidence=False,
+                                     changes_in=np.zeros(bx * by, np.uint32))
+    assert np.array_equal(out, mv_in)
+    flags = np.zeros(bx * by, np.uint32)
+    changes = np.zeros(bx * by, np.uint32)
+    flags[2 * bx + 3] = 1
+    out2, _ = oracle._truemotion_once(pyr, w, h, 2, 0, [1], mv_in, None, blksize=16, overlap=8, field_lambda=1.0,
+                                      thsad=5.12, sad_floor=0.0, reads_floor=True, confidence=False,
+                                      changes_in=flags, changes_out=changes)
+    full, _ = oracle._truemotion_once(pyr, w, h, 2, 0, [1], mv_in, None, blksize=16, overlap=8, field_lambda=1.0,
+                                      thsad=5.12, sad_floor=0.0, reads_floor=True, confidence=False)
+    near = {(r * bx + c) for r in range(1, 4) for c in range(2, 5)}
+    for b in range(bx * by):
+        want = full[0, b] if b in near else mv_in[0, b]
+        assert tuple(out2[0, b]) == tuple(want), b
+        assert changes[b] == (0 if tuple(out2[0, b]) == tuple(mv_in[0, b]) else 1)
