@@ -273,6 +273,7 @@ class NlmPass final : public Pass {
             cfg.search_radius = static_cast<int>(params_.motion.search.search_radius);
             cfg.levels = static_cast<int>(params_.motion.search.pyramid_levels);
             cfg.thsad = mc_thsad();
+            cfg.ceiling = mc_ceiling_;
         }
         return noise_.allocate(cfg);
     }

@@ -126,6 +126,7 @@ struct NoiseFrontConfig {
     bool motion = false;  // read each frame along the motion to the frame before it
     int blksize = 16, overlap = 8, search_radius = 4, levels = 2;
     float thsad = 0.0f;
+    int ceiling = 0;  // the search's escalation ceiling (lookahead.rs:505-515); 0: no escalation
 };
 
 class NoiseFront {
@@ -163,9 +164,9 @@ class NoiseFront {
     cudaEvent_t ingested_ = nullptr, read_done_ = nullptr;
     bool reads_queued_ = false;
     size_t capacity_ = 0, pushed_ = 0, released_ = 0, recorded_ = 0;
-    int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2;
+    int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2, conf_stride_ = 1;
     DeviceBuffer lookahead_, partials_, records_, scratch_, history_records_, history_results_, settings_, state_,
-        derived_, spatial_, pilot_, pyramid_, pair_;
+        derived_, spatial_, pilot_, pyramid_, pair_, escalation_;
 };
 
 // NL4D pass over one plane group (nl4d_pass.cpp).

@@ -319,6 +319,7 @@ class Nl4dPass final : public Pass {
             cfg.search_radius = static_cast<int>(opts_.motion.search_radius);
             cfg.levels = static_cast<int>(opts_.motion.pyramid_levels);
             cfg.thsad = thsad_;
+            cfg.ceiling = ceiling_;
             if (auto f = noise_.allocate(cfg)) return f;
         }
         return std::nullopt;

@@ -87,6 +87,11 @@ std::optional<Failure> NoiseFront::allocate(const NoiseFrontConfig& cfg) {
         if ((e = pyramid_.alloc(static_cast<size_t>(pyr) * sizeof(float))) != cudaSuccess)
             return fail("look-ahead pyramid", e);
         if ((e = pair_.alloc(2 * mv_stride_ * sizeof(int32_t))) != cudaSuccess) return fail("look-ahead pair", e);
+        if (cfg.ceiling > cfg.search_radius) {
+            conf_stride_ = static_cast<int>(pad8(static_cast<int64_t>(blocks_x_) * blocks_y_));
+            if ((e = escalation_.alloc(escalation_state_floats(1, conf_stride_) * sizeof(float))) != cudaSuccess)
+                return fail("look-ahead escalation state", e);
+        }
     }
     return std::nullopt;
 }
@@ -102,7 +107,9 @@ std::optional<size_t> NoiseFront::take_oldest() {
 }
 
 // One direction of the look-ahead pair between two held frames: `centre`'s blocks matched in
-// `neighbour` (lookahead.rs:460-541, without escalation, camera-model seeds or truemotion).
+// `neighbour` (lookahead.rs:460-541, without camera-model seeds or truemotion). A search that
+// escalates measures its own floor: the look-ahead's noise words belong to no window (lookahead.rs:
+// 509-515).
 std::optional<Failure> NoiseFront::search(size_t centre_frame, size_t neighbour_frame, int direction,
                                           cudaStream_t s) {
     MotionLaunch m{};
@@ -127,6 +134,12 @@ std::optional<Failure> NoiseFront::search(size_t centre_frame, size_t neighbour_
     m.conf_stride = 1;
     m.sad_floor_word = 4;
     m.thsad = cfg_.thsad;
+    if (escalation_.ptr) {
+        m.escalation = escalation_.as<float>();
+        m.ceiling = cfg_.ceiling;
+        m.conf_stride = conf_stride_;
+        m.esc_reads_floor = 0;
+    }
     cudaError_t e = launch_motion_search(m, s);
     if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("look-ahead search launch", e)};
     return std::nullopt;

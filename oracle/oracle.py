@@ -1035,7 +1035,7 @@ def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: 
 
 
 def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, height: int, *, blksize: int,
-                      overlap: int, search_radius: int, levels: int):
+                      overlap: int, search_radius: int, levels: int, thsad: float = 0.0, ceiling: int = 0):
     """Every frame's reading as a motion-compensated look-ahead takes it
     (nlmeans/denoiser/lookahead.rs:283-319, 425-458, 543-605): frame i >= 1 is searched against
     frame i - 1 (newer to older) and read along that field; frame 1 is also searched older to newer
@@ -1043,7 +1043,9 @@ def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, heigh
     (readings, Immerkaer totals)."""
     step = blksize - overlap
     mb = (max(-(-width // step), 1), max(-(-height // step), 1))
-    kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels)
+    # With `ceiling` the pair searches escalate, measuring their own floor (lookahead.rs:509-515).
+    kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=thsad,
+              ceiling=ceiling)
     rec_len = stats_blocks(width, height)[0] * stats_blocks(width, height)[1] * noise_record_len(channels)
     readings, totals, lows = [], [], []
     for i, f in enumerate(frames):

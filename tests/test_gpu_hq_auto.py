@@ -152,9 +152,9 @@ def test_hq_auto_with_the_pilot(oracle, w, h, n, d, a, s, scale, conf):
     print(par.check(min_raw=0.95))
 
 
-@pytest.mark.parametrize("w,h,n,d,est", [(112, 72, 11, 1, "auto"), (96, 64, 12, 3, "auto"),
-                                         (88, 56, 6, 2, "chained")])
-def test_hq_auto_with_motion_compensation(oracle, w, h, n, d, est):
+@pytest.mark.parametrize("w,h,n,d,est,ceiling", [(112, 72, 11, 1, "auto", 0), (96, 64, 12, 3, "auto", 0),
+                                                 (88, 56, 6, 2, "chained", 0), (96, 64, 9, 2, "auto", 8)])
+def test_hq_auto_with_motion_compensation(oracle, w, h, n, d, est, ceiling):
     """The look-ahead reads each frame along its motion to the frame before it (as NL4D's does);
     each window's fold gives h2, the offsets and the window search's SAD floor, per unit sigma
     sad_noise_floor(16, 1) (nlmeans/denoiser/noise.rs:226-229); the search scores confidence against
@@ -162,7 +162,8 @@ def test_hq_auto_with_motion_compensation(oracle, w, h, n, d, est):
     fmt = avd.SampleFormat.u8()
     frames = clip(w, h, n, seed=700 + n + d, sigma=7.0)
     estimation = avd.MotionEstimation.CHAINED if est == "chained" else avd.MotionEstimation.AUTO
-    ms = avd.MotionSearch(estimation=estimation)
+    # With a ceiling the window search and the look-ahead's pair searches escalate.
+    ms = avd.MotionSearch(estimation=estimation, max_search_escalation=max(4, ceiling))
     mode = avd.DenoisingMode.temporal(d)
     opts = avd.NlmeansOptions(motion_compensation=avd.MotionCompensationMode(ms),
                               tuning=avd.NlmTuning(search_radius=3, patch_radius=2), mode=mode)
@@ -171,7 +172,8 @@ def test_hq_auto_with_motion_compensation(oracle, w, h, n, d, est):
     got = Runner(spec).run(frames)
     strength = avd.hq_default_strength(1, d)
     f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
-    readings, totals = oracle.noise_readings_mc(f32, 1, w, h, blksize=16, overlap=8, search_radius=4, levels=2)
+    readings, totals = oracle.noise_readings_mc(f32, 1, w, h, blksize=16, overlap=8, search_radius=4, levels=2,
+                                                thsad=oracle.thsad(16, 1.0), ceiling=ceiling)
     fl = np.float32
     settings = oracle.fold_words(w, h, h2_per_inverse_variance=oracle.h2_inv_norm(float(fl(strength) * fl(255.0)), 2),
                                  h2_fixed=oracle.h2_inv_norm(strength, 2),
@@ -184,7 +186,7 @@ def test_hq_auto_with_motion_compensation(oracle, w, h, n, d, est):
         return float(dv[6]), float(dv[8]), folds[frame][2], float(dv[4])
 
     chained = est == "chained" or d >= 3
-    kw = dict(confidence=True, chained=chained, derived=derived)
+    kw = dict(confidence=True, chained=chained, derived=derived, ceiling=ceiling)
     outs = oracle.nlm_stream_mc(f32, d, 3, 2, 0.0, **kw)
     exact = oracle.nlm_stream_mc(f32, d, 3, 2, 0.0, fp64=True, **kw)
     want = [oracle.egress(o, fmt.kind, fmt.max_value(), 0.0) for o in outs]
