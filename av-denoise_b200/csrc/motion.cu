@@ -145,6 +145,10 @@ struct SearchArgs {
     const float* noise;
     int sad_floor_word;
     float thsad;
+    // Fine only, with escalation: the state the first pass records for it (escalate.rs:84-155):
+    // sections `esc_section` floats apart of kept SAD, edge bar, and first-window centre x and y.
+    float* esc_state;
+    int64_t esc_section;
 };
 
 // Winner of one window around (cdx, cdy): the reference's `search_window` for a single centre.
@@ -371,6 +375,21 @@ __global__ void __launch_bounds__(Blocked<BLK, R>::kWarps * 32) blocked_kernel(S
     }
     mv_fine[0] = dx;
     mv_fine[1] = dy;
+    if (a.esc_state) {
+        // block_match.rs:783-796: a winner on the window's outer ring records the lowest SAD off
+        // the ring as its edge bar.
+        float bar = 0.0f;
+        if (abs(dx - cdx) == R || abs(dy - cdy) == R) {
+            bar = kNoSad;
+            for (int y = 1; y < B::kSide - 1; ++y)
+                for (int x = 1; x < B::kSide - 1; ++x) bar = fminf(bar, sad_buf[warp][y * B::kSide + x]);
+        }
+        const int64_t slot = static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx;
+        a.esc_state[slot] = sad;
+        a.esc_state[a.esc_section + slot] = bar;
+        a.esc_state[2 * a.esc_section + slot] = static_cast<float>(cdx);
+        a.esc_state[3 * a.esc_section + slot] = static_cast<float>(cdy);
+    }
     if (a.confidence) {
         const float floor = a.noise[a.sad_floor_word];
         float excess = __fsub_rn(sad, floor);
@@ -910,10 +929,19 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     e.reads_floor = m.esc_reads_floor;
     e.thsad = m.thsad;
     e.state = m.escalation;
-    const dim3 rows((blocks_x + 127) / 128, blocks_y, m.neighbours);
-    record_centres_kernel<<<rows, 128, 0, s>>>(e);
-    if (cudaError_t err = dispatch_search(m.search_radius, false, a, grid, s)) return err;
-    if (cudaError_t err = launch_radius_kernel<TrackLaunch, 0>(m.search_radius, e, grid, s)) return err;
+    // The register-blocked fine kernel records the state itself; the other fine kernels are followed
+    // by the first window again.
+    const bool blocked = m.search_radius >= 1 && (m.blksize == 8 || m.blksize == 16 || m.blksize == 32);
+    if (blocked) {
+        a.esc_state = e.state;
+        a.esc_section = static_cast<int64_t>(m.neighbours) * m.conf_stride;
+        if (cudaError_t err = dispatch_search(m.search_radius, false, a, grid, s)) return err;
+    } else {
+        const dim3 rows((blocks_x + 127) / 128, blocks_y, m.neighbours);
+        record_centres_kernel<<<rows, 128, 0, s>>>(e);
+        if (cudaError_t err = dispatch_search(m.search_radius, false, a, grid, s)) return err;
+        if (cudaError_t err = launch_radius_kernel<TrackLaunch, 0>(m.search_radius, e, grid, s)) return err;
+    }
     floor_kernel<<<1, kFloorThreads, 0, s>>>(e);
     flag_kernel<<<dim3((blocks_x + 63) / 64, blocks_y, m.neighbours), 64, 0, s>>>(e);
     return launch_radius_kernel<EscalateLaunch, 0>(m.ceiling, e, grid, s);

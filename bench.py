@@ -616,7 +616,8 @@ def run_prefilters(pushes: int) -> None:
 def run_motion_compensated(pushes: int) -> None:
     """NLMeans with motion compensation on the headline luma pass: 1920x1080 u8 luma, d=2, a=5, s=2,
     strength 8, default motion search (blksize 16, overlap 8, radius 4, 2 levels, Direct at d=2 with
-    the truemotion stage), plain and then NLMeans-HQ with a pinned sigma and temporal confidence.
+    the truemotion stage), plain, with escalation to 8, and NLMeans-HQ with a pinned sigma and
+    temporal confidence.
     Prints the steady-state device time per frame of each as one JSON line."""
     import numpy as np
     import torch
@@ -637,10 +638,14 @@ def run_motion_compensated(pushes: int) -> None:
     t = avd.NlmTuning(search_radius=LUMA["a"], patch_radius=LUMA["s"], strength=LUMA["strength"])
     mode = avd.DenoisingMode.temporal(LUMA["d"])
     mc = avd.MotionCompensationMode(avd.MotionSearch())
+    # The slow presets' search: failing blocks widen from radius 4 to 8 (motion/escalate.rs).
+    mc_slow = avd.MotionCompensationMode(avd.MotionSearch(max_search_escalation=8))
     cases = {
         "plain": avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(tuning=t, mode=mode)),
         "motion compensated": avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(motion_compensation=mc, tuning=t,
                                                                            mode=mode)),
+        "motion compensated, escalation to 8": avd.NlmeansAlgorithm.fast(avd.NlmeansOptions(
+            motion_compensation=mc_slow, tuning=t, mode=mode)),
         "HQ pinned sigma 8 codes, confidence, motion compensated": avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(
             nlm=avd.NlmeansOptions(motion_compensation=mc, tuning=avd.NlmTuning(search_radius=LUMA["a"],
                                                                                patch_radius=LUMA["s"]), mode=mode),
