@@ -142,7 +142,7 @@ class AvdWindowSpan(C.Structure):
 
 
 class AvdEngineTiming(C.Structure):
-    _fields_ = [("device_time", C.c_double), ("frames", u64)]
+    _fields_ = [("device_time", C.c_double), ("frames", u64), ("exact_samples", u64)]
 
 
 class AvdPassTimings(C.Structure):
@@ -265,6 +265,7 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_nlm_backward": (C.c_int, [_P(AvdNlmBackward), C.c_void_p]),
     "avd_nlm_window_scratch_bytes": (u64, [u32]),
     "avd_nlm_window": (C.c_int, [_P(AvdNlmBackward), C.c_void_p]),
+    "avd_exp_mirror": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p]),
     "avd_batch_scratch_bytes": (u64, [C.c_size_t, u32]),
     "avd_batch_submit": (C.c_int, [_P(AvdBatchJob), C.c_size_t, u32, u32, u32, f32, u64, C.c_void_p]),
     "avd_nlm_frame_static": (C.c_int, [_P(AvdNlmeansAlgorithm), u32, u32, u32, AvdSampleFormat, AvdSampleFormat,

@@ -531,6 +531,7 @@ class WindowSpan:
 class EngineTiming:
     device_time: float
     frames: int
+    exact_samples: int = 0  # samples the exact finish recomputed over the sampled frames
 
 
 @dataclass
@@ -600,8 +601,9 @@ class Engine:
     def timing(self) -> PassTimings:
         out = _abi.AvdPassTimings()
         self._check(self._lib.avd_engine_timing(self._h, C.byref(out)))
-        luma = EngineTiming(out.luma.device_time, out.luma.frames) if out.has_luma else None
-        chroma = EngineTiming(out.chroma.device_time, out.chroma.frames) if out.has_chroma else None
+        luma = EngineTiming(out.luma.device_time, out.luma.frames, out.luma.exact_samples) if out.has_luma else None
+        chroma = (EngineTiming(out.chroma.device_time, out.chroma.frames, out.chroma.exact_samples)
+                  if out.has_chroma else None)
         return PassTimings(luma, chroma)
 
     def sample_device_time(self, every: int) -> None:
@@ -630,9 +632,11 @@ class Engine:
 
 @dataclass
 class TuningConfig:
-    """tune/setup.rs (`TuningConfig`): kept for API parity."""
+    """tune/config.rs:66-75 (`TuningConfig`). `deterministic`: every NLMeans sample in the exact
+    order of the reference's baseline, bit-identical to the CPU restatement on float outputs too
+    (slower); integer outputs match it either way."""
 
-    deterministic: bool = True
+    deterministic: bool = False
 
 
 def build_engine(spec: EngineSpec, tuning: Optional[TuningConfig] = None) -> Engine:

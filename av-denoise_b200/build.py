@@ -38,8 +38,10 @@ COMMON = [
 # Per-file flags. The NL4D collaborative filter rounds every multiply and add on its own, as its CPU
 # restatement does (built with -ffp-contract=off), so its member choices and threshold decisions
 # agree bit for bit; -fmad=false keeps nvcc from fusing any of them. The noise estimate does the same
-# for its reading and fold words, and the truemotion stage for its costs and confidences.
-PER_FILE = {"collab.cu": ["-fmad=false"], "noise_estimate.cu": ["-fmad=false"], "truemotion.cu": ["-fmad=false"]}
+# for its reading and fold words, the truemotion stage for its costs and confidences, and the exact
+# NLMeans finish for its distances, weights and sums.
+PER_FILE = {"collab.cu": ["-fmad=false"], "noise_estimate.cu": ["-fmad=false"], "truemotion.cu": ["-fmad=false"],
+            "nlm_exact.cu": ["-fmad=false"]}
 
 
 def _sources() -> list[Path]:
@@ -50,11 +52,30 @@ def _headers() -> list[Path]:
     return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h")))
 
 
+def _local_includes(src: Path, seen: set[Path] | None = None) -> set[Path]:
+    """The in-tree headers `src` includes, followed recursively (quoted includes only)."""
+    seen = set() if seen is None else seen
+    for line in src.read_text().splitlines():
+        line = line.strip()
+        if not line.startswith("#include \""):
+            continue
+        name = line.split('"')[1]
+        for base in (src.parent, CSRC, ROOT / "include"):
+            hdr = base / name
+            if hdr.exists():
+                if hdr not in seen:
+                    seen.add(hdr)
+                    _local_includes(hdr, seen)
+                break
+    return seen
+
+
 def _needs(obj: Path, src: Path, headers: list[Path]) -> bool:
     if not obj.exists():
         return True
     t = obj.stat().st_mtime
-    return src.stat().st_mtime > t or any(h.stat().st_mtime > t for h in headers)
+    deps = _local_includes(src) & set(headers)
+    return src.stat().st_mtime > t or any(h.stat().st_mtime > t for h in deps)
 
 
 def _compile(src: Path, extra: list[str]) -> Path:

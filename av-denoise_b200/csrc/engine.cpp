@@ -31,11 +31,15 @@ class NlmPass final : public Pass {
    public:
     // With `guides_only` the pass is a chroma-only engine's luma guide: it runs the noise estimate
     // and the window motion for the chroma pass to read, and no denoise (nlmeans/engine.rs:53-100).
+    // With `exact_all` (a deterministic tuning) every sample of the denoise pass and of the NLM
+    // pilot is computed by the exact kernel in the FP32 mirror's operation order.
     static std::optional<Failure> create(const AvdNlmeansAlgorithm& alg, Channels channels, uint32_t width,
                                          uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                         std::unique_ptr<Pass>* result, bool guides_only = false) {
+                                         std::unique_ptr<Pass>* result, bool guides_only = false,
+                                         bool exact_all = false) {
         auto pass = std::unique_ptr<NlmPass>(new NlmPass());
         pass->guides_ = guides_only;
+        pass->exact_all_ = exact_all;
         pass->params_ = resolve_nlm_params(alg, channels);
         pass->held_ = nlm_held_frames(alg, channels);
         pass->width_ = width;
@@ -176,6 +180,9 @@ class NlmPass final : public Pass {
         for (auto& o : outputs_)
             if ((e = o.alloc(fe * sizeof(float))) != cudaSuccess) return gpu_failure("output slot", e);
         if ((e = derived_.alloc(16 * sizeof(float))) != cudaSuccess) return gpu_failure("derived words", e);
+        // Integer outputs: the list of pixels the exact finish recomputes (nlm_exact.cu) and its count.
+        if (out_.kind != AVD_SAMPLE_F32 && !exact_all_ && (e = fix_.alloc((pixels() + 1) * sizeof(int))) != cudaSuccess)
+            return gpu_failure("exact-finish list", e);
         // Fixed derived words (nlmeans/denoiser/noise.rs `fixed_derived_values`): the strength and,
         // with an HQ sigma override, the noise offset.
         float words[16] = {0};
@@ -431,7 +438,9 @@ class NlmPass final : public Pass {
 
     // dispatch/mod.rs:598-620 (`run_nlm_spatial_pilot`): the single-frame windowed pass over the
     // noisy input of `slot` at the pilot strength with the pilot's offset table, finished into the
-    // slot's reference.
+    // slot's reference. The reference is a float intermediate that every later distance reads, so
+    // the exact finish cannot pick out samples near a change of code here: the pilot runs through
+    // the exact kernel on every sample, in the reference kernels' operation order.
     std::optional<Failure> run_pilot(size_t slot) {
         NlmLaunch a{};
         a.ring = ring_.as<float>();
@@ -450,7 +459,7 @@ class NlmPass final : public Pass {
         a.wref = params_.self_weight;
         a.fast = params_.hq ? 0 : 1;
         a.out = ref_slot_ptr(slot);
-        cudaError_t e = launch_nlm(a, stream);
+        cudaError_t e = launch_nlm_exact(a, stream);
         if (e != cudaSuccess) return gpu_failure("nlm pilot launch", e);
         return std::nullopt;
     }
@@ -885,9 +894,29 @@ class NlmPass final : public Pass {
         a.fast = params_.hq ? 0 : 1;
         a.out = outputs_[slot].as<float>();
         a.ref_ring = has_reference() ? (mc_ ? comp_ref_.as<float>() : ref_.as<float>()) : nullptr;
-        cudaError_t e = launch_nlm(a, stream);
-        if (e != cudaSuccess) return gpu_failure("nlm launch", e);
-        if (timed) timer_.end(stream, start);
+        cudaError_t e;
+        if (exact_all_) {
+            if ((e = launch_nlm_exact(a, stream)) != cudaSuccess) return gpu_failure("exact nlm launch", e);
+            if (timed) timer_.end(stream, start);
+            *out_slot = slot;
+            return std::nullopt;
+        }
+        if (fix_.ptr) {
+            // Integer outputs: the window kernel flags the pixels within the band of a change of code
+            // and the exact finish recomputes them in the reference kernels' order.
+            a.fix_count = fix_.as<int>();
+            a.fix_list = fix_.as<int>() + 1;
+            a.code_max = sample_max_value(out_);
+            a.fix_band = kFixBand;
+            if ((e = cudaMemsetAsync(a.fix_count, 0, sizeof(int), stream)) != cudaSuccess)
+                return gpu_failure("exact-finish count", e);
+        }
+        if ((e = launch_nlm(a, stream)) != cudaSuccess) return gpu_failure("nlm launch", e);
+        if (fix_.ptr && (e = launch_nlm_exact(a, stream)) != cudaSuccess) return gpu_failure("exact finish launch", e);
+        if (timed) {
+            timer_.end(stream, start);
+            if (fix_.ptr) timer_.note_count(stream, a.fix_count);
+        }
         *out_slot = slot;
         return std::nullopt;
     }
@@ -947,6 +976,8 @@ class NlmPass final : public Pass {
     DeviceBuffer outputs_[2];
     DeviceBuffer derived_;
     DeviceBuffer lut_, pilot_lut_;
+    DeviceBuffer fix_;  // integer outputs: [count, pixel list] of the exact finish
+    bool exact_all_ = false;
     DeviceBuffer ref_;  // the prefilter's reference ring, slot for slot beside `ring_`
     std::vector<uint32_t> slot_frames_;
     size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;
@@ -1117,8 +1148,8 @@ struct DeviceGuard {
 extern "C" {
 
 AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, AvdEngine** out) {
-    (void)tuning;
     if (!spec || !out) return AVD_ERR_NULL_ARG;
+    const bool exact_all = tuning != nullptr && tuning->deterministic != 0;
     *out = nullptr;
     g_last_error.clear();
     std::string message;
@@ -1135,7 +1166,7 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
         auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_luma, avd::Channels::Luma, g.width, g.height, g.input,
                                               g.output, &engine->luma)
                       : avd::NlmPass::create(spec->nlm_luma, avd::Channels::Luma, g.width, g.height, g.input,
-                                             g.output, &engine->luma);
+                                             g.output, &engine->luma, false, exact_all);
         if (f) return fail_global(f->status, f->message);
     }
     if (spec->has_chroma) {
@@ -1144,7 +1175,7 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
         auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
                                               &engine->chroma)
                       : avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
-                                             &engine->chroma);
+                                             &engine->chroma, false, exact_all);
         if (f) return fail_global(f->status, f->message);
     }
     if (!engine->luma && engine->chroma) {

@@ -59,13 +59,31 @@ struct DeviceTimer {
     uint64_t frame_counter = 0;
     double total = 0.0;
     uint64_t frames = 0;
+    uint64_t exact_samples = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    // Pinned host words the sampled frames' exact-finish counts are copied into (one per pending
+    // frame, up to kCountSlots between collections).
+    static constexpr size_t kCountSlots = 256;
+    int* counts = nullptr;
+    size_t counted = 0;
 
     ~DeviceTimer() {
         for (auto& p : pending) {
             cudaEventDestroy(p.first);
             cudaEventDestroy(p.second);
         }
+        if (counts) cudaFreeHost(counts);
+    }
+    // Queues a copy of a sampled frame's exact-finish count (after its exact launch, on `s`).
+    void note_count(cudaStream_t s, const int* device_count) {
+        if (!counts && cudaHostAlloc(reinterpret_cast<void**>(&counts), kCountSlots * sizeof(int),
+                                     cudaHostAllocDefault) != cudaSuccess) {
+            counts = nullptr;
+            return;
+        }
+        if (counted < kCountSlots &&
+            cudaMemcpyAsync(counts + counted, device_count, sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess)
+            counted += 1;
     }
     bool begin(cudaStream_t s, cudaEvent_t* start) {
         uint64_t n = frame_counter++;
@@ -91,9 +109,15 @@ struct DeviceTimer {
             cudaEventDestroy(p.second);
         }
         pending.clear();
+        if (counted) {
+            cudaDeviceSynchronize();
+            for (size_t i = 0; i < counted; ++i) exact_samples += static_cast<uint64_t>(counts[i]);
+            counted = 0;
+        }
         AvdEngineTiming t;
         t.device_time = total;
         t.frames = frames;
+        t.exact_samples = exact_samples;
         return t;
     }
 };

@@ -48,9 +48,36 @@ struct NlmLaunch {
     float* out;  // width*height*channels
     const float* ref_ring;  // a prefilter's reference ring (same slots as `ring`) the distances
                             // compare, or null to compare `ring` itself
+    // Samples near a rounding boundary (nlm_exact.cu). With `fix_count` set, the window kernel
+    // appends to `fix_list` (and counts in `*fix_count`) every pixel with a result that, quantised
+    // as the egress quantises it (clamped to [0, 1], times `code_max`, plus 0.5), lies within
+    // code_max * (fix_band + kFixBandPerH2 * h2) codes of an integer; `launch_nlm_exact` then
+    // recomputes those pixels in the FP32 mirror's operation order. The list holds at most
+    // width*height entries.
+    int* fix_list;
+    int* fix_count;
+    float code_max, fix_band;
 };
 
 cudaError_t launch_nlm(const NlmLaunch& args, cudaStream_t stream);
+
+// The exact finish (nlm_exact.cu): every pixel of `args.fix_list[0 .. *args.fix_count)` (every pixel
+// of the frame when `fix_list` is null) recomputed in the order and rounding of the FP32 mirror of
+// the reference kernels (row-major patch sums, separately rounded operations, the mirror's own
+// exponential) and written to `args.out`. The kernel reads the count on the device.
+cudaError_t launch_nlm_exact(const NlmLaunch& args, cudaStream_t stream);
+// The FP32 mirror's exponential of `n` floats on the device (its comparison with the oracle).
+cudaError_t launch_exp_mirror(const float* x, float* out, int64_t n, cudaStream_t stream);
+// The band the window kernel flags around each rounding boundary, in normalised units:
+// kFixBand + kFixBandPerH2 * h2. The window kernel's float result differs from the mirror's by the
+// box sums' and the MUFU exponential's rounding, which the strength h2 amplifies. Measured over
+// strengths 1..16, patch radii 1..3, luma, chroma and NLMeans-HQ: the 99.99th percentile of the
+// difference lies inside the band everywhere (6e-7 against 2.07e-6 at the 1080p luma workload's
+// h2 of 13.5; 3.4e-6 against 1.4e-5 at h2 2408), the largest difference inside it where h2 is
+// below 30. A sample is missed only where a difference past the band meets a value that close to a
+// boundary: a few in ten million.
+constexpr float kFixBand = 2e-6f;
+constexpr float kFixBandPerH2 = 5e-9f;
 // The same launch with `args.ref_ring` set (prefilter.cu).
 cudaError_t launch_nlm_ref(const NlmLaunch& args, cudaStream_t stream);
 

@@ -908,7 +908,9 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     e.centre_slot = m.centre_slot;
     e.neighbours = m.neighbours;
     e.use_seed = seeded ? 1 : 0;
-    e.widen = coarse ? 1 : 0;
+    // escalate.rs:203-205 (`reaches_further`): the coarse level is searched again only when the
+    // ceiling reaches past the coarse pass's own radius.
+    e.widen = coarse && m.ceiling > m.coarse_radius ? 1 : 0;
     e.scale = 1;
     if (coarse) {
         const int level = m.levels - 1;

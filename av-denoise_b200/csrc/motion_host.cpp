@@ -292,3 +292,14 @@ AvdStatus avd_nlm_window(const AvdNlmBackward* p, void* stream) {
 }
 
 }  // extern "C"
+
+AvdStatus avd_exp_mirror(uint64_t x, uint64_t out, uint64_t n, void* stream) {
+    if ((x == 0 || out == 0) && n > 0) return AVD_ERR_NULL_ARG;
+    cudaError_t e = avd::launch_exp_mirror(reinterpret_cast<const float*>(x), reinterpret_cast<float*>(out),
+                                           static_cast<int64_t>(n), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        avd_set_last_error(cudaGetErrorString(e));
+        return AVD_ERR_GPU;
+    }
+    return AVD_OK;
+}

@@ -10,12 +10,15 @@
 //
 // The array is shared by every call on a device and keeps the last call's contents. Every word a
 // call reads is first written by the same call (the frames by the ingest, the result by the
-// window kernel, the strength words by a one-thread kernel), so nothing has to be cleared, but
-// two calls whose GPU work overlaps (two streams, or two host threads) race on the array.
+// window kernel, the strength words by a one-thread kernel), except the count of samples the exact
+// finish recomputes, which each call clears first; two calls whose GPU work overlaps (two streams,
+// or two host threads) race on the array.
 //
-// The array's address for host code comes from cudaGetSymbolAddress, taken once per device with
-// that device current, on the first call made on it; make that first call before any stream
-// capture.
+// The array's address for host code comes from cudaGetSymbolAddress, taken with the device
+// current on the first call made in each CUDA context on that device (the process's primary
+// context, an application's own context, or the new primary context after a cudaDeviceReset: a
+// context is told apart by its driver-issued id, which is never reused); make that first call
+// before any stream capture.
 
 #include <cuda_runtime.h>
 
@@ -33,7 +36,8 @@ namespace avd {
 
 namespace {
 
-// 32 MiB: the frames, result and 64 strength words of one call must fit.
+// 32 MiB: the frames, result, 64 strength words and (integer outputs) the exact finish's count and
+// pixel list of one call must fit.
 constexpr size_t kStaticScratchBytes = size_t(32) << 20;
 constexpr size_t kStaticScratchFloats = kStaticScratchBytes / sizeof(float);
 constexpr size_t kWordsFloats = 64;
@@ -42,7 +46,18 @@ constexpr int kMaxDevices = 64;
 __device__ __align__(256) float g_nlm_scratch[kStaticScratchFloats];
 
 std::mutex g_setup_mutex;
-float* g_scratch_ptr[kMaxDevices] = {};
+struct SetupRecord {
+    unsigned long long context_id;  // the CUDA context the address was taken in (0: none yet)
+    float* ptr;
+};
+SetupRecord g_setup[kMaxDevices] = {};
+
+// cuCtxGetCurrent and cuCtxGetId, reached through the runtime so the library needs no link to the
+// driver library; resolved once.
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
 
 __global__ void write_strength_words(float* words, float h2, float offset) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -56,20 +71,48 @@ AvdStatus fail(AvdStatus st, const std::string& m) {
     return st;
 }
 
-// The device address of the scratch array on the current device, taken once per device.
+// The id of the calling thread's current CUDA context (0 when none is bound yet). Caller holds
+// g_setup_mutex.
+cudaError_t current_context_id(unsigned long long* id) {
+    if (g_ctx_get_current == nullptr || g_ctx_get_id == nullptr) {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0{}, q1{};
+        cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000, cudaEnableDefault, &q0);
+        if (e == cudaSuccess) e = cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return e;
+        if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return cudaErrorSymbolNotFound;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f1);
+    }
+    void* ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != 0) return cudaErrorDeviceUninitialized;
+    *id = 0;
+    if (ctx != nullptr && g_ctx_get_id(ctx, id) != 0) return cudaErrorDeviceUninitialized;
+    return cudaSuccess;
+}
+
+// The device address of the scratch array in the current context of the current device, taken
+// once per device and context.
 cudaError_t scratch_for_current_device(float** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (g_scratch_ptr[dev] == nullptr) {
+    unsigned long long id = 0;
+    if ((e = current_context_id(&id)) != cudaSuccess) return e;
+    SetupRecord& rec = g_setup[dev];
+    if (rec.ptr == nullptr || id == 0 || rec.context_id != id) {
         void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_nlm_scratch);
+        e = cudaGetSymbolAddress(&ptr, g_nlm_scratch);  // binds the primary context when none was
         if (e != cudaSuccess) return e;
-        g_scratch_ptr[dev] = static_cast<float*>(ptr);
+        if ((e = current_context_id(&id)) != cudaSuccess) return e;
+        rec.ptr = static_cast<float*>(ptr);
+        rec.context_id = id;
     }
-    *out = g_scratch_ptr[dev];
+    *out = rec.ptr;
     return cudaSuccess;
 }
 
@@ -115,7 +158,8 @@ extern "C" AvdStatus avd_nlm_frame_static(const AvdNlmeansAlgorithm* algorithm, 
     if (n_out != channels) return fail(AVD_ERR_PLANE_MISMATCH, "the output needs `channels` planes");
     const uint64_t pixels = static_cast<uint64_t>(width) * height;
     const uint64_t frame_elems = pixels * channels;
-    const uint64_t need = kWordsFloats + frame_elems * (frames + 1);
+    const bool integer_out = output.kind != AVD_SAMPLE_F32;
+    const uint64_t need = kWordsFloats + frame_elems * (frames + 1) + (integer_out ? pixels + 1 : 0);
     if (need > kStaticScratchFloats) {
         char m[256];
         std::snprintf(m, sizeof(m),
@@ -172,7 +216,18 @@ extern "C" AvdStatus avd_nlm_frame_static(const AvdNlmeansAlgorithm* algorithm, 
     a.wref = p.self_weight;
     a.fast = 1;
     a.out = result;
+    if (integer_out) {
+        // The exact finish of the samples near a change of code, as the engine runs it; the count
+        // is the one word of the array that must start at zero, so every call clears it.
+        a.fix_count = reinterpret_cast<int*>(result + frame_elems);
+        a.fix_list = a.fix_count + 1;
+        a.code_max = sample_max_value(output);
+        a.fix_band = kFixBand;
+        if ((e = cudaMemsetAsync(a.fix_count, 0, sizeof(int), s)) != cudaSuccess)
+            return fail(AVD_ERR_GPU, cudaGetErrorString(e));
+    }
     if ((e = launch_nlm(a, s)) != cudaSuccess) return fail(AVD_ERR_GPU, cudaGetErrorString(e));
+    if (integer_out && (e = launch_nlm_exact(a, s)) != cudaSuccess) return fail(AVD_ERR_GPU, cudaGetErrorString(e));
     void* o0 = reinterpret_cast<void*>(out[0].ptr);
     void* o1 = reinterpret_cast<void*>(out[channels - 1].ptr);
     e = launch_egress(result, o0, o1, static_cast<int64_t>(pixels), static_cast<int>(channels),

@@ -290,6 +290,25 @@ __device__ __forceinline__ void step(const Smem& sm, int A, const Lanes& ln, int
 
 extern __shared__ __align__(16) float smem_raw[];
 
+// Whether `v`, quantised as the egress does (engine/kernels.rs:103-153: clamped to [0, 1], times
+// the largest code, plus 0.5, truncated), lies within `band` codes of a change of code.
+__device__ __forceinline__ bool near_code_boundary(float v, float code_max, float band) {
+    const float t = fminf(fmaxf(v, 0.0f), 1.0f) * code_max + 0.5f;
+    const float f = t - floorf(t);
+    return f < band || f > 1.0f - band;
+}
+
+// Appends `pixel` to `list` where `near` holds: one atomic per warp. Every lane of the warp calls it.
+__device__ __forceinline__ void note_fix(bool near, int64_t pixel, int* list, int* count) {
+    const unsigned m = __ballot_sync(0xffffffffu, near);
+    if (m == 0) return;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (near) list[base + __popc(m & ((1u << lane) - 1u))] = static_cast<int>(pixel);
+}
+
 // Where a record tile writes instead of the output: per pixel out[2], 1/den (0 when the pixel
 // passes through), dL/dM and the argmax id, for upstream gradient `grad_out`; and the direct
 // centre-frame term dL/dout * wref M / den into `grad_centre`.
@@ -480,29 +499,37 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
 
     // Finish (accumulate.rs:175-201), written straight to the output frame.
     const int gx = X0 + col;
+    const bool flags = a.fix_count != nullptr;
+    const float band = a.code_max * (a.fix_band + kFixBandPerH2 * h2);
 #pragma unroll
     for (int k = 0; k < V; ++k) {
         const int gy = Y0 + y0 + k;
-        if (gx >= W || gy >= H) continue;
-        const float max_w = FAST ? ex2_approx(acc.m[k] * kk.x) : acc.m[k];
-        const float wsum = acc.ws[k].x + acc.ws[k].y;
-        // The centre value: the input's own (accumulate.rs:175-201 reads the input ring), which the
-        // reference-ring tile does not hold.
-        const float* orig = REF ? centre + ((int64_t)gy * W + gx) * C : sm.ctr + (y0 + k + S) * K::CSTRIDE + (col + S) * C;
-        const float self_weight = __fmul_rn(a.wref, max_w);
-        const float denom = __fadd_rn(self_weight, wsum);
-        float* dst = a.out + ((int64_t)gy * W + gx) * C;
-        if (denom > 1e-30f) {
-            const float inv = __frcp_rn(denom);
+        bool near = false;
+        if (gx < W && gy < H) {
+            const float max_w = FAST ? ex2_approx(acc.m[k] * kk.x) : acc.m[k];
+            const float wsum = acc.ws[k].x + acc.ws[k].y;
+            // The centre value: the input's own (accumulate.rs:175-201 reads the input ring), which
+            // the reference-ring tile does not hold.
+            const float* orig =
+                REF ? centre + ((int64_t)gy * W + gx) * C : sm.ctr + (y0 + k + S) * K::CSTRIDE + (col + S) * C;
+            const float self_weight = __fmul_rn(a.wref, max_w);
+            const float denom = __fadd_rn(self_weight, wsum);
+            float* dst = a.out + ((int64_t)gy * W + gx) * C;
+            if (denom > 1e-30f) {
+                const float inv = __frcp_rn(denom);
 #pragma unroll
-            for (int c = 0; c < C; ++c) {
-                const float sum_wi = acc.a[c][k].x + acc.a[c][k].y;
-                dst[c] = __fmul_rn(__fadd_rn(__fmul_rn(orig[c], self_weight), sum_wi), inv);
+                for (int c = 0; c < C; ++c) {
+                    const float sum_wi = acc.a[c][k].x + acc.a[c][k].y;
+                    const float v = __fmul_rn(__fadd_rn(__fmul_rn(orig[c], self_weight), sum_wi), inv);
+                    dst[c] = v;
+                    if (flags) near |= near_code_boundary(v, a.code_max, band);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < C; ++c) dst[c] = orig[c];  // passes through exactly
             }
-        } else {
-#pragma unroll
-            for (int c = 0; c < C; ++c) dst[c] = orig[c];
         }
+        if (flags) note_fix(near, (int64_t)gy * W + gx, a.fix_list, a.fix_count);
     }
 }
 

@@ -8,7 +8,8 @@
 //   out(p) = (sum w(o) I(p+o)) * (1 / sum w(o)).
 // A 32 x 8 CTA stages its (32+2r) x (8+2r) window once in shared memory, one thread per output
 // pixel. The sums are formed in the reference's order with every multiply and add rounded on its
-// own (no fused multiply-add), so only exp's last bits can differ from the CPU restatement.
+// own (no fused multiply-add) and the exponential is exp_mirror.cuh's, so the reference slot equals
+// the CPU restatement's bit for bit.
 //
 // The reference-ring NLM tile is the nlm.cu tile with two more shared tiles per pass for the input
 // values (nlm_tile.cuh, REF): the reference form of fused.rs:532-900.
@@ -18,6 +19,7 @@
 #include <cstdint>
 #include <mutex>
 
+#include "exp_mirror.cuh"
 #include "kernels.h"
 #include "nlm_tile.cuh"
 
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(kBx * kBy) bilateral_kernel(const float* __res
                 range_sq = __fadd_rn(range_sq, __fmul_rn(lane, lane));
             }
             const float spatial = __fmul_rn(static_cast<float>(dx * dx + dy * dy), inv_s);
-            const float w = expf(-__fadd_rn(spatial, __fmul_rn(range_sq, inv_r)));
+            const float w = exp_mirror(-__fadd_rn(spatial, __fmul_rn(range_sq, inv_r)));
 #pragma unroll
             for (int ch = 0; ch < C; ++ch) acc[ch] = __fadd_rn(acc[ch], __fmul_rn(nb[ch], w));
             wsum = __fadd_rn(wsum, w);

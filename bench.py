@@ -23,6 +23,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import tempfile
 import statistics
 import subprocess
 import sys
@@ -121,6 +122,29 @@ def plane_words(fmt, w, h):
     return fmt.plane_bytes(w * h) // 4
 
 
+def _words_u8(np, codes):
+    flat = codes.reshape(-1)
+    return np.concatenate([flat, np.zeros((-flat.size) % 4, np.uint8)]).view(np.int32)
+
+
+def oracle_frame(clip, k: int) -> tuple[list, float]:
+    """The oracle's output planes (Y, U, V codes) of frame k of the workload and the seconds it took:
+    the luma pass over the repeat-edge window of frame k, the chroma pass on frame k alone (FP32
+    mirror, OpenMP on every host thread)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    oracle.build()
+    n = len(clip)
+    t0 = time.perf_counter()
+    window = [oracle.ingest([clip[min(max(k + j, 0), n - 1)][0]], 0, 255.0) for j in range(-LUMA["d"], LUMA["d"] + 1)]
+    y = oracle.nlm_frame(window, LUMA["d"], LUMA["a"], LUMA["s"], oracle.h2_inv_norm(LUMA["strength"], LUMA["s"]))
+    uv = oracle.nlm_frame([oracle.ingest([clip[k][1], clip[k][2]], 0, 255.0)], 0, CHROMA["a"], CHROMA["s"],
+                          oracle.h2_inv_norm(CHROMA["strength"], CHROMA["s"]))
+    secs = time.perf_counter() - t0
+    return oracle.egress(y, 0, 255.0) + oracle.egress(uv, 0, 255.0), secs
+
+
 def run_gpu(args) -> None:
     import numpy as np
     import torch
@@ -146,19 +170,15 @@ def run_gpu(args) -> None:
     spec_l, spec_c = build_specs(avd)
     fmt = spec_l.geometry.input
     dims = [spec_l.geometry.plane_dims(i) for i in range(3)]
-    stream = torch.cuda.Stream()
+    # The luma and chroma engines run on two streams: chroma's short launches fill the luma
+    # launches' last wave.
+    sl, sc = torch.cuda.Stream(), torch.cuda.Stream()
     eng_l = avd.build_engine(spec_l)
     eng_c = avd.build_engine(spec_c)
-    eng_l.set_stream(stream.cuda_stream)
-    eng_c.set_stream(stream.cuda_stream)
+    eng_l.set_stream(sl.cuda_stream)
+    eng_c.set_stream(sc.cuda_stream)
 
-    def words_of(codes):
-        flat = codes.reshape(-1)
-        pad = (-flat.size) % 4
-        return np.concatenate([flat, np.zeros(pad, np.uint8)]).view(np.int32)
-
-    # Inputs resident in HBM.
-    dev_in = [[torch.from_numpy(words_of(p)).cuda() for p in f] for f in clip]
+    dev_in = [[torch.from_numpy(_words_u8(np, p)).cuda() for p in f] for f in clip]
     out = [torch.zeros(plane_words(fmt, w, h), dtype=torch.int32, device="cuda") for (w, h) in dims]
     scratch = [torch.zeros(plane_words(fmt, w, h), dtype=torch.int32, device="cuda") for (w, h) in dims]
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -170,31 +190,54 @@ def run_gpu(args) -> None:
     out_c = P([scratch[0], out[1], out[2]])
     planes_in = [P(f) for f in dev_in]
 
-    def step_device():
-        emitted = 0
-        for pl in planes_in:
-            rl = eng_l.push(pl)
-            rc = eng_c.push(pl)
-            for _ in range(rl):
-                eng_l.emit_into(out_l)
-                emitted += 1
-            for _ in range(rc):
-                eng_c.emit_into(out_c)
-        for _ in range(eng_l.finish()):
-            eng_l.emit_into(out_l)
-            emitted += 1
-        for _ in range(eng_c.finish()):
-            eng_c.emit_into(out_c)
-        return emitted
+    def step_device(capture: int = -1):
+        """One pass of the clip through both engines; with `capture`, also that frame's planes."""
+        got = {}
+        emitted_l = emitted_c = 0
 
-    launches_per_frame = 6  # per engine: ingest + nlm + egress
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step_device()
+        def emit_l():
+            nonlocal emitted_l
+            eng_l.emit_into(out_l)
+            if emitted_l == capture:
+                with torch.cuda.stream(sl):
+                    got["y"] = out[0].clone()
+            emitted_l += 1
+
+        def emit_c():
+            nonlocal emitted_c
+            eng_c.emit_into(out_c)
+            if emitted_c == capture:
+                with torch.cuda.stream(sc):
+                    got["uv"] = (out[1].clone(), out[2].clone())
+            emitted_c += 1
+
+        for pl in planes_in:
+            for _ in range(eng_l.push(pl)):
+                emit_l()
+            for _ in range(eng_c.push(pl)):
+                emit_c()
+        for _ in range(eng_l.finish()):
+            emit_l()
+        for _ in range(eng_c.finish()):
+            emit_c()
+        return emitted_l, got
+
+    def timed(fn):
+        e0, e1, ec = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(sl)
+        sc.wait_event(e0)
+        res = fn()
+        ec.record(sc)
+        sl.wait_event(ec)
+        e1.record(sl)
+        torch.cuda.synchronize()
+        return res, e0.elapsed_time(e1) / 1e3
+
+    for _ in range(args.warmup):
+        step_device()
     torch.cuda.synchronize()
 
-    clock_path = ROOT / "gpurun_out" / f"clocks_rank{rank}.csv"
-    clock_path.parent.mkdir(exist_ok=True)
+    clock_path = Path(tempfile.gettempdir()) / f"avd_bench_clocks_{os.getpid()}_rank{rank}.csv"
     proc = clocks_start(clock_path)
     eng_l.sample_device_time(1)
     times = []
@@ -203,90 +246,87 @@ def run_gpu(args) -> None:
         flush.fill_(1)
         torch.cuda.synchronize()
         barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        with torch.cuda.stream(stream):
-            n = step_device()
-        e1.record(stream)
-        torch.cuda.synchronize()
+        (n, _), t = timed(step_device)
         assert n == FRAMES
-        times.append(e0.elapsed_time(e1) / 1e3)
+        times.append(t)
     wall = time.perf_counter() - wall0
-    nlm_timing = eng_l.timing().luma
+    nlm_timing = eng_l.timing().luma  # window kernel + exact finish per luma frame
     eng_l.sample_device_time(0)
 
-    # End to end: pinned host frames -> device -> engines -> device -> pinned host.
-    host_in = [[torch.from_numpy(words_of(p)).pin_memory() for p in f] for f in clip]
+    # End to end: pinned host frames -> device -> engines -> device -> pinned host. Output frame k
+    # gathers its chroma when the chroma engine emits it (at push k) and its luma when the luma engine
+    # does (d pushes later); a 4-slot device ring holds it between.
+    host_in = [[torch.from_numpy(_words_u8(np, p)).pin_memory() for p in f] for f in clip]
     host_out = [[torch.empty(plane_words(fmt, w, h), dtype=torch.int32).pin_memory() for (w, h) in dims]
                 for _ in range(FRAMES)]
     stage = [[torch.empty(plane_words(fmt, w, h), dtype=torch.int32, device="cuda") for (w, h) in dims]
              for _ in range(2)]
     dout = [[torch.empty(plane_words(fmt, w, h), dtype=torch.int32, device="cuda") for (w, h) in dims]
             for _ in range(4)]
-    dscr = [torch.empty(plane_words(fmt, w, h), dtype=torch.int32, device="cuda") for (w, h) in dims]
+    dscr = [[torch.empty(plane_words(fmt, w, h), dtype=torch.int32, device="cuda") for (w, h) in dims]
+            for _ in range(2)]
     copy = torch.cuda.Stream()
     h2d_bytes = sum(t.numel() * 4 for f in host_in for t in f)
     d2h_bytes = sum(t.numel() * 4 for f in host_out for t in f)
 
     def step_e2e():
-        # Output frame k gathers its chroma when the chroma engine emits it (at push k) and its
-        # luma when the luma engine does (d pushes later); a 4-slot device ring holds it between.
-        free_in = [torch.cuda.Event() for _ in range(2)]
+        free_in = [[torch.cuda.Event() for _ in range(2)] for _ in range(2)]  # [slot][luma, chroma]
         free_out = [torch.cuda.Event() for _ in range(len(dout))]
-        for ev in free_in + free_out:
-            ev.record(stream)
-        luma_frame = 0
-        chroma_frame = 0
-
-        def drain(frame_idx):
-            o = frame_idx % len(dout)
-            done = torch.cuda.Event()
-            done.record(stream)
-            copy.wait_event(done)
-            with torch.cuda.stream(copy):
-                for i in range(3):
-                    host_out[frame_idx][i].copy_(dout[o][i], non_blocking=True)
-            free_out[o].record(copy)
+        chroma_done = [torch.cuda.Event() for _ in range(len(dout))]
+        for ev in free_out:
+            ev.record(copy)
+        for pair in free_in:
+            pair[0].record(sl)
+            pair[1].record(sc)
+        luma_frame = chroma_frame = 0
 
         def emit_chroma():
             nonlocal chroma_frame
             o = chroma_frame % len(dout)
-            stream.wait_event(free_out[o])
-            eng_c.emit_into(P([dscr[0], dout[o][1], dout[o][2]]))
+            sc.wait_event(free_out[o])
+            eng_c.emit_into(P([dscr[1][0], dout[o][1], dout[o][2]]))
+            chroma_done[o].record(sc)
             chroma_frame += 1
 
         def emit_luma():
             nonlocal luma_frame
             o = luma_frame % len(dout)
-            eng_l.emit_into(P([dout[o][0], dscr[1], dscr[2]]))
-            drain(luma_frame)
+            eng_l.emit_into(P([dout[o][0], dscr[0][1], dscr[0][2]]))
+            done = torch.cuda.Event()
+            done.record(sl)
+            copy.wait_event(done)
+            copy.wait_event(chroma_done[o])
+            with torch.cuda.stream(copy):
+                for i in range(3):
+                    host_out[luma_frame][i].copy_(dout[o][i], non_blocking=True)
+            free_out[o].record(copy)
             luma_frame += 1
 
         for k, f in enumerate(host_in):
-            s = k % 2
-            copy.wait_event(free_in[s])
+            s_ = k % 2
+            copy.wait_event(free_in[s_][0])
+            copy.wait_event(free_in[s_][1])
             with torch.cuda.stream(copy):
                 for i in range(3):
-                    stage[s][i].copy_(f[i], non_blocking=True)
+                    stage[s_][i].copy_(f[i], non_blocking=True)
             ready = torch.cuda.Event()
             ready.record(copy)
-            stream.wait_event(ready)
-            pl = P(stage[s])
-            rc = eng_c.push(pl)
-            for _ in range(rc):
+            sl.wait_event(ready)
+            sc.wait_event(ready)
+            pl = P(stage[s_])
+            for _ in range(eng_c.push(pl)):
                 emit_chroma()
-            rl = eng_l.push(pl)
-            free_in[s].record(stream)
-            for _ in range(rl):
+            free_in[s_][1].record(sc)
+            for _ in range(eng_l.push(pl)):
                 emit_luma()
+            free_in[s_][0].record(sl)
         for _ in range(eng_c.finish()):
             emit_chroma()
         for _ in range(eng_l.finish()):
             emit_luma()
         return luma_frame
 
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(max(3, args.warmup)):
         step_e2e()
     torch.cuda.synchronize()
     e2e_times = []
@@ -300,10 +340,29 @@ def run_gpu(args) -> None:
         assert n == FRAMES
     clocks = clocks_stop(proc, clock_path)
 
-    # Output sanity against the device run: the e2e output of the last frame equals the resident run.
+    # Output sanity: the e2e output of the last frame equals the resident run's.
     step_device()
     torch.cuda.synchronize()
     same = all(torch.equal(host_out[FRAMES - 1][i], out[i].cpu()) for i in range(3))
+
+    # The dominant kernel alone: the luma window kernel with a float output (no exact finish), timed
+    # by the engine's device timer over 16 frames of the same clip.
+    f32 = avd.SampleFormat.f32()
+    lspec = avd.EngineSpec.nlmeans(spec_l.luma, None, avd.Geometry(W, H, avd.ChromaLayout.GRAY, fmt, f32))
+    eng_w = avd.build_engine(lspec)
+    eng_w.set_stream(sl.cuda_stream)
+    wbuf = torch.empty(W * H, dtype=torch.float32, device="cuda")
+    wout = [avd.DevicePlane.from_tensor(wbuf, W, H)]
+    for rep in range(2):
+        eng_w.sample_device_time(1 if rep else 0)
+        for f in planes_in[:16]:
+            for _ in range(eng_w.push([f[0]])):
+                eng_w.emit_into(wout)
+        for _ in range(eng_w.finish()):
+            eng_w.emit_into(wout)
+    torch.cuda.synchronize()
+    win_timing = eng_w.timing().luma
+    eng_w.close()
 
     (t_step, t_e2e), (fps, fps_e2e) = replica_throughput(
         [sum(times) / len(times), sum(e2e_times) / len(e2e_times)], FRAMES, world)
@@ -311,8 +370,9 @@ def run_gpu(args) -> None:
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     luma_px = W * H
     ex2_per_launch = luma_px * n_off(LUMA["d"], LUMA["a"])
-    t_launch = nlm_timing.device_time / max(1, nlm_timing.frames)
-    achieved = ex2_per_launch / t_launch / 1e9
+    t_window = win_timing.device_time / max(1, win_timing.frames)
+    t_luma_frame = nlm_timing.device_time / max(1, nlm_timing.frames)
+    achieved = ex2_per_launch / t_window / 1e9
     mufu_peak = sms * 16 * peaks["sm_max_mhz"] * 1e6 / 1e9
     hbm_bytes = luma_px * 4 * (2 * LUMA["d"] + 1) + luma_px * 4
     line = {
@@ -329,28 +389,54 @@ def run_gpu(args) -> None:
         "dtype": "f32",
         "data": "synthetic (seeded gratings + rectangles + blurred texture, global pan and sprites, Gaussian noise)",
         "config": {"workload": "NLMeans 1920x1080 4:2:0 u8, 32 frames: luma d=2 a=5 s=2 strength 8; "
-                               "chroma spatial a=5 s=2 strength 5", "frames_per_step": FRAMES,
+                               "chroma spatial a=5 s=2 strength 5 (a luma engine and a chroma engine on two "
+                               "streams)", "frames_per_step": FRAMES,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "sfu", "kernel": "nlm_window_kernel<1,2> (luma, 604 offsets/pixel)",
+        "roofline": {"bound": "sfu", "kernel": "nlm_window_kernel<1,2,fast> (luma, 604 offsets/pixel)",
                      "achieved": round(achieved, 2), "peak": round(mufu_peak, 2), "unit": "Gex2/s",
                      "frac": round(achieved / mufu_peak, 4),
-                     # dram__bytes_read.sum + dram__bytes_write.sum of this launch in one ncu
-                     # capture (profiles/nlm_window_kernel_luma_1080p_d2a5s2.md).
+                     # dram__bytes_read.sum + dram__bytes_write.sum of one launch in an ncu capture of
+                     # the same launch, not of this run.
                      "traffic": 41.52e6 + 0.151e6,
+                     "traffic_source": "ncu capture: profiles/nlm_window_kernel_luma_1080p_d2a5s2.md",
                      "peak_note": f"MUFU ex2: {sms} SMs x 16/clk x sm_max_mhz {peaks['sm_max_mhz']} "
                                   f"({peaks['source']})",
-                     "launch_ms": round(t_launch * 1e3, 4)},
-        "roofline_hbm": {"bound": "hbm", "achieved": round(hbm_bytes / t_launch / 1e9, 2),
+                     "launch_ms": round(t_window * 1e3, 4),
+                     "luma_frame_ms_with_exact_finish": round(t_luma_frame * 1e3, 4)},
+        "roofline_hbm": {"bound": "hbm", "achieved": round(hbm_bytes / t_window / 1e9, 2),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": round(hbm_bytes / t_launch / 1e9 / peaks["hbm_gbs"], 5)},
+                         "frac": round(hbm_bytes / t_window / 1e9 / peaks["hbm_gbs"], 5)},
         "e2e": {"value": round(fps_e2e, 2), "unit": "frames/s", "h2d_bytes_per_step": h2d_bytes,
                 "d2h_bytes_per_step": d2h_bytes, "matches_resident_run": bool(same)},
-        "gpu_launches": launches_per_frame * FRAMES,
+        # per frame and engine: ingest, window, exact finish and egress
+        "gpu_launches": 8 * FRAMES,
         "clocks": clocks,
         "wall_s_timed": round(wall, 3),
     }
+    if rank == 0 and world == 1 and not args.no_nl4d:
+        line["nl4d_4k"] = nl4d_4k_section(avd, torch, np, synth, pushes=args.nl4d_pushes)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(seconds_target=args.cpu_seconds)
+        # Parity of one full frame of the timed workload (outside the timed region) and the CPU
+        # baseline: the oracle computes that frame once, timed.
+        k = FRAMES // 2
+        _, got = step_device(capture=k)
+        torch.cuda.synchronize()
+        gpu_planes = [got["y"], got["uv"][0], got["uv"][1]]
+        want, secs = oracle_frame(clip, k)
+        ident = total = max_lsb = 0
+        for g, wn, (w, h) in zip(gpu_planes, want, dims):
+            gv = g.cpu().numpy().view(np.uint8)[: w * h].reshape(h, w)
+            d_ = np.abs(gv.astype(np.int64) - wn.astype(np.int64))
+            ident += int((d_ == 0).sum())
+            total += d_.size
+            max_lsb = max(max_lsb, int(d_.max()))
+        line["parity"] = {"frame": k, "samples": total, "identical": round(ident / total, 7), "max_lsb": max_lsb,
+                          "against": "FP32 oracle (oracle/), one full 1920x1080 4:2:0 frame, luma and chroma"}
+        line["cpu_baseline"] = {"value": round(1.0 / secs, 4), "unit": "frames/s", "cores": os.cpu_count(),
+                                "kind": "port",
+                                "sample": f"one full 1920x1080 4:2:0 frame (frame {k}: luma d=2 a=5 s=2 over its "
+                                          "5-frame window + chroma a=5 s=2) through the FP32 oracle, OpenMP on "
+                                          f"{os.cpu_count()} threads, {secs:.1f} s"}
     if rank == 0:
         print(json.dumps(line))
     eng_l.close()
@@ -359,11 +445,71 @@ def run_gpu(args) -> None:
         dist.destroy_process_group()
 
 
-def cpu_baseline(seconds_target: float = 15.0) -> dict:
-    """The oracle (CPU restatement of the reference kernels, OpenMP on all host threads) on a
-    bounded crop of the same workload, scaled to frames/s of the full frame."""
-    import numpy as np
+def nl4d_4k_section(avd, torch, np, synth, pushes: int) -> dict:
+    """The NL4D half of the metric on its 4K workload: 3840x2160 4:2:0 10-bit, 7-frame window (d=3,
+    Auto resolves to Chained), spatial radius 16, hard threshold 2.7 (lambda_ht 2.7, scale 1, plain
+    threshold), 12 sprites at up to 8 px/frame, noise 20 codes + 0.02 * value variance; luma sigma
+    from the automatic noise estimate (motion-compensated look-ahead), chroma pinned at 20 codes, as a
+    luma engine and a chroma engine side by side. Frames resident in HBM; device time per push with
+    CUDA events, steady state after the window and look-ahead fill."""
+    w, h, depth, d = 3840, 2160, 10, 3
+    fmt = avd.SampleFormat.u16(depth)
+    sigma = 20.0 / 1023.0
 
+    def options(sig):
+        return avd.Nl4dOptions(sigma=sig, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
+                               pooled_threshold=False, noise_map=False)
+
+    geo = avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt)
+    engines = [avd.build_engine(avd.EngineSpec.nl4d(options(None), None, geo)),
+               avd.build_engine(avd.EngineSpec.nl4d(None, options(sigma), geo))]
+    stream = torch.cuda.Stream()
+    for eng in engines:
+        eng.set_stream(stream.cuda_stream)
+    clip = synth.make_clip(w, h, 12, depth=depth, chroma="420", sigma_luma=20.0 / 4.0, sigma_chroma=20.0 / 4.0,
+                           sprites=12, sprite_speed=8, signal_dependent=0.02, seed=2000)
+    dims = [geo.plane_dims(i) for i in range(3)]
+    bufs = []
+    for f in clip:
+        planes = []
+        for p in f:
+            flat = p.reshape(-1).astype(np.uint16)
+            planes.append(torch.from_numpy(np.concatenate([flat, np.zeros(flat.size % 2, np.uint16)]).view(np.int32)).cuda())
+        bufs.append(planes)
+    outs = [torch.zeros_like(b) for b in bufs[0]]
+
+    def dp(ts):
+        return [avd.DevicePlane.from_tensor(t, pw, ph) for t, (pw, ph) in zip(ts, dims)]
+
+    times = []
+    for i in range(pushes):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for eng in engines:
+            for _ in range(eng.push(dp(bufs[i % len(bufs)]))):
+                eng.emit_into(dp(outs))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    for eng in engines:
+        eng.close()
+    steady = times[2 * d + 1 + 8:]
+    ms = float(np.median(steady))
+    return {"workload": "NL4D 3840x2160 4:2:0 10-bit luma+chroma, d=3 (Chained), spatial_radius 16, lambda_ht 2.7, "
+                        "plain threshold; luma sigma automatic, chroma sigma pinned at 20 codes",
+            "frames_per_s": round(1000.0 / ms, 2), "ms_per_frame": round(ms, 3), "pushes_timed": len(steady)}
+
+
+def run_reference(args) -> None:
+    """The reference arm: the CPU restatement of the reference kernels (oracle/, FP32 mirror, OpenMP
+    on every host thread) on the same workload. Each step is a bounded sample: frame k's central
+    960x540 luma crop (d=2 over its 5-frame window) and 480x270 chroma crop, a quarter of a 1080p
+    4:2:0 frame's pixels; frames/s is scaled to the full frame by that pixel ratio. Warm-up steps run
+    the same sample untimed."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
 
@@ -373,44 +519,29 @@ def cpu_baseline(seconds_target: float = 15.0) -> dict:
     from av_denoise_b200 import synth
 
     oracle.build()
-    clip = synth.temporal_1080p_clip(frames=5, seed=1000)
-    cw, ch = 256, 144
-    t_luma = t_chroma = 0.0
-    reps = 0
-    t_start = time.perf_counter()
-    while True:
-        frames = [oracle.ingest([f[0][:ch, :cw]], 0, 255.0) for f in clip]
+    clip = synth.temporal_1080p_clip(frames=FRAMES, seed=1000)
+    cw, ch = W // 2, H // 2
+    x0, y0 = W // 4, H // 4
+    h2_l = oracle.h2_inv_norm(LUMA["strength"], LUMA["s"])
+    h2_c = oracle.h2_inv_norm(CHROMA["strength"], CHROMA["s"])
+
+    def sample(k):
         t0 = time.perf_counter()
-        oracle.nlm_frame(frames, LUMA["d"], LUMA["a"], LUMA["s"], oracle.h2_inv_norm(LUMA["strength"], LUMA["s"]))
-        t1 = time.perf_counter()
-        cf = oracle.ingest([clip[2][1][:ch // 2, :cw // 2], clip[2][2][:ch // 2, :cw // 2]], 0, 255.0)
-        oracle.nlm_frame([cf], 0, CHROMA["a"], CHROMA["s"], oracle.h2_inv_norm(CHROMA["strength"], CHROMA["s"]))
-        t2 = time.perf_counter()
-        t_luma += t1 - t0
-        t_chroma += t2 - t1
-        reps += 1
-        if time.perf_counter() - t_start > seconds_target:
-            break
-    scale = (W * H) / (cw * ch)
-    per_frame = (t_luma + t_chroma) / reps * scale
-    return {"value": round(1.0 / per_frame, 4), "unit": "frames/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{reps} x ({cw}x{ch} luma crop d=2 a=5 s=2 + {cw // 2}x{ch // 2} chroma crop a=5 s=2), "
-                      f"scaled by the pixel ratio {scale:.1f} to one 1080p 4:2:0 frame"}
+        win = [oracle.ingest([clip[min(max(k + j, 0), FRAMES - 1)][0][y0:y0 + ch, x0:x0 + cw]], 0, 255.0)
+               for j in range(-LUMA["d"], LUMA["d"] + 1)]
+        oracle.nlm_frame(win, LUMA["d"], LUMA["a"], LUMA["s"], h2_l)
+        f = clip[k]
+        uv = oracle.ingest([f[1][y0 // 2:y0 // 2 + ch // 2, x0 // 2:x0 // 2 + cw // 2],
+                            f[2][y0 // 2:y0 // 2 + ch // 2, x0 // 2:x0 // 2 + cw // 2]], 0, 255.0)
+        oracle.nlm_frame([uv], 0, CHROMA["a"], CHROMA["s"], h2_c)
+        return time.perf_counter() - t0
 
-
-def run_reference(args) -> None:
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    seconds = max(10.0, min(30.0, 60.0 / max(1, args.steps)))
-    vals = []
-    for _ in range(args.warmup):
-        pass
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(seconds_target=seconds)["value"])
-    cb = cpu_baseline(seconds_target=1.0)
-    v = statistics.mean(vals)
+    for i in range(args.warmup):
+        sample(i % FRAMES)
+    secs = [sample((args.warmup + i) % FRAMES) for i in range(args.steps)]
+    per_step = statistics.mean(secs)
+    fraction = (cw * ch) / (W * H)
+    v = fraction / per_step
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -419,18 +550,20 @@ def run_reference(args) -> None:
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(1e3 * FRAMES / v, 1),
+        "ms_per_step": round(1e3 * per_step, 1),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "NLMeans 1920x1080 4:2:0 u8, 32 frames: luma d=2 a=5 s=2 strength 8; "
-                               "chroma spatial a=5 s=2 strength 5", "frames_per_step": FRAMES},
+        "config": {"workload": "NLMeans 1920x1080 4:2:0 u8: luma d=2 a=5 s=2 strength 8; chroma spatial a=5 s=2 "
+                               "strength 5", "frames_per_step": fraction,
+                   "sample": f"per step: a central {cw}x{ch} luma crop (5-frame window) + {cw // 2}x{ch // 2} "
+                             "chroma crop of one frame = 1/4 of a frame's pixels; frames/s scaled by 1/4"},
         "cpu_baseline": {"value": round(v, 4), "unit": "frames/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": cb["sample"] + "; the reference's own CPU device is a software Vulkan "
-                                                  "renderer (unavailable on this box) and its Rust crate "
-                                                  "cannot be built here, so the oracle port stands in"},
+                         "sample": f"{args.steps} quarter-frame samples, OpenMP on {os.cpu_count()} threads; the "
+                                   "reference's own CPU device is a software Vulkan renderer (unavailable on this "
+                                   "box) and its Rust crate cannot be built here, so the oracle port stands in"},
         "e2e": {"value": round(v, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -1037,7 +1170,9 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the parity frame and the CPU baseline")
+    ap.add_argument("--no-nl4d", action="store_true", help="skip the NL4D 4K fields of the default line")
+    ap.add_argument("--nl4d-pushes", type=int, default=30)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     if args.once:

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define AVD_ABI_VERSION 1u
+#define AVD_ABI_VERSION 2u
 
 #if defined(__GNUC__)
 #define AVD_API __attribute__((visibility("default")))
@@ -226,10 +226,14 @@ typedef struct AvdEngineSpec {
     AvdGeometry geometry;
 } AvdEngineSpec;
 
-/* av-denoise-core/src/tune/setup.rs:79-91 (`TuningConfig`): the reference picks tuned kernel
- * candidates here. This build has one kernel per site plus a per-shape launch-shape cache. */
+/* av-denoise-core/src/tune/config.rs:66-75 (`TuningConfig`). `deterministic` ("picks only
+ * bit-identical candidates and the baseline profile"): every NLMeans sample is computed by the exact
+ * kernel in the operation order of the reference's baseline (direct row-major patch sums), so float
+ * outputs too are bit-identical to the CPU restatement; slower. Off (the default), integer outputs
+ * still match it: the fast window kernel flags the samples near a change of code and the exact
+ * kernel recomputes only those. The NLM pilot prefilter's reference always runs exactly. */
 typedef struct AvdTuning {
-    uint32_t deterministic; /* kept for API parity; every kernel here is deterministic */
+    uint32_t deterministic;
     uint32_t reserved;
 } AvdTuning;
 
@@ -246,6 +250,9 @@ typedef struct AvdWindowSpan {
 typedef struct AvdEngineTiming {
     double device_time;
     uint64_t frames;
+    /* No field in the reference: over the same sampled frames, the samples (pixels) the exact finish
+     * recomputed in the reference kernels' order (NLMeans with integer outputs; 0 otherwise). */
+    uint64_t exact_samples;
 } AvdEngineTiming;
 
 typedef struct AvdPassTimings {
@@ -635,6 +642,12 @@ AVD_API uint64_t avd_nlm_backward_scratch_bytes(uint32_t width, uint32_t height)
  * avd_nlm_window_scratch_bytes(search_radius) bytes. Queued on `stream`; allocates nothing. */
 AVD_API uint64_t avd_nlm_window_scratch_bytes(uint32_t search_radius);
 AVD_API AvdStatus avd_nlm_window(const AvdNlmBackward* args, void* stream);
+
+/* No Rust item in the reference (its `f32::exp`, helpers.rs:70-73, is lowered inside CubeCL): the
+ * exponential of the exact NLMeans finish and the bilateral prefilter (exp_mirror.cuh) over `n`
+ * device floats `x` into `out`, queued on `stream`; exposed so tests compare it with the CPU
+ * restatement bit for bit. */
+AVD_API AvdStatus avd_exp_mirror(uint64_t x, uint64_t out, uint64_t n, void* stream);
 AVD_API AvdStatus avd_nlm_backward(const AvdNlmBackward* args, void* stream);
 
 /* ---- batched launch ------------------------------------------------------------------------- */
@@ -675,9 +688,11 @@ AVD_API AvdStatus avd_batch_submit(const AvdBatchJob* jobs, size_t n_jobs, uint3
  * engine denoises it with that window. `out` receives `channels` planes. Work is queued on
  * `stream` (a cudaStream_t; NULL = legacy default) with no host synchronisation.
  *
- * The first call on a device looks up the array's device address with that device current, so
- * make it before any stream capture. Every call shares the array and leaves its contents behind;
- * each call writes every scratch word it reads, but calls whose GPU work overlaps race. */
+ * The first call in each CUDA context on a device (the primary context, a caller's own context, or
+ * the new primary context after cudaDeviceReset) looks up the array's device address with that
+ * device current, so make it before any stream capture. Every call shares the array and leaves its
+ * contents behind; each call writes every scratch word it reads (it clears the count of samples
+ * its exact finish recomputes), but calls whose GPU work overlaps race. */
 AVD_API AvdStatus avd_nlm_frame_static(const AvdNlmeansAlgorithm* algorithm, uint32_t channels, uint32_t width,
                                        uint32_t height, AvdSampleFormat input, AvdSampleFormat output,
                                        const AvdPlane* window, size_t n_window, const AvdPlane* out, size_t n_out,

@@ -338,7 +338,9 @@ void orc_motion_search(const OrcMotionArgs* a) {
                 failed[i] = low || on_edge || closest > kNeighbourDisagreement;
             }
     // escalate.rs:400-559 (`mc_escalate_search`).
-    const bool widen = a->widen_coarse && a->levels > 1 && !a->seeded;
+    // escalate.rs:203-205 (`reaches_further`): only a ceiling past the coarse pass's radius (the
+    // search radius here) searches the coarse level again.
+    const bool widen = a->widen_coarse && a->levels > 1 && !a->seeded && a->ceiling > a->search_radius;
     Level Lc{};
     int scale = 1;
     if (widen) {

@@ -51,11 +51,50 @@ inline T line_sum_sq(const T* a, const T* b, int channels) {
     return sum;
 }
 
+// The FP32 mirror's exponential. The reference writes `f32::exp` (helpers.rs:70-73,
+// bilateral.rs:72); its lowering to device code happens inside CubeCL (ChillFish8/cubecl@e3c9246,
+// not vendored), so its last-bit rounding is unknown. The mirror fixes one evaluation, written from
+// the mathematics so a CUDA kernel can repeat it operation for operation:
+//   n = rint(x * log2(e)), r = x - n*ln2 by Cody and Waite's two-constant reduction (ln2 split
+//   into a 16-bit head, so n*head is exact, and the float nearest the remainder), |r| <= ln2/2;
+//   e^r by its degree-7 Taylor polynomial (coefficients 1/k!) in Horner form with fused
+//   multiply-adds (truncation error below 0.1 ulp on the reduced range);
+//   e^x = e^r * 2^n, the power built exactly.
+// x below -87 gives 0 (e^x would be subnormal) as does NaN; x above 88 overflows to +inf where
+// n reaches 128. Measured against the double-precision exponential: within 1 ulp
+// (tests/test_oracle_nlm.py).
+constexpr float kExpLog2e = 1.44269502162933349609375f;     // float(log2(e))
+constexpr float kExpLn2Hi = 0.693145751953125f;             // ln2 to 16 bits
+constexpr float kExpLn2Lo = 1.428606765330187045037746e-06f;  // float(ln2 - kExpLn2Hi)
+
+inline float exp_mirror(float x) {
+    if (!(x >= -87.0f)) return 0.0f;
+    const float n = std::rint(x * kExpLog2e);
+    float r = std::fma(n, -kExpLn2Hi, x);
+    r = std::fma(n, -kExpLn2Lo, r);
+    float p = 1.0f / 5040.0f;
+    p = std::fma(p, r, 1.0f / 720.0f);
+    p = std::fma(p, r, 1.0f / 120.0f);
+    p = std::fma(p, r, 1.0f / 24.0f);
+    p = std::fma(p, r, 1.0f / 6.0f);
+    p = std::fma(p, r, 0.5f);
+    p = std::fma(p, r, 1.0f);
+    p = std::fma(p, r, 1.0f);
+    const int e = static_cast<int>(n) + 127;
+    uint32_t bits = e >= 255 ? 0x7f800000u : static_cast<uint32_t>(e) << 23;
+    float scale;
+    std::memcpy(&scale, &bits, sizeof(scale));
+    return p * scale;
+}
+
+inline float exp_of(float x) { return exp_mirror(x); }
+inline double exp_of(double x) { return std::exp(x); }
+
 // av-denoise-core/src/nlmeans/kernels/helpers.rs:70-73 (`welsch_weight`).
 template <typename T>
 inline T welsch(T sum, T h2, T off) {
     T excess = std::max(sum - off, T(0));
-    return std::exp(-excess * h2);
+    return exp_of(-excess * h2);
 }
 
 // The patch distance of the direct (deterministic baseline) form: the distance tile element at
@@ -65,6 +104,21 @@ template <typename T>
 inline T patch_distance(const Frame<T>& centre, const Frame<T>& nbr, int px, int py, int qx, int qy,
                         int s, T scale) {
     T sum = T(0);
+    const int C = centre.channels;
+    if (px - s >= 0 && py - s >= 0 && px + s < centre.width && py + s < centre.height && px + qx - s >= 0 &&
+        py + qy - s >= 0 && px + qx + s < centre.width && py + qy + s < centre.height) {
+        // Every tap inside the frame: the same sums in the same order, without the clamps.
+        const size_t row = static_cast<size_t>(centre.width) * C;
+        const T* c = centre.data + (static_cast<size_t>(py - s) * centre.width + (px - s)) * C;
+        const T* n = nbr.data + (static_cast<size_t>(py + qy - s) * centre.width + (px + qx - s)) * C;
+        for (int oy = 0; oy <= 2 * s; ++oy, c += row, n += row) {
+            for (int ox = 0; ox <= 2 * s; ++ox) {
+                T d = line_sum_sq(c + ox * C, n + ox * C, C) * scale;
+                sum = sum + d;
+            }
+        }
+        return sum;
+    }
     for (int oy = -s; oy <= s; ++oy) {
         for (int ox = -s; ox <= s; ++ox) {
             int tx = px + ox, ty = py + oy;
@@ -278,6 +332,11 @@ float orc_h2_inv_norm(float strength, int patch_radius) {
 // av-denoise-core/src/nlmeans/kernels/helpers.rs:70-73, exposed for the host-formula pin.
 float orc_welsch_weight(float sum, float h2, float off) { return welsch<float>(sum, h2, off); }
 
+// The FP32 mirror's exponential over an array (its accuracy pin and the GPU comparison).
+void orc_exp_mirror(const float* x, float* out, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) out[i] = exp_mirror(x[i]);
+}
+
 // One denoised frame of the windowed NLM path, FP32 mirror. `frames` holds the 2d+1 window
 // frames (normalised f32, interleaved), the centre at index d; `refs` (null = `frames`) the
 // window's reference frames the distances compare. `lut` is the (2a+1)^2 spatial offset table
@@ -360,7 +419,7 @@ void orc_bilateral_f32(const float* frame, int width, int height, int channels, 
                     }
                     float spatial = (float)(dx * dx + dy * dy) * inv_s;
                     float r = range_sq * inv_r;
-                    float w = std::exp(-(spatial + r));
+                    float w = exp_mirror(-(spatial + r));
                     for (int ch = 0; ch < channels; ++ch) {
                         float t = n[ch] * w;
                         acc[ch] = acc[ch] + t;

@@ -47,6 +47,7 @@ def lib():
         l.orc_h2_inv_norm.restype = C.c_float
         l.orc_welsch_weight.argtypes = [C.c_float, C.c_float, C.c_float]
         l.orc_welsch_weight.restype = C.c_float
+        l.orc_exp_mirror.argtypes = [_fp, _fp, C.c_int64]
         l.orc_nlm_frame_f32.argtypes = [_fpp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                         C.c_float, _fp, _fpp, _fpp, C.c_int, C.c_int, C.c_int, C.c_float, _fp]
         l.orc_nlm_frame_f64.argtypes = [_fpp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
@@ -68,6 +69,14 @@ def h2_inv_norm(strength: float, patch_radius: int) -> float:
 
 def welsch_weight(total: float, h2: float, offset: float) -> float:
     return float(lib().orc_welsch_weight(total, h2, offset))
+
+
+def exp_mirror(x: np.ndarray) -> np.ndarray:
+    """The FP32 mirror's exponential (nlm_oracle.cpp `exp_mirror`) over a float32 array."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_exp_mirror(_f(x), _f(out), x.size)
+    return out
 
 
 def words_from_codes(codes: np.ndarray, fmt_kind: int) -> np.ndarray:

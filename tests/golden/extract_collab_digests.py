@@ -2,8 +2,9 @@
 av-denoise-core/src/collab/tests/fused/recorded.rs (covered pixels, mean, RMS, mean group
 weight and eight probe pixels per case), keyed by the case label.
 
-Run here, where the reference checkout is mounted; the JSON it writes is committed, and nothing
-reads the reference at test time.
+Usage: python extract_collab_digests.py <path to the reference's collab/tests/fused/recorded.rs>.
+Run where a reference checkout is available; the JSON it writes is committed, and nothing reads the
+reference at test time.
 """
 
 import json
@@ -11,8 +12,9 @@ import re
 import sys
 from pathlib import Path
 
-SRC = Path(sys.argv[1] if len(sys.argv) > 1 else
-           "/root/reference/av-denoise-core/src/collab/tests/fused/recorded.rs")
+if len(sys.argv) != 2:
+    sys.exit("usage: extract_collab_digests.py <reference av-denoise-core/src/collab/tests/fused/recorded.rs>")
+SRC = Path(sys.argv[1])
 OUT = Path(__file__).with_name("collab_recorded.json")
 
 text = SRC.read_text()

@@ -31,7 +31,7 @@ def hq_auto(d, a, s, strength=None, confidence=True, auto_strength=True, noise_f
     return avd.NlmeansAlgorithm.hq_(avd.NlmeansHqOptions(nlm=avd.NlmeansOptions(tuning=tuning, mode=mode), hq=params))
 
 
-def check(oracle, got_planes, frames, fmt, d, a, s, strength, chroma=False, min_raw=0.95, **hq):
+def check(oracle, got_planes, frames, fmt, d, a, s, strength, chroma=False, **hq):
     bias = 0.0
     f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), bias) for p in frames]
     outs, folds = oracle.nlm_stream_hq_auto(f32, d, a, s, strength, **hq)
@@ -42,7 +42,7 @@ def check(oracle, got_planes, frames, fmt, d, a, s, strength, chroma=False, min_
     for g, wn, ex in zip(got_planes, want, exact):
         for c in range(len(wn)):
             par.add(g[c], wn[c], ex[..., c], fmt.max_value())
-    st = par.check(min_raw=min_raw)
+    st = par.check()
     print(st, "sigma*255 of the first fold:", folds[0][1][0] * 255)
     return folds
 
@@ -149,7 +149,7 @@ def test_hq_auto_with_the_pilot(oracle, w, h, n, d, a, s, scale, conf):
     par = Parity()
     for g, wn, ex in zip(got, want, exact):
         par.add(g[0], wn[0], ex[..., 0], fmt.max_value())
-    print(par.check(min_raw=0.95))
+    print(par.check())
 
 
 @pytest.mark.parametrize("w,h,n,d,est,ceiling", [(112, 72, 11, 1, "auto", 0), (96, 64, 12, 3, "auto", 0),
@@ -194,4 +194,4 @@ def test_hq_auto_with_motion_compensation(oracle, w, h, n, d, est, ceiling):
     par = Parity()
     for g, wn, ex in zip(got, want, exact):
         par.add(g[0], wn[0], ex[..., 0], fmt.max_value())
-    print(par.check(min_raw=0.95), "sigma*255 at the middle:", folds[n // 2][1][0] * 255)
+    print(par.check(), "sigma*255 at the middle:", folds[n // 2][1][0] * 255)

@@ -236,6 +236,9 @@ ESC_CASES = [
     (96, 64, 3, 2, 8, 4, 1, 5, True, 0.0),
     (200, 120, 5, 2, 32, 16, 4, 8, False, 0.05),
     (40, 24, 3, 1, 16, 8, 0, 3, False, 0.02),
+    # blksizes outside 8/16/32: the generic fine kernel, then the recorded centres and tracking
+    (120, 80, 3, 2, 12, 6, 2, 6, False, 0.02),
+    (64, 48, 3, 1, 4, 2, 1, 4, True, 0.02),
 ]
 
 

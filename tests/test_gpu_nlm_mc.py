@@ -34,14 +34,14 @@ def options(d, a, s, strength, ms, prefilter=None):
                               motion_compensation=avd.MotionCompensationMode(ms), tuning=tuning, mode=mode)
 
 
-def check(oracle, got_planes, frames, fmt, d, a, s, strength, ms, chroma=False, min_raw=0.97, **kw):
+def check(oracle, got_planes, frames, fmt, d, a, s, strength, ms, chroma=False, **kw):
     want, exact = oracle_pass(oracle, frames, fmt, d, a, s, strength, chroma=chroma, exact=True, motion=ms, **kw)
     par = Parity()
     assert len(got_planes) == len(want)
     for g, wn, ex in zip(got_planes, want, exact):
         for c in range(len(wn)):
             par.add(g[c], wn[c], ex[..., c], fmt.max_value())
-    st = par.check(min_raw=min_raw)
+    st = par.check()
     print(st)
     return st
 
@@ -80,7 +80,7 @@ def test_hq_pinned_sigma_with_confidence(oracle, d, est):
     spec = avd.EngineSpec.nlmeans(alg, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
     got = Runner(spec).run(frames)
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, avd.hq_default_strength(1, d), ms,
-          hq_sigma=sigma, hq_confidence=True, min_raw=0.95)
+          hq_sigma=sigma, hq_confidence=True)
 
 
 @pytest.mark.parametrize("prefilter,est", [(avd.PrefilterMode.bilateral(1.0, 0.06), avd.MotionEstimation.DIRECT),
@@ -112,7 +112,7 @@ def test_chroma_motion_compensated_10bit(oracle):
     f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
     oracle.nlm_stream_mc(f32, 1, 3, 2, oracle.h2_inv_norm(5.0, 2), share_writes=share)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, 1, 3, 2, 5.0, ms, chroma=True,
-          min_raw=0.95, share_reads=share)
+          share_reads=share)
 
 
 @pytest.mark.parametrize("d,est,radius,ceiling,hq", [(2, avd.MotionEstimation.DIRECT, 2, 6, False),
@@ -137,7 +137,7 @@ def test_escalating_motion_compensation(oracle, d, est, radius, ceiling, hq):
     got = Runner(spec).run(frames)
     if hq:
         check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, avd.hq_default_strength(1, d),
-              ms, hq_sigma=sigma, hq_confidence=True, min_raw=0.95)
+              ms, hq_sigma=sigma, hq_confidence=True)
     else:
         check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, 8.0, ms)
 
@@ -161,7 +161,7 @@ def test_chroma_refines_the_luma_motion(oracle, layout, shifts, d, est):
     share = oracle.MotionShare((-(-w // 8), -(-h // 8), 8, 16), (-(-cw // 8), -(-ch // 8), 8, 16), *shifts)
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 3, 2, 8.0, ms, share_writes=share)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, 3, 2, 5.0, ms, chroma=True,
-          min_raw=0.95, share_reads=share)
+          share_reads=share)
 
 
 def test_chroma_only_engine_follows_a_luma_guide(oracle):
@@ -183,4 +183,4 @@ def test_chroma_only_engine_follows_a_luma_guide(oracle):
     f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
     oracle.nlm_stream_mc(f32, d, 3, 2, oracle.h2_inv_norm(5.0, 2), share_writes=share)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, 3, 2, 5.0, ms, chroma=True,
-          min_raw=0.95, share_reads=share)
+          share_reads=share)

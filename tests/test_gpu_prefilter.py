@@ -37,14 +37,14 @@ def hq(prefilter, d, a, s, sigma, strength=None, confidence=False):
 
 
 def check(oracle, got_planes, frames, fmt, d, a, s, strength, prefilter, chroma=False, hq_sigma=None,
-          hq_confidence=False, min_raw=0.98):
+          hq_confidence=False):
     want, exact = oracle_pass(oracle, frames, fmt, d, a, s, strength, chroma=chroma, exact=True, hq_sigma=hq_sigma,
                               hq_confidence=hq_confidence, prefilter=prefilter)
     par = Parity()
     for g, wn, ex in zip(got_planes, want, exact):
         for c in range(len(wn)):
             par.add(g[c], wn[c], ex[..., c], fmt.max_value())
-    st = par.check(min_raw=min_raw)
+    st = par.check()
     print(st)
     return st
 
@@ -80,7 +80,7 @@ def test_bilateral_chroma_10bit(oracle):
                                   avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
     got = Runner(spec).run(frames)
     check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, 1, 3, 2, 6.0, prefilter,
-          chroma=True, min_raw=0.97)
+          chroma=True)
 
 
 def test_bilateral_largest_radius_on_a_small_frame(oracle):
@@ -93,7 +93,7 @@ def test_bilateral_largest_radius_on_a_small_frame(oracle):
     spec = avd.EngineSpec.nlmeans(fast(prefilter, 1, 2, 1, 12.0), None,
                                   avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
     got = Runner(spec).run(frames)
-    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, 1, 2, 1, 12.0, prefilter, min_raw=0.97)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, 1, 2, 1, 12.0, prefilter)
 
 
 @pytest.mark.parametrize("w,h,d,a,s,strength,scale", [
@@ -110,8 +110,7 @@ def test_pilot_luma(oracle, w, h, d, a, s, strength, scale):
                                   avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
     got = Runner(spec).run(frames)
     assert len(got) == len(frames)
-    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, a, s, strength, prefilter,
-          min_raw=0.95 if w < 8 else 0.98)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, a, s, strength, prefilter)
 
 
 @pytest.mark.parametrize("d,a,s,sigma,confidence", [(1, 4, 2, 10.0 / 255, False), (2, 3, 2, 6.0 / 255, True),
@@ -128,7 +127,7 @@ def test_pilot_hq_pinned_sigma(oracle, d, a, s, sigma, confidence):
     got = Runner(spec).run(frames)
     strength = avd.hq_default_strength(1, d)
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, a, s, strength, prefilter, hq_sigma=sigma,
-          hq_confidence=confidence, min_raw=0.95)
+          hq_confidence=confidence)
 
 
 def test_pilot_chroma_hq_and_bilateral_hq(oracle):
@@ -141,7 +140,7 @@ def test_pilot_chroma_hq_and_bilateral_hq(oracle):
                                       avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
         got = Runner(spec).run(frames)
         check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, 1, 3, 2, 0.8, prefilter,
-              chroma=True, hq_sigma=sigma, min_raw=0.95)
+              chroma=True, hq_sigma=sigma)
 
 
 @pytest.mark.parametrize("prefilter", [avd.PrefilterMode.bilateral(1.0, 0.1), avd.PrefilterMode.nlm_spatial(1.0)])

@@ -168,3 +168,17 @@ def test_motion_compensation_of_a_still_clip_is_the_plain_pass(oracle, d, chaine
     plain = oracle.nlm_stream_repeat(frames, d, 2, 1, h2)
     mc = oracle.nlm_stream_mc(frames, d, 2, 1, h2, chained=chained)
     assert all(np.array_equal(x, y) for x, y in zip(plain, mc))
+
+
+def test_exp_mirror_within_one_ulp(oracle):
+    # The FP32 mirror's exponential (nlm_oracle.cpp `exp_mirror`) against the double-precision
+    # exponential over the weights' whole range: within 1 ulp everywhere, exact at 0, and 0 below -87.
+    x = np.concatenate([np.linspace(-87.0, 0.0, 2_000_003, dtype=np.float32),
+                        -np.geomspace(1e-8, 1.0, 100_001).astype(np.float32),
+                        np.linspace(0.0, 88.0, 200_001, dtype=np.float32)])
+    got = oracle.exp_mirror(x).astype(np.float64)
+    want = np.exp(x.astype(np.float64))
+    ulp = np.spacing(want.astype(np.float32)).astype(np.float64)
+    err = np.abs(got - want) / ulp
+    assert err.max() <= 1.0, float(err.max())
+    assert oracle.exp_mirror(np.array([0.0, -0.0, -87.5, np.nan], np.float32)).tolist() == [1.0, 1.0, 0.0, 0.0]
