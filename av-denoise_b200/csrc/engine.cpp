@@ -1162,9 +1162,10 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
     if (dev_err != cudaSuccess) return fail_global(AVD_ERR_GPU, avd::cuda_message("cudaGetDevice", dev_err));
     const AvdGeometry& g = spec->geometry;
     const bool nl4d = spec->kind == AVD_ENGINE_NL4D;
+    const bool colour_frames = g.chroma != AVD_CHROMA_GRAY;
     if (spec->has_luma) {
         auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_luma, avd::Channels::Luma, g.width, g.height, g.input,
-                                              g.output, &engine->luma)
+                                              g.output, colour_frames, &engine->luma)
                       : avd::NlmPass::create(spec->nlm_luma, avd::Channels::Luma, g.width, g.height, g.input,
                                              g.output, &engine->luma, false, exact_all);
         if (f) return fail_global(f->status, f->message);
@@ -1173,7 +1174,7 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
         uint32_t cw, ch;
         avd::plane_dims(g, 1, &cw, &ch);
         auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
-                                              &engine->chroma)
+                                              colour_frames, &engine->chroma)
                       : avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
                                              &engine->chroma, false, exact_all);
         if (f) return fail_global(f->status, f->message);
@@ -1185,7 +1186,7 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
                                     avd::resolve_nlm_params(spec->nlm_chroma, avd::Channels::Chroma).temporal_radius > 0);
         if (moves) {
             auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Luma, g.width, g.height, g.input,
-                                                  g.output, &engine->luma, true)
+                                                  g.output, colour_frames, &engine->luma, true)
                           : avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Luma, g.width, g.height, g.input,
                                                  g.output, &engine->luma, true);
             if (f) return fail_global(f->status, f->message);

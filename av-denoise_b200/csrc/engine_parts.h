@@ -151,6 +151,9 @@ struct NoiseFrontConfig {
     int blksize = 16, overlap = 8, search_radius = 4, levels = 2;
     float thsad = 0.0f;
     int ceiling = 0;  // the search's escalation ceiling (lookahead.rs:505-515); 0: no escalation
+    // Each record carries the luma quarter fields and each reading the noise curve
+    // (noise/state.rs:297, `wants_curve`; the NL4D luma noise map).
+    bool luma_fields = false;
 };
 
 class NoiseFront {
@@ -176,6 +179,8 @@ class NoiseFront {
     // after the reads.
     std::optional<Failure> fold(uint32_t centre, cudaStream_t main);
     float* derived() const { return derived_.as<float>(); }
+    // The stream state's 16 curve ratios (noise/fold.rs:47-72), read while the curve flag is set.
+    const float* curve_ratios() const { return state_.as<float>() + 16; }
     float* spatial_table() const { return spatial_.as<float>(); }
     float* pilot_table() const { return pilot_.as<float>(); }
     void reset();
@@ -194,11 +199,14 @@ class NoiseFront {
 };
 
 // NL4D pass over one plane group (nl4d_pass.cpp).
-// With `guides_only` the pass is a chroma-only engine's luma guide: it runs the motion machinery on
-// the luma plane for the chroma pass to read, and no filter (engine/spec.rs:220-236).
+// `colour_frames` is set for frames with chroma planes, whose measured passes scale their thresholds
+// by the colour grain gains (noise/colour.rs:204-286). With `guides_only` the pass is a chroma-only
+// engine's luma guide: it runs the motion machinery on the luma plane for the chroma pass to read,
+// and no filter (engine/spec.rs:220-236).
 std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels channels, uint32_t width,
                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                        std::unique_ptr<Pass>* result, bool guides_only = false);
+                                        bool colour_frames, std::unique_ptr<Pass>* result,
+                                        bool guides_only = false);
 
 // The luma pass's window motion mapped onto the chroma pass's block grid, shared by the two passes
 // of one engine (motion/luma_ring.rs, motion/chroma_map.rs): one slot of 2d chroma fields per

@@ -231,15 +231,17 @@ cudaError_t launch_chain_compose(const int32_t* pair_ring, int32_t* mv_field, in
 // per 32x8 block partials (2 lanes each), optional frame totals (2 floats) and optional per-channel
 // lower quartile of the block sigmas (2 floats; unused channels 0). `scale` is sqrt(pi / 2) in f32.
 size_t immerkaer_partials_len(int width, int height);
-// Automatic noise estimate without motion compensation (noise_estimate.cu).
+// Automatic noise estimate (noise_estimate.cu).
 size_t noise_scratch_floats(int width, int height);
 size_t noise_records_floats(int width, int height, int channels);
-// With `mv_field` (null for none) each block reads `prev` along its motion block's vector.
+// With `mv_field` (null for none) each block reads `prev` along its motion block's vector; with
+// `luma_fields` each record also carries its four 8x8 quarters' fields, from which a reading with
+// `curve` builds the noise curve.
 cudaError_t launch_temporal_stats(const float* next, const float* prev, int channels, int width, int height,
                                   const int32_t* mv_field, int mv_blocks_x, int mv_blocks_y, int mv_step,
-                                  float* records, cudaStream_t s);
+                                  bool luma_fields, float* records, cudaStream_t s);
 cudaError_t launch_noise_reading(const float* records, int channels, int width, int height, float* scratch,
-                                 uint32_t min_accepted, float* reading, cudaStream_t s);
+                                 uint32_t min_accepted, bool curve, float* reading, cudaStream_t s);
 cudaError_t launch_noise_fold(const float* records, const float* results, int capacity, int first, int last,
                               const float* settings, int channels, int table_radius, float* state, float* derived,
                               float* spatial, float* pilot, cudaStream_t s);

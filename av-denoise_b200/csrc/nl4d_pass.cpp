@@ -46,17 +46,22 @@ class Nl4dPass final : public Pass {
    public:
     static std::optional<Failure> create(const AvdNl4dOptions& o, Channels channels, uint32_t width,
                                          uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                         std::unique_ptr<Pass>* result, bool guides_only = false) {
-        // nl4d/denoiser.rs:228-233: without a pinned sigma the front measures the noise; luma applies
-        // the noise map and chroma the colour gains, neither of which is built.
-        if (!o.has_sigma && channels == Channels::Chroma)
+                                         bool colour_frames, std::unique_ptr<Pass>* result,
+                                         bool guides_only = false) {
+        // nl4d/denoiser.rs:228-233: a luma filter pass applies the noise map (the measured luma noise
+        // curve); a measured pass over frames with chroma also scales its thresholds by the colour
+        // grain gains when it applies the noise map or filters chroma, which are not built here.
+        const bool noise_map = o.noise_map && channels == Channels::Luma && !guides_only;
+        const bool colour_gains = !o.has_sigma && colour_frames && (noise_map || channels == Channels::Chroma);
+        if (colour_gains && channels == Channels::Chroma)
             return Failure{AVD_ERR_INVALID_OPTIONS,
                            "NL4D chroma with the automatic noise estimate needs the colour grain gains, which are "
                            "not available in this build; set sigma"};
-        if (!o.has_sigma && o.noise_map)
+        if (colour_gains)
             return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "the NL4D luma noise map of the automatic noise estimate is not available in this build; "
-                           "set noise_map to false or set sigma"};
+                           "the NL4D luma noise map of the automatic noise estimate on frames with chroma needs the "
+                           "colour grain gains, which are not available in this build; set noise_map to false or "
+                           "set sigma"};
         const AvdMotionSearch& m = o.motion;
         // motion/search.rs:133-139: Auto resolves to Chained { refine_radius: 2 } at d >= 3.
         const bool chained = m.estimation == AVD_ESTIMATION_CHAINED ||
@@ -93,6 +98,7 @@ class Nl4dPass final : public Pass {
         p->ceiling_ = m.max_search_escalation > m.search_radius ? static_cast<int>(m.max_search_escalation) : 0;
         p->measures_ = !o.has_sigma;
         p->guides_ = guides_only;
+        p->noise_map_ = noise_map;
         if (auto f = p->allocate()) return f;
         *result = std::move(p);
         return std::nullopt;
@@ -306,6 +312,7 @@ class Nl4dPass final : public Pass {
             cfg.temporal_radius = d_;
             FoldCoefficients& k = cfg.coefficients;
             k.sigma_scale = opts_.sigma_scale;
+            k.curve_applies = noise_map_;
             k.weight_g_max = g_max;
             k.h2_auto = true;
             const float area = 81.0f, unit_strength = 1.2f * 1.0f * 255.0f;
@@ -320,6 +327,7 @@ class Nl4dPass final : public Pass {
             cfg.levels = static_cast<int>(opts_.motion.pyramid_levels);
             cfg.thsad = thsad_;
             cfg.ceiling = ceiling_;
+            cfg.luma_fields = noise_map_;
             if (auto f = noise_.allocate(cfg)) return f;
         }
         return std::nullopt;
@@ -328,7 +336,9 @@ class Nl4dPass final : public Pass {
     // The derived words a pass reads (sigma per channel, weight scale, curve flag, motion SAD floor):
     // the measured front's, or the pinned sigma's.
     const float* noise_words() const { return measures_ ? noise_.derived() : tables_.as<float>(); }
-    const float* noise_curve() const { return tables_.as<float>() + 8; }
+    // The luma noise curve's ratios: the measured front's (read only while its derived curve flag is
+    // set), or the pinned sigma's zeros.
+    const float* noise_curve() const { return measures_ ? noise_.curve_ratios() : tables_.as<float>() + 8; }
     const float* dct_profile() const { return tables_.as<float>() + 24; }
     const float* kaiser_taps() const { return tables_.as<float>() + 32; }
 
@@ -928,6 +938,7 @@ class Nl4dPass final : public Pass {
     std::deque<uint32_t> pending_;
     size_t tail_remaining_ = 0, pushes_ = 0;
     bool pushed_ = false, poisoned_ = false;
+    bool noise_map_ = false;  // the filter scales the luma threshold by the measured noise curve
     std::optional<uint32_t> emitted_;
     DeviceTimer timer_;
 };
@@ -936,8 +947,8 @@ class Nl4dPass final : public Pass {
 
 std::optional<Failure> create_nl4d_pass(const AvdNl4dOptions& options, Channels channels, uint32_t width,
                                         uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
-                                        std::unique_ptr<Pass>* result, bool guides_only) {
-    return Nl4dPass::create(options, channels, width, height, in, out, result, guides_only);
+                                        bool colour_frames, std::unique_ptr<Pass>* result, bool guides_only) {
+    return Nl4dPass::create(options, channels, width, height, in, out, colour_frames, result, guides_only);
 }
 
 std::optional<Failure> link_nl4d_luma_motion(Pass* luma, Pass* chroma, int shift_x, int shift_y) {

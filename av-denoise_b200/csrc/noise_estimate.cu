@@ -2,14 +2,17 @@
 // statistics, one frame's reading and the window fold into the derived words and offset tables.
 //
 // Reference behaviour (av-denoise-core/src/noise):
-//   kernels/stats.rs:141-420   `nlm_temporal_noise_stats`: per 16x16 block the per-channel sums of
+//   kernels/stats.rs:141-620   `nlm_temporal_noise_stats`: per 16x16 block the per-channel sums of
 //                              d = new - prev and d^2 and the lag-1 channel-0 product, each summed
 //                              over the block's 256 threads in thread order; each channel's texture
 //                              from 4x4 cell means (stats.rs:599-650); with a motion field, the
-//                              compensated variant's vector check. No luma quarter fields.
+//                              compensated variant's vector check; with the luma fields, each 8x8
+//                              quarter's residual sums, luma sum, minimum, maximum and flatness.
 //   kernels/sample.rs:143-803  `noise_block_derive`, `noise_block_accept`, `noise_sample_finish`:
 //                              the static gate, the outlier ceiling, the moved-texture threshold, the
-//                              kept sigmas' median and lower quartile, the median correlation.
+//                              kept sigmas' median and lower quartile, the median correlation; with
+//                              the luma fields, the noise curve (kernels/curve.rs:37-133): the static
+//                              quarters' median sigma and the 16 luma bins' medians, interpolated.
 //   kernels/window.rs:1-498, kernels/derive.rs:1-192
 //                              `noise_window_fold`: four chains' medians over the window, the stream
 //                              state, the derived words and both NLM offset tables.
@@ -39,10 +42,19 @@ constexpr float kRhoSigmaGate = 0.3f / 255.0f;
 constexpr float kOutlierFactor = 5.0f;
 constexpr float kSigmaFloor = 0.1f / 255.0f;
 constexpr float kSqrt2 = 1.41421356237309504880f;
+// The luma quarter fields (noise/temporal.rs:20-62) and the noise curve (noise/curve.rs:21-50).
+constexpr int kQuarterBase = 3, kQuarterFields = 6;
+constexpr int Q_SUM_D = 0, Q_SUM_D2 = 1, Q_LUMA_SUM = 2, Q_FLATNESS = 3, Q_LUMA_MIN = 4, Q_LUMA_MAX = 5;
+constexpr float kUnmeasuredFlatness = 3.0e38f;
+constexpr int kCurveBins = 16;
+constexpr uint32_t kMinBinQuarters = 32, kMinPopulatedBins = 3;
+constexpr float kClipLow = 4.0f / 255.0f, kClipHigh = 251.0f / 255.0f, kFlatFactor = 0.5f;
+constexpr float kFlatFloor = (1.0f / 255.0f) * (1.0f / 255.0f);
+constexpr float kQuarterStaticGate = 2.0f * kStaticGate;
 
 // Reading, fold-settings, state and derived word layouts (noise/reading.rs, fold.rs, derived.rs).
 constexpr int R_VALID = 2, R_SIGMA = 4, R_SIGMA_LOW = 6, R_RHO = 8, R_STATIC = 9, R_ACCEPTED = 10,
-              R_CURVE_VALID = 11, R_QUARTER_MEDIAN = 12, R_RATIOS = 14;
+              R_CURVE_VALID = 11, R_QUARTER_MEDIAN = 12, R_POPULATED = 13, R_RATIOS = 14;
 constexpr int F_SIGMA_SCALE = 0, F_CURVE_APPLIES = 1, F_G_MAX = 2, F_W_FLOOR = 3, F_H2_AUTO = 4, F_H2_PIV = 5,
               F_H2_FIXED = 6, F_PILOT = 7, F_OFFSET_PV = 8, F_MAIN_OFFSET = 9, F_SAD = 10, F_CONF_SAD = 11,
               F_IMM = 12, F_SEG = 13;
@@ -74,7 +86,7 @@ struct StatsMotion {
     int blocks_x, blocks_y, step;
 };
 
-template <int C, bool COMP>
+template <int C, bool COMP, bool LF>
 __global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __restrict__ next,
                                                              const float* __restrict__ prev, int width, int height,
                                                              StatsMotion motion, float* __restrict__ records) {
@@ -141,14 +153,16 @@ __global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __rest
     }
     const bool valid = gx < width && gy < height && matched;
 
-    float nv[C], d[C];
+    float nv[C], d[C], prev_luma = 0.0f;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         nv[c] = 0.0f;
         d[c] = 0.0f;
         if (valid) {
             nv[c] = next[at(gx, gy, c)];
-            d[c] = nv[c] - prev[at(gx + sx, gy + sy, c)];
+            const float p = prev[at(gx + sx, gy + sy, c)];
+            d[c] = nv[c] - p;
+            if (c == 0) prev_luma = p;
         }
         scratch[t * L + c] = d[c];
         scratch[t * L + C + c] = d[c] * d[c];
@@ -163,9 +177,9 @@ __global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __rest
         for (int i = 0; i < 256; ++i) total += scratch[i * L + t];
         out[t] = total;
     }
-    // The moved lane, then the quarter lanes as zero (no luma fields).
+    // The moved lane, then the quarter lanes as zero without the luma fields.
     if (t == 2 * C + 2) out[t] = moved ? 1.0f : 0.0f;
-    if (t > 2 * C + 2 && t < 2 * C + 27) out[t] = 0.0f;
+    if (!LF && t > 2 * C + 2 && t < 2 * C + 27) out[t] = 0.0f;
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         __syncthreads();
@@ -202,11 +216,81 @@ __global__ void __launch_bounds__(256) temporal_stats_kernel(const float* __rest
             out[texture_lane(C, c)] = pairs ? energy / static_cast<float>(pairs) : 0.0f;
         }
     }
+    if constexpr (LF) {
+        // kernels/stats.rs:476-606: each quarter's 64 pixels sit at slots quarter * 64 + position
+        // and fold in halving rounds of 32..1; an invalid pixel seeds the sum with 0, the minimum
+        // with 1e30 and the maximum with -1e30. The flatness averages the pixels' mean of new and
+        // previous luma over 2x2 cells of an 8x8 grid, scores each cell's squared difference to its
+        // right and lower neighbour inside its quarter, folds each quarter's 16 scores in halving
+        // rounds of 8..1 and divides by its 24 pairs.
+        __shared__ float qsum[256], qlo[256], qhi[256], qrd[256], qrq[256], qcells[64], qpairs[64];
+        const int quarter = (ly / 8) * 2 + lx / 8, qpos = (ly % 8) * 8 + lx % 8, slot = quarter * 64 + qpos;
+        qsum[slot] = valid ? nv[0] : 0.0f;
+        qlo[slot] = valid ? nv[0] : 1.0e30f;
+        qhi[slot] = valid ? nv[0] : -1.0e30f;
+        qrd[slot] = d[0];
+        qrq[slot] = d[0] * d[0];
+        tile[t] = valid ? 0.5f * (nv[0] + prev_luma) : 0.0f;
+        __syncthreads();
+#pragma unroll
+        for (int stride = 32; stride >= 1; stride >>= 1) {
+            if (qpos < stride) {
+                qsum[slot] += qsum[slot + stride];
+                qrd[slot] += qrd[slot + stride];
+                qrq[slot] += qrq[slot + stride];
+                qlo[slot] = fminf(qlo[slot], qlo[slot + stride]);
+                qhi[slot] = fmaxf(qhi[slot], qhi[slot + stride]);
+            }
+            __syncthreads();
+        }
+        if (t < 64) {
+            const int cy = t / 8, cx = t % 8;
+            float cell = 0.0f;
+#pragma unroll
+            for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+                for (int dx = 0; dx < 2; ++dx) cell += tile[(2 * cy + dy) * kNB + 2 * cx + dx];
+            qcells[t] = cell / 4.0f;
+        }
+        __syncthreads();
+        if (t < 64) {
+            const int cy = t / 8, cx = t % 8;
+            const float here = qcells[t];
+            float energy = 0.0f;
+            if (cx % 4 != 3) {
+                const float s = here - qcells[t + 1];
+                energy += s * s;
+            }
+            if (cy % 4 != 3) {
+                const float s = here - qcells[t + 8];
+                energy += s * s;
+            }
+            qpairs[((cy / 4) * 2 + cx / 4) * 16 + (cy % 4) * 4 + cx % 4] = energy;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int stride = 8; stride >= 1; stride >>= 1) {
+            if (t < 64 && t % 16 < stride) qpairs[t] += qpairs[t + stride];
+            __syncthreads();
+        }
+        if (qpos == 0) {
+            float* f = out + 2 * C + kQuarterBase + quarter * kQuarterFields;
+            const bool full = bw >= (quarter % 2 + 1) * 8 && bh >= (quarter / 2 + 1) * 8;
+            // An unmatched block reads as no measurable noise: its seeds and sentinel give way to zeros.
+            f[Q_SUM_D] = matched ? qrd[slot] : 0.0f;
+            f[Q_SUM_D2] = matched ? qrq[slot] : 0.0f;
+            f[Q_LUMA_SUM] = matched ? qsum[slot] : 0.0f;
+            f[Q_FLATNESS] = matched ? (full ? qpairs[quarter * 16] / 24.0f : kUnmeasuredFlatness) : 0.0f;
+            f[Q_LUMA_MIN] = matched ? qlo[slot] : 0.0f;
+            f[Q_LUMA_MAX] = matched ? qhi[slot] : 0.0f;
+        }
+    }
 }
 
 // ---- the reading ------------------------------------------------------------------------------
 
-// The per-block values the reading works from (global scratch, one array per field).
+// The per-block values the reading works from (global scratch, one array per field), then one
+// sigma and one tag per 8x8 quarter for the noise curve.
 struct BlockScratch {
     float* sigma[kNoiseChannels];
     float* texture[kNoiseChannels];
@@ -217,22 +301,30 @@ struct BlockScratch {
     float* rho;
     uint32_t* flags;  // per channel: bit 0 candidate, bit 1 measurable, bit 2 kept, bit 3 accepted; bit 8 moved,
                       // bit 9 has_rho
+    float* quarter_sigma;
+    uint32_t* quarter_tag;  // bit 8: in the static quarter set; bits 0-7: its luma bin, or kNoBin
 };
 
-enum SetKind : int { kSetReference, kSetTexture, kSetKept, kSetRho };
+constexpr uint32_t kNoBin = 0xFFu, kQuarterMember = 0x100u;
+constexpr int kBinQueries = 2 * kCurveBins;
+
+enum SetKind : int { kSetReference, kSetTexture, kSetKept, kSetRho, kSetQuarter };
 
 struct ReadingShared {
-    uint32_t hist[4][256];
-    uint32_t prefix[4], rank[4];
+    uint32_t hist[kBinQueries][256];
+    uint32_t prefix[kBinQueries], rank[kBinQueries];
     uint32_t ref_n[kNoiseChannels], excl_n[kNoiseChannels], tex_n[kNoiseChannels], kept_n[kNoiseChannels],
         acc_n[kNoiseChannels], rho_n;
     uint32_t ref_min[kNoiseChannels], ref_max[kNoiseChannels];
     float ceiling[kNoiseChannels], threshold[kNoiseChannels];
     uint32_t trusted[kNoiseChannels];
-    uint32_t result[4];
+    uint32_t result[kBinQueries];
+    uint32_t quarter_n, bin_n[kCurveBins];
 };
 
 __device__ __forceinline__ uint32_t set_key(const BlockScratch& s, int kind, int c, int i) {
+    if (kind == kSetQuarter)
+        return (s.quarter_tag[i] & kQuarterMember) ? order_key(s.quarter_sigma[i]) : kExcluded;
     const uint32_t f = s.flags[i] >> (4 * c);
     switch (kind) {
         case kSetReference: return ((f & 3u) == 3u) ? order_key(s.sigma[c][i]) : kExcluded;
@@ -243,29 +335,29 @@ __device__ __forceinline__ uint32_t set_key(const BlockScratch& s, int kind, int
     }
 }
 
-// The keys of ranks[0..nq) among the set's elements (all ranks below the set's count), exactly:
-// four 8-bit radix passes, one histogram per query, one warp scanning each query's histogram.
-__device__ void select_ranks(const BlockScratch& s, int kind, int c, int n, const uint32_t* ranks, int nq,
-                             ReadingShared& sh) {
+// Exact order statistics by four 8-bit radix passes: query q asks for the element of rank
+// sh.rank[q] among the elements that `element(i, key, first, last)` assigns to it (element i joins
+// queries first..last-1 with `key`, or none when it returns false). One histogram per query, one
+// warp scanning each query's histogram; sh.result[q] receives the key.
+template <typename Element>
+__device__ void radix_select(int n, int nq, ReadingShared& sh, Element element) {
     const int t = threadIdx.x;
-    if (t < nq) {
-        sh.prefix[t] = 0;
-        sh.rank[t] = ranks[t];
-    }
+    if (t < nq) sh.prefix[t] = 0;
     uint32_t mask = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int i = t; i < 4 * 256; i += blockDim.x) (&sh.hist[0][0])[i] = 0;
+        for (int i = t; i < nq * 256; i += blockDim.x) (&sh.hist[0][0])[i] = 0;
         __syncthreads();
         for (int i = t; i < n; i += blockDim.x) {
-            const uint32_t key = set_key(s, kind, c, i);
-            if (key == kExcluded) continue;
-            for (int q = 0; q < nq; ++q)
+            uint32_t key;
+            int first, last;
+            if (!element(i, key, first, last)) continue;
+            for (int q = first; q < last; ++q)
                 if ((key & mask) == sh.prefix[q]) atomicAdd(&sh.hist[q][(key >> shift) & 0xFFu], 1u);
         }
         __syncthreads();
         const int warp = t / 32, lane = t % 32;
-        if (warp < nq) {
-            const uint32_t* h = sh.hist[warp];
+        for (int q = warp; q < nq; q += blockDim.x / 32) {
+            const uint32_t* h = sh.hist[q];
             uint32_t mine = 0;
             for (int b = 0; b < 8; ++b) mine += h[lane * 8 + b];
             uint32_t incl = mine;
@@ -273,15 +365,15 @@ __device__ void select_ranks(const BlockScratch& s, int kind, int c, int n, cons
                 const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
                 if (lane >= o) incl += v;
             }
-            const uint32_t below = incl - mine, rank = sh.rank[warp];
+            const uint32_t below = incl - mine, rank = sh.rank[q];
             if (rank >= below && rank < incl) {
                 uint32_t seen = below, b = 0;
                 for (; b < 8; ++b) {
                     if (rank < seen + h[lane * 8 + b]) break;
                     seen += h[lane * 8 + b];
                 }
-                sh.prefix[warp] |= static_cast<uint32_t>(lane * 8 + b) << shift;
-                sh.rank[warp] = rank - seen;
+                sh.prefix[q] |= static_cast<uint32_t>(lane * 8 + b) << shift;
+                sh.rank[q] = rank - seen;
             }
         }
         mask |= 0xFFu << shift;
@@ -289,6 +381,18 @@ __device__ void select_ranks(const BlockScratch& s, int kind, int c, int n, cons
     }
     if (t < nq) sh.result[t] = sh.prefix[t];
     __syncthreads();
+}
+
+// The keys of ranks[0..nq) among one set's elements (all ranks below the set's count).
+__device__ void select_ranks(const BlockScratch& s, int kind, int c, int n, const uint32_t* ranks, int nq,
+                             ReadingShared& sh) {
+    if (static_cast<int>(threadIdx.x) < nq) sh.rank[threadIdx.x] = ranks[threadIdx.x];
+    radix_select(n, nq, sh, [&](int i, uint32_t& key, int& first, int& last) {
+        key = set_key(s, kind, c, i);
+        first = 0;
+        last = nq;
+        return key != kExcluded;
+    });
 }
 
 __device__ __forceinline__ float quartile_from_pair(float low, float high, uint32_t count) {
@@ -311,10 +415,37 @@ __device__ void set_pairs(const BlockScratch& s, int kind, int c, int nb, uint32
     __syncthreads();
 }
 
+// kernels/sample.rs:95-104 (`static_quarter_sigma`) and kernels/curve.rs:93-133: quarter q of block
+// i's sigma, whether it passes the static gates and, if it also lies flat and unclipped, its bin.
+struct QuarterRead {
+    float sigma;
+    bool passes;
+    uint32_t bin;
+};
+
+__device__ QuarterRead read_quarter(const float* r, int C, int bw, int bh, int q, float flat_limit) {
+    const int qw = min(max(bw - (q % 2) * 8, 0), 8), qh = min(max(bh - (q / 2) * 8, 0), 8);
+    const float pixels = static_cast<float>(qw * qh);
+    const float* f = r + 2 * C + kQuarterBase + q * kQuarterFields;
+    const float divisor = pixels > 0.0f ? pixels : 1.0f;
+    const float mean = f[Q_SUM_D] / divisor;
+    const float ms = f[Q_SUM_D2] / divisor;
+    QuarterRead out;
+    out.sigma = sqrtf(fmaxf(ms - mean * mean, 0.0f)) / kSqrt2;
+    out.passes = pixels > 0.0f && fabsf(mean) < kQuarterStaticGate && out.sigma > kRhoSigmaGate;
+    const float mean_luma = f[Q_LUMA_SUM] / divisor;
+    const float scaled = fmaxf(mean_luma * static_cast<float>(kCurveBins), 0.0f);
+    const uint32_t bin = static_cast<uint32_t>(fminf(scaled, static_cast<float>(kCurveBins - 1)));
+    const bool textured = f[Q_FLATNESS] > flat_limit;
+    const bool clipped = f[Q_LUMA_MIN] < kClipLow || f[Q_LUMA_MAX] > kClipHigh;
+    out.bin = (textured || clipped) ? kNoBin : bin;
+    return out;
+}
+
 template <int C>
 __global__ void __launch_bounds__(kReadingThreads) noise_reading_kernel(const float* __restrict__ records, int width,
                                                                        int height, BlockScratch s, uint32_t min_accepted,
-                                                                       float* __restrict__ reading) {
+                                                                       bool curve, float* __restrict__ reading) {
     __shared__ ReadingShared sh;
     const int t = threadIdx.x;
     const int bxn = (width + kNB - 1) / kNB, byn = (height + kNB - 1) / kNB, nb = bxn * byn;
@@ -433,6 +564,66 @@ __global__ void __launch_bounds__(kReadingThreads) noise_reading_kernel(const fl
     for (int c = 0; c < C; ++c) set_pairs(s, kSetKept, c, nb, sh.kept_n[c], kept[c], sh);
     float rho_pair[4];
     set_pairs(s, kSetRho, 0, nb, sh.rho_n, rho_pair, sh);
+
+    // The noise curve (kernels/sample.rs:482-510, kernels/curve.rs:37-133, sample.rs:717-803): the
+    // quarters of channel-0 accepted blocks that pass the static gates form the quarter set; those
+    // that are also flat (against a gate from channel 0's kept sigma median) and unclipped join the
+    // bin of their mean luma. The set's median and each bin's median are exact selects.
+    float quarter_median = 0.0f;
+    float bin_median[kCurveBins];
+    if (curve) {
+        const float sigma_median = median_from_pair(kept[0][0], kept[0][1]);
+        const float flat_limit = fmaxf(kFlatFactor * sigma_median * sigma_median, kFlatFloor);
+        if (t < kCurveBins) sh.bin_n[t] = 0;
+        if (t == 0) sh.quarter_n = 0;
+        __syncthreads();
+        const int nq = 4 * nb;
+        for (int base = 0; base < nq; base += blockDim.x) {
+            const int i = base + t;
+            uint32_t tag = kNoBin;
+            if (i < nq) {
+                const int blk = i / 4, bx = blk % bxn, by = blk / bxn;
+                const int bw = min(kNB, width - bx * kNB), bh = min(kNB, height - by * kNB);
+                const QuarterRead qr =
+                    read_quarter(records + static_cast<int64_t>(blk) * record_len(C), C, bw, bh, i % 4, flat_limit);
+                if (qr.passes && (s.flags[blk] & 8u)) tag = kQuarterMember | qr.bin;
+                s.quarter_sigma[i] = qr.sigma;
+                s.quarter_tag[i] = tag;
+            }
+            const uint32_t members = __ballot_sync(0xFFFFFFFFu, tag & kQuarterMember);
+            if ((t & 31) == 0 && members) atomicAdd(&sh.quarter_n, static_cast<uint32_t>(__popc(members)));
+            const uint32_t bin = tag & 0xFFu;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, bin);
+            if (bin < kCurveBins && (t & 31) == __ffs(peers) - 1)
+                atomicAdd(&sh.bin_n[bin], static_cast<uint32_t>(__popc(peers)));
+        }
+        __threadfence_block();
+        __syncthreads();
+        const uint32_t qn = sh.quarter_n;
+        if (qn > 0) {
+            const uint32_t ranks[2] = {(qn - 1) / 2, qn / 2};
+            select_ranks(s, kSetQuarter, 0, nq, ranks, 2, sh);
+            quarter_median = median_from_pair(key_value(sh.result[0]), key_value(sh.result[1]));
+        }
+        // Queries 2b and 2b + 1 are bin b's lower and upper median.
+        if (t < kBinQueries) {
+            const uint32_t n = sh.bin_n[t / 2];
+            sh.rank[t] = n == 0 ? 0 : ((t % 2) ? n / 2 : (n - 1) / 2);
+        }
+        radix_select(nq, kBinQueries, sh, [&](int i, uint32_t& key, int& first, int& last) {
+            const uint32_t tag = s.quarter_tag[i];
+            const uint32_t bin = tag & 0xFFu;
+            if (!(tag & kQuarterMember) || bin >= static_cast<uint32_t>(kCurveBins)) return false;
+            key = order_key(s.quarter_sigma[i]);
+            first = static_cast<int>(2 * bin);
+            last = first + 2;
+            return true;
+        });
+        for (int b = 0; b < kCurveBins; ++b)
+            bin_median[b] = sh.bin_n[b] ? median_from_pair(key_value(sh.result[2 * b]), key_value(sh.result[2 * b + 1]))
+                                        : 0.0f;
+    }
+
     if (t == 0) {
         auto channel_valid = [&](int c) { return c < C && sh.acc_n[c] >= min_accepted && sh.kept_n[c] > 0; };
         const bool valid0 = sh.rho_n > 0 && channel_valid(0);
@@ -448,7 +639,54 @@ __global__ void __launch_bounds__(kReadingThreads) noise_reading_kernel(const fl
         reading[R_RHO] = valid0 ? median_from_pair(rho_pair[0], rho_pair[1]) : 0.0f;
         reading[R_STATIC] = valid0 ? static_fraction : 0.0f;
         reading[R_ACCEPTED] = static_cast<float>(sh.acc_n[0]);
-        for (int w = R_ACCEPTED + 1; w < kReadingWords; ++w) reading[w] = 0.0f;
+        if (!curve) {
+            for (int w = R_ACCEPTED + 1; w < kReadingWords; ++w) reading[w] = 0.0f;
+        } else {
+            // curve_bin_sigma (sample.rs:747-803): flat before the first and past the last populated
+            // bin, linear between the nearest populated bin below and the nearest at or above.
+            uint32_t populated = 0;
+            int first_index = 0, last_index = 0;
+            float first_sigma = 0.0f, last_sigma = 0.0f;
+            for (int b = 0; b < kCurveBins; ++b) {
+                if (sh.bin_n[b] < kMinBinQuarters) continue;
+                if (populated == 0) {
+                    first_index = b;
+                    first_sigma = bin_median[b];
+                }
+                last_index = b;
+                last_sigma = bin_median[b];
+                ++populated;
+            }
+            const bool curve_valid =
+                valid0 && sh.quarter_n > 0 && quarter_median > 0.0f && populated >= kMinPopulatedBins;
+            const float divisor = curve_valid ? quarter_median : 1.0f;
+            for (int bin = 0; bin < kCurveBins; ++bin) {
+                int low_index = 0, high_index = 0;
+                float low_sigma = 0.0f, high_sigma = 0.0f;
+                bool has_high = false;
+                for (int b = 0; b < kCurveBins; ++b) {
+                    if (sh.bin_n[b] < kMinBinQuarters) continue;
+                    if (b < bin) {
+                        low_index = b;
+                        low_sigma = bin_median[b];
+                    }
+                    if (b >= bin && !has_high) {
+                        high_index = b;
+                        high_sigma = bin_median[b];
+                        has_high = true;
+                    }
+                }
+                const int span_bins = high_index > low_index ? high_index - low_index : 1;
+                const int offset_bins = bin - min(low_index, bin);
+                const float fraction = static_cast<float>(offset_bins) / static_cast<float>(span_bins);
+                const float between = low_sigma + (high_sigma - low_sigma) * fraction;
+                const float sigma = bin <= first_index ? first_sigma : (bin >= last_index ? last_sigma : between);
+                reading[R_RATIOS + bin] = curve_valid ? sigma / divisor : 0.0f;
+            }
+            reading[R_CURVE_VALID] = curve_valid ? 1.0f : 0.0f;
+            reading[R_QUARTER_MEDIAN] = curve_valid ? quarter_median : 0.0f;
+            reading[R_POPULATED] = static_cast<float>(populated);
+        }
     }
 }
 
@@ -620,7 +858,7 @@ __global__ void __launch_bounds__(256) noise_fold_kernel(const float* __restrict
 
 size_t noise_scratch_floats(int width, int height) {
     const size_t nb = static_cast<size_t>((width + kNB - 1) / kNB) * ((height + kNB - 1) / kNB);
-    return nb * 10;  // sigma x2, texture x2, mean0, var0, mean_lag, pairs, rho, flags
+    return nb * 18;  // sigma x2, texture x2, mean0, var0, mean_lag, pairs, rho, flags; 4 quarter sigmas, 4 tags
 }
 
 size_t noise_records_floats(int width, int height, int channels) {
@@ -629,29 +867,30 @@ size_t noise_records_floats(int width, int height, int channels) {
 
 cudaError_t launch_temporal_stats(const float* next, const float* prev, int channels, int width, int height,
                                   const int32_t* mv_field, int mv_blocks_x, int mv_blocks_y, int mv_step,
-                                  float* records, cudaStream_t s) {
+                                  bool luma_fields, float* records, cudaStream_t s) {
     if (channels < 1 || channels > 2 || width < 1 || height < 1) return cudaErrorInvalidValue;
     if (mv_field && (mv_blocks_x < 1 || mv_blocks_y < 1 || mv_step < 1)) return cudaErrorInvalidValue;
     dim3 grid((width + kNB - 1) / kNB, (height + kNB - 1) / kNB);
     if (!prev)  // the first frame of a stream has no previous frame: its records are zero
         return cudaMemsetAsync(records, 0, noise_records_floats(width, height, channels) * sizeof(float), s);
     const StatsMotion m{mv_field, mv_blocks_x, mv_blocks_y, mv_step};
-    if (channels == 1) {
-        if (mv_field)
-            temporal_stats_kernel<1, true><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
-        else
-            temporal_stats_kernel<1, false><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
-    } else {
-        if (mv_field)
-            temporal_stats_kernel<2, true><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
-        else
-            temporal_stats_kernel<2, false><<<grid, 256, 0, s>>>(next, prev, width, height, m, records);
+    auto run = [&](auto kernel) { kernel<<<grid, 256, 0, s>>>(next, prev, width, height, m, records); };
+    const int variant = (channels - 1) * 4 + (mv_field ? 2 : 0) + (luma_fields ? 1 : 0);
+    switch (variant) {
+        case 0: run(temporal_stats_kernel<1, false, false>); break;
+        case 1: run(temporal_stats_kernel<1, false, true>); break;
+        case 2: run(temporal_stats_kernel<1, true, false>); break;
+        case 3: run(temporal_stats_kernel<1, true, true>); break;
+        case 4: run(temporal_stats_kernel<2, false, false>); break;
+        case 5: run(temporal_stats_kernel<2, false, true>); break;
+        case 6: run(temporal_stats_kernel<2, true, false>); break;
+        default: run(temporal_stats_kernel<2, true, true>); break;
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_noise_reading(const float* records, int channels, int width, int height, float* scratch,
-                                 uint32_t min_accepted, float* reading, cudaStream_t s) {
+                                 uint32_t min_accepted, bool curve, float* reading, cudaStream_t s) {
     if (channels < 1 || channels > 2 || width < 1 || height < 1) return cudaErrorInvalidValue;
     if (!records) {
         spatial_reading_kernel<<<1, 32, 0, s>>>(reading);
@@ -669,10 +908,12 @@ cudaError_t launch_noise_reading(const float* records, int channels, int width, 
     b.pairs = scratch + 7 * nb;
     b.rho = scratch + 8 * nb;
     b.flags = reinterpret_cast<uint32_t*>(scratch + 9 * nb);
+    b.quarter_sigma = scratch + 10 * nb;
+    b.quarter_tag = reinterpret_cast<uint32_t*>(scratch + 14 * nb);
     if (channels == 1)
-        noise_reading_kernel<1><<<1, kReadingThreads, 0, s>>>(records, width, height, b, min_accepted, reading);
+        noise_reading_kernel<1><<<1, kReadingThreads, 0, s>>>(records, width, height, b, min_accepted, curve, reading);
     else
-        noise_reading_kernel<2><<<1, kReadingThreads, 0, s>>>(records, width, height, b, min_accepted, reading);
+        noise_reading_kernel<2><<<1, kReadingThreads, 0, s>>>(records, width, height, b, min_accepted, curve, reading);
     return cudaGetLastError();
 }
 

@@ -158,12 +158,14 @@ std::optional<Failure> NoiseFront::read_against(size_t frame, std::optional<size
     if (cfg_.temporal_radius > 0) {
         const float* p = prev ? slot(*prev) : nullptr;
         const int32_t* field = (cfg_.motion && prev) ? pair_.as<int32_t>() + direction * mv_stride_ : nullptr;
-        e = launch_temporal_stats(slot(frame), p, c, w, h, field, blocks_x_, blocks_y_, step_, records_.as<float>(), s);
+        e = launch_temporal_stats(slot(frame), p, c, w, h, field, blocks_x_, blocks_y_, step_, cfg_.luma_fields,
+                                  records_.as<float>(), s);
         if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("temporal noise stats launch", e)};
         records = records_.as<float>();
     }
     const uint32_t blocks = ((cfg_.width + 15) / 16) * ((cfg_.height + 15) / 16);
-    e = launch_noise_reading(records, c, w, h, scratch_.as<float>(), min_static_blocks(blocks), reading, s);
+    e = launch_noise_reading(records, c, w, h, scratch_.as<float>(), min_static_blocks(blocks),
+                             cfg_.luma_fields && cfg_.temporal_radius > 0, reading, s);
     if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise reading launch", e)};
     return std::nullopt;
 }

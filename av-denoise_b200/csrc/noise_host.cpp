@@ -73,13 +73,13 @@ uint64_t avd_noise_scratch_floats(uint32_t width, uint32_t height) {
 }
 
 AvdStatus avd_noise_temporal_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width, uint32_t height,
-                                   uint64_t records, void* stream) {
+                                   uint32_t luma_fields, uint64_t records, void* stream) {
     if (!next || !records) return fail(AVD_ERR_NULL_ARG, "noise temporal stats: null buffer");
     if (channels < 1 || channels > 2 || width == 0 || height == 0)
         return fail(AVD_ERR_INVALID_GEOMETRY, "noise temporal stats: bad geometry");
     cudaError_t e = avd::launch_temporal_stats(reinterpret_cast<const float*>(next), reinterpret_cast<const float*>(prev),
                                                static_cast<int>(channels), static_cast<int>(width),
-                                               static_cast<int>(height), nullptr, 0, 0, 0,
+                                               static_cast<int>(height), nullptr, 0, 0, 0, luma_fields != 0,
                                                reinterpret_cast<float*>(records), static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("noise temporal stats launch: ") + cudaGetErrorString(e));
     return AVD_OK;
@@ -87,7 +87,7 @@ AvdStatus avd_noise_temporal_stats(uint64_t next, uint64_t prev, uint32_t channe
 
 AvdStatus avd_noise_compensated_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width, uint32_t height,
                                       uint64_t mv_field, uint32_t mv_blocks_x, uint32_t mv_blocks_y, uint32_t mv_step,
-                                      uint64_t records, void* stream) {
+                                      uint32_t luma_fields, uint64_t records, void* stream) {
     if (!next || !prev || !records || !mv_field) return fail(AVD_ERR_NULL_ARG, "noise compensated stats: null buffer");
     if (channels < 1 || channels > 2 || width == 0 || height == 0 || mv_blocks_x == 0 || mv_blocks_y == 0 ||
         mv_step == 0)
@@ -95,15 +95,15 @@ AvdStatus avd_noise_compensated_stats(uint64_t next, uint64_t prev, uint32_t cha
     cudaError_t e = avd::launch_temporal_stats(
         reinterpret_cast<const float*>(next), reinterpret_cast<const float*>(prev), static_cast<int>(channels),
         static_cast<int>(width), static_cast<int>(height), reinterpret_cast<const int32_t*>(mv_field),
-        static_cast<int>(mv_blocks_x), static_cast<int>(mv_blocks_y), static_cast<int>(mv_step),
+        static_cast<int>(mv_blocks_x), static_cast<int>(mv_blocks_y), static_cast<int>(mv_step), luma_fields != 0,
         reinterpret_cast<float*>(records), static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess)
         return fail(AVD_ERR_GPU, std::string("noise compensated stats launch: ") + cudaGetErrorString(e));
     return AVD_OK;
 }
 
-AvdStatus avd_noise_reading(uint64_t records, uint32_t channels, uint32_t width, uint32_t height, uint64_t scratch,
-                            uint64_t reading, void* stream) {
+AvdStatus avd_noise_reading(uint64_t records, uint32_t channels, uint32_t width, uint32_t height, uint32_t curve,
+                            uint64_t scratch, uint64_t reading, void* stream) {
     if (!reading || (records && !scratch)) return fail(AVD_ERR_NULL_ARG, "noise reading: null buffer");
     if (channels < 1 || channels > 2 || width == 0 || height == 0)
         return fail(AVD_ERR_INVALID_GEOMETRY, "noise reading: bad geometry");
@@ -111,7 +111,8 @@ AvdStatus avd_noise_reading(uint64_t records, uint32_t channels, uint32_t width,
     cudaError_t e = avd::launch_noise_reading(reinterpret_cast<const float*>(records), static_cast<int>(channels),
                                               static_cast<int>(width), static_cast<int>(height),
                                               reinterpret_cast<float*>(scratch), avd::min_static_blocks(blocks),
-                                              reinterpret_cast<float*>(reading), static_cast<cudaStream_t>(stream));
+                                              curve != 0, reinterpret_cast<float*>(reading),
+                                              static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("noise reading launch: ") + cudaGetErrorString(e));
     return AVD_OK;
 }

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define AVD_ABI_VERSION 2u
+#define AVD_ABI_VERSION 3u
 
 #if defined(__GNUC__)
 #define AVD_API __attribute__((visibility("default")))
@@ -563,11 +563,13 @@ AVD_API AvdStatus avd_immerkaer(uint64_t frame, uint32_t channels, uint32_t widt
 AVD_API uint64_t avd_noise_records_floats(uint32_t width, uint32_t height, uint32_t channels);
 AVD_API uint64_t avd_noise_scratch_floats(uint32_t width, uint32_t height);
 
-/* The temporal residual records of f32 frame `next` against `prev` (kernels/stats.rs:141-420,
- * `nlm_temporal_noise_stats` without motion compensation and without the luma quarter fields);
- * `prev` = 0 zeroes them, as a stream's first frame reads (noise/slot.rs:40-60). */
+/* The temporal residual records of f32 frame `next` against `prev` (kernels/stats.rs:141-620,
+ * `nlm_temporal_noise_stats` without motion compensation); with `luma_fields` each record also
+ * carries its four 8x8 quarters' residual sums, luma sum, minimum, maximum and flatness
+ * (stats.rs:466-606), else those lanes read 0. `prev` = 0 zeroes the records, as a stream's first
+ * frame reads (noise/slot.rs:40-60). */
 AVD_API AvdStatus avd_noise_temporal_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width,
-                                           uint32_t height, uint64_t records, void* stream);
+                                           uint32_t height, uint32_t luma_fields, uint64_t records, void* stream);
 
 /* The records of `next` against `prev` along a motion field (kernels/stats.rs:224-330, the compensated
  * variant): `mv_field` holds an int32 (dx, dy) per block of an mv_blocks_x x mv_blocks_y grid at
@@ -576,19 +578,22 @@ AVD_API AvdStatus avd_noise_temporal_stats(uint64_t next, uint64_t prev, uint32_
  * that leaves the frame writes an all-zero record. The moved lane records each followed block. */
 AVD_API AvdStatus avd_noise_compensated_stats(uint64_t next, uint64_t prev, uint32_t channels, uint32_t width,
                                               uint32_t height, uint64_t mv_field, uint32_t mv_blocks_x,
-                                              uint32_t mv_blocks_y, uint32_t mv_step, uint64_t records, void* stream);
+                                              uint32_t mv_blocks_y, uint32_t mv_step, uint32_t luma_fields,
+                                              uint64_t records, void* stream);
 
 /* One frame's reading, AVD_NOISE_READING_WORDS floats (noise/reading.rs:7-33), from its records
  * (0 without temporal stats: the reading is then the Immerkaer words alone) through
- * kernels/sample.rs:143-803. Words 0 and 1 must already hold the frame's Immerkaer lower quartiles
- * (`sigma_low` of avd_immerkaer); the call writes the rest. `scratch` holds
- * avd_noise_scratch_floats floats. */
+ * kernels/sample.rs:143-803. With `curve` (records taken with the luma fields) the reading also
+ * holds the noise curve: its flag, the static quarters' median sigma, the populated bin count and
+ * 16 ratios (kernels/curve.rs:37-133, sample.rs:717-803). Words 0 and 1 must already hold the
+ * frame's Immerkaer lower quartiles (`sigma_low` of avd_immerkaer); the call writes the rest.
+ * `scratch` holds avd_noise_scratch_floats floats. */
 #define AVD_NOISE_READING_WORDS 30
 #define AVD_NOISE_STATE_WORDS 32
 #define AVD_NOISE_DERIVED_WORDS 11
 #define AVD_NOISE_FOLD_WORDS 16
 AVD_API AvdStatus avd_noise_reading(uint64_t records, uint32_t channels, uint32_t width, uint32_t height,
-                                    uint64_t scratch, uint64_t reading, void* stream);
+                                    uint32_t curve, uint64_t scratch, uint64_t reading, void* stream);
 
 /* The fold settings words for a plane of width x height (noise/fold.rs:118-146, `fold_words`):
  * sigma_scale, whether the consumer applies the curve, the weight-scale gain and floor, the h2

@@ -4,17 +4,20 @@
 // arithmetic of its GPU kernels (every multiply and add separately rounded, sums in the kernels'
 // order; order statistics are exact, so they come from sorting):
 //
-//   temporal stats  av-denoise-core/src/noise/kernels/stats.rs:141-420 (`nlm_temporal_noise_stats`,
-//                   uncompensated, without the luma quarter fields): per 16x16 block the per-channel
-//                   sums of d = new - prev and d^2 and the lag-1 product of neighbouring channel-0
-//                   residuals, each summed over the block's 256 threads in thread order; each
-//                   channel's texture from 4x4 cell means (stats.rs:599-650).
+//   temporal stats  av-denoise-core/src/noise/kernels/stats.rs:141-620 (`nlm_temporal_noise_stats`):
+//                   per 16x16 block the per-channel sums of d = new - prev and d^2 and the lag-1
+//                   product of neighbouring channel-0 residuals, each summed over the block's 256
+//                   threads in thread order; each channel's texture from 4x4 cell means
+//                   (stats.rs:599-650); with the luma fields, each 8x8 quarter's residual sums, luma
+//                   sum, minimum, maximum and flatness (stats.rs:466-606).
 //   reading         kernels/sample.rs:143-803 (`noise_block_derive`, `noise_block_accept`,
 //                   `noise_sample_finish`) with the host statement noise/temporal.rs:360-721: the
 //                   static gate, the outlier ceiling from the lower quartile of the measurable
 //                   candidates, the moved-texture threshold, the per-channel median and lower
 //                   quartile of the kept block sigmas, the median lag-1 correlation and the static
-//                   fraction; the Immerkaer words are the lower quartile of the cube sigmas.
+//                   fraction; the Immerkaer words are the lower quartile of the cube sigmas. With
+//                   the luma fields, the noise curve (kernels/curve.rs:37-133, sample.rs:717-803):
+//                   the static quarters' median sigma and the 16 luma bins' medians, interpolated.
 //   window fold     kernels/window.rs:1-498 (`noise_window_fold`) and kernels/derive.rs:1-192
 //                   (`correlation_factor`, `write_derived`, `write_offset_tables`): the four chains'
 //                   medians over the window, the correlation and curve medians, the stream state,
@@ -45,6 +48,12 @@ constexpr float SIGMA_OUTLIER_FACTOR = 5.0f;
 constexpr float STATIC_FRACTION_MIN = 0.05f;
 constexpr float SIGMA_FLOOR = 0.1f / 255.0f;
 constexpr float SQRT_2F = 1.41421356237309504880f;
+// The noise curve (noise/curve.rs:21-50).
+constexpr int CURVE_BINS = 16;
+constexpr uint32_t MIN_BIN_QUARTERS = 32, MIN_POPULATED_BINS = 3;
+constexpr float CLIP_LOW = 4.0f / 255.0f, CLIP_HIGH = 251.0f / 255.0f, FLAT_FACTOR = 0.5f;
+constexpr float FLAT_FLOOR = (1.0f / 255.0f) * (1.0f / 255.0f);
+constexpr float QUARTER_STATIC_GATE = 2.0f * STATIC_GATE;
 
 // Reading words (noise/reading.rs:7-33).
 constexpr int R_IMM_LOW = 0, R_VALID = 2, R_SIGMA = 4, R_SIGMA_LOW = 6, R_RHO = 8, R_STATIC = 9, R_ACCEPTED = 10,
@@ -88,6 +97,85 @@ struct Sel {
     float texture_share() const { return n() ? at((n() - 1) * 2 / 5) : 0.0f; }
 };
 
+// The luma quarter fields of a temporal record (noise/temporal.rs:20-62).
+constexpr int QUARTERS = 4, QUARTER_SIZE = 8, QUARTER_FIELDS = 6, QUARTER_BASE = 3;
+constexpr int Q_SUM_D = 0, Q_SUM_D2 = 1, Q_LUMA_SUM = 2, Q_FLATNESS = 3, Q_LUMA_MIN = 4, Q_LUMA_MAX = 5;
+constexpr float UNMEASURED_FLATNESS = 3.0e38f;
+
+// kernels/stats.rs:466-606: the four 8x8 quarters' fields of one block, from its 256 threads
+// (t = ly * 16 + lx): whether the pixel is read, its new luma, the mean of its new and previous
+// luma, and its channel-0 residual. Each quarter's 64 values sit at slot quarter * 64 + (ly % 8) * 8
+// + lx % 8 and fold in halving rounds of stride 32, 16, ..., 1. The flatness averages the mean luma
+// over 2x2 pixels into an 8x8 grid of cells; each cell adds its squared difference to its right and
+// lower neighbour inside the quarter, and the quarter's 16 cell sums fold in halving rounds of 8, 4,
+// 2, 1 and are divided by its 24 pairs. A quarter not wholly inside the frame reads
+// UNMEASURED_FLATNESS; an unmatched block (a compensated block leaving the frame) writes zeros.
+void quarter_fields(float* out, int channels, int bw, int bh, bool matched, const bool* valid, const float* new_luma,
+                    const float* mean_luma, const float* d0) {
+    float sum[256], lo[256], hi[256], rd[256], rq[256], cells[64], pairs[64];
+    for (int t = 0; t < 256; ++t) {
+        const int lx = t % NB, ly = t / NB;
+        const int slot = ((ly / 8) * 2 + lx / 8) * 64 + (ly % 8) * 8 + lx % 8;
+        const float d = valid[t] ? d0[t] : 0.0f;
+        sum[slot] = valid[t] ? new_luma[t] : 0.0f;
+        lo[slot] = valid[t] ? new_luma[t] : 1.0e30f;
+        hi[slot] = valid[t] ? new_luma[t] : -1.0e30f;
+        rd[slot] = d;
+        rq[slot] = d * d;
+    }
+    for (int stride = 32; stride >= 1; stride >>= 1)
+        for (int q = 0; q < QUARTERS; ++q)
+            for (int p = 0; p < stride; ++p) {
+                const int here = q * 64 + p, there = here + stride;
+                sum[here] += sum[there];
+                rd[here] += rd[there];
+                rq[here] += rq[there];
+                lo[here] = std::min(lo[here], lo[there]);
+                hi[here] = std::max(hi[here], hi[there]);
+            }
+    for (int t = 0; t < 64; ++t) {
+        const int cy = t / 8, cx = t % 8;
+        float cell = 0.0f;
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                const int i = (2 * cy + dy) * NB + 2 * cx + dx;
+                cell += valid[i] ? mean_luma[i] : 0.0f;
+            }
+        cells[t] = cell / 4.0f;
+    }
+    for (int t = 0; t < 64; ++t) {
+        const int cy = t / 8, cx = t % 8;
+        const float here = cells[t];
+        float energy = 0.0f;
+        if (cx % 4 != 3) {
+            const float s = here - cells[t + 1];
+            energy += s * s;
+        }
+        if (cy % 4 != 3) {
+            const float s = here - cells[t + 8];
+            energy += s * s;
+        }
+        pairs[((cy / 4) * 2 + cx / 4) * 16 + (cy % 4) * 4 + cx % 4] = energy;
+    }
+    for (int stride = 8; stride >= 1; stride >>= 1)
+        for (int t = 0; t < 64; ++t)
+            if (t % 16 < stride) pairs[t] += pairs[t + stride];
+    for (int q = 0; q < QUARTERS; ++q) {
+        float* f = out + 2 * channels + QUARTER_BASE + q * QUARTER_FIELDS;
+        if (!matched) {
+            std::fill(f, f + QUARTER_FIELDS, 0.0f);
+            continue;
+        }
+        const bool full = bw >= (q % 2 + 1) * QUARTER_SIZE && bh >= (q / 2 + 1) * QUARTER_SIZE;
+        f[Q_SUM_D] = rd[q * 64];
+        f[Q_SUM_D2] = rq[q * 64];
+        f[Q_LUMA_SUM] = sum[q * 64];
+        f[Q_FLATNESS] = full ? pairs[q * 16] / 24.0f : UNMEASURED_FLATNESS;
+        f[Q_LUMA_MIN] = lo[q * 64];
+        f[Q_LUMA_MAX] = hi[q * 64];
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -105,7 +193,8 @@ uint32_t orc_min_static_blocks(uint32_t total) {
 }
 
 // The records of `next` (its previous frame `prev`), both channel-interleaved f32 frames.
-void orc_temporal_stats(const float* next, const float* prev, int channels, int w, int h, float* records) {
+void orc_temporal_stats(const float* next, const float* prev, int channels, int w, int h, int luma_fields,
+                        float* records) {
     const int bxn = (w + NB - 1) / NB, byn = (h + NB - 1) / NB, rl = record_len(channels);
     const int lanes = 2 * channels + 1;
     std::vector<float> scratch(256 * lanes), tile(256), cells(16);
@@ -169,6 +258,17 @@ void orc_temporal_stats(const float* next, const float* prev, int channels, int 
                     }
                 out[texture_lane(channels, c)] = pairs ? energy / static_cast<float>(pairs) : 0.0f;
             }
+            if (luma_fields) {
+                bool valid[256];
+                float nl[256], ml[256];
+                for (int t = 0; t < 256; ++t) {
+                    const int gx = bx * NB + t % NB, gy = by * NB + t / NB;
+                    valid[t] = gx < w && gy < h;
+                    nl[t] = valid[t] ? value(next, gx, gy, 0) : 0.0f;
+                    ml[t] = valid[t] ? 0.5f * (nl[t] + value(prev, gx, gy, 0)) : 0.0f;
+                }
+                quarter_fields(out, channels, bw, bh, true, valid, nl, ml, d0.data());
+            }
         }
 }
 
@@ -179,7 +279,7 @@ void orc_temporal_stats(const float* next, const float* prev, int channels, int 
 // it matches inside the frame), and writes an all-zero record when the followed block leaves the
 // frame. The four variance sums are halving-tree reductions over the block's 256 threads.
 void orc_temporal_stats_mc(const float* next, const float* prev, int channels, int w, int h, const int32_t* mv,
-                           int mv_bx, int mv_by, int step, float* records) {
+                           int mv_bx, int mv_by, int step, int luma_fields, float* records) {
     const int bxn = (w + NB - 1) / NB, byn = (h + NB - 1) / NB, rl = record_len(channels);
     const int lanes = 2 * channels + 1;
     auto value = [&](const float* f, int x, int y, int c) { return f[(static_cast<int64_t>(y) * w + x) * channels + c]; };
@@ -279,13 +379,24 @@ void orc_temporal_stats_mc(const float* next, const float* prev, int channels, i
                 out[texture_lane(channels, c)] = pairs ? energy / static_cast<float>(pairs) : 0.0f;
             }
             out[2 * channels + 2] = (follows && matched) ? 1.0f : 0.0f;
+            if (luma_fields) {
+                bool valid[256];
+                float nl[256], ml[256];
+                for (int t = 0; t < 256; ++t) {
+                    const int gx = x0 + t % NB, gy = y0 + t / NB;
+                    valid[t] = gx < w && gy < h && matched;
+                    nl[t] = valid[t] ? value(next, gx, gy, 0) : 0.0f;
+                    ml[t] = valid[t] ? 0.5f * (nl[t] + value(prev, gx + sx, gy + sy, 0)) : 0.0f;
+                }
+                quarter_fields(out, channels, bw, bh, matched, valid, nl, ml, d0.data());
+            }
         }
 }
 
 // One slot's reading (READING_WORDS floats). `records` may be null without temporal stats;
 // `imm_low` holds the two Immerkaer lower quartiles (the quartile of the cube sigmas).
 void orc_noise_reading(const float* records, const float* imm_low, int channels, int w, int h, int temporal,
-                       float* reading) {
+                       int curve, float* reading) {
     std::fill(reading, reading + R_WORDS, 0.0f);
     reading[R_IMM_LOW] = imm_low[0];
     reading[R_IMM_LOW + 1] = imm_low[1];
@@ -342,6 +453,7 @@ void orc_noise_reading(const float* records, const float* imm_low, int channels,
     }
     Sel kept[NOISE_CHANNELS], rho;
     uint32_t accepted[NOISE_CHANNELS] = {0, 0};
+    std::vector<bool> block_accepted(nblocks, false);
     for (int i = 0; i < nblocks; ++i) {
         const Block& b = blocks[i];
         bool accepted0 = false;
@@ -353,6 +465,7 @@ void orc_noise_reading(const float* records, const float* imm_low, int channels,
             if (acc) accepted[c] += 1;
             if (c == 0) accepted0 = acc;
         }
+        block_accepted[i] = accepted0;
         const bool has_rho = accepted0 && b.pairs > 0.0f;
         const float variance = has_rho ? b.var0 : 1.0f;
         const float r = (b.mean_lag - b.mean[0] * b.mean[0]) / variance;
@@ -375,6 +488,85 @@ void orc_noise_reading(const float* records, const float* imm_low, int channels,
     reading[R_RHO] = valid0 ? median_from_pair(rho.median_low(), rho.median_high()) : 0.0f;
     reading[R_STATIC] = valid0 ? static_fraction : 0.0f;
     reading[R_ACCEPTED] = static_cast<float>(accepted[0]);
+    if (!curve) return;
+
+    // The noise curve (kernels/sample.rs:95-104, 482-510, 717-803; kernels/curve.rs:37-133). The
+    // flat gate scales with channel 0's kept sigma median.
+    const float sigma_median = median_from_pair(kept[0].median_low(), kept[0].median_high());
+    const float flat_limit = std::max(FLAT_FACTOR * sigma_median * sigma_median, FLAT_FLOOR);
+    Sel quarters, bins[CURVE_BINS];
+    for (int i = 0; i < nblocks; ++i) {
+        if (!block_accepted[i]) continue;
+        const int bx = i % bxn, by = i / bxn;
+        const int bw = std::min(NB, w - bx * NB), bh = std::min(NB, h - by * NB);
+        const float* r = records + static_cast<int64_t>(i) * rl;
+        for (int q = 0; q < QUARTERS; ++q) {
+            const int qw = std::min(std::max(bw - (q % 2) * QUARTER_SIZE, 0), QUARTER_SIZE);
+            const int qh = std::min(std::max(bh - (q / 2) * QUARTER_SIZE, 0), QUARTER_SIZE);
+            const float pixels = static_cast<float>(qw * qh);
+            const float* f = r + 2 * channels + QUARTER_BASE + q * QUARTER_FIELDS;
+            const float divisor = pixels > 0.0f ? pixels : 1.0f;
+            const float mean = f[Q_SUM_D] / divisor;
+            const float ms = f[Q_SUM_D2] / divisor;
+            const float sigma = std::sqrt(std::max(ms - mean * mean, 0.0f)) / SQRT_2F;
+            const bool passes = pixels > 0.0f && std::fabs(mean) < QUARTER_STATIC_GATE && sigma > RHO_SIGMA_GATE;
+            if (!passes) continue;
+            quarters.v.push_back(sigma);
+            const float mean_luma = f[Q_LUMA_SUM] / divisor;
+            const float scaled = std::max(mean_luma * static_cast<float>(CURVE_BINS), 0.0f);
+            const int bin = static_cast<int>(std::min(scaled, static_cast<float>(CURVE_BINS - 1)));
+            const bool textured = f[Q_FLATNESS] > flat_limit;
+            const bool clipped = f[Q_LUMA_MIN] < CLIP_LOW || f[Q_LUMA_MAX] > CLIP_HIGH;
+            if (!textured && !clipped) bins[bin].v.push_back(sigma);
+        }
+    }
+    quarters.done();
+    for (auto& b : bins) b.done();
+    const float quarter_median = median_from_pair(quarters.median_low(), quarters.median_high());
+    // curve_bin_sigma: flat before the first and after the last populated bin, linear between the
+    // nearest populated bin below and the nearest at or above.
+    uint32_t populated = 0;
+    int first_index = 0, last_index = 0;
+    float first_sigma = 0.0f, last_sigma = 0.0f, medians[CURVE_BINS];
+    for (int b = 0; b < CURVE_BINS; ++b) {
+        medians[b] = median_from_pair(bins[b].median_low(), bins[b].median_high());
+        if (bins[b].n() < MIN_BIN_QUARTERS) continue;
+        if (populated == 0) {
+            first_index = b;
+            first_sigma = medians[b];
+        }
+        last_index = b;
+        last_sigma = medians[b];
+        ++populated;
+    }
+    const bool curve_valid = valid0 && quarters.n() > 0 && quarter_median > 0.0f && populated >= MIN_POPULATED_BINS;
+    const float divisor = curve_valid ? quarter_median : 1.0f;
+    for (int bin = 0; bin < CURVE_BINS; ++bin) {
+        int low_index = 0, high_index = 0;
+        float low_sigma = 0.0f, high_sigma = 0.0f;
+        bool has_high = false;
+        for (int b = 0; b < CURVE_BINS; ++b) {
+            if (bins[b].n() < MIN_BIN_QUARTERS) continue;
+            if (b < bin) {
+                low_index = b;
+                low_sigma = medians[b];
+            }
+            if (b >= bin && !has_high) {
+                high_index = b;
+                high_sigma = medians[b];
+                has_high = true;
+            }
+        }
+        const int span_bins = high_index > low_index ? high_index - low_index : 1;
+        const int offset_bins = bin - std::min(low_index, bin);
+        const float fraction = static_cast<float>(offset_bins) / static_cast<float>(span_bins);
+        const float between = low_sigma + (high_sigma - low_sigma) * fraction;
+        const float sigma = bin <= first_index ? first_sigma : (bin >= last_index ? last_sigma : between);
+        reading[R_RATIOS + bin] = curve_valid ? sigma / divisor : 0.0f;
+    }
+    reading[R_CURVE_VALID] = curve_valid ? 1.0f : 0.0f;
+    reading[R_QUARTER_MEDIAN] = curve_valid ? quarter_median : 0.0f;
+    reading[R_POPULATED] = static_cast<float>(populated);
 }
 
 // kernels/derive.rs:46-64 (`correlation_factor`) with the host's segment reciprocals.

@@ -746,8 +746,10 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     completes the region d slots behind it; at the end, tail passes centred on d+1..2d (or, for a
     stream shorter than the ring, on every real frame after padding with the last frame). The
     first `context` frames are priming pushes (no head passes). With `noise`, a function of a pass's
-    centre stream frame returning (sigma, weight_scale, sad_floor), each pass reads those (the
-    automatic estimate's fold around that frame) instead of the pinned sigma's. With `share_writes`
+    centre stream frame returning (sigma, weight_scale, sad_floor) or (sigma, weight_scale,
+    sad_floor, curve), each pass reads those (the automatic estimate's fold around that frame)
+    instead of the pinned sigma's; `curve` is the 16 luma noise-curve ratios, or None while the
+    fold's curve flag is clear. With `share_writes`
     each window's field is shared for a chroma stream; with `share_reads` the window's motion is the
     shared luma field of the centre frame, searched one pixel around at one level with confidence
     (nlmeans/dispatch/motion.rs:231-310), and no motion of this plane's own is searched."""
@@ -784,9 +786,10 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
             zeroed[i] = False
         st["passes"] += 1
         slots = [phys(l) for l in range(tf) if l != centre]
-        p_sigma, p_weight, p_floor = sigma, None, sad_floor
+        p_sigma, p_weight, p_floor, p_curve = sigma, None, sad_floor, None
         if noise is not None:
-            p_sigma, p_weight, p_floor = noise(slot_frames[cs])
+            p_sigma, p_weight, p_floor, *rest = noise(slot_frames[cs])
+            p_curve = rest[0] if rest else None
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
         if share_reads is not None:
             mapped = share_reads.read(st["call"], slot_frames[cs] % tf, slot_frames[cs])
@@ -809,7 +812,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
                                   confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
                                   c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
                                   sigma=(p_sigma,) * c, weight_scale_override=p_weight, lambda_ht=lambda_ht,
-                                  kaiser_beta=kaiser_beta,
+                                  kaiser_beta=kaiser_beta, noise_curve=p_curve,
                                   pooled=pool_ratio, blksize=blksize, blk_step=step, blocks_x=bx, blocks_y=by,
                                   mv_stride=bx * by * 2, conf_stride=bx * by)
         accum[:] += acc.reshape(tf, -1)
@@ -934,8 +937,8 @@ def _noise_lib():
     l.orc_noise_record_len.restype = C.c_int
     l.orc_min_static_blocks.argtypes = [C.c_uint32]
     l.orc_min_static_blocks.restype = C.c_uint32
-    l.orc_temporal_stats.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, _fp]
-    l.orc_noise_reading.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
+    l.orc_temporal_stats.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
+    l.orc_noise_reading.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
     l.orc_temporal_stats_mc.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int,
                                         C.c_int, _fp]
     l.orc_fold_words.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, C.c_int, C.c_float,
@@ -958,17 +961,20 @@ def min_static_blocks(total: int) -> int:
     return int(_noise_lib().orc_min_static_blocks(total))
 
 
-def temporal_stats(new: np.ndarray, prev: np.ndarray, channels: int, width: int, height: int) -> np.ndarray:
-    """The temporal residual records of `new` against `prev`, (H, W, C) f32 frames."""
+def temporal_stats(new: np.ndarray, prev: np.ndarray, channels: int, width: int, height: int,
+                   luma_fields: bool = False) -> np.ndarray:
+    """The temporal residual records of `new` against `prev`, (H, W, C) f32 frames; with
+    `luma_fields`, each block's four 8x8 quarter records as well."""
     bx, by = stats_blocks(width, height)
     out = np.zeros(bx * by * noise_record_len(channels), np.float32)
     _noise_lib().orc_temporal_stats(_f(np.ascontiguousarray(new, np.float32)),
-                                    _f(np.ascontiguousarray(prev, np.float32)), channels, width, height, _f(out))
+                                    _f(np.ascontiguousarray(prev, np.float32)), channels, width, height,
+                                    int(luma_fields), _f(out))
     return out
 
 
 def temporal_stats_mc(new: np.ndarray, prev: np.ndarray, channels: int, width: int, height: int, mv: np.ndarray,
-                      mv_blocks: tuple[int, int], step: int) -> np.ndarray:
+                      mv_blocks: tuple[int, int], step: int, luma_fields: bool = False) -> np.ndarray:
     """The records of `new` against `prev` along the motion field `mv` ((bx * by, 2) int32)."""
     bx, by = stats_blocks(width, height)
     out = np.zeros(bx * by * noise_record_len(channels), np.float32)
@@ -976,18 +982,18 @@ def temporal_stats_mc(new: np.ndarray, prev: np.ndarray, channels: int, width: i
     _noise_lib().orc_temporal_stats_mc(_f(np.ascontiguousarray(new, np.float32)),
                                        _f(np.ascontiguousarray(prev, np.float32)), channels, width, height,
                                        field.ctypes.data_as(C.POINTER(C.c_int32)), mv_blocks[0], mv_blocks[1], step,
-                                       _f(out))
+                                       int(luma_fields), _f(out))
     return out
 
 
 def noise_reading(records: np.ndarray | None, imm_low, channels: int, width: int, height: int,
-                  temporal: bool) -> np.ndarray:
+                  temporal: bool, curve: bool = False) -> np.ndarray:
     """One slot's READING_WORDS reading from its records (None without temporal stats) and its two
-    Immerkaer lower quartiles."""
+    Immerkaer lower quartiles; with `curve` (records carrying the luma fields), the noise curve."""
     out = np.zeros(READING_WORDS, np.float32)
     low = np.ascontiguousarray(np.asarray(imm_low, np.float32).reshape(2))
     rec = _f(np.ascontiguousarray(records, np.float32)) if records is not None else None
-    _noise_lib().orc_noise_reading(rec, _f(low), channels, width, height, int(temporal), _f(out))
+    _noise_lib().orc_noise_reading(rec, _f(low), channels, width, height, int(temporal), int(curve), _f(out))
     return out
 
 
@@ -1024,7 +1030,8 @@ def noise_fold(records: np.ndarray, results: np.ndarray, capacity: int, first: i
     return state, derived, spatial, pilot
 
 
-def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: int, temporal: bool):
+def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: int, temporal: bool,
+                   luma_fields: bool = False):
     """Every frame's reading and Immerkaer totals, each read against the frame before it (the first
     frame's records are zero), as the look-ahead reads them without motion compensation
     (nlmeans/denoiser/lookahead.rs:425-444)."""
@@ -1037,14 +1044,15 @@ def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: 
                 rec = np.zeros(stats_blocks(width, height)[0] * stats_blocks(width, height)[1]
                                * noise_record_len(channels), np.float32)
             else:
-                rec = temporal_stats(f, frames[i - 1], channels, width, height)
-        readings.append(noise_reading(rec, low, channels, width, height, temporal))
+                rec = temporal_stats(f, frames[i - 1], channels, width, height, luma_fields)
+        readings.append(noise_reading(rec, low, channels, width, height, temporal, luma_fields))
         totals.append(tot)
     return readings, totals
 
 
 def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, height: int, *, blksize: int,
-                      overlap: int, search_radius: int, levels: int, thsad: float = 0.0, ceiling: int = 0):
+                      overlap: int, search_radius: int, levels: int, thsad: float = 0.0, ceiling: int = 0,
+                      luma_fields: bool = False):
     """Every frame's reading as a motion-compensated look-ahead takes it
     (nlmeans/denoiser/lookahead.rs:283-319, 425-458, 543-605): frame i >= 1 is searched against
     frame i - 1 (newer to older) and read along that field; frame 1 is also searched older to newer
@@ -1062,18 +1070,19 @@ def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, heigh
         totals.append(tot)
         lows.append(low)
         if i == 0:
-            readings.append(noise_reading(np.zeros(rec_len, np.float32), low, channels, width, height, True))
+            readings.append(noise_reading(np.zeros(rec_len, np.float32), low, channels, width, height, True,
+                                          luma_fields))
             continue
         pair = np.stack([np.ascontiguousarray(frames[i - 1], np.float32),
                          np.ascontiguousarray(f, np.float32)]).reshape(-1)
         pyr = motion_pyramid(pair, channels, width, height, levels)
         newer_to_older, _ = motion_search(pyr, width, height, 2, 1, [0], **kw)
-        rec = temporal_stats_mc(f, frames[i - 1], channels, width, height, newer_to_older[0], mb, step)
-        readings.append(noise_reading(rec, low, channels, width, height, True))
+        rec = temporal_stats_mc(f, frames[i - 1], channels, width, height, newer_to_older[0], mb, step, luma_fields)
+        readings.append(noise_reading(rec, low, channels, width, height, True, luma_fields))
         if i == 1:
             older_to_newer, _ = motion_search(pyr, width, height, 2, 0, [1], **kw)
-            rec0 = temporal_stats_mc(frames[0], f, channels, width, height, older_to_newer[0], mb, step)
-            readings[0] = noise_reading(rec0, lows[0], channels, width, height, True)
+            rec0 = temporal_stats_mc(frames[0], f, channels, width, height, older_to_newer[0], mb, step, luma_fields)
+            readings[0] = noise_reading(rec0, lows[0], channels, width, height, True, luma_fields)
     return readings, totals
 
 

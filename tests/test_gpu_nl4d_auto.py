@@ -1,8 +1,10 @@
-"""NL4D with the automatic noise estimate (luma, no sigma, noise map off) on the GPU through the C
-ABI against the oracle's stream restatement: the 8-frame look-ahead searches each frame against the
-one before it, reads the noise along that motion (the first frame again along the motion to the
-second), and every pass folds the window around its centre frame into the sigma, weight scale and
-motion SAD floor it filters with (nlmeans/denoiser/lookahead.rs, nl4d/denoiser.rs, noise/*).
+"""NL4D with the automatic noise estimate (luma, no sigma) on the GPU through the C ABI against the
+oracle's stream restatement: the 8-frame look-ahead searches each frame against the one before it,
+reads the noise along that motion (the first frame again along the motion to the second), and every
+pass folds the window around its centre frame into the sigma, weight scale and motion SAD floor it
+filters with (nlmeans/denoiser/lookahead.rs, nl4d/denoiser.rs, noise/*). With the noise map on (the
+default) the readings carry the luma noise curve and each pass scales its luma threshold by the
+folded curve at the reference patch's mean luma (collab/kernels/fused/mod.rs:617-660).
 
 Every stage is bit-exact, so every output sample is identical to the oracle's."""
 
@@ -16,22 +18,27 @@ from test_gpu_nl4d import check, clip
 pytestmark = pytest.mark.gpu
 
 
-def auto_noise(oracle, frames, fmt, d, *, blksize=16, overlap=8, search_radius=4, levels=2, sigma_scale=1.0):
-    """The per-pass (sigma, weight scale, SAD floor) of the measured front, by centre frame."""
+def auto_noise(oracle, frames, fmt, d, *, blksize=16, overlap=8, search_radius=4, levels=2, sigma_scale=1.0,
+               noise_map=False):
+    """The per-pass (sigma, weight scale, SAD floor, curve) of the measured front, by centre frame;
+    the curve is None unless the noise map is on and the fold's curve flag is set."""
     f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), 0.0) for p in frames]
     h, w, c = f32[0].shape
     readings, totals = oracle.noise_readings_mc(f32, c, w, h, blksize=blksize, overlap=overlap,
-                                                search_radius=search_radius, levels=levels)
+                                                search_radius=search_radius, levels=levels, luma_fields=noise_map)
     f = np.float32
     area, unit = f(81.0), f(1.2) * f(1.0) * f(255.0)
-    settings = oracle.fold_words(w, h, sigma_scale=sigma_scale, g_max=float(oracle.dct_noise_profile(0.0).max()),
+    settings = oracle.fold_words(w, h, sigma_scale=sigma_scale, curve_applies=noise_map,
+                                 g_max=float(oracle.dct_noise_profile(0.0).max()),
                                  h2_per_inverse_variance=float(f(65025.0) / (f(3.0) * unit * unit * area)),
                                  h2_fixed=float(f(65025.0) / (f(3.0) * f(1.2) * f(1.2) * area)),
                                  offset_per_variance=float(f(2.0) * f(3.0) * f(1.0) * area),
                                  sad_per_sigma=oracle.sad_noise_floor(blksize, 1.0))
     folds = oracle.fold_stream(readings, totals, settings, c, 0, d)
     derived = [fd[1] for fd in folds]
-    return (lambda frame: (float(derived[frame][0]), float(derived[frame][2]), float(derived[frame][4]))), derived
+    curves = [fd[0][16:32].copy() if fd[1][3] != 0 else None for fd in folds]
+    return (lambda frame: (float(derived[frame][0]), float(derived[frame][2]), float(derived[frame][4]),
+                           curves[frame])), derived, curves
 
 
 @pytest.mark.parametrize("w,h,n,d,estimation,context", [
@@ -49,7 +56,7 @@ def test_nl4d_auto_sigma_matches_oracle(oracle, w, h, n, d, estimation, context)
     spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
     assert spec.max_held_frames() == 2 * d + 8
     got = Runner(spec).run(frames, context=context)
-    noise, derived = auto_noise(oracle, [[f[0]] for f in frames], fmt, d)
+    noise, derived, _ = auto_noise(oracle, [[f[0]] for f in frames], fmt, d)
     chained = estimation == avd.MotionEstimation.CHAINED or (estimation == avd.MotionEstimation.AUTO and d >= 3)
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 0.0, context=context, spatial_radius=4,
           chained=chained, noise=noise)
@@ -66,6 +73,51 @@ def test_nl4d_auto_10bit_sigma_scale(oracle):
                         pooled_threshold=False, lambda_ht=2.7)
     spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
     got = Runner(spec).run(frames)
-    noise, _ = auto_noise(oracle, [[f[0]] for f in frames], fmt, d, sigma_scale=1.2)
+    noise, _, _ = auto_noise(oracle, [[f[0]] for f in frames], fmt, d, sigma_scale=1.2)
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 0.0, spatial_radius=3, noise=noise,
           pooled_threshold=False, lambda_ht=2.7)
+
+
+def graded_clip(w, h, n, seed, depth=8):
+    """A panning luma clip of a smooth horizontal ramp whose grain grows with brightness (2 to 14
+    codes), so the reading finds a rising noise curve."""
+    rng = np.random.default_rng(seed)
+    top = (1 << depth) - 1
+    y, x = np.mgrid[0:h, 0:w + 4 * n].astype(np.float32)
+    ramp = 0.06 + 0.88 * x / (w + 4 * n) + 0.02 * np.sin(y * 0.3)
+    frames = []
+    for i in range(n):
+        base = ramp[:, 2 * i:2 * i + w]
+        grain = rng.normal(0, 1, base.shape) * (2.0 + 12.0 * base) / 255.0
+        frames.append([np.clip(np.rint((base + grain) * top), 0, top).astype(np.uint8 if depth == 8 else np.uint16)])
+    return frames
+
+
+@pytest.mark.parametrize("w,h,n,d,estimation", [
+    (256, 160, 12, 2, avd.MotionEstimation.DIRECT),
+    (224, 144, 14, 3, avd.MotionEstimation.AUTO),
+    (200, 136, 6, 1, avd.MotionEstimation.DIRECT),   # shorter than the look-ahead
+])
+def test_nl4d_auto_noise_map_matches_oracle(oracle, w, h, n, d, estimation):
+    """The default NL4D call on gray frames (automatic sigma, noise map on): identical samples."""
+    fmt = avd.SampleFormat.u8()
+    frames = graded_clip(w, h, n, seed=w + n)
+    o = avd.Nl4dOptions(sigma=None, temporal_radius=d, spatial_radius=4,
+                        motion=avd.MotionSearch(estimation=estimation))
+    assert o.noise_map
+    spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    noise, _, curves = auto_noise(oracle, [f for f in frames], fmt, d, noise_map=True)
+    chained = estimation == avd.MotionEstimation.AUTO and d >= 3
+    check(oracle, [[g[0]] for g in got], frames, fmt, d, 0.0, spatial_radius=4, chained=chained, noise=noise)
+    # The brighter half of the ramp carries more grain: the folded curve rises.
+    live = [c for c in curves if c is not None]
+    assert live, "the fold never validated a curve"
+    assert all(c[13] > 1.3 * c[3] for c in live)
+
+
+def test_nl4d_noise_map_on_frames_with_chroma_needs_the_colour_gains():
+    fmt = avd.SampleFormat.u8()
+    o = avd.Nl4dOptions(sigma=None, temporal_radius=1)
+    with pytest.raises(avd.InvalidOptions, match="colour grain gains"):
+        avd.build_engine(avd.EngineSpec.nl4d(o, None, avd.Geometry(64, 48, avd.ChromaLayout.YUV420, fmt, fmt)))

@@ -40,41 +40,45 @@ def noisy_frames(w, h, channels, n, sigma_255, seed, still=False):
     return frames
 
 
+@pytest.mark.parametrize("luma_fields", [False, True])
 @pytest.mark.parametrize("w,h,channels", [(64, 48, 1), (75, 37, 2), (1920, 1080, 1), (333, 199, 2), (17, 16, 1),
-                                          (5, 3, 1)])
-def test_temporal_stats_matches_oracle(lib, oracle, w, h, channels):
+                                          (5, 3, 1), (29, 21, 1)])
+def test_temporal_stats_matches_oracle(lib, oracle, w, h, channels, luma_fields):
     import torch
 
     a, b = noisy_frames(w, h, channels, 2, 5.0, w + h)
     n = lib.avd_noise_records_floats(w, h, channels)
     out = torch.full((n,), -7.0, device="cuda")
     da, db = dev(a), dev(b)
-    assert lib.avd_noise_temporal_stats(db.data_ptr(), da.data_ptr(), channels, w, h, out.data_ptr(), stream()) == 0
+    assert lib.avd_noise_temporal_stats(db.data_ptr(), da.data_ptr(), channels, w, h, int(luma_fields),
+                                        out.data_ptr(), stream()) == 0
     zero = torch.full((n,), -7.0, device="cuda")
-    assert lib.avd_noise_temporal_stats(db.data_ptr(), 0, channels, w, h, zero.data_ptr(), stream()) == 0
+    assert lib.avd_noise_temporal_stats(db.data_ptr(), 0, channels, w, h, int(luma_fields), zero.data_ptr(),
+                                        stream()) == 0
     torch.cuda.synchronize()
-    want = oracle.temporal_stats(b, a, channels, w, h)
+    want = oracle.temporal_stats(b, a, channels, w, h, luma_fields)
     assert np.array_equal(bits(out), want.view(np.uint32))
     assert not zero.cpu().numpy().any()
 
 
-def gpu_reading(lib, records, imm_low, channels, w, h):
+def gpu_reading(lib, records, imm_low, channels, w, h, curve=False):
     import torch
 
     reading = torch.full((30,), -3.0, device="cuda")
     reading[:2] = torch.tensor(np.asarray(imm_low, np.float32))
-    scratch = torch.zeros(lib.avd_noise_scratch_floats(w, h), device="cuda")
+    scratch = torch.full((lib.avd_noise_scratch_floats(w, h),), -5.0, device="cuda")
     rec = dev(records) if records is not None else None
-    st = lib.avd_noise_reading(rec.data_ptr() if rec is not None else 0, channels, w, h, scratch.data_ptr(),
-                               reading.data_ptr(), stream())
+    st = lib.avd_noise_reading(rec.data_ptr() if rec is not None else 0, channels, w, h, int(curve),
+                               scratch.data_ptr(), reading.data_ptr(), stream())
     assert st == 0, lib.avd_last_error().decode()
     torch.cuda.synchronize()
     return reading
 
 
+@pytest.mark.parametrize("curve", [False, True])
 @pytest.mark.parametrize("w,h,channels,sigma", [(160, 96, 1, 6.0), (200, 120, 2, 3.0), (1920, 1080, 1, 8.0),
                                                 (333, 199, 2, 12.0), (48, 32, 1, 0.2)])
-def test_reading_matches_oracle_on_frames(lib, oracle, w, h, channels, sigma):
+def test_reading_matches_oracle_on_frames(lib, oracle, w, h, channels, sigma, curve):
     import torch
 
     frames = noisy_frames(w, h, channels, 3, sigma, w * 7 + channels)
@@ -86,19 +90,20 @@ def test_reading_matches_oracle_on_frames(lib, oracle, w, h, channels, sigma):
         dcur = dev(cur)
         dprev = dev(prev) if prev is not None else None
         assert lib.avd_noise_temporal_stats(dcur.data_ptr(), dprev.data_ptr() if prev is not None else 0, channels,
-                                            w, h, rec.data_ptr(), stream()) == 0
+                                            w, h, int(curve), rec.data_ptr(), stream()) == 0
         partials = torch.zeros(lib.avd_immerkaer_partials_len(w, h), device="cuda")
         totals = torch.zeros(2, device="cuda")
         reading = torch.full((30,), -3.0, device="cuda")
         scratch = torch.zeros(lib.avd_noise_scratch_floats(w, h), device="cuda")
         assert lib.avd_immerkaer(dcur.data_ptr(), channels, w, h, partials.data_ptr(), totals.data_ptr(),
                                  reading.data_ptr(), stream()) == 0
-        assert lib.avd_noise_reading(rec.data_ptr(), channels, w, h, scratch.data_ptr(), reading.data_ptr(),
-                                     stream()) == 0
+        assert lib.avd_noise_reading(rec.data_ptr(), channels, w, h, int(curve), scratch.data_ptr(),
+                                     reading.data_ptr(), stream()) == 0
         torch.cuda.synchronize()
-        o_rec = oracle.temporal_stats(cur, prev, channels, w, h) if prev is not None else np.zeros(n, np.float32)
+        o_rec = (oracle.temporal_stats(cur, prev, channels, w, h, curve) if prev is not None
+                 else np.zeros(n, np.float32))
         _, o_tot, o_low = oracle.immerkaer(cur, channels, w, h)
-        want = oracle.noise_reading(o_rec, o_low, channels, w, h, True)
+        want = oracle.noise_reading(o_rec, o_low, channels, w, h, True, curve)
         got = reading.cpu().numpy()
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (got, want)
         assert np.array_equal(bits(totals), o_tot.view(np.uint32))
