@@ -940,7 +940,7 @@ def _noise_lib():
     l.orc_temporal_stats.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
     l.orc_noise_reading.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
     l.orc_temporal_stats_mc.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32), C.c_int, C.c_int,
-                                        C.c_int, _fp]
+                                        C.c_int, C.c_int, _fp]
     l.orc_fold_words.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_float, C.c_int, C.c_float,
                                  C.c_float, C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, C.c_float, _fp]
     l.orc_noise_fold.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, _fp, C.c_int, C.c_int, _fp, _fp, _fp, _fp]

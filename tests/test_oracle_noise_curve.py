@@ -122,3 +122,16 @@ def test_a_real_stream_builds_a_curve():
     assert r[R_VALID] == 1.0 and r[R_CURVE_VALID] == 1.0 and r[R_POPULATED] >= 10
     ratios = r[R_RATIOS:R_RATIOS + 16]
     assert ratios[14] > 1.5 * ratios[2]
+
+
+def test_compensated_quarter_fields_follow_the_vector():
+    """Along a zero field the compensated records equal the plain ones, quarter fields included."""
+    import oracle as o
+
+    w, h = 40, 24
+    prev, new = _frames(w, h, 3)
+    mv = np.zeros((5 * 3, 2), np.int32)
+    for lf in (False, True):
+        plain = o.temporal_stats(new, prev, 1, w, h, lf)
+        mc = o.temporal_stats_mc(new, prev, 1, w, h, mv, (5, 3), 8, lf)
+        assert np.array_equal(plain.view(np.uint32), mc.view(np.uint32))
