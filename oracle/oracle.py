@@ -1267,3 +1267,113 @@ def nlm_forward_f64(window: list[np.ndarray], d: int, a: int, s: int, strength: 
     lut[a * side + a] = 0.0
     return nlm_frame(window, d, a, s, h2, noise_offset=pair_offset, lut=lut if spatial_offset else None, wref=wref,
                      fp64=True)
+
+
+# ---- the colour grain gains (noise/colour.rs, noise/kernels/colour.rs, colour_fit.rs) ----------
+
+COLOUR_CELLS = 976
+COLOUR_CELL_WORDS = 69
+COLOUR_FIT_PLANE_WORDS = 22
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+
+
+def _colour_lib():
+    l = lib()
+    l.orc_colour_records.argtypes = [C.c_int, C.c_int]
+    l.orc_colour_records.restype = C.c_int
+    l.orc_colour_cell.argtypes = [C.c_float, C.c_float, C.c_float]
+    l.orc_colour_cell.restype = C.c_uint32
+    l.orc_log_mirror.argtypes = [C.c_float]
+    l.orc_log_mirror.restype = C.c_float
+    l.orc_atan2_mirror.argtypes = [C.c_float, C.c_float]
+    l.orc_atan2_mirror.restype = C.c_float
+    l.orc_colour_means.argtypes = [_u32p, _u32p, _u32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_float, C.c_float, _fp, _fp]
+    l.orc_colour_accumulate.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, _i32p]
+    l.orc_colour_window.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, _fp]
+    l.orc_colour_levels.argtypes = [_fp, _fp, C.c_int, C.c_int, _fp]
+    l.orc_colour_fit.argtypes = [_fp, C.c_int, C.c_int, _fp, C.c_int, _fp, _fp, _fp]
+    l.orc_colour_lookup.argtypes = [_fp, _fp, C.c_int, _fp, _fp]
+    return l
+
+
+def colour_records(planes: int, luma: bool) -> int:
+    """The cell and extra records of one frame's sums: `planes` x 976 cells, then 16 luma
+    calibration records or one chroma record per plane."""
+    return _colour_lib().orc_colour_records(planes, int(luma))
+
+
+def colour_cell(luma: float, cb: float, cr: float) -> int:
+    return int(_colour_lib().orc_colour_cell(luma, cb, cr))
+
+
+def log_mirror(x: float) -> float:
+    return float(_colour_lib().orc_log_mirror(x))
+
+
+def atan2_mirror(y: float, x: float) -> float:
+    return float(_colour_lib().orc_atan2_mirror(y, x))
+
+
+def colour_means(luma: np.ndarray, cb: np.ndarray, cr: np.ndarray, width: int, height: int, shift_x: int,
+                 shift_y: int, samples_per_word: int, is_float: bool, eight_bit_scale: float,
+                 chroma_bias: float) -> tuple[np.ndarray, np.ndarray]:
+    """The (blocks, 3) mean luma, Cb and Cr of every block of the luma and the chroma noise grids,
+    from three word-packed planes (uint32 words)."""
+    cw, ch = -(-width // (1 << shift_x)), -(-height // (1 << shift_y))
+    nl = -(-width // 16) * -(-height // 16)
+    nc = -(-cw // 16) * -(-ch // 16)
+    lm, cm = np.zeros(nl * 3, np.float32), np.zeros(nc * 3, np.float32)
+    planes = [np.ascontiguousarray(p).view(np.uint32).reshape(-1) for p in (luma, cb, cr)]
+    _colour_lib().orc_colour_means(*[p.ctypes.data_as(_u32p) for p in planes], width, height, shift_x, shift_y,
+                                   samples_per_word, int(is_float), eight_bit_scale, chroma_bias, _f(lm), _f(cm))
+    return lm.reshape(-1, 3), cm.reshape(-1, 3)
+
+
+def colour_accumulate(records: np.ndarray, means: np.ndarray, width: int, height: int, channels: int, luma: bool,
+                      grain_scale: float) -> np.ndarray:
+    """One frame's fixed-point cell sums (int32, colour_records x 69 words)."""
+    out = np.zeros(colour_records(channels, luma) * COLOUR_CELL_WORDS, np.int32)
+    _colour_lib().orc_colour_accumulate(_f(np.ascontiguousarray(records, np.float32)),
+                                        _f(np.ascontiguousarray(means, np.float32).reshape(-1)), width, height,
+                                        channels, int(luma), grain_scale, out.ctypes.data_as(_i32p))
+    return out
+
+
+def colour_window(ring: np.ndarray, capacity: int, first: int, last: int) -> np.ndarray:
+    """The window's decoded sums of frames first..=last from a (capacity, words) int32 ring."""
+    ring = np.ascontiguousarray(ring, np.int32).reshape(capacity, -1)
+    words = ring.shape[1]
+    out = np.zeros(words, np.float32)
+    _colour_lib().orc_colour_window(ring.ctypes.data_as(_i32p), capacity, first, last, words, _f(out))
+    return out
+
+
+def colour_levels(window: np.ndarray, ceilings: np.ndarray, cells: int, mean_level: bool) -> np.ndarray:
+    out = np.zeros(cells * 2, np.float32)
+    _colour_lib().orc_colour_levels(_f(np.ascontiguousarray(window, np.float32)),
+                                    _f(np.ascontiguousarray(ceilings, np.float32)), cells, int(mean_level), _f(out))
+    return out.reshape(-1, 2)
+
+
+def colour_fit(window: np.ndarray, planes: int, luma: bool, curve=None, curve_valid: bool = False):
+    """Both fits and the gains of the window's sums: (log grain tables, log gain tables, fit headers),
+    each plane after plane."""
+    table = np.zeros(planes * COLOUR_CELLS, np.float32)
+    gains = np.zeros(planes * COLOUR_CELLS, np.float32)
+    headers = np.zeros(planes * COLOUR_FIT_PLANE_WORDS, np.float32)
+    c = np.ascontiguousarray(curve if curve is not None else np.zeros(16), np.float32)
+    _colour_lib().orc_colour_fit(_f(np.ascontiguousarray(window, np.float32)), planes, int(luma), _f(c),
+                                 int(curve_valid), _f(table), _f(gains), _f(headers))
+    return table, gains, headers
+
+
+def colour_lookup(table: np.ndarray, colours: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The table's interpolated value and its exponential at each (luma, cb, cr) colour."""
+    colours = np.ascontiguousarray(colours, np.float32).reshape(-1, 3)
+    values = np.zeros(len(colours), np.float32)
+    gains = np.zeros(len(colours), np.float32)
+    _colour_lib().orc_colour_lookup(_f(np.ascontiguousarray(table, np.float32)), _f(colours), len(colours),
+                                    _f(values), _f(gains))
+    return values, gains
