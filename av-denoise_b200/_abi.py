@@ -259,6 +259,13 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_noise_temporal_stats": (C.c_int, [u64, u64, u32, u32, u32, u32, u64, C.c_void_p]),
     "avd_noise_compensated_stats": (C.c_int, [u64, u64, u32, u32, u32, u64, u32, u32, u32, u32, u64, C.c_void_p]),
     "avd_noise_reading": (C.c_int, [u64, u32, u32, u32, u32, u64, u64, C.c_void_p]),
+    "avd_colour_records": (u64, [u32, u32]),
+    "avd_colour_means": (C.c_int, [u64, u64, u64, C.POINTER(AvdGeometry), u64, u64, C.c_void_p]),
+    "avd_colour_accumulate": (C.c_int, [u64, u64, u32, u32, u32, u32, C.c_float, u64, C.c_void_p]),
+    "avd_colour_window": (C.c_int, [u64, u32, u32, u32, u32, u64, C.c_void_p]),
+    "avd_colour_fit_scratch_floats": (u64, [u32]),
+    "avd_colour_fit": (C.c_int, [u64, u32, u32, u64, u64, u64, u64, u64, C.c_void_p]),
+    "avd_colour_lookup": (C.c_int, [u64, u64, u32, u64, u64, C.c_void_p]),
     "avd_noise_fold_words": (None, [u32, u32, f32, u32, f32, f32, u32, f32, f32, f32, f32, u32, f32, f32, _P(f32)]),
     "avd_noise_fold": (C.c_int, [u64, u64, u32, u32, u32, u64, u32, u32, u64, u64, u64, u64, C.c_void_p]),
     "avd_nlm_backward_scratch_bytes": (u64, [u32, u32]),

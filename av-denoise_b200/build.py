@@ -38,10 +38,10 @@ COMMON = [
 # Per-file flags. The NL4D collaborative filter rounds every multiply and add on its own, as its CPU
 # restatement does (built with -ffp-contract=off), so its member choices and threshold decisions
 # agree bit for bit; -fmad=false keeps nvcc from fusing any of them. The noise estimate does the same
-# for its reading and fold words, the truemotion stage for its costs and confidences, and the exact
-# NLMeans finish for its distances, weights and sums.
+# for its reading and fold words, the truemotion stage for its costs and confidences, the exact
+# NLMeans finish for its distances, weights and sums, and the colour grain gains for their fit.
 PER_FILE = {"collab.cu": ["-fmad=false"], "noise_estimate.cu": ["-fmad=false"], "truemotion.cu": ["-fmad=false"],
-            "nlm_exact.cu": ["-fmad=false"]}
+            "nlm_exact.cu": ["-fmad=false"], "colour.cu": ["-fmad=false"]}
 
 
 def _sources() -> list[Path]:

@@ -24,6 +24,7 @@
 
 #include <cstdint>
 
+#include "colour_lookup.cuh"
 #include "kernels.h"
 
 namespace avd {
@@ -640,10 +641,14 @@ __global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch
     float prof[P];
 #pragma unroll
     for (int i = 0; i < P; ++i) prof[i] = __ldg(a.dct_profile + i);
-    float col_first = 0.0f;
+    float col_first = 0.0f, col_second = 0.0f;
 #pragma unroll
-    for (int r = 0; r < P; ++r) col_first += cur[r * C];
+    for (int r = 0; r < P; ++r) {
+        col_first += cur[r * C];
+        if (C > 1) col_second += cur[r * C + 1];
+    }
     const float patch_luma = reduce8(g, col_first) / 64.0f;
+    const float patch_second = C > 1 ? reduce8(g, col_second) / 64.0f : 0.0f;
     const float bins = static_cast<float>(kCurveBins);
     const float curve_pos = fminf(fmaxf(__fsub_rn(__fmul_rn(patch_luma, bins), 0.5f), 0.0f), bins - 1.0f);
     const uint32_t lower = min(static_cast<uint32_t>(curve_pos), static_cast<uint32_t>(kCurveBins - 2));
@@ -654,9 +659,35 @@ __global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch
         const float lo = __ldg(a.noise_curve + lower), hi = __ldg(a.noise_curve + lower + 1);
         ratio = __fadd_rn(lo, __fmul_rn(__fsub_rn(hi, lo), fraction));
     }
-    const float luma_scale = curve_valid ? fminf(fmaxf(ratio, 0.33f), 3.0f) : 1.0f;
-    const float first_lambda = a.lambda_ht * luma_scale;
-    const float second_lambda = a.lambda_ht;
+    // fused/colour.rs:48-83 (`threshold_gains`): a luma patch reads the gain at its own mean luma and
+    // its block's Cb and Cr, a chroma patch at its own Cb and Cr and its block's luma.
+    float first_gain = 1.0f, second_gain = 1.0f;
+    if (a.colour_on) {
+        const uint32_t bx = (rx + P / 2) / 16, by = (ry + P / 2) / 16;
+        const float* m = a.colour_means + (by * static_cast<uint32_t>(a.colour_blocks_x) + bx) * 3;
+        if (C == 1) {
+            first_gain = exp_mirror(colour::table_value(a.colour_gains, __fmul_rn(patch_luma, a.colour_scale),
+                                                        __ldg(m + 1), __ldg(m + 2)));
+        } else {
+            const float cb = __fsub_rn(__fmul_rn(patch_luma, a.colour_scale), 128.0f);
+            const float cr = __fsub_rn(__fmul_rn(patch_second, a.colour_scale), 128.0f);
+            colour::gain_pair(a.colour_gains, a.colour_gains + colour::kCells, __ldg(m), cb, cr, &first_gain,
+                              &second_gain);
+        }
+    }
+    // fused/mod.rs:643-660: a luma gain joins the curve's scale (together clamped to 0.33..6), a
+    // chroma gain scales its channel's threshold.
+    float curve_gain = 1.0f, first_channel_gain = first_gain, scale_max = 3.0f;
+    if (C == 1) {
+        curve_gain = first_gain;
+        first_channel_gain = 1.0f;
+        scale_max = a.colour_on ? 6.0f : 3.0f;
+    }
+    const float curve_scale = fminf(fmaxf(__fmul_rn(ratio, curve_gain), 0.33f), scale_max);
+    const float flat_scale = fminf(fmaxf(curve_gain, 0.33f), scale_max);
+    const float luma_scale = curve_valid ? curve_scale : flat_scale;
+    const float first_lambda = __fmul_rn(__fmul_rn(a.lambda_ht, luma_scale), first_channel_gain);
+    const float second_lambda = __fmul_rn(a.lambda_ht, second_gain);
     const float weight_scale = __ldg(a.noise + a.weight_scale_word);
     const uint32_t ref_idx = iy * refs_x + ix;
     const int64_t plane = static_cast<int64_t>(a.width) * a.height;

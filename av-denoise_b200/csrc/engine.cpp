@@ -1042,6 +1042,7 @@ struct AvdEngine {
     AvdGeometry geometry{};
     std::unique_ptr<avd::Pass> luma, chroma;
     std::unique_ptr<avd::PassthroughRing> passthrough;
+    std::unique_ptr<avd::ColourMeans> colour;  // the block means the passes pool their grain per colour with
     bool passthrough_luma = false;  // which group the ring holds
     bool luma_guides = false;       // `luma` is a chroma-only engine's luma guide, which cleans nothing
     bool poisoned = false;
@@ -1066,6 +1067,15 @@ AvdStatus fail_global(AvdStatus st, const std::string& message) {
 AvdStatus record(AvdEngine* e, AvdStatus st, const std::string& message) {
     if (e) e->last_error = st == AVD_OK ? std::string() : message;
     return st;
+}
+
+// planar.rs:194-217 (`measure_colour`): stream frame `frame`'s block means from all three planes,
+// before its passes see it, when the passes pool colour cells.
+std::optional<Failure> measure_colour(AvdEngine* e, const AvdPlane* planes, uint32_t frame) {
+    if (!e->colour) return std::nullopt;
+    auto f = e->colour->queue(planes, frame, e->stream);
+    if (f) e->poisoned = true;
+    return f;
 }
 
 AvdStatus record(AvdEngine* e, const std::optional<Failure>& f) {
@@ -1205,6 +1215,27 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
     }
     const bool gray = g.chroma == AVD_CHROMA_GRAY;
     const bool cleans_luma = engine->luma != nullptr && !engine->luma_guides;
+    {
+        // engine/spec.rs:366-381 (`colour_blocks`) and planar.rs:176-192 (`attach_colour`): frames
+        // with chroma whose passes pool colour cells get the block means of both grids, held for the
+        // frames the passes hold; the luma pass reads the luma grid, the chroma pass the chroma grid.
+        avd::Pass* luma_pass = cleans_luma ? engine->luma.get() : nullptr;
+        const bool pools = (luma_pass && luma_pass->measures_colour()) ||
+                           (engine->chroma && engine->chroma->measures_colour());
+        if (!gray && pools) {
+            size_t held = 0;
+            for (avd::Pass* p : {engine->luma.get(), engine->chroma.get()})
+                if (p) held = std::max(held, p->max_held_frames());
+            engine->colour = std::make_unique<avd::ColourMeans>();
+            if (auto f = engine->colour->allocate(g, held)) return fail_global(f->status, f->message);
+            if (luma_pass)
+                if (auto f = luma_pass->measure_colour(engine->colour.get(), true))
+                    return fail_global(f->status, f->message);
+            if (engine->chroma)
+                if (auto f = engine->chroma->measure_colour(engine->colour.get(), false))
+                    return fail_global(f->status, f->message);
+        }
+    }
     if (!gray && cleans_luma != (engine->chroma != nullptr)) {
         // planar.rs:210-220: one slot more than the cleaned pass holds frames.
         engine->passthrough = std::make_unique<avd::PassthroughRing>();
@@ -1242,6 +1273,7 @@ AvdStatus avd_engine_push(AvdEngine* e, const AvdPlane* planes, size_t n, size_t
     if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
     if (auto f = check_frame_planes(e->geometry, planes, n, e->geometry.input)) return record(e, f);
     const uint32_t frame = e->lead()->next_frame();
+    if (auto f = measure_colour(e, planes, frame)) return record(e, f);
     size_t value = 0;
     auto f = forward(e, &value, [&](avd::Pass* p, bool luma, size_t* v) {
         return p->push(group_planes(planes, luma), v);
@@ -1266,6 +1298,7 @@ AvdStatus avd_engine_push_context(AvdEngine* e, const AvdPlane* planes, size_t n
     if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
     if (auto f = check_frame_planes(e->geometry, planes, n, e->geometry.input)) return record(e, f);
     const uint32_t frame = e->lead()->next_frame();
+    if (auto f = measure_colour(e, planes, frame)) return record(e, f);
     auto f = forward(e, nullptr, [&](avd::Pass* p, bool luma, size_t* v) {
         *v = 0;
         return p->push_context(group_planes(planes, luma));
@@ -1321,6 +1354,7 @@ AvdStatus avd_engine_reset(AvdEngine* e) {
     if (!e) return AVD_ERR_NULL_ARG;
     if (e->luma) e->luma->reset();
     if (e->chroma) e->chroma->reset();
+    if (e->colour) e->colour->clear();
     e->poisoned = false;
     return record(e, AVD_OK, "");
 }

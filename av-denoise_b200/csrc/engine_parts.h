@@ -123,6 +123,34 @@ struct DeviceTimer {
 };
 
 // ---------------------------------------------------------------------------------------------
+// The block means of the newest frames on both 16x16 noise grids (noise/colour.rs:176-330,
+// `ColourBlocks`; colour.cu). The engine measures each pushed frame's mean luma, Cb and Cr from all
+// three planes before its passes see the frame, so the luma pass reads the chroma of its blocks and
+// the chroma pass the luma of its blocks. Stream frame f keeps slot f % slots, tagged with f, so a
+// read never returns another frame's means.
+class ColourMeans {
+   public:
+    std::optional<Failure> allocate(const AvdGeometry& g, size_t held_frames);
+    std::optional<Failure> queue(const AvdPlane* planes, uint32_t frame, cudaStream_t s);
+    // Stream frame `frame`'s means (3 floats per block) on the luma or the chroma grid, or null
+    // when its slot holds another frame.
+    const float* held(bool luma_grid, uint32_t frame) const;
+    void clear();
+    // The factor from a normalised sample to the 8-bit scale (colour.rs:338-361).
+    float grain_scale() const;
+
+   private:
+    AvdGeometry geometry_{};
+    size_t slots_ = 0, luma_blocks_ = 0, chroma_blocks_ = 0;
+    std::vector<int64_t> tags_;
+    DeviceBuffer luma_, chroma_;
+};
+
+// The colour parts of one geometry and input format (colour.rs:338-361).
+float colour_grain_scale(const AvdSampleFormat& f);
+float colour_eight_bit_scale(const AvdSampleFormat& f);
+
+// ---------------------------------------------------------------------------------------------
 // A pass over one plane group.
 class Pass {
    public:
@@ -139,6 +167,10 @@ class Pass {
     virtual AvdEngineTiming timing() = 0;
     virtual void sample_device_time(uint32_t every) = 0;
     virtual std::optional<Failure> fail_for_test() = 0;
+    // Whether the pass pools its measured grain into colour cells (nl4d/engine.rs:405-411), and the
+    // block means it does so with, on the luma or the chroma grid (engine/planar.rs:176-192).
+    virtual bool measures_colour() const { return false; }
+    virtual std::optional<Failure> measure_colour(const ColourMeans*, bool) { return std::nullopt; }
     cudaStream_t stream = nullptr;
 };
 
@@ -183,6 +215,11 @@ class NoiseFront {
     const float* curve_ratios() const { return state_.as<float>() + 16; }
     float* spatial_table() const { return spatial_.as<float>(); }
     float* pilot_table() const { return pilot_.as<float>(); }
+    // Pools each reading's blocks into colour cells with the block means `means` holds (on the luma
+    // grid with `luma_grid`) and fits the grain model at each fold (noise/colour.rs:733-827).
+    std::optional<Failure> measure_colour(const ColourMeans* means, bool luma_grid);
+    // The last fold's log gain tables, 976 per channel, or null without colour.
+    const float* colour_gains() const { return colour_ ? colour_gains_.as<float>() : nullptr; }
     void reset();
 
    private:
@@ -196,6 +233,10 @@ class NoiseFront {
     int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2, conf_stride_ = 1;
     DeviceBuffer lookahead_, partials_, records_, scratch_, history_records_, history_results_, settings_, state_,
         derived_, spatial_, pilot_, pyramid_, pair_, escalation_;
+    const ColourMeans* colour_ = nullptr;
+    bool colour_luma_ = true;
+    size_t colour_words_ = 0;  // int32 words of one frame's cell sums
+    DeviceBuffer colour_cells_, colour_window_, colour_scratch_, colour_table_, colour_gains_;
 };
 
 // NL4D pass over one plane group (nl4d_pass.cpp).

@@ -116,6 +116,13 @@ struct CollabLaunch {
     int pooled;
     int radius, refine, spatial_radius, k_max;
     int mv_stride, conf_stride, blk_step, blksize, blocks_x, blocks_y;
+    // The colour grain gains (collab/kernels/fused/colour.rs): one log gain table of 976 cells per
+    // channel, the centre frame's block means (3 floats per block of this plane's 16x16 grid,
+    // colour_blocks_x across) and the factor from a sample to the 8-bit scale; read with colour_on.
+    const float* colour_gains;
+    const float* colour_means;
+    float colour_scale;
+    int colour_on, colour_blocks_x;
 };
 
 cudaError_t launch_collab(const CollabLaunch& args, cudaStream_t stream);
@@ -247,6 +254,55 @@ cudaError_t launch_noise_fold(const float* records, const float* results, int ca
                               float* spatial, float* pilot, cudaStream_t s);
 cudaError_t launch_immerkaer(const float* frame, int channels, int width, int height, float scale, float* partials,
                              float* results, float* sigma_low, cudaStream_t stream);
+
+// The colour grain gains (colour.cu). A cell table holds 976 values per plane: 16 brightness bins of
+// one neutral cell and 5 saturation levels of 12 hue sectors. A frame's cell sums hold
+// colour_records(planes, luma) records of kColourCellWords int32 words: the planes' cells, then 16
+// luma calibration records or one record per chroma plane.
+constexpr int kColourCells = 976;
+constexpr int kColourCellWords = 69;
+constexpr int kColourFitPlaneWords = 22;
+constexpr int kColourDerivedCurveWord = 3;  // the derived words' curve flag
+size_t colour_records(int planes, bool luma);
+
+// noise/kernels/colour.rs:187-340: the mean luma, Cb and Cr (8-bit scale, chroma centred on 0) of
+// every 16x16 block of the luma and of the chroma noise grid, from the three input planes.
+struct ColourMeansLaunch {
+    const uint32_t *luma, *cb, *cr;  // word-packed planes
+    int width, height, shift_x, shift_y;
+    int samples_per_word;            // 4 (8-bit), 2 (9..16-bit) or 1 (f32)
+    bool is_float;
+    float eight_bit_scale, chroma_bias;
+    float *luma_means, *chroma_means;  // 3 floats per block of each grid
+};
+cudaError_t launch_colour_means(const ColourMeansLaunch& args, cudaStream_t s);
+// noise/kernels/colour.rs:342-430: one frame's cell sums (zeroed first) from its temporal records
+// and its block means on the records' grid; `luma` pools the luma calibration records.
+cudaError_t launch_colour_accumulate(const float* records, const float* means, int width, int height, int channels,
+                                     bool luma, float grain_scale, int32_t* cells, cudaStream_t s);
+// noise/kernels/colour.rs:441-470: the decoded sums of frames first..last (frame f in ring slot
+// f % capacity, `words` int32 words per slot).
+cudaError_t launch_colour_window(const int32_t* ring, int capacity, int first, int last, int words, float* window,
+                                 cudaStream_t s);
+// noise/colour.rs:630-680 (`ColourFit::queue`): both fits and the log gain tables of the window's sums.
+struct ColourFitLaunch {
+    const float* window;
+    int planes;
+    bool luma;                 // luma: mean levels, calibration against the curve; chroma: medians
+    const float* curve;        // 16 luma curve ratios (luma only)
+    const float* derived;      // the fold's derived words: the curve flag
+    float *levels, *ceilings, *fit_cells, *fit_planes, *bases;  // scratch (colour_fit_scratch_floats)
+    float *table, *gains;      // planes x 976 each
+};
+// The scratch floats of one fit: levels (2 per cell), ceilings (1), cell records (5), plane headers
+// and the lift's 2 x 976 queries per plane.
+inline size_t colour_fit_scratch_floats(int planes) {
+    return static_cast<size_t>(planes) * (kColourCells * 8 + kColourFitPlaneWords + 2 * kColourCells);
+}
+cudaError_t launch_colour_fit(const ColourFitLaunch& args, cudaStream_t s);
+// colour_fit.rs:196-262: a table's value and its gain at each of `n` (luma, cb, cr) colours.
+cudaError_t launch_colour_lookup(const float* table, const float* colours, int n, float* values, float* gains,
+                                 cudaStream_t s);
 
 // Adjoint of one windowed NLMeans frame (nlm_backward.cu).
 struct NlmBackwardLaunch {

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <deque>
+#include <string>
 #include <vector>
 
 #include "avd_internal.h"
@@ -50,18 +51,10 @@ class Nl4dPass final : public Pass {
                                          bool guides_only = false) {
         // nl4d/denoiser.rs:228-233: a luma filter pass applies the noise map (the measured luma noise
         // curve); a measured pass over frames with chroma also scales its thresholds by the colour
-        // grain gains when it applies the noise map or filters chroma, which are not built here.
+        // grain gains when it applies the noise map or filters chroma (the engine hands it the
+        // block means, engine/planar.rs:176-192).
         const bool noise_map = o.noise_map && channels == Channels::Luma && !guides_only;
         const bool colour_gains = !o.has_sigma && colour_frames && (noise_map || channels == Channels::Chroma);
-        if (colour_gains && channels == Channels::Chroma)
-            return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "NL4D chroma with the automatic noise estimate needs the colour grain gains, which are "
-                           "not available in this build; set sigma"};
-        if (colour_gains)
-            return Failure{AVD_ERR_INVALID_OPTIONS,
-                           "the NL4D luma noise map of the automatic noise estimate on frames with chroma needs the "
-                           "colour grain gains, which are not available in this build; set noise_map to false or "
-                           "set sigma"};
         const AvdMotionSearch& m = o.motion;
         // motion/search.rs:133-139: Auto resolves to Chained { refine_radius: 2 } at d >= 3.
         const bool chained = m.estimation == AVD_ESTIMATION_CHAINED ||
@@ -99,6 +92,7 @@ class Nl4dPass final : public Pass {
         p->measures_ = !o.has_sigma;
         p->guides_ = guides_only;
         p->noise_map_ = noise_map;
+        p->colour_gains_ = colour_gains;
         if (auto f = p->allocate()) return f;
         *result = std::move(p);
         return std::nullopt;
@@ -192,6 +186,14 @@ class Nl4dPass final : public Pass {
     std::optional<uint32_t> emitted_frame() const override { return emitted_; }
     AvdEngineTiming timing() override { return timer_.collect(); }
     void sample_device_time(uint32_t every) override { timer_.every = every; }
+    bool measures_colour() const override { return colour_gains_; }
+    // nl4d/denoiser.rs:732-745 (`measure_colour`).
+    std::optional<Failure> measure_colour(const ColourMeans* means, bool luma_grid) override {
+        if (!colour_gains_ || !measures_) return std::nullopt;
+        colour_means_ = means;
+        colour_luma_grid_ = luma_grid;
+        return noise_.measure_colour(means, luma_grid);
+    }
     std::optional<Failure> fail_for_test() override {
         poisoned_ = true;
         return Failure{AVD_ERR_GPU, "forced failure"};
@@ -796,6 +798,18 @@ class Nl4dPass final : public Pass {
         a.blksize = static_cast<int>(opts_.motion.blksize);
         a.blocks_x = blocks_x_;
         a.blocks_y = blocks_y_;
+        if (colour_means_) {
+            // collab_pass.rs:71-75 (`colour_gain_inputs`): the gains of the window's fit and the
+            // block means of the pass's centre frame, on this plane's grid.
+            const uint32_t frame = slot_frames_[centre_slot];
+            a.colour_means = colour_means_->held(colour_luma_grid_, frame);
+            if (!a.colour_means)
+                return Failure{AVD_ERR_GPU, "the block colour of stream frame " + std::to_string(frame) + " is not held"};
+            a.colour_gains = noise_.colour_gains();
+            a.colour_scale = colour_means_->grain_scale();
+            a.colour_on = 1;
+            a.colour_blocks_x = (static_cast<int>(width_) + 15) / 16;
+        }
         cudaError_t e = launch_collab(a, stream);
         if (e != cudaSuccess) return gpu_failure("collab launch", e);
         return std::nullopt;
@@ -939,6 +953,9 @@ class Nl4dPass final : public Pass {
     size_t tail_remaining_ = 0, pushes_ = 0;
     bool pushed_ = false, poisoned_ = false;
     bool noise_map_ = false;  // the filter scales the luma threshold by the measured noise curve
+    bool colour_gains_ = false;  // the filter scales its thresholds by the measured colour grain gains
+    const ColourMeans* colour_means_ = nullptr;
+    bool colour_luma_grid_ = true;
     std::optional<uint32_t> emitted_;
     DeviceTimer timer_;
 };

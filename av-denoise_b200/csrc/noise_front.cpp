@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <string>
 
 #include "avd_internal.h"
 #include "engine_parts.h"
@@ -167,6 +168,35 @@ std::optional<Failure> NoiseFront::read_against(size_t frame, std::optional<size
     e = launch_noise_reading(records, c, w, h, scratch_.as<float>(), min_static_blocks(blocks),
                              cfg_.luma_fields && cfg_.temporal_radius > 0, reading, s);
     if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise reading launch", e)};
+    if (colour_ && records) {
+        // noise/colour.rs:765-790 (`queue_colour_cells`): the reading's blocks pooled into the
+        // frame's cell sums, replacing any earlier read of the same frame.
+        const float* means = colour_->held(colour_luma_, static_cast<uint32_t>(frame));
+        if (!means)
+            return Failure{AVD_ERR_GPU, "the block colour of stream frame " + std::to_string(frame) + " is not held"};
+        e = launch_colour_accumulate(records, means, w, h, c, colour_luma_, colour_->grain_scale(),
+                                     colour_cells_.as<int32_t>() + (frame % capacity_) * colour_words_, s);
+        if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("colour cells launch", e)};
+    }
+    return std::nullopt;
+}
+
+std::optional<Failure> NoiseFront::measure_colour(const ColourMeans* means, bool luma_grid) {
+    if (cfg_.temporal_radius == 0) return std::nullopt;  // colour.rs:737-745: no temporal stats, no cells
+    colour_ = means;
+    colour_luma_ = luma_grid;
+    const int planes = static_cast<int>(cfg_.channels);
+    colour_words_ = colour_records(planes, luma_grid) * kColourCellWords;
+    auto fail = [](const char* what, cudaError_t e) { return Failure{AVD_ERR_GPU, cuda_message(what, e)}; };
+    cudaError_t e;
+    if ((e = colour_cells_.alloc(capacity_ * colour_words_ * sizeof(int32_t))) != cudaSuccess ||
+        (e = colour_window_.alloc(colour_words_ * sizeof(float))) != cudaSuccess ||
+        (e = colour_scratch_.alloc(colour_fit_scratch_floats(planes) * sizeof(float))) != cudaSuccess ||
+        (e = colour_table_.alloc(static_cast<size_t>(planes) * kColourCells * sizeof(float))) != cudaSuccess ||
+        (e = colour_gains_.alloc(static_cast<size_t>(planes) * kColourCells * sizeof(float))) != cudaSuccess)
+        return fail("colour cells", e);
+    for (DeviceBuffer* b : {&colour_cells_, &colour_gains_})
+        if ((e = cudaMemset(b->ptr, 0, b->bytes)) != cudaSuccess) return fail("colour cells clear", e);
     return std::nullopt;
 }
 
@@ -227,6 +257,28 @@ std::optional<Failure> NoiseFront::fold(uint32_t centre, cudaStream_t s) {
                                       state_.as<float>(), derived_.as<float>(), spatial_.as<float>(),
                                       pilot_.as<float>(), s);
     if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise fold launch", e)};
+    if (colour_) {
+        // noise/colour.rs:793-808 (`queue_colour_window`): the window's cell sums, then the grain
+        // model fitted from them against the curve and derived words the fold just wrote.
+        e = launch_colour_window(colour_cells_.as<int32_t>(), static_cast<int>(capacity_), first, last,
+                                 static_cast<int>(colour_words_), colour_window_.as<float>(), s);
+        if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("colour window launch", e)};
+        const int planes = static_cast<int>(cfg_.channels);
+        ColourFitLaunch a{};
+        a.window = colour_window_.as<float>();
+        a.planes = planes;
+        a.luma = colour_luma_;
+        a.curve = curve_ratios();
+        a.derived = derived_.as<float>();
+        a.levels = colour_scratch_.as<float>();
+        a.ceilings = a.levels + 2 * planes * kColourCells;
+        a.fit_cells = a.ceilings + planes * kColourCells;
+        a.fit_planes = a.fit_cells + 5 * planes * kColourCells;
+        a.bases = a.fit_planes + planes * kColourFitPlaneWords;
+        a.table = colour_table_.as<float>();
+        a.gains = colour_gains_.as<float>();
+        if ((e = launch_colour_fit(a, s)) != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("colour fit launch", e)};
+    }
     return std::nullopt;
 }
 

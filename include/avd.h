@@ -595,6 +595,40 @@ AVD_API AvdStatus avd_noise_compensated_stats(uint64_t next, uint64_t prev, uint
 AVD_API AvdStatus avd_noise_reading(uint64_t records, uint32_t channels, uint32_t width, uint32_t height,
                                     uint32_t curve, uint64_t scratch, uint64_t reading, void* stream);
 
+/* The colour grain gains (av-denoise-core/src/noise/colour.rs, noise/kernels/colour.rs,
+ * noise/kernels/colour_fit.rs). A cell table holds 976 values per plane: 16 brightness bins, each
+ * one neutral cell and 5 saturation levels of 12 hue sectors. A frame's cell sums hold
+ * avd_colour_records records of 69 int32 words (count, fixed-point log grain, luma, Cb and Cr sums,
+ * a 64-bin log-grain histogram): the planes' cells, then 16 luma calibration records (luma) or one
+ * record per chroma plane. */
+AVD_API uint64_t avd_colour_records(uint32_t planes, uint32_t luma);
+/* The mean luma, Cb and Cr (8-bit scale, chroma centred on 0) of every 16x16 block of the luma and
+ * the chroma noise grids of one frame of `geometry` (kernels/colour.rs:187-340,
+ * `noise_colour_means`), 3 floats per block of each grid. */
+AVD_API AvdStatus avd_colour_means(uint64_t luma, uint64_t cb, uint64_t cr, const AvdGeometry* geometry,
+                                   uint64_t luma_means, uint64_t chroma_means, void* stream);
+/* One frame's cell sums, zeroed first, from its temporal records and its block means on the records'
+ * grid (kernels/colour.rs:342-430, `noise_colour_accumulate`); `luma` pools the luma calibration
+ * records. `grain_scale` turns a normalised residual sigma into codes on the 8-bit scale. */
+AVD_API AvdStatus avd_colour_accumulate(uint64_t records, uint64_t means, uint32_t width, uint32_t height,
+                                        uint32_t channels, uint32_t luma, float grain_scale, uint64_t cells,
+                                        void* stream);
+/* The decoded sums of frames first..=last of a ring of `capacity` frames' cell sums (frame f in slot
+ * f % capacity, `words` int32 words each; kernels/colour.rs:441-470, `noise_colour_window`). */
+AVD_API AvdStatus avd_colour_window(uint64_t ring, uint32_t capacity, uint32_t first, uint32_t last, uint32_t words,
+                                    uint64_t window, void* stream);
+/* Both fits of the window's sums and the log gain tables (noise/colour.rs:630-680, `ColourFit::queue`):
+ * `planes` tables of 976 log grains into `table` and of 976 log gains into `gains`. A luma fit
+ * (`luma`) reads the 16 curve ratios `curve` while the derived words' curve flag (word 3 of
+ * `derived`) is set. `scratch` holds avd_colour_fit_scratch_floats floats. */
+AVD_API uint64_t avd_colour_fit_scratch_floats(uint32_t planes);
+AVD_API AvdStatus avd_colour_fit(uint64_t window, uint32_t planes, uint32_t luma, uint64_t curve, uint64_t derived,
+                                 uint64_t scratch, uint64_t table, uint64_t gains, void* stream);
+/* A table's value and its exponential (the gain) at each of `n` (luma, cb, cr) colours
+ * (colour_fit.rs:196-262, `colour_table_value`, `colour_gain`). */
+AVD_API AvdStatus avd_colour_lookup(uint64_t table, uint64_t colours, uint32_t n, uint64_t values, uint64_t gains,
+                                    void* stream);
+
 /* The fold settings words for a plane of width x height (noise/fold.rs:118-146, `fold_words`):
  * sigma_scale, whether the consumer applies the curve, the weight-scale gain and floor, the h2
  * coefficient (`h2_auto` 0 for a fixed strength `h2_fixed`), the pilot factor, the noise-offset

@@ -18,6 +18,9 @@
 #include <cstring>
 #include <vector>
 
+#include "colour_table.h"
+#include "mirror_math.h"
+
 namespace {
 
 constexpr int P = 8;      // PATCH_SIZE
@@ -32,6 +35,7 @@ constexpr float WEIGHT_GAIN = ACCUM_CLAMP / WEIGHT_CLAMP;
 constexpr float VARIANCE_FLOOR = 1.0e-20f;
 constexpr float CURVE_SCALE_MIN = 0.33f;
 constexpr float CURVE_SCALE_MAX = 3.0f;
+constexpr float COLOUR_CURVE_SCALE_MAX = 6.0f;  // fused/mod.rs:57-58: curve and colour gain together
 constexpr int CURVE_BINS = 16;
 constexpr float FRAC_1_SQRT_2 = 0.70710678118654752440f;
 
@@ -253,6 +257,13 @@ struct CollabArgs {
     int mv_stride, conf_stride, blk_step, blksize, blocks_x, blocks_y;
     float c_min, lambda_ht, accum_scale, pool_ratio, weight_scale;
     int pooled, curve_valid;
+    // The colour grain gains (collab/kernels/fused/colour.rs): one log gain table per channel, the
+    // centre frame's block means on this plane's 16x16 grid, the factor from a sample to the 8-bit
+    // scale; read only with colour_on.
+    const float* colour_gains;
+    const float* colour_means;
+    float colour_scale;
+    int colour_on, colour_blocks_x;
 };
 
 struct Group {
@@ -530,7 +541,7 @@ void process_reference(const CollabArgs& a, uint32_t ref_x_index, uint32_t ref_y
         col_second[sub] = s1;
     }
     const float patch_luma = reduce8(col_first) / 64.0f;
-    (void)col_second;
+    const float patch_second = C > 1 ? reduce8(col_second) / 64.0f : 0.0f;
     const float bins = static_cast<float>(CURVE_BINS);
     const float curve_pos = std::min(std::max(patch_luma * bins - 0.5f, 0.0f), bins - 1.0f);
     const uint32_t lower = std::min<uint32_t>(static_cast<uint32_t>(curve_pos), CURVE_BINS - 2);
@@ -540,11 +551,34 @@ void process_reference(const CollabArgs& a, uint32_t ref_x_index, uint32_t ref_y
         const float lo = a.noise_curve[lower], hi = a.noise_curve[lower + 1];
         ratio = lo + (hi - lo) * fraction;
     }
-    const float curve_scale = std::min(std::max(ratio * 1.0f, CURVE_SCALE_MIN), CURVE_SCALE_MAX);
-    const float flat_scale = std::min(std::max(1.0f, CURVE_SCALE_MIN), CURVE_SCALE_MAX);
+    // fused/colour.rs:48-83 (`threshold_gains`): a luma patch reads its own mean luma and its block's
+    // Cb and Cr, a chroma patch its own Cb and Cr and its block's luma.
+    float first_gain = 1.0f, second_gain = 1.0f;
+    if (a.colour_on) {
+        const uint32_t bx = (rx + P / 2) / 16, by = (ry + P / 2) / 16;
+        const float* m = a.colour_means + (by * static_cast<uint32_t>(a.colour_blocks_x) + bx) * 3;
+        if (C == 1) {
+            first_gain = mirror::exp_mirror(colour_table::table_value(a.colour_gains, patch_luma * a.colour_scale,
+                                                                      m[1], m[2]));
+        } else {
+            const float cb = patch_luma * a.colour_scale - 128.0f, cr = patch_second * a.colour_scale - 128.0f;
+            first_gain = mirror::exp_mirror(colour_table::table_value(a.colour_gains, m[0], cb, cr));
+            second_gain = mirror::exp_mirror(colour_table::table_value(a.colour_gains + colour_table::CELLS, m[0],
+                                                                       cb, cr));
+        }
+    }
+    // A luma gain joins the curve's scale, and a chroma gain scales its channel's threshold.
+    float curve_gain = 1.0f, first_channel_gain = first_gain, scale_max = CURVE_SCALE_MAX;
+    if (C == 1) {
+        curve_gain = first_gain;
+        first_channel_gain = 1.0f;
+        scale_max = a.colour_on ? COLOUR_CURVE_SCALE_MAX : CURVE_SCALE_MAX;
+    }
+    const float curve_scale = std::min(std::max(ratio * curve_gain, CURVE_SCALE_MIN), scale_max);
+    const float flat_scale = std::min(std::max(curve_gain, CURVE_SCALE_MIN), scale_max);
     const float luma_scale = a.curve_valid ? curve_scale : flat_scale;
-    const float first_lambda = (a.lambda_ht * luma_scale) * 1.0f;
-    const float second_lambda = a.lambda_ht * 1.0f;
+    const float first_lambda = (a.lambda_ht * luma_scale) * first_channel_gain;
+    const float second_lambda = a.lambda_ht * second_gain;
     const uint32_t ref_idx = ref_y_index * refs_x + ref_x_index;
     float scaled_weight = 0.0f;
     const int plane = a.width * a.height;

@@ -40,6 +40,7 @@
 #include <cstring>
 #include <vector>
 
+#include "colour_table.h"
 #include "mirror_math.h"
 
 namespace {
@@ -47,21 +48,14 @@ namespace {
 using mirror::atan2_mirror;
 using mirror::exp_mirror;
 using mirror::log_mirror;
+using namespace colour_table;
 
 constexpr int NB = 16;
 constexpr float STATIC_GATE = 1.5f / 255.0f;
 constexpr float SQRT_2F = 1.41421356237309504880f;
-constexpr float PI_F = 3.14159265358979324f;
-constexpr float TAU_F = 6.28318530717958648f;
 constexpr float LN_2F = 0.693147180559945309f;
 
 // noise/colour.rs:24-176.
-constexpr int BRIGHTNESS_BINS = 16;
-constexpr float BRIGHTNESS_STEP = 16.0f;
-constexpr float SAT_EDGES[5] = {6.0f, 12.0f, 20.0f, 30.0f, 44.0f};
-constexpr int HUE_BINS = 12;
-constexpr int PER_BRIGHTNESS = 1 + 5 * HUE_BINS;  // 61
-constexpr int CELLS = BRIGHTNESS_BINS * PER_BRIGHTNESS;  // 976
 constexpr float NEUTRAL_SATURATION = 8.0f;
 constexpr int W_COUNT = 0, W_LOG = 1, W_LUMA = 2, W_CB = 3, W_CR = 4, W_HIST = 5;
 constexpr int HIST_BINS = 64;
@@ -73,7 +67,6 @@ constexpr float CHROMA_CENTRE = 128.0f;
 constexpr float LUMA_MIN = 20.0f, LUMA_MAX = 240.0f;
 constexpr float LUMA_GRAIN_FLOOR = 0.05f, CHROMA_GRAIN_FLOOR = 0.03f;
 constexpr float LOG_FIXED = 2048.0f, MEAN_FIXED = 16.0f;
-constexpr float SAT_CENTRES[6] = {3.0f, 9.0f, 16.0f, 25.0f, 37.0f, 51.0f};
 constexpr int FIT_THREADS = 256;
 constexpr int KERNEL_LANES = 8;
 constexpr int KNOTS = 17, LAST_KNOT = 16;
@@ -97,27 +90,6 @@ constexpr float SECTOR_COS[12] = {-C15, -H45, -S15, S15, H45, C15, C15, H45, S15
 constexpr float SECTOR_SIN[12] = {-S15, -H45, -C15, -C15, -H45, -S15, S15, H45, C15, C15, H45, S15};
 
 int record_count(int planes, bool luma) { return planes * CELLS + (luma ? BRIGHTNESS_BINS : planes); }
-
-float clampf(float v, float lo, float hi) { return std::min(std::max(v, lo), hi); }
-
-uint32_t brightness_bin(float luma) {
-    const float scaled = std::floor(luma / BRIGHTNESS_STEP);
-    return static_cast<uint32_t>(clampf(scaled, 0.0f, static_cast<float>(BRIGHTNESS_BINS - 1)));
-}
-
-// colour.rs:57-83 (`colour_cell`).
-uint32_t colour_cell(float luma, float cb, float cr) {
-    const uint32_t brightness = brightness_bin(luma);
-    const float saturation = std::sqrt(cb * cb + cr * cr);
-    uint32_t level = 0;
-    for (float edge : SAT_EDGES) level += saturation >= edge ? 1u : 0u;
-    const float hue = atan2_mirror(cr, cb);
-    const float turn = (hue + PI_F) / TAU_F;
-    const float raw_sector = std::floor(turn * static_cast<float>(HUE_BINS));
-    const uint32_t sector = static_cast<uint32_t>(std::max(raw_sector, 0.0f)) % HUE_BINS;
-    const uint32_t coloured = 1u + (std::max(level, 1u) - 1u) * HUE_BINS + sector;
-    return brightness * PER_BRIGHTNESS + (level == 0 ? 0u : coloured);
-}
 
 uint32_t histogram_bin(float log_grain) {
     const float position = std::floor((log_grain - LOG_MIN) / LOG_STEP);
@@ -144,72 +116,6 @@ float read_sample(const uint32_t* plane, int64_t index, int spw, bool is_float) 
     const int bits = 32 / spw;
     const uint32_t mask = spw == 1 ? 0xFFFFFFFFu : ((1u << bits) - 1u);
     return static_cast<float>((word >> ((index % spw) * bits)) & mask);
-}
-
-// ---- the table lookup (colour_fit.rs:88-262) ---------------------------------------------------
-
-float between(float v, float lo, float hi) { return (v - lo) / (hi - lo); }
-
-float saturation_position(float s) {
-    const float step1 = between(s, SAT_CENTRES[0], SAT_CENTRES[1]);
-    const float step2 = 1.0f + between(s, SAT_CENTRES[1], SAT_CENTRES[2]);
-    const float step3 = 2.0f + between(s, SAT_CENTRES[2], SAT_CENTRES[3]);
-    const float step4 = 3.0f + between(s, SAT_CENTRES[3], SAT_CENTRES[4]);
-    const float step5 = 4.0f + between(s, SAT_CENTRES[4], SAT_CENTRES[5]);
-    const float upper4 = s < SAT_CENTRES[4] ? step4 : step5;
-    const float upper3 = s < SAT_CENTRES[3] ? step3 : upper4;
-    const float upper2 = s < SAT_CENTRES[2] ? step2 : upper3;
-    const float position = s < SAT_CENTRES[1] ? step1 : upper2;
-    return clampf(position, 0.0f, 5.0f);
-}
-
-uint32_t table_index(uint32_t brightness, uint32_t level, uint32_t sector) {
-    const uint32_t coloured = 1u + (std::max(level, 1u) - 1u) * HUE_BINS + sector;
-    return brightness * PER_BRIGHTNESS + (level == 0 ? 0u : coloured);
-}
-
-struct Position {
-    uint32_t brightness_low, level_low, sector_low;
-    float brightness_fraction, level_fraction, hue_fraction;
-};
-
-Position table_position(float luma, float cb, float cr) {
-    Position p;
-    const float bpos = clampf(luma / BRIGHTNESS_STEP - 0.5f, 0.0f, static_cast<float>(BRIGHTNESS_BINS - 1));
-    p.brightness_low = std::min(static_cast<uint32_t>(std::floor(bpos)), static_cast<uint32_t>(BRIGHTNESS_BINS - 2));
-    p.brightness_fraction = bpos - static_cast<float>(p.brightness_low);
-    const float saturation = std::sqrt(cb * cb + cr * cr);
-    const float lpos = saturation_position(saturation);
-    p.level_low = std::min(static_cast<uint32_t>(std::floor(lpos)), 4u);
-    p.level_fraction = lpos - static_cast<float>(p.level_low);
-    const float hue = atan2_mirror(cr, cb);
-    const float hpos = (hue + PI_F) / TAU_F * static_cast<float>(HUE_BINS) - 0.5f;
-    const float hfloor = std::floor(hpos);
-    p.hue_fraction = hpos - hfloor;
-    p.sector_low = static_cast<uint32_t>(hfloor + static_cast<float>(HUE_BINS)) % HUE_BINS;
-    return p;
-}
-
-void table_corner(const Position& p, int corner, uint32_t* index, float* weight) {
-    const int bs = corner / 4, ls = (corner / 2) % 2, ss = corner % 2;
-    const float bw = bs ? p.brightness_fraction : 1.0f - p.brightness_fraction;
-    const float lw = ls ? p.level_fraction : 1.0f - p.level_fraction;
-    const float sw = ss ? p.hue_fraction : 1.0f - p.hue_fraction;
-    const uint32_t sector = (p.sector_low + ss) % HUE_BINS;
-    *index = table_index(p.brightness_low + bs, p.level_low + ls, sector);
-    *weight = bw * lw * sw;
-}
-
-float table_value(const float* table, float luma, float cb, float cr) {
-    const Position p = table_position(luma, cb, cr);
-    float value = 0.0f;
-    for (int corner = 0; corner < 8; ++corner) {
-        uint32_t index;
-        float weight;
-        table_corner(p, corner, &index, &weight);
-        value += weight * table[index];
-    }
-    return value;
 }
 
 // ---- the fit (colour_fit.rs:264-935) ------------------------------------------------------------

@@ -394,6 +394,8 @@ class CollabArgs(C.Structure):
         ("blksize", C.c_int), ("blocks_x", C.c_int), ("blocks_y", C.c_int),
         ("c_min", C.c_float), ("lambda_ht", C.c_float), ("accum_scale", C.c_float), ("pool_ratio", C.c_float),
         ("weight_scale", C.c_float), ("pooled", C.c_int), ("curve_valid", C.c_int),
+        ("colour_gains", _fp), ("colour_means", _fp), ("colour_scale", C.c_float), ("colour_on", C.c_int),
+        ("colour_blocks_x", C.c_int),
     ]
 
 
@@ -441,8 +443,9 @@ def collab_fused(ring: np.ndarray, width: int, height: int, channels: int, *, ce
                  mv_field=None, confidence=None, neighbour_slots=None, c_min=0.0, refine=0, spatial_radius=4,
                  k_max=8, sigma=(0.02,), lambda_ht=5.3, rho=0.0, profile=None, kaiser_beta=0.0,
                  noise_curve=None, pooled=None, blksize=16, blk_step=8, blocks_x=1, blocks_y=1,
-                 mv_stride=2, conf_stride=1, weight_scale_override=None):
-    """One `collab_fused` launch on the CPU. Returns (accum, wsum, group_weight)."""
+                 mv_stride=2, conf_stride=1, weight_scale_override=None, colour=None):
+    """One `collab_fused` launch on the CPU. Returns (accum, wsum, group_weight). `colour` is
+    (gains tables, block means on this plane's 16x16 grid, 8-bit scale) or None."""
     ring = np.ascontiguousarray(ring, np.float32)
     frames = ring.size // (width * height * channels)
     profile = dct_noise_profile(rho) if profile is None else np.asarray(profile, np.float32)
@@ -474,6 +477,11 @@ def collab_fused(ring: np.ndarray, width: int, height: int, channels: int, *, ce
     a.accum_scale = cross_frame_accum_scale(spatial_radius, radius)
     a.pool_ratio, a.pooled = (pooled or 0.0), int(pooled is not None)
     a.weight_scale, a.curve_valid = ws, int(noise_curve is not None)
+    if colour is not None:
+        cg = np.ascontiguousarray(colour[0], np.float32)
+        cm = np.ascontiguousarray(colour[1], np.float32).reshape(-1)
+        a.colour_gains, a.colour_means, a.colour_scale = _f(cg), _f(cm), float(colour[2])
+        a.colour_on, a.colour_blocks_x = 1, -(-width // 16)
     l = lib()
     l.orc_collab_fused.argtypes = [C.POINTER(CollabArgs)]
     l.orc_collab_fused(C.byref(a))
@@ -746,10 +754,10 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     completes the region d slots behind it; at the end, tail passes centred on d+1..2d (or, for a
     stream shorter than the ring, on every real frame after padding with the last frame). The
     first `context` frames are priming pushes (no head passes). With `noise`, a function of a pass's
-    centre stream frame returning (sigma, weight_scale, sad_floor) or (sigma, weight_scale,
-    sad_floor, curve), each pass reads those (the automatic estimate's fold around that frame)
-    instead of the pinned sigma's; `curve` is the 16 luma noise-curve ratios, or None while the
-    fold's curve flag is clear. With `share_writes`
+    centre stream frame returning (sigma, weight_scale, sad_floor), optionally followed by curve and
+    colour, each pass reads those (the automatic estimate's fold around that frame) instead of the
+    pinned sigma's; `curve` is the 16 luma noise-curve ratios, or None while the fold's curve flag
+    is clear, and `colour` the (gain tables, centre block means, 8-bit scale) of collab_fused. With `share_writes`
     each window's field is shared for a chroma stream; with `share_reads` the window's motion is the
     shared luma field of the centre frame, searched one pixel around at one level with confidence
     (nlmeans/dispatch/motion.rs:231-310), and no motion of this plane's own is searched."""
@@ -786,10 +794,11 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
             zeroed[i] = False
         st["passes"] += 1
         slots = [phys(l) for l in range(tf) if l != centre]
-        p_sigma, p_weight, p_floor, p_curve = sigma, None, sad_floor, None
+        p_sigma, p_weight, p_floor, p_curve, p_colour = sigma, None, sad_floor, None, None
         if noise is not None:
             p_sigma, p_weight, p_floor, *rest = noise(slot_frames[cs])
             p_curve = rest[0] if rest else None
+            p_colour = rest[1] if len(rest) > 1 else None
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
         if share_reads is not None:
             mapped = share_reads.read(st["call"], slot_frames[cs] % tf, slot_frames[cs])
@@ -812,7 +821,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
                                   confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
                                   c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
                                   sigma=(p_sigma,) * c, weight_scale_override=p_weight, lambda_ht=lambda_ht,
-                                  kaiser_beta=kaiser_beta, noise_curve=p_curve,
+                                  kaiser_beta=kaiser_beta, noise_curve=p_curve, colour=p_colour,
                                   pooled=pool_ratio, blksize=blksize, blk_step=step, blocks_x=bx, blocks_y=by,
                                   mv_stride=bx * by * 2, conf_stride=bx * by)
         accum[:] += acc.reshape(tf, -1)
@@ -1052,12 +1061,13 @@ def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: 
 
 def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, height: int, *, blksize: int,
                       overlap: int, search_radius: int, levels: int, thsad: float = 0.0, ceiling: int = 0,
-                      luma_fields: bool = False):
+                      luma_fields: bool = False, records_out: list | None = None):
     """Every frame's reading as a motion-compensated look-ahead takes it
     (nlmeans/denoiser/lookahead.rs:283-319, 425-458, 543-605): frame i >= 1 is searched against
     frame i - 1 (newer to older) and read along that field; frame 1 is also searched older to newer
     and frame 0 re-read along it. Frame 0 keeps its Immerkaer words from its own read. Returns
-    (readings, Immerkaer totals)."""
+    (readings, Immerkaer totals). With `records_out`, each frame's final temporal records are
+    appended to it."""
     step = blksize - overlap
     mb = (max(-(-width // step), 1), max(-(-height // step), 1))
     # With `ceiling` the pair searches escalate, measuring their own floor (lookahead.rs:509-515).
@@ -1072,6 +1082,8 @@ def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, heigh
         if i == 0:
             readings.append(noise_reading(np.zeros(rec_len, np.float32), low, channels, width, height, True,
                                           luma_fields))
+            if records_out is not None:
+                records_out.append(np.zeros(rec_len, np.float32))
             continue
         pair = np.stack([np.ascontiguousarray(frames[i - 1], np.float32),
                          np.ascontiguousarray(f, np.float32)]).reshape(-1)
@@ -1079,10 +1091,14 @@ def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, heigh
         newer_to_older, _ = motion_search(pyr, width, height, 2, 1, [0], **kw)
         rec = temporal_stats_mc(f, frames[i - 1], channels, width, height, newer_to_older[0], mb, step, luma_fields)
         readings.append(noise_reading(rec, low, channels, width, height, True, luma_fields))
+        if records_out is not None:
+            records_out.append(rec)
         if i == 1:
             older_to_newer, _ = motion_search(pyr, width, height, 2, 0, [1], **kw)
             rec0 = temporal_stats_mc(frames[0], f, channels, width, height, older_to_newer[0], mb, step, luma_fields)
             readings[0] = noise_reading(rec0, lows[0], channels, width, height, True, luma_fields)
+            if records_out is not None:
+                records_out[0] = rec0
     return readings, totals
 
 

@@ -119,3 +119,88 @@ def test_nl4d_noise_map_on_frames_with_chroma_needs_the_colour_gains():
     o = avd.Nl4dOptions(sigma=None, temporal_radius=1)
     with pytest.raises(avd.InvalidOptions, match="colour grain gains"):
         avd.build_engine(avd.EngineSpec.nl4d(o, None, avd.Geometry(64, 48, avd.ChromaLayout.YUV420, fmt, fmt)))
+
+
+def pack_plane(codes):
+    """A u8 plane as the engine's word-packed layout."""
+    flat = np.asarray(codes, np.uint8).reshape(-1)
+    return np.concatenate([flat, np.zeros((-len(flat)) % 4, np.uint8)]).view(np.uint32)
+
+
+def colour_noise(oracle, clip_frames, fmt, d, luma, *, blksize=16, overlap=8, search_radius=4, levels=2):
+    """The measured front of a luma (`luma`) or chroma NL4D pass over a 4:2:0 u8 clip with its colour
+    grain gains: per centre frame (sigma, weight scale, SAD floor, curve, colour), as the engine
+    pools each reading into its frame's cell sums and fits the window at each fold
+    (noise/colour.rs:733-827, nl4d/collab_pass.rs:71-75)."""
+    planes = [f[0:1] if luma else f[1:3] for f in clip_frames]
+    f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), 0.0) for p in planes]
+    h, w, c = f32[0].shape
+    H, W = clip_frames[0][0].shape
+    means = [oracle.colour_means(pack_plane(f[0]), pack_plane(f[1]), pack_plane(f[2]), W, H, 1, 1, 4, False, 1.0, 0.0)
+             for f in clip_frames]
+    grid = [m[0] if luma else m[1] for m in means]
+    records = []
+    readings, totals = oracle.noise_readings_mc(f32, c, w, h, blksize=blksize, overlap=overlap,
+                                                search_radius=search_radius, levels=levels, luma_fields=luma,
+                                                records_out=records)
+    f = np.float32
+    area, unit = f(81.0), f(1.2) * f(1.0) * f(255.0)
+    settings = oracle.fold_words(w, h, curve_applies=luma, g_max=float(oracle.dct_noise_profile(0.0).max()),
+                                 h2_per_inverse_variance=float(f(65025.0) / (f(3.0) * unit * unit * area)),
+                                 h2_fixed=float(f(65025.0) / (f(3.0) * f(1.2) * f(1.2) * area)),
+                                 offset_per_variance=float(f(2.0) * (f(3.0) if luma else f(1.5)) * f(1.0) * area),
+                                 sad_per_sigma=oracle.sad_noise_floor(blksize, 1.0))
+    folds = oracle.fold_stream(readings, totals, settings, c, 0, d)
+    cap = 2 * 8 + 1 + d
+    cells = [oracle.colour_accumulate(r, g, w, h, c, luma, 255.0) for r, g in zip(records, grid)]
+    ring = np.zeros((cap, len(cells[0])), np.int32)
+    out = []
+    for centre in range(len(clip_frames)):
+        first, last = oracle.noise_window(centre, len(clip_frames) - 1)
+        for fr in range(first, last + 1):
+            ring[fr % cap] = cells[fr]
+        window = oracle.colour_window(ring, cap, first, last)
+        state, derived = folds[centre][0], folds[centre][1]
+        _, gains, _ = oracle.colour_fit(window, c, luma, state[16:32], bool(derived[3]))
+        curve = state[16:32].copy() if derived[3] != 0 else None
+        out.append((float(derived[0]), float(derived[2]), float(derived[4]), curve, (gains, grid[centre], 255.0)))
+    return (lambda frame: out[frame]), out
+
+
+def colour_clip(w, h, n, seed):
+    """A 4:2:0 u8 clip panning 2 pixels a frame over coloured bands whose luma grain grows with
+    warmth (Cr above Cb) and brightness, so the colour gains move away from 1."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:h, 0:w + 4 * n].astype(np.float32)
+    luma = 40 + 170 * x / (w + 4 * n)
+    cb = 128 + 45 * np.sin(y / 23.0)
+    cr = 128 + 45 * np.cos(x / 31.0 + y / 47.0)
+    frames = []
+    for i in range(n):
+        sl = slice(2 * i, 2 * i + w)
+        lb, cbb, crb = luma[:, sl], cb[:, sl], cr[:, sl]
+        warm = np.clip((crb - cbb) / 40.0, 0, None)
+        grain = (2.0 + lb / 80.0) * (1.0 + warm)
+        yp = np.clip(np.rint(lb + rng.normal(0, 1, lb.shape) * grain), 0, 255).astype(np.uint8)
+        up = np.clip(np.rint(cbb[::2, ::2] + rng.normal(0, 1.5, (h // 2, w // 2))), 0, 255).astype(np.uint8)
+        vp = np.clip(np.rint(crb[::2, ::2] + rng.normal(0, 1.5, (h // 2, w // 2))), 0, 255).astype(np.uint8)
+        frames.append([yp, up, vp])
+    return frames
+
+
+@pytest.mark.parametrize("w,h,n,d", [(256, 192, 10, 2), (224, 160, 6, 1)])
+def test_nl4d_auto_noise_map_with_colour_gains_matches_oracle(oracle, w, h, n, d):
+    """The default NL4D call on 4:2:0 frames (automatic sigma, noise map on): the luma pass scales
+    its threshold by the noise curve and the colour grain gains; identical samples."""
+    fmt = avd.SampleFormat.u8()
+    frames = colour_clip(w, h, n, seed=w + n)
+    o = avd.Nl4dOptions(sigma=None, temporal_radius=d, spatial_radius=4,
+                        motion=avd.MotionSearch(estimation=avd.MotionEstimation.DIRECT))
+    spec = avd.EngineSpec.nl4d(o, None, avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    noise, per_pass = colour_noise(oracle, frames, fmt, d, True)
+    check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, 0.0, spatial_radius=4, noise=noise)
+    for g, src in zip(got, frames):
+        assert np.array_equal(g[1], src[1]) and np.array_equal(g[2], src[2])
+    # The gains moved off 1 somewhere once the window held enough blocks.
+    assert any(np.abs(p[4][0]).max() > 0.01 for p in per_pass)
