@@ -754,7 +754,8 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     completes the region d slots behind it; at the end, tail passes centred on d+1..2d (or, for a
     stream shorter than the ring, on every real frame after padding with the last frame). The
     first `context` frames are priming pushes (no head passes). With `noise`, a function of a pass's
-    centre stream frame returning (sigma, weight_scale, sad_floor), optionally followed by curve and
+    centre stream frame returning (sigma or per-channel sigmas, weight_scale, sad_floor), optionally
+    followed by curve and
     colour, each pass reads those (the automatic estimate's fold around that frame) instead of the
     pinned sigma's; `curve` is the 16 luma noise-curve ratios, or None while the fold's curve flag
     is clear, and `colour` the (gain tables, centre block means, 8-bit scale) of collab_fused. With `share_writes`
@@ -820,7 +821,8 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
                                   confidence=conf.reshape(-1), neighbour_slots=np.array(slots, np.uint32),
                                   c_min=c_min, refine=refine, spatial_radius=spatial_radius, k_max=8,
-                                  sigma=(p_sigma,) * c, weight_scale_override=p_weight, lambda_ht=lambda_ht,
+                                  sigma=tuple(p_sigma) if isinstance(p_sigma, (tuple, list)) else (p_sigma,) * c,
+                                  weight_scale_override=p_weight, lambda_ht=lambda_ht,
                                   kaiser_beta=kaiser_beta, noise_curve=p_curve, colour=p_colour,
                                   pooled=pool_ratio, blksize=blksize, blk_step=step, blocks_x=bx, blocks_y=by,
                                   mv_stride=bx * by * 2, conf_stride=bx * by)

@@ -119,20 +119,18 @@ def test_nl4d_continuation_skips_head_passes(oracle):
     check(oracle, [[g[0]] for g in got], [[f[0]] for f in frames], fmt, d, sigma, context=2, spatial_radius=3)
 
 
-def test_nl4d_options_this_build_rejects():
+def test_nl4d_default_options_build_on_every_layout():
+    """The reference's default NL4D call (automatic sigma, noise map on) builds on gray frames and on
+    frames with chroma, luma and chroma passes alike, as does search escalation."""
     fmt = avd.SampleFormat.u8()
-    g = avd.Geometry(64, 48, avd.ChromaLayout.GRAY, fmt, fmt)
-    # The automatic estimate with the luma noise map is built for gray frames
-    # (tests/test_gpu_nl4d_auto.py); frames with chroma also need the colour grain gains.
-    avd.build_engine(avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=1), None, g)).close()
+    for layout in (avd.ChromaLayout.GRAY, avd.ChromaLayout.YUV420, avd.ChromaLayout.YUV444):
+        g = avd.Geometry(64, 48, layout, fmt, fmt)
+        chroma = None if layout == avd.ChromaLayout.GRAY else avd.Nl4dOptions(temporal_radius=1)
+        avd.build_engine(avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=1), chroma, g)).close()
     g420 = avd.Geometry(64, 48, avd.ChromaLayout.YUV420, fmt, fmt)
-    with pytest.raises(avd.InvalidOptions, match="colour grain gains"):
-        avd.build_engine(avd.EngineSpec.nl4d(avd.Nl4dOptions(temporal_radius=1), None, g420))
-    with pytest.raises(avd.InvalidOptions, match="colour grain gains"):
-        avd.build_engine(avd.EngineSpec.nl4d(None, avd.Nl4dOptions(temporal_radius=1, noise_map=False), g420))
-    # Search escalation is built (test_nl4d_escalating_motion_matches_oracle).
+    avd.build_engine(avd.EngineSpec.nl4d(None, avd.Nl4dOptions(temporal_radius=1), g420)).close()
     escalating = avd.Nl4dOptions(sigma=0.03, temporal_radius=1, motion=avd.MotionSearch(max_search_escalation=8))
-    avd.build_engine(avd.EngineSpec.nl4d(escalating, None, g)).close()
+    avd.build_engine(avd.EngineSpec.nl4d(escalating, None, g420)).close()
 
 
 @pytest.mark.parametrize("n,d,estimation,refine_radius,context", [

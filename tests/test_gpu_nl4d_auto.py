@@ -114,13 +114,6 @@ def test_nl4d_auto_noise_map_matches_oracle(oracle, w, h, n, d, estimation):
     assert all(c[12] > 1.3 * c[2] for c in curves)
 
 
-def test_nl4d_noise_map_on_frames_with_chroma_needs_the_colour_gains():
-    fmt = avd.SampleFormat.u8()
-    o = avd.Nl4dOptions(sigma=None, temporal_radius=1)
-    with pytest.raises(avd.InvalidOptions, match="colour grain gains"):
-        avd.build_engine(avd.EngineSpec.nl4d(o, None, avd.Geometry(64, 48, avd.ChromaLayout.YUV420, fmt, fmt)))
-
-
 def pack_plane(codes):
     """A u8 plane as the engine's word-packed layout."""
     flat = np.asarray(codes, np.uint8).reshape(-1)
@@ -163,13 +156,15 @@ def colour_noise(oracle, clip_frames, fmt, d, luma, *, blksize=16, overlap=8, se
         state, derived = folds[centre][0], folds[centre][1]
         _, gains, _ = oracle.colour_fit(window, c, luma, state[16:32], bool(derived[3]))
         curve = state[16:32].copy() if derived[3] != 0 else None
-        out.append((float(derived[0]), float(derived[2]), float(derived[4]), curve, (gains, grid[centre], 255.0)))
+        sigma = float(derived[0]) if c == 1 else (float(derived[0]), float(derived[1]))
+        out.append((sigma, float(derived[2]), float(derived[4]), curve, (gains, grid[centre], 255.0)))
     return (lambda frame: out[frame]), out
 
 
 def colour_clip(w, h, n, seed):
     """A 4:2:0 u8 clip panning 2 pixels a frame over coloured bands whose luma grain grows with
-    warmth (Cr above Cb) and brightness, so the colour gains move away from 1."""
+    warmth (Cr above Cb) and brightness, Cb grain with Cb and Cr grain as Cr falls, so the colour
+    gains move away from 1."""
     rng = np.random.default_rng(seed)
     y, x = np.mgrid[0:h, 0:w + 4 * n].astype(np.float32)
     luma = 40 + 170 * x / (w + 4 * n)
@@ -182,8 +177,11 @@ def colour_clip(w, h, n, seed):
         warm = np.clip((crb - cbb) / 40.0, 0, None)
         grain = (2.0 + lb / 80.0) * (1.0 + warm)
         yp = np.clip(np.rint(lb + rng.normal(0, 1, lb.shape) * grain), 0, 255).astype(np.uint8)
-        up = np.clip(np.rint(cbb[::2, ::2] + rng.normal(0, 1.5, (h // 2, w // 2))), 0, 255).astype(np.uint8)
-        vp = np.clip(np.rint(crb[::2, ::2] + rng.normal(0, 1.5, (h // 2, w // 2))), 0, 255).astype(np.uint8)
+        cb2, cr2 = cbb[::2, ::2], crb[::2, ::2]
+        ugrain = 1.0 + 2.5 * np.clip((cb2 - 128) / 45.0, 0, None)
+        vgrain = 1.0 + 2.5 * np.clip((128 - cr2) / 45.0, 0, None)
+        up = np.clip(np.rint(cb2 + rng.normal(0, 1, cb2.shape) * ugrain), 0, 255).astype(np.uint8)
+        vp = np.clip(np.rint(cr2 + rng.normal(0, 1, cr2.shape) * vgrain), 0, 255).astype(np.uint8)
         frames.append([yp, up, vp])
     return frames
 
@@ -203,4 +201,29 @@ def test_nl4d_auto_noise_map_with_colour_gains_matches_oracle(oracle, w, h, n, d
     for g, src in zip(got, frames):
         assert np.array_equal(g[1], src[1]) and np.array_equal(g[2], src[2])
     # The gains moved off 1 somewhere once the window held enough blocks.
+    assert any(np.abs(p[4][0]).max() > 0.01 for p in per_pass)
+
+
+@pytest.mark.parametrize("d", [1, 2])
+def test_nl4d_chroma_auto_sigma_with_colour_gains_matches_oracle(oracle, d):
+    """A chroma-only engine with the automatic estimate: the luma guide measures its own noise for
+    its motion search, and the chroma pass measures both chroma channels, pools them into colour
+    cells on the chroma grid and scales each channel's threshold by its gain; identical samples."""
+    w, h, n = 192, 128, 8
+    fmt = avd.SampleFormat.u8()
+    frames = colour_clip(w, h, n, seed=77 + d)
+    o = avd.Nl4dOptions(sigma=None, temporal_radius=d, spatial_radius=4,
+                        motion=avd.MotionSearch(estimation=avd.MotionEstimation.DIRECT))
+    spec = avd.EngineSpec.nl4d(None, o, avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt))
+    got = Runner(spec).run(frames)
+    for g, f in zip(got, frames):
+        assert np.array_equal(g[0], f[0])
+    share = oracle.MotionShare((w // 8, h // 8, 8, 16), (w // 16, h // 16, 8, 16), 1, 1)
+    guide_noise, _, _ = auto_noise(oracle, [[f[0]] for f in frames], fmt, d)
+    f32 = [oracle.ingest([f[0]], fmt.kind, fmt.max_value(), 0.0) for f in frames]
+    oracle.nl4d_stream(f32, d, 0.0, spatial_radius=4, share_writes=share, noise=guide_noise)
+    noise, per_pass = colour_noise(oracle, frames, fmt, d, False)
+    check(oracle, [[g[1], g[2]] for g in got], [[f[1], f[2]] for f in frames], fmt, d, 0.0, chroma=True,
+          spatial_radius=4, share_reads=share, noise=noise)
+    assert all(p[0][0] > 0 and p[0][1] > 0 for p in per_pass)
     assert any(np.abs(p[4][0]).max() > 0.01 for p in per_pass)
