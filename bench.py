@@ -448,21 +448,18 @@ def run_gpu(args) -> None:
 def nl4d_4k_section(avd, torch, np, synth, pushes: int) -> dict:
     """The NL4D half of the metric on its 4K workload: 3840x2160 4:2:0 10-bit, 7-frame window (d=3,
     Auto resolves to Chained), spatial radius 16, hard threshold 2.7 (lambda_ht 2.7, scale 1, plain
-    threshold), 12 sprites at up to 8 px/frame, noise 20 codes + 0.02 * value variance; luma sigma
-    from the automatic noise estimate (motion-compensated look-ahead), chroma pinned at 20 codes, as a
-    luma engine and a chroma engine side by side. Frames resident in HBM; device time per push with
-    CUDA events, steady state after the window and look-ahead fill."""
+    threshold), 12 sprites at up to 8 px/frame, noise 20 codes + 0.02 * value variance; sigma from
+    the automatic noise estimate (motion-compensated look-ahead) on both plane groups, the luma noise
+    map and the colour grain gains on (the reference's defaults), luma and chroma in one engine.
+    Frames resident in HBM; device time per push with CUDA events, steady state after the window and
+    look-ahead fill."""
     w, h, depth, d = 3840, 2160, 10, 3
     fmt = avd.SampleFormat.u16(depth)
-    sigma = 20.0 / 1023.0
 
-    def options(sig):
-        return avd.Nl4dOptions(sigma=sig, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
-                               pooled_threshold=False, noise_map=False)
-
+    o = avd.Nl4dOptions(sigma=None, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
+                        pooled_threshold=False)
     geo = avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt)
-    engines = [avd.build_engine(avd.EngineSpec.nl4d(options(None), None, geo)),
-               avd.build_engine(avd.EngineSpec.nl4d(None, options(sigma), geo))]
+    engines = [avd.build_engine(avd.EngineSpec.nl4d(o, o, geo))]
     stream = torch.cuda.Stream()
     for eng in engines:
         eng.set_stream(stream.cuda_stream)
@@ -496,7 +493,7 @@ def nl4d_4k_section(avd, torch, np, synth, pushes: int) -> dict:
     steady = times[2 * d + 1 + 8:]
     ms = float(np.median(steady))
     return {"workload": "NL4D 3840x2160 4:2:0 10-bit luma+chroma, d=3 (Chained), spatial_radius 16, lambda_ht 2.7, "
-                        "plain threshold; luma sigma automatic, chroma sigma pinned at 20 codes",
+                        "plain threshold; sigma automatic on both plane groups, noise map and colour gains on",
             "frames_per_s": round(1000.0 / ms, 2), "ms_per_frame": round(ms, 3), "pushes_timed": len(steady)}
 
 
@@ -905,12 +902,10 @@ def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
     10-bit codes, 12 sprites at integer velocities up to 8 px/frame, Gaussian noise of 20 codes plus
     signal-dependent variance 0.02 * value. Eight generated frames are cycled.
 
-    Default: luma and chroma in one engine with sigma pinned at 20 codes. With `auto`, luma takes its
-    sigma from the automatic noise estimate (motion-compensated look-ahead, noise map off) and chroma
-    keeps the pinned sigma (its colour gains are not built); the two plane groups' window spans then
-    differ, which one engine rejects, so a luma engine and a chroma engine run side by side, as a
-    caller of the reference must. Prints the device time of every push and the steady-state median
-    as one JSON line."""
+    Default: luma and chroma in one engine with sigma pinned at 20 codes. With `auto`, both plane
+    groups take their sigma from the automatic noise estimate (motion-compensated look-ahead) with the
+    luma noise map and the colour grain gains on, the reference's defaults. Prints the device time of
+    every push and the steady-state median as one JSON line."""
     import numpy as np
     import torch
 
@@ -925,14 +920,11 @@ def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
 
     def options(sig):
         return avd.Nl4dOptions(sigma=sig, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
-                               pooled_threshold=False, noise_map=False)
+                               pooled_threshold=False, noise_map=sig is None)
 
     geo = avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt)
-    if auto:
-        engines = [avd.build_engine(avd.EngineSpec.nl4d(options(None), None, geo)),
-                   avd.build_engine(avd.EngineSpec.nl4d(None, options(sigma), geo))]
-    else:
-        engines = [avd.build_engine(avd.EngineSpec.nl4d(options(sigma), options(sigma), geo))]
+    o = options(None if auto else sigma)
+    engines = [avd.build_engine(avd.EngineSpec.nl4d(o, o, geo))]
     stream = torch.cuda.current_stream()
     for eng in engines:
         eng.set_stream(stream.cuda_stream)
@@ -967,7 +959,7 @@ def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
     warm = 2 * d + 1 + (8 if auto else 0)
     steady = times[warm:]
     ms = float(np.median(steady))
-    what = ("luma sigma from the automatic noise estimate, chroma sigma pinned at 20 codes (two engines)" if auto
+    what = ("sigma from the automatic noise estimate on both plane groups, noise map and colour gains on" if auto
             else "sigma pinned at 20 codes")
     print(json.dumps({"workload": "NL4D 3840x2160 4:2:0 10-bit luma+chroma, d=3 (Chained), spatial_radius 16, "
                                   "lambda_ht 2.7, plain threshold, " + what,
@@ -1152,7 +1144,7 @@ def main() -> None:
     ap.add_argument("--nl4d-4k", type=int, default=0, metavar="PUSHES",
                     help="time PUSHES pushes of the 4K 4:2:0 10-bit NL4D workload (d=3) and exit")
     ap.add_argument("--auto-sigma", action="store_true",
-                    help="with --nl4d-4k: luma sigma from the automatic noise estimate")
+                    help="with --nl4d-4k: sigma from the automatic noise estimate on both plane groups")
     ap.add_argument("--adjoint", type=int, default=0, metavar="REPS",
                     help="time the NLMeans adjoint against its forward REPS times and exit")
     ap.add_argument("--batch", type=int, default=0, metavar="REPS",
