@@ -1,13 +1,13 @@
 """The host denoiser (av-denoise/src/host/mod.rs:111-420) on the GPU: frames pushed as wire bytes
-come back identical to the same clip pushed through the device engine (the engine's outputs are
-themselves checked against the oracle in the NLMeans and NL4D tests), and the queue, plane-check,
-poison and reset rules behave as the reference's host tests expect (host/tests)."""
+come back identical to the same clip pushed through the device engine, and meet the NLMeans parity
+bar against the oracle directly; the queue, plane-check, poison and reset rules behave as the
+reference's host tests expect (host/tests)."""
 
 import numpy as np
 import pytest
 
 from conftest import avd
-from gpu_util import Runner
+from gpu_util import Parity, Runner, oracle_pass
 
 pytestmark = pytest.mark.gpu
 
@@ -86,6 +86,29 @@ def test_host_nlm_matches_engine(w, h, depth, chroma):
         assert den.plane_lengths == [len(b) for b in wire(frames[0], fmt)]
         got = run_host(den, frames, fmt, dims)
     assert_same(got, want)
+
+
+@pytest.mark.parametrize("w,h,depth", [(96, 64, 8), (67, 45, 10)])
+def test_host_nlm_matches_oracle(oracle, w, h, depth):
+    """Wire bytes in, wire bytes out, against the oracle on the same clip: every sample of both
+    plane groups identical (raw), none off by more than 1 LSB."""
+    fmt = avd.SampleFormat.u8() if depth == 8 else avd.SampleFormat.u16(depth)
+    frames = clip(w, h, 7, depth=depth, chroma="420", seed=w + depth)
+    spec = nlm_spec(w, h, chroma=avd.ChromaLayout.YUV420, fmt=fmt)
+    g = spec.geometry
+    dims = [g.plane_dims(i) for i in range(g.plane_count())]
+    with avd.HostDenoiser(spec) as den:
+        got = run_host(den, frames, fmt, dims)
+    want_y = oracle_pass(oracle, [[f[0]] for f in frames], fmt, 2, 3, 2, 8.0)
+    want_uv = oracle_pass(oracle, [[f[1], f[2]] for f in frames], fmt, 2, 3, 2, 8.0, chroma=True)
+    assert len(got) == len(want_y) == len(frames)
+    par = Parity()
+    for k in range(len(frames)):
+        par.add(got[k][0], want_y[k][0], None, fmt.max_value())
+        for c in range(2):
+            par.add(got[k][1 + c], want_uv[k][c], None, fmt.max_value())
+    st = par.stats()
+    assert st["max_lsb"] <= 1 and st["identical"] >= 0.999, st
 
 
 def test_host_nl4d_priming_matches_engine():
