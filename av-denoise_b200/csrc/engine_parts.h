@@ -227,8 +227,14 @@ class NoiseFront {
     std::optional<Failure> read_against(size_t frame, std::optional<size_t> prev, int direction, cudaStream_t s);
     NoiseFrontConfig cfg_;
     cudaStream_t side_ = nullptr;
-    cudaEvent_t ingested_ = nullptr, read_done_ = nullptr;
-    bool reads_queued_ = false;
+    cudaEvent_t ingested_ = nullptr, read_done_ = nullptr, snapshot_ = nullptr;
+    // One event per history slot, recorded after the reads of the frame in it, so a fold waits only
+    // for the frames of its window and the newest reads overlap the passes.
+    std::vector<cudaEvent_t> frame_read_;
+    bool reads_queued_ = false, snapshot_pending_ = false;
+    // The derived words the look-ahead's searches read: a copy taken as each push's reads start, so
+    // they read the previous push's fold whatever the pass's fold on the main stream writes meanwhile.
+    DeviceBuffer search_words_;
     size_t capacity_ = 0, pushed_ = 0, released_ = 0, recorded_ = 0;
     int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2, conf_stride_ = 1;
     DeviceBuffer lookahead_, partials_, records_, scratch_, history_records_, history_results_, settings_, state_,

@@ -86,42 +86,60 @@ __device__ __forceinline__ uint32_t block_key(const float* partials, int i, int 
     return __float_as_uint(sigma);
 }
 
-// The element of rank `rank` (0-based) among the blocks' keys, by an exact radix select.
-__device__ uint32_t select_rank(const float* partials, int blocks, int c, int cubes_x, int width, int height, float scale,
-                                uint32_t rank, uint32_t* hist, uint32_t* shared_state) {
-    uint32_t prefix = 0, mask = 0;
+// The elements of ranks rank[0] and rank[1] (0-based) among the blocks' keys, by one exact radix
+// select of two queries: 8-bit digits from the top, one histogram per query, lanes of a warp that
+// add to the same histogram word adding once by their count, one warp scanning each histogram.
+__device__ void select_two(const float* partials, int blocks, int c, int cubes_x, int width, int height, float scale,
+                           uint32_t* rank, uint32_t (*hist)[256], uint32_t* prefix) {
+    const int t = threadIdx.x, warp = t / 32, lane = t % 32;
+    if (t < 2) prefix[t] = 0;
+    uint32_t mask = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+        for (int b = t; b < 512; b += blockDim.x) (&hist[0][0])[b] = 0;
         __syncthreads();
-        for (int i = threadIdx.x; i < blocks; i += blockDim.x) {
-            const uint32_t key = block_key(partials, i, c, cubes_x, width, height, scale);
-            if (key != 0xFFFFFFFFu && (key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 0xFFu], 1u);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t below = 0, b = 0;
-            for (; b < 255; ++b) {
-                if (below + hist[b] > rank) break;
-                below += hist[b];
+        for (int base = 0; base < blocks; base += blockDim.x) {
+            const int i = base + t;
+            const uint32_t key = i < blocks ? block_key(partials, i, c, cubes_x, width, height, scale) : 0xFFFFFFFFu;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const bool hit = key != 0xFFFFFFFFu && (key & mask) == prefix[q];
+                const uint32_t word = hit ? static_cast<uint32_t>(q) * 256u + ((key >> shift) & 0xFFu) : 0xFFFFFFFFu;
+                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, word);
+                if (hit && lane == __ffs(peers) - 1) atomicAdd(&hist[0][0] + word, static_cast<uint32_t>(__popc(peers)));
             }
-            shared_state[0] = prefix | (b << shift);
-            shared_state[1] = rank - below;
         }
         __syncthreads();
-        prefix = shared_state[0];
-        rank = shared_state[1];
+        if (warp < 2) {
+            const uint32_t* h = hist[warp];
+            uint32_t mine = 0;
+            for (int b = 0; b < 8; ++b) mine += h[lane * 8 + b];
+            uint32_t incl = mine;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const uint32_t below = incl - mine, r = rank[warp];
+            if (r >= below && r < incl) {
+                uint32_t seen = below, b = 0;
+                for (; b < 8; ++b) {
+                    if (r < seen + h[lane * 8 + b]) break;
+                    seen += h[lane * 8 + b];
+                }
+                prefix[warp] |= static_cast<uint32_t>(lane * 8 + b) << shift;
+                rank[warp] = r - seen;
+            }
+        }
         mask |= 0xFFu << shift;
         __syncthreads();
     }
-    return prefix;
 }
 
 __global__ void __launch_bounds__(kSelectThreads) immerkaer_quartile_kernel(const float* __restrict__ partials,
                                                                          int cubes_x, int cubes_y, int width,
                                                                          int height, int channels, float scale,
                                                                          float* __restrict__ sigma_low) {
-    __shared__ uint32_t hist[256];
-    __shared__ uint32_t state[2];
+    __shared__ uint32_t hist[2][256];
+    __shared__ uint32_t prefix[2], rank[2];
     __shared__ uint32_t count_s;
     const int c = blockIdx.x;
     const int blocks = cubes_x * cubes_y;
@@ -134,18 +152,22 @@ __global__ void __launch_bounds__(kSelectThreads) immerkaer_quartile_kernel(cons
     uint32_t mine = 0;
     for (int i = threadIdx.x; i < blocks; i += blockDim.x)
         mine += block_key(partials, i, c, cubes_x, width, height, scale) != 0xFFFFFFFFu ? 1u : 0u;
-    atomicAdd(&count_s, mine);
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xFFFFFFFFu, mine, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&count_s, mine);
     __syncthreads();
     const uint32_t n = count_s;
     if (n == 0) {
         if (threadIdx.x == 0) sigma_low[c] = 0.0f;
         return;
     }
-    const float low = __uint_as_float(
-        select_rank(partials, blocks, c, cubes_x, width, height, scale, (n - 1) / 4, hist, state));
-    const float high = __uint_as_float(
-        select_rank(partials, blocks, c, cubes_x, width, height, scale, (n + 2) / 4, hist, state));
     if (threadIdx.x == 0) {
+        rank[0] = (n - 1) / 4;
+        rank[1] = (n + 2) / 4;
+    }
+    __syncthreads();
+    select_two(partials, blocks, c, cubes_x, width, height, scale, rank, hist, prefix);
+    if (threadIdx.x == 0) {
+        const float low = __uint_as_float(prefix[0]), high = __uint_as_float(prefix[1]);
         const float fraction = __fmul_rn(static_cast<float>((n - 1) % 4), 0.25f);
         sigma_low[c] = __fadd_rn(low, __fmul_rn(fraction, __fsub_rn(high, low)));
     }

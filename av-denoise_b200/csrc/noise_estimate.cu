@@ -336,23 +336,32 @@ __device__ __forceinline__ uint32_t set_key(const BlockScratch& s, int kind, int
 }
 
 // Exact order statistics by four 8-bit radix passes: query q asks for the element of rank
-// sh.rank[q] among the elements that `element(i, key, first, last)` assigns to it (element i joins
-// queries first..last-1 with `key`, or none when it returns false). One histogram per query, one
-// warp scanning each query's histogram; sh.result[q] receives the key.
+// sh.rank[q] among the elements that `element(i, key, first)` assigns to it (element i joins queries
+// first..first+span-1 with `key`, or none when it returns false). One histogram per query, one warp
+// scanning each query's histogram; sh.result[q] receives the key. Lanes of a warp that add to the
+// same histogram word add once, by their count: the keys of one set share their top bits, so plain
+// shared atomics would serialise on a few words.
 template <typename Element>
-__device__ void radix_select(int n, int nq, ReadingShared& sh, Element element) {
+__device__ void radix_select(int n, int nq, int span, ReadingShared& sh, Element element) {
     const int t = threadIdx.x;
     if (t < nq) sh.prefix[t] = 0;
     uint32_t mask = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int i = t; i < nq * 256; i += blockDim.x) (&sh.hist[0][0])[i] = 0;
         __syncthreads();
-        for (int i = t; i < n; i += blockDim.x) {
-            uint32_t key;
-            int first, last;
-            if (!element(i, key, first, last)) continue;
-            for (int q = first; q < last; ++q)
-                if ((key & mask) == sh.prefix[q]) atomicAdd(&sh.hist[q][(key >> shift) & 0xFFu], 1u);
+        for (int base = 0; base < n; base += blockDim.x) {
+            const int i = base + t;
+            uint32_t key = 0;
+            int first = 0;
+            const bool in = i < n && element(i, key, first);
+            for (int k = 0; k < span; ++k) {
+                const int q = first + k;
+                const bool hit = in && (key & mask) == sh.prefix[q];
+                const uint32_t word = hit ? static_cast<uint32_t>(q) * 256u + ((key >> shift) & 0xFFu) : 0xFFFFFFFFu;
+                const uint32_t peers = __match_any_sync(0xFFFFFFFFu, word);
+                if (hit && (t & 31) == __ffs(peers) - 1)
+                    atomicAdd(&sh.hist[0][0] + word, static_cast<uint32_t>(__popc(peers)));
+            }
         }
         __syncthreads();
         const int warp = t / 32, lane = t % 32;
@@ -387,10 +396,9 @@ __device__ void radix_select(int n, int nq, ReadingShared& sh, Element element) 
 __device__ void select_ranks(const BlockScratch& s, int kind, int c, int n, const uint32_t* ranks, int nq,
                              ReadingShared& sh) {
     if (static_cast<int>(threadIdx.x) < nq) sh.rank[threadIdx.x] = ranks[threadIdx.x];
-    radix_select(n, nq, sh, [&](int i, uint32_t& key, int& first, int& last) {
+    radix_select(n, nq, nq, sh, [&](int i, uint32_t& key, int& first) {
         key = set_key(s, kind, c, i);
         first = 0;
-        last = nq;
         return key != kExcluded;
     });
 }
@@ -610,13 +618,12 @@ __global__ void __launch_bounds__(kReadingThreads) noise_reading_kernel(const fl
             const uint32_t n = sh.bin_n[t / 2];
             sh.rank[t] = n == 0 ? 0 : ((t % 2) ? n / 2 : (n - 1) / 2);
         }
-        radix_select(nq, kBinQueries, sh, [&](int i, uint32_t& key, int& first, int& last) {
+        radix_select(nq, kBinQueries, 2, sh, [&](int i, uint32_t& key, int& first) {
             const uint32_t tag = s.quarter_tag[i];
             const uint32_t bin = tag & 0xFFu;
             if (!(tag & kQuarterMember) || bin >= static_cast<uint32_t>(kCurveBins)) return false;
             key = order_key(s.quarter_sigma[i]);
             first = static_cast<int>(2 * bin);
-            last = first + 2;
             return true;
         });
         for (int b = 0; b < kCurveBins; ++b)

@@ -34,6 +34,8 @@ NoiseFront::~NoiseFront() {
     if (side_) cudaStreamSynchronize(side_);
     if (ingested_) cudaEventDestroy(ingested_);
     if (read_done_) cudaEventDestroy(read_done_);
+    if (snapshot_) cudaEventDestroy(snapshot_);
+    for (cudaEvent_t ev : frame_read_) cudaEventDestroy(ev);
     if (side_) cudaStreamDestroy(side_);
 }
 
@@ -74,6 +76,14 @@ std::optional<Failure> NoiseFront::allocate(const NoiseFrontConfig& cfg) {
     if ((e = cudaEventCreateWithFlags(&ingested_, cudaEventDisableTiming)) != cudaSuccess) return fail("noise event", e);
     if ((e = cudaEventCreateWithFlags(&read_done_, cudaEventDisableTiming)) != cudaSuccess)
         return fail("noise event", e);
+    if ((e = cudaEventCreateWithFlags(&snapshot_, cudaEventDisableTiming)) != cudaSuccess)
+        return fail("noise event", e);
+    frame_read_.assign(capacity_, nullptr);
+    for (cudaEvent_t& ev : frame_read_)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail("noise event", e);
+    if ((e = search_words_.alloc(16 * sizeof(float))) != cudaSuccess) return fail("look-ahead noise words", e);
+    if ((e = cudaMemset(search_words_.ptr, 0, search_words_.bytes)) != cudaSuccess)
+        return fail("look-ahead noise words", e);
     float words[16];
     noise_fold_words(cfg.width, cfg.height, cfg.coefficients, words);
     if ((e = cudaMemcpy(settings_.ptr, words, sizeof(words), cudaMemcpyHostToDevice)) != cudaSuccess)
@@ -119,7 +129,7 @@ std::optional<Failure> NoiseFront::search(size_t centre_frame, size_t neighbour_
     m.inline_slots[0] = static_cast<uint32_t>(neighbour_frame % kFrames);
     m.mv_field = pair_.as<int32_t>() + direction * mv_stride_;
     m.confidence = nullptr;
-    m.noise = derived_.as<float>();
+    m.noise = search_words_.as<float>();
     m.width = static_cast<int>(cfg_.width);
     m.height = static_cast<int>(cfg_.height);
     m.frame_count = static_cast<int>(kFrames);
@@ -213,7 +223,12 @@ std::optional<Failure> NoiseFront::before_ingest(cudaStream_t main) {
 std::optional<Failure> NoiseFront::read_pushed(cudaStream_t main) {
     cudaError_t ev = cudaEventRecord(ingested_, main);
     if (ev == cudaSuccess) ev = cudaStreamWaitEvent(side_, ingested_, 0);
+    // The searches read the derived words of the folds queued before this push.
+    if (ev == cudaSuccess)
+        ev = cudaMemcpyAsync(search_words_.ptr, derived_.ptr, search_words_.bytes, cudaMemcpyDeviceToDevice, side_);
+    if (ev == cudaSuccess) ev = cudaEventRecord(snapshot_, side_);
     if (ev != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise read order", ev)};
+    snapshot_pending_ = true;
     const cudaStream_t s = side_;
     const size_t frame = pushed_;
     const int w = static_cast<int>(cfg_.width), h = static_cast<int>(cfg_.height);
@@ -238,7 +253,9 @@ std::optional<Failure> NoiseFront::read_pushed(cudaStream_t main) {
     if (auto f = read_against(frame, prev, kNewerToOlder, s)) return f;
     if (cfg_.motion && frame == 1)
         if (auto f = read_against(0, std::optional<size_t>(1), kOlderToNewer, s)) return f;
-    if ((e = cudaEventRecord(read_done_, s)) != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise read", e)};
+    if ((e = cudaEventRecord(read_done_, s)) != cudaSuccess ||
+        (e = cudaEventRecord(frame_read_[frame % capacity_], s)) != cudaSuccess)
+        return Failure{AVD_ERR_GPU, cuda_message("noise read", e)};
     reads_queued_ = true;
     pushed_ += 1;
     recorded_ = std::max(recorded_, frame + 1);
@@ -247,11 +264,19 @@ std::optional<Failure> NoiseFront::read_pushed(cudaStream_t main) {
 
 // nlmeans/denoiser/noise.rs:171-185 (`update_noise_estimate`).
 std::optional<Failure> NoiseFront::fold(uint32_t centre, cudaStream_t s) {
-    if (auto f = before_ingest(s)) return f;  // every recorded frame's reading has landed
     const int64_t newest = static_cast<int64_t>(recorded_) - 1;
     const int first = static_cast<int>(std::max<int64_t>(static_cast<int64_t>(centre) - kNoiseWindowRadius, 0));
     const int last = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(centre) + kNoiseWindowRadius, newest));
-    cudaError_t e = launch_noise_fold(history_records_.as<float>(), history_results_.as<float>(),
+    // The window's readings (the reads of its newest frame and every earlier one: the reads run in
+    // order on the side stream, and a window reaching frame 1 includes frame 0 read again) have
+    // landed, and the newest reads' searches have taken their copy of the derived words this fold
+    // overwrites. Frames newer than the window keep reading meanwhile: their history slots lie
+    // outside it, as the history holds 17 + d slots.
+    cudaError_t e = cudaSuccess;
+    if (snapshot_pending_) e = cudaStreamWaitEvent(s, snapshot_, 0);
+    if (e == cudaSuccess && last >= 0) e = cudaStreamWaitEvent(s, frame_read_[last % capacity_], 0);
+    if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("noise fold wait", e)};
+    e = launch_noise_fold(history_records_.as<float>(), history_results_.as<float>(),
                                       static_cast<int>(capacity_), first, last, settings_.as<float>(),
                                       static_cast<int>(cfg_.channels), static_cast<int>(cfg_.table_radius),
                                       state_.as<float>(), derived_.as<float>(), spatial_.as<float>(),
