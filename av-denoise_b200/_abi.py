@@ -134,7 +134,7 @@ class AvdEngineSpec(C.Structure):
 
 
 class AvdTuning(C.Structure):
-    _fields_ = [("deterministic", u32), ("reserved", u32)]
+    _fields_ = [("deterministic", u32), ("mode", u32), ("store", C.c_char_p)]
 
 
 class AvdWindowSpan(C.Structure):
@@ -260,6 +260,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_noise_compensated_stats": (C.c_int, [u64, u64, u32, u32, u32, u64, u32, u32, u32, u32, u64, C.c_void_p]),
     "avd_noise_reading": (C.c_int, [u64, u32, u32, u32, u32, u64, u64, C.c_void_p]),
     "avd_colour_records": (u64, [u32, u32]),
+    "avd_tune_variant_for_test": (C.c_int, [u32, C.c_char_p, C.c_char_p, u32, C.POINTER(C.c_float)]),
+    "avd_tune_forget": (None, []),
     "avd_colour_means": (C.c_int, [u64, u64, u64, C.POINTER(AvdGeometry), u64, u64, C.c_void_p]),
     "avd_colour_accumulate": (C.c_int, [u64, u64, u32, u32, u32, u32, C.c_float, u64, C.c_void_p]),
     "avd_colour_window": (C.c_int, [u64, u32, u32, u32, u32, u64, C.c_void_p]),

@@ -630,19 +630,44 @@ class Engine:
         self.close()
 
 
+TUNING_MODES = {"auto": 0, "cached": 1, "off": 2}
+
+
+def default_tuning_store() -> str:
+    """The library's cache directory for tuning results: $XDG_CACHE_HOME/av-denoise-b200, else
+    ~/.cache/av-denoise-b200 (created on first use)."""
+    import os
+
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    path = os.path.join(base, "av-denoise-b200")
+    os.makedirs(path, exist_ok=True)
+    return path
+
+
 @dataclass
 class TuningConfig:
-    """tune/config.rs:66-75 (`TuningConfig`). `deterministic`: every NLMeans sample in the exact
-    order of the reference's baseline, bit-identical to the CPU restatement on float outputs too
-    (slower); integer outputs match it either way."""
+    """tune/config.rs:8-75 (`TuningMode`, `TuningConfig`). `deterministic`: every NLMeans sample
+    in the exact order of the reference's baseline, bit-identical to the CPU restatement on float
+    outputs too (slower); integer outputs match it either way. `mode` ("auto", "cached" or "off")
+    picks each launch site's variant per frame shape: auto times the variants once per shape and
+    keeps the fastest. `store`: the directory results are kept in across processes (see
+    `default_tuning_store`), or None for this process only."""
 
     deterministic: bool = False
+    mode: str = "auto"
+    store: Optional[str] = None
+
+    def _c(self) -> _abi.AvdTuning:
+        if self.mode not in TUNING_MODES:
+            raise InvalidOptions(f"unknown tuning mode '{self.mode}', expected auto, cached or off")
+        return _abi.AvdTuning(int(self.deterministic), TUNING_MODES[self.mode],
+                              self.store.encode() if self.store else None)
 
 
 def build_engine(spec: EngineSpec, tuning: Optional[TuningConfig] = None) -> Engine:
     """tune/setup.rs:79-91 (`build_engine`): validates, then builds on the current CUDA device."""
     lib = _abi.load()
-    t = _abi.AvdTuning(int((tuning or TuningConfig()).deterministic), 0)
+    t = (tuning or TuningConfig())._c()
     h = C.c_void_p()
     st = lib.avd_engine_create(C.byref(spec._c()), C.byref(t), C.byref(h))
     if st:
@@ -682,7 +707,7 @@ class HostDenoiser:
 
     def __init__(self, spec: EngineSpec, tuning: Optional[TuningConfig] = None):
         self._lib = _abi.load()
-        t = _abi.AvdTuning(int((tuning or TuningConfig()).deterministic), 0)
+        t = (tuning or TuningConfig())._c()
         h = C.c_void_p()
         st = self._lib.avd_host_create(C.byref(spec._c()), C.byref(t), C.byref(h))
         if st:

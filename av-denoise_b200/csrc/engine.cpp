@@ -19,6 +19,7 @@
 
 #include "avd_internal.h"
 #include "engine_parts.h"
+#include "tune.h"
 #include "kernels.h"
 
 namespace avd {
@@ -36,10 +37,11 @@ class NlmPass final : public Pass {
     static std::optional<Failure> create(const AvdNlmeansAlgorithm& alg, Channels channels, uint32_t width,
                                          uint32_t height, const AvdSampleFormat& in, const AvdSampleFormat& out,
                                          std::unique_ptr<Pass>* result, bool guides_only = false,
-                                         bool exact_all = false) {
+                                         bool exact_all = false, const TuneOptions& tune = TuneOptions{}) {
         auto pass = std::unique_ptr<NlmPass>(new NlmPass());
         pass->guides_ = guides_only;
         pass->exact_all_ = exact_all;
+        pass->tune_ = tune;
         pass->params_ = resolve_nlm_params(alg, channels);
         pass->held_ = nlm_held_frames(alg, channels);
         pass->width_ = width;
@@ -901,6 +903,8 @@ class NlmPass final : public Pass {
             *out_slot = slot;
             return std::nullopt;
         }
+        if (window_variant_ < 0) window_variant_ = tune_window(a);
+        a.variant = window_variant_;
         if (fix_.ptr) {
             // Integer outputs: the window kernel flags the pixels within the band of a change of code
             // and the exact finish recomputes them in the reference kernels' order.
@@ -919,6 +923,37 @@ class NlmPass final : public Pass {
         }
         *out_slot = slot;
         return std::nullopt;
+    }
+
+    // tune/driver: the window kernel's variant for this pass's shape, each timed once on this very
+    // launch (without the exact-finish list) when the tuner has no choice for the shape yet.
+    int tune_window(const NlmLaunch& a) {
+        char key[160];
+        std::snprintf(key, sizeof(key), "nlm_window c%d s%d a%d d%d fast%d conf%d lut%d %dx%d", a.channels,
+                      a.patch_radius, a.search_radius, a.pairs, a.fast, a.conf ? 1 : 0, a.spatial_lut ? 1 : 0,
+                      a.width, a.height);
+        const int variants = a.ref_ring ? 1 : nlm_window_variants(a.channels, a.patch_radius, a.fast != 0);
+        return tuned_variant(tune_, key, variants, [&](int v) {
+            NlmLaunch t = a;
+            t.variant = v;
+            t.fix_list = nullptr;
+            t.fix_count = nullptr;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            float ms = -1.0f;
+            if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess &&
+                launch_nlm(t, stream) == cudaSuccess && cudaEventRecord(e0, stream) == cudaSuccess) {
+                bool ok = true;
+                for (int rep = 0; rep < 3 && ok; ++rep) ok = launch_nlm(t, stream) == cudaSuccess;
+                if (ok && cudaEventRecord(e1, stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+                    cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+                    ms /= 3.0f;
+                else
+                    ms = -1.0f;
+            }
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            return ms;
+        });
     }
 
     // nlmeans/denoiser/mod.rs:557-573 (`flush_step_gpu`) without look-ahead.
@@ -978,6 +1013,8 @@ class NlmPass final : public Pass {
     DeviceBuffer lut_, pilot_lut_;
     DeviceBuffer fix_;  // integer outputs: [count, pixel list] of the exact finish
     bool exact_all_ = false;
+    TuneOptions tune_;
+    int window_variant_ = -1;  // the tuned window kernel variant, chosen at the first window launch
     DeviceBuffer ref_;  // the prefilter's reference ring, slot for slot beside `ring_`
     std::vector<uint32_t> slot_frames_;
     size_t ring_head_ = 0, frames_loaded_ = 0, real_pushes_ = 0;
@@ -1160,6 +1197,12 @@ extern "C" {
 AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, AvdEngine** out) {
     if (!spec || !out) return AVD_ERR_NULL_ARG;
     const bool exact_all = tuning != nullptr && tuning->deterministic != 0;
+    avd::TuneOptions tune;
+    if (tuning) {
+        if (tuning->mode > AVD_TUNING_OFF) return fail_global(AVD_ERR_INVALID_OPTIONS, "unknown tuning mode");
+        tune.mode = static_cast<avd::TuneMode>(tuning->mode);
+        if (tuning->store) tune.store = tuning->store;
+    }
     *out = nullptr;
     g_last_error.clear();
     std::string message;
@@ -1177,7 +1220,7 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
         auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_luma, avd::Channels::Luma, g.width, g.height, g.input,
                                               g.output, colour_frames, &engine->luma)
                       : avd::NlmPass::create(spec->nlm_luma, avd::Channels::Luma, g.width, g.height, g.input,
-                                             g.output, &engine->luma, false, exact_all);
+                                             g.output, &engine->luma, false, exact_all, tune);
         if (f) return fail_global(f->status, f->message);
     }
     if (spec->has_chroma) {
@@ -1186,7 +1229,7 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
         auto f = nl4d ? avd::create_nl4d_pass(spec->nl4d_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
                                               colour_frames, &engine->chroma)
                       : avd::NlmPass::create(spec->nlm_chroma, avd::Channels::Chroma, cw, ch, g.input, g.output,
-                                             &engine->chroma, false, exact_all);
+                                             &engine->chroma, false, exact_all, tune);
         if (f) return fail_global(f->status, f->message);
     }
     if (!engine->luma && engine->chroma) {

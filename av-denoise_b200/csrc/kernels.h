@@ -57,9 +57,14 @@ struct NlmLaunch {
     int* fix_list;
     int* fix_count;
     float code_max, fix_band;
+    // The window kernel's launch variant (0: the baseline), one of nlm_window_variants(): the same
+    // code built for a different number of resident CTAs per SM, so a variant trades registers for
+    // occupancy and changes how many waves a frame's tiles take, never the results.
+    int variant;
 };
 
 cudaError_t launch_nlm(const NlmLaunch& args, cudaStream_t stream);
+int nlm_window_variants(int channels, int patch_radius, bool fast);
 
 // The exact finish (nlm_exact.cu): every pixel of `args.fix_list[0 .. *args.fix_count)` (every pixel
 // of the frame when `fix_list` is null) recomputed in the order and rounding of the FP32 mirror of

@@ -48,6 +48,32 @@ __global__ void __launch_bounds__(kThreads, C == 1 && FAST ? 5 : 4) nlm_window_k
     nlm_tile<C, S, FAST>(a, blockIdx.x, blockIdx.y);
 }
 
+// The tuner's variants of the window kernel (patch radius up to kVariantMaxS): the same tile built
+// for MINB resident CTAs per SM. The baseline's MINB is 5 for luma without offsets and 4 otherwise;
+// variant 1 holds one CTA fewer (more registers), variant 2 one more.
+constexpr int kVariantMaxS = 4;
+template <int C, bool FAST>
+constexpr int baseline_minb() {
+    return C == 1 && FAST ? 5 : 4;
+}
+template <int C, int S, bool FAST, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) nlm_window_variant_kernel(NlmLaunch a) {
+    nlm_tile<C, S, FAST>(a, blockIdx.x, blockIdx.y);
+}
+
+template <int C, int S, bool FAST, int MINB>
+cudaError_t launch_variant(const NlmLaunch& a, dim3 grid, size_t smem, cudaStream_t stream) {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(nlm_window_variant_kernel<C, S, FAST, MINB>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    nlm_window_variant_kernel<C, S, FAST, MINB><<<grid, kThreads, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
 // Persistent batch: every CTA takes tiles from one counter until the batch's tiles run out. Tile t
 // belongs to the job j with prefix[j] <= t < prefix[j + 1]; jobs are whole launch descriptions.
 template <int C, int S, bool FAST>
@@ -87,6 +113,11 @@ cudaError_t launch_csf(const NlmLaunch& a, cudaStream_t stream) {
     if (attr_err != cudaSuccess) return attr_err;
     dim3 grid((a.width + kTX - 1) / kTX, (a.height + K::TY - 1) / K::TY);
     size_t smem = nlm_smem_bytes<C, S>(a.search_radius, a.pairs, false);
+    if constexpr (S <= kVariantMaxS) {
+        constexpr int base = baseline_minb<C, FAST>();
+        if (a.variant == 1) return launch_variant<C, S, FAST, base - 1>(a, grid, smem, stream);
+        if (a.variant == 2) return launch_variant<C, S, FAST, base + 1>(a, grid, smem, stream);
+    }
     nlm_window_kernel<C, S, FAST><<<grid, kThreads, smem, stream>>>(a);
     return cudaGetLastError();
 }
@@ -145,6 +176,10 @@ int nlm_tile_rows(int /*channels*/, int patch_radius) {
 }
 
 int nlm_tile_cols() { return kTX; }
+
+int nlm_window_variants(int /*channels*/, int patch_radius, bool /*fast*/) {
+    return patch_radius <= kVariantMaxS ? 3 : 1;
+}
 
 cudaError_t launch_nlm_batch(const NlmLaunch* jobs, const int* prefix, int njobs, int* counter, int channels,
                              int patch_radius, bool fast, int max_search_radius, int max_pairs, cudaStream_t stream) {

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define AVD_ABI_VERSION 3u
+#define AVD_ABI_VERSION 4u
 
 #if defined(__GNUC__)
 #define AVD_API __attribute__((visibility("default")))
@@ -226,16 +226,32 @@ typedef struct AvdEngineSpec {
     AvdGeometry geometry;
 } AvdEngineSpec;
 
-/* av-denoise-core/src/tune/config.rs:66-75 (`TuningConfig`). `deterministic` ("picks only
- * bit-identical candidates and the baseline profile"): every NLMeans sample is computed by the exact
- * kernel in the operation order of the reference's baseline (direct row-major patch sums), so float
- * outputs too are bit-identical to the CPU restatement; slower. Off (the default), integer outputs
- * still match it: the fast window kernel flags the samples near a change of code and the exact
- * kernel recomputes only those. The NLM pilot prefilter's reference always runs exactly. */
+/* av-denoise-core/src/tune/config.rs:8-75 (`TuningMode`, `TuningConfig`). `deterministic` ("picks
+ * only bit-identical candidates and the baseline profile"): every NLMeans sample is computed by the
+ * exact kernel in the operation order of the reference's baseline (direct row-major patch sums), so
+ * float outputs too are bit-identical to the CPU restatement; slower. Off (the default), integer
+ * outputs still match it: the fast window kernel flags the samples near a change of code and the
+ * exact kernel recomputes only those. The NLM pilot prefilter's reference always runs exactly.
+ *
+ * `mode` picks each launch site's variant (same results, different launch shapes) per frame shape:
+ * AUTO (the default) uses the remembered or stored choice and times every variant once on the
+ * site's first launch for a shape without one; CACHED uses stored choices only, else the baseline;
+ * OFF runs every baseline. `store` is the directory of the results file
+ * (`av-denoise-b200-tune.jsonl`, one JSON object per device and shape); null keeps results for
+ * this process only. A null AvdTuning means all defaults. */
+typedef enum AvdTuningMode { AVD_TUNING_AUTO = 0, AVD_TUNING_CACHED = 1, AVD_TUNING_OFF = 2 } AvdTuningMode;
 typedef struct AvdTuning {
     uint32_t deterministic;
-    uint32_t reserved;
+    uint32_t mode;     /* AvdTuningMode */
+    const char* store; /* directory of the per-shape results, or null */
 } AvdTuning;
+
+/* The tuner's choice for one launch-site key among `variants` under AvdTuning's `mode` and `store`,
+ * with variant v timed as `times_ms[v]` instead of a launch (tune/store.rs, driver/mod.rs): the
+ * store's tests drive it without a GPU. avd_tune_forget drops the results this process remembers. */
+AVD_API int avd_tune_variant_for_test(uint32_t mode, const char* store, const char* key, uint32_t variants,
+                                      const float* times_ms);
+AVD_API void avd_tune_forget(void);
 
 /* av-denoise-core/src/engine/mod.rs:40-62 (`WindowSpan`, `EdgePadding`). */
 typedef struct AvdWindowSpan {
