@@ -1,7 +1,8 @@
 // CPU ORACLE - test infrastructure only (see nlm_oracle.cpp for the rules it follows).
 //
-// A C++17 restatement of av-denoise's block-matching motion search without the camera-model
-// candidate, and of the truemotion stage that can end it:
+// A C++17 restatement of av-denoise's block-matching motion search with its camera-model candidate
+// (a second window around each neighbour's prediction, motion/kernels/candidates.rs), and of the
+// truemotion stage that can end it:
 //   pyramid: av-denoise-core/src/motion/kernels/pyramid.rs:10-61 (lane-0 extract, 2x2 average,
 //            odd edge repeated) and motion/pyramid.rs:82-107 (levels built one after another);
 //   coarse:  motion/kernels/block_match.rs:117-215 and motion/analyse.rs:100-150 (the smallest
@@ -68,11 +69,15 @@ struct Level {
 struct Best {
     int dx, dy;
     float sad;
+    float mean;      // the window's mean SAD (block_match.rs:744-751)
+    float edge_bar;  // the lowest SAD off the outer ring when the winner sits on it, else 0
+    int centre_dx, centre_dy;
 };
 
-// block_match.rs:674-760 for one centre; `sads_out`, when given, receives every candidate's SAD.
-Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy, int cdx, int cdy, int R,
-                   std::vector<float>* sads_out = nullptr) {
+// block_match.rs:674-760 and 787-849 for one centre: every candidate's SAD summed row-major, the
+// lowest SAD with the first row-major index, the centre winning a tie, SADs at or above 1e30 never
+// chosen; the mean sums every SAD in row-major order.
+Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy, int cdx, int cdy, int R) {
     const int b = L.blksize, side = 2 * R + 1;
     const float* cf = L.base + centre_slot * L.slot;
     const float* nf = L.base + nbr_slot * L.slot;
@@ -93,7 +98,7 @@ Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy
                 }
             sads[dy * side + dx] = sad;
         }
-    Best best{cdx, cdy, 1.0e30f};
+    Best best{cdx, cdy, 1.0e30f, 0.0f, 0.0f, cdx, cdy};
     for (int i = 0; i < side * side; ++i)
         if (sads[i] < best.sad) {
             best.sad = sads[i];
@@ -101,10 +106,72 @@ Best search_window(const Level& L, int centre_slot, int nbr_slot, int ox, int oy
             best.dy = cdy + i / side - R;
         }
     const float centre_sad = sads[R * side + R];
-    if (centre_sad <= best.sad) best = Best{cdx, cdy, centre_sad};
-    if (sads_out) *sads_out = sads;
+    if (centre_sad <= best.sad) {
+        best.sad = centre_sad;
+        best.dx = cdx;
+        best.dy = cdy;
+    }
+    float total = 0.0f;
+    for (int i = 0; i < side * side; ++i) total += sads[i];
+    best.mean = total * (1.0f / static_cast<float>(side * side));
+    if (std::abs(best.dx - cdx) == R || std::abs(best.dy - cdy) == R) {
+        float bar = 1.0e30f;
+        for (int y = 1; y < side - 1; ++y)
+            for (int x = 1; x < side - 1; ++x) bar = std::min(bar, sads[y * side + x]);
+        best.edge_bar = bar;
+    }
     return best;
 }
+
+// candidates.rs:71-121 (`model_displacement`): the motion neighbour n's camera model predicts at a
+// block's centre on a level `scale` times smaller, capped to the level and rounded half up.
+void model_displacement(const float* predictions, int n, int ox, int oy, int blksize, int scale, int lw, int lh,
+                        int* dx, int* dy) {
+    const float* p = predictions + n * 6;
+    const float s = static_cast<float>(scale);
+    const int half = blksize / 2;
+    const float cx = static_cast<float>(ox + half) * s, cy = static_cast<float>(oy + half) * s;
+    const float mx = p[0] * cx + p[1] * cy + p[4];
+    const float my = p[2] * cx + p[3] * cy + p[5];
+    float ldx = (mx - cx) / s, ldy = (my - cy) / s;
+    const float limx = static_cast<float>(lw), limy = static_cast<float>(lh);
+    ldx = ldx < -limx ? -limx : (ldx > limx ? limx : ldx);
+    ldy = ldy < -limy ? -limy : (ldy > limy ? limy : ldy);
+    const float rx = std::floor(ldx + 0.5f), ry = std::floor(ldy + 0.5f);
+    *dx = std::isnan(rx) ? 0 : static_cast<int>(rx);
+    *dy = std::isnan(ry) ? 0 : static_cast<int>(ry);
+}
+
+// candidates.rs:123-134 (`predicts_motion`).
+bool predicts_motion(const float* predictions, int n) {
+    const float* p = predictions + n * 6;
+    return p[0] != 1.0f || p[3] != 1.0f || p[1] != 0.0f || p[2] != 0.0f || p[4] != 0.0f || p[5] != 0.0f;
+}
+
+// block_match.rs:213-265 and 384-470 with candidates.rs:136-166: the window around `seed`, then,
+// when the model moves anything and its point lies outside that window, the window around the
+// model's point, which wins only when its SAD plus `bias` is below the incumbent's.
+Best search_with_model(const Level& L, int cs, int ns, int ox, int oy, int sdx, int sdy, int R,
+                       const float* predictions, int n, int scale, float bias) {
+    Best best = search_window(L, cs, ns, ox, oy, sdx, sdy, R);
+    if (!predictions) return best;
+    int mdx, mdy;
+    model_displacement(predictions, n, ox, oy, L.blksize, scale, L.width, L.height, &mdx, &mdy);
+    const bool outside = std::abs(mdx - sdx) > R || std::abs(mdy - sdy) > R;
+    if (!(predicts_motion(predictions, n) && outside)) return best;
+    const Best ch = search_window(L, cs, ns, ox, oy, mdx, mdy, R);
+    if (ch.sad + bias < best.sad) best = ch;
+    return best;
+}
+
+// analyse.rs:150-157 (`coarse_floor_scale`).
+float coarse_floor_scale(int coarse_blksize, int blksize, int scale) {
+    const float coarse_area = static_cast<float>(coarse_blksize * coarse_blksize);
+    const float fine_area = static_cast<float>(blksize * blksize);
+    return coarse_area / fine_area / static_cast<float>(scale);
+}
+
+constexpr float kModelCandidateBias = 0.125f;  // candidates.rs:6-11
 
 float match_confidence(float sad, float floor, float thsad) {
     float excess = sad - floor;
@@ -196,6 +263,14 @@ struct OrcMotionArgs {
     // search again `ceiling` either side of their first window's centre; `esc_reads_floor` takes the
     // floor from the noise word when it is positive; `widen_coarse` searches the coarse level again.
     uint32_t ceiling, esc_reads_floor, widen_coarse;
+    // motion/analyse.rs:41-60: with `predictions` (6 words per neighbour) every block also searches
+    // around its neighbour's camera-model prediction; with `sad_out` the fine pass writes each
+    // block's winning SAD, then `neighbours * conf_stride` values on, its window's mean SAD.
+    const float* predictions;
+    float* sad_out;
+    // motion/context.rs:30-45: the coarse pass's radius and how many times wider its blocks are than
+    // the content a fine block covers.
+    uint32_t coarse_radius, coarse_block_factor;
 };
 
 int64_t orc_motion_pyramid_floats(int w, int h, int frames, int levels) { return level_base(w, h, frames, levels); }
@@ -227,30 +302,43 @@ void orc_motion_search(const OrcMotionArgs* a) {
     const int bx_n = (w + step - 1) / step > 1 ? (w + step - 1) / step : 1;
     const int by_n = (h + step - 1) / step > 1 ? (h + step - 1) / step : 1;
     const int R = static_cast<int>(a->search_radius);
+    const int Rc = static_cast<int>(a->coarse_radius);
+    const int factor = a->coarse_block_factor > 0 ? static_cast<int>(a->coarse_block_factor) : 1;
     const bool coarse = a->levels > 1 && !a->seeded;
     const bool seeded = coarse || a->seeded;
+    const float* noise_floor = a->noise ? a->noise + a->sad_floor_word : nullptr;
+    const float model_floor = a->predictions && noise_floor ? *noise_floor : 0.0f;
+    // analyse.rs:118-148 (`coarse_level`): the smallest level, its blocks `factor` times the content a
+    // fine block covers there.
+    Level Lc{};
+    int scale = 1;
+    float floor_scale = 1.0f;
+    if (a->levels > 1) {
+        const int level = static_cast<int>(a->levels) - 1;
+        scale = 1 << level;
+        level_dims(w, h, level, &Lc.width, &Lc.height);
+        Lc.base = a->pyramid + level_base(w, h, frames, level);
+        Lc.slot = slot_pixels(w, h, level);
+        Lc.blksize = (static_cast<int>(a->blksize) / scale > 2 ? static_cast<int>(a->blksize) / scale : 2) * factor;
+        Lc.step = step / scale > 1 ? step / scale : 1;
+        Lc.blocks_x = (Lc.width + Lc.step - 1) / Lc.step > 1 ? (Lc.width + Lc.step - 1) / Lc.step : 1;
+        Lc.blocks_y = (Lc.height + Lc.step - 1) / Lc.step > 1 ? (Lc.height + Lc.step - 1) / Lc.step : 1;
+        floor_scale = coarse_floor_scale(Lc.blksize, static_cast<int>(a->blksize), scale);
+    }
     if (coarse) {
-        const int level = static_cast<int>(a->levels) - 1, scale = 1 << level;
-        Level L{};
-        level_dims(w, h, level, &L.width, &L.height);
-        L.base = a->pyramid + level_base(w, h, frames, level);
-        L.slot = slot_pixels(w, h, level);
-        L.blksize = static_cast<int>(a->blksize) / scale > 2 ? static_cast<int>(a->blksize) / scale : 2;
-        L.step = step / scale > 1 ? step / scale : 1;
-        L.blocks_x = (L.width + L.step - 1) / L.step > 1 ? (L.width + L.step - 1) / L.step : 1;
-        L.blocks_y = (L.height + L.step - 1) / L.step > 1 ? (L.height + L.step - 1) / L.step : 1;
-        const int s = L.step * scale;
+        const int s = Lc.step * scale;
+        const float bias = kModelCandidateBias * model_floor * floor_scale;
 #pragma omp parallel for collapse(2) schedule(dynamic)
         for (int n = 0; n < static_cast<int>(a->neighbours); ++n)
-            for (int by = 0; by < L.blocks_y; ++by)
-                for (int bx = 0; bx < L.blocks_x; ++bx) {
-                    const Best b = search_window(L, static_cast<int>(a->centre_slot),
-                                                 static_cast<int>(a->neighbour_slots[n]), bx * L.step, by * L.step, 0,
-                                                 0, R);
+            for (int by = 0; by < Lc.blocks_y; ++by)
+                for (int bx = 0; bx < Lc.blocks_x; ++bx) {
+                    const Best b = search_with_model(Lc, static_cast<int>(a->centre_slot),
+                                                     static_cast<int>(a->neighbour_slots[n]), bx * Lc.step,
+                                                     by * Lc.step, 0, 0, Rc, a->predictions, n, scale, bias);
                     const int c0 = std::min(bx * s / step, bx_n);
-                    const int c1 = bx == L.blocks_x - 1 ? bx_n : std::min((bx + 1) * s / step, bx_n);
+                    const int c1 = bx == Lc.blocks_x - 1 ? bx_n : std::min((bx + 1) * s / step, bx_n);
                     const int r0 = std::min(by * s / step, by_n);
-                    const int r1 = by == L.blocks_y - 1 ? by_n : std::min((by + 1) * s / step, by_n);
+                    const int r1 = by == Lc.blocks_y - 1 ? by_n : std::min((by + 1) * s / step, by_n);
                     int32_t* mv = a->mv_field + static_cast<int64_t>(n) * a->mv_stride;
                     for (int r = r0; r < r1; ++r)
                         for (int c = c0; c < c1; ++c) {
@@ -265,7 +353,8 @@ void orc_motion_search(const OrcMotionArgs* a) {
     const int neighbours = static_cast<int>(a->neighbours), blocks = bx_n * by_n;
     const int C = static_cast<int>(a->ceiling);
     const bool escalates = C > R;
-    // escalate.rs:60-67: the kept SAD, the edge bar, and the first window's centre of every block.
+    const int64_t means_base = static_cast<int64_t>(neighbours) * a->conf_stride;
+    // escalate.rs:60-67: the kept SAD, the edge bar, and the winning window's centre of every block.
     std::vector<float> kept, edge;
     std::vector<int> centre_x, centre_y;
     if (escalates) {
@@ -274,42 +363,31 @@ void orc_motion_search(const OrcMotionArgs* a) {
         centre_x.assign(kept.size(), 0);
         centre_y.assign(kept.size(), 0);
     }
+    const float fine_bias = kModelCandidateBias * model_floor;
 #pragma omp parallel for collapse(2) schedule(dynamic)
     for (int n = 0; n < neighbours; ++n)
         for (int by = 0; by < by_n; ++by)
             for (int bx = 0; bx < bx_n; ++bx) {
                 int32_t* mv = a->mv_field + static_cast<int64_t>(n) * a->mv_stride + (by * bx_n + bx) * 2;
                 const int sdx = seeded ? mv[0] : 0, sdy = seeded ? mv[1] : 0;
-                std::vector<float> sads;
-                const Best b = search_window(L, static_cast<int>(a->centre_slot), static_cast<int>(a->neighbour_slots[n]),
-                                             bx * step, by * step, sdx, sdy, R, escalates ? &sads : nullptr);
+                const Best b = search_with_model(L, static_cast<int>(a->centre_slot),
+                                                 static_cast<int>(a->neighbour_slots[n]), bx * step, by * step, sdx,
+                                                 sdy, R, a->predictions, n, 1, fine_bias);
+                const int64_t slot = static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx;
                 if (escalates) {
-                    // block_match.rs:783-796: a winner on the window's outer ring records the lowest
-                    // SAD off that ring as its edge bar, else 0.
                     const size_t i = static_cast<size_t>(n) * blocks + by * bx_n + bx;
                     kept[i] = b.sad;
-                    centre_x[i] = sdx;
-                    centre_y[i] = sdy;
-                    float bar = 0.0f;
-                    if (std::abs(b.dx - sdx) == R || std::abs(b.dy - sdy) == R) {
-                        const int side = 2 * R + 1;
-                        bar = 1.0e30f;
-                        for (int y = 1; y < side - 1; ++y)
-                            for (int x = 1; x < side - 1; ++x) bar = std::min(bar, sads[y * side + x]);
-                    }
-                    edge[i] = bar;
+                    centre_x[i] = b.centre_dx;
+                    centre_y[i] = b.centre_dy;
+                    edge[i] = b.edge_bar;
                 }
                 mv[0] = b.dx;
                 mv[1] = b.dy;
-                if (a->confidence) {
-                    const float floor = a->noise[a->sad_floor_word];
-                    float excess = b.sad - floor;
-                    if (excess < 0.0f) excess = 0.0f;
-                    const float t2 = a->thsad * a->thsad, e2 = excess * excess;
-                    float c = (t2 - e2) / (t2 + e2);
-                    if (c < 0.0f) c = 0.0f;
-                    a->confidence[static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx] = c;
+                if (a->sad_out) {
+                    a->sad_out[slot] = b.sad;
+                    a->sad_out[means_base + slot] = b.mean;
                 }
+                if (a->confidence) a->confidence[slot] = match_confidence(b.sad, a->noise[a->sad_floor_word], a->thsad);
             }
     if (!escalates) return;
     // escalate.rs:168-257: the floor the flags and margins score against.
@@ -337,20 +415,12 @@ void orc_motion_search(const OrcMotionArgs* a) {
                 const bool on_edge = kept[i] + margin < edge[i];
                 failed[i] = low || on_edge || closest > kNeighbourDisagreement;
             }
-    // escalate.rs:400-559 (`mc_escalate_search`).
-    // escalate.rs:203-205 (`reaches_further`): only a ceiling past the coarse pass's radius (the
-    // search radius here) searches the coarse level again.
-    const bool widen = a->widen_coarse && a->levels > 1 && !a->seeded && a->ceiling > a->search_radius;
-    Level Lc{};
-    int scale = 1;
-    if (widen) {
-        const int level = static_cast<int>(a->levels) - 1;
-        scale = 1 << level;
-        level_dims(w, h, level, &Lc.width, &Lc.height);
-        Lc.base = a->pyramid + level_base(w, h, frames, level);
-        Lc.slot = slot_pixels(w, h, level);
-        Lc.blksize = static_cast<int>(a->blksize) / scale > 2 ? static_cast<int>(a->blksize) / scale : 2;
-    }
+    // escalate.rs:400-559 (`mc_escalate_search`). escalate.rs:203-205 (`reaches_further`): only a
+    // ceiling past the coarse pass's radius searches the coarse level again, around no motion and the
+    // camera model's prediction, the model's window winning by more than 1/8 of the floor scaled to
+    // the coarse block.
+    const bool widen = a->widen_coarse && a->levels > 1 && !a->seeded && C > Rc;
+    const float coarse_bias = kModelCandidateBias * floor * floor_scale;
 #pragma omp parallel for collapse(2) schedule(dynamic)
     for (int n = 0; n < neighbours; ++n)
         for (int by = 0; by < by_n; ++by)
@@ -360,7 +430,8 @@ void orc_motion_search(const OrcMotionArgs* a) {
                 const int cs = static_cast<int>(a->centre_slot), ns = static_cast<int>(a->neighbour_slots[n]);
                 Best best = search_window(L, cs, ns, bx * step, by * step, centre_x[i], centre_y[i], C);
                 if (widen) {
-                    const Best cb = search_window(Lc, cs, ns, bx * step / scale, by * step / scale, 0, 0, C);
+                    const Best cb = search_with_model(Lc, cs, ns, bx * step / scale, by * step / scale, 0, 0, C,
+                                                      a->predictions, n, scale, coarse_bias);
                     const int cx = cb.dx * scale, cy = cb.dy * scale;
                     if (cx != centre_x[i] || cy != centre_y[i]) {
                         const Best ch = search_window(L, cs, ns, bx * step, by * step, cx, cy, C);
@@ -368,20 +439,20 @@ void orc_motion_search(const OrcMotionArgs* a) {
                     }
                 }
                 if (best.sad + margin < kept[i]) {
+                    const int64_t slot = static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx;
                     int32_t* mv = a->mv_field + static_cast<int64_t>(n) * a->mv_stride + (by * bx_n + bx) * 2;
                     mv[0] = best.dx;
                     mv[1] = best.dy;
-                    if (a->confidence)
-                        a->confidence[static_cast<int64_t>(n) * a->conf_stride + by * bx_n + bx] =
-                            match_confidence(best.sad, a->noise[a->sad_floor_word], a->thsad);
+                    if (a->sad_out) a->sad_out[slot] = best.sad;
+                    if (a->confidence) a->confidence[slot] = match_confidence(best.sad, a->noise[a->sad_floor_word], a->thsad);
                 }
             }
 }
 
 // One truemotion pass (motion/truemotion/kernels/truemotion/mod.rs:560-763, `mc_truemotion` with
 // the serial scoring of score.rs:7-61) over level 0 of `pyramid`: every block of every neighbour
-// picks its vector from `mv_in` (and `seeds`, when given) into `mv_out`, with its confidence when
-// `confidence` is given. No camera model (no prediction candidate).
+// picks its vector from `mv_in` (and `seeds` and the camera model's prediction, when given) into
+// `mv_out`, with its confidence when `confidence` is given.
 struct OrcTruemotionArgs {
     const float* pyramid;
     const uint32_t* neighbour_slots;
@@ -398,6 +469,10 @@ struct OrcTruemotionArgs {
     // vector and keeps its confidence; `changes_out` flags each block whose pick left its own vector.
     const uint32_t* changes_in;
     uint32_t* changes_out;
+    // mod.rs:878-900: with `predictions`, the camera model's prediction is a candidate; with
+    // `sad_out`, every rescored block writes its winning SAD there (conf layout).
+    const float* predictions;
+    float* sad_out;
 };
 
 namespace {
@@ -487,7 +562,7 @@ void orc_truemotion_pass(const OrcTruemotionArgs* a) {
                 std::sort(ys.begin(), ys.end());
                 median = Vec2{xs[(xs.size() - 1) / 2], ys[(ys.size() - 1) / 2]};
             }
-            // candidates.rs:178-306 (`gather_candidates`), without the model's prediction.
+            // candidates.rs:178-306 (`gather_candidates`).
             std::vector<Vec2> list;
             push_unique(list, own);
             push_unique(list, median);
@@ -496,6 +571,11 @@ void orc_truemotion_pass(const OrcTruemotionArgs* a) {
                 if (on_grid(col + side_dx[sd], row + side_dy[sd], bx_n, by_n))
                     push_unique(list, field(a->mv_in, col + side_dx[sd], row + side_dy[sd]));
             push_unique(list, Vec2{0, 0});
+            if (a->predictions && predicts_motion(a->predictions, n)) {
+                Vec2 m;
+                model_displacement(a->predictions, n, ox, oy, b, 1, w, h, &m.dx, &m.dy);
+                push_unique(list, m);
+            }
             if (a->seeds) {
                 push_unique(list, field(a->seeds, col, row));
                 for (int corner = 0; corner < 4; ++corner) {
@@ -594,6 +674,7 @@ void orc_truemotion_pass(const OrcTruemotionArgs* a) {
             if (a->confidence)
                 a->confidence[static_cast<int64_t>(n) * a->conf_stride + blk] =
                     pass_confidence(best_sad, a->noise[a->sad_field], a->thsad);
+            if (a->sad_out) a->sad_out[static_cast<int64_t>(n) * a->conf_stride + blk] = best_sad;
             if (a->changes_out)
                 a->changes_out[static_cast<int64_t>(n) * a->conf_stride + blk] =
                     (best.dx == own.dx && best.dy == own.dy) ? 0u : 1u;

@@ -498,7 +498,8 @@ class MotionArgs(C.Structure):
                                    "overlap", "search_radius", "levels", "mv_stride", "conf_stride",
                                    "sad_floor_word")] + [("thsad", C.c_float), ("seeded", C.c_uint32),
                                                          ("keep_seeds", C.POINTER(C.c_int32))] + \
-        [(n, C.c_uint32) for n in ("ceiling", "esc_reads_floor", "widen_coarse")]
+        [(n, C.c_uint32) for n in ("ceiling", "esc_reads_floor", "widen_coarse")] + \
+        [("predictions", _fp), ("sad_out", _fp), ("coarse_radius", C.c_uint32), ("coarse_block_factor", C.c_uint32)]
 
 
 class TruemotionArgs(C.Structure):
@@ -509,7 +510,8 @@ class TruemotionArgs(C.Structure):
                                    "overlap", "mv_stride", "conf_stride", "sad_field", "reads_floor",
                                    "refine_radius")] + [(n, C.c_float) for n in ("lambda_base", "lambda_noise",
                                                                                  "surcharge", "fade_level", "thsad")] + \
-        [("changes_in", C.POINTER(C.c_uint32)), ("changes_out", C.POINTER(C.c_uint32))]
+        [("changes_in", C.POINTER(C.c_uint32)), ("changes_out", C.POINTER(C.c_uint32)),
+         ("predictions", _fp), ("sad_out", _fp)]
 
 
 # motion/truemotion/params.rs:4-33 and motion/confidence.rs:10.
@@ -528,10 +530,13 @@ def truemotion_values(field_lambda: float, blksize: int, thsad_value: float) -> 
 
 def truemotion_pass(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
                     mv_in: np.ndarray, seeds: np.ndarray | None, *, blksize=16, overlap=8, field_lambda=1.0,
-                    thsad=0.0, sad_floor=0.0, reads_floor=True, confidence=False, passes=1):
-    """The truemotion stage (no camera model): returns (mv (n, blocks, 2), conf (n, blocks)). With
-    `passes` 2 (a search that escalates, truemotion/params.rs:9-12, 79-90) the second pass reads the
-    first's field and rescores only the blocks next to one it changed (truemotion/stage.rs:82-142)."""
+                    thsad=0.0, sad_floor=0.0, reads_floor=True, confidence=False, passes=1, predictions=None,
+                    sad_out: np.ndarray | None = None):
+    """The truemotion stage: returns (mv (n, blocks, 2), conf (n, blocks)). With `passes` 2 (a search
+    that escalates, truemotion/params.rs:9-12, 79-90) the second pass reads the first's field and
+    rescores only the blocks next to one it changed (truemotion/stage.rs:82-142). With `predictions`
+    (6 words per neighbour) the camera model's prediction is a candidate; with `sad_out` (f32, one per
+    block per neighbour) every rescored block writes its winning SAD there."""
     mv = mv_in
     conf = None
     changes = None
@@ -540,14 +545,15 @@ def truemotion_pass(pyramid: np.ndarray, width: int, height: int, frames: int, c
         mv, c = _truemotion_once(pyramid, width, height, frames, centre_slot, neighbour_slots, mv, seeds,
                                  blksize=blksize, overlap=overlap, field_lambda=field_lambda, thsad=thsad,
                                  sad_floor=sad_floor, reads_floor=reads_floor, confidence=confidence,
-                                 changes_in=changes, changes_out=out_changes, conf_in=conf)
+                                 changes_in=changes, changes_out=out_changes, conf_in=conf, predictions=predictions,
+                                 sad_out=sad_out)
         conf, changes = c, out_changes
     return mv, conf
 
 
 def _truemotion_once(pyramid, width, height, frames, centre_slot, neighbour_slots, mv_in, seeds, *, blksize,
                      overlap, field_lambda, thsad, sad_floor, reads_floor, confidence, changes_in=None,
-                     changes_out=None, conf_in=None):
+                     changes_out=None, conf_in=None, predictions=None, sad_out=None):
     step = blksize - overlap
     bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
     slots = np.ascontiguousarray(neighbour_slots, np.uint32)
@@ -571,6 +577,9 @@ def _truemotion_once(pyramid, width, height, frames, centre_slot, neighbour_slot
     a.lambda_base, a.lambda_noise, a.surcharge, a.fade_level, a.thsad = lb, ln, TRUEMOTION["surcharge"], fade, thsad
     a.changes_in = changes_in.ctypes.data_as(C.POINTER(C.c_uint32)) if changes_in is not None else None
     a.changes_out = changes_out.ctypes.data_as(C.POINTER(C.c_uint32)) if changes_out is not None else None
+    pred = np.ascontiguousarray(predictions, np.float32).reshape(-1) if predictions is not None else None
+    a.predictions = _f(pred) if pred is not None else None
+    a.sad_out = _f(sad_out) if sad_out is not None else None
     l = lib()
     l.orc_truemotion_pass.argtypes = [C.POINTER(TruemotionArgs)]
     l.orc_truemotion_pass(C.byref(a))
@@ -594,8 +603,15 @@ def motion_pyramid(ring: np.ndarray, channels: int, width: int, height: int, lev
 def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, centre_slot: int, neighbour_slots,
                   *, blksize=16, overlap=8, search_radius=4, levels=2, confidence=False, sad_floor=0.0,
                   thsad=0.0, seeds: np.ndarray | None = None, field_lambda: float = 0.0, reads_floor: bool = True,
-                  ceiling: int = 0, esc_reads_floor: bool = False):
-    """One block-matching search (no camera model). Returns (mv (n, blocks, 2), conf).
+                  ceiling: int = 0, esc_reads_floor: bool = False, predictions=None, sad_out: np.ndarray | None = None,
+                  coarse_radius: int | None = None, coarse_block_factor: int = 1):
+    """One block-matching search. Returns (mv (n, blocks, 2), conf).
+    With `predictions` (6 words per neighbour) every pass also searches around the neighbour's camera
+    model prediction, that window winning by more than 1/8 of `sad_floor` (scaled to the coarse
+    block on the coarse level). With `sad_out` (f32, 2 * n * blocks) the fine pass writes each
+    block's winning SAD and then its window's mean SAD; the truemotion stage and the escalation
+    replace the winning SAD. `coarse_radius` (default `search_radius`) and `coarse_block_factor` shape
+    the coarse pass (motion/context.rs:99-105).
     With `seeds` (n, blocks, 2) the search refines around them and skips the coarse pass. With
     `ceiling` > `search_radius` the blocks that fail search again `ceiling` around their first
     window (motion/escalate.rs), the coarse level too when a coarse pass ran, and the truemotion
@@ -623,13 +639,19 @@ def motion_search(pyramid: np.ndarray, width: int, height: int, frames: int, cen
     coarse = levels > 1 and seeds is None
     kept = np.zeros_like(mv) if (field_lambda > 0.0 and coarse) else None
     a.keep_seeds = kept.ctypes.data_as(C.POINTER(C.c_int32)) if kept is not None else None
+    pred = np.ascontiguousarray(predictions, np.float32).reshape(-1) if predictions is not None else None
+    a.predictions = _f(pred) if pred is not None else None
+    a.sad_out = _f(sad_out) if sad_out is not None else None
+    a.coarse_radius = search_radius if coarse_radius is None else coarse_radius
+    a.coarse_block_factor = coarse_block_factor
     l = lib()
     l.orc_motion_search.argtypes = [C.POINTER(MotionArgs)]
     l.orc_motion_search(C.byref(a))
     if field_lambda > 0.0:
         return truemotion_pass(pyramid, width, height, frames, centre_slot, slots, mv, kept, blksize=blksize,
                                overlap=overlap, field_lambda=field_lambda, thsad=thsad, sad_floor=sad_floor,
-                               reads_floor=reads_floor, confidence=confidence, passes=2 if escalates else 1)
+                               reads_floor=reads_floor, confidence=confidence, passes=2 if escalates else 1,
+                               predictions=pred, sad_out=sad_out)
     return mv.reshape(n, bx * by, 2), conf.reshape(n, bx * by)
 
 
@@ -643,6 +665,200 @@ def thsad(blksize: int, thsad_scale: float) -> float:
     """motion/confidence.rs:27-30 in f32."""
     f = np.float32
     return float(f(f(thsad_scale) * f(blksize * blksize)) * f(0.02))
+
+
+# ---- camera model (global_oracle.cpp; motion/global/) ---------------------------------------------
+
+MODEL_WORDS = 5
+AFFINE_WORDS = 6
+NO_PAIR = 0xFFFFFFFF
+HIGH_PASS_RADIUS = 8          # global/producer.rs:44-49
+ACQUISITION_COARSE_RADIUS = 12  # producer.rs:54-55
+ACQUISITION_COARSE_FACTOR = 2   # producer.rs:57-60
+MAX_PYRAMID_LEVELS = 3          # motion/search.rs:183
+
+
+def _i32(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def compose_models(models: np.ndarray, gaps: np.ndarray, neighbours: int, max_steps: int,
+                   past_neighbours: int) -> np.ndarray:
+    """motion/kernels/global.rs:18-119: one prediction (m00, m01, m10, m11, tx, ty) per neighbour
+    from the model ring `models` and the gap table `gaps` (ring slots, NO_PAIR for none)."""
+    m = np.ascontiguousarray(models, np.float32).reshape(-1)
+    g = np.ascontiguousarray(gaps, np.uint32).reshape(-1)
+    out = np.zeros(neighbours * AFFINE_WORDS, np.float32)
+    l = lib()
+    l.orc_compose_models.argtypes = [_fp, _u32p, _fp, C.c_uint32, C.c_uint32, C.c_uint32]
+    l.orc_compose_models(_f(m), g.ctypes.data_as(_u32p), _f(out), neighbours, max_steps, past_neighbours)
+    return out
+
+
+def compose_gaps(window_frames, centre: int, max_steps: int, slot_of) -> np.ndarray:
+    """global/compose.rs:18-64: the gap table of a window of stream frames, each gap the ring slot
+    (`slot_of(newer_frame)`) of a pair that steps exactly one frame, else NO_PAIR."""
+    def gap(older):
+        return slot_of(window_frames[older + 1]) if window_frames[older + 1] == window_frames[older] + 1 else NO_PAIR
+
+    positions = [p for p in range(len(window_frames)) if p != centre]
+    gaps = np.full(len(positions) * max_steps, NO_PAIR, np.uint32)
+    for row, p in enumerate(positions):
+        dist = abs(p - centre)
+        assert dist <= max_steps
+        for step in range(dist):
+            older = centre - step - 1 if p < centre else centre + step
+            gaps[row * max_steps + step] = gap(older)
+    return gaps
+
+
+def block_means(plane: np.ndarray, width: int, height: int, blksize: int, step: int) -> np.ndarray:
+    """motion/kernels/global.rs:121-155: each block's mean sample."""
+    bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
+    src = np.ascontiguousarray(plane, np.float32).reshape(-1)
+    out = np.zeros(bx * by, np.float32)
+    l = lib()
+    l.orc_block_means.argtypes = [_fp, _fp] + [C.c_int] * 6
+    l.orc_block_means(_f(src), _f(out), width, height, blksize, step, bx, by)
+    return out
+
+
+def high_pass(plane: np.ndarray, width: int, height: int, radius: int = HIGH_PASS_RADIUS) -> np.ndarray:
+    """motion/kernels/pyramid.rs:66-132: the plane minus its (2r+1)^2 box mean, rows then columns."""
+    src = np.ascontiguousarray(plane, np.float32).reshape(-1)
+    rows = np.zeros_like(src)
+    out = np.zeros_like(src)
+    l = lib()
+    l.orc_high_pass.argtypes = [_fp, _fp, _fp, C.c_int, C.c_int, C.c_int]
+    l.orc_high_pass(_f(src), _f(rows), _f(out), width, height, radius)
+    return out
+
+
+def model_fit(field: np.ndarray, width: int, height: int, blksize: int, overlap: int, *, sad: np.ndarray | None = None,
+              has_contrast: bool = False, older_to_newer: bool = True, models: np.ndarray | None = None,
+              slot: int = 0, prior: int | None = None):
+    """global/fit.rs:196-250 (`run_model_fit`): fits one direction of a pair field into ring slot
+    `slot` of `models` (updated in place; a one-slot ring when None). `sad` holds the winning SADs,
+    then, with `has_contrast`, the window means and the block means, one block count apart. Returns
+    (models, state)."""
+    step = blksize - overlap
+    bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
+    f = np.ascontiguousarray(field, np.int32).reshape(-1)
+    ring = np.zeros(MODEL_WORDS, np.float32) if models is None else models
+    assert ring.dtype == np.float32 and ring.flags["C_CONTIGUOUS"]
+    sd = np.ascontiguousarray(sad, np.float32).reshape(-1) if sad is not None else None
+    state = np.zeros(8, np.float32)
+    l = lib()
+    l.orc_model_fit.argtypes = [C.POINTER(C.c_int32), _fp, C.c_int, C.c_uint32, C.c_int] + [C.c_int] * 7 + \
+        [_fp, C.c_uint32, _fp]
+    l.orc_model_fit(_i32(f), _f(sd) if sd is not None else None, int(has_contrast), bx * by, int(older_to_newer),
+                    width, height, blksize, step, bx, by, -1 if prior is None else prior, _f(ring), slot, _f(state))
+    return ring, state
+
+
+def fit_bands(field: np.ndarray, width: int, height: int, blksize: int, overlap: int, *, sad=None,
+              has_contrast: bool = False) -> np.ndarray:
+    """global.rs:286-392: the four bar bounds (top end, bottom start, left end, right start)."""
+    step = blksize - overlap
+    bx, by = max(-(-width // step), 1), max(-(-height // step), 1)
+    f = np.ascontiguousarray(field, np.int32).reshape(-1)
+    sd = np.ascontiguousarray(sad, np.float32).reshape(-1) if sad is not None else None
+    bands = np.zeros(4, np.uint32)
+    l = lib()
+    l.orc_fit_bands.argtypes = [C.POINTER(C.c_int32), _fp, C.c_int, C.c_uint32] + [C.c_int] * 6 + [_u32p]
+    l.orc_fit_bands(_i32(f), _f(sd) if sd is not None else None, int(has_contrast), bx * by, width, height, blksize,
+                    step, bx, by, bands.ctypes.data_as(_u32p))
+    return bands
+
+
+class PairModels:
+    """global/producer.rs (`PairModelProducer`): one camera model per adjacent pair of pushed luma
+    frames, kept by stream frame (the engine's ring of `held + window + 2` slots never drops a model a
+    window still reads). Each push normalised luma loses its local mean, its block means are
+    measured, and it is matched against the frame before it: first a deep search (3 levels, coarse
+    radius 12 with blocks twice as wide, the search's escalation, the truemotion stage whose SADs
+    replace the search's) fitted from scratch, then the mode's own search around that model's
+    prediction, fitted again with the first fit as its prior. The first frame of a run, and a frame
+    that does not follow the last one pushed, writes identity."""
+
+    def __init__(self, width: int, height: int, *, blksize=16, overlap=8, search_radius=4, levels=2, ceiling=0):
+        self.w, self.h = width, height
+        self.blksize, self.overlap, self.radius, self.levels = blksize, overlap, search_radius, levels
+        self.ceiling = ceiling if ceiling > search_radius else 0
+        step = blksize - overlap
+        self.bx, self.by = max(-(-width // step), 1), max(-(-height // step), 1)
+        lp = lib()
+        lp.orc_motion_pyramid_floats.argtypes = [C.c_int] * 4
+        lp.orc_motion_pyramid_floats.restype = C.c_int64
+        self.pyramid = np.zeros(lp.orc_motion_pyramid_floats(width, height, 2, MAX_PYRAMID_LEVELS), np.float32)
+        self.models: dict[int, np.ndarray] = {}
+        self.run = None  # (first, last)
+        self.means = np.zeros(self.bx * self.by, np.float32)
+
+    def reset(self):
+        self.run = None
+
+    def model(self, frame: int) -> np.ndarray:
+        return self.models.get(frame, np.array([1, 0, 0, 0, 0], np.float32))
+
+    def _build(self, luma: np.ndarray, slot: int):
+        w, h = self.w, self.h
+        self.means = block_means(luma, w, h, self.blksize, self.blksize - self.overlap)
+        hp = high_pass(luma, w, h)
+        lp = lib()
+        lp.orc_motion_pyramid_build.argtypes = [_fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _fp, C.c_int]
+        lp.orc_motion_pyramid_build(_f(hp), 1, w, h, 2, 0, MAX_PYRAMID_LEVELS, _f(self.pyramid), slot)
+
+    def push(self, luma: np.ndarray, frame: int):
+        """Fits the pair from stream frame `frame - 1` to `frame`; `luma` is the normalised plane."""
+        newer = frame % 2
+        self._build(np.ascontiguousarray(luma, np.float32).reshape(-1), newer)
+        run = self.run
+        if run is None or not (run[0] < frame and (run[1] == frame or run[1] + 1 == frame)):
+            self.run = (frame, frame)
+            self.models[frame] = np.array([1, 0, 0, 0, 0], np.float32)
+            return
+        self.run = (run[0], frame)
+        older = (frame - 1) % 2
+        blocks = self.bx * self.by
+        th = thsad(self.blksize, 1.0)
+        kw = dict(blksize=self.blksize, overlap=self.overlap, search_radius=self.radius, thsad=th, sad_floor=0.0,
+                  ceiling=self.ceiling, esc_reads_floor=False)
+        ring = np.zeros(MODEL_WORDS, np.float32)
+        # producer.rs:435-480: the deep search, ending with the truemotion stage.
+        sad = np.zeros(3 * blocks, np.float32)
+        sad[2 * blocks:] = self.means
+        mv, _ = motion_search(self.pyramid, self.w, self.h, 2, older, [newer], levels=MAX_PYRAMID_LEVELS,
+                              field_lambda=1.0, reads_floor=False, sad_out=sad[:2 * blocks],
+                              coarse_radius=ACQUISITION_COARSE_RADIUS, coarse_block_factor=ACQUISITION_COARSE_FACTOR,
+                              **kw)
+        model_fit(mv[0], self.w, self.h, self.blksize, self.overlap, sad=sad, has_contrast=True, models=ring)
+        # producer.rs:415-420: the one-step prediction, then the mode's search around it.
+        pred = compose_models(ring, np.zeros(1, np.uint32), 1, 1, 0)
+        sad2 = np.zeros(3 * blocks, np.float32)
+        sad2[2 * blocks:] = self.means
+        mv2, _ = motion_search(self.pyramid, self.w, self.h, 2, older, [newer], levels=self.levels, predictions=pred,
+                               sad_out=sad2[:2 * blocks], **kw)
+        model_fit(mv2[0], self.w, self.h, self.blksize, self.overlap, sad=sad2, has_contrast=True, models=ring,
+                  prior=0)
+        self.models[frame] = ring.copy()
+
+    def compose_window(self, window_frames, centre: int) -> np.ndarray:
+        """nlmeans/denoiser/seeds.rs:136-160: every neighbour's prediction for a window of stream
+        frames (positions before `centre` are past neighbours), 2d steps each."""
+        nb = len(window_frames) - 1
+        frames = sorted(set(window_frames))
+        index = {f: i for i, f in enumerate(frames)}
+        ring = np.concatenate([self.model(f) for f in frames]).astype(np.float32)
+        gaps = compose_gaps(window_frames, centre, nb, lambda f: index[f])
+        return compose_models(ring, gaps, nb, nb, centre)
+
+    def compose_pair(self, older: int, newer: int) -> tuple[np.ndarray, np.ndarray]:
+        """seeds.rs:104-134: (older-to-newer, newer-to-older) predictions of one pair; a pair that does
+        not step exactly one frame predicts no motion."""
+        ring = self.model(newer).astype(np.float32)
+        gap = np.array([0 if newer == older + 1 else NO_PAIR], np.uint32)
+        return compose_models(ring, gap, 1, 1, 0), compose_models(ring, gap, 1, 1, 1)
 
 
 # ---- NL4D engine over a stream (nl4d/engine.rs, nl4d/denoiser.rs) --------------------------------
