@@ -163,7 +163,8 @@ class AvdMotionPass(C.Structure):
                [(n, u32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize", "overlap",
                                    "search_radius", "levels", "mv_stride", "conf_stride", "sad_floor_word")] + \
                [("thsad", f32), ("seeded", u32), ("keep_seeds", u64), ("escalation", u64), ("ceiling", u32),
-                ("esc_reads_floor", u32)]
+                ("esc_reads_floor", u32), ("predictions", u64), ("sad", u64), ("coarse_radius", u32),
+                ("coarse_block_factor", u32)]
 
 
 class AvdTruemotionPass(C.Structure):
@@ -171,7 +172,14 @@ class AvdTruemotionPass(C.Structure):
                                    "noise")] + \
                [(n, u32) for n in ("width", "height", "frame_count", "centre_slot", "neighbours", "blksize", "overlap",
                                    "mv_stride", "conf_stride", "sad_field", "reads_floor")] + \
-               [("field_lambda", f32), ("thsad", f32)]
+               [("field_lambda", f32), ("thsad", f32), ("predictions", u64), ("sad", u64)]
+
+
+class AvdModelFit(C.Structure):
+    _fields_ = [("field", u64), ("sad", u64)] + \
+               [(n, u32) for n in ("has_contrast", "means_offset", "older_to_newer", "width", "height", "blksize",
+                                   "overlap")] + \
+               [("prior", C.c_int32), ("models", u64), ("slot", u32), ("scratch", u64)]
 
 
 class AvdNlmBackward(C.Structure):
@@ -249,6 +257,11 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_motion_search": (C.c_int, [_P(AvdMotionPass), C.c_void_p]),
     "avd_truemotion_pass": (C.c_int, [_P(AvdTruemotionPass), C.c_void_p]),
     "avd_escalation_state_floats": (u64, [u32, u32]),
+    "avd_model_fit_scratch_floats": (u64, [u32]),
+    "avd_model_fit": (C.c_int, [_P(AvdModelFit), C.c_void_p]),
+    "avd_compose_models": (C.c_int, [u64, u64, u64, u32, u32, u32, C.c_void_p]),
+    "avd_block_means": (C.c_int, [u64, u64, u32, u32, u32, u32, C.c_void_p]),
+    "avd_high_pass": (C.c_int, [u64, u64, u64, u32, u32, u32, C.c_void_p]),
     "avd_chain_compose": (C.c_int, [u64, u64, u32, u32, u32, u32, u32, u32, u32, u32, u32, C.c_void_p]),
     "avd_sad_noise_floor": (f32, [u32, f32]),
     "avd_thsad": (f32, [u32, f32]),

@@ -39,9 +39,10 @@ COMMON = [
 # restatement does (built with -ffp-contract=off), so its member choices and threshold decisions
 # agree bit for bit; -fmad=false keeps nvcc from fusing any of them. The noise estimate does the same
 # for its reading and fold words, the truemotion stage for its costs and confidences, the exact
-# NLMeans finish for its distances, weights and sums, and the colour grain gains for their fit.
+# NLMeans finish for its distances, weights and sums, the colour grain gains for their fit, and the
+# camera model for its fit and composition.
 PER_FILE = {"collab.cu": ["-fmad=false"], "noise_estimate.cu": ["-fmad=false"], "truemotion.cu": ["-fmad=false"],
-            "nlm_exact.cu": ["-fmad=false"], "colour.cu": ["-fmad=false"]}
+            "nlm_exact.cu": ["-fmad=false"], "colour.cu": ["-fmad=false"], "camera.cu": ["-fmad=false"]}
 
 
 def _sources() -> list[Path]:

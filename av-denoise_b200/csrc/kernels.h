@@ -161,6 +161,13 @@ struct MotionLaunch {
     // else measured from the first pass's SADs; `thsad` must be positive.
     float* escalation;
     int ceiling, esc_reads_floor;
+    // The camera model (motion/kernels/candidates.rs): with `predictions` (6 words per neighbour,
+    // `noise` required) every pass also searches around the neighbour's prediction, that window
+    // winning by more than 1/8 of noise word `sad_floor_word` (scaled to the coarse block on the
+    // coarse level). With `sad`, the fine pass writes each block's winning SAD and then, neighbours *
+    // conf_stride values on, its window's mean SAD; escalation replaces an improved block's SAD.
+    const float* predictions;
+    float* sad;
 };
 
 size_t escalation_state_floats(int neighbours, int conf_stride);
@@ -196,8 +203,50 @@ struct TruemotionLaunch {
     // `changes_out` flags the blocks whose pick left their own vector (conf layout).
     const uint32_t* changes_in;
     uint32_t* changes_out;
+    // mod.rs:878-900: with `predictions` (6 words per neighbour) the camera model's prediction at the
+    // block is a candidate when the model moves anything; with `sad`, every rescored block writes
+    // its winning SAD there (conf layout).
+    const float* predictions;
+    float* sad;
 };
 cudaError_t launch_truemotion(const TruemotionLaunch& args, cudaStream_t stream);
+
+// ---- the camera model (camera.cu; av-denoise-core/src/motion/global, kernels/global.rs) ------------
+//
+// A pair model is 5 f32 words (a, b, tx, ty, valid) mapping a luma position of the older frame into
+// the newer one, x' = a x - b y + tx, y' = b x + a y + ty; a prediction is 6 words (m00 m01 m10 m11
+// tx ty) per neighbour.
+
+// global/fit.rs:196-250 (`run_model_fit`): fits one direction of a pair field into ring slot `slot`
+// of `models`, from ring slot `prior` when it is at least 0. `sad` (or null) holds the winning SADs,
+// then, with `has_contrast`, the window means and the block means, `means_offset` values apart.
+// `scratch` holds model_fit_scratch_floats(blocks) floats: the 8 state words first.
+struct ModelFitLaunch {
+    const int32_t* field;
+    const float* sad;
+    bool has_contrast;
+    int means_offset;
+    bool older_to_newer;
+    int width, height, blksize, step;
+    int prior;
+    float* models;
+    int slot;
+    float* scratch;
+};
+size_t model_fit_scratch_floats(int blocks);
+cudaError_t launch_model_fit(const ModelFitLaunch& args, cudaStream_t stream);
+// global.rs:18-119 (`mc_compose_models`): `gaps` holds `max_steps` ring slots (or 0xFFFFFFFF) per
+// neighbour, from the centre outward; the first `past_neighbours` neighbours lie behind the centre.
+cudaError_t launch_compose_models(const float* models, const uint32_t* gaps, float* out, int neighbours,
+                                  int max_steps, int past_neighbours, cudaStream_t stream);
+// global.rs:121-155 (`mc_block_means`) on the block grid of blksize / step.
+cudaError_t launch_block_means(const float* plane, float* out, int width, int height, int blksize, int step,
+                               cudaStream_t stream);
+// pyramid.rs:66-132: `out` = `plane` minus its (2 radius + 1)^2 box mean; `rows` is scratch.
+cudaError_t launch_high_pass(const float* plane, float* rows, float* out, int width, int height, int radius,
+                             cudaStream_t stream);
+// global.rs:157-172 (`mc_model_identity`).
+cudaError_t launch_model_identity(float* models, int slot, cudaStream_t stream);
 
 // motion/kernels/compensate.rs (`mc_warp`) for every neighbour of a window in one launch: ring slot
 // slots[n] of `src_ring` (and `src_ref`, when set) warped along neighbour n's field into the same

@@ -12,8 +12,14 @@
 //                                tie, and the window's centre wins a tie with that pick.
 //   kernels/block_match.rs:505-521  confidence = max(0, (T^2 - e^2) / (T^2 + e^2)),
 //                                e = max(SAD - floor, 0).
-//   analyse.rs:100-150           the coarse level: blksize max(b / 2^l, 2), step max(s / 2^l, 1),
-//                                its winner scaled by 2^l seeds every fine block it covers.
+//   analyse.rs:100-157           the coarse level: blksize max(b / 2^l, 2) times the coarse block
+//                                factor, step max(s / 2^l, 1), its winner scaled by 2^l seeds every
+//                                fine block it covers.
+//   block_match.rs:213-265, 384-578 with candidates.rs  the camera model: a second window around
+//                                each neighbour's prediction when it moves anything and lies outside
+//                                the first window, winning only by more than 1/8 of the SAD floor
+//                                (scaled to the coarse block on the coarse level); the winning
+//                                window's mean SAD and edge bar go with its winner.
 //
 // Layout in HBM: the pyramid holds, level after level, `frame_count` slots of that level's
 // pixels, each slot padded to a multiple of 8 floats (32 bytes). Vectors are (dx, dy) i32 pairs per
@@ -29,14 +35,17 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "camera_model.cuh"
 #include "kernels.h"
 
 namespace avd {
 namespace {
 
 constexpr int kMaxBlk = 32;
-constexpr int kMaxRadius = 8;
+constexpr int kMaxRadius = 8;           // fine windows and escalation ceilings
+constexpr int kAcquisitionRadius = 12;  // the camera model's deep coarse search (global/producer.rs:54-55)
 constexpr float kNoSad = 1.0e30f;
+constexpr float kModelCandidateBias = 0.125f;  // candidates.rs:6-11
 constexpr int kMaxNeighbours = MotionLaunch::kMaxInlineSlots;
 
 __device__ __forceinline__ int clamp_to(int v, int limit) { return v < 0 ? 0 : (v >= limit ? limit - 1 : v); }
@@ -69,6 +78,26 @@ struct SearchLevel {
     int blksize, step, blocks_x, blocks_y;
 };
 
+// One window's result (block_match.rs:580-600, `WindowBest`): the winner, its SAD, the window's
+// mean SAD (when measured), the edge bar (the lowest SAD off the outer ring when the winner sits on
+// it, else 0) and the window's centre.
+struct WinBest {
+    int dx, dy;
+    float sad, mean, bar;
+    int cdx, cdy;
+};
+
+// candidates.rs:136-156 (`model_centre`): whether neighbour n's prediction adds a window of radius R
+// beside the one around (sdx, sdy): the model moves anything and its point lies outside that window.
+// Every thread of a CTA (or lane of a warp) reads the same words, so the answer is uniform.
+__device__ __forceinline__ bool model_window(const float* predictions, int n, int ox, int oy, int blksize, int scale,
+                                             int lw, int lh, int R, int sdx, int sdy, int* mdx, int* mdy) {
+    if (!predictions) return false;
+    const float* p = predictions + n * kAffineWords;
+    model_point(p, ox, oy, blksize, scale, lw, lh, mdx, mdy);
+    return predicts_motion(p) && (abs(*mdx - sdx) > R || abs(*mdy - sdy) > R);
+}
+
 // The best offset of one window, at thread 0. `sads` holds every candidate's SAD.
 template <int R>
 __device__ __forceinline__ void window_argmin(const float* sads, unsigned long long* warp_keys, int* best_index) {
@@ -76,10 +105,13 @@ __device__ __forceinline__ void window_argmin(const float* sads, unsigned long l
     constexpr int kCand = kSide * kSide;
     const int t = threadIdx.x;
     unsigned long long key = ~0ull;
-    if (t < kCand) {
-        const float s = sads[t];
+    for (int i = t; i < kCand; i += blockDim.x) {
+        const float s = sads[i];
         // Only SADs below the 1e30 start count, and NaN never compares below it.
-        if (s < kNoSad) key = (static_cast<unsigned long long>(__float_as_uint(s)) << 32) | static_cast<unsigned>(t);
+        if (s < kNoSad) {
+            const unsigned long long k = (static_cast<unsigned long long>(__float_as_uint(s)) << 32) | static_cast<unsigned>(i);
+            key = k < key ? k : key;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -116,17 +148,72 @@ __device__ __forceinline__ void score_window(const SearchLevel& L, int64_t centr
         window[i] = L.pyramid[nbr_base + static_cast<int64_t>(sy) * L.width + sx];
     }
     __syncthreads();
-    if (t < kSide * kSide) {
-        const int dy = t / kSide, dx = t - dy * kSide;
+    for (int c = t; c < kSide * kSide; c += blockDim.x) {
+        const int dy = c / kSide, dx = c - dy * kSide;
         float sad = 0.0f;
         for (int iy = 0; iy < b; ++iy) {
             const float* wrow = window + (iy + dy) * wside + dx;
             const float* crow = centre_tile + iy * b;
             for (int ix = 0; ix < b; ++ix) sad = __fadd_rn(sad, fabsf(__fsub_rn(crow[ix], wrow[ix])));
         }
-        sads[t] = sad;
+        sads[c] = sad;
     }
     __syncthreads();
+}
+
+// The winner of a scored window around (cdx, cdy) (block_match.rs:720-785): the lowest SAD with the
+// first row-major index, the centre winning a tie; the mean sums every SAD in row-major order;
+// the edge bar is the lowest SAD off the outer ring (1e30 at radius 0) when the winner sits on it.
+template <int R>
+__device__ __forceinline__ WinBest window_result(const float* sads, int best_index, int cdx, int cdy, bool want_mean,
+                                                 bool want_bar) {
+    constexpr int kSide = 2 * R + 1;
+    constexpr int kCand = kSide * kSide;
+    WinBest r{cdx, cdy, kNoSad, 0.0f, 0.0f, cdx, cdy};
+    if (best_index >= 0) {
+        r.sad = sads[best_index];
+        r.dx = cdx + best_index % kSide - R;
+        r.dy = cdy + best_index / kSide - R;
+    }
+    const float centre_sad = sads[R * kSide + R];
+    if (centre_sad <= r.sad) {
+        r.sad = centre_sad;
+        r.dx = cdx;
+        r.dy = cdy;
+    }
+    if (want_mean) {
+        float total = 0.0f;
+        for (int i = 0; i < kCand; ++i) total = __fadd_rn(total, sads[i]);
+        r.mean = __fmul_rn(total, __fdiv_rn(1.0f, static_cast<float>(kCand)));
+    }
+    if (want_bar && (abs(r.dx - cdx) == R || abs(r.dy - cdy) == R)) {
+        float bar = kNoSad;
+        for (int y = 1; y < kSide - 1; ++y)
+            for (int x = 1; x < kSide - 1; ++x) bar = fminf(bar, sads[y * kSide + x]);
+        r.bar = bar;
+    }
+    return r;
+}
+
+template <int R>
+struct WindowScratch {
+    float centre_tile[kMaxBlk * kMaxBlk];
+    float window[(kMaxBlk + 2 * R) * (kMaxBlk + 2 * R)];
+    float sads[(2 * R + 1) * (2 * R + 1)];
+    unsigned long long warp_keys[((2 * R + 1) * (2 * R + 1) + 31) / 32];
+    int best_index;
+};
+
+// One window around (cdx, cdy), the result at thread 0; every thread must call it.
+template <int R>
+__device__ __forceinline__ WinBest window_best(const SearchLevel& L, int64_t centre_base, int64_t nbr_base, int ox,
+                                               int oy, int cdx, int cdy, WindowScratch<R>& w, bool want_mean,
+                                               bool want_bar) {
+    score_window<R>(L, centre_base, nbr_base, ox, oy, cdx, cdy, w.centre_tile, w.window, w.sads);
+    window_argmin<R>(w.sads, w.warp_keys, &w.best_index);
+    WinBest r{cdx, cdy, kNoSad, 0.0f, 0.0f, cdx, cdy};
+    if (threadIdx.x == 0) r = window_result<R>(w.sads, w.best_index, cdx, cdy, want_mean, want_bar);
+    return r;
 }
 
 struct SearchArgs {
@@ -146,62 +233,55 @@ struct SearchArgs {
     int sad_floor_word;
     float thsad;
     // Fine only, with escalation: the state the first pass records for it (escalate.rs:84-155):
-    // sections `esc_section` floats apart of kept SAD, edge bar, and first-window centre x and y.
+    // sections `esc_section` floats apart of kept SAD, edge bar, and the winning window's centre.
     float* esc_state;
     int64_t esc_section;
+    // The camera model (candidates.rs): 6 prediction words per neighbour, or null; its window wins
+    // by more than 1/8 of noise word `sad_floor_word`, times `floor_scale` on the coarse level.
+    const float* predictions;
+    float floor_scale;
+    // Fine only: winning SADs, then `sad_means` values on, the windows' mean SADs (conf layout).
+    float* sad_out;
+    int64_t sad_means;
 };
 
-// Winner of one window around (cdx, cdy): the reference's `search_window` for a single centre.
-template <int R>
-__device__ __forceinline__ void search_one(const SearchArgs& a, int bx, int by, int n, int cdx, int cdy, int* out_dx,
-                                           int* out_dy, float* out_sad) {
-    constexpr int kSide = 2 * R + 1;
-    __shared__ float centre_tile[kMaxBlk * kMaxBlk];
-    __shared__ float window[(kMaxBlk + 2 * kMaxRadius) * (kMaxBlk + 2 * kMaxRadius)];
-    __shared__ float sads[kSide * kSide];
-    __shared__ unsigned long long warp_keys[(kSide * kSide + 31) / 32];
-    __shared__ int best_index;
-    const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
-    const uint32_t nbr_slot = a.neighbour_slots ? a.neighbour_slots[n] : a.slots[n];
-    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(nbr_slot) * a.L.slot_pixels;
-    const int ox = bx * a.L.step, oy = by * a.L.step;
-    score_window<R>(a.L, centre_base, nbr_base, ox, oy, cdx, cdy, centre_tile, window, sads);
-    window_argmin<R>(sads, warp_keys, &best_index);
-    if (threadIdx.x == 0) {
-        float best_sad = kNoSad;
-        int bdx = cdx, bdy = cdy;
-        if (best_index >= 0) {
-            best_sad = sads[best_index];
-            bdx = cdx + (best_index % kSide) - R;
-            bdy = cdy + (best_index / kSide) - R;
-        }
-        // A tie resolves to the window's centre (block_match.rs:735-742).
-        const float centre_sad = sads[R * kSide + R];
-        if (centre_sad <= best_sad) {
-            best_sad = centre_sad;
-            bdx = cdx;
-            bdy = cdy;
-        }
-        *out_dx = bdx;
-        *out_dy = bdy;
-        *out_sad = best_sad;
-    }
+__device__ __forceinline__ uint32_t search_slot(const SearchArgs& a, int n) {
+    return a.neighbour_slots ? a.neighbour_slots[n] : a.slots[n];
 }
 
+// The model's bias: 1/8 of the window's SAD floor, scaled to the level (block_match.rs:156-159).
+__device__ __forceinline__ float model_bias(const SearchArgs& a, float level_scale_factor) {
+    if (!a.predictions || !a.noise) return 0.0f;
+    return __fmul_rn(__fmul_rn(kModelCandidateBias, a.noise[a.sad_floor_word]), level_scale_factor);
+}
+
+// block_match.rs:520-578 (`search_candidates`) over the window around (sdx, sdy) and, when the
+// camera model adds one, the window around its point, which replaces the first only when its SAD
+// plus `bias` is lower. The result is valid at thread 0; every thread must call it.
 template <int R>
-__global__ void __launch_bounds__(320) coarse_kernel(SearchArgs a) {
-    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
-    int dx = 0, dy = 0;
-    float sad = 0.0f;
-    search_one<R>(a, bx, by, n, 0, 0, &dx, &dy, &sad);
-    if (threadIdx.x != 0) return;
-    // block_match.rs:190-214: every fine block inside this coarse block's region takes the scaled
-    // winner; the last coarse block on each axis reaches the fine grid's edge.
+__device__ __forceinline__ WinBest search_candidates(const SearchArgs& a, int bx, int by, int n, int sdx, int sdy,
+                                                     int scale, float bias, bool want_mean, bool want_bar) {
+    __shared__ WindowScratch<R> w;
+    const int64_t cb = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
+    const int64_t nb = a.L.level_base + static_cast<int64_t>(search_slot(a, n)) * a.L.slot_pixels;
+    const int ox = bx * a.L.step, oy = by * a.L.step;
+    WinBest best = window_best<R>(a.L, cb, nb, ox, oy, sdx, sdy, w, want_mean, want_bar);
+    int mdx, mdy;
+    if (model_window(a.predictions, n, ox, oy, a.L.blksize, scale, a.L.width, a.L.height, R, sdx, sdy, &mdx, &mdy)) {
+        const WinBest ch = window_best<R>(a.L, cb, nb, ox, oy, mdx, mdy, w, want_mean, want_bar);
+        if (threadIdx.x == 0 && __fadd_rn(ch.sad, bias) < best.sad) best = ch;
+    }
+    return best;
+}
+
+// block_match.rs:190-214: every fine block inside coarse block (bx, by)'s region takes the scaled
+// winner; the last coarse block on each axis reaches the fine grid's edge.
+__device__ __forceinline__ void seed_fine_blocks(const SearchArgs& a, int bx, int by, int n, int dx, int dy) {
     const int s = a.L.step * a.level_scale;
     const int c0 = min(bx * s / a.fine_step, a.fine_blocks_x);
-    const int c1 = bx == static_cast<int>(gridDim.x) - 1 ? a.fine_blocks_x : min((bx + 1) * s / a.fine_step, a.fine_blocks_x);
+    const int c1 = bx == a.L.blocks_x - 1 ? a.fine_blocks_x : min((bx + 1) * s / a.fine_step, a.fine_blocks_x);
     const int r0 = min(by * s / a.fine_step, a.fine_blocks_y);
-    const int r1 = by == static_cast<int>(gridDim.y) - 1 ? a.fine_blocks_y : min((by + 1) * s / a.fine_step, a.fine_blocks_y);
+    const int r1 = by == a.L.blocks_y - 1 ? a.fine_blocks_y : min((by + 1) * s / a.fine_step, a.fine_blocks_y);
     int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride;
     for (int r = r0; r < r1; ++r)
         for (int c = c0; c < c1; ++c) {
@@ -210,28 +290,53 @@ __global__ void __launch_bounds__(320) coarse_kernel(SearchArgs a) {
         }
 }
 
-template <int R>
-__global__ void __launch_bounds__(320) fine_kernel(SearchArgs a) {
-    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
+__device__ __forceinline__ float match_confidence(float sad, float floor, float thsad) {
+    float excess = __fsub_rn(sad, floor);
+    if (excess < 0.0f) excess = 0.0f;
+    const float t2 = __fmul_rn(thsad, thsad);
+    const float e2 = __fmul_rn(excess, excess);
+    const float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
+    return c < 0.0f ? 0.0f : c;
+}
+
+// The outputs of one fine block (block_match.rs:480-510 and escalate.rs:140-155): the vector, the
+// escalation state, the SAD and window mean, and the confidence.
+__device__ __forceinline__ void write_fine(const SearchArgs& a, int bx, int by, int n, const WinBest& b) {
     int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
+    mv[0] = b.dx;
+    mv[1] = b.dy;
+    const int64_t slot = static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx;
+    if (a.esc_state) {
+        a.esc_state[slot] = b.sad;
+        a.esc_state[a.esc_section + slot] = b.bar;
+        a.esc_state[2 * a.esc_section + slot] = static_cast<float>(b.cdx);
+        a.esc_state[3 * a.esc_section + slot] = static_cast<float>(b.cdy);
+    }
+    if (a.sad_out) {
+        a.sad_out[slot] = b.sad;
+        a.sad_out[a.sad_means + slot] = b.mean;
+    }
+    if (a.confidence) a.confidence[slot] = match_confidence(b.sad, a.noise[a.sad_floor_word], a.thsad);
+}
+
+template <int R>
+__global__ void __launch_bounds__(((2 * R + 1) * (2 * R + 1) + 31) / 32 * 32) coarse_kernel(SearchArgs a) {
+    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
+    const WinBest b = search_candidates<R>(a, bx, by, n, 0, 0, a.level_scale, model_bias(a, a.floor_scale), false, false);
+    if (threadIdx.x != 0) return;
+    seed_fine_blocks(a, bx, by, n, b.dx, b.dy);
+}
+
+template <int R>
+__global__ void __launch_bounds__(((2 * R + 1) * (2 * R + 1) + 31) / 32 * 32) fine_kernel(SearchArgs a) {
+    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
+    const int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
     const int sdx = a.use_seed ? mv[0] : 0;
     const int sdy = a.use_seed ? mv[1] : 0;
-    int dx = 0, dy = 0;
-    float sad = 0.0f;
-    search_one<R>(a, bx, by, n, sdx, sdy, &dx, &dy, &sad);
+    const WinBest b = search_candidates<R>(a, bx, by, n, sdx, sdy, 1, model_bias(a, 1.0f), a.sad_out != nullptr,
+                                           a.esc_state != nullptr);
     if (threadIdx.x != 0) return;
-    mv[0] = dx;
-    mv[1] = dy;
-    if (a.confidence) {
-        const float floor = a.noise[a.sad_floor_word];
-        float excess = __fsub_rn(sad, floor);
-        if (excess < 0.0f) excess = 0.0f;
-        const float t2 = __fmul_rn(a.thsad, a.thsad);
-        const float e2 = __fmul_rn(excess, excess);
-        float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
-        if (c < 0.0f) c = 0.0f;
-        a.confidence[static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx] = c;
-    }
+    write_fine(a, bx, by, n, b);
 }
 
 // Register-blocked search for the common block sizes: one warp per (block, neighbour), several
@@ -307,29 +412,6 @@ __device__ __forceinline__ void blocked_window(const SearchLevel& L, int64_t cen
     *best_key = key;
 }
 
-template <int BLK, int R>
-__device__ __forceinline__ void blocked_pick(const float* sads, unsigned long long key, int cdx, int cdy, int* out_dx,
-                                             int* out_dy, float* out_sad) {
-    using B = Blocked<BLK, R>;
-    float best_sad = kNoSad;
-    int bdx = cdx, bdy = cdy;
-    if (key != ~0ull) {
-        const int idx = static_cast<int>(key & 0xffffffffu);
-        best_sad = sads[idx];
-        bdx = cdx + idx % B::kSide - R;
-        bdy = cdy + idx / B::kSide - R;
-    }
-    const float centre_sad = sads[R * B::kSide + R];
-    if (centre_sad <= best_sad) {
-        best_sad = centre_sad;
-        bdx = cdx;
-        bdy = cdy;
-    }
-    *out_dx = bdx;
-    *out_dy = bdy;
-    *out_sad = best_sad;
-}
-
 template <int BLK, int R, bool COARSE>
 __global__ void __launch_bounds__(Blocked<BLK, R>::kWarps * 32) blocked_kernel(SearchArgs a) {
     using B = Blocked<BLK, R>;
@@ -339,83 +421,48 @@ __global__ void __launch_bounds__(Blocked<BLK, R>::kWarps * 32) blocked_kernel(S
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int bx = blockIdx.x * B::kWarps + warp, by = blockIdx.y, n = blockIdx.z;
     if (bx >= a.L.blocks_x) return;  // the whole warp leaves; only warp-scoped syncs follow
-    const uint32_t nbr_slot = a.neighbour_slots ? a.neighbour_slots[n] : a.slots[n];
     const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
-    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(nbr_slot) * a.L.slot_pixels;
+    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(search_slot(a, n)) * a.L.slot_pixels;
     const int ox = bx * a.L.step, oy = by * a.L.step;
     int cdx = 0, cdy = 0;
-    int32_t* mv_fine = nullptr;
-    if (!COARSE) {
-        mv_fine = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
-        if (a.use_seed) {
-            cdx = mv_fine[0];
-            cdy = mv_fine[1];
-        }
+    if (!COARSE && a.use_seed) {
+        const int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
+        cdx = mv[0];
+        cdy = mv[1];
     }
+    const bool want_mean = !COARSE && a.sad_out != nullptr, want_bar = !COARSE && a.esc_state != nullptr;
     unsigned long long key;
     blocked_window<BLK, R>(a.L, centre_base, nbr_base, ox, oy, cdx, cdy, centre_tiles[warp], windows[warp],
                            sad_buf[warp], lane, &key);
+    WinBest best{cdx, cdy, kNoSad, 0.0f, 0.0f, cdx, cdy};
+    if (lane == 0) best = window_result<R>(sad_buf[warp], key == ~0ull ? -1 : static_cast<int>(key & 0xffffffffu), cdx,
+                                           cdy, want_mean, want_bar);
+    int mdx, mdy;
+    const int scale = COARSE ? a.level_scale : 1;
+    if (model_window(a.predictions, n, ox, oy, BLK, scale, a.L.width, a.L.height, R, cdx, cdy, &mdx, &mdy)) {
+        blocked_window<BLK, R>(a.L, centre_base, nbr_base, ox, oy, mdx, mdy, centre_tiles[warp], windows[warp],
+                               sad_buf[warp], lane, &key);
+        if (lane == 0) {
+            const WinBest ch = window_result<R>(sad_buf[warp], key == ~0ull ? -1 : static_cast<int>(key & 0xffffffffu),
+                                                mdx, mdy, want_mean, want_bar);
+            if (__fadd_rn(ch.sad, model_bias(a, COARSE ? a.floor_scale : 1.0f)) < best.sad) best = ch;
+        }
+    }
     if (lane != 0) return;
-    int dx, dy;
-    float sad;
-    blocked_pick<BLK, R>(sad_buf[warp], key, cdx, cdy, &dx, &dy, &sad);
     if (COARSE) {
-        const int s = a.L.step * a.level_scale;
-        const int c0 = min(bx * s / a.fine_step, a.fine_blocks_x);
-        const int c1 = bx == a.L.blocks_x - 1 ? a.fine_blocks_x : min((bx + 1) * s / a.fine_step, a.fine_blocks_x);
-        const int r0 = min(by * s / a.fine_step, a.fine_blocks_y);
-        const int r1 = by == a.L.blocks_y - 1 ? a.fine_blocks_y : min((by + 1) * s / a.fine_step, a.fine_blocks_y);
-        int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride;
-        for (int r = r0; r < r1; ++r)
-            for (int c = c0; c < c1; ++c) {
-                mv[(r * a.fine_blocks_x + c) * 2] = dx * a.level_scale;
-                mv[(r * a.fine_blocks_x + c) * 2 + 1] = dy * a.level_scale;
-            }
+        seed_fine_blocks(a, bx, by, n, best.dx, best.dy);
         return;
     }
-    mv_fine[0] = dx;
-    mv_fine[1] = dy;
-    if (a.esc_state) {
-        // block_match.rs:783-796: a winner on the window's outer ring records the lowest SAD off
-        // the ring as its edge bar.
-        float bar = 0.0f;
-        if (abs(dx - cdx) == R || abs(dy - cdy) == R) {
-            bar = kNoSad;
-            for (int y = 1; y < B::kSide - 1; ++y)
-                for (int x = 1; x < B::kSide - 1; ++x) bar = fminf(bar, sad_buf[warp][y * B::kSide + x]);
-        }
-        const int64_t slot = static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx;
-        a.esc_state[slot] = sad;
-        a.esc_state[a.esc_section + slot] = bar;
-        a.esc_state[2 * a.esc_section + slot] = static_cast<float>(cdx);
-        a.esc_state[3 * a.esc_section + slot] = static_cast<float>(cdy);
-    }
-    if (a.confidence) {
-        const float floor = a.noise[a.sad_floor_word];
-        float excess = __fsub_rn(sad, floor);
-        if (excess < 0.0f) excess = 0.0f;
-        const float t2 = __fmul_rn(a.thsad, a.thsad);
-        const float e2 = __fmul_rn(excess, excess);
-        float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
-        if (c < 0.0f) c = 0.0f;
-        a.confidence[static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx] = c;
-    }
+    write_fine(a, bx, by, n, best);
 }
 
 // The fine pass at radius 0 (the HQ confidence pass scores every block where it stands): one thread
 // per (block, neighbour). The single candidate's SAD is the same sequential row-major sum the
 // windowed kernels take, so vectors, SADs and confidences are theirs bit for bit; a SAD that is not
 // below the 1e30 start leaves the search's 1e30 (block_match.rs:735-742).
-__global__ void __launch_bounds__(128) zero_radius_fine_kernel(SearchArgs a) {
-    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y, n = blockIdx.z;
-    if (bx >= a.L.blocks_x) return;
-    int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
-    const int cdx = a.use_seed ? mv[0] : 0;
-    const int cdy = a.use_seed ? mv[1] : 0;
-    const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
-    const uint32_t nbr_slot = a.neighbour_slots ? a.neighbour_slots[n] : a.slots[n];
-    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(nbr_slot) * a.L.slot_pixels;
-    const int ox = bx * a.L.step, oy = by * a.L.step, b = a.L.blksize;
+__device__ __forceinline__ float point_sad(const SearchArgs& a, int64_t centre_base, int64_t nbr_base, int ox, int oy,
+                                           int cdx, int cdy) {
+    const int b = a.L.blksize;
     float sad = 0.0f;
     for (int iy = 0; iy < b; ++iy) {
         const int64_t crow = centre_base + static_cast<int64_t>(clamp_to(oy + iy, a.L.height)) * a.L.width;
@@ -427,29 +474,44 @@ __global__ void __launch_bounds__(128) zero_radius_fine_kernel(SearchArgs a) {
             sad = __fadd_rn(sad, fabsf(__fsub_rn(c, w)));
         }
     }
-    if (!(sad <= kNoSad)) sad = kNoSad;
-    mv[0] = cdx;
-    mv[1] = cdy;
-    if (a.confidence) {
-        const float floor = a.noise[a.sad_floor_word];
-        float excess = __fsub_rn(sad, floor);
-        if (excess < 0.0f) excess = 0.0f;
-        const float t2 = __fmul_rn(a.thsad, a.thsad);
-        const float e2 = __fmul_rn(excess, excess);
-        float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
-        if (c < 0.0f) c = 0.0f;
-        a.confidence[static_cast<int64_t>(n) * a.conf_stride + by * a.L.blocks_x + bx] = c;
+    return sad;
+}
+
+__global__ void __launch_bounds__(128) zero_radius_fine_kernel(SearchArgs a) {
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y, n = blockIdx.z;
+    if (bx >= a.L.blocks_x) return;
+    const int32_t* mv = a.mv_field + static_cast<int64_t>(n) * a.mv_stride + (by * a.L.blocks_x + bx) * 2;
+    const int cdx = a.use_seed ? mv[0] : 0;
+    const int cdy = a.use_seed ? mv[1] : 0;
+    const int64_t centre_base = a.L.level_base + static_cast<int64_t>(a.centre_slot) * a.L.slot_pixels;
+    const int64_t nbr_base = a.L.level_base + static_cast<int64_t>(search_slot(a, n)) * a.L.slot_pixels;
+    const int ox = bx * a.L.step, oy = by * a.L.step;
+    // A window of one candidate: its SAD is the mean, and its winner always sits on the outer ring
+    // with nothing inside it (block_match.rs:803-820).
+    const float raw = point_sad(a, centre_base, nbr_base, ox, oy, cdx, cdy);
+    WinBest best{cdx, cdy, raw <= kNoSad ? raw : kNoSad, raw, kNoSad, cdx, cdy};
+    int mdx, mdy;
+    if (model_window(a.predictions, n, ox, oy, a.L.blksize, 1, a.L.width, a.L.height, 0, cdx, cdy, &mdx, &mdy)) {
+        const float mraw = point_sad(a, centre_base, nbr_base, ox, oy, mdx, mdy);
+        const float msad = mraw <= kNoSad ? mraw : kNoSad;
+        if (__fadd_rn(msad, model_bias(a, 1.0f)) < best.sad) best = WinBest{mdx, mdy, msad, mraw, kNoSad, mdx, mdy};
     }
+    write_fine(a, bx, by, n, best);
 }
 
 template <int BLK, int R>
 cudaError_t launch_blocked(bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
     using B = Blocked<BLK, R>;
     dim3 g((grid.x + B::kWarps - 1) / B::kWarps, grid.y, grid.z);
-    if (coarse)
+    if (coarse) {
         blocked_kernel<BLK, R, true><<<g, B::kWarps * 32, 0, s>>>(a);
-    else
-        blocked_kernel<BLK, R, false><<<g, B::kWarps * 32, 0, s>>>(a);
+    } else {
+        if constexpr (R <= kMaxRadius) {
+            blocked_kernel<BLK, R, false><<<g, B::kWarps * 32, 0, s>>>(a);
+        } else {
+            return cudaErrorInvalidValue;
+        }
+    }
     return cudaGetLastError();
 }
 
@@ -469,10 +531,15 @@ cudaError_t launch_search(bool coarse, const SearchArgs& a, dim3 grid, cudaStrea
     }
     constexpr int kCand = (2 * R + 1) * (2 * R + 1);
     const int threads = ((kCand + 31) / 32) * 32;
-    if (coarse)
+    if (coarse) {
         coarse_kernel<R><<<grid, threads, 0, s>>>(a);
-    else
-        fine_kernel<R><<<grid, threads, 0, s>>>(a);
+    } else {
+        if constexpr (R <= kMaxRadius) {
+            fine_kernel<R><<<grid, threads, 0, s>>>(a);
+        } else {
+            return cudaErrorInvalidValue;
+        }
+    }
     return cudaGetLastError();
 }
 
@@ -480,8 +547,8 @@ cudaError_t launch_search(bool coarse, const SearchArgs& a, dim3 grid, cudaStrea
 //
 // With a ceiling above the first radius, blocks that fail their first window search again around
 // the same centre at the ceiling. The state holds four sections of neighbours * conf_stride floats
-// (kept SAD, edge bar then failure flag, first window centre x and y) and the SAD floor after them.
-// Every stage reads only what the launch before it wrote, so the result does not depend on the
+// (kept SAD, edge bar then failure flag, winning window's centre x and y) and the SAD floor after
+// them. Every stage reads only what the launch before it wrote, so the result does not depend on the
 // order blocks run in.
 
 constexpr float kEscalateBelowConfidence = 0.5f;  // escalate.rs:14-17
@@ -506,53 +573,10 @@ struct EscalateArgs {
     int sad_floor_word, reads_floor;
     float thsad;
     float* state;
+    const float* predictions;  // the coarse search's camera-model window, or null
+    float floor_scale;         // the SAD floor from a fine block to a coarse one
+    float* sad_out;            // winning SADs (conf layout), replaced when a block improves; or null
 };
-
-__device__ __forceinline__ float match_confidence(float sad, float floor, float thsad) {
-    float excess = __fsub_rn(sad, floor);
-    if (excess < 0.0f) excess = 0.0f;
-    const float t2 = __fmul_rn(thsad, thsad);
-    const float e2 = __fmul_rn(excess, excess);
-    const float c = __fdiv_rn(__fsub_rn(t2, e2), __fadd_rn(t2, e2));
-    return c < 0.0f ? 0.0f : c;
-}
-
-template <int R>
-struct WindowScratch {
-    float centre_tile[kMaxBlk * kMaxBlk];
-    float window[(kMaxBlk + 2 * kMaxRadius) * (kMaxBlk + 2 * kMaxRadius)];
-    float sads[(2 * R + 1) * (2 * R + 1)];
-    unsigned long long warp_keys[((2 * R + 1) * (2 * R + 1) + 31) / 32];
-    int best_index;
-};
-
-// The winner of the window around (cdx, cdy), valid at thread 0; every thread must call it.
-template <int R>
-__device__ __forceinline__ void window_best(const SearchLevel& L, int64_t centre_base, int64_t nbr_base, int ox,
-                                            int oy, int cdx, int cdy, WindowScratch<R>& w, int* out_dx, int* out_dy,
-                                            float* out_sad) {
-    constexpr int kSide = 2 * R + 1;
-    score_window<R>(L, centre_base, nbr_base, ox, oy, cdx, cdy, w.centre_tile, w.window, w.sads);
-    window_argmin<R>(w.sads, w.warp_keys, &w.best_index);
-    if (threadIdx.x == 0) {
-        float best_sad = kNoSad;
-        int bdx = cdx, bdy = cdy;
-        if (w.best_index >= 0) {
-            best_sad = w.sads[w.best_index];
-            bdx = cdx + (w.best_index % kSide) - R;
-            bdy = cdy + (w.best_index / kSide) - R;
-        }
-        const float centre_sad = w.sads[R * kSide + R];
-        if (centre_sad <= best_sad) {
-            best_sad = centre_sad;
-            bdx = cdx;
-            bdy = cdy;
-        }
-        *out_dx = bdx;
-        *out_dy = bdy;
-        *out_sad = best_sad;
-    }
-}
 
 __device__ __forceinline__ uint32_t escalate_slot(const EscalateArgs& e, int n, int bx, int by) {
     return static_cast<uint32_t>(n) * e.conf_stride + by * e.L.blocks_x + bx;
@@ -560,45 +584,6 @@ __device__ __forceinline__ uint32_t escalate_slot(const EscalateArgs& e, int n, 
 
 __device__ __forceinline__ int64_t escalate_section(const EscalateArgs& e) {
     return static_cast<int64_t>(e.neighbours) * e.conf_stride;
-}
-
-// The first window's centre of every block: its seed, or no motion.
-__global__ void __launch_bounds__(128) record_centres_kernel(EscalateArgs e) {
-    const int bx = blockIdx.x * blockDim.x + threadIdx.x, by = blockIdx.y, n = blockIdx.z;
-    if (bx >= e.L.blocks_x) return;
-    const int32_t* mv = e.mv_field + static_cast<int64_t>(n) * e.mv_stride + (by * e.L.blocks_x + bx) * 2;
-    const int64_t sec = escalate_section(e);
-    const uint32_t slot = escalate_slot(e, n, bx, by);
-    e.state[kStateCentreX * sec + slot] = e.use_seed ? static_cast<float>(mv[0]) : 0.0f;
-    e.state[kStateCentreY * sec + slot] = e.use_seed ? static_cast<float>(mv[1]) : 0.0f;
-}
-
-// block_match.rs:783-796 with escalate.rs:84-155: the first window again, for its kept SAD and,
-// when the winner sits on the window's outer ring, its edge bar (the lowest SAD off the ring).
-template <int R>
-__global__ void __launch_bounds__(320) track_kernel(EscalateArgs e) {
-    constexpr int kSide = 2 * R + 1;
-    __shared__ WindowScratch<R> w;
-    const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
-    const int64_t sec = escalate_section(e);
-    const uint32_t slot = escalate_slot(e, n, bx, by);
-    const int cdx = static_cast<int>(e.state[kStateCentreX * sec + slot]);
-    const int cdy = static_cast<int>(e.state[kStateCentreY * sec + slot]);
-    const uint32_t nslot = e.neighbour_slots ? e.neighbour_slots[n] : e.slots[n];
-    const int64_t cb = static_cast<int64_t>(e.centre_slot) * e.L.slot_pixels;
-    const int64_t nb = static_cast<int64_t>(nslot) * e.L.slot_pixels;
-    int dx, dy;
-    float sad;
-    window_best<R>(e.L, cb, nb, bx * e.L.step, by * e.L.step, cdx, cdy, w, &dx, &dy, &sad);
-    if (threadIdx.x != 0) return;
-    float bar = 0.0f;
-    if (abs(dx - cdx) == R || abs(dy - cdy) == R) {
-        bar = kNoSad;
-        for (int y = 1; y < kSide - 1; ++y)
-            for (int x = 1; x < kSide - 1; ++x) bar = fminf(bar, w.sads[y * kSide + x]);
-    }
-    e.state[kStateSad * sec + slot] = sad;
-    e.state[kStateFlag * sec + slot] = bar;
 }
 
 __device__ unsigned count_keys(const unsigned* keys, unsigned lo, unsigned hi, unsigned* counter) {
@@ -690,9 +675,9 @@ __global__ void __launch_bounds__(64) flag_kernel(EscalateArgs e) {
     e.state[kStateFlag * sec + slot] = (low || on_edge || closest > kNeighbourDisagreement) ? 1.0f : 0.0f;
 }
 
-// escalate.rs:400-559 (`mc_escalate_search`), without the camera model's candidate.
+// escalate.rs:400-640 (`mc_escalate_search`, `coarse_search`).
 template <int C>
-__global__ void __launch_bounds__(320) escalate_kernel(EscalateArgs e) {
+__global__ void __launch_bounds__(((2 * C + 1) * (2 * C + 1) + 31) / 32 * 32) escalate_kernel(EscalateArgs e) {
     __shared__ WindowScratch<C> w;
     __shared__ int coarse_vec[2];
     const int bx = blockIdx.x, by = blockIdx.y, n = blockIdx.z;
@@ -701,17 +686,26 @@ __global__ void __launch_bounds__(320) escalate_kernel(EscalateArgs e) {
     if (e.state[kStateFlag * sec + slot] == 0.0f) return;  // uniform across the CTA
     const int cdx = static_cast<int>(e.state[kStateCentreX * sec + slot]);
     const int cdy = static_cast<int>(e.state[kStateCentreY * sec + slot]);
-    const float margin = __fmul_rn(kEscalateSadMargin, e.state[kStateSections * sec]);
+    const float sad_floor = e.state[kStateSections * sec];
+    const float margin = __fmul_rn(kEscalateSadMargin, sad_floor);
     const uint32_t nslot = e.neighbour_slots ? e.neighbour_slots[n] : e.slots[n];
-    int dx, dy, kx = 0, ky = 0;
-    float sad;
+    int kx = 0, ky = 0;
     if (e.widen) {
+        // The coarse level again at the ceiling around no motion and, with the camera model, its
+        // prediction, which wins by more than 1/8 of the floor scaled to the coarse block.
         const int64_t cb = e.Lc.level_base + static_cast<int64_t>(e.centre_slot) * e.Lc.slot_pixels;
         const int64_t nb = e.Lc.level_base + static_cast<int64_t>(nslot) * e.Lc.slot_pixels;
-        window_best<C>(e.Lc, cb, nb, bx * e.L.step / e.scale, by * e.L.step / e.scale, 0, 0, w, &kx, &ky, &sad);
+        const int ox = bx * e.L.step / e.scale, oy = by * e.L.step / e.scale;
+        WinBest cbest = window_best<C>(e.Lc, cb, nb, ox, oy, 0, 0, w, false, false);
+        int mdx, mdy;
+        if (model_window(e.predictions, n, ox, oy, e.Lc.blksize, e.scale, e.Lc.width, e.Lc.height, C, 0, 0, &mdx, &mdy)) {
+            const WinBest ch = window_best<C>(e.Lc, cb, nb, ox, oy, mdx, mdy, w, false, false);
+            const float bias = __fmul_rn(__fmul_rn(kModelCandidateBias, sad_floor), e.floor_scale);
+            if (threadIdx.x == 0 && __fadd_rn(ch.sad, bias) < cbest.sad) cbest = ch;
+        }
         if (threadIdx.x == 0) {
-            coarse_vec[0] = kx * e.scale;
-            coarse_vec[1] = ky * e.scale;
+            coarse_vec[0] = cbest.dx * e.scale;
+            coarse_vec[1] = cbest.dy * e.scale;
         }
         __syncthreads();
         kx = coarse_vec[0];
@@ -719,54 +713,35 @@ __global__ void __launch_bounds__(320) escalate_kernel(EscalateArgs e) {
     }
     const int64_t cb = static_cast<int64_t>(e.centre_slot) * e.L.slot_pixels;
     const int64_t nb = static_cast<int64_t>(nslot) * e.L.slot_pixels;
-    window_best<C>(e.L, cb, nb, bx * e.L.step, by * e.L.step, cdx, cdy, w, &dx, &dy, &sad);
+    WinBest best = window_best<C>(e.L, cb, nb, bx * e.L.step, by * e.L.step, cdx, cdy, w, false, false);
     if (e.widen && (kx != cdx || ky != cdy)) {  // uniform: every thread holds the same vectors
-        int dx2, dy2;
-        float sad2;
-        window_best<C>(e.L, cb, nb, bx * e.L.step, by * e.L.step, kx, ky, w, &dx2, &dy2, &sad2);
-        if (threadIdx.x == 0 && __fadd_rn(sad2, margin) < sad) {
-            dx = dx2;
-            dy = dy2;
-            sad = sad2;
-        }
+        const WinBest ch = window_best<C>(e.L, cb, nb, bx * e.L.step, by * e.L.step, kx, ky, w, false, false);
+        if (threadIdx.x == 0 && __fadd_rn(ch.sad, margin) < best.sad) best = ch;
     }
     if (threadIdx.x != 0) return;
-    if (__fadd_rn(sad, margin) < e.state[kStateSad * sec + slot]) {
+    if (__fadd_rn(best.sad, margin) < e.state[kStateSad * sec + slot]) {
         int32_t* mv = e.mv_field + static_cast<int64_t>(n) * e.mv_stride + (by * e.L.blocks_x + bx) * 2;
-        mv[0] = dx;
-        mv[1] = dy;
-        e.state[kStateSad * sec + slot] = sad;
-        if (e.confidence) e.confidence[slot] = match_confidence(sad, e.noise[e.sad_floor_word], e.thsad);
+        mv[0] = best.dx;
+        mv[1] = best.dy;
+        e.state[kStateSad * sec + slot] = best.sad;
+        if (e.sad_out) e.sad_out[slot] = best.sad;
+        if (e.confidence) e.confidence[slot] = match_confidence(best.sad, e.noise[e.sad_floor_word], e.thsad);
     }
 }
 
-template <template <int> class K, int R>
-cudaError_t launch_radius_kernel(int radius, const EscalateArgs& e, dim3 grid, cudaStream_t s) {
+template <int R>
+cudaError_t launch_escalate(int radius, const EscalateArgs& e, dim3 grid, cudaStream_t s) {
     if (radius == R) {
         constexpr int kCand = (2 * R + 1) * (2 * R + 1);
-        K<R>::launch(e, grid, ((kCand + 31) / 32) * 32, s);
+        escalate_kernel<R><<<grid, ((kCand + 31) / 32) * 32, 0, s>>>(e);
         return cudaGetLastError();
     }
     if constexpr (R < kMaxRadius) {
-        return launch_radius_kernel<K, R + 1>(radius, e, grid, s);
+        return launch_escalate<R + 1>(radius, e, grid, s);
     } else {
         return cudaErrorInvalidValue;
     }
 }
-
-template <int R>
-struct TrackLaunch {
-    static void launch(const EscalateArgs& e, dim3 g, int threads, cudaStream_t s) {
-        track_kernel<R><<<g, threads, 0, s>>>(e);
-    }
-};
-
-template <int R>
-struct EscalateLaunch {
-    static void launch(const EscalateArgs& e, dim3 g, int threads, cudaStream_t s) {
-        escalate_kernel<R><<<g, threads, 0, s>>>(e);
-    }
-};
 
 cudaError_t dispatch_search(int radius, bool coarse, const SearchArgs& a, dim3 grid, cudaStream_t s) {
     switch (radius) {
@@ -779,6 +754,7 @@ cudaError_t dispatch_search(int radius, bool coarse, const SearchArgs& a, dim3 g
         case 6: return launch_search<6>(coarse, a, grid, s);
         case 7: return launch_search<7>(coarse, a, grid, s);
         case 8: return launch_search<8>(coarse, a, grid, s);
+        case kAcquisitionRadius: return coarse ? launch_search<kAcquisitionRadius>(true, a, grid, s) : cudaErrorInvalidValue;
         default: return cudaErrorInvalidValue;
     }
 }
@@ -836,23 +812,37 @@ cudaError_t launch_pyramid_build(const float* ring, int channels, int width, int
 
 cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     if (!m.neighbour_slots && m.neighbours > kMaxNeighbours) return cudaErrorInvalidValue;
+    if (m.predictions && !m.noise) return cudaErrorInvalidValue;
     const int step = m.blksize - m.overlap;
     const int blocks_x = (m.width + step - 1) / step > 1 ? (m.width + step - 1) / step : 1;
     const int blocks_y = (m.height + step - 1) / step > 1 ? (m.height + step - 1) / step : 1;
     const bool coarse = m.levels > 1 && !m.seeded;
     const bool seeded = coarse || m.seeded;
-    if (coarse) {
+    const int factor = m.coarse_block_factor > 0 ? m.coarse_block_factor : 1;
+    // analyse.rs:118-157 (`coarse_level`): the smallest level, its blocks `factor` times the content
+    // a fine block covers there, and the SAD floor's scale from a fine block to a coarse one.
+    SearchLevel Lc{};
+    int scale = 1;
+    float floor_scale = 1.0f;
+    if (m.levels > 1) {
         const int level = m.levels - 1;
-        const int scale = 1 << level;
+        scale = 1 << level;
+        pyramid_level_dims(m.width, m.height, level, &Lc.width, &Lc.height);
+        Lc.pyramid = m.pyramid;
+        Lc.level_base = pyramid_level_base(m.width, m.height, m.frame_count, level);
+        Lc.slot_pixels = pyramid_slot_pixels(m.width, m.height, level);
+        Lc.blksize = (m.blksize / scale > 2 ? m.blksize / scale : 2) * factor;
+        Lc.step = step / scale > 1 ? step / scale : 1;
+        Lc.blocks_x = (Lc.width + Lc.step - 1) / Lc.step > 1 ? (Lc.width + Lc.step - 1) / Lc.step : 1;
+        Lc.blocks_y = (Lc.height + Lc.step - 1) / Lc.step > 1 ? (Lc.height + Lc.step - 1) / Lc.step : 1;
+        if (Lc.blksize > kMaxBlk) return cudaErrorInvalidValue;
+        const float coarse_area = static_cast<float>(Lc.blksize * Lc.blksize);
+        const float fine_area = static_cast<float>(m.blksize * m.blksize);
+        floor_scale = coarse_area / fine_area / static_cast<float>(scale);
+    }
+    if (coarse) {
         SearchArgs a{};
-        pyramid_level_dims(m.width, m.height, level, &a.L.width, &a.L.height);
-        a.L.pyramid = m.pyramid;
-        a.L.level_base = pyramid_level_base(m.width, m.height, m.frame_count, level);
-        a.L.slot_pixels = pyramid_slot_pixels(m.width, m.height, level);
-        a.L.blksize = (m.blksize / scale > 2 ? m.blksize / scale : 2) * m.coarse_block_factor;
-        a.L.step = step / scale > 1 ? step / scale : 1;
-        a.L.blocks_x = (a.L.width + a.L.step - 1) / a.L.step > 1 ? (a.L.width + a.L.step - 1) / a.L.step : 1;
-        a.L.blocks_y = (a.L.height + a.L.step - 1) / a.L.step > 1 ? (a.L.height + a.L.step - 1) / a.L.step : 1;
+        a.L = Lc;
         a.neighbour_slots = m.neighbour_slots;
         for (int i = 0; i < kMaxNeighbours; ++i) a.slots[i] = m.inline_slots[i];
         a.centre_slot = m.centre_slot;
@@ -862,8 +852,11 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
         a.fine_blocks_x = blocks_x;
         a.fine_blocks_y = blocks_y;
         a.fine_step = step;
-        if (a.L.blksize > kMaxBlk) return cudaErrorInvalidValue;
-        dim3 grid(a.L.blocks_x, a.L.blocks_y, m.neighbours);
+        a.noise = m.noise;
+        a.sad_floor_word = m.sad_floor_word;
+        a.predictions = m.predictions;
+        a.floor_scale = floor_scale;
+        dim3 grid(Lc.blocks_x, Lc.blocks_y, m.neighbours);
         if (cudaError_t e = dispatch_search(m.coarse_radius, true, a, grid, s)) return e;
         // analyse.rs:268-277 (`keep_seeds`): the coarse field, before the fine pass overwrites it.
         if (m.keep_seeds)
@@ -893,14 +886,19 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     a.noise = m.noise;
     a.sad_floor_word = m.sad_floor_word;
     a.thsad = m.thsad;
+    a.predictions = m.predictions;
+    a.floor_scale = 1.0f;
+    a.sad_out = m.sad;
+    a.sad_means = static_cast<int64_t>(m.neighbours) * m.conf_stride;
     if (a.L.blksize > kMaxBlk) return cudaErrorInvalidValue;
     dim3 grid(blocks_x, blocks_y, m.neighbours);
     const bool escalates = m.escalation && m.ceiling > m.search_radius;
     if (!escalates) return dispatch_search(m.search_radius, false, a, grid, s);
     if (m.ceiling > kMaxRadius || m.thsad <= 0.0f || !m.noise) return cudaErrorInvalidValue;
-    // analyse.rs:234-262 and escalate.rs:19-57: record the first windows' centres, run the first
-    // pass, then keep its SADs and edge bars, measure the floor, flag the failures and search them
-    // again at the ceiling (the coarse level too, when a coarse pass seeded the search).
+    // analyse.rs:234-262 and escalate.rs:19-57: the first pass records each block's kept SAD, edge
+    // bar and winning window's centre; then the floor, the failure flags, and the failures searched
+    // again at the ceiling (the coarse level too, when a coarse pass seeded the search and the
+    // ceiling reaches past its radius, escalate.rs:203-205).
     EscalateArgs e{};
     e.L = a.L;
     e.neighbour_slots = m.neighbour_slots;
@@ -908,20 +906,9 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     e.centre_slot = m.centre_slot;
     e.neighbours = m.neighbours;
     e.use_seed = seeded ? 1 : 0;
-    // escalate.rs:203-205 (`reaches_further`): the coarse level is searched again only when the
-    // ceiling reaches past the coarse pass's own radius.
     e.widen = coarse && m.ceiling > m.coarse_radius ? 1 : 0;
-    e.scale = 1;
-    if (coarse) {
-        const int level = m.levels - 1;
-        e.scale = 1 << level;
-        pyramid_level_dims(m.width, m.height, level, &e.Lc.width, &e.Lc.height);
-        e.Lc.pyramid = m.pyramid;
-        e.Lc.level_base = pyramid_level_base(m.width, m.height, m.frame_count, level);
-        e.Lc.slot_pixels = pyramid_slot_pixels(m.width, m.height, level);
-        e.Lc.blksize = (m.blksize / e.scale > 2 ? m.blksize / e.scale : 2) * m.coarse_block_factor;
-        if (e.Lc.blksize > kMaxBlk) return cudaErrorInvalidValue;
-    }
+    e.scale = scale;
+    e.Lc = Lc;
     e.mv_field = m.mv_field;
     e.mv_stride = m.mv_stride;
     e.confidence = m.confidence;
@@ -931,22 +918,15 @@ cudaError_t launch_motion_search(const MotionLaunch& m, cudaStream_t s) {
     e.reads_floor = m.esc_reads_floor;
     e.thsad = m.thsad;
     e.state = m.escalation;
-    // The register-blocked fine kernel records the state itself; the other fine kernels are followed
-    // by the first window again.
-    const bool blocked = m.search_radius >= 1 && (m.blksize == 8 || m.blksize == 16 || m.blksize == 32);
-    if (blocked) {
-        a.esc_state = e.state;
-        a.esc_section = static_cast<int64_t>(m.neighbours) * m.conf_stride;
-        if (cudaError_t err = dispatch_search(m.search_radius, false, a, grid, s)) return err;
-    } else {
-        const dim3 rows((blocks_x + 127) / 128, blocks_y, m.neighbours);
-        record_centres_kernel<<<rows, 128, 0, s>>>(e);
-        if (cudaError_t err = dispatch_search(m.search_radius, false, a, grid, s)) return err;
-        if (cudaError_t err = launch_radius_kernel<TrackLaunch, 0>(m.search_radius, e, grid, s)) return err;
-    }
+    e.predictions = m.predictions;
+    e.floor_scale = floor_scale;
+    e.sad_out = m.sad;
+    a.esc_state = e.state;
+    a.esc_section = static_cast<int64_t>(m.neighbours) * m.conf_stride;
+    if (cudaError_t err = dispatch_search(m.search_radius, false, a, grid, s)) return err;
     floor_kernel<<<1, kFloorThreads, 0, s>>>(e);
     flag_kernel<<<dim3((blocks_x + 63) / 64, blocks_y, m.neighbours), 64, 0, s>>>(e);
-    return launch_radius_kernel<EscalateLaunch, 0>(m.ceiling, e, grid, s);
+    return launch_escalate<0>(m.ceiling, e, grid, s);
 }
 
 size_t escalation_state_floats(int neighbours, int conf_stride) {

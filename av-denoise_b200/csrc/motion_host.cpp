@@ -72,8 +72,18 @@ AvdStatus avd_motion_search(const AvdMotionPass* p, void* stream) {
     m.blksize = static_cast<int>(p->blksize);
     m.overlap = static_cast<int>(p->overlap);
     m.search_radius = static_cast<int>(p->search_radius);
-    m.coarse_radius = static_cast<int>(p->search_radius);
-    m.coarse_block_factor = 1;
+    m.coarse_radius = static_cast<int>(p->coarse_radius ? p->coarse_radius : p->search_radius);
+    m.coarse_block_factor = p->coarse_block_factor > 1 ? static_cast<int>(p->coarse_block_factor) : 1;
+    if (p->levels > 1 && (m.coarse_radius > 12 || (m.coarse_radius > 8 && m.coarse_radius != 12)))
+        return fail(AVD_ERR_INVALID_OPTIONS, "motion search: coarse_radius must be in 1..=8 or 12");
+    if (p->levels > 1 && m.coarse_block_factor > 4)
+        return fail(AVD_ERR_INVALID_OPTIONS, "motion search: coarse_block_factor must be at most 4");
+    if (p->predictions && !p->noise)
+        return fail(AVD_ERR_INVALID_OPTIONS, "motion search: the camera model needs the noise words");
+    if (p->sad && p->conf_stride < bx * by)
+        return fail(AVD_ERR_INVALID_OPTIONS, "motion search: SAD output needs conf_stride >= blocks");
+    m.predictions = reinterpret_cast<const float*>(p->predictions);
+    m.sad = reinterpret_cast<float*>(p->sad);
     m.levels = static_cast<int>(p->levels);
     m.mv_stride = static_cast<int>(p->mv_stride);
     m.conf_stride = static_cast<int>(p->conf_stride);
@@ -142,6 +152,10 @@ AvdStatus avd_truemotion_pass(const AvdTruemotionPass* p, void* stream) {
     t.surcharge = 0.125f;
     t.fade_level = 2.0f * std::max(p->thsad, 0.0f);
     t.thsad = p->thsad;
+    t.predictions = reinterpret_cast<const float*>(p->predictions);
+    t.sad = reinterpret_cast<float*>(p->sad);
+    if (t.sad && p->conf_stride < bx * by)
+        return fail(AVD_ERR_INVALID_OPTIONS, "truemotion: SAD output needs conf_stride >= blocks");
     cudaError_t e = avd::launch_truemotion(t, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("truemotion launch: ") + cudaGetErrorString(e));
     return AVD_OK;
@@ -301,5 +315,77 @@ AvdStatus avd_exp_mirror(uint64_t x, uint64_t out, uint64_t n, void* stream) {
         avd_set_last_error(cudaGetErrorString(e));
         return AVD_ERR_GPU;
     }
+    return AVD_OK;
+}
+
+// ---- the camera model (include/avd.h) --------------------------------------------------------------
+
+uint64_t avd_model_fit_scratch_floats(uint32_t blocks) {
+    return static_cast<uint64_t>(avd::model_fit_scratch_floats(static_cast<int>(blocks)));
+}
+
+AvdStatus avd_model_fit(const AvdModelFit* p, void* stream) {
+    if (!p || !p->field || !p->models || !p->scratch) return fail(AVD_ERR_NULL_ARG, "model fit: null buffer");
+    if (p->width == 0 || p->height == 0 || p->blksize < 2 || p->blksize > 32 || p->overlap >= p->blksize)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "model fit: bad geometry");
+    if (p->has_contrast && !p->sad) return fail(AVD_ERR_INVALID_OPTIONS, "model fit: contrast needs the SADs");
+    const uint32_t step = p->blksize - p->overlap;
+    const uint32_t bx = std::max<uint32_t>((p->width + step - 1) / step, 1);
+    const uint32_t by = std::max<uint32_t>((p->height + step - 1) / step, 1);
+    if (p->has_contrast && p->means_offset < bx * by)
+        return fail(AVD_ERR_INVALID_OPTIONS, "model fit: means_offset below the block count");
+    if (bx + by > 12 * 1024) return fail(AVD_ERR_INVALID_GEOMETRY, "model fit: block grid too large");
+    avd::ModelFitLaunch l{};
+    l.field = reinterpret_cast<const int32_t*>(p->field);
+    l.sad = reinterpret_cast<const float*>(p->sad);
+    l.has_contrast = p->has_contrast != 0;
+    l.means_offset = static_cast<int>(p->means_offset);
+    l.older_to_newer = p->older_to_newer != 0;
+    l.width = static_cast<int>(p->width);
+    l.height = static_cast<int>(p->height);
+    l.blksize = static_cast<int>(p->blksize);
+    l.step = static_cast<int>(step);
+    l.prior = p->prior;
+    l.models = reinterpret_cast<float*>(p->models);
+    l.slot = static_cast<int>(p->slot);
+    l.scratch = reinterpret_cast<float*>(p->scratch);
+    cudaError_t e = avd::launch_model_fit(l, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("model fit launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+AvdStatus avd_compose_models(uint64_t models, uint64_t gaps, uint64_t out, uint32_t neighbours, uint32_t max_steps,
+                             uint32_t past_neighbours, void* stream) {
+    if (!models || !out || (max_steps && !gaps)) return fail(AVD_ERR_NULL_ARG, "compose models: null buffer");
+    if (neighbours == 0 || past_neighbours > neighbours) return fail(AVD_ERR_INVALID_OPTIONS, "compose models: bad counts");
+    cudaError_t e = avd::launch_compose_models(reinterpret_cast<const float*>(models),
+                                               reinterpret_cast<const uint32_t*>(gaps), reinterpret_cast<float*>(out),
+                                               static_cast<int>(neighbours), static_cast<int>(max_steps),
+                                               static_cast<int>(past_neighbours), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("compose models launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+AvdStatus avd_block_means(uint64_t plane, uint64_t out, uint32_t width, uint32_t height, uint32_t blksize,
+                          uint32_t overlap, void* stream) {
+    if (!plane || !out) return fail(AVD_ERR_NULL_ARG, "block means: null buffer");
+    if (width == 0 || height == 0 || blksize == 0 || overlap >= blksize)
+        return fail(AVD_ERR_INVALID_GEOMETRY, "block means: bad geometry");
+    cudaError_t e = avd::launch_block_means(reinterpret_cast<const float*>(plane), reinterpret_cast<float*>(out),
+                                            static_cast<int>(width), static_cast<int>(height), static_cast<int>(blksize),
+                                            static_cast<int>(blksize - overlap), static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("block means launch: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
+AvdStatus avd_high_pass(uint64_t plane, uint64_t rows, uint64_t out, uint32_t width, uint32_t height, uint32_t radius,
+                        void* stream) {
+    if (!plane || !rows || !out) return fail(AVD_ERR_NULL_ARG, "high pass: null buffer");
+    if (width == 0 || height == 0 || radius > 64) return fail(AVD_ERR_INVALID_GEOMETRY, "high pass: bad geometry");
+    cudaError_t e = avd::launch_high_pass(reinterpret_cast<const float*>(plane), reinterpret_cast<float*>(rows),
+                                          reinterpret_cast<float*>(out), static_cast<int>(width),
+                                          static_cast<int>(height), static_cast<int>(radius),
+                                          static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("high pass launch: ") + cudaGetErrorString(e));
     return AVD_OK;
 }

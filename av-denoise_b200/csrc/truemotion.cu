@@ -17,8 +17,9 @@
 //                       the block's own vector, the ring within the refine radius around it, each
 //                       replacing the best only when strictly cheaper;
 //   mod.rs:448-463, 492-535  the vector, and the confidence max(0, (T^2 - e^2) / (T^2 + e^2)).
-// One pass, no camera-model candidate and no change flags (the stage runs a second pass only after
-// a search that escalates).
+// With the camera model's predictions its point at the block joins the list after zero; with a SAD
+// output every rescored block writes its winning SAD. A second pass, after a search that escalates,
+// reads the change flags of the first.
 //
 // Layout and design: one warp per (block, neighbour), four per CTA, each with its own slice of
 // shared memory: the staged 3x3 field and seeds, the candidate list, a |difference| tile and the
@@ -35,6 +36,7 @@
 
 #include <cstdint>
 
+#include "camera_model.cuh"
 #include "kernels.h"
 
 namespace avd {
@@ -235,6 +237,11 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
             }
         }
         count = push_unique(w.list, count, 0, 0);
+        if (t.predictions && predicts_motion(t.predictions + n * kAffineWords)) {
+            int mdx, mdy;
+            model_point(t.predictions + n * kAffineWords, ox, oy, B, 1, t.width, t.height, &mdx, &mdy);
+            count = push_unique(w.list, count, mdx, mdy);
+        }
         if (seeds) {
             count = push_unique(w.list, count, ss[8], ss[9]);
             for (int corner = 0; corner < 4; ++corner) {
@@ -354,6 +361,7 @@ __global__ void __launch_bounds__(kWarps * 32) truemotion_kernel(TruemotionLaunc
             if (c < 0.0f) c = 0.0f;
             t.confidence[static_cast<int64_t>(n) * t.conf_stride + blk] = c;
         }
+        if (t.sad) t.sad[static_cast<int64_t>(n) * t.conf_stride + blk] = best_sad;
         if (t.changes_out)
             t.changes_out[static_cast<int64_t>(n) * t.conf_stride + blk] =
                 (best_x == field[2 * blk] && best_y == field[2 * blk + 1]) ? 0u : 1u;

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define AVD_ABI_VERSION 4u
+#define AVD_ABI_VERSION 5u
 
 #if defined(__GNUC__)
 #define AVD_API __attribute__((visibility("default")))
@@ -486,9 +486,9 @@ AVD_API AvdStatus avd_motion_pyramid_build(uint64_t ring, uint32_t channels, uin
                                            uint32_t frame_count, uint32_t ring_slot, uint32_t levels,
                                            uint64_t pyramid, uint32_t pyramid_slot, void* stream);
 
-/* One block-matching motion search over a built pyramid, as `run_analyse` runs it without the
- * camera-model candidate, before its truemotion stage (av-denoise-core/src/motion/analyse.rs:170-266),
- * and as `run_confidence` runs it with `search_radius` 0 and one level (motion/confidence.rs:39-66). */
+/* One block-matching motion search over a built pyramid, as `run_analyse` runs it before its
+ * truemotion stage (av-denoise-core/src/motion/analyse.rs:170-266), and as `run_confidence` runs it
+ * with `search_radius` 0 and one level (motion/confidence.rs:39-66). */
 typedef struct AvdMotionPass {
     uint64_t pyramid;         /* f32, avd_motion_pyramid_floats(width, height, frame_count, levels) */
     uint64_t neighbour_slots; /* u32 pyramid slot of each neighbour */
@@ -510,6 +510,16 @@ typedef struct AvdMotionPass {
     uint32_t ceiling;         /* motion/context.rs:55-71: max_search_escalation; at most 8 */
     uint32_t esc_reads_floor; /* 1: a positive noise word `sad_floor_word` is the escalation floor; else it
                                * is measured from the first pass's SADs (escalate.rs:168-257) */
+    uint64_t predictions; /* f32, 6 words per neighbour (m00 m01 m10 m11 tx ty): the camera model's
+                           * prediction, a second search window at every level when it moves anything
+                           * and lies outside the first, winning by more than 1/8 of noise word
+                           * `sad_floor_word` (motion/kernels/candidates.rs, block_match.rs:98-265);
+                           * 0 = no camera model (`noise` is then optional) */
+    uint64_t sad;         /* f32, 2 * neighbours * conf_stride: each block's winning SAD, then its window's
+                           * mean SAD (analyse.rs:41-60); 0 = not written */
+    uint32_t coarse_radius;       /* motion/context.rs:34-37: the coarse pass's radius, 1..=8 or 12;
+                                   * 0 = search_radius */
+    uint32_t coarse_block_factor; /* context.rs:38-40: coarse blocks this many times wider; 0 or 1 = 1 */
 } AvdMotionPass;
 
 /* The f32 values the escalation state of a search over `neighbours` neighbours holds: four
@@ -519,9 +529,9 @@ AVD_API uint64_t avd_escalation_state_floats(uint32_t neighbours, uint32_t conf_
 AVD_API AvdStatus avd_motion_search(const AvdMotionPass* pass, void* stream);
 
 /* One pass of the truemotion stage that ends a search (av-denoise-core/src/motion/truemotion/
- * stage.rs:29-145 with kernels/truemotion/mod.rs:560-763), without the camera-model candidate:
- * every block of every neighbour picks its vector in `mv_in` again from its own vector, its 3x3
- * lower median, its four adjacent blocks' vectors, zero and, with `seeds`, its own and its four
+ * stage.rs:29-145 with kernels/truemotion/mod.rs:560-763): every block of every neighbour picks its
+ * vector in `mv_in` again from its own vector, its 3x3 lower median, its four adjacent blocks'
+ * vectors, zero, with `predictions` the camera model's point, and with `seeds` its own and its four
  * diagonal blocks' seeds, at cost SAD + lambda * |v - median|_1 (+ SAD / 8 off the median), with
  * lambda = field_lambda * blksize^2 * 0.02 + field_lambda * floor faded by the median's excess SAD
  * over 2 * thsad, then the ring of radius 1 around a new winner. The floor is noise word
@@ -539,7 +549,49 @@ typedef struct AvdTruemotionPass {
     uint32_t blksize, overlap, mv_stride, conf_stride, sad_field, reads_floor;
     float field_lambda; /* > 0 */
     float thsad;
+    uint64_t predictions; /* f32, 6 words per neighbour; 0 = no camera-model candidate */
+    uint64_t sad;         /* f32 per block per neighbour, `conf_stride` apart: each block's winning SAD;
+                           * 0 = not written */
 } AvdTruemotionPass;
+
+/* ---- the camera model (av-denoise-core/src/motion/global, motion/kernels/global.rs) -------------
+ * A pair model is 5 f32 words (a, b, tx, ty, valid) mapping a luma position of the older frame into
+ * the newer one: x' = a x - b y + tx, y' = b x + a y + ty (global/model.rs:6-10). */
+
+/* global/fit.rs:196-250 (`run_model_fit`): fits one direction of a pair field into ring slot `slot`
+ * of `models`, starting from ring slot `prior` when it is valid and would be accepted (-1: none).
+ * `sad` (0 = none) holds each block's winning SAD and, with `has_contrast`, its window mean SAD and its
+ * mean sample, `means_offset` values apart. `scratch` holds avd_model_fit_scratch_floats(blocks) f32;
+ * its first 8 words end as the fit's state. */
+typedef struct AvdModelFit {
+    uint64_t field;   /* i32 (dx, dy) per block: one direction of a pair field */
+    uint64_t sad;
+    uint32_t has_contrast, means_offset, older_to_newer;
+    uint32_t width, height, blksize, overlap;
+    int32_t prior;
+    uint64_t models;
+    uint32_t slot;
+    uint64_t scratch;
+} AvdModelFit;
+
+AVD_API uint64_t avd_model_fit_scratch_floats(uint32_t blocks);
+AVD_API AvdStatus avd_model_fit(const AvdModelFit* fit, void* stream);
+
+/* global/compose.rs:66-101 (`run_compose_models`) with kernels/global.rs:18-119: one prediction per
+ * neighbour from the ring `models` and the device gap table `gaps` (`max_steps` ring slots per
+ * neighbour from the centre outward, 0xFFFFFFFF for none); the first `past_neighbours` lie behind the
+ * centre. `out` takes 6 f32 per neighbour. */
+AVD_API AvdStatus avd_compose_models(uint64_t models, uint64_t gaps, uint64_t out, uint32_t neighbours,
+                                     uint32_t max_steps, uint32_t past_neighbours, void* stream);
+
+/* motion/kernels/global.rs:121-155 (`mc_block_means`): each block's mean sample of an f32 plane. */
+AVD_API AvdStatus avd_block_means(uint64_t plane, uint64_t out, uint32_t width, uint32_t height, uint32_t blksize,
+                                  uint32_t overlap, void* stream);
+
+/* motion/kernels/pyramid.rs:66-132 (`mc_box_rows`, `mc_high_pass_cols`): an f32 plane minus its
+ * (2 radius + 1)^2 box mean into `out`; `rows` is a plane of scratch. */
+AVD_API AvdStatus avd_high_pass(uint64_t plane, uint64_t rows, uint64_t out, uint32_t width, uint32_t height,
+                                uint32_t radius, void* stream);
 
 AVD_API AvdStatus avd_truemotion_pass(const AvdTruemotionPass* pass, void* stream);
 
