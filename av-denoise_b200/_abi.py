@@ -257,6 +257,7 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_motion_search": (C.c_int, [_P(AvdMotionPass), C.c_void_p]),
     "avd_truemotion_pass": (C.c_int, [_P(AvdTruemotionPass), C.c_void_p]),
     "avd_escalation_state_floats": (u64, [u32, u32]),
+    "avd_engine_models": (C.c_int, [_E, _P(f32), u32, _P(u32)]),
     "avd_model_fit_scratch_floats": (u64, [u32]),
     "avd_model_fit": (C.c_int, [_P(AvdModelFit), C.c_void_p]),
     "avd_compose_models": (C.c_int, [u64, u64, u64, u32, u32, u32, C.c_void_p]),

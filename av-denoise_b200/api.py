@@ -598,6 +598,20 @@ class Engine:
         self._check(self._lib.avd_engine_max_held_frames(self._h, C.byref(out)))
         return out.value
 
+    def camera_models(self):
+        """The camera-model ring after the queued work, (depth, 5) f32 (a, b, tx, ty, valid; stream
+        frame f in row f % depth), or None when the engine fits no models (engine/spec.rs:403-415)."""
+        import numpy as np
+
+        depth = C.c_uint32(0)
+        self._check(self._lib.avd_engine_models(self._h, None, 0, C.byref(depth)))
+        if depth.value == 0:
+            return None
+        out = np.zeros(depth.value * 5, np.float32)
+        self._check(self._lib.avd_engine_models(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size,
+                                                C.byref(depth)))
+        return out.reshape(depth.value, 5)
+
     def timing(self) -> PassTimings:
         out = _abi.AvdPassTimings()
         self._check(self._lib.avd_engine_timing(self._h, C.byref(out)))

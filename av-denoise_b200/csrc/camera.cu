@@ -62,9 +62,9 @@ enum BandWord { kTop = 0, kBottom = 1, kLeft = 2, kRight = 3 };
 
 __device__ __forceinline__ int clamp_to(int v, int limit) { return v < 0 ? 0 : (v >= limit ? limit - 1 : v); }
 
-__global__ void __launch_bounds__(32) compose_kernel(const float* __restrict__ models, const uint32_t* __restrict__ gaps,
-                                                     float* __restrict__ out, int neighbours, int max_steps,
-                                                     int past_neighbours) {
+__device__ __forceinline__ void compose_one(const float* __restrict__ models, const uint32_t* __restrict__ gaps,
+                                            float* __restrict__ out, int neighbours, int max_steps,
+                                            int past_neighbours) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= neighbours) return;
     const bool past = n < past_neighbours;
@@ -111,6 +111,23 @@ __global__ void __launch_bounds__(32) compose_kernel(const float* __restrict__ m
     o[3] = acc_a;
     o[4] = acc_tx;
     o[5] = acc_ty;
+}
+
+__global__ void __launch_bounds__(32) compose_kernel(const float* __restrict__ models, const uint32_t* __restrict__ gaps,
+                                                     float* __restrict__ out, int neighbours, int max_steps,
+                                                     int past_neighbours) {
+    compose_one(models, gaps, out, neighbours, max_steps, past_neighbours);
+}
+
+// The same composition with the gap table passed by value, for tables the host builds per window.
+struct InlineGaps {
+    uint32_t g[kMaxInlineGaps];
+};
+
+__global__ void __launch_bounds__(32) compose_inline_kernel(const float* __restrict__ models, InlineGaps gaps,
+                                                            float* __restrict__ out, int neighbours, int max_steps,
+                                                            int past_neighbours) {
+    compose_one(models, gaps.g, out, neighbours, max_steps, past_neighbours);
 }
 
 __global__ void __launch_bounds__(256) block_means_kernel(const float* __restrict__ plane, float* __restrict__ out,
@@ -498,6 +515,17 @@ cudaError_t launch_compose_models(const float* models, const uint32_t* gaps, flo
                                   int past_neighbours, cudaStream_t s) {
     if (!models || !gaps || !out || neighbours < 1 || max_steps < 0) return cudaErrorInvalidValue;
     compose_kernel<<<(neighbours + 31) / 32, 32, 0, s>>>(models, gaps, out, neighbours, max_steps, past_neighbours);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compose_inline(const float* models, const uint32_t* host_gaps, float* out, int neighbours,
+                                  int max_steps, int past_neighbours, cudaStream_t s) {
+    if (!models || !out || neighbours < 1 || max_steps < 0 || neighbours * max_steps > kMaxInlineGaps)
+        return cudaErrorInvalidValue;
+    InlineGaps gaps{};
+    for (int i = 0; i < neighbours * max_steps; ++i) gaps.g[i] = host_gaps[i];
+    compose_inline_kernel<<<(neighbours + 31) / 32, 32, 0, s>>>(models, gaps, out, neighbours, max_steps,
+                                                                past_neighbours);
     return cudaGetLastError();
 }
 

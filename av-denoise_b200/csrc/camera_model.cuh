@@ -5,10 +5,9 @@
 
 #include <cuda_runtime.h>
 
-namespace avd {
+#include "kernels.h"
 
-constexpr int kAffineWords = 6;  // a prediction: m00 m01 m10 m11 tx ty
-constexpr int kModelWords = 5;   // a pair model: a b tx ty valid (global/model.rs:6-10)
+namespace avd {
 
 // candidates.rs:123-134 (`predicts_motion`): whether the prediction `p` moves anything.
 __device__ __forceinline__ bool predicts_motion(const float* p) {

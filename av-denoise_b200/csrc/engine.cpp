@@ -158,6 +158,29 @@ class NlmPass final : public Pass {
         return Failure{AVD_ERR_GPU, "forced failure"};
     }
 
+    std::optional<std::pair<PairModelMode, int>> pair_model_mode() const override {
+        if (!mc_ || reads_share_) return std::nullopt;
+        const AvdMotionSearch& m = params_.motion.search;
+        PairModelMode mode;
+        mode.blksize = static_cast<int>(m.blksize);
+        mode.overlap = static_cast<int>(m.overlap);
+        mode.search_radius = static_cast<int>(m.search_radius);
+        mode.ceiling = mc_ceiling_;
+        mode.levels = static_cast<int>(m.pyramid_levels);
+        return std::make_pair(mode, static_cast<int>(params_.temporal_radius));
+    }
+
+    std::optional<Failure> attach_models(const PairModels* models) override {
+        if (!mc_ || reads_share_) return std::nullopt;
+        models_ = models;
+        cudaError_t e = pred_window_.alloc(2 * params_.temporal_radius * kAffineWords * sizeof(float));
+        if (e == cudaSuccess) e = pred_pair_.alloc(2 * kAffineWords * sizeof(float));
+        if (e != cudaSuccess) return gpu_failure("prediction buffers", e);
+        if (measures_)
+            if (auto f = noise_.attach_models(models)) return f;
+        return std::nullopt;
+    }
+
    private:
     NlmPass() = default;
 
@@ -561,6 +584,13 @@ class NlmPass final : public Pass {
         }
         if (ring_head_ == 0) return std::nullopt;
         const size_t older = (slot + total_frames() - 1) % total_frames();
+        // stages.rs:15-22, 172-180 with seeds.rs:104-134: both directions' predictions between the
+        // older slot's frame and the frame entering now (its slot records it after this search), the
+        // searches scored against zeroed noise words.
+        if (models_)
+            if (auto f = models_->compose_pair(slot_frames_[older], static_cast<uint32_t>(real_pushes_), pred_pair_.as<float>(),
+                                               pred_pair_.as<float>() + kAffineWords, stream))
+                return f;
         for (int dir = 0; dir < 2; ++dir) {
             MotionLaunch m = mc_launch();
             m.inline_slots[0] = static_cast<uint32_t>(dir == 0 ? slot : older);
@@ -568,6 +598,10 @@ class NlmPass final : public Pass {
             m.neighbours = 1;
             m.mv_field = pair + dir * mc_mv_stride_;
             m.confidence = nullptr;
+            if (models_) {
+                m.predictions = pred_pair_.as<float>() + dir * kAffineWords;
+                m.noise = models_->zero_noise();
+            }
             // motion/chain.rs:54-62: each direction ends with the stage at the unscaled penalty.
             if (auto f = search_then_truemotion(m, false)) return f;
         }
@@ -613,6 +647,7 @@ class NlmPass final : public Pass {
         t.surcharge = 0.125f;
         t.fade_level = 2.0f * std::max(m.thsad, 0.0f);
         t.thsad = m.thsad;
+        t.predictions = m.predictions;
         if (two_passes) {
             // truemotion/stage.rs:82-142: the second pass reads the first's field back into the
             // search's and rescores only the blocks next to one the first changed.
@@ -690,6 +725,14 @@ class NlmPass final : public Pass {
             if ((e = launch_motion_search(m, stream)) != cudaSuccess) return gpu_failure("seeded refine launch", e);
         } else {
             m.esc_reads_floor = 1;
+            if (models_) {
+                // dispatch/motion.rs:190-195 with seeds.rs:136-160: every neighbour's prediction for
+                // the window's stream frames (the chained seeds already carry the camera's motion).
+                uint32_t frames[2 * kMaxTemporalRadius + 1];
+                for (int l = 0; l <= 2 * d; ++l) frames[l] = slot_frames_[phys_frame(l)];
+                if (auto f = models_->compose_window(frames, 2 * d + 1, d, pred_window_.as<float>(), stream)) return f;
+                m.predictions = pred_window_.as<float>();
+            }
             if (auto f = search_then_truemotion(m, true)) return f;
         }
         if (writes_share_) {
@@ -996,6 +1039,8 @@ class NlmPass final : public Pass {
     static constexpr int kFixedSadFloor = 4;  // the window search's floor among the fixed words
 
     bool mc_ = false, mc_chained_ = false, mc_conf_ = false;
+    const PairModels* models_ = nullptr;  // the camera models the searches start from, or none
+    DeviceBuffer pred_window_, pred_pair_;  // window predictions (2d x 6), pair predictions (2 x 6)
     int mc_refine_radius_ = 2, mc_bx_ = 1, mc_by_ = 1, mc_mv_stride_ = 2, mc_conf_stride_ = 1;
     int mc_ceiling_ = 0;  // the escalation ceiling; 0 when the search does not escalate
     DeviceBuffer mc_pyr_, mc_ref_pyr_, comp_, comp_ref_, mc_mv_, tm_seeds_, tm_field_, mc_conf_buf_, pair_ring_;
@@ -1080,6 +1125,7 @@ struct AvdEngine {
     std::unique_ptr<avd::Pass> luma, chroma;
     std::unique_ptr<avd::PassthroughRing> passthrough;
     std::unique_ptr<avd::ColourMeans> colour;  // the block means the passes pool their grain per colour with
+    std::unique_ptr<avd::PairModels> models;   // the camera models the luma motion pass searches from
     bool passthrough_luma = false;  // which group the ring holds
     bool luma_guides = false;       // `luma` is a chroma-only engine's luma guide, which cleans nothing
     bool poisoned = false;
@@ -1104,6 +1150,15 @@ AvdStatus fail_global(AvdStatus st, const std::string& message) {
 AvdStatus record(AvdEngine* e, AvdStatus st, const std::string& message) {
     if (e) e->last_error = st == AVD_OK ? std::string() : message;
     return st;
+}
+
+// planar.rs:253-268 (`fit_pair_model`): stream frame `frame`'s camera model from its luma plane, before
+// its passes see it; a failure poisons the engine, as the ring may hold a partly written model.
+std::optional<Failure> fit_pair_model(AvdEngine* e, const AvdPlane* planes, uint32_t frame) {
+    if (!e->models) return std::nullopt;
+    auto f = e->models->push(planes[0], frame, e->stream);
+    if (f) e->poisoned = true;
+    return f;
 }
 
 // planar.rs:194-217 (`measure_colour`): stream frame `frame`'s block means from all three planes,
@@ -1256,6 +1311,17 @@ AvdStatus avd_engine_create(const AvdEngineSpec* spec, const AvdTuning* tuning, 
                                            *static_cast<avd::NlmPass*>(engine->chroma.get()), shift_x, shift_y);
         if (f) return fail_global(f->status, f->message);
     }
+    if (engine->luma) {
+        // engine/spec.rs:426-450 (`pair_model_producer`): with a pass that searches luma motion over a
+        // window, camera models fitted on the luma plane with that pass's search, in a ring covering
+        // the frames the engine holds, the window and two more.
+        if (auto mode = engine->luma->pair_model_mode()) {
+            const size_t depth = engine->lead()->max_held_frames() + (2 * static_cast<size_t>(mode->second) + 1) + 2;
+            engine->models = std::make_unique<avd::PairModels>();
+            if (auto f = engine->models->allocate(g, mode->first, depth)) return fail_global(f->status, f->message);
+            if (auto f = engine->luma->attach_models(engine->models.get())) return fail_global(f->status, f->message);
+        }
+    }
     const bool gray = g.chroma == AVD_CHROMA_GRAY;
     const bool cleans_luma = engine->luma != nullptr && !engine->luma_guides;
     {
@@ -1316,6 +1382,7 @@ AvdStatus avd_engine_push(AvdEngine* e, const AvdPlane* planes, size_t n, size_t
     if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
     if (auto f = check_frame_planes(e->geometry, planes, n, e->geometry.input)) return record(e, f);
     const uint32_t frame = e->lead()->next_frame();
+    if (auto f = fit_pair_model(e, planes, frame)) return record(e, f);
     if (auto f = measure_colour(e, planes, frame)) return record(e, f);
     size_t value = 0;
     auto f = forward(e, &value, [&](avd::Pass* p, bool luma, size_t* v) {
@@ -1341,6 +1408,7 @@ AvdStatus avd_engine_push_context(AvdEngine* e, const AvdPlane* planes, size_t n
     if (e->poisoned) return record(e, AVD_ERR_NEEDS_RESET, avd_status_message(AVD_ERR_NEEDS_RESET));
     if (auto f = check_frame_planes(e->geometry, planes, n, e->geometry.input)) return record(e, f);
     const uint32_t frame = e->lead()->next_frame();
+    if (auto f = fit_pair_model(e, planes, frame)) return record(e, f);
     if (auto f = measure_colour(e, planes, frame)) return record(e, f);
     auto f = forward(e, nullptr, [&](avd::Pass* p, bool luma, size_t* v) {
         *v = 0;
@@ -1398,7 +1466,21 @@ AvdStatus avd_engine_reset(AvdEngine* e) {
     if (e->luma) e->luma->reset();
     if (e->chroma) e->chroma->reset();
     if (e->colour) e->colour->clear();
+    if (e->models) e->models->reset();
     e->poisoned = false;
+    return record(e, AVD_OK, "");
+}
+
+AvdStatus avd_engine_models(AvdEngine* e, float* out, uint32_t capacity, uint32_t* depth) {
+    if (!e || !depth) return AVD_ERR_NULL_ARG;
+    DeviceGuard dg(e->device);
+    *depth = e->models ? static_cast<uint32_t>(e->models->depth()) : 0u;
+    if (!e->models || !out) return record(e, AVD_OK, "");
+    const size_t words = e->models->depth() * avd::kModelWords;
+    if (capacity < words) return record(e, AVD_ERR_INVALID_OPTIONS, "camera models: buffer below depth * 5 words");
+    cudaError_t err = cudaStreamSynchronize(e->stream);
+    if (err == cudaSuccess) err = cudaMemcpy(out, e->models->ring(), words * sizeof(float), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return record(e, AVD_ERR_GPU, avd::cuda_message("camera models read", err));
     return record(e, AVD_OK, "");
 }
 

@@ -151,6 +151,50 @@ float colour_grain_scale(const AvdSampleFormat& f);
 float colour_eight_bit_scale(const AvdSampleFormat& f);
 
 // ---------------------------------------------------------------------------------------------
+// The camera models (motion/global/producer.rs `PairModelProducer`, nlmeans/denoiser/seeds.rs
+// `ModelSeeds`): one similarity per adjacent pair of pushed luma frames, fitted before the passes
+// see the frame, and composed into the predictions the luma motion pass searches from. Stream frame
+// f's model (the pair f - 1 -> f) keeps ring slot f % depth; the ring covers the frames the passes
+// hold and their window, so a window never reads a slot a newer frame took.
+struct PairModelMode {
+    int blksize = 16, overlap = 8, search_radius = 4, ceiling = 0, levels = 2;
+};
+
+class PairModels {
+   public:
+    std::optional<Failure> allocate(const AvdGeometry& g, const PairModelMode& mode, size_t depth);
+    // producer.rs:327-372 (`push`): fits the pair from stream frame `frame - 1` to `frame` from the
+    // luma plane; a frame that does not follow the last one pushed starts a run and writes identity.
+    std::optional<Failure> push(const AvdPlane& luma, uint32_t frame, cudaStream_t s);
+    void reset() { running_ = false; }
+    // seeds.rs:136-160: the prediction of every neighbour of a window of stream frames (positions
+    // before `centre` lie behind it), 6 floats each, into `out`.
+    std::optional<Failure> compose_window(const uint32_t* window_frames, int count, int centre, float* out,
+                                          cudaStream_t s) const;
+    // seeds.rs:104-134: the pair's predictions older -> newer (when `older_to_newer` is set) and newer
+    // -> older; a pair that does not step one frame predicts no motion.
+    std::optional<Failure> compose_pair(uint32_t older, uint32_t newer, float* older_to_newer, float* newer_to_older,
+                                        cudaStream_t s) const;
+    // Zeroed noise words: a pair search with predictions keeps its seed only on exact ties.
+    const float* zero_noise() const { return zero_noise_.as<float>(); }
+    const float* ring() const { return models_.as<float>(); }
+    size_t depth() const { return depth_; }
+
+   private:
+    uint32_t slot(uint32_t frame) const { return static_cast<uint32_t>(frame % depth_); }
+    std::optional<Failure> match(bool deep, int older, int newer, cudaStream_t s);
+
+    AvdGeometry geometry_{};
+    PairModelMode mode_{};
+    size_t depth_ = 0;
+    int blocks_x_ = 0, blocks_y_ = 0, mv_stride_ = 0, conf_stride_ = 0;
+    bool running_ = false;
+    uint32_t run_first_ = 0, run_last_ = 0;
+    DeviceBuffer models_, luma_, rows_, high_, pyramid_, field_, sad_, predictions_, seeds_, tm_field_, changes_,
+        escalation_, scratch_, zero_noise_;
+};
+
+// ---------------------------------------------------------------------------------------------
 // A pass over one plane group.
 class Pass {
    public:
@@ -169,6 +213,12 @@ class Pass {
     virtual std::optional<Failure> fail_for_test() = 0;
     // Whether the pass pools its measured grain into colour cells (nl4d/engine.rs:405-411), and the
     // block means it does so with, on the luma or the chroma grid (engine/planar.rs:176-192).
+    // engine/spec.rs:426-450 (`pair_model_producer`): the search of a pass that estimates luma
+    // motion over a window, which the camera models fit with, and its temporal radius.
+    virtual std::optional<std::pair<PairModelMode, int>> pair_model_mode() const { return std::nullopt; }
+    // nlmeans/denoiser/seeds.rs:162-208 (`set_shared_motion`): the pass's own searches start from the
+    // camera models too (a pass that refines luma motion runs no search and takes none).
+    virtual std::optional<Failure> attach_models(const PairModels*) { return std::nullopt; }
     virtual bool measures_colour() const { return false; }
     virtual std::optional<Failure> measure_colour(const ColourMeans*, bool) { return std::nullopt; }
     cudaStream_t stream = nullptr;
@@ -196,6 +246,9 @@ class NoiseFront {
     NoiseFront& operator=(const NoiseFront&) = delete;
     ~NoiseFront();
     std::optional<Failure> allocate(const NoiseFrontConfig& cfg);
+    // lookahead.rs:310-316 and seeds.rs:104-134: the look-ahead's pair searches also search around
+    // the camera models' pair predictions, keeping their seed only on exact ties.
+    std::optional<Failure> attach_models(const PairModels* models);
     // Orders a write into a look-ahead slot on `main` after the reads queued on the side stream.
     std::optional<Failure> before_ingest(cudaStream_t main);
     // The look-ahead slot of stream frame `frame`.
@@ -235,6 +288,8 @@ class NoiseFront {
     // The derived words the look-ahead's searches read: a copy taken as each push's reads start, so
     // they read the previous push's fold whatever the pass's fold on the main stream writes meanwhile.
     DeviceBuffer search_words_;
+    const PairModels* models_ = nullptr;
+    DeviceBuffer pair_predictions_;  // older -> newer, then newer -> older, 6 floats each
     size_t capacity_ = 0, pushed_ = 0, released_ = 0, recorded_ = 0;
     int step_ = 8, blocks_x_ = 1, blocks_y_ = 1, mv_stride_ = 2, conf_stride_ = 1;
     DeviceBuffer lookahead_, partials_, records_, scratch_, history_records_, history_results_, settings_, state_,

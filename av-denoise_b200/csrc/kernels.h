@@ -212,6 +212,9 @@ struct TruemotionLaunch {
 cudaError_t launch_truemotion(const TruemotionLaunch& args, cudaStream_t stream);
 
 // ---- the camera model (camera.cu; av-denoise-core/src/motion/global, kernels/global.rs) ------------
+
+constexpr int kAffineWords = 6;  // a prediction: m00 m01 m10 m11 tx ty
+constexpr int kModelWords = 5;   // a pair model: a b tx ty valid (global/model.rs:6-10)
 //
 // A pair model is 5 f32 words (a, b, tx, ty, valid) mapping a luma position of the older frame into
 // the newer one, x' = a x - b y + tx, y' = b x + a y + ty; a prediction is 6 words (m00 m01 m10 m11
@@ -238,6 +241,11 @@ cudaError_t launch_model_fit(const ModelFitLaunch& args, cudaStream_t stream);
 // global.rs:18-119 (`mc_compose_models`): `gaps` holds `max_steps` ring slots (or 0xFFFFFFFF) per
 // neighbour, from the centre outward; the first `past_neighbours` neighbours lie behind the centre.
 cudaError_t launch_compose_models(const float* models, const uint32_t* gaps, float* out, int neighbours,
+                                  int max_steps, int past_neighbours, cudaStream_t stream);
+// The same with a host gap table of neighbours * max_steps entries (at most kMaxInlineGaps), passed
+// to the kernel by value.
+constexpr int kMaxInlineGaps = 256;
+cudaError_t launch_compose_inline(const float* models, const uint32_t* host_gaps, float* out, int neighbours,
                                   int max_steps, int past_neighbours, cudaStream_t stream);
 // global.rs:121-155 (`mc_block_means`) on the block grid of blksize / step.
 cudaError_t launch_block_means(const float* plane, float* out, int width, int height, int blksize, int step,

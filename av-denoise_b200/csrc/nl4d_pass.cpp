@@ -198,6 +198,27 @@ class Nl4dPass final : public Pass {
         poisoned_ = true;
         return Failure{AVD_ERR_GPU, "forced failure"};
     }
+    std::optional<std::pair<PairModelMode, int>> pair_model_mode() const override {
+        if (d_ == 0 || reads_share_) return std::nullopt;
+        PairModelMode mode;
+        mode.blksize = static_cast<int>(opts_.motion.blksize);
+        mode.overlap = static_cast<int>(opts_.motion.overlap);
+        mode.search_radius = static_cast<int>(opts_.motion.search_radius);
+        mode.ceiling = ceiling_;
+        mode.levels = static_cast<int>(opts_.motion.pyramid_levels);
+        return std::make_pair(mode, static_cast<int>(d_));
+    }
+    // nl4d/denoiser.rs:463-466 with nlmeans/denoiser/seeds.rs:162-208.
+    std::optional<Failure> attach_models(const PairModels* models) override {
+        if (d_ == 0 || reads_share_) return std::nullopt;
+        models_ = models;
+        cudaError_t e = pred_window_.alloc(2 * d_ * kAffineWords * sizeof(float));
+        if (e == cudaSuccess) e = pred_pair_.alloc(2 * kAffineWords * sizeof(float));
+        if (e != cudaSuccess) return gpu_failure("prediction buffers", e);
+        if (measures_)
+            if (auto f = noise_.attach_models(models)) return f;
+        return std::nullopt;
+    }
 
    private:
     Nl4dPass() = default;
@@ -477,6 +498,13 @@ class Nl4dPass final : public Pass {
         if (!chained_ || ring_head_ == 0) return std::nullopt;
         const size_t older = (newer + tf() - 1) % tf();
         int32_t* pair = pair_ring_.as<int32_t>() + (ring_head_ % (2 * d_)) * 2 * mv_stride_;
+        // stages.rs:15-22, 172-180 with seeds.rs:104-134: both directions' predictions between the
+        // older slot's frame and the frame entering now (its slot records it after this search), the
+        // searches scored against zeroed noise words.
+        if (models_)
+            if (auto f = models_->compose_pair(slot_frames_[older], static_cast<uint32_t>(real_pushes_), pred_pair_.as<float>(),
+                                               pred_pair_.as<float>() + kAffineWords, stream))
+                return f;
         for (int dir = 0; dir < 2; ++dir) {
             MotionLaunch m = search_launch();
             m.neighbour_slots = nullptr;
@@ -485,6 +513,10 @@ class Nl4dPass final : public Pass {
             m.neighbours = 1;
             m.mv_field = pair + dir * mv_stride_;
             m.confidence = nullptr;
+            if (models_) {
+                m.predictions = pred_pair_.as<float>() + dir * kAffineWords;
+                m.noise = models_->zero_noise();
+            }
             // motion/chain.rs:54-62: each direction ends with the stage at the unscaled penalty.
             if (auto f = search_then_truemotion(m, false)) return f;
         }
@@ -533,6 +565,7 @@ class Nl4dPass final : public Pass {
         t.lambda_noise = lambda * 1.0f;
         t.surcharge = 0.125f;
         t.fade_level = 2.0f * std::max(m.thsad, 0.0f);
+        t.predictions = m.predictions;
         t.thsad = m.thsad;
         if (two_passes) {
             // truemotion/stage.rs:82-142: the second pass reads the first's field back into the
@@ -730,6 +763,16 @@ class Nl4dPass final : public Pass {
             m.escalation = esc_state_.as<float>();
             m.ceiling = ceiling_;
             m.esc_reads_floor = 1;
+        }
+        if (models_) {
+            // dispatch/motion.rs:190-195 with seeds.rs:136-160: every neighbour's prediction for the
+            // window's stream frames (the chained seeds already carry the camera's motion).
+            uint32_t frames[2 * kMaxTemporalRadius + 1];
+            for (uint32_t l = 0; l < tf(); ++l) frames[l] = slot_frames_[phys(l)];
+            if (auto f = models_->compose_window(frames, static_cast<int>(tf()), static_cast<int>(centre),
+                                                 pred_window_.as<float>(), stream))
+                return f;
+            m.predictions = pred_window_.as<float>();
         }
         // nlmeans/dispatch/motion.rs:201-206: the window's floor scales the stage's penalty.
         return search_then_truemotion(m, true);
@@ -935,6 +978,8 @@ class Nl4dPass final : public Pass {
     bool writes_share_ = false, reads_share_ = false;
     bool guides_ = false;  // a chroma-only engine's luma pass: motion only (engine/spec.rs:220-236)
     bool chained_ = false;
+    const PairModels* models_ = nullptr;  // the camera models the searches start from, or none
+    DeviceBuffer pred_window_, pred_pair_;  // window predictions (2d x 6), pair predictions (2 x 6)
     int refine_radius_ = 2;
     int ceiling_ = 0;                   // the escalation ceiling; 0 when the search does not escalate
     DeviceBuffer esc_state_, tm_changes_;  // escalation state, truemotion change flags

@@ -118,9 +118,18 @@ std::optional<size_t> NoiseFront::take_oldest() {
 }
 
 // One direction of the look-ahead pair between two held frames: `centre`'s blocks matched in
-// `neighbour` (lookahead.rs:460-541, without camera-model seeds or truemotion). A search that
+// `neighbour` (lookahead.rs:460-541, with the camera model's pair prediction when the engine fits
+// models, and no truemotion stage). A search that
 // escalates measures its own floor: the look-ahead's noise words belong to no window (lookahead.rs:
 // 509-515).
+std::optional<Failure> NoiseFront::attach_models(const PairModels* models) {
+    models_ = models;
+    if (!models_ || !cfg_.motion) return std::nullopt;
+    cudaError_t e = pair_predictions_.alloc(2 * kAffineWords * sizeof(float));
+    if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("look-ahead pair predictions", e)};
+    return std::nullopt;
+}
+
 std::optional<Failure> NoiseFront::search(size_t centre_frame, size_t neighbour_frame, int direction,
                                           cudaStream_t s) {
     MotionLaunch m{};
@@ -150,6 +159,12 @@ std::optional<Failure> NoiseFront::search(size_t centre_frame, size_t neighbour_
         m.ceiling = cfg_.ceiling;
         m.conf_stride = conf_stride_;
         m.esc_reads_floor = 0;
+    }
+    if (models_) {
+        // lookahead.rs:500-541: with the camera models each direction also searches around its pair
+        // prediction, scored against zeroed noise words.
+        m.predictions = pair_predictions_.as<float>() + direction * kAffineWords;
+        m.noise = models_->zero_noise();
     }
     cudaError_t e = launch_motion_search(m, s);
     if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("look-ahead search launch", e)};
@@ -240,6 +255,11 @@ std::optional<Failure> NoiseFront::read_pushed(cudaStream_t main) {
                                              static_cast<int>(frame % kFrames), s);
         if (e != cudaSuccess) return Failure{AVD_ERR_GPU, cuda_message("look-ahead pyramid launch", e)};
         if (prev) {
+            if (models_)
+                if (auto f = models_->compose_pair(static_cast<uint32_t>(*prev), static_cast<uint32_t>(frame),
+                                                   frame == 1 ? pair_predictions_.as<float>() : nullptr,
+                                                   pair_predictions_.as<float>() + kAffineWords, s))
+                    return f;
             if (auto f = search(frame, *prev, kNewerToOlder, s)) return f;
             if (frame == 1)
                 if (auto f = search(*prev, frame, kOlderToNewer, s)) return f;

@@ -590,6 +590,11 @@ AVD_API AvdStatus avd_block_means(uint64_t plane, uint64_t out, uint32_t width, 
 
 /* motion/kernels/pyramid.rs:66-132 (`mc_box_rows`, `mc_high_pass_cols`): an f32 plane minus its
  * (2 radius + 1)^2 box mean into `out`; `rows` is a plane of scratch. */
+/* engine/spec.rs:403-415 (`build_with_models`): the engine's camera-model ring copied to `out` (depth
+ * slots of 5 f32 words: a, b, tx, ty, valid; stream frame f's pair model in slot f % depth) after the
+ * queued work; `*depth` is 0 when the engine fits no models (out may then be null). */
+AVD_API AvdStatus avd_engine_models(AvdEngine* engine, float* out, uint32_t capacity, uint32_t* depth);
+
 AVD_API AvdStatus avd_high_pass(uint64_t plane, uint64_t rows, uint64_t out, uint32_t width, uint32_t height,
                                 uint32_t radius, void* stream);
 

@@ -242,7 +242,8 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
                   sad_floor: float = 0.0, thsad_scale: float = 1.0, blksize: int = 16, overlap: int = 8,
                   search_radius: int = 4, levels: int = 2, chained: bool = False, refine_radius: int = 2,
                   prefilter=None, fp64: bool = False, derived=None, share_writes=None,
-                  share_reads=None, ceiling: int = 0) -> list[np.ndarray]:
+                  share_reads=None, ceiling: int = 0, camera_model: bool = True,
+                  models: "PairModels | None" = None) -> list[np.ndarray]:
     """NLMeans with motion compensation over a stream with repeat edges, replayed slot by slot as
     the ring runs it (nlmeans/denoiser/ring.rs, stages.rs:62-209, dispatch/motion.rs:104-487):
       - each slot write (and each edge copy) builds the slot's pyramids; with Chained estimation it
@@ -259,7 +260,12 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
     centre stream frame returning (h2, noise_offset, lut, sad_floor) (the automatic estimate's fold
     around that frame), each window reads those instead. `share_writes` / `share_reads` (a
     `MotionShare`) share each window's field with a chroma pass, or take the luma pass's mapped field
-    and search one pixel around it at one level, as in `nl4d_stream`. Returns one output per input."""
+    and search one pixel around it at one level, as in `nl4d_stream`. With `camera_model` (the
+    engine's default, engine/spec.rs:426-450) a pass that searches its own motion also searches
+    around the camera models fitted on channel 0 of the frames (`models`, else a `PairModels` fed
+    every frame in order): the Direct window search around each neighbour's composed prediction,
+    the Chained pair searches around the pair's prediction with zeroed noise words. Returns one output
+    per input."""
     n = len(frames)
     h, w, c = frames[0].shape
     tf = 2 * d + 1
@@ -273,6 +279,11 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
     st = dict(head=0, loaded=0, call=0)
     if share_reads is not None:
         chained, levels = False, 1
+    if camera_model and share_reads is None and models is None and d > 0:
+        models = pair_models_for([f[..., 0] for f in frames], w, h, blksize=blksize, overlap=overlap,
+                                 search_radius=search_radius, levels=levels, ceiling=ceiling)
+    if not camera_model or share_reads is not None:
+        models = None
     outs = []
 
     def search_pyramid():
@@ -291,8 +302,9 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
             pyr = search_pyramid()
             kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=th,
                       field_lambda=1.0, reads_floor=False, ceiling=ceiling)
-            fwd, _ = motion_search(pyr, w, h, tf, older, [slot], **kw)
-            bwd, _ = motion_search(pyr, w, h, tf, slot, [older], **kw)
+            o2n, n2o = models.compose_pair(slot_frame[older], frame_idx) if models is not None else (None, None)
+            fwd, _ = motion_search(pyr, w, h, tf, older, [slot], predictions=o2n, **kw)
+            bwd, _ = motion_search(pyr, w, h, tf, slot, [older], predictions=n2o, **kw)
             pairs[st["head"] % (2 * d)] = (fwd[0], bwd[0])
 
     def duplicate_last():
@@ -329,10 +341,11 @@ def nlm_stream_mc(frames: list[np.ndarray], d: int, a: int, s: int, h2: float, *
                                    search_radius=refine_radius, levels=levels, confidence=confidence,
                                    sad_floor=w_floor, thsad=th, seeds=seeds, ceiling=ceiling, esc_reads_floor=True)
         else:
+            pred = models.compose_window([slot_frame[p] for p in phys], d) if models is not None else None
             mv, cf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                    search_radius=search_radius, levels=levels, confidence=confidence,
                                    sad_floor=w_floor, thsad=th, field_lambda=1.0, reads_floor=True, ceiling=ceiling,
-                                   esc_reads_floor=True)
+                                   esc_reads_floor=True, predictions=pred)
         if share_writes is not None:
             share_writes.write(st["call"], slot_frame[cs] % tf, slot_frame[cs], mv)
         window, refs = [], []
@@ -771,6 +784,15 @@ def fit_bands(field: np.ndarray, width: int, height: int, blksize: int, overlap:
     return bands
 
 
+def pair_models_for(luma_frames, width: int, height: int, **mode) -> "PairModels":
+    """A `PairModels` fed every normalised luma frame of a stream in push order (frame i at index i):
+    the models are causal, and the engine's ring keeps every model a window reads."""
+    pm = PairModels(width, height, **mode)
+    for i, f in enumerate(luma_frames):
+        pm.push(np.ascontiguousarray(f, np.float32), i)
+    return pm
+
+
 class PairModels:
     """global/producer.rs (`PairModelProducer`): one camera model per adjacent pair of pushed luma
     frames, kept by stream frame (the engine's ring of `held + window + 2` slots never drops a model a
@@ -957,8 +979,9 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
                 levels=2, refine=2, spatial_radius=9, lambda_ht=4.158, c_min=0.05, kaiser_beta=2.0,
                 pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0, chained: bool = False,
                 refine_radius: int = 2, noise=None, field_lambda: float = 1.0, share_writes: MotionShare | None = None,
-                share_reads: MotionShare | None = None, ceiling: int = 0) -> list[np.ndarray]:
-    """The NL4D engine with a pinned sigma and Direct or Chained motion (no camera model) over a
+                share_reads: MotionShare | None = None, ceiling: int = 0, camera_model: bool = True,
+                models: "PairModels | None" = None) -> list[np.ndarray]:
+    """The NL4D engine with a pinned sigma and Direct or Chained motion over a
     stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order. With
     `field_lambda` > 0 the truemotion stage ends the Direct window search (reading the window's SAD
     floor) and each pair search (without it); the chained refine runs none
@@ -977,7 +1000,10 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     is clear, and `colour` the (gain tables, centre block means, 8-bit scale) of collab_fused. With `share_writes`
     each window's field is shared for a chroma stream; with `share_reads` the window's motion is the
     shared luma field of the centre frame, searched one pixel around at one level with confidence
-    (nlmeans/dispatch/motion.rs:231-310), and no motion of this plane's own is searched."""
+    (nlmeans/dispatch/motion.rs:231-310), and no motion of this plane's own is searched. With
+    `camera_model` a pass that searches its own motion also searches around the camera models
+    fitted on channel 0 of the pushed frames (`models`, else a `PairModels` fed every frame in
+    order), as in `nlm_stream_mc`."""
     h, w, c = frames[0].shape
     tf = 2 * d + 1
     step = blksize - overlap
@@ -988,6 +1014,11 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     st = dict(head=0, loaded=0, real=0, passes=0, cont=context > 0, call=0)
     if share_reads is not None:
         chained, levels = False, 1
+    if camera_model and share_reads is None and models is None and d > 0:
+        models = pair_models_for([f[..., 0] for f in frames], w, h, blksize=blksize, overlap=overlap,
+                                 search_radius=search_radius, levels=levels, ceiling=ceiling)
+    if not camera_model or share_reads is not None:
+        models = None
     slot_frames = [0] * tf
     zeroed = [False] * tf
     sad_floor = sad_noise_floor(blksize, sigma)
@@ -1028,10 +1059,11 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
                                      search_radius=refine_radius, levels=levels, confidence=True,
                                      sad_floor=p_floor, thsad=th, seeds=seeds, ceiling=ceiling, esc_reads_floor=True)
         else:
+            pred = models.compose_window([slot_frames[phys(l)] for l in range(tf)], centre) if models is not None else None
             mv, conf = motion_search(pyr, w, h, tf, cs, slots, blksize=blksize, overlap=overlap,
                                      search_radius=search_radius, levels=levels, confidence=True,
                                      sad_floor=p_floor, thsad=th, field_lambda=field_lambda, reads_floor=True,
-                                     ceiling=ceiling, esc_reads_floor=True)
+                                     ceiling=ceiling, esc_reads_floor=True, predictions=pred)
         if share_writes is not None:
             share_writes.write(st["call"], slot_frames[cs] % tf, slot_frames[cs], mv)
         acc, ws, _ = collab_fused(ring.reshape(-1), w, h, c, centre_slot=cs, radius=d, mv_field=mv.reshape(-1),
@@ -1062,8 +1094,9 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
         pyr = motion_pyramid(ring.reshape(-1), c, w, h, levels)
         kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=th,
                   field_lambda=field_lambda, reads_floor=False, ceiling=ceiling)
-        fwd, _ = motion_search(pyr, w, h, tf, older, [newer], **kw)
-        bwd, _ = motion_search(pyr, w, h, tf, newer, [older], **kw)
+        o2n, n2o = models.compose_pair(slot_frames[older], st["real"]) if models is not None else (None, None)
+        fwd, _ = motion_search(pyr, w, h, tf, older, [newer], predictions=o2n, **kw)
+        bwd, _ = motion_search(pyr, w, h, tf, newer, [older], predictions=n2o, **kw)
         pairs[st["head"] % (2 * d)] = (fwd[0], bwd[0])
 
     def push(frame):
@@ -1279,19 +1312,27 @@ def noise_readings(frames: list[np.ndarray], channels: int, width: int, height: 
 
 def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, height: int, *, blksize: int,
                       overlap: int, search_radius: int, levels: int, thsad: float = 0.0, ceiling: int = 0,
-                      luma_fields: bool = False, records_out: list | None = None):
+                      luma_fields: bool = False, records_out: list | None = None, camera_model: bool = True,
+                      models: "PairModels | None" = None):
     """Every frame's reading as a motion-compensated look-ahead takes it
     (nlmeans/denoiser/lookahead.rs:283-319, 425-458, 543-605): frame i >= 1 is searched against
     frame i - 1 (newer to older) and read along that field; frame 1 is also searched older to newer
     and frame 0 re-read along it. Frame 0 keeps its Immerkaer words from its own read. Returns
     (readings, Immerkaer totals). With `records_out`, each frame's final temporal records are
-    appended to it."""
+    appended to it. With `camera_model` each pair search also searches around the pair's camera-model
+    prediction (lookahead.rs:310-316), the models fitted on channel 0 of the frames."""
     step = blksize - overlap
     mb = (max(-(-width // step), 1), max(-(-height // step), 1))
     # With `ceiling` the pair searches escalate, measuring their own floor (lookahead.rs:509-515).
     kw = dict(blksize=blksize, overlap=overlap, search_radius=search_radius, levels=levels, thsad=thsad,
               ceiling=ceiling)
     rec_len = stats_blocks(width, height)[0] * stats_blocks(width, height)[1] * noise_record_len(channels)
+    if camera_model and models is None:
+        models = pair_models_for([np.asarray(f, np.float32).reshape(height, width, channels)[..., 0] for f in frames],
+                                 width, height, blksize=blksize, overlap=overlap, search_radius=search_radius,
+                                 levels=levels, ceiling=ceiling)
+    if not camera_model:
+        models = None
     readings, totals, lows = [], [], []
     for i, f in enumerate(frames):
         _, tot, low = immerkaer(f, channels, width, height)
@@ -1306,13 +1347,14 @@ def noise_readings_mc(frames: list[np.ndarray], channels: int, width: int, heigh
         pair = np.stack([np.ascontiguousarray(frames[i - 1], np.float32),
                          np.ascontiguousarray(f, np.float32)]).reshape(-1)
         pyr = motion_pyramid(pair, channels, width, height, levels)
-        newer_to_older, _ = motion_search(pyr, width, height, 2, 1, [0], **kw)
+        o2n, n2o = models.compose_pair(i - 1, i) if models is not None else (None, None)
+        newer_to_older, _ = motion_search(pyr, width, height, 2, 1, [0], predictions=n2o, **kw)
         rec = temporal_stats_mc(f, frames[i - 1], channels, width, height, newer_to_older[0], mb, step, luma_fields)
         readings.append(noise_reading(rec, low, channels, width, height, True, luma_fields))
         if records_out is not None:
             records_out.append(rec)
         if i == 1:
-            older_to_newer, _ = motion_search(pyr, width, height, 2, 0, [1], **kw)
+            older_to_newer, _ = motion_search(pyr, width, height, 2, 0, [1], predictions=o2n, **kw)
             rec0 = temporal_stats_mc(frames[0], f, channels, width, height, older_to_newer[0], mb, step, luma_fields)
             readings[0] = noise_reading(rec0, lows[0], channels, width, height, True, luma_fields)
             if records_out is not None:

@@ -314,3 +314,45 @@ def test_search_without_a_model_is_unchanged(lib, oracle):
                              radius=4, levels=2, predictions=None, floor=0.5, thsad=oracle.thsad(16, 1.0), ceiling=8)
     assert np.array_equal(got, want)
     assert np.array_equal(bits(sad), bits(want_sad))
+
+
+# ---- the engine's producer ----------------------------------------------------------------------------
+
+def pan_clip(w, h, n, velocity, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for f in range(n):
+        v = render((1.0, 0.0, velocity[0] * f, velocity[1] * f), w, h) * 200.0 + 20.0
+        out.append([np.clip(np.round(v + rng.normal(0, 3.0, (h, w))), 0, 255).astype(np.uint8)])
+    return out
+
+
+@pytest.mark.parametrize("d,estimation,velocity", [(1, "DIRECT", (21, -4)), (2, "CHAINED", (-18, 6))])
+def test_engine_fits_the_oracle_camera_models(oracle, d, estimation, velocity):
+    """An NLMeans engine with motion compensation fits one model per pushed frame pair, bit for bit
+    the oracle's producer fed the same normalised luma, and recovers the pan."""
+    from conftest import avd
+    from gpu_util import Runner
+    from test_gpu_nlm_mc import options, search
+
+    w, h, n = 256, 144, 6
+    fmt = avd.SampleFormat.u8()
+    frames = pan_clip(w, h, n, velocity, seed=d)
+    ms = search(getattr(avd.MotionEstimation, estimation))
+    spec = avd.EngineSpec.nlmeans(avd.NlmeansAlgorithm.fast(options(d, 2, 1, 8.0, ms)), None,
+                                  avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    r = Runner(spec)
+    pm = oracle.PairModels(w, h)
+    keep = []
+    for i, frame in enumerate(frames):
+        bufs, planes = r.planes_for(frame, fmt)
+        keep.append(bufs)
+        for _ in range(r.engine.push(planes)):
+            r.emit()
+        pm.push(oracle.ingest([frame[0]], fmt.kind, fmt.max_value())[..., 0], i)
+        ring = r.engine.camera_models()
+        assert ring is not None and ring.shape[0] == r.engine.max_held_frames() + 2 * d + 1 + 2
+        got = ring[i % ring.shape[0]]
+        assert np.array_equal(bits(got), bits(pm.model(i))), (i, got, pm.model(i))
+        if i > 0:
+            assert got[4] == 1.0 and abs(got[2] - velocity[0]) < 0.5 and abs(got[3] - velocity[1]) < 0.5, got

@@ -133,9 +133,10 @@ def colour_noise(oracle, clip_frames, fmt, d, luma, *, blksize=16, overlap=8, se
              for f in clip_frames]
     grid = [m[0] if luma else m[1] for m in means]
     records = []
+    # A chroma pass refines the luma pass's motion and fits no camera models of its own.
     readings, totals = oracle.noise_readings_mc(f32, c, w, h, blksize=blksize, overlap=overlap,
                                                 search_radius=search_radius, levels=levels, luma_fields=luma,
-                                                records_out=records)
+                                                records_out=records, camera_model=luma)
     f = np.float32
     area, unit = f(81.0), f(1.2) * f(1.0) * f(255.0)
     settings = oracle.fold_words(w, h, curve_applies=luma, g_max=float(oracle.dct_noise_profile(0.0).max()),
