@@ -356,3 +356,49 @@ def test_engine_fits_the_oracle_camera_models(oracle, d, estimation, velocity):
         assert np.array_equal(bits(got), bits(pm.model(i))), (i, got, pm.model(i))
         if i > 0:
             assert got[4] == 1.0 and abs(got[2] - velocity[0]) < 0.5 and abs(got[3] - velocity[1]) < 0.5, got
+
+
+def _moved_share(oracle, frames, fmt, d, ms, **kw):
+    """How many output samples the camera model moves: the oracle with and without it."""
+    f32 = [oracle.ingest(p, fmt.kind, fmt.max_value(), 0.0) for p in frames]
+    with_model = oracle.nlm_stream_mc(f32, d, 2, 1, oracle.h2_inv_norm(8.0, 1), blksize=ms.blksize,
+                                      overlap=ms.overlap, search_radius=ms.search_radius, levels=ms.pyramid_levels,
+                                      thsad_scale=1.0, **kw)
+    without = oracle.nlm_stream_mc(f32, d, 2, 1, oracle.h2_inv_norm(8.0, 1), blksize=ms.blksize,
+                                   overlap=ms.overlap, search_radius=ms.search_radius, levels=ms.pyramid_levels,
+                                   thsad_scale=1.0, camera_model=False, **kw)
+    return float(np.mean([np.mean(a != b) for a, b in zip(with_model, without)]))
+
+
+@pytest.mark.parametrize("d,estimation", [(2, "DIRECT"), (3, "CHAINED")])
+def test_nlm_fast_pan_past_the_search_matches_oracle(oracle, d, estimation):
+    """A pan of 14 px per frame, past the 4 + 4 * 2 reach of the unseeded search: the camera model's
+    window finds it, and the engine matches the oracle that replays the same models."""
+    from conftest import avd
+    from gpu_util import Runner
+    from test_gpu_nlm_mc import check, options, search
+
+    w, h, n = 192, 112, 7
+    fmt = avd.SampleFormat.u8()
+    frames = pan_clip(w, h, n, (14, -3), seed=40 + d)
+    ms = search(getattr(avd.MotionEstimation, estimation))
+    spec = avd.EngineSpec.nlmeans(avd.NlmeansAlgorithm.fast(options(d, 2, 1, 8.0, ms)), None,
+                                  avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    check(oracle, got, frames, fmt, d, 2, 1, 8.0, ms)
+    assert _moved_share(oracle, frames, fmt, d, ms, chained=estimation == "CHAINED") > 0.01, \
+        "premise: the camera model changes the output"
+
+
+def test_nl4d_fast_pan_past_the_search_matches_oracle(oracle):
+    from conftest import avd
+    from gpu_util import Runner
+    from test_gpu_nl4d import check, opts
+
+    w, h, n, d = 160, 96, 6, 2
+    fmt = avd.SampleFormat.u8()
+    frames = pan_clip(w, h, n, (-13, 4), seed=5)
+    spec = avd.EngineSpec.nl4d(opts(d, 6.0 / 255, spatial_radius=4), None,
+                               avd.Geometry(w, h, avd.ChromaLayout.GRAY, fmt, fmt))
+    got = Runner(spec).run(frames)
+    check(oracle, got, frames, fmt, d, 6.0 / 255, spatial_radius=4)
