@@ -16,11 +16,13 @@
 //                                polish; the score against no motion and the plausibility bounds.
 //
 // Layout and design: a model is 5 f32 words (a, b, tx, ty, valid) in a ring of slots; a fit keeps 8
-// state words, 4 band words, one weight per block and 8 partial sums per 256 blocks in its scratch.
-// Each fit stage is one launch of 256-thread CTAs (one block per thread) that reduce their 8 lane
-// sums by a fixed halving tree, and one single-CTA launch that adds the partials thread by thread and
-// halves again, so the sums, and the model, are the same bits on every run and match the CPU
-// restatement. The file is built with -fmad=false: every multiply and add rounds on its own.
+// state words, 4 band words, a launch count, the bars' line counts, one weight per block and 8 partial
+// sums per 256 blocks in its scratch. The bars take one launch of one CTA per block row (integer
+// counts); each fit stage one launch of 256-thread CTAs (one block per thread) that reduce their 8
+// lane sums by a fixed halving tree, the last CTA to finish then adding the partials thread by
+// thread and halving again before it updates the state, so the sums, and the model, are the same
+// bits on every run and match the CPU restatement. The file is built with -fmad=false: every
+// multiply and add rounds on its own.
 
 #include <cuda_runtime.h>
 
@@ -191,6 +193,8 @@ struct FitArgs {
     int older_to_newer;
     int width, height, blksize, step, blocks_x, blocks_y;
     uint32_t* bands;
+    unsigned* done;         // CTAs finished in the current launch (the last one finishes the stage)
+    uint32_t* row_moving;   // blocks_y, then blocks_x line counts of the bars
     float* weights;
     float* state;
     float* partials;
@@ -226,9 +230,10 @@ __device__ __forceinline__ uint32_t band_line(uint32_t start, uint32_t steps, bo
 
 // global.rs:855-882 (`leading_band`).
 __device__ uint32_t leading_band(const uint32_t* moving, uint32_t start, bool upward, uint32_t last, uint32_t width) {
+    // The counts come from every CTA of the launch: read past L1.
     uint32_t steps = 0;
-    while (steps < last && moving[band_line(start, steps, upward)] == 0u) ++steps;
-    const uint32_t edge_moving = moving[band_line(start, steps, upward)];
+    while (steps < last && __ldcg(moving + band_line(start, steps, upward)) == 0u) ++steps;
+    const uint32_t edge_moving = __ldcg(moving + band_line(start, steps, upward));
     const bool is_short = steps * 3 <= last;
     const bool edge_ok = steps < last && edge_moving * 8 >= kBandEdgeEighths * width;
     return steps > 0 && is_short && edge_ok ? steps : 0u;
@@ -239,31 +244,50 @@ __device__ __forceinline__ bool bands_pair(uint32_t a, uint32_t b) {
     return shorter > 0 && longer - shorter <= kBandPairSlack;
 }
 
-// global.rs:286-392 (`mc_fit_bands`): one CTA; the line counts live in dynamic shared memory.
+// The last CTA of a launch: every CTA's writes are fenced before its count, so the CTA that counts
+// last sees them all. It resets the count for the next launch. Uniform across the CTA.
+__device__ __forceinline__ bool last_cta(unsigned* done) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned before = atomicAdd(done, 1u);
+        last = before == gridDim.x - 1;
+        if (last) *done = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// global.rs:286-392 (`mc_fit_bands`): one CTA per block row counts the row's blocks that belong to
+// the picture and adds each to its column's count (integer sums: the order does not matter); the
+// last CTA walks the bars.
 __global__ void __launch_bounds__(kFitThreads) fit_bands_kernel(FitArgs f) {
-    extern __shared__ uint32_t moving[];
+    __shared__ uint32_t row_count;
     const uint32_t bx = static_cast<uint32_t>(f.blocks_x), by = static_cast<uint32_t>(f.blocks_y);
-    uint32_t* row_moving = moving;
-    uint32_t* col_moving = moving + by;
+    uint32_t* row_moving = f.row_moving;
+    uint32_t* col_moving = f.row_moving + by;
     const uint32_t w = static_cast<uint32_t>(f.width), h = static_cast<uint32_t>(f.height);
     const uint32_t b = static_cast<uint32_t>(f.blksize), s = static_cast<uint32_t>(f.step);
     const uint32_t inside_rows = (h > b ? h - b : 0) / s, inside_cols = (w > b ? w - b : 0) / s;
     const uint32_t interior_rows = by > 2 ? by - 2 : 0, interior_cols = bx > 2 ? bx - 2 : 0;
     const uint32_t last_row = min(inside_rows, interior_rows), last_col = min(inside_cols, interior_cols);
-    for (uint32_t row = threadIdx.x; row < by; row += kFitThreads) {
-        uint32_t count = 0;
-        if (row >= 1 && row <= last_row)
-            for (uint32_t col = 1; col <= last_col; ++col) count += block_in_picture(f, static_cast<int>(row * bx + col));
-        row_moving[row] = count;
-    }
-    for (uint32_t col = threadIdx.x; col < bx; col += kFitThreads) {
-        uint32_t count = 0;
-        if (col >= 1 && col <= last_col)
-            for (uint32_t row = 1; row <= last_row; ++row) count += block_in_picture(f, static_cast<int>(row * bx + col));
-        col_moving[col] = count;
-    }
+    const uint32_t row = blockIdx.x;
+    if (threadIdx.x == 0) row_count = 0;
     __syncthreads();
-    if (threadIdx.x != 0) return;
+    uint32_t count = 0;
+    if (row >= 1 && row <= last_row)
+        for (uint32_t col = 1 + threadIdx.x; col <= last_col; col += kFitThreads) {
+            const uint32_t moving = block_in_picture(f, static_cast<int>(row * bx + col));
+            count += moving;
+            if (moving) atomicAdd(col_moving + col, 1u);
+        }
+    count = __reduce_add_sync(0xffffffffu, count);
+    if ((threadIdx.x & 31) == 0 && count) atomicAdd(&row_count, count);
+    __syncthreads();
+    if (threadIdx.x == 0) row_moving[row] = row_count;
+    if (!last_cta(f.done) || threadIdx.x != 0) return;
     uint32_t top = 0, bottom = 0, left = 0, right = 0;
     if (last_row >= 1 && last_col >= 1) {
         top = leading_band(row_moving, 1, true, last_row, last_col);
@@ -330,6 +354,85 @@ __device__ __forceinline__ void reduce_lanes(float (*scratch)[kFitThreads]) {
 #pragma unroll
             for (int lane = 0; lane < kFitLanes; ++lane) scratch[lane][threadIdx.x] += scratch[lane][threadIdx.x + stride];
         __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void write_reference(float* state, float valid, float a, float b, float tx, float ty) {
+    state[kRefValid] = valid;
+    state[kRef] = a;
+    state[kRef + 1] = b;
+    state[kRef + 2] = tx;
+    state[kRef + 3] = ty;
+}
+
+// global.rs:579-738 (`mc_fit_finish`), run by the last CTA of the stage's launch: every thread adds
+// its share of the partials in order, the halving tree adds the threads' sums.
+template <int STAGE>
+__device__ void finish_stage(const FitArgs& f, int groups, float (*scratch)[kFitThreads]) {
+    __syncthreads();
+#pragma unroll
+    for (int lane = 0; lane < kFitLanes; ++lane) {
+        float sum = 0.0f;
+        for (int i = threadIdx.x; i < groups; i += kFitThreads) sum += __ldcg(f.partials + i * kFitLanes + lane);
+        scratch[lane][threadIdx.x] = sum;
+    }
+    __syncthreads();
+    reduce_lanes(scratch);
+    if (threadIdx.x != 0) return;
+    float* state = f.state;
+    const float centre_x = static_cast<float>(f.width) * 0.5f, centre_y = static_cast<float>(f.height) * 0.5f;
+    if (STAGE == kWeigh) {
+        const float base = scratch[0][0], base_sad = scratch[1][0];
+        const float safe_base = fmaxf(base, 1e-12f);
+        state[kSadScale] = base > 0.0f ? base_sad / safe_base : 0.0f;
+        state[kScaleLimit] = kUnlimitedScale;
+        write_reference(state, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f);
+    } else if (STAGE == kGate) {
+        const float* p = f.models + static_cast<int64_t>(f.prior_slot) * kModelWords;
+        if (p[4] != 0.0f && beats_still(scratch[0][0], scratch[1][0], scratch[2][0])) {
+            const float ctx = p[2] + p[0] * centre_x - p[1] * centre_y - centre_x;
+            const float cty = p[3] + p[1] * centre_x + p[0] * centre_y - centre_y;
+            state[kScaleLimit] = kFitInlierCap;
+            write_reference(state, 1.0f, p[0], p[1], ctx, cty);
+        }
+    } else if (STAGE == kSolve || STAGE == kPolish) {
+        const float weight = scratch[0][0];
+        const float inverse_weight = 1.0f / fmaxf(weight, kMinFitWeight);
+        const float mean_px = scratch[1][0] * inverse_weight, mean_py = scratch[2][0] * inverse_weight;
+        const float mean_dx = scratch[3][0] * inverse_weight, mean_dy = scratch[4][0] * inverse_weight;
+        const float spread = scratch[7][0] - weight * (mean_px * mean_px + mean_py * mean_py);
+        const float dot = scratch[5][0] - weight * (mean_px * mean_dx + mean_py * mean_dy);
+        const float cross = scratch[6][0] - weight * (mean_px * mean_dy - mean_py * mean_dx);
+        float valid = 0.0f, a = 1.0f, b = 0.0f, tx = 0.0f, ty = 0.0f;
+        if (weight >= kMinFitWeight && spread > kMinFitSpread * weight) {
+            const float inverse_spread = 1.0f / spread;
+            valid = 1.0f;
+            a = 1.0f + dot * inverse_spread;
+            b = cross * inverse_spread;
+            tx = mean_px + mean_dx - (a * mean_px - b * mean_py);
+            ty = mean_py + mean_dy - (b * mean_px + a * mean_py);
+        }
+        write_reference(state, valid, a, b, tx, ty);
+    } else {
+        const bool ref_valid = state[kRefValid] != 0.0f;
+        const float a = state[kRef], b = state[kRef + 1];
+        const float tx = state[kRef + 2] + centre_x - (a * centre_x - b * centre_y);
+        const float ty = state[kRef + 3] + centre_y - (b * centre_x + a * centre_y);
+        const bool passes = beats_still(scratch[0][0], scratch[1][0], scratch[2][0]);
+        const float zoom = sqrtf(a * a + b * b);
+        const bool zoom_ok = fabsf(zoom - 1.0f) <= kMaxZoomChange;
+        const bool roll_ok = a > 0.0f && fabsf(b) <= kMaxRollTan * a;
+        const float fx = static_cast<float>(f.width), fy = static_cast<float>(f.height);
+        const float limit = kMaxCornerShift * kMaxCornerShift;
+        const bool top_ok = corner_shift_sq(a, b, tx, ty, 0.0f, 0.0f) <= limit && corner_shift_sq(a, b, tx, ty, fx, 0.0f) <= limit;
+        const bool bottom_ok = corner_shift_sq(a, b, tx, ty, 0.0f, fy) <= limit && corner_shift_sq(a, b, tx, ty, fx, fy) <= limit;
+        const bool accepted = ref_valid && passes && zoom_ok && roll_ok && top_ok && bottom_ok;
+        float* m = f.models + static_cast<int64_t>(f.slot) * kModelWords;
+        m[0] = accepted ? a : 1.0f;
+        m[1] = accepted ? b : 0.0f;
+        m[2] = accepted ? tx : 0.0f;
+        m[3] = accepted ? ty : 0.0f;
+        m[4] = accepted ? 1.0f : 0.0f;
     }
 }
 
@@ -418,97 +521,22 @@ __global__ void __launch_bounds__(kFitThreads) fit_sums_kernel(FitArgs f, float 
     __syncthreads();
     reduce_lanes(scratch);
     if (threadIdx.x < kFitLanes) f.partials[blockIdx.x * kFitLanes + threadIdx.x] = scratch[threadIdx.x][0];
+    if (last_cta(f.done)) finish_stage<STAGE>(f, static_cast<int>(gridDim.x), scratch);
 }
 
-__device__ __forceinline__ void write_reference(float* state, float valid, float a, float b, float tx, float ty) {
-    state[kRefValid] = valid;
-    state[kRef] = a;
-    state[kRef + 1] = b;
-    state[kRef + 2] = tx;
-    state[kRef + 3] = ty;
-}
-
-// global.rs:579-738 (`mc_fit_finish`): one CTA.
-template <int STAGE>
-__global__ void __launch_bounds__(kFitThreads) fit_finish_kernel(FitArgs f, int groups) {
-    __shared__ float scratch[kFitLanes][kFitThreads];
-#pragma unroll
-    for (int lane = 0; lane < kFitLanes; ++lane) {
-        float sum = 0.0f;
-        for (int i = threadIdx.x; i < groups; i += kFitThreads) sum += f.partials[i * kFitLanes + lane];
-        scratch[lane][threadIdx.x] = sum;
-    }
-    __syncthreads();
-    reduce_lanes(scratch);
-    if (threadIdx.x != 0) return;
-    float* state = f.state;
-    const float centre_x = static_cast<float>(f.width) * 0.5f, centre_y = static_cast<float>(f.height) * 0.5f;
-    if (STAGE == kWeigh) {
-        const float base = scratch[0][0], base_sad = scratch[1][0];
-        const float safe_base = fmaxf(base, 1e-12f);
-        state[kSadScale] = base > 0.0f ? base_sad / safe_base : 0.0f;
-        state[kScaleLimit] = kUnlimitedScale;
-        write_reference(state, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f);
-    } else if (STAGE == kGate) {
-        const float* p = f.models + static_cast<int64_t>(f.prior_slot) * kModelWords;
-        if (p[4] != 0.0f && beats_still(scratch[0][0], scratch[1][0], scratch[2][0])) {
-            const float ctx = p[2] + p[0] * centre_x - p[1] * centre_y - centre_x;
-            const float cty = p[3] + p[1] * centre_x + p[0] * centre_y - centre_y;
-            state[kScaleLimit] = kFitInlierCap;
-            write_reference(state, 1.0f, p[0], p[1], ctx, cty);
-        }
-    } else if (STAGE == kSolve || STAGE == kPolish) {
-        const float weight = scratch[0][0];
-        const float inverse_weight = 1.0f / fmaxf(weight, kMinFitWeight);
-        const float mean_px = scratch[1][0] * inverse_weight, mean_py = scratch[2][0] * inverse_weight;
-        const float mean_dx = scratch[3][0] * inverse_weight, mean_dy = scratch[4][0] * inverse_weight;
-        const float spread = scratch[7][0] - weight * (mean_px * mean_px + mean_py * mean_py);
-        const float dot = scratch[5][0] - weight * (mean_px * mean_dx + mean_py * mean_dy);
-        const float cross = scratch[6][0] - weight * (mean_px * mean_dy - mean_py * mean_dx);
-        float valid = 0.0f, a = 1.0f, b = 0.0f, tx = 0.0f, ty = 0.0f;
-        if (weight >= kMinFitWeight && spread > kMinFitSpread * weight) {
-            const float inverse_spread = 1.0f / spread;
-            valid = 1.0f;
-            a = 1.0f + dot * inverse_spread;
-            b = cross * inverse_spread;
-            tx = mean_px + mean_dx - (a * mean_px - b * mean_py);
-            ty = mean_py + mean_dy - (b * mean_px + a * mean_py);
-        }
-        write_reference(state, valid, a, b, tx, ty);
-    } else {
-        const bool ref_valid = state[kRefValid] != 0.0f;
-        const float a = state[kRef], b = state[kRef + 1];
-        const float tx = state[kRef + 2] + centre_x - (a * centre_x - b * centre_y);
-        const float ty = state[kRef + 3] + centre_y - (b * centre_x + a * centre_y);
-        const bool passes = beats_still(scratch[0][0], scratch[1][0], scratch[2][0]);
-        const float zoom = sqrtf(a * a + b * b);
-        const bool zoom_ok = fabsf(zoom - 1.0f) <= kMaxZoomChange;
-        const bool roll_ok = a > 0.0f && fabsf(b) <= kMaxRollTan * a;
-        const float fx = static_cast<float>(f.width), fy = static_cast<float>(f.height);
-        const float limit = kMaxCornerShift * kMaxCornerShift;
-        const bool top_ok = corner_shift_sq(a, b, tx, ty, 0.0f, 0.0f) <= limit && corner_shift_sq(a, b, tx, ty, fx, 0.0f) <= limit;
-        const bool bottom_ok = corner_shift_sq(a, b, tx, ty, 0.0f, fy) <= limit && corner_shift_sq(a, b, tx, ty, fx, fy) <= limit;
-        const bool accepted = ref_valid && passes && zoom_ok && roll_ok && top_ok && bottom_ok;
-        float* m = f.models + static_cast<int64_t>(f.slot) * kModelWords;
-        m[0] = accepted ? a : 1.0f;
-        m[1] = accepted ? b : 0.0f;
-        m[2] = accepted ? tx : 0.0f;
-        m[3] = accepted ? ty : 0.0f;
-        m[4] = accepted ? 1.0f : 0.0f;
-    }
-}
 
 template <int STAGE>
 void fit_stage(const FitArgs& f, int groups, float scale, cudaStream_t s) {
     fit_sums_kernel<STAGE><<<groups, kFitThreads, 0, s>>>(f, scale);
-    fit_finish_kernel<STAGE><<<1, kFitThreads, 0, s>>>(f, groups);
 }
 
 }  // namespace
 
+// The scratch: 8 state words, 4 band words, the launch count (and 3 spare), blocks + 2 line counts
+// (blocks_x + blocks_y never exceeds blocks + 1), one weight per block, 8 partials per 256 blocks.
 size_t model_fit_scratch_floats(int blocks) {
     const size_t groups = (static_cast<size_t>(blocks) + kFitThreads - 1) / kFitThreads;
-    return 8 + 4 + static_cast<size_t>(blocks) + groups * kFitLanes;
+    return 8 + 4 + 4 + (static_cast<size_t>(blocks) + 2) + static_cast<size_t>(blocks) + groups * kFitLanes;
 }
 
 cudaError_t launch_compose_models(const float* models, const uint32_t* gaps, float* out, int neighbours, int max_steps,
@@ -573,15 +601,18 @@ cudaError_t launch_model_fit(const ModelFitLaunch& l, cudaStream_t s) {
     const int groups = (blocks + kFitThreads - 1) / kFitThreads;
     f.state = l.scratch;
     f.bands = reinterpret_cast<uint32_t*>(l.scratch + 8);
-    f.weights = l.scratch + 12;
-    f.partials = l.scratch + 12 + blocks;
+    f.done = reinterpret_cast<unsigned*>(l.scratch + 12);
+    f.row_moving = reinterpret_cast<uint32_t*>(l.scratch + 16);
+    f.weights = l.scratch + 16 + (blocks + 2);
+    f.partials = f.weights + blocks;
     f.models = l.models;
     f.prior_slot = l.prior >= 0 ? l.prior : 0;
     f.slot = l.slot;
-    const size_t band_bytes = static_cast<size_t>(f.blocks_x + f.blocks_y) * sizeof(uint32_t);
-    if (band_bytes > 48 * 1024) return cudaErrorInvalidValue;
     // global/fit.rs:212-234: bars; weigh; the gate on a prior; solves at 16, 8, 4, 2; polish; score.
-    fit_bands_kernel<<<1, kFitThreads, band_bytes, s>>>(f);
+    // The launch count and the line counts start at zero; each launch's last CTA leaves the count at 0.
+    cudaError_t e = cudaMemsetAsync(f.done, 0, (4 + static_cast<size_t>(blocks) + 2) * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    fit_bands_kernel<<<f.blocks_y, kFitThreads, 0, s>>>(f);
     fit_stage<kWeigh>(f, groups, kFitInlierCap, s);
     if (l.prior >= 0) fit_stage<kGate>(f, groups, kFitInlierCap, s);
     for (float scale : {16.0f, 8.0f, 4.0f, 2.0f}) fit_stage<kSolve>(f, groups, scale, s);

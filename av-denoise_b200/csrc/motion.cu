@@ -340,17 +340,19 @@ __global__ void __launch_bounds__(((2 * R + 1) * (2 * R + 1) + 31) / 32 * 32) fi
 }
 
 // Register-blocked search for the common block sizes: one warp per (block, neighbour), several
-// blocks per CTA. Each work item is one candidate row and three adjacent offsets along it; per
-// block row it holds BLK + 2 window values in registers and scores the three offsets from them,
-// so a SAD term costs about two thirds of a shared load instead of two. Every SAD is still the
+// blocks per CTA. Each work item is one candidate row and three adjacent offsets along it (five for
+// the wide coarse window of the camera model's first search); per block row it holds BLK + 2 (or
+// BLK + 4) window values in registers and scores the offsets from them, so a SAD term costs well
+// under one shared load instead of two. Every SAD is still the
 // sequential row-major sum, so the vectors are the generic kernels' bit for bit.
 template <int BLK, int R>
 struct Blocked {
     static constexpr int kSide = 2 * R + 1;
-    static constexpr int kGroups = (kSide + 2) / 3;
+    static constexpr int kWide = R > kMaxRadius ? 5 : 3;  // offsets per work item
+    static constexpr int kGroups = (kSide + kWide - 1) / kWide;
     static constexpr int kItems = kSide * kGroups;
     static constexpr int kRows = BLK + 2 * R;
-    static constexpr int kReach = kGroups * 3 + BLK - 1;                 // columns the last group reads
+    static constexpr int kReach = kGroups * kWide + BLK - 1;             // columns the last group reads
     static constexpr int kStride = (kReach > kRows ? kReach : kRows) | 1;  // odd: spreads the banks
     static constexpr int kWarps = BLK >= 32 ? 2 : 4;
     static constexpr int kWindow = kStride * kRows;
@@ -374,25 +376,25 @@ __device__ __forceinline__ void blocked_window(const SearchLevel& L, int64_t cen
     }
     __syncwarp();
     for (int item = lane; item < B::kItems; item += 32) {
-        const int dy = item / B::kGroups, dx0 = (item % B::kGroups) * 3;
-        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+        const int dy = item / B::kGroups, dx0 = (item % B::kGroups) * B::kWide;
+        float part[B::kWide];
+#pragma unroll
+        for (int k = 0; k < B::kWide; ++k) part[k] = 0.0f;
         for (int iy = 0; iy < BLK; ++iy) {
             const float* wrow = window + (iy + dy) * B::kStride + dx0;
             const float* crow = centre_tile + iy * BLK;
-            float w[BLK + 2];
+            float w[BLK + B::kWide - 1];
 #pragma unroll
-            for (int k = 0; k < BLK + 2; ++k) w[k] = wrow[k];
+            for (int k = 0; k < BLK + B::kWide - 1; ++k) w[k] = wrow[k];
 #pragma unroll
             for (int ix = 0; ix < BLK; ++ix) {
                 const float c = crow[ix];
-                s0 = __fadd_rn(s0, fabsf(__fsub_rn(c, w[ix])));
-                s1 = __fadd_rn(s1, fabsf(__fsub_rn(c, w[ix + 1])));
-                s2 = __fadd_rn(s2, fabsf(__fsub_rn(c, w[ix + 2])));
+#pragma unroll
+                for (int k = 0; k < B::kWide; ++k) part[k] = __fadd_rn(part[k], fabsf(__fsub_rn(c, w[ix + k])));
             }
         }
-        const float part[3] = {s0, s1, s2};
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < B::kWide; ++k)
             if (dx0 + k < B::kSide) sads[dy * B::kSide + dx0 + k] = part[k];
     }
     __syncwarp();
