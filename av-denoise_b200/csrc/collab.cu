@@ -478,35 +478,87 @@ __device__ __forceinline__ void load_row(float (&dst)[C], const float* __restric
     for (int c = 0; c < C; ++c) dst[c] = __ldg(colp + static_cast<size_t>(row) * width * C + c);
 }
 
-// The lane's column distance with the window rows held in a ring of 8 registers; PH is the ring
-// phase, so every index is a compile-time constant. Same operation order as column_ssd.
-template <int C, int PH>
-__device__ __forceinline__ float ring_ssd(const float (&ref)[P * C], const float (&ring)[P][C]) {
-    float s = 0.0f;
+// The group sums of eight candidates at once, each lane's eight column distances in `v`: the same
+// pairwise tree as reduce8 (partners xor 1, then 2, then 4), each level keeping half the candidates
+// on each side, so every total has the bits reduce8 gives it. Lane `sub` ends with the total of
+// candidate (sub & 1) * 4 + (sub & 2) + ((sub >> 2) & 1).
+__device__ __forceinline__ float reduce_scatter8(const GroupCtx& g, const float (&v)[8]) {
+    const bool b0 = g.sub & 1, b1 = g.sub & 2, b2 = g.sub & 4;
+    float u[4];
 #pragma unroll
-    for (int r = 0; r < P; ++r)
+    for (int j = 0; j < 4; ++j) {
+        const float give = b0 ? v[j] : v[4 + j];
+        const float keep = b0 ? v[4 + j] : v[j];
+        u[j] = __fadd_rn(keep, __shfl_xor_sync(g.mask, give, 1));
+    }
+    float w[2];
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-            const float d = ref[r * C + c] - ring[(PH + r) & 7][c];
-            s = __fadd_rn(s, __fmul_rn(d, d));
-        }
-    return s;
+    for (int j = 0; j < 2; ++j) {
+        const float give = b1 ? u[j] : u[2 + j];
+        const float keep = b1 ? u[2 + j] : u[j];
+        w[j] = __fadd_rn(keep, __shfl_xor_sync(g.mask, give, 2));
+    }
+    const float give = b2 ? w[0] : w[1];
+    const float keep = b2 ? w[1] : w[0];
+    return __fadd_rn(keep, __shfl_xor_sync(g.mask, give, 4));
 }
 
-template <int C, int PH>
-__device__ __forceinline__ void centre_step(const GroupCtx& g, const float (&cur)[P * C], float (&ring)[P][C],
-                                            const float* __restrict__ colp, int width, uint32_t top, uint32_t j,
-                                            uint32_t col, uint32_t ww, bool self_col, uint32_t self_row, float scale,
-                                            float& best_d, uint32_t& best_i, float& worst_d, uint32_t& worst_i) {
-    load_row<C>(ring[(PH + 7) & 7], colp, top + j + 7, width);
-    float d = reduce8(g, ring_ssd<C, PH>(cur, ring)) * scale;
+__device__ __forceinline__ int scattered_candidate(int sub) { return (sub & 1) * 4 + (sub & 2) + ((sub >> 2) & 1); }
+
+// Eight candidate rows jb..jb+7 of window column `col` (the lane's sample column `colp`): `rows`
+// holds window rows jb..jb+6 on entry and jb+8..jb+14 on exit. Each candidate's distance is its
+// column sums in row order, the group's pairwise sum (reduce8's tree), times the channel scale;
+// the candidates that beat the list's worst key join it one at a time, in any order (the list is
+// the 8 smallest (distance, visiting index) pairs whatever the order they arrive in).
+template <int C>
+__device__ __forceinline__ void centre_batch(const GroupCtx& g, const float (&cur)[P * C], float (&rows)[15][C],
+                                             const float* __restrict__ colp, int width, uint32_t top, uint32_t jb,
+                                             uint32_t hh, uint32_t col, uint32_t ww, bool self_col,
+                                             uint32_t self_row, float scale, float& best_d, uint32_t& best_i,
+                                             float& worst_d, uint32_t& worst_i) {
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+        if (jb + x < hh) {
+            load_row<C>(rows[7 + x], colp, top + jb + 7 + x, width);
+        } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) rows[7 + x][c] = 0.0f;
+        }
+    }
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int r = 0; r < P; ++r)
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const float d = cur[r * C + c] - rows[k + r][c];
+                sum = __fadd_rn(sum, __fmul_rn(d, d));
+            }
+        v[k] = sum;
+    }
+    const uint32_t j = jb + static_cast<uint32_t>(scattered_candidate(g.sub));
+    float d = reduce_scatter8(g, v) * scale;
     if (self_col && j == self_row) d = kSelfPin;
     const uint32_t i = j * ww + col;
-    if (d < kUnfilled && key_less(d, i, worst_d, worst_i)) {
-        shift_insert8_key(g, best_d, best_i, d, i);
-        worst_d = __shfl_sync(g.mask, best_d, 7, 8);
-        worst_i = __shfl_sync(g.mask, best_i, 7, 8);
+    const bool wins = j < hh && d < kUnfilled && key_less(d, i, worst_d, worst_i);
+    unsigned m = __ballot_sync(g.mask, wins) & g.mask;
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const float dd = __shfl_sync(g.mask, d, src);
+        const uint32_t ii = __shfl_sync(g.mask, i, src);
+        if (key_less(dd, ii, worst_d, worst_i)) {  // uniform: every lane holds the same words
+            shift_insert8_key(g, best_d, best_i, dd, ii);
+            worst_d = __shfl_sync(g.mask, best_d, 7, 8);
+            worst_i = __shfl_sync(g.mask, best_i, 7, 8);
+        }
     }
+#pragma unroll
+    for (int r = 0; r < 7; ++r)
+#pragma unroll
+        for (int c = 0; c < C; ++c) rows[r][c] = rows[8 + r][c];
 }
 
 // Member words per reference patch: 8 packed positions, then k_use | use_grid << 8.
@@ -535,8 +587,9 @@ __global__ void __launch_bounds__(kThreads, 5) collab_search_kernel(CollabLaunch
 #pragma unroll
         for (int c = 0; c < C; ++c) cur[r * C + c] = __ldg(centre + ((static_cast<size_t>(ry) + r) * a.width + rx + g.sub) * C + c);
 
-    // Centre search (fused/centre.rs:213-258) over the clipped window, column by column with the
-    // column's rows sliding through registers: one load per candidate and lane.
+    // Centre search (fused/centre.rs:213-258) over the clipped window, column by column, eight
+    // candidate rows at a time with the column's rows in registers: one load per candidate and lane,
+    // one reduce-scatter of the group per eight candidates.
     const uint32_t left = clamp_top_left(static_cast<int>(rx) - a.spatial_radius, max_x);
     const uint32_t right = clamp_top_left(static_cast<int>(rx) + a.spatial_radius, max_x);
     const uint32_t top = clamp_top_left(static_cast<int>(ry) - a.spatial_radius, max_y);
@@ -548,24 +601,12 @@ __global__ void __launch_bounds__(kThreads, 5) collab_search_kernel(CollabLaunch
         const float* colp = centre + static_cast<size_t>(cx + g.sub) * C;
         const bool self_col = cx == rx;
         const uint32_t col = cx - left, self_row = ry - top;
-        float ring[P][C];
+        float rows[15][C];
 #pragma unroll
-        for (int r = 0; r < P - 1; ++r) load_row<C>(ring[r], colp, top + r, a.width);
-        for (uint32_t jb = 0; jb < hh; jb += 8) {
-#define AVD_CENTRE_STEP(PH)                                                                                      \
-    if (jb + PH < hh)                                                                                            \
-        centre_step<C, PH>(g, cur, ring, colp, a.width, top, jb + PH, col, ww, self_col, self_row, scale, best_d, \
-                           best_i, worst_d, worst_i);
-            AVD_CENTRE_STEP(0)
-            AVD_CENTRE_STEP(1)
-            AVD_CENTRE_STEP(2)
-            AVD_CENTRE_STEP(3)
-            AVD_CENTRE_STEP(4)
-            AVD_CENTRE_STEP(5)
-            AVD_CENTRE_STEP(6)
-            AVD_CENTRE_STEP(7)
-#undef AVD_CENTRE_STEP
-        }
+        for (int r = 0; r < P - 1; ++r) load_row<C>(rows[r], colp, top + r, a.width);
+        for (uint32_t jb = 0; jb < hh; jb += 8)
+            centre_batch<C>(g, cur, rows, colp, a.width, top, jb, hh, col, ww, self_col, self_row, scale, best_d,
+                            best_i, worst_d, worst_i);
     }
     const uint32_t n_live = ww * hh;
     int k_use = 1;
