@@ -565,7 +565,7 @@ __device__ __forceinline__ void centre_batch(const GroupCtx& g, const float (&cu
 constexpr int kMemberWords = 9;
 
 template <int C, int GF, int COVERS>
-__global__ void __launch_bounds__(kThreads, 5) collab_search_kernel(CollabLaunch a) {
+__global__ void __launch_bounds__(kThreads, C == 1 ? 5 : 4) collab_search_kernel(CollabLaunch a) {
     const int lane = threadIdx.x & 31;
     const int group = threadIdx.x >> 3;
     GroupCtx g;
