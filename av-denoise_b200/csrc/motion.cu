@@ -382,15 +382,24 @@ __device__ __forceinline__ void blocked_window(const SearchLevel& L, int64_t cen
         for (int k = 0; k < B::kWide; ++k) part[k] = 0.0f;
         for (int iy = 0; iy < BLK; ++iy) {
             const float* wrow = window + (iy + dy) * B::kStride + dx0;
-            const float* crow = centre_tile + iy * BLK;
+            // The block row in registers, four samples per shared load (rows start 16-byte aligned).
+            const float4* crow = reinterpret_cast<const float4*>(centre_tile + iy * BLK);
+            float c[BLK];
+#pragma unroll
+            for (int q = 0; q < BLK / 4; ++q) {
+                const float4 v = crow[q];
+                c[4 * q] = v.x;
+                c[4 * q + 1] = v.y;
+                c[4 * q + 2] = v.z;
+                c[4 * q + 3] = v.w;
+            }
             float w[BLK + B::kWide - 1];
 #pragma unroll
             for (int k = 0; k < BLK + B::kWide - 1; ++k) w[k] = wrow[k];
 #pragma unroll
             for (int ix = 0; ix < BLK; ++ix) {
-                const float c = crow[ix];
 #pragma unroll
-                for (int k = 0; k < B::kWide; ++k) part[k] = __fadd_rn(part[k], fabsf(__fsub_rn(c, w[ix + k])));
+                for (int k = 0; k < B::kWide; ++k) part[k] = __fadd_rn(part[k], fabsf(__fsub_rn(c[ix], w[ix + k])));
             }
         }
 #pragma unroll
@@ -417,7 +426,7 @@ __device__ __forceinline__ void blocked_window(const SearchLevel& L, int64_t cen
 template <int BLK, int R, bool COARSE>
 __global__ void __launch_bounds__(Blocked<BLK, R>::kWarps * 32) blocked_kernel(SearchArgs a) {
     using B = Blocked<BLK, R>;
-    __shared__ float centre_tiles[B::kWarps][BLK * BLK];
+    __shared__ __align__(16) float centre_tiles[B::kWarps][BLK * BLK];
     __shared__ float windows[B::kWarps][B::kWindow];
     __shared__ float sad_buf[B::kWarps][B::kSide * B::kSide];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
