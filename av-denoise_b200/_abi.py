@@ -142,7 +142,8 @@ class AvdWindowSpan(C.Structure):
 
 
 class AvdEngineTiming(C.Structure):
-    _fields_ = [("device_time", C.c_double), ("frames", u64), ("exact_samples", u64)]
+    _fields_ = [("device_time", C.c_double), ("frames", u64), ("exact_samples", u64), ("core_time", C.c_double),
+                ("core_launches", u64)]
 
 
 class AvdPassTimings(C.Structure):

@@ -532,6 +532,8 @@ class EngineTiming:
     device_time: float
     frames: int
     exact_samples: int = 0  # samples the exact finish recomputed over the sampled frames
+    core_time: float = 0.0  # the core launches' device time over the sampled frames (NL4D: search + filter)
+    core_launches: int = 0
 
 
 @dataclass
@@ -615,8 +617,10 @@ class Engine:
     def timing(self) -> PassTimings:
         out = _abi.AvdPassTimings()
         self._check(self._lib.avd_engine_timing(self._h, C.byref(out)))
-        luma = EngineTiming(out.luma.device_time, out.luma.frames, out.luma.exact_samples) if out.has_luma else None
-        chroma = (EngineTiming(out.chroma.device_time, out.chroma.frames, out.chroma.exact_samples)
+        luma = (EngineTiming(out.luma.device_time, out.luma.frames, out.luma.exact_samples, out.luma.core_time,
+                             out.luma.core_launches) if out.has_luma else None)
+        chroma = (EngineTiming(out.chroma.device_time, out.chroma.frames, out.chroma.exact_samples,
+                               out.chroma.core_time, out.chroma.core_launches)
                   if out.has_chroma else None)
         return PassTimings(luma, chroma)
 

@@ -61,6 +61,11 @@ struct DeviceTimer {
     uint64_t frames = 0;
     uint64_t exact_samples = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    // The pass's core launches (the NL4D group search and filter) inside sampled frames.
+    bool sampling = false;
+    double core_total = 0.0;
+    uint64_t core_launches = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> core_pending;
     // Pinned host words the sampled frames' exact-finish counts are copied into (one per pending
     // frame, up to kCountSlots between collections).
     static constexpr size_t kCountSlots = 256;
@@ -68,10 +73,11 @@ struct DeviceTimer {
     size_t counted = 0;
 
     ~DeviceTimer() {
-        for (auto& p : pending) {
-            cudaEventDestroy(p.first);
-            cudaEventDestroy(p.second);
-        }
+        for (auto* list : {&pending, &core_pending})
+            for (auto& p : *list) {
+                cudaEventDestroy(p.first);
+                cudaEventDestroy(p.second);
+            }
         if (counts) cudaFreeHost(counts);
     }
     // Queues a copy of a sampled frame's exact-finish count (after its exact launch, on `s`).
@@ -87,7 +93,8 @@ struct DeviceTimer {
     }
     bool begin(cudaStream_t s, cudaEvent_t* start) {
         uint64_t n = frame_counter++;
-        if (every == 0 || n % every != 0) return false;
+        sampling = every != 0 && n % every == 0;
+        if (!sampling) return false;
         cudaEventCreate(start);
         cudaEventRecord(*start, s);
         return true;
@@ -97,6 +104,20 @@ struct DeviceTimer {
         cudaEventCreate(&stop);
         cudaEventRecord(stop, s);
         pending.emplace_back(start, stop);
+        sampling = false;
+    }
+    // Events around one core launch of a sampled frame (no-ops otherwise).
+    void core_begin(cudaStream_t s, cudaEvent_t* start) {
+        if (!sampling) return;
+        cudaEventCreate(start);
+        cudaEventRecord(*start, s);
+    }
+    void core_end(cudaStream_t s, cudaEvent_t start) {
+        if (!sampling) return;
+        cudaEvent_t stop;
+        cudaEventCreate(&stop);
+        cudaEventRecord(stop, s);
+        core_pending.emplace_back(start, stop);
     }
     AvdEngineTiming collect() {
         for (auto& p : pending) {
@@ -109,6 +130,16 @@ struct DeviceTimer {
             cudaEventDestroy(p.second);
         }
         pending.clear();
+        for (auto& p : core_pending) {
+            float ms = 0.0f;
+            if (cudaEventSynchronize(p.second) == cudaSuccess && cudaEventElapsedTime(&ms, p.first, p.second) == cudaSuccess) {
+                core_total += ms * 1e-3;
+                core_launches += 1;
+            }
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+        core_pending.clear();
         if (counted) {
             cudaDeviceSynchronize();
             for (size_t i = 0; i < counted; ++i) exact_samples += static_cast<uint64_t>(counts[i]);
@@ -118,6 +149,8 @@ struct DeviceTimer {
         t.device_time = total;
         t.frames = frames;
         t.exact_samples = exact_samples;
+        t.core_time = core_total;
+        t.core_launches = core_launches;
         return t;
     }
 };

@@ -853,7 +853,10 @@ class Nl4dPass final : public Pass {
             a.colour_on = 1;
             a.colour_blocks_x = (static_cast<int>(width_) + 15) / 16;
         }
+        cudaEvent_t core{};
+        timer_.core_begin(stream, &core);
         cudaError_t e = launch_collab(a, stream);
+        timer_.core_end(stream, core);
         if (e != cudaSuccess) return gpu_failure("collab launch", e);
         return std::nullopt;
     }

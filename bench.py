@@ -479,7 +479,11 @@ def nl4d_4k_section(avd, torch, np, synth, pushes: int) -> dict:
         return [avd.DevicePlane.from_tensor(t, pw, ph) for t, (pw, ph) in zip(ts, dims)]
 
     times = []
+    fill = 2 * d + 1 + 8
     for i in range(pushes):
+        if i == fill:
+            for eng in engines:
+                eng.sample_device_time(1)  # events around every steady-state pass and its core launch
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for eng in engines:
@@ -488,13 +492,40 @@ def nl4d_4k_section(avd, torch, np, synth, pushes: int) -> dict:
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
+    timing = engines[0].timing()
     for eng in engines:
         eng.close()
-    steady = times[2 * d + 1 + 8:]
+    steady = times[fill:]
     ms = float(np.median(steady))
+
+    # The group search's algorithmic FP32 operations per launch: every reference patch's clipped
+    # centre window (33 x 33 inside the frame) and at least one 5 x 5 refine rectangle per volume
+    # and neighbour frame, each candidate 64 squared differences per channel (sub, mul, add: the
+    # oracle's unfused order) plus the group sum and the scale (8).
+    def search_ops(pw, ph, c):
+        def axis(n):
+            top = n - 8
+            return sum(min(min(i * 4, top) + 16, top) - max(min(i * 4, top) - 16, 0) + 1
+                       for i in range((top + 3) // 4 + 1))
+        refs = ((pw - 8 + 3) // 4 + 1) * ((ph - 8 + 3) // 4 + 1)
+        per_candidate = 64 * c * 3 + 8
+        return (axis(pw) * axis(ph) + refs * 2 * (2 * d) * 25) * per_candidate
+
+    unfused_rate = 148 * 128 * 1.965e9  # FP32 lanes x the B200's top SM clock: one operation per lane per clock
+    core = {}
+    for name, t, (pw, ph), c in (("luma", timing.luma, dims[0], 1), ("chroma", timing.chroma, dims[1], 2)):
+        if t is None or t.core_launches == 0:
+            continue
+        launch_s = t.core_time / t.core_launches
+        ops = search_ops(pw, ph, c)
+        core[name] = {"launch_ms": round(launch_s * 1e3, 3), "search_gops": round(ops / 1e9, 1),
+                      "achieved_tops": round(ops / launch_s / 1e12, 2),
+                      "frac_unfused_fp32": round(ops / launch_s / unfused_rate, 3)}
     return {"workload": "NL4D 3840x2160 4:2:0 10-bit luma+chroma, d=3 (Chained), spatial_radius 16, lambda_ht 2.7, "
                         "plain threshold; sigma automatic on both plane groups, noise map and colour gains on",
-            "frames_per_s": round(1000.0 / ms, 2), "ms_per_frame": round(ms, 3), "pushes_timed": len(steady)}
+            "frames_per_s": round(1000.0 / ms, 2), "ms_per_frame": round(ms, 3), "pushes_timed": len(steady),
+            "group_search": dict(core, note="CUDA events around each steady-state pass's group search + filter "
+                                            "launch; operations counted for the search alone, so a lower bound")}
 
 
 def run_reference(args) -> None:

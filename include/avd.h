@@ -269,6 +269,10 @@ typedef struct AvdEngineTiming {
     /* No field in the reference: over the same sampled frames, the samples (pixels) the exact finish
      * recomputed in the reference kernels' order (NLMeans with integer outputs; 0 otherwise). */
     uint64_t exact_samples;
+    /* No field in the reference: over the same sampled frames, the device time of the pass's core
+     * launches (NL4D: the group search and the group filter) and how many there were. */
+    double core_time;
+    uint64_t core_launches;
 } AvdEngineTiming;
 
 typedef struct AvdPassTimings {
