@@ -117,6 +117,7 @@ class AvdNl4dOptions(C.Structure):
         ("pooled_threshold", u32),
         ("grain_data", u32),
         ("temporal_radius", u32),
+        ("wiener", u32),
     ]
 
 
@@ -156,7 +157,11 @@ class AvdCollabPass(C.Structure):
                [(n, u32) for n in ("width", "height", "channels", "centre_slot", "sigma_word", "weight_scale_word",
                                    "curve_valid_word", "radius", "refine", "spatial_radius", "k_max", "mv_stride",
                                    "conf_stride", "blk_step", "blksize", "blocks_x", "blocks_y", "pooled")] + \
-               [(n, f32) for n in ("c_min", "lambda_ht", "accum_scale", "pool_ratio")]
+               [(n, f32) for n in ("c_min", "lambda_ht", "accum_scale", "pool_ratio")] + [("wiener", u32)]
+
+
+class AvdCollabAdjoint(C.Structure):
+    _fields_ = [(n, u64) for n in ("grad_accum", "grad_wsum", "grad_ring", "grad_sigma_refs")]
 
 
 class AvdMotionPass(C.Structure):
@@ -250,6 +255,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_host_sample_device_time": (None, [_H, u32]),
     "avd_collab_pass": (C.c_int, [_P(AvdCollabPass), C.c_void_p]),
     "avd_collab_member_bytes": (u64, [u32, u32]),
+    "avd_collab_refs": (u64, [u32, u32]),
+    "avd_collab_adjoint": (C.c_int, [_P(AvdCollabPass), _P(AvdCollabAdjoint), C.c_void_p]),
     "avd_dct_noise_profile": (None, [f32, _P(f32)]),
     "avd_kaiser_window": (None, [f32, _P(f32)]),
     "avd_cross_frame_accum_scale": (f32, [u32, u32]),

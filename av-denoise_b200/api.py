@@ -448,6 +448,9 @@ class Nl4dOptions:
     pooled_threshold: bool = True
     grain_data: bool = False
     temporal_radius: int = 2
+    # The empirical Wiener stage after the threshold: an extension, off by default (the reference's
+    # filter stops at the threshold).
+    wiener: bool = False
 
     def _c(self) -> _abi.AvdNl4dOptions:
         return _abi.AvdNl4dOptions(self.motion._c(), int(self.sigma is not None), float(self.sigma or 0.0),
@@ -455,7 +458,7 @@ class Nl4dOptions:
                                    int(self.lambda_ht is not None), float(self.lambda_ht or 0.0),
                                    self.lambda_ht_scale, self.c_min, self.kaiser_beta, self.field_lambda,
                                    int(self.noise_map), int(self.pooled_threshold), int(self.grain_data),
-                                   self.temporal_radius)
+                                   self.temporal_radius, int(self.wiener))
 
 
 @dataclass

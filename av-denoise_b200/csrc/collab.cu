@@ -140,7 +140,7 @@ __device__ __forceinline__ void transpose8(const GroupCtx& g, float* region, flo
 // the lane's retained variance.
 __device__ __forceinline__ float pooled_threshold(const GroupCtx& g, float (&s)[MAX_K][P], const float (&v)[MAX_K],
                                                   const float (&prof)[P], int k_use, float threshold,
-                                                  float dc_lambda) {
+                                                  float dc_lambda, bool wiener, uint64_t& bits) {
     const int sub = g.sub;
     const bool dc_lane = sub == 0, has_up = sub > 0, has_down = sub < 7;
     const float vertical = 1.0f + (has_up ? 1.0f : 0.0f) + (has_down ? 1.0f : 0.0f);
@@ -176,8 +176,19 @@ __device__ __forceinline__ float pooled_threshold(const GroupCtx& g, float (&s)[
                 keep = dc_lane ? own : keep;
                 if (j == 0) keep = keep || dc_lane;
             }
-            kept_profile += keep ? prof[i] : 0.0f;
-            if (j < k_use && !keep) s[j][i] = 0.0f;
+            const bool live = j < k_use;
+            if (wiener && live && keep) {
+                const float cv = lane_var * prof[i];
+                const float zz = coeff * coeff;
+                const float den = zz + cv;
+                const float gain = den > 0.0f ? zz / den : 1.0f;
+                kept_profile += (gain * gain) * prof[i];
+                s[j][i] = gain * coeff;
+            } else {
+                kept_profile += keep ? prof[i] : 0.0f;
+                if (live && !keep) s[j][i] = 0.0f;
+            }
+            if (keep && live) bits |= uint64_t{1} << (j * 8 + i);
             previous = current;
             current = next;
         }
@@ -642,20 +653,19 @@ __global__ void __launch_bounds__(kThreads, C == 1 ? 5 : 4) collab_search_kernel
     if (g.sub == 0) words[MAX_K] = static_cast<uint32_t>(k_use) | (use_grid ? 0x100u : 0u);
 }
 
-template <int C, int GF>
-__global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch a) {
-    __shared__ float transpose_buf[kGroups * kRegion];
-    const int lane = threadIdx.x & 31;
-    const int group = threadIdx.x >> 3;
-    GroupCtx g;
-    g.sub = threadIdx.x & 7;
-    g.mask = 0xFFu << (lane & ~7);
-    float* region = transpose_buf + group * kRegion;
+// What filter_group (fused/mod.rs:559-850) settles before its transforms: the members and their
+// ring slots, the group size and layout, and each channel's threshold multiplier.
+struct GroupPlan {
+    uint32_t member_pos[MAX_K];
+    int member_slot[MAX_K];
+    int k_use;
+    bool use_grid;
+    float first_lambda, second_lambda;
+};
 
-    const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
-    const uint32_t ix = blockIdx.x * kGroups + group;
-    if (ix >= refs_x) return;
-    const uint32_t iy = blockIdx.y;
+template <int C>
+__device__ __forceinline__ void plan_group(const CollabLaunch& a, const GroupCtx& g, uint32_t ix, uint32_t iy,
+                                           uint32_t refs_x, GroupPlan& plan) {
     const uint32_t max_x = a.width - P, max_y = a.height - P;
     const uint32_t rx = min(ix * STEP, max_x), ry = min(iy * STEP, max_y);
     const float* centre = a.ring + static_cast<size_t>(a.centre_slot) * a.frame_elems;
@@ -665,23 +675,16 @@ __global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch
 #pragma unroll
         for (int c = 0; c < C; ++c) cur[r * C + c] = __ldg(centre + ((static_cast<size_t>(ry) + r) * a.width + rx + g.sub) * C + c);
     const uint32_t* words = a.members + static_cast<size_t>(iy * refs_x + ix) * kMemberWords;
-    uint32_t member_pos[MAX_K];
 #pragma unroll
-    for (int m = 0; m < MAX_K; ++m) member_pos[m] = __ldg(words + m);
+    for (int m = 0; m < MAX_K; ++m) plan.member_pos[m] = __ldg(words + m);
     const uint32_t meta = __ldg(words + MAX_K);
-    int k_use = static_cast<int>(meta & 0xFFu);
-    const bool use_grid = (meta & 0x100u) != 0;
-
-    // filter_group (fused/mod.rs:559-850).
-    int member_slot[MAX_K];
+    plan.k_use = static_cast<int>(meta & 0xFFu);
+    plan.use_grid = (meta & 0x100u) != 0;
 #pragma unroll
     for (int m = 0; m < MAX_K; ++m) {
-        const uint32_t t = member_pos[m] >> 26;
-        member_slot[m] = t > 0 ? static_cast<int>(__ldg(a.neighbour_slots + t - 1)) : a.centre_slot;
+        const uint32_t t = plan.member_pos[m] >> 26;
+        plan.member_slot[m] = t > 0 ? static_cast<int>(__ldg(a.neighbour_slots + t - 1)) : a.centre_slot;
     }
-    float prof[P];
-#pragma unroll
-    for (int i = 0; i < P; ++i) prof[i] = __ldg(a.dct_profile + i);
     float col_first = 0.0f, col_second = 0.0f;
 #pragma unroll
     for (int r = 0; r < P; ++r) {
@@ -727,8 +730,136 @@ __global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch
     const float curve_scale = fminf(fmaxf(__fmul_rn(ratio, curve_gain), 0.33f), scale_max);
     const float flat_scale = fminf(fmaxf(curve_gain, 0.33f), scale_max);
     const float luma_scale = curve_valid ? curve_scale : flat_scale;
-    const float first_lambda = __fmul_rn(__fmul_rn(a.lambda_ht, luma_scale), first_channel_gain);
-    const float second_lambda = __fmul_rn(a.lambda_ht, second_gain);
+    plan.first_lambda = __fmul_rn(__fmul_rn(a.lambda_ht, luma_scale), first_channel_gain);
+    plan.second_lambda = __fmul_rn(a.lambda_ht, second_gain);
+}
+
+// The 2D DCT of every member (column DCT, transpose, row DCT), then the member-axis transform.
+template <int GF>
+__device__ __forceinline__ void stack_forward(const GroupCtx& g, float* region, float (&s)[MAX_K][P], int k_use,
+                                              bool use_grid) {
+#pragma unroll
+    for (int m = 0; m < MAX_K; ++m) {
+        dct8_fwd(s[m]);
+        transpose8(g, region, s[m]);
+        dct8_fwd(s[m]);
+    }
+    if (GF > 1 && use_grid) {
+        grid_fwd<(GF > 1 ? GF : 2)>(s);
+    } else {
+        if (k_use >= 8) haar_level(s, 8, false);
+        if (k_use >= 4) haar_level(s, 4, false);
+        if (k_use >= 2) haar_level(s, 2, false);
+    }
+}
+
+template <int GF>
+__device__ __forceinline__ void stack_inverse(const GroupCtx& g, float* region, float (&s)[MAX_K][P], int k_use,
+                                              bool use_grid) {
+    if (GF > 1 && use_grid) {
+        grid_inv<(GF > 1 ? GF : 2)>(s);
+    } else {
+        if (k_use >= 2) haar_level(s, 2, true);
+        if (k_use >= 4) haar_level(s, 4, true);
+        if (k_use >= 8) haar_level(s, 8, true);
+    }
+#pragma unroll
+    for (int m = 0; m < MAX_K; ++m) {
+        dct8_inv(s[m]);
+        transpose8(g, region, s[m]);
+        dct8_inv(s[m]);
+    }
+}
+
+// Channel c of every member into the stack (lane `sub` column `sub`), with the propagated noise
+// variance of each member-axis coefficient, then the forward transforms.
+template <int C, int GF>
+__device__ __forceinline__ void group_spectrum(const CollabLaunch& a, const GroupCtx& g, float* region,
+                                               const GroupPlan& plan, int c, float (&s)[MAX_K][P],
+                                               float (&mv)[MAX_K]) {
+    const float sig = __ldg(a.noise + a.sigma_word + c);
+    const float base_sig2 = sig * sig;
+#pragma unroll
+    for (int m = 0; m < MAX_K; ++m) {
+        const uint32_t mx = plan.member_pos[m] & 0x1FFFu, my = (plan.member_pos[m] >> 13) & 0x1FFFu;
+        const float* src = a.ring + static_cast<size_t>(plan.member_slot[m]) * a.frame_elems;
+        mv[m] = base_sig2;
+#pragma unroll
+        for (int r = 0; r < P; ++r) s[m][r] = __ldg(src + ((static_cast<size_t>(my) + r) * a.width + mx + g.sub) * C + c);
+    }
+    if (GF > 1 && plan.use_grid) {
+        grid_variance<(GF > 1 ? GF : 2)>(mv);
+    } else {
+        if (plan.k_use >= 8) variance_level(mv, 8);
+        if (plan.k_use >= 4) variance_level(mv, 4);
+        if (plan.k_use >= 2) variance_level(mv, 2);
+    }
+    stack_forward<GF>(g, region, s, plan.k_use, plan.use_grid);
+}
+
+// The threshold (pooled or per coefficient) and, with `a.wiener`, the empirical Wiener gain
+// z^2 / (z^2 + v) on every kept coefficient (an extension: the reference stops at the threshold).
+// Returns the lane's retained variance (sum of g^2 v over its kept coefficients) and sets bit
+// j * 8 + i of `bits` for every kept coefficient of a live member-axis slot j.
+__device__ __forceinline__ float threshold_group(const CollabLaunch& a, const GroupCtx& g, float (&s)[MAX_K][P],
+                                                 const float (&mv)[MAX_K], const float (&prof)[P], int k_use,
+                                                 float channel_lambda, uint64_t& bits) {
+    bits = 0;
+    if (a.pooled)
+        return pooled_threshold(g, s, mv, prof, k_use, channel_lambda * a.pool_ratio, channel_lambda, a.wiener != 0,
+                                bits);
+    float retained = 0.0f;
+    const float prof_sub = __ldg(a.dct_profile + g.sub);
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+        const float factor = prof[i] * prof_sub;
+#pragma unroll
+        for (int j = 0; j < MAX_K; ++j) {
+            if (j < k_use) {
+                const float cv = mv[j] * factor;
+                bool keep = fabsf(s[j][i]) >= channel_lambda * sqrtf(cv);
+                if (j == 0 && i == 0 && g.sub == 0) keep = true;
+                if (keep && a.wiener) {
+                    const float zz = s[j][i] * s[j][i];
+                    const float den = zz + cv;
+                    const float gain = den > 0.0f ? zz / den : 1.0f;
+                    s[j][i] = gain * s[j][i];
+                    retained += (gain * gain) * cv;
+                } else if (keep) {
+                    retained += cv;
+                } else {
+                    s[j][i] = 0.0f;
+                }
+                if (keep) bits |= uint64_t{1} << (j * 8 + i);
+            }
+        }
+    }
+    return retained;
+}
+
+__device__ __forceinline__ float group_weight_of(float sum) {
+    return (isnan(sum) || isinf(sum)) ? 0.0f : 1.0f / fmaxf(sum, kReciprocalFloor);
+}
+
+template <int C, int GF>
+__global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch a) {
+    __shared__ float transpose_buf[kGroups * kRegion];
+    const int lane = threadIdx.x & 31;
+    const int group = threadIdx.x >> 3;
+    GroupCtx g;
+    g.sub = threadIdx.x & 7;
+    g.mask = 0xFFu << (lane & ~7);
+    float* region = transpose_buf + group * kRegion;
+
+    const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
+    const uint32_t ix = blockIdx.x * kGroups + group;
+    if (ix >= refs_x) return;
+    const uint32_t iy = blockIdx.y;
+    GroupPlan plan;
+    plan_group<C>(a, g, ix, iy, refs_x, plan);
+    float prof[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) prof[i] = __ldg(a.dct_profile + i);
     const float weight_scale = __ldg(a.noise + a.weight_scale_word);
     const uint32_t ref_idx = iy * refs_x + ix;
     const int64_t plane = static_cast<int64_t>(a.width) * a.height;
@@ -740,91 +871,178 @@ __global__ void __launch_bounds__(kThreads, 3) collab_filter_kernel(CollabLaunch
 
 #pragma unroll 1
     for (int c = 0; c < C; ++c) {
-        const float sig = __ldg(a.noise + a.sigma_word + c);
-        const float base_sig2 = sig * sig;
         float s[MAX_K][P];
         float mv[MAX_K];
-#pragma unroll
-        for (int m = 0; m < MAX_K; ++m) {
-            const uint32_t mx = member_pos[m] & 0x1FFFu, my = (member_pos[m] >> 13) & 0x1FFFu;
-            const float* src = a.ring + static_cast<size_t>(member_slot[m]) * a.frame_elems;
-            mv[m] = base_sig2;
-#pragma unroll
-            for (int r = 0; r < P; ++r) s[m][r] = __ldg(src + ((static_cast<size_t>(my) + r) * a.width + mx + g.sub) * C + c);
-        }
-        if (GF > 1 && use_grid) {
-            grid_variance<(GF > 1 ? GF : 2)>(mv);
-        } else {
-            if (k_use >= 8) variance_level(mv, 8);
-            if (k_use >= 4) variance_level(mv, 4);
-            if (k_use >= 2) variance_level(mv, 2);
-        }
-#pragma unroll
-        for (int m = 0; m < MAX_K; ++m) {
-            dct8_fwd(s[m]);
-            transpose8(g, region, s[m]);
-            dct8_fwd(s[m]);
-        }
-        if (GF > 1 && use_grid) {
-            grid_fwd<(GF > 1 ? GF : 2)>(s);
-        } else {
-            if (k_use >= 8) haar_level(s, 8, false);
-            if (k_use >= 4) haar_level(s, 4, false);
-            if (k_use >= 2) haar_level(s, 2, false);
-        }
-        const float channel_lambda = c == 0 ? first_lambda : second_lambda;
-        float retained = 0.0f;
-        if (a.pooled) {
-            retained = pooled_threshold(g, s, mv, prof, k_use, channel_lambda * a.pool_ratio, channel_lambda);
-        } else {
-            const float prof_sub = __ldg(a.dct_profile + g.sub);
-#pragma unroll
-            for (int i = 0; i < P; ++i) {
-                const float factor = prof[i] * prof_sub;
-#pragma unroll
-                for (int j = 0; j < MAX_K; ++j) {
-                    if (j < k_use) {
-                        const float cv = mv[j] * factor;
-                        bool keep = fabsf(s[j][i]) >= channel_lambda * sqrtf(cv);
-                        if (j == 0 && i == 0 && g.sub == 0) keep = true;
-                        if (keep) retained += cv;
-                        else s[j][i] = 0.0f;
-                    }
-                }
-            }
-        }
-        const float sum = reduce8(g, retained);
-        const float weight = (isnan(sum) || isinf(sum)) ? 0.0f : 1.0f / fmaxf(sum, kReciprocalFloor);
+        group_spectrum<C, GF>(a, g, region, plan, c, s, mv);
+        uint64_t bits;
+        const float retained =
+            threshold_group(a, g, s, mv, prof, plan.k_use, c == 0 ? plan.first_lambda : plan.second_lambda, bits);
+        const float weight = group_weight_of(reduce8(g, retained));
         if (c == 0) {
             if (g.sub == 0) a.group_weight[ref_idx] = weight;
             scaled_weight = weight * weight_scale;
         }
-        if (GF > 1 && use_grid) {
-            grid_inv<(GF > 1 ? GF : 2)>(s);
-        } else {
-            if (k_use >= 2) haar_level(s, 2, true);
-            if (k_use >= 4) haar_level(s, 4, true);
-            if (k_use >= 8) haar_level(s, 8, true);
-        }
-#pragma unroll
-        for (int m = 0; m < MAX_K; ++m) {
-            dct8_inv(s[m]);
-            transpose8(g, region, s[m]);
-            dct8_inv(s[m]);
-        }
+        stack_inverse<GF>(g, region, s, plan.k_use, plan.use_grid);
         // aggregate.rs:176-211 (`scatter_patch`).
 #pragma unroll
         for (int m = 0; m < MAX_K; ++m) {
-            if (m >= k_use) break;
-            const uint32_t mx = member_pos[m] & 0x1FFFu, my = (member_pos[m] >> 13) & 0x1FFFu;
+            if (m >= plan.k_use) break;
+            const uint32_t mx = plan.member_pos[m] & 0x1FFFu, my = (plan.member_pos[m] >> 13) & 0x1FFFu;
 #pragma unroll
             for (int r = 0; r < P; ++r) {
                 const float w = scaled_weight * (kaiser_r[r] * kaiser_sub);
-                const int64_t pixel = member_slot[m] * plane + (static_cast<int64_t>(my) + r) * a.width + mx + g.sub;
+                const int64_t pixel = plan.member_slot[m] * plane + (static_cast<int64_t>(my) + r) * a.width + mx + g.sub;
                 atomicAdd(a.accum + pixel * C + c, to_fixed(s[m][r] * w, a.accum_scale));
                 if (c == 0) atomicAdd(a.wsum + pixel, to_fixed_weight(w, a.accum_scale));
             }
         }
+    }
+}
+
+// The adjoint of one pass with its groups and keep decisions held fixed (an extension: the
+// reference has none). The pass is read as a smooth function of the ring and the noise levels:
+// per group Y = M g Z (Z the forward transform of the members, M the keep mask, g the Wiener
+// gain or 1), weight w = ws / R with R channel 0's retained variance, and every member pixel adds
+// clamp(w K est, -5, 5) to A and clamp(w K, 0, 1) to W (A and W in real units: the accumulators
+// hold A x accum_scale and W x accum_scale x 5). Given dL/dA and dL/dW it adds dL/d(ring) and
+// writes each reference patch's share of dL/d(sigma_c), the weight-scale word read as proportional
+// to sigma_0^2 as the engine derives it (aggregate.rs:79-99), so that with the hard threshold a
+// group weight does not move with sigma at all (R moves as sigma_0^2 too). The
+// keep masks are recomputed from the ring with the filter's own arithmetic, so they are the
+// forward's bit for bit. Z waits in shared memory for the Wiener terms, one float per thread and
+// coefficient, thread-minor so a warp's stores hit 32 banks.
+template <int C, int GF>
+__global__ void __launch_bounds__(kThreads, 2) collab_adjoint_kernel(CollabLaunch a, CollabAdjointLaunch b) {
+    __shared__ float transpose_buf[kGroups * kRegion];
+    __shared__ float spectrum[MAX_K * P * kThreads];
+    const int lane = threadIdx.x & 31;
+    const int group = threadIdx.x >> 3;
+    GroupCtx g;
+    g.sub = threadIdx.x & 7;
+    g.mask = 0xFFu << (lane & ~7);
+    float* region = transpose_buf + group * kRegion;
+
+    const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
+    const uint32_t ix = blockIdx.x * kGroups + group;
+    if (ix >= refs_x) return;
+    const uint32_t iy = blockIdx.y;
+    GroupPlan plan;
+    plan_group<C>(a, g, ix, iy, refs_x, plan);
+    float prof[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) prof[i] = __ldg(a.dct_profile + i);
+    const float prof_sub = prof[g.sub];
+    const float weight_scale = __ldg(a.noise + a.weight_scale_word);
+    const uint32_t ref_idx = iy * refs_x + ix;
+    const int64_t plane = static_cast<int64_t>(a.width) * a.height;
+    float kaiser_r[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) kaiser_r[r] = __ldg(a.kaiser + r);
+    const float kaiser_sub = __ldg(a.kaiser + g.sub);
+
+    // Channel 0's weight first when a second channel is processed before it.
+    float weight = 0.0f, retained0 = 0.0f;
+    if (C > 1) {
+        float s[MAX_K][P];
+        float mv[MAX_K];
+        group_spectrum<C, GF>(a, g, region, plan, 0, s, mv);
+        uint64_t bits;
+        retained0 = reduce8(g, threshold_group(a, g, s, mv, prof, plan.k_use, plan.first_lambda, bits));
+        weight = group_weight_of(retained0);
+    }
+    float dweight = 0.0f;  // this lane's share of dL/d(w ws)
+#pragma unroll 1
+    for (int step = 0; step < C; ++step) {
+        const int c = C - 1 - step;  // channel 0 last: its retained variance carries every channel's dL/dw
+        float s[MAX_K][P];
+        float mv[MAX_K];
+        group_spectrum<C, GF>(a, g, region, plan, c, s, mv);
+#pragma unroll
+        for (int j = 0; j < MAX_K; ++j)
+#pragma unroll
+            for (int i = 0; i < P; ++i) spectrum[(j * P + i) * kThreads + threadIdx.x] = s[j][i];
+        uint64_t bits;
+        const float retained =
+            threshold_group(a, g, s, mv, prof, plan.k_use, c == 0 ? plan.first_lambda : plan.second_lambda, bits);
+        if (C == 1) {
+            retained0 = reduce8(g, retained);
+            weight = group_weight_of(retained0);
+        }
+        const float scaled_weight = weight * weight_scale;
+        stack_inverse<GF>(g, region, s, plan.k_use, plan.use_grid);
+        // Back through the scatter: s becomes d est, and each pixel adds its share of dL/dw.
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) {
+            const uint32_t mx = plan.member_pos[m] & 0x1FFFu, my = (plan.member_pos[m] >> 13) & 0x1FFFu;
+#pragma unroll
+            for (int r = 0; r < P; ++r) {
+                const float window = kaiser_r[r] * kaiser_sub;
+                const float w = scaled_weight * window;
+                float d_est = 0.0f;
+                if (m < plan.k_use) {
+                    const int64_t pixel =
+                        plan.member_slot[m] * plane + (static_cast<int64_t>(my) + r) * a.width + mx + g.sub;
+                    float d_w = 0.0f;
+                    const float e = s[m][r];
+                    if (fabsf(e * w) < kAccumClamp) {
+                        const float ga = __ldg(b.grad_accum + pixel * C + c);
+                        d_est = ga * w;
+                        d_w = ga * e;
+                    }
+                    if (c == 0 && w > 0.0f && w < 1.0f) d_w += __ldg(b.grad_wsum + pixel);
+                    dweight += d_w * window;
+                }
+                s[m][r] = d_est;
+            }
+        }
+        stack_forward<GF>(g, region, s, plan.k_use, plan.use_grid);  // s = dL/dY
+        const float sig = __ldg(a.noise + a.sigma_word + c);
+        float d_retained = 0.0f, d_sigma = 0.0f;
+        if (c == 0) {
+            const float total = reduce8(g, dweight);
+            const bool live = !(isnan(retained0) || isinf(retained0)) && retained0 > kReciprocalFloor;
+            d_retained = live ? -total * weight_scale * weight * weight : 0.0f;
+            if (g.sub == 0 && sig > 0.0f) d_sigma = total * 2.0f * scaled_weight / sig;  // through the word
+        }
+        const bool wiener = a.wiener != 0;
+#pragma unroll
+        for (int j = 0; j < MAX_K; ++j)
+#pragma unroll
+            for (int i = 0; i < P; ++i) {
+                const bool keep = (bits >> (j * 8 + i)) & 1u;
+                const float var_unit = prof[i] * prof_sub;  // v / sigma^2
+                const float v = mv[j] * var_unit;
+                const float dy = s[j][i];
+                float dz = dy, dv = c == 0 ? d_retained : 0.0f;
+                if (wiener) {
+                    const float z = spectrum[(j * P + i) * kThreads + threadIdx.x];
+                    const float den = z * z + v;
+                    if (den > 0.0f) {
+                        const float gain = z * z / den;
+                        const float inv = 1.0f / den;
+                        dz = dy * gain * (z * z + 3.0f * v) * inv;
+                        dv = -dy * gain * z * inv;
+                        if (c == 0) {
+                            dz += d_retained * 4.0f * gain * z * v * v * inv * inv;
+                            dv += d_retained * gain * gain * (z * z - v) * inv;
+                        }
+                    }
+                }
+                s[j][i] = keep ? dz : 0.0f;
+                if (keep) d_sigma += dv * 2.0f * sig * var_unit;
+            }
+        stack_inverse<GF>(g, region, s, plan.k_use, plan.use_grid);  // s = dL/dX
+#pragma unroll
+        for (int m = 0; m < MAX_K; ++m) {
+            if (m >= plan.k_use) break;
+            const uint32_t mx = plan.member_pos[m] & 0x1FFFu, my = (plan.member_pos[m] >> 13) & 0x1FFFu;
+            float* dst = b.grad_ring + static_cast<size_t>(plan.member_slot[m]) * a.frame_elems;
+#pragma unroll
+            for (int r = 0; r < P; ++r)
+                atomicAdd(dst + ((static_cast<size_t>(my) + r) * a.width + mx + g.sub) * C + c, s[m][r]);
+        }
+        d_sigma = reduce8(g, d_sigma);
+        if (g.sub == 0) b.grad_sigma_refs[static_cast<size_t>(ref_idx) * C + c] = d_sigma;
     }
 }
 
@@ -863,12 +1081,41 @@ cudaError_t upload_taps() {
     return e;
 }
 
+template <int C, int GF>
+cudaError_t launch_adjoint_cg(const CollabLaunch& a, const CollabAdjointLaunch& b, cudaStream_t stream) {
+    const uint32_t refs_x = (a.width - P + STEP - 1) / STEP + 1;
+    const uint32_t refs_y = (a.height - P + STEP - 1) / STEP + 1;
+    dim3 grid((refs_x + kGroups - 1) / kGroups, refs_y);
+    collab_adjoint_kernel<C, GF><<<grid, kThreads, 0, stream>>>(a, b);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 size_t collab_member_words(int width, int height) {
     if (width < P || height < P) return 0;
     const size_t rx = (width - P + STEP - 1) / STEP + 1, ry = (height - P + STEP - 1) / STEP + 1;
     return rx * ry * kMemberWords;
+}
+
+cudaError_t launch_collab_adjoint(const CollabLaunch& a, const CollabAdjointLaunch& b, cudaStream_t stream) {
+    if (!a.members || !b.grad_accum || !b.grad_wsum || !b.grad_ring || !b.grad_sigma_refs)
+        return cudaErrorInvalidValue;
+    if (a.width < P || a.height < P || a.radius < 0 || a.radius > 8) return cudaErrorInvalidValue;
+    cudaError_t e = upload_taps();
+    if (e != cudaSuccess) return e;
+    const int gf = a.radius == 0 ? 1 : (a.radius == 1 ? 2 : 4);
+    if (a.channels == 1) {
+        if (gf == 1) return launch_adjoint_cg<1, 1>(a, b, stream);
+        if (gf == 2) return launch_adjoint_cg<1, 2>(a, b, stream);
+        return launch_adjoint_cg<1, 4>(a, b, stream);
+    }
+    if (a.channels == 2) {
+        if (gf == 1) return launch_adjoint_cg<2, 1>(a, b, stream);
+        if (gf == 2) return launch_adjoint_cg<2, 2>(a, b, stream);
+        return launch_adjoint_cg<2, 4>(a, b, stream);
+    }
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_collab(const CollabLaunch& a, cudaStream_t stream) {

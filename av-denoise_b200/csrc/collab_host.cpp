@@ -66,7 +66,12 @@ float avd_cross_frame_accum_scale(uint32_t spatial_radius, uint32_t temporal_rad
     return static_cast<float>(std::pow(2.0, exponent));
 }
 
-AvdStatus avd_collab_pass(const AvdCollabPass* p, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// The checked launch arguments of one pass, or the status that refuses it.
+AvdStatus pass_launch(const AvdCollabPass* p, avd::CollabLaunch& a) {
     if (!p || !p->ring || !p->accum || !p->wsum || !p->group_weight || !p->noise || !p->dct_profile || !p->kaiser ||
         !p->members)
         return AVD_ERR_NULL_ARG;
@@ -77,7 +82,7 @@ AvdStatus avd_collab_pass(const AvdCollabPass* p, void* stream) {
         return AVD_ERR_INVALID_OPTIONS;
     }
     if (p->radius > 0 && (!p->mv_field || !p->confidence || !p->neighbour_slots)) return AVD_ERR_NULL_ARG;
-    avd::CollabLaunch a{};
+    a = avd::CollabLaunch{};
     a.ring = reinterpret_cast<const float*>(p->ring);
     a.width = static_cast<int>(p->width);
     a.height = static_cast<int>(p->height);
@@ -113,9 +118,45 @@ AvdStatus avd_collab_pass(const AvdCollabPass* p, void* stream) {
     a.blksize = static_cast<int>(p->blksize);
     a.blocks_x = static_cast<int>(p->blocks_x);
     a.blocks_y = static_cast<int>(p->blocks_y);
+    a.wiener = p->wiener != 0;
+    return AVD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+AvdStatus avd_collab_pass(const AvdCollabPass* p, void* stream) {
+    avd::CollabLaunch a;
+    const AvdStatus st = pass_launch(p, a);
+    if (st != AVD_OK) return st;
     cudaError_t e = avd::launch_collab(a, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) {
         avd_set_last_error(std::string("collab launch: ") + cudaGetErrorString(e));
+        return AVD_ERR_GPU;
+    }
+    return AVD_OK;
+}
+
+uint64_t avd_collab_refs(uint32_t width, uint32_t height) {
+    if (width < 8 || height < 8) return 0;
+    return static_cast<uint64_t>((width - 8 + 3) / 4 + 1) * ((height - 8 + 3) / 4 + 1);
+}
+
+AvdStatus avd_collab_adjoint(const AvdCollabPass* p, const AvdCollabAdjoint* adj, void* stream) {
+    if (!adj || !adj->grad_accum || !adj->grad_wsum || !adj->grad_ring || !adj->grad_sigma_refs)
+        return AVD_ERR_NULL_ARG;
+    avd::CollabLaunch a;
+    const AvdStatus st = pass_launch(p, a);
+    if (st != AVD_OK) return st;
+    avd::CollabAdjointLaunch b{};
+    b.grad_accum = reinterpret_cast<const float*>(adj->grad_accum);
+    b.grad_wsum = reinterpret_cast<const float*>(adj->grad_wsum);
+    b.grad_ring = reinterpret_cast<float*>(adj->grad_ring);
+    b.grad_sigma_refs = reinterpret_cast<float*>(adj->grad_sigma_refs);
+    cudaError_t e = avd::launch_collab_adjoint(a, b, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) {
+        avd_set_last_error(std::string("collab adjoint launch: ") + cudaGetErrorString(e));
         return AVD_ERR_GPU;
     }
     return AVD_OK;

@@ -128,9 +128,23 @@ struct CollabLaunch {
     const float* colour_means;
     float colour_scale;
     int colour_on, colour_blocks_x;
+    // The empirical Wiener stage after the threshold (an extension the reference does not have):
+    // each kept coefficient z of noise variance v scaled by z^2 / (z^2 + v).
+    int wiener;
 };
 
 cudaError_t launch_collab(const CollabLaunch& args, cudaStream_t stream);
+
+// The adjoint of one collab pass (collab.cu: collab_adjoint_kernel), run after the pass with the
+// same arguments and the member words its search left in `members`. A and W are the accumulators
+// in real units (accum / accum_scale, wsum / (5 accum_scale)).
+struct CollabAdjointLaunch {
+    const float* grad_accum;  // dL/dA, laid out as the accumulators (slots x pixels x channels)
+    const float* grad_wsum;   // dL/dW, slots x pixels
+    float* grad_ring;         // dL/d(ring), laid out as the ring, added into
+    float* grad_sigma_refs;   // each reference patch's share of dL/d(sigma_c), refs x channels, written
+};
+cudaError_t launch_collab_adjoint(const CollabLaunch& args, const CollabAdjointLaunch& adjoint, cudaStream_t stream);
 // The scratch words between the search and filter launches: 9 per reference patch.
 size_t collab_member_words(int width, int height);
 

@@ -831,6 +831,7 @@ class Nl4dPass final : public Pass {
         a.accum_scale = accum_scale_;
         a.pool_ratio = pool_ratio_;
         a.pooled = opts_.pooled_threshold ? 1 : 0;
+        a.wiener = opts_.wiener ? 1 : 0;
         a.radius = static_cast<int>(d_);
         a.refine = static_cast<int>(opts_.refine);
         a.spatial_radius = static_cast<int>(opts_.spatial_radius);

@@ -206,7 +206,7 @@ _PRESETS = {"veryfast": Preset.VERYFAST, "fast": Preset.FAST, "base": Preset.BAS
 _NLM_ONLY = ("strength", "luma_strength", "chroma_strength", "patch_radius", "search_radius", "variant", "prefilter",
              "motion_compensation")
 _NL4D_ONLY = ("luma_lambda_ht", "chroma_lambda_ht", "lambda_ht", "lambda_ht_scale", "luma_lambda_ht_scale",
-              "chroma_lambda_ht_scale", "spatial_radius", "refine", "noise_map", "pooled_threshold")
+              "chroma_lambda_ht_scale", "spatial_radius", "refine", "noise_map", "pooled_threshold", "wiener")
 _KNOWN = set(_NLM_ONLY + _NL4D_ONLY + ("preset", "channel_mode", "device", "accelerators", "temporal_radius",
                                        "sigma", "sigma_scale", "tune", "deterministic", "luma_sigma_scale",
                                        "chroma_sigma_scale"))
@@ -350,6 +350,7 @@ def vs_plane_options(raw: dict, algorithm: str) -> PlaneOptions:
             refine=_nonnegative(raw["refine"], "refine") if "refine" in raw else d.refine,
             noise_map=bool(raw.get("noise_map", d.noise_map)),
             pooled_threshold=bool(raw.get("pooled_threshold", d.pooled_threshold)),
+            wiener=bool(raw.get("wiener", d.wiener)),
             motion=motion))
     # tune/config.rs:22-38: trimmed and case-insensitive.
     text = raw.get("tune", "auto")

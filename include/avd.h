@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define AVD_ABI_VERSION 5u
+#define AVD_ABI_VERSION 6u
 
 #if defined(__GNUC__)
 #define AVD_API __attribute__((visibility("default")))
@@ -208,6 +208,9 @@ typedef struct AvdNl4dOptions {
     uint32_t pooled_threshold;
     uint32_t grain_data; /* accepted and validated; AV1 grain measurement is not built */
     uint32_t temporal_radius;
+    /* Nonzero adds the empirical Wiener stage after the threshold (an extension the reference does
+     * not have; off by default, which is the reference's filter). */
+    uint32_t wiener;
 } AvdNl4dOptions;
 
 /* ---- engine spec --------------------------------------------------------------------------- */
@@ -457,7 +460,20 @@ typedef struct AvdCollabPass {
     uint32_t mv_stride, conf_stride, blk_step, blksize, blocks_x, blocks_y;
     uint32_t pooled;
     float c_min, lambda_ht, accum_scale, pool_ratio;
+    /* Nonzero adds the empirical Wiener stage after the threshold: each kept coefficient z of noise
+     * variance v is scaled by z^2 / (z^2 + v) and the group weight counts g^2 v. An extension: the
+     * reference's filter stops at the threshold (fused/mod.rs:112-134). */
+    uint32_t wiener;
 } AvdCollabPass;
+
+/* The gradients of one pass's adjoint. A and W are the accumulators in real units
+ * (accum / accum_scale and wsum / (5 accum_scale)); the normalised frame is A / W. */
+typedef struct AvdCollabAdjoint {
+    uint64_t grad_accum;      /* f32 dL/dA, laid out as `accum` */
+    uint64_t grad_wsum;       /* f32 dL/dW, laid out as `wsum` */
+    uint64_t grad_ring;       /* f32 dL/d(ring), laid out as `ring`, added into */
+    uint64_t grad_sigma_refs; /* f32 per reference patch and channel, its share of dL/d(sigma_c), written */
+} AvdCollabAdjoint;
 
 /* av-denoise-core/src/collab/kernels/fused/mod.rs:170 (`collab_fused`): one pass, queued on
  * `stream`. Adds into `accum`/`wsum` (integer adds: the result does not depend on scheduling). */
@@ -467,6 +483,16 @@ AVD_API AvdStatus avd_collab_pass(const AvdCollabPass* pass, void* stream);
  * and its filter (the reference's split search profile hands the same member words over,
  * av-denoise-core/src/collab/kernels/fused/split.rs). */
 AVD_API uint64_t avd_collab_member_bytes(uint32_t width, uint32_t height);
+
+/* Reference patches of one pass over a width x height plane (the rows of `grad_sigma_refs`). */
+AVD_API uint64_t avd_collab_refs(uint32_t width, uint32_t height);
+
+/* The adjoint of the pass `pass` describes, queued on `stream` after that pass (it reads the
+ * member words the pass's search left in `members`). Holds the groups and every keep decision
+ * fixed and reads the pass as A and W above: adds dL/d(ring) and writes each reference patch's
+ * share of dL/d(sigma) (sigma from the `noise` words; the weight-scale word read as proportional to
+ * sigma_0^2, as the engine derives it). An extension with no counterpart in the reference. */
+AVD_API AvdStatus avd_collab_adjoint(const AvdCollabPass* pass, const AvdCollabAdjoint* adjoint, void* stream);
 
 /* av-denoise-core/src/collab/kernels/transforms.rs:196-221 (`dct_noise_profile`). */
 AVD_API void avd_dct_noise_profile(float rho, float* out8);

@@ -264,6 +264,16 @@ struct CollabArgs {
     const float* colour_means;
     float colour_scale;
     int colour_on, colour_blocks_x;
+    // The empirical Wiener stage, an extension the reference does not have (its filter stops at the
+    // threshold): each kept coefficient z of noise variance v is scaled by g = z^2 / (z^2 + v), the
+    // group's thresholded spectrum serving as its own pilot, and the retained variance counts
+    // g^2 v. Zero keeps the reference's filter.
+    int wiener;
+    // Records of the pass, written when not null: the 9 member words per reference patch (8 packed
+    // positions, then k_use | use_grid << 8), and per reference patch, channel and lane the 64 keep
+    // decisions (bit j * 8 + i for member-axis coefficient j, slot i).
+    uint32_t* member_record;
+    uint64_t* mask_record;
 };
 
 struct Group {
@@ -408,7 +418,7 @@ namespace {
 // fused/pooled.rs: keep a coefficient on the mean energy of itself and its four frequency
 // neighbours (shuffled across lanes for the vertical ones). Returns each lane's retained variance.
 void pooled_threshold(Stack& s, const float* v, const float* prof, int k_use, float threshold, float dc_lambda,
-                      float* retained) {
+                      bool wiener, float* retained, uint64_t* bits) {
     float bar = threshold * threshold;
     for (int sub = 0; sub < P; ++sub) retained[sub] = 0.0f;
     for (int j = 0; j < MAX_K; ++j) {
@@ -450,8 +460,18 @@ void pooled_threshold(Stack& s, const float* v, const float* prof, int k_use, fl
                     if (j == 0) keep = keep || dc_lane;
                 }
                 const bool live = j < k_use;
-                kept_profile = kept_profile + (keep ? prof[i] : 0.0f);
-                out[sub][i] = (live && !keep) ? 0.0f : coeff;
+                if (wiener && live && keep) {
+                    const float cv = lane_var[sub] * prof[i];
+                    const float zz = coeff * coeff;
+                    const float den = zz + cv;
+                    const float gain = den > 0.0f ? zz / den : 1.0f;
+                    kept_profile = kept_profile + (gain * gain) * prof[i];
+                    out[sub][i] = gain * coeff;
+                } else {
+                    kept_profile = kept_profile + (keep ? prof[i] : 0.0f);
+                    out[sub][i] = (live && !keep) ? 0.0f : coeff;
+                }
+                if (keep && live) bits[sub] |= uint64_t{1} << (j * 8 + i);
             }
             if (j < k_use) retained[sub] = retained[sub] + kept_profile * lane_var[sub];
         }
@@ -522,6 +542,12 @@ void process_reference(const CollabArgs& a, uint32_t ref_x_index, uint32_t ref_y
             for (int m = 0; m < MAX_K; ++m) member_pos[m] = grid_pos[m];
             k_use = MAX_K;
         }
+    }
+
+    if (a.member_record) {
+        uint32_t* words = a.member_record + static_cast<size_t>(ref_y_index * refs_x + ref_x_index) * (MAX_K + 1);
+        for (int m = 0; m < MAX_K; ++m) words[m] = member_pos[m];
+        words[MAX_K] = k_use | (use_grid ? 0x100u : 0u);
     }
 
     // filter_group (mod.rs:559-850).
@@ -619,9 +645,10 @@ void process_reference(const CollabArgs& a, uint32_t ref_x_index, uint32_t ref_y
         }
         const float channel_lambda = c == 0 ? first_lambda : second_lambda;
         float retained[P];
+        uint64_t bits[P] = {};
         if (a.pooled) {
             pooled_threshold(s, mv, a.dct_profile, static_cast<int>(k_use), channel_lambda * a.pool_ratio,
-                             channel_lambda, retained);
+                             channel_lambda, a.wiener != 0, retained, bits);
         } else {
             for (int sub = 0; sub < P; ++sub) {
                 const float prof_sub = a.dct_profile[sub];
@@ -634,13 +661,25 @@ void process_reference(const CollabArgs& a, uint32_t ref_x_index, uint32_t ref_y
                         float& coeff = s.v[j][sub][i];
                         bool keep = std::fabs(coeff) >= channel_lambda * std::sqrt(cv);
                         if (j == 0 && i == 0 && sub == 0) keep = true;
-                        if (keep) rv = rv + cv;
-                        else coeff = 0.0f;
+                        if (keep && a.wiener) {
+                            const float zz = coeff * coeff;
+                            const float den = zz + cv;
+                            const float gain = den > 0.0f ? zz / den : 1.0f;
+                            coeff = gain * coeff;
+                            rv = rv + (gain * gain) * cv;
+                        } else if (keep) {
+                            rv = rv + cv;
+                        } else {
+                            coeff = 0.0f;
+                        }
+                        if (keep) bits[sub] |= uint64_t{1} << (j * 8 + i);
                     }
                 }
                 retained[sub] = rv;
             }
         }
+        if (a.mask_record)
+            for (int sub = 0; sub < P; ++sub) a.mask_record[(static_cast<size_t>(ref_idx) * C + c) * P + sub] = bits[sub];
         const float sum = reduce8(retained);
         const float weight = safe_reciprocal(sum, RECIPROCAL_FLOOR);
         if (c == 0) {

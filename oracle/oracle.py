@@ -408,7 +408,20 @@ class CollabArgs(C.Structure):
         ("c_min", C.c_float), ("lambda_ht", C.c_float), ("accum_scale", C.c_float), ("pool_ratio", C.c_float),
         ("weight_scale", C.c_float), ("pooled", C.c_int), ("curve_valid", C.c_int),
         ("colour_gains", _fp), ("colour_means", _fp), ("colour_scale", C.c_float), ("colour_on", C.c_int),
-        ("colour_blocks_x", C.c_int),
+        ("colour_blocks_x", C.c_int), ("wiener", C.c_int), ("member_record", _u32p),
+        ("mask_record", C.POINTER(C.c_uint64)),
+    ]
+
+
+class Collab64Args(C.Structure):
+    _fields_ = [
+        ("ring", _dp), ("members", _u32p), ("masks", C.POINTER(C.c_uint64)), ("neighbour_slots", _u32p),
+        ("sigma", _dp), ("dct_profile", _fp), ("kaiser", _fp), ("weight_scale", C.c_double),
+        ("weight_scale_sigma", C.c_double),
+        ("width", C.c_int), ("height", C.c_int), ("channels", C.c_int), ("centre_slot", C.c_int),
+        ("grid_frames", C.c_int), ("wiener", C.c_int),
+        ("accum", _dp), ("wsum", _dp), ("grad_accum", _dp), ("grad_wsum", _dp), ("grad_ring", _dp),
+        ("grad_sigma", _dp),
     ]
 
 
@@ -456,9 +469,12 @@ def collab_fused(ring: np.ndarray, width: int, height: int, channels: int, *, ce
                  mv_field=None, confidence=None, neighbour_slots=None, c_min=0.0, refine=0, spatial_radius=4,
                  k_max=8, sigma=(0.02,), lambda_ht=5.3, rho=0.0, profile=None, kaiser_beta=0.0,
                  noise_curve=None, pooled=None, blksize=16, blk_step=8, blocks_x=1, blocks_y=1,
-                 mv_stride=2, conf_stride=1, weight_scale_override=None, colour=None):
+                 mv_stride=2, conf_stride=1, weight_scale_override=None, colour=None, wiener=False,
+                 record=None):
     """One `collab_fused` launch on the CPU. Returns (accum, wsum, group_weight). `colour` is
-    (gains tables, block means on this plane's 16x16 grid, 8-bit scale) or None."""
+    (gains tables, block means on this plane's 16x16 grid, 8-bit scale) or None. `wiener` adds the
+    empirical Wiener stage. A dict passed as `record` receives the pass's member words ("members",
+    9 u32 per reference patch) and keep masks ("masks", refs x channels x 8 u64)."""
     ring = np.ascontiguousarray(ring, np.float32)
     frames = ring.size // (width * height * channels)
     profile = dct_noise_profile(rho) if profile is None else np.asarray(profile, np.float32)
@@ -495,10 +511,62 @@ def collab_fused(ring: np.ndarray, width: int, height: int, channels: int, *, ce
         cm = np.ascontiguousarray(colour[1], np.float32).reshape(-1)
         a.colour_gains, a.colour_means, a.colour_scale = _f(cg), _f(cm), float(colour[2])
         a.colour_on, a.colour_blocks_x = 1, -(-width // 16)
+    a.wiener = int(bool(wiener))
+    refs = refs_along(width) * refs_along(height)
+    if record is not None:
+        record["members"] = np.zeros(refs * 9, np.uint32)
+        record["masks"] = np.zeros(refs * channels * 8, np.uint64)
+        a.member_record = record["members"].ctypes.data_as(_u32p)
+        a.mask_record = record["masks"].ctypes.data_as(C.POINTER(C.c_uint64))
+        record["weight_scale"] = ws
+        record["sigma"] = sig
+        record["profile"] = profile
+        record["kaiser"] = kaiser
     l = lib()
     l.orc_collab_fused.argtypes = [C.POINTER(CollabArgs)]
     l.orc_collab_fused(C.byref(a))
     return accum, wsum, gw
+
+
+def collab64(ring: np.ndarray, width: int, height: int, channels: int, record: dict, *, centre_slot=0, radius=0,
+             neighbour_slots=None, sigma=None, wiener=False, grad_accum=None, grad_wsum=None):
+    """The f64 pass of collab_adjoint_oracle.cpp over the groups and keep masks of `record` (from
+    `collab_fused(..., record=...)`). Without gradients returns (accum, wsum) in real units; with
+    `grad_accum` and `grad_wsum` returns (grad_ring, grad_sigma). `sigma` (per channel, f64)
+    defaults to the recorded pass's."""
+    ring = np.ascontiguousarray(ring, np.float64)
+    frames = ring.size // (width * height * channels)
+    sig = np.ascontiguousarray(record["sigma"] if sigma is None else sigma, np.float64)
+    if sig.size < channels:
+        sig = np.full(channels, sig[0], np.float64)
+    slots = np.ascontiguousarray(neighbour_slots if neighbour_slots is not None else np.zeros(1, np.uint32),
+                                 np.uint32)
+    prof = np.ascontiguousarray(record["profile"], np.float32)
+    kai = np.ascontiguousarray(record["kaiser"], np.float32)
+    a = Collab64Args()
+    a.ring, a.members = ring.ctypes.data_as(_dp), record["members"].ctypes.data_as(_u32p)
+    a.masks = record["masks"].ctypes.data_as(C.POINTER(C.c_uint64))
+    a.neighbour_slots, a.sigma = slots.ctypes.data_as(_u32p), sig.ctypes.data_as(_dp)
+    a.dct_profile, a.kaiser, a.weight_scale = _f(prof), _f(kai), float(record["weight_scale"])
+    a.weight_scale_sigma = float(np.float32(record["sigma"][0]))
+    a.width, a.height, a.channels, a.centre_slot = width, height, channels, centre_slot
+    a.grid_frames, a.wiener = grid_frames(radius), int(bool(wiener))
+    l = lib()
+    l.orc64_collab_pass.argtypes = [C.POINTER(Collab64Args)]
+    if grad_accum is None:
+        accum = np.zeros(width * height * channels * frames, np.float64)
+        wsum = np.zeros(width * height * frames, np.float64)
+        a.accum, a.wsum = accum.ctypes.data_as(_dp), wsum.ctypes.data_as(_dp)
+        l.orc64_collab_pass(C.byref(a))
+        return accum, wsum
+    ga = np.ascontiguousarray(grad_accum, np.float64)
+    gw = np.ascontiguousarray(grad_wsum, np.float64)
+    grad_ring = np.zeros_like(ring)
+    grad_sigma = np.zeros(channels, np.float64)
+    a.grad_accum, a.grad_wsum = ga.ctypes.data_as(_dp), gw.ctypes.data_as(_dp)
+    a.grad_ring, a.grad_sigma = grad_ring.ctypes.data_as(_dp), grad_sigma.ctypes.data_as(_dp)
+    l.orc64_collab_pass(C.byref(a))
+    return grad_ring, grad_sigma
 
 
 # ---- block-matching motion search (motion_oracle.cpp) -------------------------------------------
@@ -980,7 +1048,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
                 pool_ratio: float | None = None, thsad_scale=1.0, context: int = 0, chained: bool = False,
                 refine_radius: int = 2, noise=None, field_lambda: float = 1.0, share_writes: MotionShare | None = None,
                 share_reads: MotionShare | None = None, ceiling: int = 0, camera_model: bool = True,
-                models: "PairModels | None" = None) -> list[np.ndarray]:
+                models: "PairModels | None" = None, wiener: bool = False) -> list[np.ndarray]:
     """The NL4D engine with a pinned sigma and Direct or Chained motion over a
     stream of (H, W, C) f32 frames; returns the emitted (H, W, C) f32 frames in order. With
     `field_lambda` > 0 the truemotion stage ends the Direct window search (reading the window's SAD
@@ -1003,7 +1071,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
     (nlmeans/dispatch/motion.rs:231-310), and no motion of this plane's own is searched. With
     `camera_model` a pass that searches its own motion also searches around the camera models
     fitted on channel 0 of the pushed frames (`models`, else a `PairModels` fed every frame in
-    order), as in `nlm_stream_mc`."""
+    order), as in `nlm_stream_mc`. `wiener` adds the empirical Wiener stage to every pass."""
     h, w, c = frames[0].shape
     tf = 2 * d + 1
     step = blksize - overlap
@@ -1073,7 +1141,7 @@ def nl4d_stream(frames: list[np.ndarray], d: int, sigma: float, *, blksize=16, o
                                   weight_scale_override=p_weight, lambda_ht=lambda_ht,
                                   kaiser_beta=kaiser_beta, noise_curve=p_curve, colour=p_colour,
                                   pooled=pool_ratio, blksize=blksize, blk_step=step, blocks_x=bx, blocks_y=by,
-                                  mv_stride=bx * by * 2, conf_stride=bx * by)
+                                  mv_stride=bx * by * 2, conf_stride=bx * by, wiener=wiener)
         accum[:] += acc.reshape(tf, -1)
         wsum[:] += ws.reshape(tf, -1)
 

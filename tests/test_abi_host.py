@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.avd_abi_version() == 5
+    assert lib.avd_abi_version() == 6
 
 
 def test_status_messages(lib):
