@@ -1067,6 +1067,72 @@ def run_adjoint(reps: int) -> None:
     print(json.dumps({"workload": "NLMeans adjoint, 1920x1080 luma f32 window, d=2 a=5 s=2 strength 8",
                       "forward_ms": round(f_ms, 4), "backward_ms": round(b_ms, 4),
                       "backward_over_forward": round(b_ms / f_ms, 3)}))
+    run_nl4d_adjoint(reps)
+
+
+def run_nl4d_adjoint(reps: int) -> None:
+    """The NL4D collab pass (`avd_collab_pass`: group search and filter) against its adjoint
+    (`avd_collab_adjoint`) on one 1920x1080 luma window of 5 frames (temporal radius 2, spatial
+    radius 9, refine 2, plain threshold 2.7 sigma, zero motion at full confidence), with and without
+    the Wiener stage. CUDA events on one stream; the accumulators are cleared outside the timed
+    region. One JSON line per setting."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import av_denoise_b200_loader
+
+    av_denoise_b200_loader.load()
+    from av_denoise_b200 import _abi, synth
+    from av_denoise_b200.autograd import Nl4dPassConfig, _Nl4dState
+
+    lib = _abi.load()
+    w, h, d = W, H, 2
+    clip = synth.make_clip(w, h, 2 * d + 1, depth=8, chroma="gray", sigma_luma=10.0, global_motion=0, sprites=3,
+                           seed=9)
+    window = torch.from_numpy(np.stack([f[0].astype(np.float32) / 255.0 for f in clip])[..., None].copy()).cuda()
+    sigma = torch.tensor([10.0 / 255.0], device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    for wiener in (False, True):
+        cfg = Nl4dPassConfig(radius=d, spatial_radius=9, refine=2, lambda_ht=2.7, wiener=wiener)
+        st = _Nl4dState(window, sigma, cfg)
+        grad_accum = torch.randn(st.accum.numel(), device="cuda")
+        grad_wsum = torch.randn(st.wsum.numel(), device="cuda")
+        grad_window = torch.zeros_like(window)
+        grad_refs = torch.empty(st.refs, device="cuda")
+        adj = _abi.AvdCollabAdjoint(grad_accum.data_ptr(), grad_wsum.data_ptr(), grad_window.data_ptr(),
+                                    grad_refs.data_ptr())
+
+        def backward():
+            code = lib.avd_collab_adjoint(C.byref(st.p), C.byref(adj), C.c_void_p(stream.cuda_stream))
+            if code != 0:
+                raise RuntimeError(lib.avd_last_error().decode())
+
+        fwd, bwd = [], []
+        for i in range(reps + 2):
+            st.accum.zero_()
+            st.wsum.zero_()
+            f = timed(st.run)
+            grad_window.zero_()
+            b = timed(backward)
+            if i >= 2:
+                fwd.append(f)
+                bwd.append(b)
+        f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
+        print(json.dumps({"workload": "NL4D collab pass adjoint, 1920x1080 luma window of 5 frames, spatial radius 9, "
+                                      "refine 2, threshold 2.7" + (", Wiener stage" if wiener else ""),
+                          "forward_ms": round(f_ms, 4), "backward_ms": round(b_ms, 4),
+                          "backward_over_forward": round(b_ms / f_ms, 3)}))
 
 
 def run_batch(reps: int) -> None:
