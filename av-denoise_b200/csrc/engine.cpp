@@ -158,6 +158,8 @@ class NlmPass final : public Pass {
         return Failure{AVD_ERR_GPU, "forced failure"};
     }
 
+    bool reads_luma() const override { return reads_share_; }
+
     std::optional<std::pair<PairModelMode, int>> pair_model_mode() const override {
         if (!mc_ || reads_share_) return std::nullopt;
         const AvdMotionSearch& m = params_.motion.search;
@@ -1120,6 +1122,29 @@ class PassthroughRing {
 
 // ---------------------------------------------------------------------------------------------
 // The planar engine: engine/planar.rs:104-580.
+// A second stream for a chroma pass that runs beside the luma pass of the same push, forked from
+// and joined back into the engine's stream with two events; made on first use.
+struct SideStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+
+    cudaError_t ensure() {
+        cudaError_t e = cudaSuccess;
+        if (!stream) e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess && !fork) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        if (e == cudaSuccess && !join) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+        return e;
+    }
+    ~SideStream() {
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+    }
+};
+
 struct AvdEngine {
     AvdGeometry geometry{};
     std::unique_ptr<avd::Pass> luma, chroma;
@@ -1131,9 +1156,13 @@ struct AvdEngine {
     bool poisoned = false;
     int device = 0;
     cudaStream_t stream = nullptr;
+    SideStream side;  // declared after the passes: destroyed (and drained) before them
     std::string last_error;
 
     avd::Pass* lead() const { return luma ? luma.get() : chroma.get(); }
+    // The chroma pass of a push runs beside the luma pass when it reads nothing the luma pass (or
+    // the engine's colour measurement) writes in that push.
+    bool overlaps_chroma() const { return luma && chroma && !luma_guides && !colour && !chroma->reads_luma(); }
 };
 
 namespace {
@@ -1385,9 +1414,24 @@ AvdStatus avd_engine_push(AvdEngine* e, const AvdPlane* planes, size_t n, size_t
     if (auto f = fit_pair_model(e, planes, frame)) return record(e, f);
     if (auto f = measure_colour(e, planes, frame)) return record(e, f);
     size_t value = 0;
+    // The chroma pass on the side stream, forked after everything queued so far and joined back
+    // before anything the caller queues next: the luma kernels' tail waves share the GPU with it.
+    const bool overlap = e->overlaps_chroma() && e->side.ensure() == cudaSuccess &&
+                         cudaEventRecord(e->side.fork, e->stream) == cudaSuccess &&
+                         cudaStreamWaitEvent(e->side.stream, e->side.fork, 0) == cudaSuccess;
+    if (overlap) e->chroma->stream = e->side.stream;
     auto f = forward(e, &value, [&](avd::Pass* p, bool luma, size_t* v) {
         return p->push(group_planes(planes, luma), v);
     });
+    if (overlap) {
+        e->chroma->stream = e->stream;
+        cudaError_t err = cudaEventRecord(e->side.join, e->side.stream);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(e->stream, e->side.join, 0);
+        if (err != cudaSuccess && !f) {
+            e->poisoned = true;
+            f = Failure{AVD_ERR_GPU, avd::cuda_message("side stream join", err)};
+        }
+    }
     if (f) return record(e, f);
     if (e->passthrough) {
         const AvdPlane* src = e->passthrough_luma ? planes : planes + 1;

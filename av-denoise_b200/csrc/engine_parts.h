@@ -254,6 +254,9 @@ class Pass {
     virtual std::optional<Failure> attach_models(const PairModels*) { return std::nullopt; }
     virtual bool measures_colour() const { return false; }
     virtual std::optional<Failure> measure_colour(const ColourMeans*, bool) { return std::nullopt; }
+    // Whether the pass reads anything the luma pass of the same push writes (the shared luma
+    // motion); a chroma pass that does not may run beside the luma pass on a second stream.
+    virtual bool reads_luma() const { return false; }
     cudaStream_t stream = nullptr;
 };
 

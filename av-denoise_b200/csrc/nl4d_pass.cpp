@@ -198,6 +198,8 @@ class Nl4dPass final : public Pass {
         poisoned_ = true;
         return Failure{AVD_ERR_GPU, "forced failure"};
     }
+    bool reads_luma() const override { return reads_share_; }
+
     std::optional<std::pair<PairModelMode, int>> pair_model_mode() const override {
         if (d_ == 0 || reads_share_) return std::nullopt;
         PairModelMode mode;
