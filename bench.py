@@ -240,6 +240,7 @@ def run_gpu(args) -> None:
     clock_path = Path(tempfile.gettempdir()) / f"avd_bench_clocks_{os.getpid()}_rank{rank}.csv"
     proc = clocks_start(clock_path)
     eng_l.sample_device_time(1)
+    eng_c.sample_device_time(1)
     times = []
     wall0 = time.perf_counter()
     for _ in range(args.steps):
@@ -252,6 +253,9 @@ def run_gpu(args) -> None:
     wall = time.perf_counter() - wall0
     nlm_timing = eng_l.timing().luma  # window kernel + exact finish per luma frame
     eng_l.sample_device_time(0)
+    ct = eng_c.timing()
+    chroma_timing = ct.chroma if ct.chroma is not None else ct.luma  # the chroma engine's one pass
+    eng_c.sample_device_time(0)
 
     # End to end: pinned host frames -> device -> engines -> device -> pinned host. Output frame k
     # gathers its chroma when the chroma engine emits it (at push k) and its luma when the luma engine
@@ -402,7 +406,14 @@ def run_gpu(args) -> None:
                      "peak_note": f"MUFU ex2: {sms} SMs x 16/clk x sm_max_mhz {peaks['sm_max_mhz']} "
                                   f"({peaks['source']})",
                      "launch_ms": round(t_window * 1e3, 4),
-                     "luma_frame_ms_with_exact_finish": round(t_luma_frame * 1e3, 4)},
+                     "luma_frame_ms_with_exact_finish": round(t_luma_frame * 1e3, 4),
+                     # pixels per luma frame the exact finish recomputed in the reference's order
+                     "exact_samples_per_frame": round(nlm_timing.exact_samples / max(1, nlm_timing.frames), 1),
+                     # the chroma engine's frame (window kernel + exact finish) on its own stream
+                     "chroma_frame_ms_with_exact_finish": round(
+                         chroma_timing.device_time / max(1, chroma_timing.frames) * 1e3, 4),
+                     "chroma_exact_samples_per_frame": round(
+                         chroma_timing.exact_samples / max(1, chroma_timing.frames), 1)},
         "roofline_hbm": {"bound": "hbm", "achieved": round(hbm_bytes / t_window / 1e9, 2),
                          "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(hbm_bytes / t_window / 1e9 / peaks["hbm_gbs"], 5)},
