@@ -26,7 +26,9 @@
 // How (B200 layout). One warp per flagged pixel, no block-wide barriers: many pixels are in
 // flight on every SM, which hides the latency of the window staging and of the order-bound folds.
 // For each pass the warp stages its pixel's search windows (the (2(a+s)+1)^2 neighbourhood of each
-// frame the pass compares, coordinates clamped) in its own shared memory, then every lane forms
+// frame the pass compares, coordinates clamped) in its own shared memory (a launch with only the
+// single-frame pass double-buffers it: the next pixel's copies fly while this one is computed, and
+// the averaged samples are read from the window too), then every lane forms
 // distances two at a time as two independent chains (a pair's forward and backward offset, or two
 // spatial offsets), reading the centre patch as a broadcast and the taps at immediate offsets when
 // the patch radius is a template argument (0..3; a generic loop reading the frames covers larger
@@ -183,10 +185,96 @@ __global__ void __launch_bounds__(kWarps * 32) nlm_exact_kernel(NlmLaunch a, int
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     };
+    // A single-frame launch (no pair passes) stages one window per pixel, so its windows are
+    // double-buffered in the two window slots: the next pixel's copies are in flight while this
+    // pixel's distances are formed.
+    const bool prefetch = S >= 0 && a.pairs == 0;
+    auto issue = [&](float* dst, int64_t item) {
+        const int pn = a.fix_list ? a.fix_list[item] : static_cast<int>(item);
+        const int qx = pn % W, qy = pn / W, n = rs * rs;
+        for (int k = lane; k < n; k += 32) {
+            const int ry = k / rs, rx = k - ry * rs;
+            const float* src = at<C>(rctr, qx - R + rx, qy - R + ry, W, H);
+            const unsigned dst_s = static_cast<unsigned>(__cvta_generic_to_shared(dst + k * C));
+            if (C == 1)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst_s), "l"(src) : "memory");
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst_s), "l"(src) : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    // The single-frame pass's items of pixel (px, py) into `it` (rows: W, then per channel I w, over
+    // q != 0), from the staged window `sw`; every lane calls it.
+    auto single_items = [&](float* it, const float* sw, int px, int py) {
+        // rows: W, then per channel I w, over q != 0; a lane forms items j and j + 32
+        const int n = nq - 1;
+        for (int j = lane; j < n; j += 64) {
+            const bool two = j + 32 < n;
+            const int l0 = j < mid ? j : j + 1;
+            const int j1 = two ? j + 32 : j;
+            const int l1 = j1 < mid ? j1 : j1 + 1;
+            const int qx0 = qtab[l0] - A, qy0 = qtab[l0 + nq] - A;
+            const int qx1 = qtab[l1] - A, qy1 = qtab[l1 + nq] - A;
+            float2 d;
+            if (S >= 0) {
+                d = distances_staged<C, (S >= 0 ? S : 0)>(
+                    sw + (R - s) * wstride + (R - s) * C, wstride,
+                    sw + (R + qy0 - s) * wstride + (R + qx0 - s) * C,
+                    sw + (R + qy1 - s) * wstride + (R + qx1 - s) * C, wstride, scale);
+            } else {
+                d = distances_generic<C>(rctr, px, py, s, rctr, px + qx0 - s, py + qy0 - s, rctr,
+                                         px + qx1 - s, py + qy1 - s, W, H, scale);
+            }
+            const float w0 = welsch_mirror(d.x, h2, lut ? __ldg(a.spatial_lut + l0) : 0.0f);
+            const float w1 = welsch_mirror(d.y, h2, lut ? __ldg(a.spatial_lut + l1) : 0.0f);
+            float v0[C], v1[C];
+            if (S >= 0 && !a.ref_ring) {
+                // The staged centre window holds the same clamped samples.
+                const float* n0 = sw + (R + qy0) * wstride + (R + qx0) * C;
+                const float* n1 = sw + (R + qy1) * wstride + (R + qx1) * C;
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    v0[c] = n0[c];
+                    v1[c] = n1[c];
+                }
+            } else {
+                const float* n0 = at<C>(ctr, px + qx0, py + qy0, W, H);
+                const float* n1 = at<C>(ctr, px + qx1, py + qy1, W, H);
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    v0[c] = __ldg(n0 + c);
+                    v1[c] = __ldg(n1 + c);
+                }
+            }
+            it[j] = w0;
+#pragma unroll
+            for (int c = 0; c < C; ++c) it[(1 + c) * n + j] = __fmul_rn(v0[c], w0);
+            if (two) {
+                it[j + 32] = w1;
+#pragma unroll
+                for (int c = 0; c < C; ++c) it[(1 + c) * n + j + 32] = __fmul_rn(v1[c], w1);
+            }
+        }
+    };
 
-    for (int64_t i = (int64_t)blockIdx.x * kWarps + warp; i < count; i += (int64_t)gridDim.x * kWarps) {
+    const int64_t first = (int64_t)blockIdx.x * kWarps + warp, stride = (int64_t)gridDim.x * kWarps;
+    int cur = 0;
+    if (prefetch && first < count) issue(win0, first);
+
+    for (int64_t i = first; i < count; i += stride) {
         const int pix = a.fix_list ? a.fix_list[i] : static_cast<int>(i);
         const int px = pix % W, py = pix / W;
+        float* sw = win0;  // the staged window of the single-frame pass
+        if (prefetch) {
+            sw = cur ? win1 : win0;
+            if (i + stride < count) {
+                issue(cur ? win0 : win1, i + stride);
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            }
+            __syncwarp();
+        }
         // lanes 0..kRoles-1: the frame's accumulators (sum I w per channel, sum w, max w)
         float acc = 0.0f;
 
@@ -241,54 +329,34 @@ __global__ void __launch_bounds__(kWarps * 32) nlm_exact_kernel(NlmLaunch a, int
                             wf = __fmul_rn(wf, cf);
                             wb = __fmul_rn(wb, cb);
                         }
-                        const float* fp = at<C>(fwd, px + qx, py + qy, W, H);
-                        const float* bp = at<C>(bwd, px - qx, py - qy, W, H);
                         it[q] = wf;
                         it[nq + q] = wb;
+                        if (S >= 0 && !a.ref_ring) {
+                            // The averaged samples are the staged windows' own (same clamped pixels).
+                            const float* fp = win0 + (R + qy) * wstride + (R + qx) * C;
+                            const float* bp = win1 + (R - qy) * wstride + (R - qx) * C;
 #pragma unroll
-                        for (int c = 0; c < C; ++c) {
-                            it[(2 + 2 * c) * nq + q] = __fmul_rn(__ldg(fp + c), wf);
-                            it[(3 + 2 * c) * nq + q] = __fmul_rn(__ldg(bp + c), wb);
+                            for (int c = 0; c < C; ++c) {
+                                it[(2 + 2 * c) * nq + q] = __fmul_rn(fp[c], wf);
+                                it[(3 + 2 * c) * nq + q] = __fmul_rn(bp[c], wb);
+                            }
+                        } else {
+                            const float* fp = at<C>(fwd, px + qx, py + qy, W, H);
+                            const float* bp = at<C>(bwd, px - qx, py - qy, W, H);
+#pragma unroll
+                            for (int c = 0; c < C; ++c) {
+                                it[(2 + 2 * c) * nq + q] = __fmul_rn(__ldg(fp + c), wf);
+                                it[(3 + 2 * c) * nq + q] = __fmul_rn(__ldg(bp + c), wb);
+                            }
                         }
                     }
                 } else {
-                    if (S >= 0) {
+                    if (S >= 0 && !prefetch) {
                         __syncwarp();
                         stage(win0, rctr, px, py, R);
                         __syncwarp();
                     }
-                    // rows: W, then per channel I w, over q != 0; a lane forms items j and j + 32
-                    const int n = nq - 1;
-                    for (int j = lane; j < n; j += 64) {
-                        const bool two = j + 32 < n;
-                        const int l0 = j < mid ? j : j + 1;
-                        const int j1 = two ? j + 32 : j;
-                        const int l1 = j1 < mid ? j1 : j1 + 1;
-                        const int qx0 = qtab[l0] - A, qy0 = qtab[l0 + nq] - A;
-                        const int qx1 = qtab[l1] - A, qy1 = qtab[l1 + nq] - A;
-                        float2 d;
-                        if (S >= 0) {
-                            d = distances_staged<C, (S >= 0 ? S : 0)>(
-                                win0 + (R - s) * wstride + (R - s) * C, wstride,
-                                win0 + (R + qy0 - s) * wstride + (R + qx0 - s) * C,
-                                win0 + (R + qy1 - s) * wstride + (R + qx1 - s) * C, wstride, scale);
-                        } else {
-                            d = distances_generic<C>(rctr, px, py, s, rctr, px + qx0 - s, py + qy0 - s, rctr,
-                                                     px + qx1 - s, py + qy1 - s, W, H, scale);
-                        }
-                        const float w0 = welsch_mirror(d.x, h2, lut ? __ldg(a.spatial_lut + l0) : 0.0f);
-                        const float w1 = welsch_mirror(d.y, h2, lut ? __ldg(a.spatial_lut + l1) : 0.0f);
-                        const float* n0 = at<C>(ctr, px + qx0, py + qy0, W, H);
-                        const float* n1 = at<C>(ctr, px + qx1, py + qy1, W, H);
-                        it[j] = w0;
-#pragma unroll
-                        for (int c = 0; c < C; ++c) it[(1 + c) * n + j] = __fmul_rn(__ldg(n0 + c), w0);
-                        if (two) {
-                            it[j + 32] = w1;
-#pragma unroll
-                            for (int c = 0; c < C; ++c) it[(1 + c) * n + j + 32] = __fmul_rn(__ldg(n1 + c), w1);
-                        }
-                    }
+                    single_items(it, sw, px, py);
                 }
                 off += pass_floats(C, side, p < a.pairs);
             }
@@ -359,6 +427,7 @@ __global__ void __launch_bounds__(kWarps * 32) nlm_exact_kernel(NlmLaunch a, int
                 }
             }
         }
+        cur ^= 1;  // every lane is past this pixel's window reads (the fold's __syncwarp)
     }
 }
 

@@ -240,7 +240,6 @@ def run_gpu(args) -> None:
     clock_path = Path(tempfile.gettempdir()) / f"avd_bench_clocks_{os.getpid()}_rank{rank}.csv"
     proc = clocks_start(clock_path)
     eng_l.sample_device_time(1)
-    eng_c.sample_device_time(1)
     times = []
     wall0 = time.perf_counter()
     for _ in range(args.steps):
@@ -253,6 +252,11 @@ def run_gpu(args) -> None:
     wall = time.perf_counter() - wall0
     nlm_timing = eng_l.timing().luma  # window kernel + exact finish per luma frame
     eng_l.sample_device_time(0)
+    # The chroma engine's frame, sampled on one more (untimed) step so the timed steps carry only
+    # the luma engine's sampling events.
+    eng_c.sample_device_time(1)
+    step_device()
+    torch.cuda.synchronize()
     ct = eng_c.timing()
     chroma_timing = ct.chroma if ct.chroma is not None else ct.luma  # the chroma engine's one pass
     eng_c.sample_device_time(0)
