@@ -161,8 +161,18 @@ struct Smem {
     int nstride, nrows, ncols;
 };
 
+// Whether a tile CTA stages its centre tile in the row-sum buffers: with the centre runs kept in
+// registers (CTR_REG) the staged tile is read once, before the first step writes a row sum, and the
+// finish reads the centre values from the frame, so the tile needs no space of its own. That keeps a
+// luma tile at s=2, a=5 and two pairs under 38 KB, six CTAs to an SM. Not in the adjoint's record
+// tiles, whose finish reads the staged tile.
+template <int C, int S, bool REC>
+__host__ __device__ constexpr bool centre_in_row_sums() {
+    return Cfg<C, S>::CTR_REG && !REC && round_up4(Cfg<C, S>::CROWS * Cfg<C, S>::CSTRIDE) <= 2 * Cfg<C, S>::HS_BUF;
+}
+
 // Dynamic shared memory of one tile CTA for search radius A, `pairs` temporal pair passes and,
-// with `ref`, the input value tiles beside the reference tiles.
+// with `ref`, the input value tiles beside the reference tiles (forward tiles, not the records).
 template <int C, int S>
 inline size_t nlm_smem_bytes(int A, int pairs, bool ref) {
     using K = Cfg<C, S>;
@@ -170,7 +180,8 @@ inline size_t nlm_smem_bytes(int A, int pairs, bool ref) {
     const int ncols = kTX + 2 * S + 2 * A;
     const int nstride = nbr_stride(ncols, C);
     const size_t tiles = (size_t)round_up4((pairs > 0 ? 2 : 1) * nrows * nstride);
-    const size_t floats = (size_t)round_up4(K::CROWS * K::CSTRIDE) + (ref ? 2 : 1) * tiles + (size_t)2 * K::HS_BUF;
+    const size_t ctr = centre_in_row_sums<C, S, false>() ? 0 : (size_t)round_up4(K::CROWS * K::CSTRIDE);
+    const size_t floats = ctr + (ref ? 2 : 1) * tiles + (size_t)2 * K::HS_BUF;
     return floats * sizeof(float);
 }
 
@@ -338,17 +349,24 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
     const int y0 = (tid >> 5) * V;
     const int side = 2 * A + 1;
 
+    constexpr bool kCtrAlias = centre_in_row_sums<C, S, REC>();
     Smem sm;
     sm.nrows = K::TY + 2 * S + 2 * A;
     sm.ncols = kTX + 2 * S + 2 * A;
     sm.nstride = nbr_stride(sm.ncols, C);
-    sm.ctr = smem_raw;
-    sm.nbr[0] = sm.ctr + round_up4(K::CROWS * K::CSTRIDE);
-    sm.nbr[1] = sm.nbr[0] + sm.nrows * sm.nstride;
     const int tile_floats = round_up4((a.pairs > 0 ? 2 : 1) * sm.nrows * sm.nstride);
+    if (kCtrAlias) {
+        sm.hs = smem_raw;
+        sm.ctr = smem_raw;  // read by the centre runs before the first step writes a row sum
+        sm.nbr[0] = smem_raw + 2 * K::HS_BUF;
+    } else {
+        sm.ctr = smem_raw;
+        sm.nbr[0] = sm.ctr + round_up4(K::CROWS * K::CSTRIDE);
+    }
+    sm.nbr[1] = sm.nbr[0] + sm.nrows * sm.nstride;
     sm.val[0] = sm.nbr[0] + tile_floats;
     sm.val[1] = sm.val[0] + sm.nrows * sm.nstride;
-    sm.hs = sm.nbr[0] + (REF ? 2 : 1) * tile_floats;
+    if (!kCtrAlias) sm.hs = sm.nbr[0] + (REF ? 2 : 1) * tile_floats;
 
     const float h2 = __ldg(a.derived + a.h2_word);
     const float off_pair = __ldg(a.derived + a.offset_word);
@@ -510,8 +528,8 @@ __device__ __forceinline__ void nlm_tile(const NlmLaunch& a, int tile_x, int til
             const float wsum = acc.ws[k].x + acc.ws[k].y;
             // The centre value: the input's own (accumulate.rs:175-201 reads the input ring), which
             // the reference-ring tile does not hold.
-            const float* orig =
-                REF ? centre + ((int64_t)gy * W + gx) * C : sm.ctr + (y0 + k + S) * K::CSTRIDE + (col + S) * C;
+            const float* orig = (REF || kCtrAlias) ? centre + ((int64_t)gy * W + gx) * C
+                                                   : sm.ctr + (y0 + k + S) * K::CSTRIDE + (col + S) * C;
             const float self_weight = __fmul_rn(a.wref, max_w);
             const float denom = __fadd_rn(self_weight, wsum);
             float* dst = a.out + ((int64_t)gy * W + gx) * C;
