@@ -228,10 +228,10 @@ AvdStatus avd_nlm_backward(const AvdNlmBackward* p, void* stream) {
         return fail(AVD_ERR_INVALID_OPTIONS, "nlm backward: radius past the NLMeans limits");
     if (avd::nlm_backward_smem_bytes(static_cast<int>(p->channels), static_cast<int>(p->temporal_radius),
                                      static_cast<int>(p->search_radius), static_cast<int>(p->patch_radius)) >
-        200u * 1024u)
+        226u * 1024u)
         return fail(AVD_ERR_INVALID_OPTIONS,
-                    "nlm backward: the staged frames and gradient tiles, 2 (2d+1)(32+2(a+s))(8+2(a+s)) x channels "
-                    "floats, exceed 200 KiB of shared memory");
+                    "nlm backward: the staged frames and gradient tiles exceed the 226 KiB of dynamic shared memory a "
+                    "CTA may hold");
     if (!(p->strength > 0.0f)) return fail(AVD_ERR_INVALID_OPTIONS, "nlm backward: strength must be positive");
     avd::NlmBackwardLaunch l{};
     l.window = reinterpret_cast<const float*>(p->window);

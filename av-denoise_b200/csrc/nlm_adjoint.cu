@@ -30,6 +30,7 @@
 
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 
 #include "kernels.h"
 #include "nlm_tile.cuh"
@@ -58,7 +59,7 @@ size_t grad_smem_bytes(int A) {
     const size_t tile = (size_t)round_up4(nrows * nstride);
     constexpr int RPS = (K::TY + 2 * S + 3) / 4;  // extended rows per column strip
     const size_t floats = (size_t)round_up4(K::CROWS * K::CSTRIDE) + 4 * tile + (size_t)K::HR * kHsStride +
-                          (size_t)2 * K::TY * kTX + (size_t)2 * 4 * RPS * kTX;
+                          (size_t)2 * (2 * S + 1 + 4 * RPS) * kTX + (size_t)2 * 4 * RPS * (kTX + 4 * S);
     return floats * sizeof(float);
 }
 
@@ -109,8 +110,9 @@ __device__ void flush_tile(const float* tile, int stride, int rows, int cols, fl
     }
 }
 
-__device__ __forceinline__ void add_to(float* p, float v, bool atomic) {
-    if (atomic)
+template <bool ATOMIC>
+__device__ __forceinline__ void add_to(float* p, float v) {
+    if constexpr (ATOMIC)
         atomicAdd(p, v);
     else
         *p += v;
@@ -144,8 +146,15 @@ __global__ void __launch_bounds__(kThreads) nlm_grad_kernel(GradArgs g) {
     float* gt0 = nbr1 + tile_floats;
     float* gt1 = gt0 + tile_floats;
     float* hs = gt1 + tile_floats;                              // HR x kHsStride
-    float2* et = reinterpret_cast<float2*>(hs + K::HR * kHsStride);  // TY x 32 lane pairs: dL/dD * 2 scale
-    float2* gv = et + K::TY * kTX;                              // 4 RPS x 32 lane pairs: its vertical box
+    // dL/dD * 2 scale per tile row and lane pair, rows -ETOP..-1 and TY..4 RPS - 1 held at zero so the
+    // vertical box reads them unguarded; then its vertical box on the extended rows, each row padded
+    // with 2s zero lane pairs on both sides so the horizontal box reads them unguarded.
+    constexpr int ETOP = 2 * S + 1;
+    constexpr int GVW = kTX + 4 * S;
+    float2* et_raw = reinterpret_cast<float2*>(hs + K::HR * kHsStride);
+    float2* et = et_raw + ETOP * kTX;
+    float2* gv = et_raw + (ETOP + 4 * RPS) * kTX;
+    for (int i = tid; i < (ETOP + 4 * RPS) * kTX + 4 * RPS * GVW; i += kThreads) et_raw[i] = f2(0.0f, 0.0f);
 
     const float h2 = g.h2;
     const float off_pair = __ldg(a.derived + a.offset_word);
@@ -207,8 +216,11 @@ __global__ void __launch_bounds__(kThreads) nlm_grad_kernel(GradArgs g) {
     }
 
     // One step: two offsets (lanes) against the staged tiles t0 / t1, their gradient tiles g0 / g1.
-    auto grad_step = [&](const float* t0, const float* t1, float* g0, float* g1, int dx0, int dy0, int dx1, int dy1,
-                         int id0, int id1, float2 negoff, bool atomic) {
+    // `atomic_tag` (std::true_type or std::false_type): whether the two lanes may scatter into the
+    // same gradient tile (the single-frame pass) and so add with shared atomics.
+    auto grad_step = [&](auto atomic_tag, const float* t0, const float* t1, float* g0, float* g1, int dx0, int dy0,
+                         int dx1, int dy1, int id0, int id1, float2 negoff) {
+        constexpr bool kAtomic = decltype(atomic_tag)::value;
         // Phase 1: the row box sums of both lanes' squared differences (the forward's).
         for (int slot = tid; slot < K::TASK_SLOTS; slot += kThreads) {
             const int r = ((slot >> 5) << 3) + (slot & 7);
@@ -256,8 +268,8 @@ __global__ void __launch_bounds__(kThreads) nlm_grad_kernel(GradArgs g) {
                     for (int c = 0; c < C; ++c) {
                         gw0 += pg.gamma[c][k] * (t0[i0 + c] - pg.out[c][k]);
                         gw1 += pg.gamma[c][k] * (t1[i1 + c] - pg.out[c][k]);
-                        add_to(g0 + i0 + c, pg.gamma[c][k] * w.x, atomic);
-                        add_to(g1 + i1 + c, pg.gamma[c][k] * w.y, atomic);
+                        add_to<kAtomic>(g0 + i0 + c, pg.gamma[c][k] * w.x);
+                        add_to<kAtomic>(g1 + i1 + c, pg.gamma[c][k] * w.y);
                     }
                     if (x.x > 0.0f && w.x > 0.0f) {
                         E.x = gw0 * w.x * e_scale;
@@ -275,31 +287,25 @@ __global__ void __launch_bounds__(kThreads) nlm_grad_kernel(GradArgs g) {
         // Phase 3: the vertical box of dL/dD onto this strip's extended rows.
         {
             const int e0 = strip * RPS;
-            float2 sum = f2(0.0f, 0.0f);
+            const float2* ec = et + e0 * kTX + col;
+            float2 sum = ec[-2 * S * kTX];
 #pragma unroll
-            for (int r = e0 - 2 * S; r <= e0; ++r)
-                if (r >= 0 && r < K::TY) sum = add2(sum, et[r * kTX + col]);
+            for (int r = 1 - 2 * S; r <= 0; ++r) sum = add2(sum, ec[r * kTX]);
+            float2* gc = gv + e0 * GVW + 2 * S + col;
 #pragma unroll
             for (int i = 0; i < RPS; ++i) {
-                const int ey = e0 + i;
-                if (ey >= EH) break;
-                if (i > 0) {
-                    if (ey < K::TY) sum = add2(sum, et[ey * kTX + col]);
-                    const int rs = ey - 2 * S - 1;
-                    if (rs >= 0 && rs < K::TY) sum = sub2(sum, et[rs * kTX + col]);
-                }
-                gv[ey * kTX + col] = sum;
+                if (e0 + i >= EH) break;
+                if (i > 0) sum = sub2(add2(sum, ec[i * kTX]), ec[(i - 2 * S - 1) * kTX]);
+                gc[i * GVW] = sum;
             }
         }
         __syncthreads();
         // Phase 4: the horizontal box, then the distance terms of both lanes at one extended cell.
         auto cell = [&](int ey, int ex, float* acc) {
-            float2 G = f2(0.0f, 0.0f);
+            const float2* gr = gv + ey * GVW + ex;  // padded columns ex .. ex + 2s hold lane pairs ex - 2s .. ex
+            float2 G = gr[2 * S];
 #pragma unroll
-            for (int t = 0; t <= 2 * S; ++t) {
-                const int cx = ex - t;
-                if (cx >= 0 && cx < kTX) G = add2(G, gv[ey * kTX + cx]);
-            }
+            for (int u = 2 * S - 1; u >= 0; --u) G = add2(G, gr[u]);
             if (G.x == 0.0f && G.y == 0.0f) return;
             const float* cc = ctr + ey * K::CSTRIDE + ex * C;
             const int i0 = (ey + dy0 + A) * nstride + (ex + dx0 + A) * C;
@@ -309,8 +315,8 @@ __global__ void __launch_bounds__(kThreads) nlm_grad_kernel(GradArgs g) {
                 const float term0 = G.x * (cc[c] - t0[i0 + c]);
                 const float term1 = G.y * (cc[c] - t1[i1 + c]);
                 acc[c] += term0 + term1;
-                add_to(g0 + i0 + c, -term0, atomic);
-                add_to(g1 + i1 + c, -term1, atomic);
+                add_to<kAtomic>(g0 + i0 + c, -term0);
+                add_to<kAtomic>(g1 + i1 + c, -term1);
             }
         };
 #pragma unroll
@@ -342,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) nlm_grad_kernel(GradArgs g) {
             for (int qx = -A; qx <= A; ++qx) {
                 const int id0 = 2 * ((p * side + qy + A) * side + qx + A);
                 // Each lane scatters into its own frame's tile, one cell per pixel: no atomics.
-                grad_step(nbr0, nbr1, gt0, gt1, qx, qy, -qx, -qy, id0, id0 + 1, negoff, false);
+                grad_step(std::false_type{}, nbr0, nbr1, gt0, gt1, qx, qy, -qx, -qy, id0, id0 + 1, negoff);
             }
         __syncthreads();
         flush_tile<C>(gt0, nstride, nrows, ncols, g.grad_window + a.slot_fwd[p] * a.frame_elems, X0 - S - A,
@@ -365,8 +371,8 @@ __global__ void __launch_bounds__(kThreads) nlm_grad_kernel(GradArgs g) {
             const int l1 = i + 1 < mid ? i + 1 : i + 2;
             float2 negoff = f2(0.0f, 0.0f);
             if (!FAST && a.spatial_lut) negoff = f2(-__ldg(a.spatial_lut + l0), -__ldg(a.spatial_lut + l1));
-            grad_step(nbr0, nbr0, gt0, gt0, l0 % side - A, l0 / side - A, l1 % side - A, l1 / side - A,
-                      spatial_base + i, spatial_base + i + 1, negoff, true);
+            grad_step(std::true_type{}, nbr0, nbr0, gt0, gt0, l0 % side - A, l0 / side - A, l1 % side - A, l1 / side - A,
+                      spatial_base + i, spatial_base + i + 1, negoff);
         }
     }
     __syncthreads();
@@ -445,7 +451,7 @@ cudaError_t launch_adjoint_s(const NlmLaunch& a, const RecordOut& rec, const Gra
                 attr = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         for (auto f : {nlm_grad_kernel<C, S, true>, nlm_grad_kernel<C, S, false>})
             if (attr == cudaSuccess)
-                attr = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+                attr = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 226 * 1024);
     });
     if (attr != cudaSuccess) return attr;
     if (a.fast) {
@@ -485,8 +491,9 @@ size_t nlm_backward_smem_bytes(int channels, int /*temporal_radius*/, int search
     const int cw = kTX + 2 * patch_radius, crows = ty + 2 * patch_radius;
     const int rps = (ty + 2 * patch_radius + 3) / 4;
     const size_t floats = (size_t)round_up4(crows * nbr_stride(cw, channels)) + 4 * (size_t)round_up4(nrows * nstride) +
-                          (size_t)(ty + 2 * patch_radius) * kHsStride + (size_t)2 * ty * kTX +
-                          (size_t)2 * 4 * rps * kTX;
+                          (size_t)(ty + 2 * patch_radius) * kHsStride +
+                          (size_t)2 * (2 * patch_radius + 1 + 4 * rps) * kTX +
+                          (size_t)2 * 4 * rps * (kTX + 4 * patch_radius);
     return floats * sizeof(float);
 }
 
