@@ -941,7 +941,7 @@ def run_nl4d(pushes: int, size: str) -> None:
                       "push_ms": [round(t, 3) for t in times]}))
 
 
-def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
+def run_nl4d_4k(pushes: int, auto: bool = False, wiener: bool = False) -> None:
     """NL4D on the 4K workload: 3840x2160 4:2:0 10-bit, 7-frame window (d=3, Auto estimation resolves
     to Chained), spatial radius 16, hard threshold 2.7 (lambda_ht 2.7, scale 1, pooled threshold and
     noise map off), motion at its defaults. Synthetic frames: the gratings/rectangles/texture base in
@@ -950,8 +950,9 @@ def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
 
     Default: luma and chroma in one engine with sigma pinned at 20 codes. With `auto`, both plane
     groups take their sigma from the automatic noise estimate (motion-compensated look-ahead) with the
-    luma noise map and the colour grain gains on, the reference's defaults. Prints the device time of
-    every push and the steady-state median as one JSON line."""
+    luma noise map and the colour grain gains on, the reference's defaults. With `wiener`, every pass
+    adds the empirical Wiener stage after the threshold. Prints the device time of every push and the
+    steady-state median as one JSON line."""
     import numpy as np
     import torch
 
@@ -966,7 +967,7 @@ def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
 
     def options(sig):
         return avd.Nl4dOptions(sigma=sig, temporal_radius=d, spatial_radius=16, lambda_ht=2.7, lambda_ht_scale=1.0,
-                               pooled_threshold=False, noise_map=sig is None)
+                               pooled_threshold=False, noise_map=sig is None, wiener=wiener)
 
     geo = avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt)
     o = options(None if auto else sigma)
@@ -1006,7 +1007,7 @@ def run_nl4d_4k(pushes: int, auto: bool = False) -> None:
     steady = times[warm:]
     ms = float(np.median(steady))
     what = ("sigma from the automatic noise estimate on both plane groups, noise map and colour gains on" if auto
-            else "sigma pinned at 20 codes")
+            else "sigma pinned at 20 codes") + (", Wiener stage" if wiener else "")
     print(json.dumps({"workload": "NL4D 3840x2160 4:2:0 10-bit luma+chroma, d=3 (Chained), spatial_radius 16, "
                                   "lambda_ht 2.7, plain threshold, " + what,
                       "ms_per_frame": round(ms, 3), "frames_per_s": round(1000.0 / ms, 2),
@@ -1255,6 +1256,7 @@ def main() -> None:
     ap.add_argument("--nl4d-size", default="1080", choices=["1080", "2160"])
     ap.add_argument("--nl4d-4k", type=int, default=0, metavar="PUSHES",
                     help="time PUSHES pushes of the 4K 4:2:0 10-bit NL4D workload (d=3) and exit")
+    ap.add_argument("--wiener", action="store_true", help="with --nl4d-4k: the Wiener stage after the threshold")
     ap.add_argument("--auto-sigma", action="store_true",
                     help="with --nl4d-4k: sigma from the automatic noise estimate on both plane groups")
     ap.add_argument("--adjoint", type=int, default=0, metavar="REPS",
@@ -1284,7 +1286,7 @@ def main() -> None:
     elif args.nl4d:
         run_nl4d(args.nl4d, args.nl4d_size)
     elif args.nl4d_4k:
-        run_nl4d_4k(args.nl4d_4k, auto=args.auto_sigma)
+        run_nl4d_4k(args.nl4d_4k, auto=args.auto_sigma, wiener=args.wiener)
     elif args.adjoint:
         run_adjoint(args.adjoint)
     elif args.batch:
