@@ -338,3 +338,20 @@ def test_exp_mirror_matches_oracle_bit_for_bit(lib, oracle):
     got = dy.cpu().numpy()
     want = oracle.exp_mirror(x)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_one_engine_runs_chroma_beside_luma():
+    """One engine cleaning luma and chroma runs each push's chroma pass on a second stream beside the
+    luma pass (it reads nothing the luma pass writes): every output plane equals, bit for bit, what a
+    luma-only engine and a chroma-only engine give over the same 9 frames of 4:2:0 u8."""
+    w, h = 256, 144
+    fmt = avd.SampleFormat.u8()
+    frames = clip(w, h, 9, chroma="420", seed=41)
+    geo = avd.Geometry(w, h, avd.ChromaLayout.YUV420, fmt, fmt)
+    both = Runner(avd.EngineSpec.nlmeans(nlm(1, 5, 2, 8.0), nlm(1, 5, 2, 5.0), geo)).run(frames)
+    luma = Runner(avd.EngineSpec.nlmeans(nlm(1, 5, 2, 8.0), None, geo)).run(frames)
+    chroma = Runner(avd.EngineSpec.nlmeans(None, nlm(1, 5, 2, 5.0), geo)).run(frames)
+    assert len(both) == len(luma) == len(chroma) == 9
+    for b, l, c in zip(both, luma, chroma):
+        assert np.array_equal(b[0], l[0])
+        assert np.array_equal(b[1], c[1]) and np.array_equal(b[2], c[2])
