@@ -160,6 +160,11 @@ class AvdCollabPass(C.Structure):
                [(n, f32) for n in ("c_min", "lambda_ht", "accum_scale", "pool_ratio")] + [("wiener", u32)]
 
 
+class AvdBatchIngest(C.Structure):
+    _fields_ = [(n, u64) for n in ("plane0", "plane1", "frame")] + [(n, u32) for n in ("width", "height", "channels",
+                                                                                       "bits")]
+
+
 class AvdCollabAdjoint(C.Structure):
     _fields_ = [(n, u64) for n in ("grad_accum", "grad_wsum", "grad_ring", "grad_sigma_refs")]
 
@@ -256,6 +261,8 @@ PROTOTYPES: dict[str, tuple] = {
     "avd_collab_pass": (C.c_int, [_P(AvdCollabPass), C.c_void_p]),
     "avd_collab_member_bytes": (u64, [u32, u32]),
     "avd_collab_refs": (u64, [u32, u32]),
+    "avd_batch_ingest_scratch_bytes": (u64, [C.c_size_t]),
+    "avd_batch_ingest": (C.c_int, [_P(AvdBatchIngest), C.c_size_t, u64, C.c_void_p]),
     "avd_collab_adjoint": (C.c_int, [_P(AvdCollabPass), _P(AvdCollabAdjoint), C.c_void_p]),
     "avd_dct_noise_profile": (None, [f32, _P(f32)]),
     "avd_kaiser_window": (None, [f32, _P(f32)]),

@@ -123,4 +123,64 @@ AvdStatus avd_batch_submit(const AvdBatchJob* jobs, size_t n_jobs, uint32_t chan
     return AVD_OK;
 }
 
+namespace {
+
+struct IngestLayout {
+    size_t items, prefix, total;
+};
+
+IngestLayout ingest_layout(size_t n) {
+    IngestLayout l{};
+    l.items = 0;
+    l.prefix = align16(n * sizeof(avd::BatchIngestItem));
+    l.total = align16(l.prefix + (n + 1) * sizeof(int64_t));
+    return l;
+}
+
+}  // namespace
+
+uint64_t avd_batch_ingest_scratch_bytes(size_t n_items) { return ingest_layout(n_items).total; }
+
+AvdStatus avd_batch_ingest(const AvdBatchIngest* items, size_t n_items, uint64_t scratch, void* stream) {
+    if (!items || !scratch) return fail(AVD_ERR_NULL_ARG, "batch ingest: null items or scratch");
+    if (n_items == 0) return AVD_OK;
+    if (n_items > static_cast<size_t>(1) << 30) return fail(AVD_ERR_INVALID_OPTIONS, "batch ingest: too many items");
+    const IngestLayout L = ingest_layout(n_items);
+    std::vector<unsigned char> host(L.total, 0);
+    auto* table = reinterpret_cast<avd::BatchIngestItem*>(host.data() + L.items);
+    auto* prefix = reinterpret_cast<int64_t*>(host.data() + L.prefix);
+    int64_t words = 0;
+    for (size_t i = 0; i < n_items; ++i) {
+        const AvdBatchIngest& b = items[i];
+        if (!b.plane0 || !b.frame || (b.channels == 2 && !b.plane1))
+            return fail(AVD_ERR_NULL_ARG, "batch ingest: item " + std::to_string(i) + " has a null buffer");
+        if (b.channels < 1 || b.channels > 2 || b.width == 0 || b.height == 0)
+            return fail(AVD_ERR_INVALID_GEOMETRY, "batch ingest: item " + std::to_string(i) + " has a bad geometry");
+        if (b.bits < 8 || b.bits > 16)
+            return fail(AVD_ERR_INVALID_OPTIONS, "batch ingest: item " + std::to_string(i) + " has bits outside 8..16");
+        avd::BatchIngestItem& t = table[i];
+        t.plane0 = reinterpret_cast<const uint32_t*>(b.plane0);
+        t.plane1 = reinterpret_cast<const uint32_t*>(b.plane1);
+        t.dst = reinterpret_cast<float*>(b.frame);
+        t.pixels = static_cast<int64_t>(b.width) * b.height;
+        t.channels = static_cast<int>(b.channels);
+        t.samples_per_word = b.bits == 8 ? 4 : 2;
+        t.max_value = static_cast<float>((1u << b.bits) - 1u);
+        prefix[i] = words;
+        words += (t.pixels + t.samples_per_word - 1) / t.samples_per_word;
+    }
+    prefix[n_items] = words;
+    auto s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(reinterpret_cast<void*>(scratch), host.data(), L.total, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        auto* dev = reinterpret_cast<unsigned char*>(scratch);
+        e = avd::launch_batch_ingest(reinterpret_cast<const avd::BatchIngestItem*>(dev + L.items),
+                                     reinterpret_cast<const int64_t*>(dev + L.prefix), static_cast<int>(n_items), words,
+                                     s);
+    }
+    // The staging copy above is pageable: cudaMemcpyAsync has consumed `host` before returning.
+    if (e != cudaSuccess) return fail(AVD_ERR_GPU, std::string("batch ingest: ") + cudaGetErrorString(e));
+    return AVD_OK;
+}
+
 }  // extern "C"

@@ -46,6 +46,34 @@ __global__ void ingest_words_kernel(const uint32_t* __restrict__ p0, const uint3
     }
 }
 
+// Many frames of mixed depth and size in one launch (no counterpart in the reference, which ingests
+// one frame per launch): each thread takes global words, finds its frame by a binary search of the
+// word prefix, and converts as ingest_words_kernel does, the same correctly rounded division.
+__global__ void batch_ingest_kernel(const BatchIngestItem* __restrict__ items, const int64_t* __restrict__ prefix,
+                                    int n, int64_t total) {
+    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < total; w += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(prefix + mid) <= w) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchIngestItem& it = items[lo];
+        const int64_t local = w - __ldg(prefix + lo);
+        const int spw = it.samples_per_word, bits = 32 / spw;
+        const uint32_t mask = (1u << bits) - 1u;
+        const uint32_t w0 = __ldg(it.plane0 + local);
+        const uint32_t w1 = it.channels > 1 ? __ldg(it.plane1 + local) : 0u;
+        for (int lane = 0; lane < spw; ++lane) {
+            const int64_t p = local * spw + lane;
+            if (p >= it.pixels) break;
+            it.dst[p * it.channels] = __fdiv_rn(static_cast<float>((w0 >> (lane * bits)) & mask), it.max_value);
+            if (it.channels > 1)
+                it.dst[p * 2 + 1] = __fdiv_rn(static_cast<float>((w1 >> (lane * bits)) & mask), it.max_value);
+        }
+    }
+}
+
 // av-denoise-core/src/engine/kernels.rs:64-90.
 template <int C>
 __global__ void ingest_f32_kernel(const float* __restrict__ p0, const float* __restrict__ p1, float* __restrict__ slot,
@@ -115,6 +143,13 @@ cudaError_t launch_ingest(const void* plane0, const void* plane1, float* slot, i
         if (channels == 1) ingest_words_kernel<2, 1><<<g, kBlock, 0, stream>>>(w0, w1, slot, pixels, fmt.max_value);
         else ingest_words_kernel<2, 2><<<g, kBlock, 0, stream>>>(w0, w1, slot, pixels, fmt.max_value);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_ingest(const BatchIngestItem* items, const int64_t* word_prefix, int n, int64_t total_words,
+                                cudaStream_t stream) {
+    if (n <= 0 || total_words <= 0) return cudaSuccess;
+    batch_ingest_kernel<<<grid_for(total_words), kBlock, 0, stream>>>(items, word_prefix, n, total_words);
     return cudaGetLastError();
 }
 

@@ -18,6 +18,22 @@ struct PlaneFormat {
 
 // av-denoise-core/src/engine/kernels.rs:25-90 (`ingest_words`, `ingest_f32`): planes -> one
 // interleaved f32 ring slot.
+// One frame of a batched ingest: `channels` word planes (plane1 for the second channel) of
+// `pixels` samples packed `samples_per_word` to a 32-bit word, normalised by `max_value` into the
+// interleaved f32 frame `dst`.
+struct BatchIngestItem {
+    const uint32_t* plane0;
+    const uint32_t* plane1;
+    float* dst;
+    int64_t pixels;
+    int channels, samples_per_word;
+    float max_value;
+};
+// Every item's words in one launch; `word_prefix[i]` is the first global word of item i
+// (word_prefix[n] the total), both tables in device memory.
+cudaError_t launch_batch_ingest(const BatchIngestItem* items, const int64_t* word_prefix, int n, int64_t total_words,
+                                cudaStream_t stream);
+
 cudaError_t launch_ingest(const void* plane0, const void* plane1, float* slot, int64_t pixels, int channels,
                           PlaneFormat fmt, float bias, cudaStream_t stream);
 

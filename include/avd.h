@@ -816,6 +816,23 @@ AVD_API uint64_t avd_batch_scratch_bytes(size_t n_jobs, uint32_t search_radius);
 AVD_API AvdStatus avd_batch_submit(const AvdBatchJob* jobs, size_t n_jobs, uint32_t channels, uint32_t search_radius,
                                    uint32_t patch_radius, float self_weight, uint64_t scratch, void* stream);
 
+/* No counterpart in the reference (it ingests one frame per launch). The word planes of many frames
+ * of mixed size and bit depth normalised into f32 frames by one launch, so a batch of clips of 8-,
+ * 10- and 12-bit sources feeds avd_batch_submit without a launch per frame. Each item: `channels`
+ * planes (plane1 for the second channel), samples of `bits` bits (8: four to a 32-bit word; 9..16:
+ * two), normalised by 2^bits - 1 exactly as the engine's ingest does (a correctly rounded
+ * division), interleaved into `frame` (width x height x channels f32). */
+typedef struct AvdBatchIngest {
+    uint64_t plane0, plane1, frame;
+    uint32_t width, height, channels, bits;
+} AvdBatchIngest;
+
+/* The scratch one batched ingest of `n_items` items needs (its item table and word prefix). */
+AVD_API uint64_t avd_batch_ingest_scratch_bytes(size_t n_items);
+
+/* Queues the ingest on `stream`: one copy of its table into `scratch`, then one launch. */
+AVD_API AvdStatus avd_batch_ingest(const AvdBatchIngest* items, size_t n_items, uint64_t scratch, void* stream);
+
 /* ---- allocation-free entry point ----------------------------------------------------------- */
 
 /* No counterpart in the reference. One fast-variant NLMeans output frame for callers that cannot

@@ -7,6 +7,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from conftest import avd
+
 pytestmark = pytest.mark.gpu
 
 
@@ -79,3 +81,42 @@ def test_batch_equals_frames_alone(lib, oracle, c, a, s, offset):
     idx = [i for i, cl in enumerate(clips) if cl[0] is frames and cl[1] == centre][0]
     got = outs[idx].cpu().numpy().reshape(ref.shape)
     assert np.abs(got - ref).max() < 2e-5
+
+
+def test_batch_ingest_of_mixed_depths():
+    """`avd_batch_ingest`: frames of 8-, 10- and 12-bit words, one and two channels, odd sizes, in one
+    launch; every f32 sample equals code / (2^bits - 1) correctly rounded (the engine's ingest), on two
+    calls in a row."""
+    import ctypes as C
+
+    import torch
+
+    from av_denoise_b200 import _abi
+
+    lib = avd.load()
+    rng = np.random.default_rng(12)
+    shapes = [(37, 21, 1, 8), (64, 9, 2, 10), (33, 17, 1, 12), (8, 8, 2, 8), (91, 45, 2, 12), (15, 3, 1, 10)]
+    keep, items, want = [], [], []
+    for w, h, ch, bits in shapes:
+        codes = [rng.integers(0, 2 ** bits, w * h) for _ in range(ch)]
+        dt = np.uint8 if bits == 8 else np.uint16
+        per = 4 if bits == 8 else 2
+        planes = []
+        for c in codes:
+            raw = c.astype(dt)
+            raw = np.concatenate([raw, np.zeros((-raw.size) % per, dt)])
+            planes.append(torch.from_numpy(raw.view(np.int32).copy()).cuda())
+        frame = torch.full((w * h * ch,), -1.0, dtype=torch.float32, device="cuda")
+        keep += planes + [frame]
+        items.append(_abi.AvdBatchIngest(planes[0].data_ptr(), planes[1].data_ptr() if ch == 2 else 0,
+                                         frame.data_ptr(), w, h, ch, bits))
+        want.append((np.stack(codes, -1).astype(np.float32) / np.float32(2 ** bits - 1)).reshape(-1))
+    arr = (_abi.AvdBatchIngest * len(items))(*items)
+    scratch = torch.empty(lib.avd_batch_ingest_scratch_bytes(len(items)) // 4 + 1, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        st = lib.avd_batch_ingest(arr, len(items), scratch.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert st == 0, lib.avd_last_error().decode()
+        torch.cuda.synchronize()
+        frames = [t for i, t in enumerate(keep) if t.dtype == torch.float32]
+        for got, exp in zip(frames, want):
+            assert np.array_equal(got.cpu().numpy().view(np.uint32), exp.view(np.uint32))
